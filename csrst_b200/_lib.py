@@ -1,0 +1,108 @@
+"""ctypes binding of libcsrst_gpu.so (the C ABI in include/csrst.h).
+
+The library is the product: there is no CPU path behind these calls.  If
+the shared library is missing or cannot be loaded, every call raises.
+"""
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+SO = HERE / "libcsrst_gpu.so"
+
+D = C.POINTER(C.c_double)
+I = C.POINTER(C.c_int)
+U8 = C.POINTER(C.c_uint8)
+
+
+class Config(C.Structure):
+    """csrst_config: run set-up mirroring src/main.cpp:111-136."""
+    _fields_ = [("Nx", C.c_int), ("Ny", C.c_int), ("shape_order", C.c_int), ("flags", C.c_int),
+                ("length_before", C.c_double), ("length_after", C.c_double),
+                ("width", C.c_double), ("phi_deg", C.c_double), ("ekin_mev", C.c_double),
+                ("bz", C.c_double), ("dt", C.c_double), ("charge_mass", C.c_double)]
+
+
+ERRORS = {0: "ok", -1: "invalid argument", -2: "CUDA error", -3: "geometry",
+          -4: "no particles", -5: "window fit", -6: "window move", -7: "crossings",
+          -8: "window wall"}
+
+
+class CsrstError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"csrst error {code} ({ERRORS.get(code, '?')}): {msg}")
+        self.code = code
+
+
+_LIB = None
+
+
+def lib():
+    """Loads the CUDA library once; raises if it is absent."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not SO.exists():
+        raise RuntimeError(f"{SO} is missing: build it with `python -m csrst_b200.build`")
+    L = C.CDLL(str(SO))
+    P = C.c_void_p
+    sig = {
+        "csrst_create": ([C.POINTER(Config), C.POINTER(P)], C.c_int),
+        "csrst_destroy": ([P], C.c_int),
+        "csrst_get_error": ([P, C.c_char_p, C.c_size_t], C.c_int),
+        "csrst_stream": ([P], C.c_void_p),
+        "csrst_sync": ([P], C.c_int),
+        "csrst_get_info": ([P, D], C.c_int),
+        "csrst_get_geometry": ([P, U8, D, C.c_long, C.POINTER(C.c_long)], C.c_int),
+        "csrst_set_static_fields": ([P, D, D, D, D], C.c_int),
+        "csrst_get_static_fields": ([P, D, D, D, D], C.c_int),
+        "csrst_reset_outside": ([P], C.c_int),
+        "csrst_load_particles": ([P, D, D, D, D, D, C.c_size_t], C.c_int),
+        "csrst_get_particles": ([P, D, D, D, D], C.c_int),
+        "csrst_get_old_positions": ([P, D, D], C.c_int),
+        "csrst_get_window": ([P, I, D, I], C.c_int),
+        "csrst_get_window_field": ([P, C.c_int, D], C.c_int),
+        "csrst_push": ([P, C.c_int], C.c_int),
+        "csrst_drift": ([P, C.c_double], C.c_int),
+        "csrst_half_h": ([P], C.c_int),
+        "csrst_update_e": ([P, C.c_int], C.c_int),
+        "csrst_move_window": ([P], C.c_int),
+        "csrst_step_first": ([P], C.c_int),
+        "csrst_step_second": ([P], C.c_int),
+        "csrst_step": ([P, C.c_int], C.c_int),
+        "csrst_diag_moments": ([P, D], C.c_int),
+        "csrst_diag_wake": ([P, D, C.c_int], C.c_int),
+        "csrst_gather": ([C.c_int, C.c_int, D, C.c_int, C.c_int, D, D, D, D, C.c_size_t, D], C.c_int),
+        "csrst_deposit": ([C.c_int, C.c_int, D, D, D, D, D, C.c_size_t, D, D, C.c_double, C.c_int,
+                           C.c_int, C.c_int, C.c_int, C.c_double, D], C.c_int),
+        "csrst_charge_diff": ([C.c_int, D, D, D, D, D, C.c_size_t, D, D, C.c_int, C.c_int, C.c_int,
+                               C.c_int, C.c_double, D], C.c_int),
+    }
+    for name, (args, res) in sig.items():
+        f = getattr(L, name)
+        f.argtypes = args
+        f.restype = res
+    _LIB = L
+    return L
+
+
+def exported_symbols():
+    """Names of the entry points the binding declares (all must be exported)."""
+    lib()
+    return [n for n in dir(_LIB) if n.startswith("csrst_")]
+
+
+def ptr(a):
+    return a.ctypes.data_as(D)
+
+
+def f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def check(code, handle=None):
+    if code != 0:
+        buf = C.create_string_buffer(512)
+        lib().csrst_get_error(handle, buf, 512)
+        raise CsrstError(code, buf.value.decode(errors="replace"))

@@ -1,0 +1,778 @@
+// C ABI of libcsrst_gpu.so (declared in include/csrst.h): the handle, device
+// memory, the order of kernel launches for one time step and its CUDA graph.
+#include <cub/cub.cuh>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/csrst.h"
+#include "kernels.cuh"
+
+namespace csrst {
+
+__global__ void k_gather_perm(const long long *perm, long long n, const double *a, double *b) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i < n) b[i] = a[perm[i]];
+}
+__global__ void k_sort_keys(const double *x, const double *y, long long n, const WinState *ws,
+                            double h1, unsigned long long *kx, long long *idx) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  kx[i] = (unsigned long long)dbl_ord(x[i]) ^ 0x8000000000000000ull;
+  idx[i] = i;
+}
+// y slice of the window (PartBunch::sortParticles, PartBunch.cpp:1826-1829)
+__global__ void k_slice_keys(const double *y, const long long *idx, long long n, const WinState *ws,
+                             double h1, unsigned int *ks) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double mn1 = ord_dbl(ws->bb[ws->cur][1]);
+  const int lp2 = (int)floor((mn1 - ws->mo1) / h1);
+  ks[i] = (unsigned int)((int)floor((y[idx[i]] - ws->mo1) / h1) - lp2);
+}
+__global__ void k_acc_to_plane(const unsigned long long *acc, Plane p, int L0, int L1, double inv) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= L0 * L1) return;
+  p.at(k % L0, k / L0) = (double)(long long)acc[k] * inv;
+}
+__global__ void k_set_pending_old(const double *x, const double *y, const double *px, const double *py,
+                                  long long n, double half, int pending, double *ox, double *oy) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double a = x[i], b = y[i];
+  if (pending) {
+    const double r = inv_gamma(px[i], py[i]);
+    a = a + (-(half * px[i] * r));
+    b = b + (-(half * py[i] * r));
+  }
+  ox[i] = a; oy[i] = b;
+}
+
+}  // namespace csrst
+
+using namespace csrst;
+
+namespace {
+
+enum BBoxState { kBBInvalid, kBBValid, kBBValidIfPending };
+
+static std::string g_create_error;
+
+}  // namespace
+
+struct csrst_handle {
+  csrst_config cfg{};
+  int order = 0;
+  cudaStream_t s = nullptr;
+  BendDev b{};
+  double dt = 0, half = 0, chh = 0, shh = 0, bwidth = 0;
+  int pitch = 0;
+  double *Ex = nullptr, *Ey = nullptr, *Hx = nullptr, *Hy = nullptr;
+  uint8_t *mask = nullptr;
+  CutCellDev *cells = nullptr;
+  int ncells = 0;
+  int *cutidx = nullptr;
+  // window
+  int L0 = 0, L1 = 0, wpitch = 0;
+  double *win = nullptr;  // 6 planes
+  double *scratch = nullptr;
+  unsigned long long *acc = nullptr;  // 2 * L0 * L1
+  double acc_scale = 0;
+  bool acc_fresh[2] = {false, false};
+  WinState *ws = nullptr;
+  // particles
+  long long n = 0;
+  double *x = nullptr, *y = nullptr, *px = nullptr, *py = nullptr, *q = nullptr;
+  double *ox = nullptr, *oy = nullptr;
+  bool pending = false;
+  BBoxState bb = kBBInvalid;
+  int push_grid = 0;
+  // diagnostics scratch
+  double *dscratch = nullptr, *dmean = nullptr, *dout = nullptr;
+  // graph of one step
+  cudaGraphExec_t graph = nullptr;
+  std::string err;
+};
+
+namespace {
+
+int fail(csrst_handle *h, int code, const std::string &msg) {
+  if (h) h->err = msg;
+  else g_create_error = msg;
+  return code;
+}
+
+int cuda_fail(csrst_handle *h, cudaError_t e, const char *where) {
+  return fail(h, CSRST_E_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+#define CK(call)                                              \
+  do {                                                        \
+    cudaError_t e_ = (call);                                  \
+    if (e_ != cudaSuccess) return cuda_fail(h, e_, #call);    \
+  } while (0)
+
+Plane plane(double *p, int pitch) { return Plane{p, pitch}; }
+
+Plane wplane(const csrst_handle *h, int k) {
+  return Plane{h->win + (size_t)k * h->wpitch * (h->L1 + 2), h->wpitch};
+}
+
+FieldArgs field_args(csrst_handle *h, int comp) {
+  FieldArgs a{};
+  const size_t ps = (size_t)h->pitch * (h->b.Ny + 2);
+  a.Ex = plane(h->Ex, h->pitch); a.Ey = plane(h->Ey, h->pitch);
+  a.Hx = plane(h->Hx, h->pitch); a.Hy = plane(h->Hy, h->pitch);
+  (void)ps;
+  a.mask = h->mask;
+  a.Nx = h->b.Nx; a.Ny = h->b.Ny;
+  a.mEx = wplane(h, 0); a.mEy = wplane(h, 1); a.mHx = wplane(h, 2); a.mHy = wplane(h, 3);
+  a.mJx = wplane(h, 4); a.mJy = wplane(h, 5);
+  a.L0 = h->L0; a.L1 = h->L1;
+  a.cells = h->cells; a.ncells = h->ncells;
+  a.ws = h->ws;
+  a.acc = h->acc ? h->acc + (size_t)(comp == 1 ? 1 : 0) * h->L0 * h->L1 : nullptr;
+  a.acc_inv = h->acc_scale > 0 ? 1.0 / h->acc_scale : 0.0;
+  const double h0 = h->b.hr0, h1 = h->b.hr1, dt = h->dt;
+  // TETMSolver.hh:121-125 and TETMSolver.cpp:87-127
+  const double etax = kC * dt / h0, etay = kC * dt / h1;
+  const double Z0 = std::sqrt(kMu0 / kEps0);
+  a.chx = 0.5 * etax / Z0; a.chy = 0.5 * etay / Z0;
+  a.kex = etay * Z0; a.key = etax * Z0;
+  a.dteps = kC * dt * Z0;
+  a.mhx = -0.5 * (dt / (h0 * kMu0)); a.mhy = +0.5 * (dt / (h1 * kMu0));
+  a.de = dt / kEps0;
+  a.h0 = h0; a.h1 = h1;
+  return a;
+}
+
+// Host copy of the Bend set-up (Bend ctor and Bend::Init, Bend.cpp:60-124).
+void bend_setup(csrst_handle *h) {
+  const csrst_config &c = h->cfg;
+  BendDev &b = h->b;
+  const double mass = 0.511e6, ekin = c.ekin_mev * 1e6;
+  b.Nx = c.Nx; b.Ny = c.Ny; b.Lb = c.length_before; b.La = c.length_after; b.w = c.width;
+  if (std::abs(c.bz) > 1e-8) {
+    b.R = std::sqrt(ekin * ekin + 2. * ekin * mass) / (kC * std::abs(c.bz));
+    b.phi = -c.bz / std::abs(c.bz) * std::abs(c.phi_deg) * kPi / 180.;
+  } else {
+    b.R = 9999999.9;
+    b.phi = 0.0;
+  }
+  const double cosphi = std::cos(b.phi), sinphi = std::abs(std::sin(b.phi));
+  double dl, dw;
+  if (std::abs(c.bz) > 1e-8) {
+    dl = (c.length_before + c.length_after * cosphi + (b.R + 0.5 * c.width) * sinphi);
+    dw = ((b.R - 0.5 * c.width) * (1 - cosphi) + c.width + c.length_after * sinphi);
+  } else {
+    dl = c.length_after + c.length_before;
+    dw = c.width;
+  }
+  b.hr0 = dl / (c.Nx - 2);
+  b.hr1 = dw / (c.Ny - 2);
+  if (c.bz <= 0.0) {
+    b.org0 = 0 - b.hr0; b.org1 = (c.width - dw) - b.hr1;
+    b.cen0 = c.length_before; b.cen1 = 0.5 * c.width - b.R;
+  } else {
+    b.org0 = -b.hr0; b.org1 = -b.hr1;
+    b.cen0 = c.length_before; b.cen1 = 0.5 * c.width + b.R;
+  }
+  b.cphi = std::cos(b.phi);
+  b.sphi = std::sin(b.phi);
+  h->dt = c.dt > 0 ? c.dt : b.hr0 / kC;
+  h->half = 0.5 * h->dt * kC;
+  h->chh = std::cos(0.5 * b.phi);
+  h->shh = std::sin(0.5 * b.phi);
+  h->bwidth = 2 * b.R * std::abs(h->shh);
+}
+
+void free_particles(csrst_handle *h) {
+  cudaFree(h->x); cudaFree(h->y); cudaFree(h->px); cudaFree(h->py); cudaFree(h->q);
+  cudaFree(h->ox); cudaFree(h->oy);
+  h->x = h->y = h->px = h->py = h->q = h->ox = h->oy = nullptr;
+  cudaFree(h->win); cudaFree(h->scratch); cudaFree(h->acc);
+  h->win = h->scratch = nullptr; h->acc = nullptr;
+  if (h->graph) { cudaGraphExecDestroy(h->graph); h->graph = nullptr; }
+  h->n = 0;
+}
+
+int check_err(csrst_handle *h) {
+  int e = 0;
+  CK(cudaMemcpyAsync(&e, &h->ws->err, sizeof(int), cudaMemcpyDeviceToHost, h->s));
+  CK(cudaStreamSynchronize(h->s));
+  if (e) {
+    const char *m = e == kErrWindowFit ? "bunch no longer fits the window"
+                  : e == kErrWindowMove ? "window move out of range"
+                  : e == kErrCrossings ? "too many cell-border crossings in one push"
+                  : e == kErrWindowWall ? "window touches a non-inside cell"
+                  : "device error";
+    return fail(h, e, m);
+  }
+  return CSRST_OK;
+}
+
+PushArgs push_args(csrst_handle *h, int jcomp) {
+  PushArgs a{};
+  a.x = h->x; a.y = h->y; a.px = h->px; a.py = h->py; a.q = h->q; a.n = h->n;
+  a.ws = h->ws;
+  a.mEx = wplane(h, 0).p; a.mEy = wplane(h, 1).p; a.mHx = wplane(h, 2).p; a.mHy = wplane(h, 3).p;
+  a.wpitch = h->wpitch;
+  a.acc = h->acc + (size_t)jcomp * h->L0 * h->L1;
+  a.acc_scale = h->acc_scale;
+  a.jcomp = jcomp;
+  a.pending = h->pending ? 1 : 0;
+  a.half = h->half;
+  a.fact1 = h->half * h->cfg.charge_mass;
+  a.fact2 = a.fact1 * kC;
+  a.h0 = h->b.hr0; a.h1 = h->b.hr1; a.dt = h->dt;
+  a.bz = h->cfg.bz; a.Lb = h->b.Lb; a.hw = 0.5 * h->b.w;
+  a.chh = h->chh; a.shh = h->shh; a.bwidth = h->bwidth;
+  a.use_smem = 1;
+  return a;
+}
+
+// PartBunch::push_particles on the device (no host synchronisation).
+int push_async(csrst_handle *h, int jcomp) {
+  const bool bb_ok = h->bb == kBBValid || (h->bb == kBBValidIfPending && h->pending);
+  if (h->cfg.flags & 1) {  // keep oldR for inspection
+    k_set_pending_old<<<(unsigned)((h->n + 255) / 256), 256, 0, h->s>>>(h->x, h->y, h->px, h->py, h->n,
+                                                                       h->half, h->pending, h->ox, h->oy);
+  }
+  if (!bb_ok) launch_bbox_next(h->x, h->y, h->px, h->py, h->n, h->half, h->pending, h->ws, h->s);
+  launch_push_prep(h->ws, h->b.hr0, h->b.hr1, h->order, h->s);
+  launch_push(push_args(h, jcomp), h->order, h->L0, h->L1, h->push_grid, h->s);
+  launch_global_bounds(h->ws, h->b.hr0, h->b.hr1, h->s);
+  h->pending = false;
+  h->bb = kBBValidIfPending;
+  h->acc_fresh[jcomp] = true;
+  return CSRST_OK;
+}
+
+// drift(-dt/2) right after a push: defer it into the next push.
+void drift_back(csrst_handle *h) {
+  if (h->pending) {  // materialise the older one first
+    launch_drift(h->x, h->y, h->px, h->py, h->n, (-0.5 * h->dt) * kC, h->s);
+    h->bb = kBBInvalid;
+  }
+  h->pending = true;
+  if (h->bb == kBBValidIfPending) h->bb = kBBValid;
+}
+
+void materialise(csrst_handle *h) {
+  if (!h->pending) return;
+  launch_drift(h->x, h->y, h->px, h->py, h->n, (-0.5 * h->dt) * kC, h->s);
+  h->pending = false;
+  // the stored box of the next gather positions stays exact: R_true + h v(P)
+  // has the same bits whether the drift was deferred or applied
+}
+
+void half_h_async(csrst_handle *h) {
+  FieldArgs a = field_args(h, 0);
+  launch_half_h(a, h->s);
+  launch_exchange(a, 0, h->s);
+}
+
+void update_e_async(csrst_handle *h, int comp) {
+  FieldArgs a = field_args(h, comp);
+  launch_update_e(a, comp, h->s);
+  launch_exchange(a, comp == 0 ? 1 : 2, h->s);
+  h->acc_fresh[comp] = false;
+}
+
+void move_async(csrst_handle *h) {
+  launch_move(field_args(h, 0), h->scratch, h->b.hr0, h->b.hr1, h->s);
+}
+
+// TETMSolver::updateField_firstStep + updateField_secondStep + moveMesh.
+void step_async(csrst_handle *h) {
+  push_async(h, 0);
+  half_h_async(h);
+  update_e_async(h, 0);
+  half_h_async(h);
+  drift_back(h);
+  push_async(h, 1);
+  update_e_async(h, 1);
+  drift_back(h);
+  move_async(h);
+}
+
+int need_bunch(csrst_handle *h) {
+  if (!h) return CSRST_E_ARG;
+  if (h->n <= 0 || !h->win) return fail(h, CSRST_E_NO_PARTICLES, "no bunch loaded");
+  return CSRST_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int csrst_create(const csrst_config *cfg, csrst_handle **out) {
+  if (!cfg || !out) return fail(nullptr, CSRST_E_ARG, "null argument");
+  *out = nullptr;
+  if (cfg->Nx < 8 || cfg->Ny < 8 || cfg->shape_order < 0 || cfg->shape_order > 2 || !(cfg->width > 0))
+    return fail(nullptr, CSRST_E_ARG, "invalid configuration");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+    return fail(nullptr, CSRST_E_CUDA, "no CUDA device");
+  csrst_handle *h = new csrst_handle;
+  h->cfg = *cfg;
+  h->order = cfg->shape_order;
+  bend_setup(h);
+  auto bad = [&](cudaError_t e, const char *w) {
+    g_create_error = std::string(w) + ": " + cudaGetErrorString(e);
+    csrst_destroy(h);
+    return CSRST_E_CUDA;
+  };
+  cudaError_t e;
+  if ((e = cudaStreamCreateWithFlags(&h->s, cudaStreamNonBlocking)) != cudaSuccess) return bad(e, "stream");
+  const int Nx = cfg->Nx, Ny = cfg->Ny;
+  h->pitch = ((Nx + 2 + 31) / 32) * 32;
+  const size_t ps = (size_t)h->pitch * (Ny + 2);
+  double **planes[4] = {&h->Ex, &h->Ey, &h->Hx, &h->Hy};
+  for (double **p : planes) {
+    if ((e = cudaMalloc(p, ps * sizeof(double))) != cudaSuccess) return bad(e, "static fields");
+    if ((e = cudaMemsetAsync(*p, 0, ps * sizeof(double), h->s)) != cudaSuccess) return bad(e, "memset");
+  }
+  if ((e = cudaMalloc(&h->mask, (size_t)Nx * Ny)) != cudaSuccess) return bad(e, "mask");
+  if ((e = cudaMalloc(&h->ws, sizeof(WinState))) != cudaSuccess) return bad(e, "window state");
+  if ((e = cudaMemsetAsync(h->ws, 0, sizeof(WinState), h->s)) != cudaSuccess) return bad(e, "memset");
+  const size_t nd = moments_scratch_doubles();
+  if ((e = cudaMalloc(&h->dscratch, nd * sizeof(double))) != cudaSuccess) return bad(e, "diag");
+  if ((e = cudaMalloc(&h->dmean, 8 * sizeof(double))) != cudaSuccess) return bad(e, "diag");
+  if ((e = cudaMalloc(&h->dout, 32 * sizeof(double))) != cudaSuccess) return bad(e, "diag");
+  int rc = build_geometry(h->b, h->mask, &h->cells, &h->ncells, &h->cutidx, h->s);
+  if (rc != kOk) {
+    g_create_error = rc == kErrGeometry ? "bend geometry: the reference asserts for this configuration"
+                                        : "geometry build failed";
+    csrst_destroy(h);
+    return rc;
+  }
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  h->push_grid = 2 * sms;
+  *out = h;
+  return CSRST_OK;
+}
+
+int csrst_destroy(csrst_handle *h) {
+  if (!h) return CSRST_OK;
+  if (h->s) cudaStreamSynchronize(h->s);
+  free_particles(h);
+  cudaFree(h->Ex); cudaFree(h->Ey); cudaFree(h->Hx); cudaFree(h->Hy);
+  cudaFree(h->mask); cudaFree(h->cells); cudaFree(h->cutidx); cudaFree(h->ws);
+  cudaFree(h->dscratch); cudaFree(h->dmean); cudaFree(h->dout);
+  if (h->s) cudaStreamDestroy(h->s);
+  delete h;
+  return CSRST_OK;
+}
+
+int csrst_get_error(const csrst_handle *h, char *buf, size_t len) {
+  if (!buf || len == 0) return CSRST_E_ARG;
+  const std::string &m = h ? h->err : g_create_error;
+  std::snprintf(buf, len, "%s", m.c_str());
+  return CSRST_OK;
+}
+
+void *csrst_stream(csrst_handle *h) { return h ? (void *)h->s : nullptr; }
+
+int csrst_sync(csrst_handle *h) {
+  if (!h) return CSRST_E_ARG;
+  CK(cudaStreamSynchronize(h->s));
+  CK(cudaGetLastError());
+  return check_err(h);
+}
+
+int csrst_get_info(csrst_handle *h, double *info8) {
+  if (!h || !info8) return CSRST_E_ARG;
+  double v[8] = {h->b.hr0, h->b.hr1, h->b.org0, h->b.org1, h->dt, h->acc_scale, (double)h->ncells,
+                 (double)h->wpitch};
+  std::memcpy(info8, v, sizeof(v));
+  return CSRST_OK;
+}
+
+int csrst_get_geometry(csrst_handle *h, uint8_t *inside, double *cells, long max_cells, long *ncells) {
+  if (!h) return CSRST_E_ARG;
+  if (inside) CK(cudaMemcpyAsync(inside, h->mask, (size_t)h->b.Nx * h->b.Ny, cudaMemcpyDeviceToHost, h->s));
+  if (ncells) *ncells = h->ncells;
+  if (cells && max_cells > 0 && h->ncells > 0) {
+    std::vector<CutCellDev> c(h->ncells);
+    CK(cudaMemcpyAsync(c.data(), h->cells, c.size() * sizeof(CutCellDev), cudaMemcpyDeviceToHost, h->s));
+    CK(cudaStreamSynchronize(h->s));
+    for (long k = 0; k < (long)c.size() && k < max_cells; ++k) {
+      double v[7] = {(double)c[k].i, (double)c[k].j, c[k].l0, c[k].l1, c[k].area, c[k].n0, c[k].n1};
+      std::memcpy(cells + 7 * k, v, sizeof(v));
+    }
+  }
+  CK(cudaStreamSynchronize(h->s));
+  return CSRST_OK;
+}
+
+int csrst_set_static_fields(csrst_handle *h, const double *ex, const double *ey, const double *hzx,
+                            const double *hzy) {
+  if (!h) return CSRST_E_ARG;
+  const double *src[4] = {ex, ey, hzx, hzy};
+  double *dst[4] = {h->Ex, h->Ey, h->Hx, h->Hy};
+  for (int k = 0; k < 4; ++k) {
+    if (!src[k]) continue;
+    CK(cudaMemcpy2DAsync(dst[k] + h->pitch + 1, h->pitch * sizeof(double), src[k], h->b.Nx * sizeof(double),
+                         h->b.Nx * sizeof(double), h->b.Ny, cudaMemcpyHostToDevice, h->s));
+  }
+  CK(cudaStreamSynchronize(h->s));
+  return CSRST_OK;
+}
+
+int csrst_get_static_fields(csrst_handle *h, double *ex, double *ey, double *hzx, double *hzy) {
+  if (!h) return CSRST_E_ARG;
+  double *dst[4] = {ex, ey, hzx, hzy};
+  const double *src[4] = {h->Ex, h->Ey, h->Hx, h->Hy};
+  for (int k = 0; k < 4; ++k) {
+    if (!dst[k]) continue;
+    CK(cudaMemcpy2DAsync(dst[k], h->b.Nx * sizeof(double), src[k] + h->pitch + 1, h->pitch * sizeof(double),
+                         h->b.Nx * sizeof(double), h->b.Ny, cudaMemcpyDeviceToHost, h->s));
+  }
+  CK(cudaStreamSynchronize(h->s));
+  return CSRST_OK;
+}
+
+int csrst_reset_outside(csrst_handle *h) {
+  if (!h) return CSRST_E_ARG;
+  launch_reset_outside(field_args(h, 0), h->cutidx, h->s);
+  CK(cudaStreamSynchronize(h->s));
+  return CSRST_OK;
+}
+
+int csrst_load_particles(csrst_handle *h, const double *x, const double *y, const double *px,
+                         const double *py, const double *q, size_t n) {
+  if (!h || (n > 0 && (!x || !y || !px || !py || !q))) return CSRST_E_ARG;
+  if (n == 0) return fail(h, CSRST_E_NO_PARTICLES, "empty bunch");
+  double qmax = 0.0;
+  for (size_t i = 0; i < n; ++i) {
+    if (!std::isfinite(x[i]) || !std::isfinite(y[i]) || !std::isfinite(px[i]) || !std::isfinite(py[i]) ||
+        !std::isfinite(q[i]))
+      return fail(h, CSRST_E_ARG, "non-finite particle data at index " + std::to_string(i));
+    qmax = std::fmax(qmax, std::fabs(q[i]));
+  }
+  CK(cudaStreamSynchronize(h->s));
+  free_particles(h);
+  const long long N = (long long)n;
+  h->n = N;
+  const size_t nb = n * sizeof(double);
+  double *tmp[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+  for (double **p : {&h->x, &h->y, &h->px, &h->py, &h->q, &h->ox, &h->oy}) CK(cudaMalloc(p, nb));
+  for (int k = 0; k < 5; ++k) CK(cudaMalloc(&tmp[k], nb));
+  const double *src[5] = {x, y, px, py, q};
+  for (int k = 0; k < 5; ++k) CK(cudaMemcpyAsync(tmp[k], src[k], nb, cudaMemcpyHostToDevice, h->s));
+  // particle box on the static mesh -> window +-5 cells (main.cpp:198-217)
+  WinState w0{};
+  w0.cur = 0;
+  CK(cudaMemcpyAsync(h->ws, &w0, sizeof(WinState), cudaMemcpyHostToDevice, h->s));
+  launch_bbox_next(tmp[0], tmp[1], tmp[2], tmp[3], N, 0.0, 0, h->ws, h->s);
+  long long bb[4];
+  CK(cudaMemcpyAsync(bb, h->ws->bb[0], sizeof(bb), cudaMemcpyDeviceToHost, h->s));
+  CK(cudaStreamSynchronize(h->s));
+  const double mn0 = ord_dbl(bb[0]), mn1 = ord_dbl(bb[1]), mx0 = ord_dbl(bb[2]), mx1 = ord_dbl(bb[3]);
+  int d[4] = {(int)std::floor((mn0 - h->b.org0) / h->b.hr0), (int)std::floor((mx0 - h->b.org0) / h->b.hr0),
+              (int)std::floor((mn1 - h->b.org1) / h->b.hr1), (int)std::floor((mx1 - h->b.org1) / h->b.hr1)};
+  d[0] -= 5; d[1] += 5; d[2] -= 5; d[3] += 5;
+  h->L0 = d[1] - d[0] + 1; h->L1 = d[3] - d[2] + 1;
+  h->wpitch = h->L0 + 2;
+  w0.P0 = d[0]; w0.P1 = d[2]; w0.L0 = h->L0; w0.L1 = h->L1;
+  w0.mo0 = h->b.org0 + d[0] * h->b.hr0;
+  w0.mo1 = h->b.org1 + d[2] * h->b.hr1;
+  w0.bb[0][0] = bb[0]; w0.bb[0][1] = bb[1]; w0.bb[0][2] = bb[2]; w0.bb[0][3] = bb[3];
+  CK(cudaMemcpyAsync(h->ws, &w0, sizeof(WinState), cudaMemcpyHostToDevice, h->s));
+  const size_t wp = (size_t)h->wpitch * (h->L1 + 2);
+  CK(cudaMalloc(&h->win, 6 * wp * sizeof(double)));
+  CK(cudaMemsetAsync(h->win, 0, 6 * wp * sizeof(double), h->s));
+  CK(cudaMalloc(&h->scratch, 4 * wp * sizeof(double)));
+  CK(cudaMalloc(&h->acc, 2 * (size_t)h->L0 * h->L1 * sizeof(unsigned long long)));
+  CK(cudaMemsetAsync(h->acc, 0, 2 * (size_t)h->L0 * h->L1 * sizeof(unsigned long long), h->s));
+  // PartBunch::sortParticles: y slice of the window, then x (stable radix sorts)
+  {
+    unsigned long long *kx = nullptr, *kx2 = nullptr;
+    unsigned int *ks = nullptr, *ks2 = nullptr;
+    long long *i1 = nullptr, *i2 = nullptr;
+    void *ct = nullptr;
+    size_t ctb = 0, ctb2 = 0;
+    CK(cudaMalloc(&kx, n * 8)); CK(cudaMalloc(&kx2, n * 8));
+    CK(cudaMalloc(&ks, n * 4)); CK(cudaMalloc(&ks2, n * 4));
+    CK(cudaMalloc(&i1, n * 8)); CK(cudaMalloc(&i2, n * 8));
+    const unsigned g = (unsigned)((n + 255) / 256);
+    k_sort_keys<<<g, 256, 0, h->s>>>(tmp[0], tmp[1], N, h->ws, h->b.hr1, kx, i1);
+    CK(cub::DeviceRadixSort::SortPairs(nullptr, ctb, kx, kx2, i1, i2, (int)n, 0, 64, h->s));
+    CK(cub::DeviceRadixSort::SortPairs(nullptr, ctb2, ks, ks2, i2, i1, (int)n, 0, 32, h->s));
+    CK(cudaMalloc(&ct, ctb > ctb2 ? ctb : ctb2));
+    CK(cub::DeviceRadixSort::SortPairs(ct, ctb, kx, kx2, i1, i2, (int)n, 0, 64, h->s));
+    k_slice_keys<<<g, 256, 0, h->s>>>(tmp[1], i2, N, h->ws, h->b.hr1, ks);
+    CK(cub::DeviceRadixSort::SortPairs(ct, ctb2, ks, ks2, i2, i1, (int)n, 0, 32, h->s));
+    double *dst[5] = {h->x, h->y, h->px, h->py, h->q};
+    for (int k = 0; k < 5; ++k) k_gather_perm<<<g, 256, 0, h->s>>>(i1, N, tmp[k], dst[k]);
+    CK(cudaStreamSynchronize(h->s));
+    cudaFree(kx); cudaFree(kx2); cudaFree(ks); cudaFree(ks2); cudaFree(i1); cudaFree(i2); cudaFree(ct);
+  }
+  for (int k = 0; k < 5; ++k) cudaFree(tmp[k]);
+  CK(cudaMemcpyAsync(h->ox, h->x, nb, cudaMemcpyDeviceToDevice, h->s));
+  CK(cudaMemcpyAsync(h->oy, h->y, nb, cudaMemcpyDeviceToDevice, h->s));
+  // 64-bit fixed-point scale of the current: a power of two with the
+  // largest possible per-cell sum (every particle, 4x margin) below 2^62.
+  const double bound = 4.0 * (double)n * (qmax > 0 ? qmax : 1e-30) * kC / (h->b.hr0 * h->b.hr1);
+  h->acc_scale = std::ldexp(1.0, (int)std::floor(std::log2(std::ldexp(1.0, 62) / bound)));
+  // window fill (copyFields + exchangeBoundaries, main.cpp:335-342)
+  FieldArgs fa = field_args(h, 0);
+  launch_copy_to_window(fa, h->s);
+  launch_exchange(fa, 0, h->s);
+  launch_exchange(fa, 1, h->s);
+  launch_exchange(fa, 2, h->s);
+  launch_check_window(fa, h->s);
+  h->pending = false;
+  h->bb = kBBInvalid;
+  h->acc_fresh[0] = h->acc_fresh[1] = false;
+  launch_bbox_next(h->x, h->y, h->px, h->py, N, h->half, 0, h->ws, h->s);
+  h->bb = kBBValid;
+  CK(cudaStreamSynchronize(h->s));
+  CK(cudaGetLastError());
+  return check_err(h);
+}
+
+int csrst_get_particles(csrst_handle *h, double *x, double *y, double *px, double *py) {
+  int rc = need_bunch(h);
+  if (rc) return rc;
+  materialise(h);
+  const size_t nb = (size_t)h->n * sizeof(double);
+  if (x) CK(cudaMemcpyAsync(x, h->x, nb, cudaMemcpyDeviceToHost, h->s));
+  if (y) CK(cudaMemcpyAsync(y, h->y, nb, cudaMemcpyDeviceToHost, h->s));
+  if (px) CK(cudaMemcpyAsync(px, h->px, nb, cudaMemcpyDeviceToHost, h->s));
+  if (py) CK(cudaMemcpyAsync(py, h->py, nb, cudaMemcpyDeviceToHost, h->s));
+  CK(cudaStreamSynchronize(h->s));
+  return check_err(h);
+}
+
+int csrst_get_old_positions(csrst_handle *h, double *ox, double *oy) {
+  int rc = need_bunch(h);
+  if (rc) return rc;
+  if (!(h->cfg.flags & 1)) return fail(h, CSRST_E_ARG, "create the handle with flags & 1 to keep oldR");
+  const size_t nb = (size_t)h->n * sizeof(double);
+  if (ox) CK(cudaMemcpyAsync(ox, h->ox, nb, cudaMemcpyDeviceToHost, h->s));
+  if (oy) CK(cudaMemcpyAsync(oy, h->oy, nb, cudaMemcpyDeviceToHost, h->s));
+  CK(cudaStreamSynchronize(h->s));
+  return CSRST_OK;
+}
+
+int csrst_get_window(csrst_handle *h, int *w4, double *origin2, int *gb4) {
+  int rc = need_bunch(h);
+  if (rc) return rc;
+  WinState w;
+  CK(cudaMemcpyAsync(&w, h->ws, sizeof(WinState), cudaMemcpyDeviceToHost, h->s));
+  CK(cudaStreamSynchronize(h->s));
+  if (w4) { w4[0] = w.P0; w4[1] = w.P1; w4[2] = w.L0; w4[3] = w.L1; }
+  if (origin2) { origin2[0] = w.mo0; origin2[1] = w.mo1; }
+  if (gb4) std::memcpy(gb4, w.gb, sizeof(w.gb));
+  return CSRST_OK;
+}
+
+int csrst_get_window_field(csrst_handle *h, int which, double *out) {
+  int rc = need_bunch(h);
+  if (rc) return rc;
+  if (which < 0 || which > 5 || !out) return fail(h, CSRST_E_ARG, "which must be 0..5");
+  if (which >= 4 && h->acc_fresh[which - 4]) {
+    const int c = which - 4;
+    k_acc_to_plane<<<(h->L0 * h->L1 + 255) / 256, 256, 0, h->s>>>(h->acc + (size_t)c * h->L0 * h->L1,
+                                                                wplane(h, which), h->L0, h->L1,
+                                                                1.0 / h->acc_scale);
+  }
+  const size_t wp = (size_t)h->wpitch * (h->L1 + 2);
+  CK(cudaMemcpyAsync(out, h->win + (size_t)which * wp, wp * sizeof(double), cudaMemcpyDeviceToHost, h->s));
+  CK(cudaStreamSynchronize(h->s));
+  return CSRST_OK;
+}
+
+int csrst_push(csrst_handle *h, int jcomp) {
+  int rc = need_bunch(h);
+  if (rc) return rc;
+  if (jcomp != 0 && jcomp != 1) return fail(h, CSRST_E_ARG, "jcomp must be 0 or 1");
+  push_async(h, jcomp);
+  return CSRST_OK;
+}
+
+int csrst_drift(csrst_handle *h, double dt) {
+  int rc = need_bunch(h);
+  if (rc) return rc;
+  if (!h->pending && dt == -0.5 * h->dt) {
+    drift_back(h);
+    return CSRST_OK;
+  }
+  materialise(h);
+  launch_drift(h->x, h->y, h->px, h->py, h->n, dt * kC, h->s);
+  h->bb = kBBInvalid;
+  return CSRST_OK;
+}
+
+int csrst_half_h(csrst_handle *h) {
+  int rc = need_bunch(h);
+  if (rc) return rc;
+  half_h_async(h);
+  return CSRST_OK;
+}
+
+int csrst_update_e(csrst_handle *h, int comp) {
+  int rc = need_bunch(h);
+  if (rc) return rc;
+  if (comp != 0 && comp != 1) return fail(h, CSRST_E_ARG, "comp must be 0 or 1");
+  update_e_async(h, comp);
+  return CSRST_OK;
+}
+
+int csrst_move_window(csrst_handle *h) {
+  int rc = need_bunch(h);
+  if (rc) return rc;
+  move_async(h);
+  return CSRST_OK;
+}
+
+int csrst_step_first(csrst_handle *h) {
+  int rc = need_bunch(h);
+  if (rc) return rc;
+  push_async(h, 0);
+  half_h_async(h);
+  update_e_async(h, 0);
+  half_h_async(h);
+  drift_back(h);
+  return CSRST_OK;
+}
+
+int csrst_step_second(csrst_handle *h) {
+  int rc = need_bunch(h);
+  if (rc) return rc;
+  push_async(h, 1);
+  update_e_async(h, 1);
+  drift_back(h);
+  return CSRST_OK;
+}
+
+int csrst_step(csrst_handle *h, int nsteps) {
+  int rc = need_bunch(h);
+  if (rc) return rc;
+  if (nsteps < 0) return fail(h, CSRST_E_ARG, "nsteps < 0");
+  // The graph is recorded in the steady state of the loop: the stored
+  // positions owe the trailing -dt/2 drift and the box of the next gather
+  // positions is current.  Anything else runs one step eagerly first.
+  while (nsteps > 0 && !(h->pending && h->bb == kBBValid)) {
+    step_async(h);
+    --nsteps;
+  }
+  if (nsteps == 0) return CSRST_OK;
+  if (!h->graph) {
+    cudaGraph_t g;
+    CK(cudaStreamBeginCapture(h->s, cudaStreamCaptureModeThreadLocal));
+    step_async(h);
+    CK(cudaStreamEndCapture(h->s, &g));
+    cudaError_t e = cudaGraphInstantiate(&h->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return cuda_fail(h, e, "cudaGraphInstantiate");
+    --nsteps;
+    CK(cudaGraphLaunch(h->graph, h->s));
+  }
+  for (int k = 0; k < nsteps; ++k) CK(cudaGraphLaunch(h->graph, h->s));
+  return CSRST_OK;
+}
+
+int csrst_diag_moments(csrst_handle *h, double *out18) {
+  int rc = need_bunch(h);
+  if (rc) return rc;
+  if (!out18) return CSRST_E_ARG;
+  launch_moments(h->x, h->y, h->px, h->py, h->n, h->half, h->pending, h->dscratch, h->dmean, h->dout, h->s);
+  CK(cudaMemcpyAsync(out18, h->dout, 18 * sizeof(double), cudaMemcpyDeviceToHost, h->s));
+  CK(cudaStreamSynchronize(h->s));
+  return check_err(h);
+}
+
+int csrst_diag_wake(csrst_handle *h, double *out, int n) {
+  int rc = need_bunch(h);
+  if (rc) return rc;
+  if (!out || n != h->L0 - 4) return fail(h, CSRST_E_ARG, "wake buffer must hold L0 - 4 values");
+  launch_moments(h->x, h->y, h->px, h->py, h->n, h->half, h->pending, h->dscratch, h->dmean, h->dout, h->s);
+  double *d = nullptr;
+  CK(cudaMallocAsync(&d, (size_t)n * sizeof(double), h->s));
+  launch_wake(h->ws, wplane(h, 0).p, wplane(h, 1).p, h->wpitch, h->L0, h->b.hr0, h->b.hr1, h->dmean, d, h->s);
+  CK(cudaMemcpyAsync(out, d, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, h->s));
+  CK(cudaFreeAsync(d, h->s));
+  CK(cudaStreamSynchronize(h->s));
+  return check_err(h);
+}
+
+// ---- stand-alone ScatterGatherImpl / ShapeFunction entry points ----
+
+int csrst_gather(int order, int comp, const double *patch, int nx, int ny, const double *o2, const double *hh2,
+                 const double *x, const double *y, size_t n, double *out) {
+  csrst_handle *h = nullptr;
+  if (order < 0 || order > 2 || comp < 0 || comp > 2 || !patch || nx <= 0 || ny <= 0 || !o2 || !hh2)
+    return fail(h, CSRST_E_ARG, "invalid gather arguments");
+  if (n == 0) return CSRST_OK;
+  double *dp, *dx, *dy, *dout;
+  CK(cudaMalloc(&dp, (size_t)nx * ny * 8)); CK(cudaMalloc(&dx, n * 8)); CK(cudaMalloc(&dy, n * 8));
+  CK(cudaMalloc(&dout, n * 8));
+  CK(cudaMemcpy(dp, patch, (size_t)nx * ny * 8, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(dx, x, n * 8, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(dy, y, n * 8, cudaMemcpyHostToDevice));
+  launch_gather(order, comp, dp, nx, o2[0], o2[1], hh2[0], hh2[1], dx, dy, (long long)n, dout, 0);
+  CK(cudaMemcpy(out, dout, n * 8, cudaMemcpyDeviceToHost));
+  cudaFree(dp); cudaFree(dx); cudaFree(dy); cudaFree(dout);
+  CK(cudaGetLastError());
+  return CSRST_OK;
+}
+
+static int run_fixed(int kind, int order, int comp, const double *ox, const double *oy, const double *x,
+                     const double *y, const double *q, size_t n, const double *o2, const double *hh2, double dt,
+                     int i0, int j0, int ni, int nj, double scale, double *J) {
+  csrst_handle *h = nullptr;
+  if (order < 0 || order > 2 || ni <= 0 || nj <= 0 || !o2 || !hh2 || !J || !(scale > 0))
+    return fail(h, CSRST_E_ARG, "invalid deposit arguments");
+  const size_t m = (size_t)ni * nj;
+  unsigned long long *acc;
+  double *dJ;
+  int *derr;
+  CK(cudaMalloc(&acc, m * 8)); CK(cudaMalloc(&dJ, m * 8)); CK(cudaMalloc(&derr, 4));
+  CK(cudaMemset(acc, 0, m * 8)); CK(cudaMemset(derr, 0, 4));
+  double *d[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+  const double *s[5] = {ox, oy, x, y, q};
+  if (n > 0)
+    for (int k = 0; k < 5; ++k) {
+      CK(cudaMalloc(&d[k], n * 8));
+      CK(cudaMemcpy(d[k], s[k], n * 8, cudaMemcpyHostToDevice));
+    }
+  if (kind == 0)
+    launch_deposit(order, comp, d[0], d[1], d[2], d[3], d[4], (long long)n, o2[0], o2[1], hh2[0], hh2[1], dt,
+                   i0, j0, ni, nj, acc, scale, derr, 0);
+  else
+    launch_charge_diff(order, d[0], d[1], d[2], d[3], d[4], (long long)n, o2[0], o2[1], hh2[0], hh2[1], i0, j0,
+                       ni, nj, acc, scale, 0);
+  launch_fixed_to_double(acc, dJ, (long long)m, 1.0 / scale, 0);
+  int e = 0;
+  CK(cudaMemcpy(J, dJ, m * 8, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(&e, derr, 4, cudaMemcpyDeviceToHost));
+  if (kind == 1)
+    for (size_t k = 0; k < m; ++k) J[k] = J[k] / (hh2[0] * hh2[1]);
+  cudaFree(acc); cudaFree(dJ); cudaFree(derr);
+  for (double *p : d) cudaFree(p);
+  CK(cudaGetLastError());
+  return e ? fail(h, e, "too many cell-border crossings") : CSRST_OK;
+}
+
+int csrst_deposit(int order, int comp, const double *ox, const double *oy, const double *x, const double *y,
+                  const double *q, size_t n, const double *o2, const double *hh2, double dt, int i0, int j0,
+                  int ni, int nj, double scale, double *J) {
+  if (comp != 0 && comp != 1) return fail(nullptr, CSRST_E_ARG, "comp must be 0 or 1");
+  return run_fixed(0, order, comp, ox, oy, x, y, q, n, o2, hh2, dt, i0, j0, ni, nj, scale, J);
+}
+
+int csrst_charge_diff(int order, const double *ox, const double *oy, const double *x, const double *y,
+                      const double *q, size_t n, const double *o2, const double *hh2, int i0, int j0, int ni,
+                      int nj, double scale, double *rho) {
+  return run_fixed(1, order, 0, ox, oy, x, y, q, n, o2, hh2, 0.0, i0, j0, ni, nj, scale, rho);
+}
+
+}  // extern "C"

@@ -1,0 +1,250 @@
+// Diagnostics on the device: beam moments (PartBunch::calcBeamParameters /
+// calcMoments, PartBunch.cpp:584-767), the longitudinal field along the bunch
+// axis that the CSR wake integrates (IntegrateElongCommand::execute,
+// IntegrateElong.cpp:38-89) and the charge difference used by the FP64
+// continuity check.  All reductions run in FP64 with a fixed order (per-CTA
+// partials reduced by one CTA), so they are reproducible run to run.
+#include "kernels.cuh"
+#include "shapes.cuh"
+
+namespace csrst {
+
+constexpr int kDiagBlocks = 296;
+
+// True position when the -dt/2 drift is still pending on the stored R.
+__device__ __forceinline__ void true_pos(double &x, double &y, double p0, double p1, double half,
+                                         int pending) {
+  if (!pending) return;
+  const double r = inv_gamma(p0, p1);
+  x = x + (-(half * p0 * r));
+  y = y + (-(half * p1 * r));
+}
+
+template <int NV>
+__device__ void block_sum(double (&v)[NV], double *out) {
+  __shared__ double sh[NV][32];
+#pragma unroll
+  for (int k = 0; k < NV; ++k)
+    for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_down_sync(0xffffffffu, v[k], o);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  if (lane == 0)
+    for (int k = 0; k < NV; ++k) sh[k][w] = v[k];
+  __syncthreads();
+  if (threadIdx.x < NV) {
+    double s = 0.0;
+    for (int q = 0; q < nw; ++q) s += sh[threadIdx.x][q];
+    out[threadIdx.x] = s;
+  }
+  __syncthreads();
+}
+
+// pass 1: sum x, px, y, py, gamma; min/max x, y.  part[b * 9 + k]
+__global__ void __launch_bounds__(256) k_mom1(const double *x, const double *y, const double *px,
+                                              const double *py, long long n, double half,
+                                              int pending, double *part) {
+  double v[5] = {0, 0, 0, 0, 0};
+  double mn0 = INFINITY, mn1 = INFINITY, mx0 = -INFINITY, mx1 = -INFINITY;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    double a = x[i], b = y[i];
+    const double p0 = px[i], p1 = py[i];
+    true_pos(a, b, p0, p1, half, pending);
+    v[0] += a; v[1] += p0; v[2] += b; v[3] += p1;
+    v[4] += sqrt(1.0 + (p0 * p0 + p1 * p1));
+    mn0 = fmin(mn0, a); mn1 = fmin(mn1, b); mx0 = fmax(mx0, a); mx1 = fmax(mx1, b);
+  }
+  block_sum<5>(v, part + blockIdx.x * 9);
+  double m[4] = {mn0, mn1, -mx0, -mx1};
+  __shared__ double sm[4][32];
+  for (int k = 0; k < 4; ++k)
+    for (int o = 16; o > 0; o >>= 1) m[k] = fmin(m[k], __shfl_down_sync(0xffffffffu, m[k], o));
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  if (lane == 0)
+    for (int k = 0; k < 4; ++k) sm[k][w] = m[k];
+  __syncthreads();
+  if (threadIdx.x < 4) {
+    double s = INFINITY;
+    for (int q = 0; q < nw; ++q) s = fmin(s, sm[threadIdx.x][q]);
+    part[blockIdx.x * 9 + 5 + threadIdx.x] = s;
+  }
+}
+
+// pass 2: second moments of (x', px', y', py') in the frame of the mean
+// momentum, centred on the mean position (PartBunch.cpp:724-745).
+__global__ void __launch_bounds__(256) k_mom2(const double *x, const double *y, const double *px,
+                                              const double *py, long long n, double half,
+                                              int pending, const double *mean, double *part) {
+  const double aR0 = mean[0], aR1 = mean[1], aP0 = mean[2], aP1 = mean[3];
+  const double am = sqrt(aP0 * aP0 + aP1 * aP1), cph = aP0 / am, sph = aP1 / am;
+  double v[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    double a = x[i], b = y[i];
+    const double p0 = px[i], p1 = py[i];
+    true_pos(a, b, p0, p1, half, pending);
+    double q[4];
+    q[1] = cph * p0 + sph * p1;
+    q[3] = -sph * p0 + cph * p1;
+    q[0] = a - aR0; q[2] = b - aR1;
+    const double t = cph * q[0] + sph * q[2];
+    q[2] = -sph * q[0] + cph * q[2];
+    q[0] = t;
+    int k = 0;
+    for (int r = 0; r < 4; ++r)
+      for (int c = 0; c <= r; ++c) v[k++] += q[r] * q[c];
+  }
+  block_sum<10>(v, part + blockIdx.x * 10);
+}
+
+// Final reduction and the derived quantities; out[18] as the oracle's layout:
+// rmean2 pmean2 rrms2 prms2 eps2 rmin2 rmax2 Ekin dE, pad.
+__global__ void k_mom_final1(const double *part, int nb, long long n, double *mean, double *out) {
+  if (threadIdx.x != 0) return;
+  double s[5] = {0, 0, 0, 0, 0}, m[4] = {INFINITY, INFINITY, INFINITY, INFINITY};
+  for (int b = 0; b < nb; ++b) {
+    for (int k = 0; k < 5; ++k) s[k] += part[b * 9 + k];
+    for (int k = 0; k < 4; ++k) m[k] = fmin(m[k], part[b * 9 + 5 + k]);
+  }
+  const double N = (double)n;
+  mean[0] = s[0] / N; mean[1] = s[2] / N; mean[2] = s[1] / N; mean[3] = s[3] / N; mean[4] = s[4] / N;
+  out[0] = mean[0]; out[1] = mean[1]; out[2] = mean[2]; out[3] = mean[3];
+  out[10] = m[0]; out[11] = m[1]; out[12] = -m[2]; out[13] = -m[3];
+}
+
+__global__ void k_mom_final2(const double *part, int nb, long long n, const double *mean, double *out) {
+  if (threadIdx.x != 0) return;
+  double M[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+  for (int b = 0; b < nb; ++b)
+    for (int k = 0; k < 10; ++k) M[k] += part[b * 10 + k];
+  // packed lower triangle: (0,0)=0 (1,0)=1 (1,1)=2 (2,0)=3 (2,1)=4 (2,2)=5 (3,0)=6 (3,1)=7 (3,2)=8 (3,3)=9
+  const double N = (double)n;
+  const double pm0 = mean[2], pm1 = mean[3];
+  const double c1 = pm0 * pm0 + pm1 * pm1;
+  const double rsq[2] = {M[0], M[5]};
+  double psq[2] = {M[2] - N * c1, M[9] - N * 0.0};
+  const double rp[2] = {M[1], M[8]};
+  for (int i = 0; i < 2; ++i) {
+    if (psq[i] < 0) psq[i] = 0;
+    const double e2 = (rsq[i] * psq[i] - rp[i] * rp[i]) / (N * N);
+    out[4 + i] = sqrt(rsq[i] / N);
+    out[6 + i] = sqrt(psq[i] / N);
+    out[8 + i] = sqrt(fmax(e2, 0.0));
+  }
+  const double m0 = 0.51099906e-03 * 1000;
+  const double ek = (mean[4] - 1.0) * m0;
+  out[14] = ek;
+  out[15] = out[6] * sqrt(ek * (ek + 2. * m0) / (1. + ek * (ek + 2. * m0) / (m0 * m0)));
+  out[16] = 0.0; out[17] = 0.0;
+}
+
+// E_s = cos(p) Ex + sin(p) Ey sampled at i = 2 .. L0-3 along the mean
+// momentum direction through the centroid; NaN where the sample's cell lies
+// outside the window.  The samples use the CIC edge gather of
+// ScatterGatherImpl on the window.
+__global__ void k_wake(const WinState *ws, const double *mEx, const double *mEy, int wpitch,
+                       double h0, double h1, const double *mean, double *out) {
+  const int L0 = ws->L0, L1 = ws->L1;
+  const int i = 2 + blockIdx.x * blockDim.x + threadIdx.x;
+  if (i > L0 - 3) return;
+  const double r0 = mean[0], r1 = mean[1], p0 = mean[2], p1 = mean[3];
+  const double lenP = sqrt(p0 * p0 + p1 * p1);
+  const double cP = p0 / lenP, sP = p1 / lenP;
+  const double mo0 = ws->mo0, mo1 = ws->mo1;
+  const double l0 = mo0 + i * h0 - r0;
+  const double a0 = cP * l0 + sP * 0.0 + r0;
+  const double a1 = -sP * l0 + cP * 0.0 + r1;
+  const int ci = (int)floor((a0 - mo0) / h0), cj = (int)floor((a1 - mo1) / h1);
+  if (ci < 0 || cj < 0 || ci >= L0 || cj >= L1) { out[i - 2] = NAN; return; }
+  const PatchView pex{mEx + wpitch + 1, wpitch}, pey{mEy + wpitch + 1, wpitch};
+  const double pp0 = (a0 - mo0) * (1.0 / h0), pp1 = (a1 - mo1) * (1.0 / h1);
+  const double e0 = gather_edge<0>(pex, pp0, pp1, 0), e1 = gather_edge<0>(pey, pp0, pp1, 1);
+  out[i - 2] = cP * e0 + sP * e1;
+}
+
+// Charge difference rho(R) - rho(oldR) at vertices for the charge shape that
+// matches the deposit order (get*ChargeDensityDiffImpl), fixed point.
+template <int ORDER>
+__global__ void k_charge_diff(const double *ox, const double *oy, const double *x, const double *y,
+                              const double *q, long long n, double org0, double org1, double h0,
+                              double h1, int i0, int j0, int ni, int nj, unsigned long long *acc,
+                              double scale) {
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n;
+       k += (long long)gridDim.x * blockDim.x) {
+    const double qq = q[k];
+    for (int pass = 0; pass < 2; ++pass) {
+      const double sg = pass == 0 ? 1.0 : -1.0;
+      const double X = pass == 0 ? x[k] : ox[k], Y = pass == 0 ? y[k] : oy[k];
+      auto add = [&](int i, int j, double v) {
+        i -= i0; j -= j0;
+        if (i < 0 || j < 0 || i >= ni || j >= nj) return;
+        atomicAdd(&acc[(size_t)j * ni + i], (unsigned long long)__double2ll_rn(sg * v * scale));
+      };
+      if (ORDER == 0) {
+        const double a = (X - org0) / h0, b = (Y - org1) / h1;
+        const int I = (int)floor(a), J = (int)floor(b);
+        const double t0 = a - I, t1 = b - J;
+        add(I, J, (1.0 - t0) * (1.0 - t1) * qq);
+        add(I + 1, J, t0 * (1.0 - t1) * qq);
+        add(I, J + 1, (1.0 - t0) * t1 * qq);
+        add(I + 1, J + 1, t0 * t1 * qq);
+      } else if (ORDER == 1) {
+        const double n0 = (X - org0) / h0, n1 = (Y - org1) / h1;
+        const int I = (int)floor(n0 + 0.5), J = (int)floor(n1 + 0.5);
+        const double a = n0 - I, b = n1 - J;
+        const double sxm = qq * (0.5 - a) * (0.5 - a) * 0.5, sxp = qq * (0.5 + a) * (0.5 + a) * 0.5;
+        const double sx = qq - sxm - sxp;
+        const double sym = (0.5 - b) * (0.5 - b) * 0.5, syp = (0.5 + b) * (0.5 + b) * 0.5;
+        const double sy = 1.0 - sym - syp;
+        const double wx[3] = {sxm, sx, sxp}, wy[3] = {sym, sy, syp};
+        for (int bb = 0; bb < 3; ++bb)
+          for (int aa = 0; aa < 3; ++aa) add(I - 1 + aa, J - 1 + bb, wx[aa] * wy[bb]);
+      } else {
+        const double n0 = (X - org0) / h0, n1 = (Y - org1) / h1;
+        const int I = (int)floor(n0), J = (int)floor(n1);
+        const double a = n0 - I, b = n1 - J;
+        const double s6 = 1.0 / 6.0;
+        const double wx[4] = {s6 * ((1.0 - a) * (1.0 - a) * (1.0 - a)), s6 * (4.0 - 3.0 * a * a * (2.0 - a)),
+                              s6 * (4.0 - 3.0 * (1.0 - a) * (1.0 - a) * (1.0 + a)), s6 * (a * a * a)};
+        const double wy[4] = {s6 * ((1.0 - b) * (1.0 - b) * (1.0 - b)), s6 * (4.0 - 3.0 * b * b * (2.0 - b)),
+                              s6 * (4.0 - 3.0 * (1.0 - b) * (1.0 - b) * (1.0 + b)), s6 * (b * b * b)};
+        for (int bb = 0; bb < 4; ++bb)
+          for (int aa = 0; aa < 4; ++aa) add(I - 1 + aa, J - 1 + bb, qq * wx[aa] * wy[bb]);
+      }
+    }
+  }
+}
+
+// --- host launchers -----------------------------------------------------------
+
+void launch_moments(const double *x, const double *y, const double *px, const double *py, long long n,
+                    double half, int pending, double *part, double *mean, double *out, cudaStream_t s) {
+  k_mom1<<<kDiagBlocks, 256, 0, s>>>(x, y, px, py, n, half, pending, part);
+  k_mom_final1<<<1, 32, 0, s>>>(part, kDiagBlocks, n, mean, out);
+  k_mom2<<<kDiagBlocks, 256, 0, s>>>(x, y, px, py, n, half, pending, mean, part);
+  k_mom_final2<<<1, 32, 0, s>>>(part, kDiagBlocks, n, mean, out);
+}
+
+size_t moments_scratch_doubles() { return (size_t)kDiagBlocks * 10; }
+
+void launch_wake(const WinState *ws, const double *mEx, const double *mEy, int wpitch, int L0, double h0,
+                 double h1, const double *mean, double *out, cudaStream_t s) {
+  const int n = L0 - 4;
+  if (n <= 0) return;
+  k_wake<<<(n + 127) / 128, 128, 0, s>>>(ws, mEx, mEy, wpitch, h0, h1, mean, out);
+}
+
+void launch_charge_diff(int order, const double *ox, const double *oy, const double *x, const double *y,
+                        const double *q, long long n, double org0, double org1, double h0, double h1,
+                        int i0, int j0, int ni, int nj, unsigned long long *acc, double scale,
+                        cudaStream_t s) {
+  if (n <= 0) return;
+  const int blocks = (int)((n + 255) / 256 < 4096 ? (n + 255) / 256 : 4096);
+  if (order == 0)
+    k_charge_diff<0><<<blocks, 256, 0, s>>>(ox, oy, x, y, q, n, org0, org1, h0, h1, i0, j0, ni, nj, acc, scale);
+  else if (order == 1)
+    k_charge_diff<1><<<blocks, 256, 0, s>>>(ox, oy, x, y, q, n, org0, org1, h0, h1, i0, j0, ni, nj, acc, scale);
+  else
+    k_charge_diff<2><<<blocks, 256, 0, s>>>(ox, oy, x, y, q, n, org0, org1, h0, h1, i0, j0, ni, nj, acc, scale);
+}
+
+}  // namespace csrst

@@ -1,0 +1,408 @@
+// Field kernels: the TE/TM split Yee update on the static mesh and on the
+// moving window, the conformal cut-cell corrections, the window <-> static
+// strip exchange and the window move.
+//
+// One sub-step (half-H, Ex or Ey) is one launch: the static sweep over the
+// masked regular cells, the sparse cut-cell list and the window cells are
+// disjoint sets of elements that read only fields the launch does not write,
+// so they run as three block ranges of the same grid
+// (TETMSolver.hh:142-206, :241-261; SCBoundaryCondition.hh:391-431).
+// The strip exchange that follows each sub-step is a pure copy between
+// disjoint element sets (Communicator::exchangeBoundaries,
+// Communicator.hh:575-876), launched separately because the next sub-step
+// reads what it writes.
+#include "kernels.cuh"
+
+namespace csrst {
+
+constexpr int kTX = 32, kTY = 8;
+
+// Half H update (first and third sub-step).
+__global__ void __launch_bounds__(256) k_half_h(FieldArgs a) {
+  const int b = blockIdx.x;
+  const double zero = 0.0;
+  (void)zero;
+  if (b < a.nbS) {
+    const int i = (b % a.tilesX) * kTX + (threadIdx.x % kTX);
+    const int j = (b / a.tilesX) * kTY + (threadIdx.x / kTX);
+    if (i >= a.Nx || j >= a.Ny) return;
+    if (!a.mask[(size_t)j * a.Nx + i]) return;
+    const double ey0 = a.Ey.at(i, j), ey1 = a.Ey.at(i + 1, j);
+    const double ex0 = a.Ex.at(i, j), ex1 = a.Ex.at(i, j + 1);
+    double &hx = a.Hx.at(i, j), &hy = a.Hy.at(i, j);
+    hx = hx - a.chx * (ey1 - ey0);
+    hy = hy + a.chy * (ex1 - ex0);
+  } else if (b < a.nbS + a.nbC) {
+    const int k = (b - a.nbS) * blockDim.x + threadIdx.x;
+    if (k >= a.ncells) return;
+    const CutCellDev c = a.cells[k];
+    const double u0 = a.mhx * (c.n1 * a.Ey.at(c.i + 1, c.j) - c.l1 * a.Ey.at(c.i, c.j)) / c.area;
+    const double u1 = a.mhy * (c.n0 * a.Ex.at(c.i, c.j + 1) - c.l0 * a.Ex.at(c.i, c.j)) / c.area;
+    a.Hx.at(c.i, c.j) += u0;
+    a.Hy.at(c.i, c.j) += u1;
+  } else {
+    const int k = (b - a.nbS - a.nbC) * blockDim.x + threadIdx.x;
+    if (k >= a.L0 * a.L1) return;
+    const int i = k % a.L0, j = k / a.L0;
+    double &hx = a.mHx.at(i, j), &hy = a.mHy.at(i, j);
+    hx = hx - a.chx * (a.mEy.at(i + 1, j) - a.mEy.at(i, j));
+    hy = hy + a.chy * (a.mEx.at(i, j + 1) - a.mEx.at(i, j));
+  }
+}
+
+// E update: comp 0 = Ex (TETMSolver.hh:165-172), comp 1 = Ey (:241-249).  The
+// static mesh carries no current in the reference loop (its J is reset to
+// zero every step, main.cpp:388, :494), so it enters as 0.0.  The window
+// current comes from the fixed-point accumulator of the last push, which is
+// converted, stored for diagnostics and cleared for the next deposit.
+template <int COMP>
+__global__ void __launch_bounds__(256) k_update_e(FieldArgs a, double zeroJ) {
+  const int b = blockIdx.x;
+  if (b < a.nbS) {
+    const int i = (b % a.tilesX) * kTX + (threadIdx.x % kTX);
+    const int j = (b / a.tilesX) * kTY + (threadIdx.x / kTX);
+    if (i >= a.Nx || j >= a.Ny) return;
+    if (!a.mask[(size_t)j * a.Nx + i]) return;
+    if (COMP == 0) {
+      double &e = a.Ex.at(i, j);
+      e = e + (a.kex * (a.Hx.at(i, j) - a.Hx.at(i, j - 1) + a.Hy.at(i, j) - a.Hy.at(i, j - 1)) - a.dteps * zeroJ);
+    } else {
+      double &e = a.Ey.at(i, j);
+      e = e - (a.key * (a.Hx.at(i, j) - a.Hx.at(i - 1, j) + a.Hy.at(i, j) - a.Hy.at(i - 1, j)) + a.dteps * zeroJ);
+    }
+  } else if (b < a.nbS + a.nbC) {
+    const int k = (b - a.nbS) * blockDim.x + threadIdx.x;
+    if (k >= a.ncells) return;
+    const CutCellDev c = a.cells[k];
+    if (c.area < kMinArea) return;
+    if (COMP == 0) {
+      if (!(c.l0 > kSpaceEps)) return;
+      const double u0 = (a.Hx.at(c.i, c.j) - a.Hx.at(c.i, c.j - 1)) / a.h1;
+      const double u1 = (a.Hy.at(c.i, c.j) - a.Hy.at(c.i, c.j - 1)) / a.h1;
+      a.Ex.at(c.i, c.j) += a.de * (u0 + u1 - zeroJ);
+    } else {
+      if (!(c.l1 > kSpaceEps)) return;
+      const double u0 = -(a.Hx.at(c.i, c.j) - a.Hx.at(c.i - 1, c.j)) / a.h0;
+      const double u1 = -(a.Hy.at(c.i, c.j) - a.Hy.at(c.i - 1, c.j)) / a.h0;
+      a.Ey.at(c.i, c.j) += a.de * (u0 + u1 - zeroJ);
+    }
+  } else {
+    const int k = (b - a.nbS - a.nbC) * blockDim.x + threadIdx.x;
+    if (k >= a.L0 * a.L1) return;
+    const int i = k % a.L0, j = k / a.L0;
+    const double J = (double)(long long)a.acc[k] * a.acc_inv;
+    a.acc[k] = 0ull;
+    if (COMP == 0) {
+      a.mJx.at(i, j) = J;
+      double &e = a.mEx.at(i, j);
+      e = e + (a.kex * (a.mHx.at(i, j) - a.mHx.at(i, j - 1) + a.mHy.at(i, j) - a.mHy.at(i, j - 1)) - a.dteps * J);
+    } else {
+      a.mJy.at(i, j) = J;
+      double &e = a.mEy.at(i, j);
+      e = e - (a.key * (a.mHx.at(i, j) - a.mHx.at(i - 1, j) + a.mHy.at(i, j) - a.mHy.at(i - 1, j)) + a.dteps * J);
+    }
+  }
+}
+
+// Strip exchange between the window and the static mesh for one field
+// (which: 0 = H as the sum Hzx + Hzy split 1/2 1/2, 1 = Ex, 2 = Ey).
+// Strips (Communicator.cpp:640-642):
+//   H : window last column and last row -> static; static column left of and
+//       row below the window (corners included) -> window guard ring.
+//   Ex: window first row -> static; static row above the window -> window guard.
+//   Ey: window first column -> static; static column right of the window -> window guard.
+// No element is both read and written, so every thread copies one element.
+__global__ void k_exchange(FieldArgs a, int which) {
+  const WinState *ws = a.ws;
+  const int P0 = ws->P0, P1 = ws->P1, L0 = a.L0, L1 = a.L1;
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  // segment table: (to_window, count)
+  int si, sj, wi, wj;  // static and window coordinates of the element
+  bool to_window;
+  if (which == 0) {
+    if (k < L1) { wi = L0 - 1; wj = k; to_window = false; }
+    else if ((k -= L1) < L0) { wi = k; wj = L1 - 1; to_window = false; }
+    else if ((k -= L0) < L1 + 2) { wi = -1; wj = k - 1; to_window = true; }
+    else if ((k -= L1 + 2) < L0 + 2) { wi = k - 1; wj = -1; to_window = true; }
+    else return;
+  } else if (which == 1) {
+    if (k < L0) { wi = k; wj = 0; to_window = false; }
+    else if ((k -= L0) < L0 + 2) { wi = k - 1; wj = L1; to_window = true; }
+    else return;
+  } else {
+    if (k < L1) { wi = 0; wj = k; to_window = false; }
+    else if ((k -= L1) < L1 + 2) { wi = L0; wj = k - 1; to_window = true; }
+    else return;
+  }
+  si = wi + P0; sj = wj + P1;
+  if (to_window) {
+    if (si < 0 || si >= a.Nx || sj < 0 || sj >= a.Ny) return;
+    if (which == 0) {
+      const double v = a.Hx.at(si, sj) + a.Hy.at(si, sj);
+      a.mHx.at(wi, wj) = 0.5 * v; a.mHy.at(wi, wj) = 0.5 * v;
+    } else if (which == 1) {
+      a.mEx.at(wi, wj) = a.Ex.at(si, sj);
+    } else {
+      a.mEy.at(wi, wj) = a.Ey.at(si, sj);
+    }
+  } else {
+    if (si < -1 || si > a.Nx || sj < -1 || sj > a.Ny) return;
+    if (which == 0) {
+      const double v = a.mHx.at(wi, wj) + a.mHy.at(wi, wj);
+      a.Hx.at(si, sj) = 0.5 * v; a.Hy.at(si, sj) = 0.5 * v;
+    } else if (which == 1) {
+      a.Ex.at(si, sj) = a.mEx.at(wi, wj);
+    } else {
+      a.Ey.at(si, sj) = a.mEy.at(wi, wj);
+    }
+  }
+}
+
+// Copy the static fields into the window interior (Communicator::copy via
+// copyFields, main.cpp:335-337).
+__global__ void k_copy_to_window(FieldArgs a) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= a.L0 * a.L1) return;
+  const int i = k % a.L0, j = k / a.L0;
+  const int si = i + a.ws->P0, sj = j + a.ws->P1;
+  if (si < 0 || sj < 0 || si >= a.Nx || sj >= a.Ny) return;
+  a.mEx.at(i, j) = a.Ex.at(si, sj); a.mEy.at(i, j) = a.Ey.at(si, sj);
+  a.mHx.at(i, j) = a.Hx.at(si, sj); a.mHy.at(i, j) = a.Hy.at(si, sj);
+}
+
+// Set err if the window or its one-cell ring touches a cell that is not a
+// regular inside cell: the fused sub-step launches assume the strip exchange
+// and the cut-cell corrections never meet.
+__device__ void check_window_clear(const FieldArgs &a, WinState *ws) {
+  const int P0 = ws->P0, P1 = ws->P1;
+  const int per = 2 * (a.L0 + 2) + 2 * a.L1;
+  for (int k = threadIdx.x; k < per; k += blockDim.x) {
+    int i, j;
+    if (k < a.L0 + 2) { i = k - 1; j = -1; }
+    else if (k < 2 * (a.L0 + 2)) { i = k - (a.L0 + 2) - 1; j = a.L1; }
+    else if (k < 2 * (a.L0 + 2) + a.L1) { i = -1; j = k - 2 * (a.L0 + 2); }
+    else { i = a.L0; j = k - 2 * (a.L0 + 2) - a.L1; }
+    const int si = i + P0, sj = j + P1;
+    if (si < 0 || sj < 0 || si >= a.Nx || sj >= a.Ny || !a.mask[(size_t)sj * a.Nx + si])
+      set_err(ws, kErrWindowWall);
+  }
+}
+
+__global__ void k_check_window(FieldArgs a) { check_window_clear(a, a.ws); }
+
+// Window move (moveMesh, main.cpp:562-652, and exchangeBoundariesMovingMesh,
+// Communicator.cpp:123-642).  One CTA: reads the last deposit's particle
+// bounds, shifts the window by whole cells through a scratch copy, updates
+// the window position and origin, then refreshes the strips.
+struct MoveArgs {
+  FieldArgs f;
+  double *scratch;      // 4 window planes
+  double h0, h1;
+};
+
+__global__ void __launch_bounds__(1024) k_move(MoveArgs m) {
+  FieldArgs &a = m.f;
+  WinState *ws = a.ws;
+  const int L[2] = {a.L0, a.L1};
+  __shared__ int s_move[3];
+  if (threadIdx.x == 0) {
+    int ok = 1, ideal1[2];
+    for (int d = 0; d < 2; ++d) {
+      const int len = ws->gb[2 * d + 1] - ws->gb[2 * d] + 1;
+      if (len >= L[d]) { ok = 0; break; }
+      const unsigned diff = (unsigned)(L[d] - len);
+      const unsigned up = (unsigned)floor(diff / 2.0);
+      ideal1[d] = L[d] - (int)up - 2;
+    }
+    int moveI = 0, dj = 0;
+    if (!ok) set_err(ws, kErrWindowFit);
+    else {
+      moveI = ws->gb[1] - ideal1[0] - 1;
+      dj = ws->gb[3] - ideal1[1] - 1;
+      if (moveI < 0 || moveI > 1 || dj < -1 || dj > 1) { set_err(ws, kErrWindowMove); ok = 0; }
+    }
+    s_move[0] = ok; s_move[1] = moveI; s_move[2] = dj;
+    if (ok) { ws->moves[0] = moveI; ws->moves[1] = dj; }
+  }
+  __syncthreads();
+  if (!s_move[0]) return;
+  const int moveI = s_move[1], m1 = s_move[2];
+  if (moveI == 0 && m1 == 0) return;
+  const int W0 = a.L0 + 2, W1 = a.L1 + 2, np = W0 * W1;
+  Plane *pl[4] = {&a.mEx, &a.mEy, &a.mHx, &a.mHy};
+  // phase A: snapshot
+  for (int k = threadIdx.x; k < 4 * np; k += blockDim.x) {
+    const int f = k / np, r = k % np;
+    m.scratch[k] = pl[f]->p[r];
+  }
+  __syncthreads();
+  // phase B: shifted copy over the reference's loop ranges
+  const int i0 = -moveI, i1 = a.L0 - 1;
+  int j0 = -(m1 > 0 ? m1 : 0), j1 = a.L1 - 1 - (m1 < 0 ? m1 : 0);
+  if (m1 == 0) { j0 -= 1; j1 += 1; }
+  const int ni = i1 - i0 + 1, cnt = ni * (j1 - j0 + 1);
+  for (int k = threadIdx.x; k < 4 * cnt; k += blockDim.x) {
+    const int f = k / cnt, r = k % cnt;
+    const int i = i0 + r % ni, j = j0 + r / ni;
+    pl[f]->at(i, j) = m.scratch[(size_t)f * np + (size_t)(j + m1 + 1) * W0 + (i + moveI + 1)];
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    ws->P0 += moveI; ws->P1 += m1;
+    ws->mo0 += moveI * m.h0;
+    ws->mo1 += m1 * m.h1;
+  }
+  __syncthreads();
+  // phase C: strip layers; type 0..2 window -> static (Hz, Ex, Ey), 3..5 static -> window.
+  const int P0 = ws->P0, P1 = ws->P1, Ld0 = a.L0 - 1, Ld1 = a.L1 - 1;
+  int lay[12][5], nl = 0;
+  auto add = [&](int t, int b0, int e0, int b1, int e1) {
+    lay[nl][0] = t; lay[nl][1] = b0; lay[nl][2] = e0; lay[nl][3] = b1; lay[nl][4] = e1; ++nl;
+  };
+  // layers grouped by type, in the reference's list order
+  for (int t = 0; t < 6; ++t) {
+    if (moveI == 1) {
+      switch (t) {
+        case 0: add(0, -1, -1, -m1, Ld1 - m1 - 1); break;
+        case 1: add(1, -1, -1, 1 - m1, Ld1 - m1); break;
+        case 2: add(2, 0, 0, -m1, Ld1 - m1); break;
+        case 3: add(3, Ld0 + P0, Ld0 + P0, P1, Ld1 + P1); break;
+        case 4: add(4, Ld0 + P0, Ld0 + P0, P1, Ld1 + P1 + 1); break;
+        case 5: add(5, Ld0 + P0 + 1, Ld0 + P0 + 1, P1, Ld1 + P1); break;
+      }
+    }
+    if (m1 == 1) {
+      switch (t) {
+        case 0: add(0, -moveI, Ld0 - 1 - moveI, -1, -1); break;
+        case 1: add(1, -moveI, Ld0 - moveI, 0, 0); break;
+        case 2: add(2, 1 - moveI, Ld0 - moveI, -1, -1); break;
+        case 3: add(3, P0, Ld0 + P0, Ld1 + P1, Ld1 + P1); break;
+        case 4: add(4, P0, Ld0 + P0, Ld1 + 1 + P1, Ld1 + 1 + P1); break;
+        case 5: add(5, P0, Ld0 + P0 + 1, Ld1 + P1, Ld1 + P1); break;
+      }
+    } else if (m1 == -1) {
+      switch (t) {
+        case 0: add(0, -moveI, Ld0 - moveI - 1, Ld1, Ld1); break;
+        case 1: add(1, -moveI, Ld0 - moveI, Ld1 + 1, Ld1 + 1); break;
+        case 2: add(2, 1 - moveI, Ld0 - moveI, Ld1 + 1, Ld1 + 1); break;
+        case 3: add(3, P0, Ld0 + P0, P1 - 1, P1 - 1); break;
+        case 4: add(4, P0, Ld0 + P0, P1, P1); break;
+        case 5: add(5, P0, Ld0 + P0 + 1, P1, P1); break;
+      }
+    }
+  }
+  // clip each layer (window layers to [-1, L] and the static domain; static
+  // layers to the static domain and the window incl. guards)
+  int beg[13];
+  beg[0] = 0;
+  for (int l = 0; l < nl; ++l) {
+    int *y = lay[l];
+    if (y[0] < 3) {
+      y[1] = max(max(y[1], -1), -P0); y[2] = min(min(y[2], a.L0), a.Nx - 1 - P0);
+      y[3] = max(max(y[3], -1), -P1); y[4] = min(min(y[4], a.L1), a.Ny - 1 - P1);
+    } else {
+      y[1] = max(max(y[1], 0), P0 - 1); y[2] = min(min(y[2], a.Nx - 1), P0 + a.L0);
+      y[3] = max(max(y[3], 0), P1 - 1); y[4] = min(min(y[4], a.Ny - 1), P1 + a.L1);
+    }
+    const int c = (y[2] >= y[1] && y[4] >= y[3]) ? (y[2] - y[1] + 1) * (y[4] - y[3] + 1) : 0;
+    beg[l + 1] = beg[l] + c;
+  }
+  const int total = beg[nl];
+  double *vals = m.scratch;  // the snapshot is no longer needed
+  for (int k = threadIdx.x; k < total; k += blockDim.x) {
+    int l = 0;
+    while (k >= beg[l + 1]) ++l;
+    const int *y = lay[l];
+    const int w = y[2] - y[1] + 1, r = k - beg[l];
+    const int i = y[1] + r % w, j = y[3] + r / w;
+    double v;
+    switch (y[0]) {
+      case 0: v = a.mHx.at(i, j) + a.mHy.at(i, j); break;
+      case 1: v = a.mEx.at(i, j); break;
+      case 2: v = a.mEy.at(i, j); break;
+      case 3: v = a.Hx.at(i, j) + a.Hy.at(i, j); break;
+      case 4: v = a.Ex.at(i, j); break;
+      default: v = a.Ey.at(i, j); break;
+    }
+    vals[k] = v;
+  }
+  __syncthreads();
+  for (int k = threadIdx.x; k < total; k += blockDim.x) {
+    int l = 0;
+    while (k >= beg[l + 1]) ++l;
+    const int *y = lay[l];
+    const int w = y[2] - y[1] + 1, r = k - beg[l];
+    const int i = y[1] + r % w, j = y[3] + r / w;
+    const double v = vals[k];
+    switch (y[0]) {
+      case 0: a.Hx.at(i + P0, j + P1) = 0.5 * v; a.Hy.at(i + P0, j + P1) = 0.5 * v; break;
+      case 1: a.Ex.at(i + P0, j + P1) = v; break;
+      case 2: a.Ey.at(i + P0, j + P1) = v; break;
+      case 3: a.mHx.at(i - P0, j - P1) = 0.5 * v; a.mHy.at(i - P0, j - P1) = 0.5 * v; break;
+      case 4: a.mEx.at(i - P0, j - P1) = v; break;
+      default: a.mEy.at(i - P0, j - P1) = v; break;
+    }
+  }
+  __syncthreads();
+  check_window_clear(a, ws);
+}
+
+// SCBoundaryCondition::resetOutsideDomain (SCBoundaryCondition.hh:163-195):
+// E = 0 on cells that are neither inside nor a kept cut cell, and on cut
+// cells per component.  cutidx maps a cell to its cut-cell entry or -1.
+__global__ void k_reset_outside(FieldArgs a, const int *cutidx) {
+  const long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (k >= (long long)a.Nx * a.Ny) return;
+  if (a.mask[k]) return;
+  const int i = (int)(k % a.Nx), j = (int)(k / a.Nx);
+  const int c = cutidx[k];
+  if (c < 0) { a.Ex.at(i, j) = 0.0; a.Ey.at(i, j) = 0.0; return; }
+  const CutCellDev cc = a.cells[c];
+  if (cc.l0 < kSpaceEps) a.Ex.at(i, j) = 0.0;
+  if (cc.l1 < kSpaceEps) a.Ey.at(i, j) = 0.0;
+  if (cc.area < kMinArea) { a.Ex.at(i, j) = 0.0; a.Ey.at(i, j) = 0.0; }
+}
+
+// --- host launchers -----------------------------------------------------------
+
+static int sub_grid(FieldArgs &a) {
+  a.tilesX = (a.Nx + kTX - 1) / kTX;
+  a.nbS = a.tilesX * ((a.Ny + kTY - 1) / kTY);
+  a.nbC = (a.ncells + 255) / 256;
+  const int nbM = (a.L0 * a.L1 + 255) / 256;
+  return a.nbS + a.nbC + nbM;
+}
+
+void launch_half_h(FieldArgs a, cudaStream_t s) {
+  const int g = sub_grid(a);
+  k_half_h<<<g, 256, 0, s>>>(a);
+}
+
+void launch_update_e(FieldArgs a, int comp, cudaStream_t s) {
+  const int g = sub_grid(a);
+  if (comp == 0) k_update_e<0><<<g, 256, 0, s>>>(a, 0.0);
+  else k_update_e<1><<<g, 256, 0, s>>>(a, 0.0);
+}
+
+void launch_exchange(FieldArgs a, int which, cudaStream_t s) {
+  const int n = which == 0 ? 2 * (a.L0 + a.L1) + 4 : which == 1 ? 2 * a.L0 + 2 : 2 * a.L1 + 2;
+  k_exchange<<<(n + 127) / 128, 128, 0, s>>>(a, which);
+}
+
+void launch_copy_to_window(FieldArgs a, cudaStream_t s) {
+  k_copy_to_window<<<(a.L0 * a.L1 + 255) / 256, 256, 0, s>>>(a);
+}
+
+void launch_check_window(FieldArgs a, cudaStream_t s) { k_check_window<<<1, 256, 0, s>>>(a); }
+
+void launch_move(FieldArgs a, double *scratch, double h0, double h1, cudaStream_t s) {
+  MoveArgs m{a, scratch, h0, h1};
+  k_move<<<1, 1024, 0, s>>>(m);
+}
+
+void launch_reset_outside(FieldArgs a, const int *cutidx, cudaStream_t s) {
+  const long long n = (long long)a.Nx * a.Ny;
+  k_reset_outside<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(a, cutidx);
+}
+
+}  // namespace csrst

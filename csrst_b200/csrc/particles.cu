@@ -1,0 +1,380 @@
+// Particle kernels: the fused relativistic push (drift + gather + kick +
+// drift + current deposit) and its window bookkeeping, plus stand-alone
+// gather / scatter / deposit kernels behind ScatterGatherImpl and the shape
+// functions.
+//
+// One push kernel replaces PartBunch::push_particles (PartBunch.cpp:215-519):
+//   R0 = R (minus the trailing -dt/2 drift of the previous sub-step when it is
+//        still pending), R1 = R0 + h v(P), gather E, Hz at R1, kick/rotate,
+//   R2 = R1 + h v(P'), deposit J(jcomp) for R0 -> R2.
+// The bounding box of R1 (which fixes the gather patch origin, exactly as
+// getFields does) is produced by the previous push, so each push streams the
+// particles once: 32 B in, 32 B out per particle.
+//
+// The current is accumulated as 64-bit fixed point: each contribution is
+// rounded once to a multiple of 1/scale and integer-added, first in a
+// shared-memory copy of the window per CTA, then into the global window.
+// Integer addition is exact and associative, so the result is bitwise the
+// same for any launch shape, CTA count or scheduling order.
+#include "kernels.cuh"
+#include "shapes.cuh"
+
+namespace csrst {
+
+__device__ __forceinline__ void warp_bbox(double &mn0, double &mn1, double &mx0, double &mx1) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    mn0 = fmin(mn0, __shfl_xor_sync(0xffffffffu, mn0, o));
+    mn1 = fmin(mn1, __shfl_xor_sync(0xffffffffu, mn1, o));
+    mx0 = fmax(mx0, __shfl_xor_sync(0xffffffffu, mx0, o));
+    mx1 = fmax(mx1, __shfl_xor_sync(0xffffffffu, mx1, o));
+  }
+}
+
+// Reduce a per-thread box over the CTA and merge it into dst[4] with atomics.
+__device__ void block_bbox(double mn0, double mn1, double mx0, double mx1, long long *dst) {
+  __shared__ double sb[4][32];
+  warp_bbox(mn0, mn1, mx0, mx1);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+  if (lane == 0) { sb[0][w] = mn0; sb[1][w] = mn1; sb[2][w] = mx0; sb[3][w] = mx1; }
+  __syncthreads();
+  if (w == 0) {
+    mn0 = lane < nw ? sb[0][lane] : INFINITY;
+    mn1 = lane < nw ? sb[1][lane] : INFINITY;
+    mx0 = lane < nw ? sb[2][lane] : -INFINITY;
+    mx1 = lane < nw ? sb[3][lane] : -INFINITY;
+    warp_bbox(mn0, mn1, mx0, mx1);
+    if (lane == 0 && mn0 <= mx0) {
+      atomicMin(&dst[0], dbl_ord(mn0));
+      atomicMin(&dst[1], dbl_ord(mn1));
+      atomicMax(&dst[2], dbl_ord(mx0));
+      atomicMax(&dst[3], dbl_ord(mx1));
+    }
+  }
+  __syncthreads();
+}
+
+__device__ __forceinline__ void bbox_reset(long long *b) {
+  b[0] = dbl_ord(INFINITY); b[1] = dbl_ord(INFINITY);
+  b[2] = dbl_ord(-INFINITY); b[3] = dbl_ord(-INFINITY);
+}
+
+// Positions R1 = R0 + h v(P) of the next push; fills slot `cur` of the window
+// state.  pending: the stored R still owes the -dt/2 drift.
+__global__ void k_bbox_next(const double *x, const double *y, const double *px, const double *py,
+                            long long n, double half, int pending, WinState *ws) {
+  double mn0 = INFINITY, mn1 = INFINITY, mx0 = -INFINITY, mx1 = -INFINITY;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const double p0 = px[i], p1 = py[i];
+    const double r = inv_gamma(p0, p1);
+    const double w0 = half * p0 * r, w1 = half * p1 * r;
+    double a0 = x[i], a1 = y[i];
+    if (pending) { a0 = a0 + (-w0); a1 = a1 + (-w1); }
+    a0 = a0 + w0; a1 = a1 + w1;
+    mn0 = fmin(mn0, a0); mn1 = fmin(mn1, a1); mx0 = fmax(mx0, a0); mx1 = fmax(mx1, a1);
+  }
+  block_bbox(mn0, mn1, mx0, mx1, ws->bb[ws->cur]);
+}
+
+__global__ void k_bbox_clear(WinState *ws, int slot) {
+  if (threadIdx.x == 0) bbox_reset(ws->bb[slot < 0 ? ws->cur : slot]);
+}
+
+// Before a push: derive the gather patches from the particle box of the
+// positions the push will gather at (PartBunch::getLocalPDomain and
+// getFields), and reset the accumulators the push will fill.
+// em: getExtraMarginEdge (x first, x last, y first, y last); cm: getExtraMarginCell.
+__global__ void k_push_prep(WinState *ws, double h0, double h1, int em0, int em2, int cm0) {
+  if (threadIdx.x != 0) return;
+  const int c = ws->cur;
+  const double mn0 = ord_dbl(ws->bb[c][0]), mn1 = ord_dbl(ws->bb[c][1]);
+  const double mx0 = ord_dbl(ws->bb[c][2]), mx1 = ord_dbl(ws->bb[c][3]);
+  int lp[4];
+  if (mn0 <= mx0) {
+    lp[0] = (int)floor((mn0 - ws->mo0) / h0); lp[1] = (int)floor((mx0 - ws->mo0) / h0);
+    lp[2] = (int)floor((mn1 - ws->mo1) / h1); lp[3] = (int)floor((mx1 - ws->mo1) / h1);
+  } else {  // no particles: PartBunch::getLocalPDomain with Rmin = Rmax = 0
+    lp[0] = lp[1] = (int)floor((0.0 - ws->mo0) / h0);
+    lp[2] = lp[3] = (int)floor((0.0 - ws->mo1) / h1);
+  }
+  for (int k = 0; k < 4; ++k) ws->lp[k] = lp[k];
+  const double po0 = ws->mo0 + lp[0] * h0, po1 = ws->mo1 + lp[2] * h1;
+  ws->hz_o0 = po0 + cm0 * h0; ws->hz_o1 = po1 + cm0 * h1;
+  ws->ex_o0 = po0 + em0 * h0; ws->ex_o1 = po1 + em2 * h1;
+  ws->ey_o0 = po0 + em2 * h0; ws->ey_o1 = po1 + em0 * h1;
+  ws->hz_I = lp[0] + cm0; ws->hz_J = lp[2] + cm0;
+  ws->ex_I = lp[0] + em0; ws->ex_J = lp[2] + em2;
+  ws->ey_I = lp[0] + em2; ws->ey_J = lp[2] + em0;
+  bbox_reset(ws->bb[1 - c]);
+  bbox_reset(ws->bball);
+}
+
+// After a push: flip the bbox slot.
+__global__ void k_push_post(WinState *ws) {
+  if (threadIdx.x == 0) ws->cur = 1 - ws->cur;
+}
+
+template <int ORDER, bool SMEM>
+__global__ void __launch_bounds__(256) k_push(PushArgs a) {
+  extern __shared__ unsigned long long sacc[];
+  __shared__ int tb[4];  // touched box of this CTA (window cells)
+  WinState *ws = a.ws;
+  const int L0 = ws->L0, L1 = ws->L1;
+  const int ncell = L0 * L1;
+  if (SMEM) {
+    for (int k = threadIdx.x; k < ncell; k += blockDim.x) sacc[k] = 0ull;
+    if (threadIdx.x == 0) { tb[0] = L0; tb[1] = L1; tb[2] = -1; tb[3] = -1; }
+    __syncthreads();
+  }
+  const double mo0 = ws->mo0, mo1 = ws->mo1;
+  const double h0 = a.h0, h1 = a.h1;
+  const double ood0 = 1.0 / h0, ood1 = 1.0 / h1;
+  const int wp = a.wpitch;
+  // Patch views: relative (0,0) is absolute window index (I, J); the window
+  // plane stores absolute (i, j) at (j + 1) * wp + (i + 1).
+  const PatchView pex{a.mEx + (ptrdiff_t)(ws->ex_J + 1) * wp + (ws->ex_I + 1), wp};
+  const PatchView pey{a.mEy + (ptrdiff_t)(ws->ey_J + 1) * wp + (ws->ey_I + 1), wp};
+  const PatchView phx{a.mHx + (ptrdiff_t)(ws->hz_J + 1) * wp + (ws->hz_I + 1), wp};
+  const PatchView phy{a.mHy + (ptrdiff_t)(ws->hz_J + 1) * wp + (ws->hz_I + 1), wp};
+  const double exo0 = ws->ex_o0, exo1 = ws->ex_o1, eyo0 = ws->ey_o0, eyo1 = ws->ey_o1;
+  const double hzo0 = ws->hz_o0, hzo1 = ws->hz_o1;
+
+  double amn0 = INFINITY, amn1 = INFINITY, amx0 = -INFINITY, amx1 = -INFINITY;  // R0 u R2
+  double bmn0 = INFINITY, bmn1 = INFINITY, bmx0 = -INFINITY, bmx1 = -INFINITY;  // next R1
+  bool overflow = false;
+  const double scale = a.acc_scale;
+  int ti0 = L0, tj0 = L1, ti1 = -1, tj1 = -1;  // cells this thread touched
+  auto sink = [&](int i, int j, double v) {
+    if (i < 0 || j < 0 || i >= L0 || j >= L1) return;
+    const unsigned long long iv = (unsigned long long)__double2ll_rn(v * scale);
+    const int k = j * L0 + i;
+    if (SMEM) {
+      atomicAdd(&sacc[k], iv);
+      ti0 = min(ti0, i); tj0 = min(tj0, j); ti1 = max(ti1, i); tj1 = max(tj1, j);
+    } else {
+      atomicAdd(&a.acc[k], iv);
+    }
+  };
+
+  // Each CTA owns a contiguous slice of the (cell-ordered) particles.
+  const long long per = (a.n + gridDim.x - 1) / gridDim.x;
+  const long long beg = (long long)blockIdx.x * per;
+  const long long end = beg + per < a.n ? beg + per : a.n;
+  for (long long i = beg + threadIdx.x; i < end; i += blockDim.x) {
+    double x = a.x[i], y = a.y[i];
+    double p0 = a.px[i], p1 = a.py[i];
+    const double q = a.q[i];
+    double r = inv_gamma(p0, p1);
+    double w0 = a.half * p0 * r, w1 = a.half * p1 * r;
+    if (a.pending) { x = x + (-w0); y = y + (-w1); }          // drift_particles(-dt/2)
+    const double r0x = x, r0y = y;                             // oldR
+    x = x + w0; y = y + w1;                                    // R1
+    // gather (FieldPatch::gather x3; Hz = Hzx + Hzy on the fly)
+    const double E0 = gather_edge<ORDER>(pex, (x - exo0) * ood0, (y - exo1) * ood1, 0);
+    const double E1 = gather_edge<ORDER>(pey, (x - eyo0) * ood0, (y - eyo1) * ood1, 1);
+    const double hpp0 = (x - hzo0) * ood0, hpp1 = (y - hzo1) * ood1;
+    const double Hf = gather_cell<ORDER>(SumView{phx, phy}, hpp0, hpp1);
+    // hard-edge dipole
+    const double D0 = x - a.Lb, D1 = y - a.hw;
+    const double dist = a.chh * D0 - a.shh * D1;
+    const double bext = (dist > 0.0 && dist < a.bwidth) ? a.bz : 0.0;
+    const double B = kMu0 * Hf + 0.5 * bext;
+    // kick + rotation (PartBunch.cpp:366-383)
+    const double k0 = a.fact1 * E0, k1 = a.fact1 * E1;
+    double u0 = p0 + k0, u1 = p1 + k1;
+    const double aa = a.fact2 * B * inv_gamma(u0, u1);
+    const double s0 = u0 + aa * u1, s1 = u1 + aa * (-u0);
+    const double tmp = 1.0 + aa * aa;
+    u0 = ((1.0 + aa * aa) * s0 + aa * s1) / tmp;
+    u1 = ((1.0 + aa * aa) * s1 - aa * s0) / tmp;
+    p0 = u0 + k0; p1 = u1 + k1;
+    r = inv_gamma(p0, p1);
+    w0 = a.half * p0 * r; w1 = a.half * p1 * r;
+    x = x + w0; y = y + w1;                                    // R2
+    a.x[i] = x; a.y[i] = y; a.px[i] = p0; a.py[i] = p1;
+    // current deposit R0 -> R2 in window coordinates
+    if (!deposit_particle<ORDER>(a.jcomp, q, r0x, r0y, x, y, mo0, mo1, h0, h1, a.dt, sink))
+      overflow = true;
+    amn0 = fmin(amn0, fmin(x, r0x)); amn1 = fmin(amn1, fmin(y, r0y));
+    amx0 = fmax(amx0, fmax(x, r0x)); amx1 = fmax(amx1, fmax(y, r0y));
+    // next push gathers at (R2 - h v) + h v
+    const double nx = (x + (-w0)) + w0, ny = (y + (-w1)) + w1;
+    bmn0 = fmin(bmn0, nx); bmn1 = fmin(bmn1, ny); bmx0 = fmax(bmx0, nx); bmx1 = fmax(bmx1, ny);
+  }
+  if (overflow) set_err(ws, kErrCrossings);
+  block_bbox(amn0, amn1, amx0, amx1, ws->bball);
+  block_bbox(bmn0, bmn1, bmx0, bmx1, ws->bb[1 - ws->cur]);
+  if (SMEM) {
+    if (ti1 >= 0) { atomicMin(&tb[0], ti0); atomicMin(&tb[1], tj0); atomicMax(&tb[2], ti1); atomicMax(&tb[3], tj1); }
+    __syncthreads();
+    const int i0 = tb[0], j0 = tb[1], i1 = tb[2], j1 = tb[3];
+    if (i1 >= i0) {
+      const int w = i1 - i0 + 1, cnt = w * (j1 - j0 + 1);
+      for (int k = threadIdx.x; k < cnt; k += blockDim.x) {
+        const int i = i0 + k % w, j = j0 + k / w;
+        const unsigned long long v = sacc[j * L0 + i];
+        if (v) atomicAdd(&a.acc[j * L0 + i], v);
+      }
+    }
+  }
+}
+
+// After the last push of a step: the deposit's particle bounds relative to
+// the window (PartBunch::getLocalPDomainInclOld -> setGlobalBounds).
+__global__ void k_global_bounds(WinState *ws, double h0, double h1) {
+  if (threadIdx.x != 0) return;
+  const double mn0 = ord_dbl(ws->bball[0]), mn1 = ord_dbl(ws->bball[1]);
+  const double mx0 = ord_dbl(ws->bball[2]), mx1 = ord_dbl(ws->bball[3]);
+  if (!(mn0 <= mx0)) { ws->gb[0] = 0; ws->gb[1] = -1; ws->gb[2] = 0; ws->gb[3] = -1; return; }
+  ws->gb[0] = (int)floor((mn0 - ws->mo0) / h0);
+  ws->gb[1] = (int)floor((mx0 - ws->mo0) / h0);
+  ws->gb[2] = (int)floor((mn1 - ws->mo1) / h1);
+  ws->gb[3] = (int)floor((mx1 - ws->mo1) / h1);
+}
+
+// Stand-alone drift (PartBunch::drift_particles, PartBunch.cpp:179-187).
+__global__ void k_drift(double *x, double *y, const double *px, const double *py, long long n,
+                        double full) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const double p0 = px[i], p1 = py[i];
+    const double r = inv_gamma(p0, p1);
+    x[i] += full * p0 * r;
+    y[i] += full * p1 * r;
+  }
+}
+
+// --- stand-alone ScatterGatherImpl / ShapeFunction kernels --------------------
+
+template <int ORDER>
+__global__ void k_gather(int comp, const double *patch, int nx, double o0, double o1, double h0,
+                         double h1, const double *x, const double *y, long long n, double *out) {
+  const PatchView f{patch, nx};
+  const double ood0 = 1.0 / h0, ood1 = 1.0 / h1;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const double pp0 = (x[i] - o0) * ood0, pp1 = (y[i] - o1) * ood1;
+    out[i] = comp < 2 ? gather_edge<ORDER>(f, pp0, pp1, comp) : gather_cell<ORDER>(f, pp0, pp1);
+  }
+}
+
+// Deposit of stand-alone particle arrays into a dense fixed-point patch at
+// absolute index (i0, j0) of a mesh with origin (org0, org1).
+template <int ORDER>
+__global__ void k_deposit(int comp, const double *ox, const double *oy, const double *x,
+                          const double *y, const double *q, long long n, double org0, double org1,
+                          double h0, double h1, double dt, int i0, int j0, int ni, int nj,
+                          unsigned long long *acc, double scale, int *err) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    auto sink = [&](int a, int b, double v) {
+      a -= i0; b -= j0;
+      if (a < 0 || b < 0 || a >= ni || b >= nj) return;
+      atomicAdd(&acc[(size_t)b * ni + a], (unsigned long long)__double2ll_rn(v * scale));
+    };
+    if (!deposit_particle<ORDER>(comp, q[i], ox[i], oy[i], x[i], y[i], org0, org1, h0, h1, dt, sink))
+      atomicExch(err, kErrCrossings);
+  }
+}
+
+__global__ void k_fixed_to_double(const unsigned long long *acc, double *out, long long n, double inv) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    out[i] = (double)(long long)acc[i] * inv;
+}
+
+// --- host launchers -----------------------------------------------------------
+
+void launch_bbox_next(const double *x, const double *y, const double *px, const double *py,
+                      long long n, double half, int pending, WinState *ws, cudaStream_t s) {
+  k_bbox_clear<<<1, 32, 0, s>>>(ws, -1);
+  const int blocks = n > 0 ? (int)((n + 255) / 256 < 1184 ? (n + 255) / 256 : 1184) : 1;
+  k_bbox_next<<<blocks, 256, 0, s>>>(x, y, px, py, n, half, pending, ws);
+}
+
+void launch_push_prep(WinState *ws, double h0, double h1, int order, cudaStream_t s) {
+  int em0, em2, cm0;
+  if (order == 0) { em0 = -1; em2 = 0; cm0 = -1; }
+  else if (order == 1) { em0 = -1; em2 = -1; cm0 = -1; }
+  else { em0 = -2; em2 = -1; cm0 = -2; }
+  k_push_prep<<<1, 32, 0, s>>>(ws, h0, h1, em0, em2, cm0);
+}
+
+int push_smem_limit() {
+  static int lim = -1;
+  if (lim < 0) {
+    int dev = 0, v = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    lim = v - 1024;
+  }
+  return lim;
+}
+
+template <int ORDER>
+static void push_order(const PushArgs &a, int L0, int L1, int grid, cudaStream_t s) {
+  const size_t sm = (size_t)L0 * L1 * sizeof(unsigned long long);
+  if (a.use_smem && (long long)sm <= push_smem_limit()) {
+    static bool attr = false;
+    if (!attr) {
+      cudaFuncSetAttribute(k_push<ORDER, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           push_smem_limit());
+      attr = true;
+    }
+    k_push<ORDER, true><<<grid, 256, sm, s>>>(a);
+  } else {
+    k_push<ORDER, false><<<grid, 256, 0, s>>>(a);
+  }
+}
+
+void launch_push(const PushArgs &a, int order, int L0, int L1, int grid, cudaStream_t s) {
+  if (order == 0) push_order<0>(a, L0, L1, grid, s);
+  else if (order == 1) push_order<1>(a, L0, L1, grid, s);
+  else push_order<2>(a, L0, L1, grid, s);
+  k_push_post<<<1, 32, 0, s>>>(a.ws);
+}
+
+void launch_global_bounds(WinState *ws, double h0, double h1, cudaStream_t s) {
+  k_global_bounds<<<1, 32, 0, s>>>(ws, h0, h1);
+}
+
+void launch_drift(double *x, double *y, const double *px, const double *py, long long n, double full,
+                  cudaStream_t s) {
+  if (n <= 0) return;
+  const int blocks = (int)((n + 255) / 256 < 4096 ? (n + 255) / 256 : 4096);
+  k_drift<<<blocks, 256, 0, s>>>(x, y, px, py, n, full);
+}
+
+void launch_gather(int order, int comp, const double *patch, int nx, double o0, double o1,
+                   double h0, double h1, const double *x, const double *y, long long n, double *out,
+                   cudaStream_t s) {
+  if (n <= 0) return;
+  const int blocks = (int)((n + 255) / 256 < 4096 ? (n + 255) / 256 : 4096);
+  if (order == 0) k_gather<0><<<blocks, 256, 0, s>>>(comp, patch, nx, o0, o1, h0, h1, x, y, n, out);
+  else if (order == 1) k_gather<1><<<blocks, 256, 0, s>>>(comp, patch, nx, o0, o1, h0, h1, x, y, n, out);
+  else k_gather<2><<<blocks, 256, 0, s>>>(comp, patch, nx, o0, o1, h0, h1, x, y, n, out);
+}
+
+void launch_deposit(int order, int comp, const double *ox, const double *oy, const double *x,
+                    const double *y, const double *q, long long n, double org0, double org1,
+                    double h0, double h1, double dt, int i0, int j0, int ni, int nj,
+                    unsigned long long *acc, double scale, int *err, cudaStream_t s) {
+  if (n <= 0) return;
+  const int blocks = (int)((n + 255) / 256 < 4096 ? (n + 255) / 256 : 4096);
+  if (order == 0)
+    k_deposit<0><<<blocks, 256, 0, s>>>(comp, ox, oy, x, y, q, n, org0, org1, h0, h1, dt, i0, j0, ni, nj, acc, scale, err);
+  else if (order == 1)
+    k_deposit<1><<<blocks, 256, 0, s>>>(comp, ox, oy, x, y, q, n, org0, org1, h0, h1, dt, i0, j0, ni, nj, acc, scale, err);
+  else
+    k_deposit<2><<<blocks, 256, 0, s>>>(comp, ox, oy, x, y, q, n, org0, org1, h0, h1, dt, i0, j0, ni, nj, acc, scale, err);
+}
+
+void launch_fixed_to_double(const unsigned long long *acc, double *out, long long n, double inv,
+                            cudaStream_t s) {
+  if (n <= 0) return;
+  const int blocks = (int)((n + 255) / 256 < 4096 ? (n + 255) / 256 : 4096);
+  k_fixed_to_double<<<blocks, 256, 0, s>>>(acc, out, n, inv);
+}
+
+}  // namespace csrst

@@ -1,0 +1,322 @@
+// Device shape functions: field gather (ScatterGatherImpl) and the
+// charge-conserving current deposit (Zeroth/First/SecondOrderShapeFunction).
+//
+// The arithmetic keeps the reference's operation order so that, built with
+// --fmad=false, every gathered value and every deposit weight is the same
+// IEEE double the reference computes.  ORDER 0 = IntCIC with the
+// Villasenor-Buneman deposit, 1 = IntS1 (TSC) with the S1 x S2 deposit,
+// 2 = IntS2 (cubic) with the S2 x S3 deposit.
+#pragma once
+
+#include "common.cuh"
+
+namespace csrst {
+
+// A read-only view of a field patch: value(I, J) for patch-relative indices.
+struct PatchView {
+  const double *base;  // address of patch-relative (0, 0)
+  int pitch;
+  __device__ __forceinline__ double operator()(int i, int j) const {
+    return __ldg(base + (ptrdiff_t)j * pitch + i);
+  }
+};
+
+// Hz patch built from the split components, Hz = Hzx + Hzy element by element
+// (PartBunch::getFields, PartBunch.cpp:1012-1017).
+struct SumView {
+  PatchView a, b;
+  __device__ __forceinline__ double operator()(int i, int j) const { return a(i, j) + b(i, j); }
+};
+
+// --- gather -----------------------------------------------------------------
+
+// Edge component `comp` at patch coordinates (pp0, pp1) = (R - origin) / h.
+// ScatterGatherImpl.hh:69-104 (CIC), :201-253 (S1), :406-468 (S2).
+template <int ORDER, class F>
+__device__ __forceinline__ double gather_edge(const F &f, double pp0, double pp1, int comp) {
+  if (ORDER == 0) {
+    long l0 = (long)floor(pp0 + (comp == 0 ? 0.5 : 0.0));
+    long l1 = (long)floor(pp1 + (comp == 1 ? 0.5 : 0.0));
+    if (comp == 0) l0 -= 1; else l1 -= 1;
+    double g0 = (double)l0, g1 = (double)l1;
+    if (comp == 0) g0 += 0.5; else g1 += 0.5;
+    const double d0 = pp0 - g0, d1 = pp1 - g1;
+    const int I = (int)l0, J = (int)l1;
+    return ((1 - d1) * ((1 - d0) * f(I, J) + d0 * f(I + 1, J)) +
+            d1 * ((1 - d0) * f(I, J + 1) + d0 * f(I + 1, J + 1)));
+  } else if (ORDER == 1) {
+    long l0 = (long)floor(pp0 + (comp == 0 ? 0.0 : 0.5));
+    long l1 = (long)floor(pp1 + (comp == 1 ? 0.0 : 0.5));
+    double g0 = (double)l0, g1 = (double)l1;
+    if (comp == 0) g0 += 0.5; else g1 += 0.5;
+    const double d0 = pp0 - g0, d1 = pp1 - g1;
+    const double bx = 0.75 - d0 * d0, cx = 0.5 * (0.5 + d0) * (0.5 + d0), ax = 1.0 - (bx + cx);
+    const double by = 0.75 - d1 * d1, cy = 0.5 * (0.5 + d1) * (0.5 + d1), ay = 1.0 - (by + cy);
+    const int I = (int)l0, J = (int)l1;
+    return (ay * (ax * f(I - 1, J - 1) + bx * f(I, J - 1) + cx * f(I + 1, J - 1)) +
+            by * (ax * f(I - 1, J) + bx * f(I, J) + cx * f(I + 1, J)) +
+            cy * (ax * f(I - 1, J + 1) + bx * f(I, J + 1) + cx * f(I + 1, J + 1)));
+  } else {
+    long l0 = (long)floor(pp0 + (comp == 0 ? 0.5 : 0.0));
+    long l1 = (long)floor(pp1 + (comp == 1 ? 0.5 : 0.0));
+    if (comp == 0) l0 -= 1; else l1 -= 1;
+    double g0 = (double)l0, g1 = (double)l1;
+    if (comp == 0) g0 += 0.5; else g1 += 0.5;
+    const double d0 = pp0 - g0, d1 = pp1 - g1;
+    const double q0 = d0 * d0, q1 = d1 * d1;
+    const double t23 = 2.0 / 3.0, t16 = 1.0 / 6.0;
+    const double bx = t23 - q0 * (1 - 0.5 * d0), cx = t23 - 0.5 * (1 - d0) * (1 - q0), ex = t16 * q0 * d0;
+    const double ax = 1.0 - (bx + cx + ex);
+    const double by = t23 - q1 * (1 - 0.5 * d1), cy = t23 - 0.5 * (1 - d1) * (1 - q1), ey = t16 * q1 * d1;
+    const double ay = 1.0 - (by + cy + ey);
+    const int I = (int)l0, J = (int)l1;
+    // The last term reads (I+1, J+2), as the reference does (ScatterGatherImpl.hh:467).
+    return (ay * (ax * f(I - 1, J - 1) + bx * f(I, J - 1) + cx * f(I + 1, J - 1) + ex * f(I + 2, J - 1)) +
+            by * (ax * f(I - 1, J) + bx * f(I, J) + cx * f(I + 1, J) + ex * f(I + 2, J)) +
+            cy * (ax * f(I - 1, J + 1) + bx * f(I, J + 1) + cx * f(I + 1, J + 1) + ex * f(I + 2, J + 1)) +
+            ey * (ax * f(I - 1, J + 2) + bx * f(I, J + 2) + cx * f(I + 1, J + 2) + ex * f(I + 1, J + 2)));
+  }
+}
+
+// Cell-centred field.  ScatterGatherImpl.hh:106-134, :255-301, :470-527.
+template <int ORDER, class F>
+__device__ __forceinline__ double gather_cell(const F &f, double pp0, double pp1) {
+  if (ORDER == 0) {
+    const long l0 = (long)floor(pp0 - 0.5), l1 = (long)floor(pp1 - 0.5);
+    const double d0 = pp0 - (l0 + 0.5), d1 = pp1 - (l1 + 0.5);
+    const int I = (int)l0, J = (int)l1;
+    return ((1 - d1) * ((1 - d0) * f(I, J) + d0 * f(I + 1, J)) +
+            d1 * ((1 - d0) * f(I, J + 1) + d0 * f(I + 1, J + 1)));
+  } else if (ORDER == 1) {
+    const long l0 = (long)floor(pp0), l1 = (long)floor(pp1);
+    const double d0 = pp0 - (l0 + 0.5), d1 = pp1 - (l1 + 0.5);
+    const double bx = 0.75 - d0 * d0, cx = 0.5 * (0.5 + d0) * (0.5 + d0), ax = 1.0 - (bx + cx);
+    const double by = 0.75 - d1 * d1, cy = 0.5 * (0.5 + d1) * (0.5 + d1), ay = 1.0 - (by + cy);
+    const int I = (int)l0, J = (int)l1;
+    return (ay * (ax * f(I - 1, J - 1) + bx * f(I, J - 1) + cx * f(I + 1, J - 1)) +
+            by * (ax * f(I - 1, J) + bx * f(I, J) + cx * f(I + 1, J)) +
+            cy * (ax * f(I - 1, J + 1) + bx * f(I, J + 1) + cx * f(I + 1, J + 1)));
+  } else {
+    const long l0 = (long)floor(pp0 - 0.5), l1 = (long)floor(pp1 - 0.5);
+    const double d0 = pp0 - (l0 + 0.5), d1 = pp1 - (l1 + 0.5);
+    const double q0 = d0 * d0, q1 = d1 * d1;
+    const double t23 = 2.0 / 3.0, t16 = 1.0 / 6.0;
+    const double bx = t23 - q0 * (1 - 0.5 * d0), cx = t23 - 0.5 * (1 - d0) * (1 - q0), ex = t16 * q0 * d0;
+    const double ax = 1.0 - (bx + cx + ex);
+    const double by = t23 - q1 * (1 - 0.5 * d1), cy = t23 - 0.5 * (1 - d1) * (1 - q1), ey = t16 * q1 * d1;
+    const double ay = 1.0 - (by + cy + ey);
+    const int I = (int)l0, J = (int)l1;
+    return (ay * (ax * f(I - 1, J - 1) + bx * f(I, J - 1) + cx * f(I + 1, J - 1) + ex * f(I + 2, J - 1)) +
+            by * (ax * f(I - 1, J) + bx * f(I, J) + cx * f(I + 1, J) + ex * f(I + 2, J)) +
+            cy * (ax * f(I - 1, J + 1) + bx * f(I, J + 1) + cx * f(I + 1, J + 1) + ex * f(I + 2, J + 1)) +
+            ey * (ax * f(I - 1, J + 2) + bx * f(I, J + 2) + cx * f(I + 1, J + 2) + ex * f(I + 1, J + 2)));
+  }
+}
+
+// --- deposit ----------------------------------------------------------------
+
+constexpr int kMaxCross = 12;  // end points + border crossings kept per push
+
+struct Cross {
+  double f, s0, s1;
+};
+
+// Border crossings of the segment old -> new (positions relative to the mesh
+// origin): src/utils.hh:427-489 (cell borders) and :364-425 (dual cells,
+// DUAL = true).  The interior entries are sorted by fraction with a stable
+// insertion sort (what libstdc++ std::sort does on so few items) and merged
+// when two fractions differ by less than 1e-6 (std::unique with samePos).
+// Returns the number of points, or -1 if more crossings than kMaxCross.
+template <bool DUAL>
+__device__ __forceinline__ int border_crossings(Cross *xs, double o0, double o1, double n0, double n1,
+                                                double h0, double h1) {
+  int Ii, Ji, If, Jf;
+  if (DUAL) {
+    Ii = (int)floor(o0 / h0 - 0.5); Ji = (int)floor(o1 / h1 - 0.5);
+    If = (int)floor(n0 / h0 - 0.5); Jf = (int)floor(n1 / h1 - 0.5);
+  } else {
+    Ii = (int)floor(o0 / h0); Ji = (int)floor(o1 / h1);
+    If = (int)floor(n0 / h0); Jf = (int)floor(n1 / h1);
+  }
+  const int nx = abs(If - Ii), ny = abs(Jf - Ji);
+  if (nx + ny + 2 > kMaxCross) return -1;
+  const double D0 = n0 - o0, D1 = n1 - o1;
+  int n = 0;
+  xs[n++].f = 0.0;
+  int I = Ii, J = Ji;
+  while (I < If) {
+    const double x = DUAL ? h0 * (I + 1.5) : h0 * (I + 1);
+    const double f = (x - o0) / D0;
+    xs[n].f = f; xs[n].s0 = x; xs[n].s1 = o1 + f * D1; ++I; ++n;
+  }
+  while (I > If) {
+    const double x = DUAL ? h0 * (I + 0.5) : h0 * I;
+    const double f = (x - o0) / D0;
+    xs[n].f = f; xs[n].s0 = x; xs[n].s1 = o1 + f * D1; --I; ++n;
+  }
+  while (J < Jf) {
+    const double y = DUAL ? h1 * (J + 1.5) : h1 * (J + 1);
+    const double f = (y - o1) / D1;
+    xs[n].f = f; xs[n].s0 = o0 + f * D0; xs[n].s1 = y; ++J; ++n;
+  }
+  while (J > Jf) {
+    const double y = DUAL ? h1 * (J + 0.5) : h1 * J;
+    const double f = (y - o1) / D1;
+    xs[n].f = f; xs[n].s0 = o0 + f * D0; xs[n].s1 = y; --J; ++n;
+  }
+  xs[n++].f = 1.0;
+  for (int a = 2; a < n - 1; ++a) {  // stable insertion sort of xs[1 .. n-2]
+    Cross v = xs[a];
+    int b = a;
+    while (b > 1 && v.f < xs[b - 1].f) { xs[b] = xs[b - 1]; --b; }
+    xs[b] = v;
+  }
+  int dest = 0;
+  for (int k = 1; k < n; ++k)
+    if (!(fabs(xs[dest].f - xs[k].f) < 1e-6)) xs[++dest] = xs[k];
+  const int num = dest + 1;
+  xs[0].s0 = o0; xs[0].s1 = o1;
+  xs[num - 1].s0 = n0; xs[num - 1].s1 = n1;
+  return num;
+}
+
+// Calls sink(i, j, value) for every current contribution of one particle
+// moving old -> new (absolute positions; the mesh origin is org; indices are
+// mesh cells).  Returns false on a crossing overflow.
+template <int ORDER, class Sink>
+__device__ __forceinline__ bool deposit_particle(int comp, double q, double ao0, double ao1, double an0,
+                                                 double an1, double org0, double org1, double h0, double h1,
+                                                 double dt, Sink &&sink) {
+  Cross xs[kMaxCross];
+  // crossings are taken relative to the mesh origin (utils.hh:435-436)
+  const double o0 = ao0 - org0, o1 = ao1 - org1, n0 = an0 - org0, n1 = an1 - org1;
+  const double ood0 = 1.0 / h0, ood1 = 1.0 / h1;
+  if (ORDER == 0) {
+    // ZerothOrderShapeFunction.cpp:171-294
+    const double oodt0 = 1.0 / (h1 * dt), oodt1 = 1.0 / (h0 * dt);
+    const int n = border_crossings<false>(xs, o0, o1, n0, n1, h0, h1);
+    if (n < 0) return false;
+    for (int k = 0; k + 1 < n; ++k) {
+      const double xi0 = xs[k].s0 * ood0, xi1 = xs[k].s1 * ood1;
+      const double xf0 = xs[k + 1].s0 * ood0, xf1 = xs[k + 1].s1 * ood1;
+      const double c0 = (xi0 + xf0) * 0.5, c1 = (xi1 + xf1) * 0.5;
+      const int I = (int)floor(c0), J = (int)floor(c1);
+      if (comp == 0) {
+        const double D0 = q * (xf0 - xi0) * oodt0;
+        sink(I, J, D0 * (J + 1 - c1));
+        sink(I, J + 1, D0 * (c1 - J));
+      } else {
+        const double D1 = q * (xf1 - xi1) * oodt1;
+        sink(I, J, D1 * (I + 1 - c0));
+        sink(I + 1, J, D1 * (c0 - I));
+      }
+    }
+    return true;
+  }
+  // the full displacement uses the absolute positions (R - oldR)
+  const double Dx0 = an0 - ao0, Dx1 = an1 - ao1;
+  const double cov = sqrt(Dx0 * Dx0 + Dx1 * Dx1);
+  if (cov == 0.0) return true;  // a particle that does not move carries no current
+  const double oodt0 = ood0 / dt, oodt1 = ood1 / dt;
+  const double dl0 = Dx0 * ood0, dl1 = Dx1 * ood1;
+  const double half = 0.5, onethird = 1.0 / 3.0;
+  const int n = border_crossings<ORDER == 1>(xs, o0, o1, n0, n1, h0, h1);
+  if (n < 0) return false;
+  for (int k = 0; k + 1 < n; ++k) {
+    const double xi0 = xs[k].s0 * ood0, xi1 = xs[k].s1 * ood1;
+    const double xf0 = xs[k + 1].s0 * ood0, xf1 = xs[k + 1].s1 * ood1;
+    const double sg0 = xs[k + 1].s0 - xs[k].s0, sg1 = xs[k + 1].s1 - xs[k].s1;
+    const double tau = sqrt(sg0 * sg0 + sg1 * sg1) / cov;
+    if (ORDER == 1) {
+      // FirstOrderShapeFunction.cpp:179-329 with getCurrentX/Y (:540-683):
+      // integral of S1 along the current times S2 across it, in tau.
+      const double c0 = (xi0 + xf0) * 0.5, c1 = (xi1 + xf1) * 0.5;
+      const int I = (int)floor(c0 + 0.5), J = (int)floor(c1 + 0.5);
+      const double a_al = comp == 0 ? (I + 0.5 - xi0) : (J + 0.5 - xi1);   // along the current
+      const double b_cr = comp == 0 ? (J - xi1) : (I - xi0);               // across it
+      const double d_al = comp == 0 ? dl0 : dl1, d_cr = comp == 0 ? dl1 : dl0;
+      const double cd = comp == 0 ? (q * oodt1) * dl0 : (q * oodt0) * dl1;
+      const double onefourth = half * half;
+      const double tp2 = tau * tau * half;
+      const double tp3 = tp2 * tau * 2 * onethird;
+      const double Am = a_al, Bm = -d_al * tau, A0 = 1.0 - a_al, B0 = d_al * tau;
+      double A2[3], B2[3], C2[3];
+      A2[0] = half * (half + b_cr) * (half + b_cr) * tau;
+      B2[0] = -(half + b_cr) * d_cr * tp2;
+      C2[0] = half * d_cr * d_cr * tp3;
+      A2[1] = (0.75 - b_cr * b_cr) * tau;
+      B2[1] = 2 * b_cr * d_cr * tp2;
+      C2[1] = -d_cr * d_cr * tp3;
+      A2[2] = half * (half - b_cr) * (half - b_cr) * tau;
+      B2[2] = (half - b_cr) * d_cr * tp2;
+      C2[2] = half * d_cr * d_cr * tp3;
+#pragma unroll
+      for (int t = 0; t < 3; ++t) {
+        const double s = A2[t] + B2[t] + C2[t];
+        const double m = half * A2[t] + onethird * B2[t] + onefourth * C2[t];
+        const double jm = cd * ((Am + Bm) * s - Bm * m);
+        const double j0 = cd * ((A0 + B0) * s - B0 * m);
+        if (comp == 0) { sink(I - 1, J - 1 + t, jm); sink(I, J - 1 + t, j0); }
+        else { sink(I - 1 + t, J - 1, jm); sink(I - 1 + t, J, j0); }
+      }
+    } else {
+      // SecondOrderShapeFunction.cpp:179-346 with getCurrentX/Y (:583-826):
+      // S2 along the current times S3 across it.
+      const double c0 = 0.5 * (xi0 + xf0), c1 = 0.5 * (xi1 + xf1);
+      const int I = (int)(long)floor(c0), J = (int)(long)floor(c1);
+      const double a0 = I + 0.5 - xi0, a1 = J + 0.5 - xi1;
+      const double b0 = I - xi0, b1 = J - xi1;
+      const double tp2 = tau * tau / 2;
+      const double tp3 = tp2 * tau * 2 / 3;
+      const double tp4 = tp2 * tp2;
+      const double onefourth = 0.25, onefifth = 0.2, onesixth = half * onethird;
+      const double a = comp == 0 ? a0 : a1, dl = comp == 0 ? dl0 : dl1, dl2 = dl * dl;
+      const double b = comp == 0 ? b1 : b0, de = comp == 0 ? dl1 : dl0;
+      const double de2 = de * de, de3 = de2 * de;
+      const double cd = comp == 0 ? (q * oodt1) * dl0 : (q * oodt0) * dl1;
+      double sA[3], sB[3], sC[3];
+      if (comp == 0) {
+        sA[0] = half * (half + a) * (half + a); sC[0] = half * dl2 * tp2;
+        sA[2] = half * (0.5 - a) * (0.5 - a);   sC[2] = half * dl2 * tp2;
+      } else {
+        sA[0] = (half + a) * (half + a) * half; sC[0] = dl2 * half * tp2;
+        sA[2] = (half - a) * (half - a) * half; sC[2] = dl2 * half * tp2;
+      }
+      sB[0] = -(half + a) * dl * tau;
+      sA[1] = 0.75 - a * a; sB[1] = 2 * a * dl * tau; sC[1] = -dl2 * tp2;
+      sB[2] = (half - a) * dl * tau;
+      double tA[4], tB[4], tC[4], tD[4];
+      tA[0] = (1 + b) * (1 + b) * (1 + b) * onesixth * tau;
+      tB[0] = -(1 + b) * (1 + b) * de * half * tp2;
+      tC[0] = (1 + b) * de2 * half * tp3;
+      tD[0] = -de3 * onesixth * tp4;
+      tA[1] = (4 - 3 * b * b * (2 + b)) * onesixth * tau;
+      tB[1] = b * de * (3 * b + 4) * half * tp2;
+      tC[1] = -de2 * (2 + 3 * b) * half * tp3;
+      tD[1] = de3 * half * tp4;
+      tA[2] = (4 - 3 * (b + 1) * (b + 1) * (1 - b)) * onesixth * tau;
+      tB[2] = (1 - 2 * b - 3 * b * b) * de * half * tp2;
+      tC[2] = (1 + 3 * b) * de2 * half * tp3;
+      tD[2] = -de3 * half * tp4;
+      tA[3] = -b * b * b * onesixth * tau;
+      tB[3] = b * b * de * half * tp2;
+      tC[3] = -b * de2 * half * tp3;
+      tD[3] = de3 * onesixth * tp4;
+#pragma unroll
+      for (int t = 0; t < 4; ++t) {
+#pragma unroll
+        for (int s = 0; s < 3; ++s) {
+          const double v = cd * ((sA[s] + sB[s] + sC[s]) * (tD[t] + tC[t] + tB[t] + tA[t])
+                                 + (sC[s] * (tD[t] - tA[t]) - sB[s] * tB[t]) * onethird
+                                 + (sC[s] * tC[t] - sB[s] * tD[t]) * onefifth
+                                 - sB[s] * tC[t] * onefourth - sB[s] * tA[t] * half);
+          if (comp == 0) sink(I - 1 + s, J - 1 + t, v);
+          else sink(I - 1 + t, J - 1 + s, v);
+        }
+      }
+    }
+  }
+  return true;
+}
+
+}  // namespace csrst

@@ -1,0 +1,233 @@
+"""Host-side mirror of the reference's PIC-loop interfaces over the C ABI.
+
+Class and method names follow the reference so that a caller of TETMSolver,
+PartBunch and ScatterGatherImpl finds the same operations:
+
+  TETMSolver.updateField_firstStep / updateField_secondStep   (TETMSolver.hh:50-70)
+  PartBunch.push_particles / drift_particles / calcBeamParameters /
+            getGlobalBounds                                   (PartBunch.hh:46-112)
+  ScatterGatherImpl.gather                                    (ScatterGatherImpl.hh:27-64)
+  ShapeFunction.getCurrentDensityBase / getChargeDensityDiff  (ShapeFunction.hh:141-508)
+  moveMesh                                                    (main.cpp:562-652)
+  IntegrateElong (per-step E_s samples)                       (IntegrateElong.cpp:38-89)
+
+All state lives on the GPU in one csrst handle; nothing here computes physics.
+"""
+import ctypes as C
+
+import numpy as np
+
+from ._lib import Config, check, f64, lib, ptr, D
+
+IntCIC, IntS1, IntS2 = 0, 1, 2
+
+
+class Simulation:
+    """Owns one csrst handle: static mesh, moving window and bunch."""
+
+    def __init__(self, cfg, keep_old=False):
+        c = Config()
+        for k, v in cfg.dict().items():
+            setattr(c, k, v)
+        if keep_old:
+            c.flags |= 1
+        self.cfg = cfg
+        h = C.c_void_p()
+        check(lib().csrst_create(C.byref(c), C.byref(h)))
+        self._h = h
+        self.Nx, self.Ny = cfg.Nx, cfg.Ny
+        self.n = 0
+
+    @property
+    def h(self):
+        if self._h is None:
+            raise RuntimeError("handle destroyed")
+        return self._h
+
+    def close(self):
+        if getattr(self, "_h", None) is not None:
+            lib().csrst_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _ck(self, code):
+        check(code, self.h)
+
+    # -- set-up ---------------------------------------------------------------
+    def info(self):
+        out = np.zeros(8)
+        self._ck(lib().csrst_get_info(self.h, ptr(out)))
+        return dict(zip(("hx", "hy", "ox", "oy", "dt", "fixed_scale", "ncells", "wpitch"), out.tolist()))
+
+    def geometry(self):
+        inside = np.zeros(self.Nx * self.Ny, np.uint8)
+        n = C.c_long()
+        self._ck(lib().csrst_get_geometry(self.h, inside.ctypes.data_as(C.POINTER(C.c_uint8)), None, 0,
+                                          C.byref(n)))
+        cells = np.zeros((max(n.value, 1), 7))
+        self._ck(lib().csrst_get_geometry(self.h, None, ptr(cells), n.value, C.byref(n)))
+        return inside.reshape(self.Ny, self.Nx), cells[:n.value]
+
+    def set_static(self, ex, ey, hzx, hzy):
+        a = [f64(v).reshape(-1) for v in (ex, ey, hzx, hzy)]
+        self._ck(lib().csrst_set_static_fields(self.h, *map(ptr, a)))
+
+    def get_static(self):
+        a = [np.zeros(self.Nx * self.Ny) for _ in range(4)]
+        self._ck(lib().csrst_get_static_fields(self.h, *map(ptr, a)))
+        return [v.reshape(self.Ny, self.Nx) for v in a]
+
+    def reset_outside(self):
+        self._ck(lib().csrst_reset_outside(self.h))
+
+    def load(self, x, y, px, py, q):
+        a = list(map(f64, (x, y, px, py, q)))
+        self.n = len(a[0])
+        self._ck(lib().csrst_load_particles(self.h, *map(ptr, a), self.n))
+
+    # -- state ----------------------------------------------------------------
+    def particles(self):
+        a = [np.zeros(self.n) for _ in range(4)]
+        self._ck(lib().csrst_get_particles(self.h, *map(ptr, a)))
+        return a
+
+    def old_positions(self):
+        a = [np.zeros(self.n) for _ in range(2)]
+        self._ck(lib().csrst_get_old_positions(self.h, *map(ptr, a)))
+        return a
+
+    def window(self):
+        w = (C.c_int * 4)()
+        o = np.zeros(2)
+        gb = (C.c_int * 4)()
+        self._ck(lib().csrst_get_window(self.h, w, ptr(o), gb))
+        return list(w), o, list(gb)
+
+    def window_field(self, which):
+        w, _, _ = self.window()
+        out = np.zeros((w[3] + 2) * (w[2] + 2))
+        self._ck(lib().csrst_get_window_field(self.h, which, ptr(out)))
+        return out.reshape(w[3] + 2, w[2] + 2)
+
+    # -- loop pieces ----------------------------------------------------------
+    def push(self, jcomp):
+        self._ck(lib().csrst_push(self.h, jcomp))
+
+    def drift(self, dt):
+        self._ck(lib().csrst_drift(self.h, dt))
+
+    def half_h(self):
+        self._ck(lib().csrst_half_h(self.h))
+
+    def update_e(self, comp):
+        self._ck(lib().csrst_update_e(self.h, comp))
+
+    def move(self):
+        self._ck(lib().csrst_move_window(self.h))
+
+    def step(self, n=1):
+        self._ck(lib().csrst_step(self.h, n))
+
+    def sync(self):
+        self._ck(lib().csrst_sync(self.h))
+
+    def stream(self):
+        return lib().csrst_stream(self.h)
+
+    def moments(self):
+        out = np.zeros(18)
+        self._ck(lib().csrst_diag_moments(self.h, ptr(out)))
+        return out
+
+    def wake(self):
+        w, _, _ = self.window()
+        out = np.zeros(max(w[2] - 4, 0))
+        self._ck(lib().csrst_diag_wake(self.h, ptr(out), len(out)))
+        return out
+
+
+class PartBunch:
+    """PartBunch (PartBunch.hh:35-206) over a Simulation's bunch."""
+
+    def __init__(self, sim: Simulation):
+        self.sim = sim
+
+    def push_particles(self, jcomp):
+        self.sim.push(jcomp)
+
+    def drift_particles(self, dt):
+        self.sim.drift(dt)
+
+    def getGlobalBounds(self):
+        return self.sim.window()[2]
+
+    def calcBeamParameters(self):
+        m = self.sim.moments()
+        keys = ("rmean", "pmean", "rrms", "prms", "eps_norm", "rmin", "rmax")
+        out = {k: m[2 * i:2 * i + 2] for i, k in enumerate(keys)}
+        out["Ekin"], out["dE"] = m[14], m[15]
+        return out
+
+
+class TETMSolver:
+    """TETMSolver (TETMSolver.hh:38-103): the two half steps of one time step."""
+
+    def __init__(self, sim: Simulation):
+        self.sim = sim
+
+    def getDT(self):
+        return self.sim.info()["dt"]
+
+    def updateField_firstStep(self):
+        check(lib().csrst_step_first(self.sim.h), self.sim.h)
+
+    def updateField_secondStep(self):
+        check(lib().csrst_step_second(self.sim.h), self.sim.h)
+
+
+def moveMesh(sim: Simulation):
+    sim.move()
+
+
+class ScatterGatherImpl:
+    """ScatterGatherImpl<IntOp, double> (ScatterGatherImpl.hh:27-644)."""
+
+    def __init__(self, order):
+        self.order = order
+
+    def gather(self, patch, origin, spacing, x, y, comp):
+        """comp 0/1: edge-centred component; comp 2: cell-centred field."""
+        patch = f64(patch)
+        x, y = f64(x), f64(y)
+        out = np.zeros(len(x))
+        o, hh = f64(origin), f64(spacing)
+        ny, nx = patch.shape
+        check(lib().csrst_gather(self.order, comp, ptr(patch), nx, ny, ptr(o), ptr(hh), ptr(x), ptr(y),
+                                 len(x), ptr(out)))
+        return out
+
+
+class ShapeFunction:
+    """ShapeFunction<IntOp> current and charge kernels (ShapeFunction.hh:141-508)."""
+
+    def __init__(self, order):
+        self.order = order
+
+    def getCurrentDensityBase(self, comp, ox, oy, x, y, q, origin, spacing, dt, i0, j0, ni, nj, scale):
+        J = np.zeros((nj, ni))
+        a = list(map(f64, (ox, oy, x, y, q)))
+        check(lib().csrst_deposit(self.order, comp, *map(ptr, a), len(a[0]), ptr(f64(origin)),
+                                  ptr(f64(spacing)), dt, i0, j0, ni, nj, scale, ptr(J)))
+        return J
+
+    def getChargeDensityDiff(self, ox, oy, x, y, q, origin, spacing, i0, j0, ni, nj, scale):
+        r = np.zeros((nj, ni))
+        a = list(map(f64, (ox, oy, x, y, q)))
+        check(lib().csrst_charge_diff(self.order, *map(ptr, a), len(a[0]), ptr(f64(origin)),
+                                      ptr(f64(spacing)), i0, j0, ni, nj, scale, ptr(r)))
+        return r

@@ -1,0 +1,129 @@
+"""Run configurations and seeded synthetic bunches.
+
+The reference reads its run set-up from the command line (src/main.cpp:111-136)
+and builds its bunch from GSL Halton sequences (src/Distribution.cpp:55-130).
+Here a configuration is derived from physical targets (grid, cell size, bend
+radius, pipe width, beam energy) and the bunch comes from a seeded numpy
+Philox generator; both sides of every parity check read the same arrays.
+"""
+import math
+from dataclasses import dataclass, asdict
+
+import numpy as np
+
+C_LIGHT = 299792458.0
+MASS_EV = 0.511e6                 # rest mass used by Bend (src/Bend.cpp:66)
+M_E_GEV = 0.51099906e-03          # Physics::m_e (src/Physics.cpp:54)
+CHARGE_MASS = -1e-9 / M_E_GEV     # PartBunch charge-to-mass ratio (src/main.cpp:223)
+
+
+@dataclass
+class RunConfig:
+    Nx: int
+    Ny: int
+    length_before: float
+    length_after: float
+    width: float
+    phi_deg: float
+    ekin_mev: float
+    bz: float
+    shape_order: int = 0
+    dt: float = 0.0               # <= 0: hx / c, the reference's fixed choice (main.cpp:187)
+    charge_mass: float = CHARGE_MASS
+    flags: int = 0
+
+    def dict(self):
+        return asdict(self)
+
+
+@dataclass
+class BunchSpec:
+    n: int
+    gamma: float
+    sigma_s: float                # rms length (x) [m]
+    sigma_x: float                # rms width (y) [m]
+    energy_spread: float          # relative rms of gamma
+    charge: float                 # total charge [C], negative for electrons
+    x0: float                     # centroid x [m]
+    y0: float                     # centroid y [m]
+    seed: int = 1
+
+
+def bend_config(Nx, Ny, h, R, width, gamma, shape_order=0, cfl=None, length_after=None):
+    """Chooses the bend angle and the drift before the bend so that the
+    reference's domain rule (Bend::Init, src/Bend.cpp:92-105) gives cells of
+    size h on an Nx x Ny mesh.  The drift after the bend defaults to 50
+    cells: the reference's wall crossing (Bend::crossBoundary) finds the end
+    wall only in the straight section after the bend, so a zero-length drift
+    there makes its cut-cell areas assert."""
+    if length_after is None:
+        length_after = 50 * h
+    ekin_mev = (gamma - 1.0) * MASS_EV * 1e-6
+    ekin = ekin_mev * 1e6
+    p_ev = math.sqrt(ekin * ekin + 2.0 * ekin * MASS_EV)
+    bz = p_ev / (C_LIGHT * R)
+    dom_w = (Ny - 2) * h
+    if dom_w <= width:
+        raise ValueError("the mesh must be taller than the pipe")
+
+    def width_of(phi):
+        return (R - 0.5 * width) * (1 - math.cos(phi)) + width + length_after * math.sin(phi)
+
+    lo, hi = 0.0, 0.5 * math.pi
+    for _ in range(200):
+        mid = 0.5 * (lo + hi)
+        lo, hi = (mid, hi) if width_of(mid) < dom_w else (lo, mid)
+    phi = 0.5 * (lo + hi)
+    lb = (Nx - 2) * h - length_after * math.cos(phi) - (R + 0.5 * width) * math.sin(phi)
+    if lb <= 0:
+        raise ValueError("mesh too short for this bend")
+    dt = 0.0 if cfl is None else cfl * h / C_LIGHT
+    return RunConfig(Nx=Nx, Ny=Ny, length_before=lb, length_after=length_after, width=width,
+                     phi_deg=math.degrees(phi), ekin_mev=ekin_mev, bz=bz,
+                     shape_order=shape_order, dt=dt)
+
+
+def make_bunch(spec: BunchSpec):
+    """Gaussian bunch: x ~ N(x0, sigma_s), y ~ N(y0, sigma_x),
+    gamma_i = gamma (1 + N(0, spread)), P = (beta gamma, 0)."""
+    g = np.random.Generator(np.random.Philox(spec.seed))
+    x = spec.x0 + spec.sigma_s * g.standard_normal(spec.n)
+    y = spec.y0 + spec.sigma_x * g.standard_normal(spec.n)
+    gam = spec.gamma * (1.0 + spec.energy_spread * g.standard_normal(spec.n))
+    px = np.sqrt(gam * gam - 1.0)
+    py = np.zeros(spec.n)
+    q = np.full(spec.n, spec.charge / spec.n)
+    return x, y, px, py, q
+
+
+# Named workloads.  C1/C2 follow the reference's headline configurations;
+# the "small" ones are the same physics on meshes the CPU oracle runs in
+# seconds.
+def workload(name):
+    if name == "c1":      # 2048 x 512, h = 10 um, R = 1 m, 5 mm pipe, CIC, CFL 0.5, 2e5 particles
+        h = 10e-6
+        cfg = bend_config(2048, 512, h, 1.0, 5e-3, 1000.0, shape_order=0, cfl=0.5)
+        spec = BunchSpec(n=200_000, gamma=1000.0, sigma_s=50e-6, sigma_x=20e-6,
+                         energy_spread=1e-4, charge=-1e-9, x0=50 * h + 6 * 50e-6,
+                         y0=0.5 * 5e-3, seed=11)
+    elif name == "c2":    # 8192 x 1024, h = 5 um, TSC, 4e6 particles
+        h = 5e-6
+        cfg = bend_config(8192, 1024, h, 1.0, 5e-3, 1000.0, shape_order=1, cfl=0.5)
+        spec = BunchSpec(n=4_000_000, gamma=1000.0, sigma_s=50e-6, sigma_x=20e-6,
+                         energy_spread=1e-4, charge=-1e-9, x0=50 * h + 6 * 50e-6,
+                         y0=0.5 * 5e-3, seed=12)
+    elif name.startswith("small"):
+        # small-<order>[-bend]: 512 x 104 mesh at 20 um, 2 mm pipe, R = 0.25 m,
+        # 4000 particles; "-bend" starts the bunch at the dipole entrance.
+        parts = name.split("-")
+        order = int(parts[1]) if len(parts) > 1 else 0
+        h = 20e-6
+        cfg = bend_config(512, 104, h, 0.25, 2e-3, 1000.0, shape_order=order, cfl=0.5)
+        x0 = 40 * h + 6 * 60e-6
+        if "bend" in parts:
+            x0 = cfg.length_before + 6 * 60e-6
+        spec = BunchSpec(n=4000, gamma=1000.0, sigma_s=60e-6, sigma_x=40e-6,
+                         energy_spread=1e-4, charge=-1e-9, x0=x0, y0=0.5 * 2e-3, seed=3)
+    else:
+        raise KeyError(name)
+    return cfg, spec

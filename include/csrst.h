@@ -1,0 +1,147 @@
+/* C ABI of the B200 CSRST per-time-step PIC loop (libcsrst_gpu.so).
+ *
+ * The reference (kreischtauf/CSRST) has no FFI: its boundary is the C++
+ * classes TETMSolver, PartBunch and ScatterGatherImpl over IPPL fields.
+ * Each entry point below names the reference interface it replaces.  The
+ * C++ facades in include/csrst/ keep those class shapes on top of this ABI.
+ *
+ * Conventions
+ *  - Every call returns an int status: 0 on success, a negative CSRST_E_*
+ *    code on failure; csrst_get_error() returns the message of the last one.
+ *  - Host buffers are copied; device memory is owned by the handle.
+ *  - One handle per thread.  A handle is bound to one device and one CUDA
+ *    stream; calls are asynchronous on that stream except the ones that
+ *    return host data, which synchronise it.
+ *  - Arrays of the static mesh are Nx*Ny doubles, x fastest, no guard cells.
+ *    Window arrays are (L0+2)*(L1+2) doubles including the one-cell guard ring.
+ */
+#ifndef CSRST_H
+#define CSRST_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CSRST_OK 0
+#define CSRST_E_ARG (-1)           /* invalid argument */
+#define CSRST_E_CUDA (-2)          /* CUDA runtime error or no device */
+#define CSRST_E_GEOMETRY (-3)      /* bend geometry where the reference asserts */
+#define CSRST_E_NO_PARTICLES (-4)  /* the call needs a loaded bunch */
+#define CSRST_E_WINDOW_FIT (-5)    /* bunch no longer fits the window (moveMesh PAssert) */
+#define CSRST_E_WINDOW_MOVE (-6)   /* window would move by other than 0/1 cell in x, -1..1 in y */
+#define CSRST_E_CROSSINGS (-7)     /* a particle crossed more cell borders than one push allows */
+#define CSRST_E_WINDOW_WALL (-8)   /* window or its ring touches a non-inside cell */
+
+typedef struct csrst_handle csrst_handle;
+
+/* Run set-up.  Mirrors the command line of src/main.cpp:111-136 for the
+ * parts the time step uses.  shape_order: 0 = IntCIC (ZerothOrderShapeFunction),
+ * 1 = IntS1 / TSC (FirstOrderShapeFunction), 2 = IntS2 (SecondOrderShapeFunction). */
+typedef struct {
+  int Nx, Ny;                 /* static mesh vertices per direction (-x, -y) */
+  int shape_order;
+  int flags;                  /* reserved, 0 */
+  double length_before;       /* drift before the bend [m] (--lengthbefore) */
+  double length_after;        /* drift after the bend [m] (-l) */
+  double width;               /* pipe width [m] (-w) */
+  double phi_deg;             /* bending angle [deg] (-P) */
+  double ekin_mev;            /* kinetic energy [MeV] (-E) */
+  double bz;                  /* dipole field [T] (-B) */
+  double dt;                  /* time step [s]; <= 0 selects hx / c (main.cpp:187) */
+  double charge_mass;         /* charge-to-mass ratio of PartBunch (main.cpp:223: -1e-9 / m_e[GeV]) */
+} csrst_config;
+
+/* Creates the handle on the current CUDA device: bend geometry, inside mask
+ * and cut-cell list (Bend::Init + SCBoundaryCondition ctor, main.cpp:168-197),
+ * zero static fields. */
+int csrst_create(const csrst_config *cfg, csrst_handle **out);
+int csrst_destroy(csrst_handle *h);
+/* Message of the last failed call on this handle (or of csrst_create when h is NULL). */
+int csrst_get_error(const csrst_handle *h, char *buf, size_t len);
+/* CUDA stream of the handle (a cudaStream_t). */
+void *csrst_stream(csrst_handle *h);
+int csrst_sync(csrst_handle *h);
+
+/* Geometry: info8 = hx, hy, origin x, origin y, dt, fixed-point scale of the
+ * current deposit, number of cut cells, window pitch.  Replaces Bend::Init /
+ * getInsideMask / SCBoundaryCondition::getBoundaryCells (Bend.cpp:85-124,
+ * SCBoundaryCondition.hh:433-441). */
+int csrst_get_info(csrst_handle *h, double *info8);
+/* inside: Nx*Ny bytes; cells: 7 doubles per cut cell (i, j, lambda0, lambda1,
+ * area, lambdaToNeighbours0, lambdaToNeighbours1), at most max_cells. */
+int csrst_get_geometry(csrst_handle *h, uint8_t *inside, double *cells, long max_cells, long *ncells);
+
+/* Static mesh fields (EFD components 0/1, HFD components 0/1). */
+int csrst_set_static_fields(csrst_handle *h, const double *ex, const double *ey,
+                            const double *hzx, const double *hzy);
+int csrst_get_static_fields(csrst_handle *h, double *ex, double *ey, double *hzx, double *hzy);
+/* SCBoundaryCondition::resetOutsideDomain (SCBoundaryCondition.hh:163-195). */
+int csrst_reset_outside(csrst_handle *h);
+
+/* Loads the bunch (PartBunch ctor + sortParticles, PartBunch.cpp:48-150,
+ * :1817-1844), opens the moving window around it (main.cpp:198-217) and
+ * fills it from the static mesh (copyFields + exchangeBoundaries,
+ * main.cpp:335-342).  q: charge per macro-particle [C]. */
+int csrst_load_particles(csrst_handle *h, const double *x, const double *y, const double *px,
+                         const double *py, const double *q, size_t n);
+/* Current bunch in the handle's (cell-sorted) order. */
+int csrst_get_particles(csrst_handle *h, double *x, double *y, double *px, double *py);
+/* oldR of the last push (PartBunch::oldR). */
+int csrst_get_old_positions(csrst_handle *h, double *ox, double *oy);
+/* Window: w4 = position (ddim.first) x, y, size L0, L1; origin2; gb4 = last
+ * deposit's particle bounds in window cells (PartBunch::getGlobalBounds). */
+int csrst_get_window(csrst_handle *h, int *w4, double *origin2, int *gb4);
+/* which: 0 Ex, 1 Ey, 2 Hzx, 3 Hzy, 4 Jx, 5 Jy of the window, incl. guards. */
+int csrst_get_window_field(csrst_handle *h, int which, double *out);
+
+/* PartBunch::push_particles(mmE, mmH, mmJ, dt, Jcomp) (PartBunch.cpp:215-519). */
+int csrst_push(csrst_handle *h, int jcomp);
+/* PartBunch::drift_particles(dt) (PartBunch.cpp:179-187). */
+int csrst_drift(csrst_handle *h, double dt);
+/* Field sub-steps of TETMSolver::updateField_firstStep/secondStep, each with
+ * its strip exchange and cut-cell correction (TETMSolver.hh:142-206, :241-261). */
+int csrst_half_h(csrst_handle *h);
+int csrst_update_e(csrst_handle *h, int comp);
+/* moveMesh (main.cpp:562-652). */
+int csrst_move_window(csrst_handle *h);
+/* TETMSolver::updateField_firstStep / updateField_secondStep (TETMSolver.hh:110-266). */
+int csrst_step_first(csrst_handle *h);
+int csrst_step_second(csrst_handle *h);
+/* nsteps iterations of the main loop body (main.cpp:390-506): first step,
+ * second step, window move.  Captured once as a CUDA graph and replayed. */
+int csrst_step(csrst_handle *h, int nsteps);
+
+/* Beam moments (PartBunch::calcBeamParameters, PartBunch.cpp:584-657):
+ * out18 = rmean2, pmean2, rrms2, prms2, eps_norm2, rmin2, rmax2, Ekin[MeV], dE, 0, 0. */
+int csrst_diag_moments(csrst_handle *h, double *out18);
+/* Longitudinal field along the bunch axis at window columns 2 .. L0-3
+ * (IntegrateElongCommand::execute, IntegrateElong.cpp:38-89); NaN where the
+ * sample lies outside the window.  n must be L0 - 4. */
+int csrst_diag_wake(csrst_handle *h, double *out, int n);
+
+/* ScatterGatherImpl<IntOp>::gather (ScatterGatherImpl.hh:27-47) on a dense
+ * host patch (nx * ny, x fastest) with origin o and spacing hh; comp 0/1 =
+ * edge component, 2 = cell-centred.  Runs on the current device. */
+int csrst_gather(int order, int comp, const double *patch, int nx, int ny, const double *o2,
+                 const double *hh2, const double *x, const double *y, size_t n, double *out);
+/* ShapeFunction<IntOp>::getCurrentDensityBase{X,Y} (ShapeFunction.hh:173-204):
+ * current of particles moving old -> new on a mesh with origin o2, spacing
+ * hh2, into a dense (ni x nj) patch whose element (0,0) is mesh index
+ * (i0, j0).  Accumulated in 64-bit fixed point with the given scale. */
+int csrst_deposit(int order, int comp, const double *ox, const double *oy, const double *x,
+                  const double *y, const double *q, size_t n, const double *o2, const double *hh2,
+                  double dt, int i0, int j0, int ni, int nj, double scale, double *J);
+/* Charge difference rho(new) - rho(old) at vertices for the charge shape of
+ * the same order (get*ChargeDensityDiffImpl), divided by the cell area. */
+int csrst_charge_diff(int order, const double *ox, const double *oy, const double *x,
+                      const double *y, const double *q, size_t n, const double *o2,
+                      const double *hh2, int i0, int j0, int ni, int nj, double scale, double *rho);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CSRST_H */

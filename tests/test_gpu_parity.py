@@ -1,0 +1,273 @@
+"""GPU parity: the CUDA path through the C ABI against the CPU oracle.
+
+Bar: bit-exact (array_equal) for geometry, gathers, particle positions and
+momenta, cell indices, window position and all fields when the oracle
+accumulates the current in the same 64-bit fixed point as the GPU; within a
+stated relative tolerance against the oracle's plain FP64 current sums
+(the reference's order of summation).
+"""
+import numpy as np
+import pytest
+
+from csrst_b200 import CsrstError, ScatterGatherImpl, ShapeFunction, Simulation, TETMSolver
+from csrst_b200.workloads import make_bunch, workload
+
+pytestmark = pytest.mark.gpu
+
+C_LIGHT = 299792458.0
+
+
+def smooth_fields(cfg, seed, amp=2e5):
+    """Smooth random fields on the static mesh (V/m, A/m)."""
+    rng = np.random.default_rng(seed)
+    j, i = np.mgrid[0:cfg.Ny, 0:cfg.Nx]
+    out = []
+    for k in range(4):
+        f = np.zeros((cfg.Ny, cfg.Nx))
+        for _ in range(3):
+            kx, ky = rng.uniform(0.01, 0.2, 2)
+            ph = rng.uniform(0, 6.3, 2)
+            f += rng.uniform(-1, 1) * np.sin(kx * i + ph[0]) * np.cos(ky * j + ph[1])
+        out.append(f * (amp if k < 2 else amp / 376.73))
+    return out
+
+
+def pair(name, oracle, fixed=True, fields=True, keep_old=False, seed=0):
+    cfg, spec = workload(name)
+    g = Simulation(cfg, keep_old=keep_old)
+    bunch = make_bunch(spec)
+    d = cfg.dict()
+    d["order"] = cfg.shape_order
+    if fields:
+        f = smooth_fields(cfg, seed)
+        g.set_static(*f)
+    g.load(*bunch)
+    if fixed:
+        d["fixed_scale"] = g.info()["fixed_scale"]
+    o = oracle.Sim(d)
+    if fields:
+        o.set_static(*f)
+    o.load(*bunch)
+    return cfg, g, o
+
+
+def assert_same_state(g, o, fields=True):
+    for a, b in zip(g.particles(), o.particles()):
+        assert np.array_equal(a, b)
+    wg, og, bg = g.window()
+    wo, oo, bo = o.window()
+    assert wg == wo and np.array_equal(og, oo)
+    if fields:
+        for a, b in zip(g.get_static(), o.get_static()):
+            assert np.array_equal(a, b)
+        for k in range(4):
+            assert np.array_equal(g.window_field(k), o.window_field(k)), k
+
+
+def test_geometry_bit_exact(gpu_lib, oracle):
+    for name in ("small-0", "c1"):
+        cfg, _ = workload(name)
+        g = Simulation(cfg)
+        gi, gc = g.geometry()
+        oi, oc = oracle.geometry(cfg.Nx, cfg.Ny, cfg.length_before, cfg.length_after, cfg.width,
+                                 cfg.phi_deg, cfg.ekin_mev, cfg.bz)
+        assert np.array_equal(gi, oi)
+        assert np.array_equal(gc, oc)
+        g.close()
+
+
+@pytest.mark.parametrize("order", [0, 1, 2])
+def test_gather_golden_and_random(gpu_lib, oracle, order):
+    sg = ScatterGatherImpl(order)
+    x, y = np.array([3.3]), np.array([3.2])
+    for comp in (0, 1, 2):
+        w = oracle.scatter(order, comp, (21, 21), (0, 0), (1, 1), x, y, [1.0])
+        v = sg.gather((w != 0).astype(float), (0, 0), (1, 1), x, y, comp)[0]
+        assert abs(v - 1.0) < 1e-12   # test/scattergather.cpp:133-166, :218-269, :344-416
+    rng = np.random.default_rng(order)
+    patch = rng.standard_normal((40, 50))
+    xs = rng.uniform(4, 44, 2000) * 1e-5 + 1e-3
+    ys = rng.uniform(4, 34, 2000) * 2e-5 - 2e-3
+    for comp in (0, 1, 2):
+        a = sg.gather(patch, (1e-3, -2e-3), (1e-5, 2e-5), xs, ys, comp)
+        b = oracle.gather(order, comp, patch, (1e-3, -2e-3), (1e-5, 2e-5), xs, ys)
+        assert np.array_equal(a, b)
+
+
+def random_moves(n, h, seed, cfl=0.5):
+    rng = np.random.default_rng(seed)
+    ox = rng.uniform(6, 14, n) * h[0]
+    oy = rng.uniform(6, 14, n) * h[1]
+    ang = rng.uniform(0, 2 * np.pi, n)
+    r = rng.uniform(0, cfl, n) * min(h)
+    return ox, oy, ox + r * np.cos(ang), oy + r * np.sin(ang), rng.uniform(-2e-15, 2e-15, n)
+
+
+@pytest.mark.parametrize("order", [0, 1, 2])
+def test_deposit_parity_and_continuity(gpu_lib, oracle, order):
+    h = (1e-5, 1.2e-5)
+    dt = 0.5 * h[0] / C_LIGHT
+    ox, oy, x, y, q = random_moves(20000, h, order)
+    bound = 4.0 * len(q) * np.abs(q).max() * C_LIGHT / (h[0] * h[1])
+    scale = 2.0 ** np.floor(np.log2(2.0 ** 62 / bound))
+    sf = ShapeFunction(order)
+    J = {}
+    for comp in (0, 1):
+        a = sf.getCurrentDensityBase(comp, ox, oy, x, y, q, (0, 0), h, dt, 0, 0, 24, 24, scale)
+        b = oracle.deposit(order, comp, ox, oy, x, y, q, (0, 0), h, dt, 0, 0, 24, 24, fixed_scale=scale)
+        c = oracle.deposit(order, comp, ox, oy, x, y, q, (0, 0), h, dt, 0, 0, 24, 24)
+        assert np.array_equal(a, b)                                   # same fixed point: bit-exact
+        assert np.abs(a - c).max() <= 1e-12 * np.abs(c).max()         # reference FP64 order: 1e-12
+        J[comp] = a
+    rho = sf.getChargeDensityDiff(ox, oy, x, y, q, (0, 0), h, 0, 0, 24, 24, scale)
+    res = rho[1:, 1:] / dt + (J[0][1:, 1:] - J[0][1:, :-1]) / h[0] + (J[1][1:, 1:] - J[1][:-1, 1:]) / h[1]
+    assert np.abs(res).max() <= 1e-10 * np.abs(rho / dt).max()
+
+
+@pytest.mark.parametrize("name", ["small-0", "small-1", "small-2", "small-1-bend"])
+def test_push_bit_exact(gpu_lib, oracle, name):
+    cfg, g, o = pair(name, oracle, keep_old=True)
+    g.push(0)
+    o.push(0)
+    assert_same_state(g, o, fields=False)
+    for a, b in zip(g.old_positions(), o.old_positions()):
+        assert np.array_equal(a, b)
+    assert g.window()[2] == o.window()[2]               # PartBunch::getGlobalBounds
+    assert np.array_equal(g.window_field(4), o.window_field(4))   # J_x of the window
+
+
+@pytest.mark.parametrize("name", ["small-0", "small-1"])
+def test_field_substeps_bit_exact(gpu_lib, oracle, name):
+    cfg, g, o = pair(name, oracle)
+    for s in (g, o):
+        s.push(0)
+        s.half_h()
+    assert_same_state(g, o)
+    for s in (g, o):
+        s.update_e(0)
+        s.half_h()
+    assert_same_state(g, o)
+    for s in (g, o):
+        s.drift(-0.5 * s.dt if s is o else -0.5 * g.info()["dt"])
+        s.push(1)
+        s.update_e(1)
+    assert_same_state(g, o)
+
+
+@pytest.mark.parametrize("name", ["small-0", "small-1", "small-2", "small-1-bend"])
+def test_steps_bit_exact_fixed_point(gpu_lib, oracle, name):
+    cfg, g, o = pair(name, oracle)
+    g.step(12)       # graph-captured steps
+    o.step(12)
+    assert_same_state(g, o)
+    assert np.array_equal(g.window_field(4), o.window_field(4))
+    assert np.array_equal(g.window_field(5), o.window_field(5))
+
+
+def test_tetm_solver_api_matches_graph_path(gpu_lib):
+    cfg, spec = workload("small-1")
+    b = make_bunch(spec)
+    a, c = Simulation(cfg), Simulation(cfg)
+    for s in (a, c):
+        s.load(*b)
+    solver = TETMSolver(a)
+    for _ in range(5):
+        solver.updateField_firstStep()
+        solver.updateField_secondStep()
+        a.move()
+    c.step(5)
+    for u, v in zip(a.particles(), c.particles()):
+        assert np.array_equal(u, v)
+    for u, v in zip(a.get_static(), c.get_static()):
+        assert np.array_equal(u, v)
+
+
+@pytest.mark.parametrize("name", ["small-0", "small-1-bend"])
+def test_steps_vs_reference_summation(gpu_lib, oracle, name):
+    """Against the oracle's FP64 current sums (the reference's order)."""
+    cfg, g, o = pair(name, oracle, fixed=False)
+    g.step(12)
+    o.step(12)
+    h = g.info()["hx"]
+    gx, gy, gpx, gpy = g.particles()
+    ox, oy, opx, opy = o.particles()
+    assert np.abs(gx - ox).max() <= 1e-9 * h and np.abs(gy - oy).max() <= 1e-9 * h
+    assert np.abs(gpx - opx).max() <= 1e-12 * np.abs(opx).max()
+    assert np.abs(gpy - opy).max() <= 1e-12 * np.abs(opx).max()
+    # cell indices of the window (bit-exact)
+    w, org, _ = g.window()
+    assert np.array_equal(np.floor((gx - org[0]) / h), np.floor((ox - org[0]) / h))
+    for a, b in zip(g.get_static(), o.get_static()):
+        assert np.abs(a - b).max() <= 1e-9 * max(np.abs(b).max(), 1e-300)
+
+
+def test_moments_and_wake(gpu_lib, oracle):
+    cfg, g, o = pair("small-1", oracle)
+    g.step(6)
+    o.step(6)
+    mg, mo = g.moments(), o.moments()
+    for k in range(16):
+        assert abs(mg[k] - mo[k]) <= 1e-10 * max(abs(mo[k]), 1e-30), k
+    wg = g.wake()
+    wo = o.wake(mo[:2], mo[2:4])
+    assert np.array_equal(np.isnan(wg), np.isnan(wo))
+    ok = ~np.isnan(wo)
+    assert np.abs(wg[ok] - wo[ok]).max() <= 1e-9 * np.abs(wo[ok]).max()
+
+
+def test_c1_full_size_bit_exact(gpu_lib, oracle):
+    """The 2048 x 512 / 2e5-particle workload, 4 steps, against the oracle."""
+    cfg, g, o = pair("c1", oracle, fields=False)
+    g.step(4)
+    o.step(4)
+    assert_same_state(g, o)
+
+
+def test_continuity_full_size(gpu_lib):
+    """Deposit + charge difference of 4e6 particles (the TSC workload's
+    bunch) moving for one step: residual <= 1e-10 relative."""
+    cfg, spec = workload("c2")
+    x, y, px, py, q = make_bunch(spec)
+    h = (5e-6, 5e-6)
+    dt = 0.5 * h[0] / C_LIGHT
+    gam = np.sqrt(1 + px * px + py * py)
+    nx, ny = x + C_LIGHT * dt * px / gam, y + 1e-3 * h[1] * np.sin(x / h[0])
+    org = (x.min() - 10 * h[0], y.min() - 10 * h[1])
+    ni = int((x.max() - org[0]) / h[0]) + 20
+    nj = int((y.max() - org[1]) / h[1]) + 20
+    bound = 4.0 * len(q) * np.abs(q).max() * C_LIGHT / (h[0] * h[1])
+    scale = 2.0 ** np.floor(np.log2(2.0 ** 62 / bound))
+    sf = ShapeFunction(1)
+    jx = sf.getCurrentDensityBase(0, x, y, nx, ny, q, org, h, dt, 0, 0, ni, nj, scale)
+    jy = sf.getCurrentDensityBase(1, x, y, nx, ny, q, org, h, dt, 0, 0, ni, nj, scale)
+    rho = sf.getChargeDensityDiff(x, y, nx, ny, q, org, h, 0, 0, ni, nj, scale)
+    res = rho[1:, 1:] / dt + (jx[1:, 1:] - jx[1:, :-1]) / h[0] + (jy[1:, 1:] - jy[:-1, 1:]) / h[1]
+    assert np.abs(res).max() <= 1e-10 * np.abs(rho / dt).max()
+
+
+def test_deterministic_rerun(gpu_lib):
+    cfg, spec = workload("small-2")
+    b = make_bunch(spec)
+    runs = []
+    for _ in range(2):
+        s = Simulation(cfg)
+        s.load(*b)
+        s.step(8)
+        runs.append(s.particles() + s.get_static())
+        s.close()
+    for a, c in zip(*runs):
+        assert np.array_equal(a, c)
+
+
+def test_error_paths(gpu_lib):
+    cfg, spec = workload("small-0")
+    s = Simulation(cfg)
+    with pytest.raises(CsrstError) as e:
+        s.push(0)
+    assert e.value.code == -4
+    x, y, px, py, q = make_bunch(spec)
+    x = x.copy()
+    x[17] = np.nan
+    with pytest.raises(CsrstError) as e:
+        s.load(x, y, px, py, q)
+    assert e.value.code == -1
