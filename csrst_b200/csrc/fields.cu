@@ -203,6 +203,7 @@ struct MoveArgs {
 __global__ void __launch_bounds__(1024) k_move(MoveArgs m) {
   FieldArgs &a = m.f;
   WinState *ws = a.ws;
+  if (ws->err) return;
   const int L[2] = {a.L0, a.L1};
   __shared__ int s_move[3];
   if (threadIdx.x == 0) {

@@ -99,6 +99,11 @@ __global__ void k_push_prep(WinState *ws, double h0, double h1, int em0, int em2
     lp[2] = lp[3] = (int)floor((0.0 - ws->mo1) / h1);
   }
   for (int k = 0; k < 4; ++k) ws->lp[k] = lp[k];
+  // Every gather tap lies within [lp - 2, lp + 2] (the cubic edge stencil
+  // reaches furthest); the window planes hold one guard cell.  A bunch that
+  // no longer fits stops the run instead of reading outside the window.
+  if (mn0 <= mx0 && (lp[0] - 2 < -1 || lp[1] + 2 > ws->L0 || lp[2] - 2 < -1 || lp[3] + 2 > ws->L1))
+    set_err(ws, kErrWindowFit);
   const double po0 = ws->mo0 + lp[0] * h0, po1 = ws->mo1 + lp[2] * h1;
   ws->hz_o0 = po0 + cm0 * h0; ws->hz_o1 = po1 + cm0 * h1;
   ws->ex_o0 = po0 + em0 * h0; ws->ex_o1 = po1 + em2 * h1;
@@ -120,6 +125,7 @@ __global__ void __launch_bounds__(256) k_push(PushArgs a) {
   extern __shared__ unsigned long long sacc[];
   __shared__ int tb[4];  // touched box of this CTA (window cells)
   WinState *ws = a.ws;
+  if (ws->err) return;  // uniform: every thread reads the same flag
   const int L0 = ws->L0, L1 = ws->L1;
   const int ncell = L0 * L1;
   if (SMEM) {
@@ -165,6 +171,10 @@ __global__ void __launch_bounds__(256) k_push(PushArgs a) {
     double x = a.x[i], y = a.y[i];
     double p0 = a.px[i], p1 = a.py[i];
     const double q = a.q[i];
+    if (!(isfinite(x) && isfinite(y) && isfinite(p0) && isfinite(p1))) {
+      set_err(ws, kErrWindowFit);
+      continue;
+    }
     double r = inv_gamma(p0, p1);
     double w0 = a.half * p0 * r, w1 = a.half * p1 * r;
     if (a.pending) { x = x + (-w0); y = y + (-w1); }          // drift_particles(-dt/2)
