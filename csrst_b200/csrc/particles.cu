@@ -125,7 +125,10 @@ __global__ void __launch_bounds__(256) k_push(PushArgs a) {
   extern __shared__ unsigned long long sacc[];
   __shared__ int tb[4];  // touched box of this CTA (window cells)
   WinState *ws = a.ws;
-  if (ws->err) return;  // uniform: every thread reads the same flag
+  __shared__ int s_err;
+  if (threadIdx.x == 0) s_err = *(volatile int *)&ws->err;
+  __syncthreads();
+  if (s_err) return;  // the whole CTA leaves together
   const int L0 = ws->L0, L1 = ws->L1;
   const int ncell = L0 * L1;
   if (SMEM) {
