@@ -1,0 +1,338 @@
+#!/usr/bin/env python
+"""Throughput of the CSRST per-time-step PIC loop on B200.
+
+A step is one full time step of the reference's main loop (main.cpp:390-506):
+TETMSolver::updateField_firstStep, updateField_secondStep and moveMesh, i.e.
+two relativistic pushes with gather and charge-conserving deposit, four
+TE/TM field sub-steps on the static mesh, the cut cells and the moving
+window, their strip exchanges and the window move.
+
+Default workload: 8192 x 1024 static mesh at 5 um, 4e6 macro-particles,
+TSC (IntS1 gather + first-order deposit), CFL 0.5, FP64 (the plain FP64 GPU
+path).  Synthetic seeded bunch (Gaussian, sigma_s 50 um, sigma_x 20 um,
+energy spread 1e-4, 1 nC); zero initial fields.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+Under torchrun each rank runs an independent replica (the loop does not
+shard; the ensemble members are independent units): value = all ranks'
+particle-steps / max-over-ranks time.
+"""
+import argparse
+import json
+import math
+import os
+import re
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+if str(ROOT) not in sys.path:
+    sys.path.insert(0, str(ROOT))
+
+METRIC = "particle-steps/s, Yee cell-updates/s; FP32 vs FP64 GPU at ≤1e-3 CSR-wake err"
+UNIT = "particle-steps/s"
+# algorithmic bytes per unit (FP64): the fused Yee update reads and writes
+# Ex, Ey, Hzx, Hzy and reads a 1-byte mask per cell-step; a push streams
+# position and momentum in and out per particle.
+YEE_BYTES = 65
+PUSH_BYTES = 64
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    p.add_argument("--workload", default="c2")
+    p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    p.add_argument("--no-e2e", action="store_true")
+    return p.parse_args()
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def peaks():
+    f = ROOT / "MEASURED_PEAKS.json"
+    if f.exists():
+        d = json.loads(f.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profile_traffic(key):
+    """Per-step DRAM bytes of a kernel group from the committed ncu summary
+    (profiles/*.md lines 'traffic[<key>] = <bytes>'), or None."""
+    for f in sorted((ROOT / "profiles").glob("*.md")):
+        m = re.search(r"traffic\[" + re.escape(key) + r"\]\s*=\s*([0-9.eE+]+)", f.read_text())
+        if m:
+            return float(m.group(1))
+    return None
+
+
+class Clocks:
+    """nvidia-smi sampler over the timed region."""
+
+    def __init__(self, index):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={index}", f"--query-gpu={q}",
+                                       "--format=csv,noheader,nounits", "-lms", "100"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        self.p.wait()
+        rows = [r.split(",") for r in Path(self.f.name).read_text().splitlines() if r.strip()]
+        os.unlink(self.f.name)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4)
+                          if len(r) > 5 + k and r[5 + k].strip() == "Active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons, "samples": len(rows)}
+
+
+def run_b200(args, world, rank, local):
+    import torch
+    from csrst_b200 import Simulation
+    from csrst_b200.workloads import make_bunch, workload
+
+    torch.cuda.set_device(local)
+    cfg, spec = workload(args.workload)
+    spec.seed += rank
+    bunch = make_bunch(spec)
+    n = spec.n
+    sim = Simulation(cfg)
+    sim.load(*bunch)
+    stream = torch.cuda.ExternalStream(sim.stream())
+    sim.step(args.warmup)
+    sim.sync()
+
+    # ---- timed region: graph-captured steps, inputs resident in HBM ----
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    clocks = Clocks(local) if rank == 0 else None
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    sim.step(args.steps)
+    t1.record(stream)
+    sim.sync()
+    torch.cuda.synchronize()
+    ms = t0.elapsed_time(t1)
+    clk = clocks.stop() if clocks else None
+    if world > 1:
+        t = torch.tensor([ms], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+        torch.distributed.barrier()
+    ms_step = ms / args.steps
+    value = world * n * args.steps / (ms * 1e-3)
+    cells = cfg.Nx * cfg.Ny
+
+    # ---- kernel attribution: the same steps launched group by group ----
+    groups = {"push": 0.0, "yee": 0.0, "move": 0.0}
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(8)]
+    dt = sim.info()["dt"]
+    ksteps = min(args.steps, 10)
+    sim.sync()
+    for _ in range(ksteps):
+        ev[0].record(stream); sim.push(0); ev[1].record(stream)
+        sim.half_h(); sim.update_e(0); sim.half_h(); ev[2].record(stream)
+        sim.drift(-0.5 * dt)
+        ev[3].record(stream); sim.push(1); ev[4].record(stream)
+        sim.update_e(1); ev[5].record(stream)
+        sim.drift(-0.5 * dt)
+        ev[6].record(stream); sim.move(); ev[7].record(stream)
+        sim.sync()
+        groups["push"] += ev[0].elapsed_time(ev[1]) + ev[3].elapsed_time(ev[4])
+        groups["yee"] += ev[1].elapsed_time(ev[2]) + ev[4].elapsed_time(ev[5])
+        groups["move"] += ev[6].elapsed_time(ev[7])
+    for k in groups:
+        groups[k] /= ksteps
+    hbm, src = peaks()
+
+    def roof(key, bytes_step, ms_):
+        ach = bytes_step / (ms_ * 1e-3) / 1e9
+        tr = profile_traffic(f"{key},{args.workload},fp64")
+        return {"kernel": key, "bound": "hbm", "achieved": round(ach, 1), "peak": hbm, "unit": "GB/s",
+                "frac": round(ach / hbm, 4), "traffic": tr, "peak_source": f"{src} hbm_gbs",
+                "algorithmic_bytes_per_step": bytes_step, "ms_per_step": round(ms_, 4)}
+
+    r_yee = roof("yee", YEE_BYTES * cells, groups["yee"])
+    r_push = roof("push", 2 * PUSH_BYTES * n, groups["push"])
+    dominant, other = (r_yee, r_push) if groups["yee"] >= groups["push"] else (r_push, r_yee)
+
+    out = {"metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_step, 4),
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+           "data": "synthetic (seeded Gaussian bunch, zero initial fields)",
+           "config": {"workload": f"{args.workload}: {cfg.Nx}x{cfg.Ny} static mesh, h={1e6 * sim.info()['hx']:.3g}um,"
+                                  f" {n} particles, shape order {cfg.shape_order}, CFL 0.5, FP64",
+                      "Nx": cfg.Nx, "Ny": cfg.Ny, "particles": n, "shape_order": cfg.shape_order,
+                      "window": sim.window()[0][2:], "precision": "fp64", "parallelism": f"replicas x{world}",
+                      "l2": "inputs larger than L2 (fields 4 x %.0f MB, particles %.0f MB)" % (
+                          cells * 8 / 1e6, n * 40 / 1e6)},
+           "cell_updates_per_s": round(world * cells * args.steps / (ms * 1e-3), 1),
+           "roofline": dominant, "roofline_other": other,
+           "kernel_ms_per_step": {k: round(v, 4) for k, v in groups.items()},
+           "clocks": clk}
+    # launches per step: 2 pushes x (prep, push, post, bounds) + 4 sub-steps x
+    # (sweep, exchange) + move
+    out["gpu_launches"] = args.steps * (2 * 4 + 4 * 2 + 1)
+    sim.close()
+
+    if not args.no_e2e:
+        out["e2e"] = run_e2e(args, cfg, spec, bunch, rank, world)
+    if rank == 0 and world == 1 and not args.no_cpu:
+        out["cpu_baseline"] = cpu_baseline(cfg, spec, bunch)
+    return out if rank == 0 else None
+
+
+def run_e2e(args, cfg, spec, bunch, rank, world):
+    """The same metric through the C ABI with host buffers: the bunch goes
+    up from pinned host memory, every step returns the beam moments to the
+    host, and the bunch comes back at the end."""
+    import torch
+    from csrst_b200 import Simulation
+    n = spec.n
+    pinned = [torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy() for a in bunch]
+    outp = [torch.empty(n, dtype=torch.float64).pin_memory().numpy() for _ in range(4)]
+    sim = Simulation(cfg)
+    stream = torch.cuda.ExternalStream(sim.stream())
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    t = time.perf_counter()
+    sim.load(*pinned)
+    for _ in range(args.warmup + args.steps):
+        sim.step(1)
+        sim.moments()
+    from csrst_b200._lib import lib, ptr
+    lib().csrst_get_particles(sim.h, *map(ptr, outp))
+    torch.cuda.synchronize()
+    el = time.perf_counter() - t
+    if world > 1:
+        tt = torch.tensor([el], device="cuda")
+        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
+        el = float(tt.item())
+    k = args.warmup + args.steps
+    sim.close()
+    return {"value": round(world * n * k / el, 1), "unit": UNIT,
+            "h2d_bytes_per_step": int(5 * 8 * n / k), "d2h_bytes_per_step": int(18 * 8 + 4 * 8 * n / k),
+            "steps": k, "includes": "bunch upload, window set-up and sort, steps, per-step moments, bunch download"}
+
+
+def oracle_sample(cfg, spec, bunch, frac, nsteps):
+    """Times the oracle on the full static mesh with a particle sample; the
+    full-workload step time is fields + (N / sample) x particles."""
+    from oracle import oracle as O
+    d = cfg.dict()
+    d["order"] = cfg.shape_order
+    s = O.Sim(d)
+    ns = max(1000, int(spec.n * frac))
+    idx = np.linspace(0, spec.n - 1, ns).astype(np.int64)
+    s.load(*[a[idx] for a in bunch])
+    tf = tp = tm = 0.0
+    for _ in range(nsteps):
+        a = time.perf_counter(); s.push(0); b = time.perf_counter()
+        s.half_h(); s.update_e(0); s.half_h(); c = time.perf_counter()
+        s.drift(-0.5 * s.dt); s.push(1); e = time.perf_counter()
+        s.update_e(1); f = time.perf_counter()
+        s.drift(-0.5 * s.dt); s.move(); g = time.perf_counter()
+        tp += (b - a) + (e - c)
+        tf += (c - b) + (f - e)
+        tm += g - f
+    tp, tf, tm = tp / nsteps, tf / nsteps, tm / nsteps
+    full = tf + tm + tp * spec.n / ns
+    return full, tf, tp, ns
+
+
+def cpu_baseline(cfg, spec, bunch):
+    full, tf, tp, ns = oracle_sample(cfg, spec, bunch, 1 / 16, 2)
+    return {"value": round(spec.n / full, 1), "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"oracle (C++ restatement, -O2 -ffp-contract=off), 1 thread: 2 steps on the full "
+                      f"{cfg.Nx}x{cfg.Ny} mesh with {ns} of {spec.n} particles; step time = fields "
+                      f"{tf:.3f}s + particles {tp:.3f}s x {spec.n / ns:.0f}"}
+
+
+def _ref_worker(args):
+    name, frac, nsteps, seed = args
+    from csrst_b200.workloads import make_bunch, workload
+    cfg, spec = workload(name)
+    spec.seed = seed
+    return oracle_sample(cfg, spec, make_bunch(spec), frac, nsteps)
+
+
+def run_reference(args, world, rank):
+    """The reference arm: the CPU restatement of the reference loop on the
+    box's host cores (independent replicas, one per core), same workload."""
+    if rank != 0:
+        return None
+    import multiprocessing as mp
+    from csrst_b200.workloads import workload
+    cfg, spec = workload(args.workload)
+    cores = max(1, min(os.cpu_count() or 1, 32))
+    # bounded: each replica runs (warmup + steps) sample steps of ~1/64 of the bunch
+    nsteps = max(1, min(args.steps + args.warmup, 4))
+    t = time.perf_counter()
+    with mp.get_context("spawn").Pool(cores) as pool:
+        res = pool.map(_ref_worker, [(args.workload, 1 / 64, nsteps, 100 + k) for k in range(cores)])
+    wall = time.perf_counter() - t
+    fulls = [r[0] for r in res]
+    value = sum(spec.n / f for f in fulls)
+    ms = 1e3 * float(np.mean(fulls))
+    return {"impl": "reference", "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": args.workload, "Nx": cfg.Nx, "Ny": cfg.Ny, "particles": spec.n,
+                       "shape_order": cfg.shape_order},
+            "cpu_baseline": {"value": round(value, 1), "unit": UNIT, "cores": cores, "kind": "port",
+                             "sample": f"{cores} replica processes of the oracle, each {nsteps} steps on the full "
+                                       f"mesh with 1/64 of the bunch, particle time scaled to the full bunch; "
+                                       f"wall {wall:.1f}s"},
+            "e2e": {"value": round(value, 1), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    args = parse()
+    world, rank, local = dist_setup()
+    if world > 1:
+        import torch
+        import datetime
+        torch.cuda.set_device(local)
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    try:
+        out = run_reference(args, world, rank) if args.impl == "reference" else run_b200(args, world, rank, local)
+    finally:
+        if world > 1:
+            import torch
+            torch.distributed.destroy_process_group()
+    if out is not None:
+        print(json.dumps(out), flush=True)
+
+
+if __name__ == "__main__":
+    main()

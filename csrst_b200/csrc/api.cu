@@ -488,7 +488,7 @@ int csrst_load_particles(csrst_handle *h, const double *x, const double *y, cons
   const size_t wp = (size_t)h->wpitch * (h->L1 + 2);
   CK(cudaMalloc(&h->win, 6 * wp * sizeof(double)));
   CK(cudaMemsetAsync(h->win, 0, 6 * wp * sizeof(double), h->s));
-  CK(cudaMalloc(&h->scratch, 4 * wp * sizeof(double)));
+  CK(cudaMalloc(&h->scratch, 6 * wp * sizeof(double)));
   CK(cudaMalloc(&h->acc, 2 * (size_t)h->L0 * h->L1 * sizeof(unsigned long long)));
   CK(cudaMemsetAsync(h->acc, 0, 2 * (size_t)h->L0 * h->L1 * sizeof(unsigned long long), h->s));
   // PartBunch::sortParticles: y slice of the window, then x (stable radix sorts)

@@ -70,30 +70,32 @@ __global__ void __launch_bounds__(256) k_mom1(const double *x, const double *y, 
 }
 
 // pass 2: second moments of (x', px', y', py') in the frame of the mean
-// momentum, centred on the mean position (PartBunch.cpp:724-745).
+// momentum, centred on the mean position (PartBunch.cpp:724-745).  The
+// reference forms sum(px'^2) - N |<p>|^2, which cancels to 1e-8 for a beam
+// with 1e-4 energy spread; here px' is centred on |<p>| first and the
+// identity sum(px'^2) - N m^2 = sum((px'-m)^2) + 2 m sum(px'-m) restores the
+// same quantity without the cancellation.  Sums: q0^2, q2^2, (q1-m)^2, q3^2,
+// q0 (q1-m), q0, q2 q3, (q1-m).
 __global__ void __launch_bounds__(256) k_mom2(const double *x, const double *y, const double *px,
                                               const double *py, long long n, double half,
                                               int pending, const double *mean, double *part) {
   const double aR0 = mean[0], aR1 = mean[1], aP0 = mean[2], aP1 = mean[3];
   const double am = sqrt(aP0 * aP0 + aP1 * aP1), cph = aP0 / am, sph = aP1 / am;
-  double v[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+  double v[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x) {
     double a = x[i], b = y[i];
     const double p0 = px[i], p1 = py[i];
     true_pos(a, b, p0, p1, half, pending);
-    double q[4];
-    q[1] = cph * p0 + sph * p1;
-    q[3] = -sph * p0 + cph * p1;
-    q[0] = a - aR0; q[2] = b - aR1;
-    const double t = cph * q[0] + sph * q[2];
-    q[2] = -sph * q[0] + cph * q[2];
-    q[0] = t;
-    int k = 0;
-    for (int r = 0; r < 4; ++r)
-      for (int c = 0; c <= r; ++c) v[k++] += q[r] * q[c];
+    const double q1 = cph * p0 + sph * p1 - am;
+    const double q3 = -sph * p0 + cph * p1;
+    const double d0 = a - aR0, d2 = b - aR1;
+    const double q0 = cph * d0 + sph * d2;
+    const double q2 = -sph * d0 + cph * d2;
+    v[0] += q0 * q0; v[1] += q2 * q2; v[2] += q1 * q1; v[3] += q3 * q3;
+    v[4] += q0 * q1; v[5] += q0; v[6] += q2 * q3; v[7] += q1;
   }
-  block_sum<10>(v, part + blockIdx.x * 10);
+  block_sum<8>(v, part + blockIdx.x * 10);
 }
 
 // Final reduction and the derived quantities; out[18] as the oracle's layout:
@@ -113,16 +115,14 @@ __global__ void k_mom_final1(const double *part, int nb, long long n, double *me
 
 __global__ void k_mom_final2(const double *part, int nb, long long n, const double *mean, double *out) {
   if (threadIdx.x != 0) return;
-  double M[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+  double M[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   for (int b = 0; b < nb; ++b)
-    for (int k = 0; k < 10; ++k) M[k] += part[b * 10 + k];
-  // packed lower triangle: (0,0)=0 (1,0)=1 (1,1)=2 (2,0)=3 (2,1)=4 (2,2)=5 (3,0)=6 (3,1)=7 (3,2)=8 (3,3)=9
+    for (int k = 0; k < 8; ++k) M[k] += part[b * 10 + k];
   const double N = (double)n;
-  const double pm0 = mean[2], pm1 = mean[3];
-  const double c1 = pm0 * pm0 + pm1 * pm1;
-  const double rsq[2] = {M[0], M[5]};
-  double psq[2] = {M[2] - N * c1, M[9] - N * 0.0};
-  const double rp[2] = {M[1], M[8]};
+  const double am = sqrt(mean[2] * mean[2] + mean[3] * mean[3]);
+  const double rsq[2] = {M[0], M[1]};
+  double psq[2] = {M[2] + 2.0 * am * M[7], M[3]};
+  const double rp[2] = {M[4] + am * M[5], M[6]};
   for (int i = 0; i < 2; ++i) {
     if (psq[i] < 0) psq[i] = 0;
     const double e2 = (rsq[i] * psq[i] - rp[i] * rp[i]) / (N * N);

@@ -196,7 +196,7 @@ __global__ void k_check_window(FieldArgs a) { check_window_clear(a, a.ws); }
 // the window position and origin, then refreshes the strips.
 struct MoveArgs {
   FieldArgs f;
-  double *scratch;      // 4 window planes
+  double *scratch;      // 6 window planes
   double h0, h1;
 };
 
@@ -230,9 +230,9 @@ __global__ void __launch_bounds__(1024) k_move(MoveArgs m) {
   const int moveI = s_move[1], m1 = s_move[2];
   if (moveI == 0 && m1 == 0) return;
   const int W0 = a.L0 + 2, W1 = a.L1 + 2, np = W0 * W1;
-  Plane *pl[4] = {&a.mEx, &a.mEy, &a.mHx, &a.mHy};
+  Plane *pl[6] = {&a.mEx, &a.mEy, &a.mHx, &a.mHy, &a.mJx, &a.mJy};
   // phase A: snapshot
-  for (int k = threadIdx.x; k < 4 * np; k += blockDim.x) {
+  for (int k = threadIdx.x; k < 6 * np; k += blockDim.x) {
     const int f = k / np, r = k % np;
     m.scratch[k] = pl[f]->p[r];
   }
@@ -242,7 +242,7 @@ __global__ void __launch_bounds__(1024) k_move(MoveArgs m) {
   int j0 = -(m1 > 0 ? m1 : 0), j1 = a.L1 - 1 - (m1 < 0 ? m1 : 0);
   if (m1 == 0) { j0 -= 1; j1 += 1; }
   const int ni = i1 - i0 + 1, cnt = ni * (j1 - j0 + 1);
-  for (int k = threadIdx.x; k < 4 * cnt; k += blockDim.x) {
+  for (int k = threadIdx.x; k < 6 * cnt; k += blockDim.x) {
     const int f = k / cnt, r = k % cnt;
     const int i = i0 + r % ni, j = j0 + r / ni;
     pl[f]->at(i, j) = m.scratch[(size_t)f * np + (size_t)(j + m1 + 1) * W0 + (i + moveI + 1)];

@@ -314,13 +314,22 @@ void launch_push_prep(WinState *ws, double h0, double h1, int order, cudaStream_
   k_push_prep<<<1, 32, 0, s>>>(ws, h0, h1, em0, em2, cm0);
 }
 
-int push_smem_limit() {
-  static int lim = -1;
+// Largest dynamic shared memory the window accumulator may use for this
+// kernel: the opt-in per-block limit minus the kernel's static shared memory.
+template <int ORDER>
+static long long push_smem_limit() {
+  static long long lim = -1;
   if (lim < 0) {
     int dev = 0, v = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-    lim = v - 1024;
+    cudaFuncAttributes fa{};
+    cudaFuncGetAttributes(&fa, k_push<ORDER, true>);
+    lim = (long long)v - (long long)fa.sharedSizeBytes;
+    if (cudaFuncSetAttribute(k_push<ORDER, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lim) !=
+        cudaSuccess)
+      lim = 0;  // use the global-atomic variant
+    cudaGetLastError();
   }
   return lim;
 }
@@ -328,13 +337,7 @@ int push_smem_limit() {
 template <int ORDER>
 static void push_order(const PushArgs &a, int L0, int L1, int grid, cudaStream_t s) {
   const size_t sm = (size_t)L0 * L1 * sizeof(unsigned long long);
-  if (a.use_smem && (long long)sm <= push_smem_limit()) {
-    static bool attr = false;
-    if (!attr) {
-      cudaFuncSetAttribute(k_push<ORDER, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           push_smem_limit());
-      attr = true;
-    }
+  if (a.use_smem && (long long)sm <= push_smem_limit<ORDER>()) {
     k_push<ORDER, true><<<grid, 256, sm, s>>>(a);
   } else {
     k_push<ORDER, false><<<grid, 256, 0, s>>>(a);

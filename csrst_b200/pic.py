@@ -221,13 +221,15 @@ class ShapeFunction:
     def getCurrentDensityBase(self, comp, ox, oy, x, y, q, origin, spacing, dt, i0, j0, ni, nj, scale):
         J = np.zeros((nj, ni))
         a = list(map(f64, (ox, oy, x, y, q)))
-        check(lib().csrst_deposit(self.order, comp, *map(ptr, a), len(a[0]), ptr(f64(origin)),
-                                  ptr(f64(spacing)), dt, i0, j0, ni, nj, scale, ptr(J)))
+        o, hh = f64(origin), f64(spacing)   # keep the arrays alive across the call
+        check(lib().csrst_deposit(self.order, comp, *map(ptr, a), len(a[0]), ptr(o), ptr(hh), dt, i0,
+                                  j0, ni, nj, scale, ptr(J)))
         return J
 
     def getChargeDensityDiff(self, ox, oy, x, y, q, origin, spacing, i0, j0, ni, nj, scale):
         r = np.zeros((nj, ni))
         a = list(map(f64, (ox, oy, x, y, q)))
-        check(lib().csrst_charge_diff(self.order, *map(ptr, a), len(a[0]), ptr(f64(origin)),
-                                      ptr(f64(spacing)), i0, j0, ni, nj, scale, ptr(r)))
+        o, hh = f64(origin), f64(spacing)
+        check(lib().csrst_charge_diff(self.order, *map(ptr, a), len(a[0]), ptr(o), ptr(hh), i0, j0, ni,
+                                      nj, scale, ptr(r)))
         return r
