@@ -135,7 +135,9 @@ int csrst_deposit(int order, int comp, const double *ox, const double *oy, const
                   const double *y, const double *q, size_t n, const double *o2, const double *hh2,
                   double dt, int i0, int j0, int ni, int nj, double scale, double *J);
 /* Charge difference rho(new) - rho(old) at vertices for the charge shape of
- * the same order (get*ChargeDensityDiffImpl), divided by the cell area. */
+ * the same order (get*ChargeDensityDiffImpl), divided by the cell area.  The
+ * fixed-point scale applies to the charge before the division: pick it from
+ * the total |q| (e.g. the largest power of two with 4 sum|q| * scale < 2^62). */
 int csrst_charge_diff(int order, const double *ox, const double *oy, const double *x,
                       const double *y, const double *q, size_t n, const double *o2,
                       const double *hh2, int i0, int j0, int ni, int nj, double scale, double *rho);

@@ -94,6 +94,11 @@ def test_gather_golden_and_random(gpu_lib, oracle, order):
         assert np.array_equal(a, b)
 
 
+def charge_scale(q):
+    """Fixed-point scale for a charge sum: a power of two with 4 sum|q| below 2^62."""
+    return 2.0 ** np.floor(np.log2(2.0 ** 62 / (4.0 * np.abs(q).sum())))
+
+
 def random_moves(n, h, seed, cfl=0.5):
     rng = np.random.default_rng(seed)
     ox = rng.uniform(6, 14, n) * h[0]
@@ -119,7 +124,7 @@ def test_deposit_parity_and_continuity(gpu_lib, oracle, order):
         assert np.array_equal(a, b)                                   # same fixed point: bit-exact
         assert np.abs(a - c).max() <= 1e-12 * np.abs(c).max()         # reference FP64 order: 1e-12
         J[comp] = a
-    rho = sf.getChargeDensityDiff(ox, oy, x, y, q, (0, 0), h, 0, 0, 24, 24, scale)
+    rho = sf.getChargeDensityDiff(ox, oy, x, y, q, (0, 0), h, 0, 0, 24, 24, charge_scale(q))
     res = rho[1:, 1:] / dt + (J[0][1:, 1:] - J[0][1:, :-1]) / h[0] + (J[1][1:, 1:] - J[1][:-1, 1:]) / h[1]
     assert np.abs(res).max() <= 1e-10 * np.abs(rho / dt).max()
 
@@ -207,10 +212,15 @@ def test_moments_and_wake(gpu_lib, oracle):
     o.step(6)
     mg, mo = g.moments(), o.moments()
     # groups: rmean, pmean, rrms, prms, eps, rmin, rmax, (Ekin, dE); each
-    # within 1e-9 of the group's magnitude (the oracle sums in long double)
-    for a, b in ((0, 2), (2, 4), (4, 6), (6, 8), (8, 10), (10, 12), (12, 14), (14, 15), (15, 16)):
+    # within 1e-9 of the group's magnitude.  The momentum spread follows the
+    # reference's formula sum(p'^2) - N |<p>|^2 with <p> rounded to double
+    # (PartBunch.cpp:620-628): for |<p>| ~ 1e3 and spread ~ 1e-1 that
+    # formula itself carries ~1e-8 relative error, which bounds prms, eps
+    # and dE; the GPU centres p' first and is the more accurate of the two.
+    for a, b, tol in ((0, 2, 1e-9), (2, 4, 1e-9), (4, 6, 1e-9), (6, 8, 1e-7), (8, 10, 1e-7),
+                      (10, 12, 1e-9), (12, 14, 1e-9), (14, 15, 1e-9), (15, 16, 1e-7)):
         scale = np.abs(mo[a:b]).max()
-        assert np.abs(mg[a:b] - mo[a:b]).max() <= 1e-9 * scale, (a, mg[a:b], mo[a:b])
+        assert np.abs(mg[a:b] - mo[a:b]).max() <= tol * scale, (a, mg[a:b], mo[a:b])
     wg = g.wake()
     wo = o.wake(mo[:2], mo[2:4])
     assert np.array_equal(np.isnan(wg), np.isnan(wo))
@@ -243,7 +253,7 @@ def test_continuity_full_size(gpu_lib):
     sf = ShapeFunction(1)
     jx = sf.getCurrentDensityBase(0, x, y, nx, ny, q, org, h, dt, 0, 0, ni, nj, scale)
     jy = sf.getCurrentDensityBase(1, x, y, nx, ny, q, org, h, dt, 0, 0, ni, nj, scale)
-    rho = sf.getChargeDensityDiff(x, y, nx, ny, q, org, h, 0, 0, ni, nj, scale)
+    rho = sf.getChargeDensityDiff(x, y, nx, ny, q, org, h, 0, 0, ni, nj, charge_scale(q))
     res = rho[1:, 1:] / dt + (jx[1:, 1:] - jx[1:, :-1]) / h[0] + (jy[1:, 1:] - jy[:-1, 1:]) / h[1]
     assert np.abs(res).max() <= 1e-10 * np.abs(rho / dt).max()
 
