@@ -121,7 +121,7 @@ __global__ void k_push_post(WinState *ws) {
 }
 
 template <int ORDER, bool SMEM>
-__global__ void __launch_bounds__(256) k_push(PushArgs a) {
+__global__ void __launch_bounds__(256, 2) k_push(PushArgs a) {
   extern __shared__ unsigned long long sacc[];
   __shared__ int tb[4];  // touched box of this CTA (window cells)
   WinState *ws = a.ws;
@@ -155,14 +155,13 @@ __global__ void __launch_bounds__(256) k_push(PushArgs a) {
   const double scale = a.acc_scale;
   int ti0 = L0, tj0 = L1, ti1 = -1, tj1 = -1;  // cells this thread touched
   auto sink = [&](int i, int j, double v) {
-    if (i < 0 || j < 0 || i >= L0 || j >= L1) return;
-    const unsigned long long iv = (unsigned long long)__double2ll_rn(v * scale);
-    const int k = j * L0 + i;
+    const bool in = i >= 0 && j >= 0 && i < L0 && j < L1;
+    const long long iv = __double2ll_rn(v * scale);
     if (SMEM) {
-      atomicAdd(&sacc[k], iv);
-      ti0 = min(ti0, i); tj0 = min(tj0, j); ti1 = max(ti1, i); tj1 = max(tj1, j);
+      if (in) { ti0 = min(ti0, i); tj0 = min(tj0, j); ti1 = max(ti1, i); tj1 = max(tj1, j); }
+      warp_add(sacc, in ? j * L0 + i : -1, iv);
     } else {
-      atomicAdd(&a.acc[k], iv);
+      warp_add(a.acc, in ? j * L0 + i : -1, iv);
     }
   };
 
@@ -283,8 +282,8 @@ __global__ void k_deposit(int comp, const double *ox, const double *oy, const do
        i += (long long)gridDim.x * blockDim.x) {
     auto sink = [&](int a, int b, double v) {
       a -= i0; b -= j0;
-      if (a < 0 || b < 0 || a >= ni || b >= nj) return;
-      atomicAdd(&acc[(size_t)b * ni + a], (unsigned long long)__double2ll_rn(v * scale));
+      const bool in = a >= 0 && b >= 0 && a < ni && b < nj;
+      warp_add(acc, in ? b * ni + a : -1, __double2ll_rn(v * scale));
     };
     if (!deposit_particle<ORDER>(comp, q[i], ox[i], oy[i], x[i], y[i], org0, org1, h0, h1, dt, sink))
       atomicExch(err, kErrCrossings);
