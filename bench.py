@@ -91,7 +91,7 @@ class Clocks:
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
         try:
             self.p = subprocess.Popen(["nvidia-smi", f"--id={index}", f"--query-gpu={q}",
-                                       "--format=csv,noheader,nounits", "-lms", "100"],
+                                       "--format=csv,noheader,nounits", "-lms", "50"],
                                       stdout=self.f, stderr=subprocess.DEVNULL)
         except Exception:
             self.p = None
@@ -127,6 +127,9 @@ def run_b200(args, world, rank, local):
     sim = Simulation(cfg)
     sim.load(*bunch)
     stream = torch.cuda.ExternalStream(sim.stream())
+    # clocks are sampled from before the warm-up to the end of the kernel
+    # attribution pass: the GPU runs this workload the whole time
+    clocks = Clocks(local) if rank == 0 else None
     sim.step(args.warmup)
     sim.sync()
 
@@ -134,7 +137,6 @@ def run_b200(args, world, rank, local):
     if world > 1:
         torch.distributed.barrier()
     torch.cuda.synchronize()
-    clocks = Clocks(local) if rank == 0 else None
     t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     t0.record(stream)
     sim.step(args.steps)
@@ -142,7 +144,6 @@ def run_b200(args, world, rank, local):
     sim.sync()
     torch.cuda.synchronize()
     ms = t0.elapsed_time(t1)
-    clk = clocks.stop() if clocks else None
     if world > 1:
         t = torch.tensor([ms], device="cuda")
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
@@ -172,6 +173,7 @@ def run_b200(args, world, rank, local):
         groups["move"] += ev[6].elapsed_time(ev[7])
     for k in groups:
         groups[k] /= ksteps
+    clk = clocks.stop() if clocks else None
     hbm, src = peaks()
 
     def roof(key, bytes_step, ms_):
