@@ -78,6 +78,8 @@ def lib():
                            C.c_int, C.c_int, C.c_int, C.c_double, D], C.c_int),
         "csrst_charge_diff": ([C.c_int, D, D, D, D, D, C.c_size_t, D, D, C.c_int, C.c_int, C.c_int,
                                C.c_int, C.c_double, D], C.c_int),
+        "csrst_deposit_noalloc": ([C.c_int, C.c_int, P, P, P, P, P, C.c_size_t, D, D, C.c_double,
+                                   C.c_int, C.c_int, C.c_int, C.c_int, C.c_double, P, P], C.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)

@@ -142,6 +142,27 @@ int csrst_charge_diff(int order, const double *ox, const double *oy, const doubl
                       const double *y, const double *q, size_t n, const double *o2,
                       const double *hh2, int i0, int j0, int ni, int nj, double scale, double *rho);
 
+/* Allocation-free csrst_deposit, for callers that cannot let a library
+ * allocate device memory: a host framework that owns all device memory
+ * through its own pool and budget, or a time loop that must not stall the
+ * device (cudaMalloc and cudaFree synchronise it).  No counterpart in the
+ * reference, which deposits on the CPU.
+ *  - ox, oy, x, y, q and J are DEVICE pointers owned by the caller; o2 and
+ *    hh2 are host arrays of 2 doubles.  Same result as csrst_deposit.
+ *  - The fixed-point accumulator is a file-scope __device__ array of 2^20
+ *    cells (8 MiB) that every GPU which loads the library holds until exit;
+ *    ni * nj above 2^20 is rejected with CSRST_E_ARG.  Nothing is allocated
+ *    or freed (no cudaMalloc, cudaFree or allocating library call).
+ *  - The first call on a device looks up the array's device address
+ *    (cudaGetSymbolAddress) and should come before any stream capture.
+ *  - Runs on `stream` (a cudaStream_t, NULL = default stream) and returns
+ *    after it has finished.  All calls share the one array per device, so
+ *    calls that overlap on the GPU (other threads or streams) race. */
+int csrst_deposit_noalloc(int order, int comp, const double *ox, const double *oy, const double *x,
+                          const double *y, const double *q, size_t n, const double *o2,
+                          const double *hh2, double dt, int i0, int j0, int ni, int nj, double scale,
+                          double *J, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
