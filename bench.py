@@ -96,6 +96,15 @@ class Clocks:
         except Exception:
             self.p = None
 
+    def soak(self, sim, seconds=0.8):
+        """Keeps the GPU on this workload until the sampler has produced
+        samples under load (the timed region alone is often shorter than the
+        sampling period).  Untimed steps, like the warm-up."""
+        t = time.perf_counter()
+        while time.perf_counter() - t < seconds:
+            sim.step(20)
+            sim.sync()
+
     def stop(self):
         if self.p is None:
             return None
@@ -132,6 +141,8 @@ def run_b200(args, world, rank, local):
     clocks = Clocks(local) if rank == 0 else None
     sim.step(args.warmup)
     sim.sync()
+    if clocks:
+        clocks.soak(sim)
 
     # ---- timed region: graph-captured steps, inputs resident in HBM ----
     if world > 1:

@@ -302,17 +302,23 @@ __device__ __forceinline__ void deposit_segment(int comp, double q, double a0, d
 // 1e-6 merging and end-point substitution as border_crossings, kept in
 // registers.  Returns false when a particle crosses more borders; the caller
 // then takes the general path.
+// floor(v / h - shift) with the IEEE quotient, as the reference computes it.
+// v * (1/h) is within a few ulps of the rounded quotient, so its floor is the
+// same integer unless it lies within 1e-9 of an integer; only then is the
+// division carried out.
+__device__ __forceinline__ int floor_div(double v, double h, double ooh, double shift) {
+  const double a = v * ooh - shift;
+  const double f = floor(a);
+  if (a - f > 1e-9 && (f + 1.0) - a > 1e-9) return (int)f;
+  return (int)floor(v / h - shift);
+}
+
 template <bool DUAL, class Seg>
 __device__ __forceinline__ bool segments_fast(double o0, double o1, double n0, double n1, double h0, double h1,
                                               Seg &&seg) {
-  int Ii, Ji, If, Jf;
-  if (DUAL) {
-    Ii = (int)floor(o0 / h0 - 0.5); Ji = (int)floor(o1 / h1 - 0.5);
-    If = (int)floor(n0 / h0 - 0.5); Jf = (int)floor(n1 / h1 - 0.5);
-  } else {
-    Ii = (int)floor(o0 / h0); Ji = (int)floor(o1 / h1);
-    If = (int)floor(n0 / h0); Jf = (int)floor(n1 / h1);
-  }
+  const double sh = DUAL ? 0.5 : 0.0, ooh0 = 1.0 / h0, ooh1 = 1.0 / h1;
+  const int Ii = floor_div(o0, h0, ooh0, sh), Ji = floor_div(o1, h1, ooh1, sh);
+  const int If = floor_div(n0, h0, ooh0, sh), Jf = floor_div(n1, h1, ooh1, sh);
   if (abs(If - Ii) > 1 || abs(Jf - Ji) > 1) return false;
   const double D0 = n0 - o0, D1 = n1 - o1;
   const bool hx = If != Ii, hy = Jf != Ji;
