@@ -59,6 +59,7 @@ def lib():
         "csrst_get_static_fields": ([P, D, D, D, D], C.c_int),
         "csrst_reset_outside": ([P], C.c_int),
         "csrst_load_particles": ([P, D, D, D, D, D, C.c_size_t], C.c_int),
+        "csrst_initial_fields": ([P, C.c_double, C.c_double, C.c_int, D], C.c_int),
         "csrst_get_particles": ([P, D, D, D, D], C.c_int),
         "csrst_get_old_positions": ([P, D, D], C.c_int),
         "csrst_get_window": ([P, I, D, I], C.c_int),

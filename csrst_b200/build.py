@@ -10,7 +10,7 @@ import sys
 from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
-SRC = ["api.cu", "geometry.cu", "particles.cu", "fields.cu", "diag.cu", "noalloc.cu"]
+SRC = ["api.cu", "geometry.cu", "particles.cu", "fields.cu", "diag.cu", "poisson.cu", "noalloc.cu"]
 OUT = HERE / "libcsrst_gpu.so"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "--fmad=false", "-lineinfo", "-Xcompiler", "-fPIC",

@@ -88,6 +88,7 @@ struct csrst_handle {
   double *x = nullptr, *y = nullptr, *px = nullptr, *py = nullptr, *q = nullptr;
   double *ox = nullptr, *oy = nullptr;
   bool pending = false;
+  bool fresh = false;  // loaded, no push yet
   BBoxState bb = kBBInvalid;
   int push_grid = 0;
   // diagnostics scratch
@@ -246,6 +247,7 @@ int push_async(csrst_handle *h, int jcomp) {
   launch_push(push_args(h, jcomp), h->order, h->L0, h->L1, h->push_grid, h->s);
   launch_global_bounds(h->ws, h->b.hr0, h->b.hr1, h->s);
   h->pending = false;
+  h->fresh = false;
   h->bb = kBBValidIfPending;
   h->acc_fresh[jcomp] = true;
   return CSRST_OK;
@@ -533,8 +535,43 @@ int csrst_load_particles(csrst_handle *h, const double *x, const double *y, cons
   h->acc_fresh[0] = h->acc_fresh[1] = false;
   launch_bbox_next(h->x, h->y, h->px, h->py, N, h->half, 0, h->ws, h->s);
   h->bb = kBBValid;
+  h->fresh = true;
   CK(cudaStreamSynchronize(h->s));
   CK(cudaGetLastError());
+  return check_err(h);
+}
+
+int csrst_initial_fields(csrst_handle *h, double tol_first, double tol_rest, int max_iter, double *report8) {
+  int rc = need_bunch(h);
+  if (rc) return rc;
+  if (!h->fresh) return fail(h, CSRST_E_ARG, "initial fields need a freshly loaded bunch (before the first push)");
+  if (!(tol_first > 0) || !(tol_rest > 0) || max_iter < 1) return fail(h, CSRST_E_ARG, "invalid tolerance");
+  PoissonInput in{};
+  in.x = h->x; in.y = h->y; in.px = h->px; in.py = h->py; in.q = h->q; in.n = h->n;
+  in.order = h->order;
+  in.mask = h->mask; in.cutidx = h->cutidx; in.cells = h->cells;
+  in.b = h->b; in.dt = h->dt;
+  in.Ex = plane(h->Ex, h->pitch); in.Ey = plane(h->Ey, h->pitch);
+  in.Hx = plane(h->Hx, h->pitch); in.Hy = plane(h->Hy, h->pitch);
+  in.tol_first = tol_first; in.tol_rest = tol_rest; in.maxit = max_iter;
+  PoissonReport rep{};
+  std::string msg;
+  rc = poisson_initial_fields(in, &rep, h->s, &msg);
+  if (rc) return fail(h, rc == kErrCuda ? CSRST_E_CUDA : CSRST_E_ARG, "initial fields: " + msg);
+  // resetOutsideDomain, then copyFields + exchangeBoundaries (main.cpp:248, :335-342)
+  FieldArgs fa = field_args(h, 0);
+  launch_reset_outside(fa, h->cutidx, h->s);
+  launch_copy_to_window(fa, h->s);
+  launch_exchange(fa, 0, h->s);
+  launch_exchange(fa, 1, h->s);
+  launch_exchange(fa, 2, h->s);
+  CK(cudaStreamSynchronize(h->s));
+  CK(cudaGetLastError());
+  if (report8) {
+    report8[0] = rep.gamma;
+    for (int k = 0; k < 3; ++k) { report8[1 + 2 * k] = rep.iters[k]; report8[2 + 2 * k] = rep.relres[k]; }
+    report8[7] = rep.levels;
+  }
   return check_err(h);
 }
 

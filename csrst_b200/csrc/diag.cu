@@ -179,37 +179,7 @@ __global__ void k_charge_diff(const double *ox, const double *oy, const double *
         if (i < 0 || j < 0 || i >= ni || j >= nj) return;
         atomicAdd(&acc[(size_t)j * ni + i], (unsigned long long)__double2ll_rn(sg * v * scale));
       };
-      if (ORDER == 0) {
-        const double a = (X - org0) / h0, b = (Y - org1) / h1;
-        const int I = (int)floor(a), J = (int)floor(b);
-        const double t0 = a - I, t1 = b - J;
-        add(I, J, (1.0 - t0) * (1.0 - t1) * qq);
-        add(I + 1, J, t0 * (1.0 - t1) * qq);
-        add(I, J + 1, (1.0 - t0) * t1 * qq);
-        add(I + 1, J + 1, t0 * t1 * qq);
-      } else if (ORDER == 1) {
-        const double n0 = (X - org0) / h0, n1 = (Y - org1) / h1;
-        const int I = (int)floor(n0 + 0.5), J = (int)floor(n1 + 0.5);
-        const double a = n0 - I, b = n1 - J;
-        const double sxm = qq * (0.5 - a) * (0.5 - a) * 0.5, sxp = qq * (0.5 + a) * (0.5 + a) * 0.5;
-        const double sx = qq - sxm - sxp;
-        const double sym = (0.5 - b) * (0.5 - b) * 0.5, syp = (0.5 + b) * (0.5 + b) * 0.5;
-        const double sy = 1.0 - sym - syp;
-        const double wx[3] = {sxm, sx, sxp}, wy[3] = {sym, sy, syp};
-        for (int bb = 0; bb < 3; ++bb)
-          for (int aa = 0; aa < 3; ++aa) add(I - 1 + aa, J - 1 + bb, wx[aa] * wy[bb]);
-      } else {
-        const double n0 = (X - org0) / h0, n1 = (Y - org1) / h1;
-        const int I = (int)floor(n0), J = (int)floor(n1);
-        const double a = n0 - I, b = n1 - J;
-        const double s6 = 1.0 / 6.0;
-        const double wx[4] = {s6 * ((1.0 - a) * (1.0 - a) * (1.0 - a)), s6 * (4.0 - 3.0 * a * a * (2.0 - a)),
-                              s6 * (4.0 - 3.0 * (1.0 - a) * (1.0 - a) * (1.0 + a)), s6 * (a * a * a)};
-        const double wy[4] = {s6 * ((1.0 - b) * (1.0 - b) * (1.0 - b)), s6 * (4.0 - 3.0 * b * b * (2.0 - b)),
-                              s6 * (4.0 - 3.0 * (1.0 - b) * (1.0 - b) * (1.0 + b)), s6 * (b * b * b)};
-        for (int bb = 0; bb < 4; ++bb)
-          for (int aa = 0; aa < 4; ++aa) add(I - 1 + aa, J - 1 + bb, qq * wx[aa] * wy[bb]);
-      }
+      charge_shape<ORDER>(X, Y, qq, org0, org1, h0, h1, add);
     }
   }
 }

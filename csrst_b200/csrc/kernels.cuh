@@ -1,6 +1,8 @@
 // Argument blocks and host launchers shared by the kernel files and the C ABI.
 #pragma once
 
+#include <string>
+
 #include "common.cuh"
 
 namespace csrst {
@@ -92,5 +94,27 @@ void launch_charge_diff(int order, const double *ox, const double *oy, const dou
                         const double *q, long long n, double org0, double org1, double h0, double h1,
                         int i0, int j0, int ni, int nj, unsigned long long *acc, double scale,
                         cudaStream_t s);
+
+// poisson.cu: initial fields of the bunch (PoissonSolver::computeField)
+struct PoissonInput {
+  const double *x, *y, *px, *py, *q;  // bunch on the device, positions R
+  long long n;
+  int order;                          // charge shape
+  const uint8_t *mask;                // inside mask, Nx * Ny
+  const int *cutidx;                  // cut-cell index per cell or -1
+  const CutCellDev *cells;
+  BendDev b;
+  double dt;
+  Plane Ex, Ey, Hx, Hy;               // static planes written
+  double tol_first, tol_rest;         // relative residual of solve 1 and of solves 2, 3
+  int maxit;
+};
+struct PoissonReport {
+  double gamma;
+  int iters[3];
+  double relres[3];
+  int levels;
+};
+int poisson_initial_fields(const PoissonInput &in, PoissonReport *rep, cudaStream_t s, std::string *msg);
 
 }  // namespace csrst

@@ -405,4 +405,48 @@ __device__ __forceinline__ void warp_add(unsigned long long *acc, int k, long lo
   }
 }
 
+// Vertex charge shape of one particle (getChargeDensityImpl and
+// getChargeDensityDiffImpl of ZerothOrderShapeFunction.cpp:355-366,
+// FirstOrderShapeFunction.cpp:391-416, SecondOrderShapeFunction.cpp:408-441):
+// add(i, j, w) for every vertex weight w of charge qq at (X, Y).
+template <int ORDER, class Add>
+__device__ __forceinline__ void charge_shape(double X, double Y, double qq, double org0, double org1, double h0,
+                                             double h1, Add &&add) {
+  if (ORDER == 0) {
+    const double a = (X - org0) / h0, b = (Y - org1) / h1;
+    const int I = (int)floor(a), J = (int)floor(b);
+    const double t0 = a - I, t1 = b - J;
+    add(I, J, (1.0 - t0) * (1.0 - t1) * qq);
+    add(I + 1, J, t0 * (1.0 - t1) * qq);
+    add(I, J + 1, (1.0 - t0) * t1 * qq);
+    add(I + 1, J + 1, t0 * t1 * qq);
+  } else if (ORDER == 1) {
+    const double n0 = (X - org0) / h0, n1 = (Y - org1) / h1;
+    const int I = (int)floor(n0 + 0.5), J = (int)floor(n1 + 0.5);
+    const double a = n0 - I, b = n1 - J;
+    const double sxm = qq * (0.5 - a) * (0.5 - a) * 0.5, sxp = qq * (0.5 + a) * (0.5 + a) * 0.5;
+    const double sx = qq - sxm - sxp;
+    const double sym = (0.5 - b) * (0.5 - b) * 0.5, syp = (0.5 + b) * (0.5 + b) * 0.5;
+    const double sy = 1.0 - sym - syp;
+    const double wx[3] = {sxm, sx, sxp}, wy[3] = {sym, sy, syp};
+#pragma unroll
+    for (int bb = 0; bb < 3; ++bb)
+#pragma unroll
+      for (int aa = 0; aa < 3; ++aa) add(I - 1 + aa, J - 1 + bb, wx[aa] * wy[bb]);
+  } else {
+    const double n0 = (X - org0) / h0, n1 = (Y - org1) / h1;
+    const int I = (int)floor(n0), J = (int)floor(n1);
+    const double a = n0 - I, b = n1 - J;
+    const double s6 = 1.0 / 6.0;
+    const double wx[4] = {s6 * ((1.0 - a) * (1.0 - a) * (1.0 - a)), s6 * (4.0 - 3.0 * a * a * (2.0 - a)),
+                          s6 * (4.0 - 3.0 * (1.0 - a) * (1.0 - a) * (1.0 + a)), s6 * (a * a * a)};
+    const double wy[4] = {s6 * ((1.0 - b) * (1.0 - b) * (1.0 - b)), s6 * (4.0 - 3.0 * b * b * (2.0 - b)),
+                          s6 * (4.0 - 3.0 * (1.0 - b) * (1.0 - b) * (1.0 + b)), s6 * (b * b * b)};
+#pragma unroll
+    for (int bb = 0; bb < 4; ++bb)
+#pragma unroll
+      for (int aa = 0; aa < 4; ++aa) add(I - 1 + aa, J - 1 + bb, qq * wx[aa] * wy[bb]);
+  }
+}
+
 }  // namespace csrst

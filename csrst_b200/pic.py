@@ -90,6 +90,15 @@ class Simulation:
         self.n = len(a[0])
         self._ck(lib().csrst_load_particles(self.h, *map(ptr, a), self.n))
 
+    def initial_fields(self, tol_first=1e-12, tol_rest=1e-6, max_iter=500):
+        """PoissonSolver::computeField for the loaded bunch (PoissonSolver.cpp:85-201):
+        writes Ey, Hz, Ex of the static mesh and refills the window.  Returns
+        {"gamma", "solves": [(iterations, relative residual)] * 3, "levels"}."""
+        r = np.zeros(8)
+        self._ck(lib().csrst_initial_fields(self.h, tol_first, tol_rest, int(max_iter), ptr(r)))
+        return {"gamma": r[0], "solves": [(int(r[1 + 2 * k]), r[2 + 2 * k]) for k in range(3)],
+                "levels": int(r[7])}
+
     # -- state ----------------------------------------------------------------
     def particles(self):
         a = [np.zeros(self.n) for _ in range(4)]
@@ -192,6 +201,19 @@ class TETMSolver:
 
 def moveMesh(sim: Simulation):
     sim.move()
+
+
+class PoissonSolver:
+    """PoissonSolver (PoissonSolver.hh:47-125) over a Simulation's loaded bunch."""
+
+    def __init__(self, sim: Simulation):
+        self.sim = sim
+
+    def computeField(self, tol=1e-12, maxIterations=500):
+        """The three solves of PoissonSolver::computeField (PoissonSolver.cpp:85-201),
+        the first to tol, the others to 1e-6 as the reference does (:172), then
+        SCBoundaryCondition::resetOutsideDomain (main.cpp:248)."""
+        return self.sim.initial_fields(tol, 1e-6, maxIterations)
 
 
 class ScatterGatherImpl:

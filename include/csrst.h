@@ -87,6 +87,16 @@ int csrst_reset_outside(csrst_handle *h);
  * main.cpp:335-342).  q: charge per macro-particle [C]. */
 int csrst_load_particles(csrst_handle *h, const double *x, const double *y, const double *px,
                          const double *py, const double *q, size_t n);
+/* Initial fields of the loaded bunch (main.cpp:232-248): the three boosted
+ * electrostatic solves of PoissonSolver::computeField (PoissonSolver.cpp:85-201)
+ * on the matrix of cutoffStencil (:678-766) fill Ey, Hz and Ex of the static
+ * mesh (fillFields, :441-507), then SCBoundaryCondition::resetOutsideDomain
+ * runs and the window is refilled.  Multigrid-preconditioned CG in FP64 on the
+ * GPU replaces Trilinos ML + BlockCG.  tol_first / tol_rest: relative residual
+ * of the first solve (main.cpp:94, 1e-12) and of the other two (1e-6);
+ * max_iter per solve (main.cpp:93, 500).  report8 (may be NULL): gamma,
+ * iterations and relative residual of each solve, multigrid levels. */
+int csrst_initial_fields(csrst_handle *h, double tol_first, double tol_rest, int max_iter, double *report8);
 /* Current bunch in the handle's (cell-sorted) order. */
 int csrst_get_particles(csrst_handle *h, double *x, double *y, double *px, double *py);
 /* oldR of the last push (PartBunch::oldR). */

@@ -5,6 +5,7 @@
 //             getGlobalBounds                                   (src/PartBunch.hh:46-112)
 //   ScatterGatherImpl<IntOp, double>::gather                    (src/ScatterGatherImpl.hh:27-64)
 //   moveMesh                                                    (src/main.cpp:562-652)
+//   PoissonSolver::computeField                                 (src/PoissonSolver.cpp:85-201)
 // IPPL field and attribute types are replaced by plain host arrays; the
 // fields and the bunch themselves live on the GPU inside a Simulation.
 // Failures throw csrst::Error (the reference aborts through PAssert).
@@ -117,6 +118,24 @@ class TETMSolver {
 };
 
 inline void moveMesh(Simulation &s) { check(csrst_move_window(s.handle()), s.handle()); }
+
+// Initial fields of the loaded bunch (PoissonSolver::computeField,
+// src/PoissonSolver.cpp:85-201, followed by resetOutsideDomain as in
+// src/main.cpp:232-248).  tol is the first solve's relative residual; the
+// other two use 1e-6 as the reference does (PoissonSolver.cpp:172).
+class PoissonSolver {
+ public:
+  explicit PoissonSolver(Simulation &s) : s_(s) {}
+  void computeField(double tol = 1e-12, int maxIterations = 500) {
+    check(csrst_initial_fields(s_.handle(), tol, 1e-6, maxIterations, report_.data()), s_.handle());
+  }
+  // gamma, (iterations, relative residual) of each solve, multigrid levels
+  const std::array<double, 8> &report() const { return report_; }
+
+ private:
+  Simulation &s_;
+  std::array<double, 8> report_{};
+};
 
 // A dense field patch on the host (the reference's FieldPatch<double>,
 // src/FieldPatch.hh:33-132): element (i, j) at data[j * nx + i].

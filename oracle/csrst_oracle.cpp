@@ -1133,6 +1133,205 @@ int move_window(Sim &s) {
   return 0;
 }
 
+// Vertex charge shape of one particle (getChargeDensityImpl /
+// getChargeDensityDiffImpl of Zeroth/First/SecondOrderShapeFunction):
+// add(i, j, sg * w) for every vertex weight w of charge qq at (X, Y).
+template <class Add>
+void charge_shape(int order, double X, double Y, double qq, double sg, double org0, double org1, double h0,
+                  double h1, Add &&add) {
+  const double onesixth = 1.0 / 6.0;
+  if (order == 0) {  // ZerothOrderShapeFunction.cpp:355-366
+    double xi0 = (X - org0) / h0, xi1 = (Y - org1) / h1;
+    int I = (int)std::floor(xi0), J = (int)std::floor(xi1);
+    double t0 = xi0 - I, t1 = xi1 - J;
+    add(I, J, sg * ((1.0 - t0) * (1.0 - t1) * qq));
+    add(I + 1, J, sg * (t0 * (1.0 - t1) * qq));
+    add(I, J + 1, sg * ((1.0 - t0) * t1 * qq));
+    add(I + 1, J + 1, sg * (t0 * t1 * qq));
+  } else if (order == 1) {  // FirstOrderShapeFunction.cpp:391-416
+    double n0 = (X - org0) / h0, n1 = (Y - org1) / h1;
+    int I = (int)std::floor(n0 + 0.5), J = (int)std::floor(n1 + 0.5);
+    double a = n0 - I, b = n1 - J;
+    double sxm = qq * (0.5 - a) * (0.5 - a) * 0.5, sxp = qq * (0.5 + a) * (0.5 + a) * 0.5;
+    double sx = qq - sxm - sxp;
+    double sym = (0.5 - b) * (0.5 - b) * 0.5, syp = (0.5 + b) * (0.5 + b) * 0.5;
+    double sy = 1.0 - sym - syp;
+    double wx[3] = {sxm, sx, sxp}, wy[3] = {sym, sy, syp};
+    for (int bb = 0; bb < 3; ++bb)
+      for (int aa = 0; aa < 3; ++aa) add(I - 1 + aa, J - 1 + bb, sg * (wx[aa] * wy[bb]));
+  } else {  // SecondOrderShapeFunction.cpp:408-441
+    double n0 = (X - org0) / h0, n1 = (Y - org1) / h1;
+    int I = (int)std::floor(n0), J = (int)std::floor(n1);
+    double a = n0 - I, b = n1 - J;
+    auto p3 = [](double v) { return v * v * v; };
+    double wx[4] = {onesixth * p3(1.0 - a), onesixth * (4.0 - 3.0 * a * a * (2.0 - a)),
+                    onesixth * (4.0 - 3.0 * (1.0 - a) * (1.0 - a) * (1.0 + a)), onesixth * p3(a)};
+    double wy[4] = {onesixth * p3(1.0 - b), onesixth * (4.0 - 3.0 * b * b * (2.0 - b)),
+                    onesixth * (4.0 - 3.0 * (1.0 - b) * (1.0 - b) * (1.0 + b)), onesixth * p3(b)};
+    for (int bb = 0; bb < 4; ++bb)
+      for (int aa = 0; aa < 4; ++aa) add(I - 1 + aa, J - 1 + bb, sg * (qq * wx[aa] * wy[bb]));
+  }
+}
+
+// ---- initial fields: boosted electrostatic solve ---------------------------
+// PoissonSolver::computeField (PoissonSolver.cpp:85-201) with the matrix of
+// cutoffStencil (:678-766).  The reference solves with Trilinos ML-preconditioned
+// BlockCG; here the same matrix is solved by CG with a y-line Jacobi
+// preconditioner (an independent method, so that it checks the GPU solver).
+struct PoissonSys {
+  int Nx = 0, Ny = 0;
+  double EW = 0, NS = 0, D = 0;
+  std::vector<uint8_t> good, act;  // good: inside or cut area > 0.5; act: good and i < maxX
+};
+
+void poisson_setup(const Sim &s, double gamma, PoissonSys &p) {
+  const int Nx = s.b.Nx, Ny = s.b.Ny;
+  p.Nx = Nx; p.Ny = Ny;
+  const double hr0 = s.b.hr0 * gamma, hr1 = s.b.hr1;  // PoissonSolver ctor, :70-71
+  p.EW = -1 / (hr0 * hr0);
+  p.NS = -1 / (hr1 * hr1);
+  p.D = -2 * (p.EW + p.NS);
+  const long maxX = (long)(size_t)(s.b.Lb / s.b.hr0);  // Bend::getLengthStraightSection
+  p.good.assign((size_t)Nx * Ny, 0);
+  p.act.assign((size_t)Nx * Ny, 0);
+  for (int j = 0; j < Ny; ++j)
+    for (int i = 0; i < Nx; ++i) {
+      const size_t k = (size_t)j * Nx + i;
+      const int c = s.inv[k];
+      p.good[k] = s.inside[k] || (c > -1 && s.cells[c].area > 0.5);
+      p.act[k] = p.good[k] && i < maxX;
+    }
+}
+
+// Out-of-domain neighbours count as not good (Dirichlet zero).
+inline bool pgood(const PoissonSys &p, int i, int j) {
+  return i >= 0 && j >= 0 && i < p.Nx && j < p.Ny && p.good[(size_t)j * p.Nx + i];
+}
+inline bool pact(const PoissonSys &p, int i, int j) {
+  return i >= 0 && j >= 0 && i < p.Nx && j < p.Ny && p.act[(size_t)j * p.Nx + i];
+}
+
+// Solve A phi = b.  Rows that are not active are identity rows, so
+// phi = b there; their values move to the right-hand side of the active rows
+// they couple to.  x holds the initial guess on entry (active entries used).
+// Returns the iteration count; relres receives ||r|| / ||b_active||.
+int poisson_solve(const PoissonSys &p, const std::vector<double> &b, std::vector<double> &x, double tol,
+                  int maxit, double *relres) {
+  const int Nx = p.Nx, Ny = p.Ny;
+  const size_t n = (size_t)Nx * Ny;
+  std::vector<double> f(n, 0.0), r(n, 0.0), z(n, 0.0), d(n, 0.0), q(n, 0.0);
+  for (int j = 0; j < Ny; ++j)
+    for (int i = 0; i < Nx; ++i) {
+      const size_t k = (size_t)j * Nx + i;
+      if (!p.act[k]) { x[k] = b[k]; continue; }
+      double v = b[k];
+      const int di[4] = {0, -1, 1, 0}, dj[4] = {-1, 0, 0, 1};
+      for (int t = 0; t < 4; ++t) {
+        const int a = i + di[t], c = j + dj[t];
+        if (pgood(p, a, c) && !pact(p, a, c)) v -= (dj[t] ? p.NS : p.EW) * b[(size_t)c * Nx + a];
+      }
+      f[k] = v;
+    }
+  auto apply = [&](const std::vector<double> &u, std::vector<double> &out) {
+    for (int j = 0; j < Ny; ++j)
+      for (int i = 0; i < Nx; ++i) {
+        const size_t k = (size_t)j * Nx + i;
+        if (!p.act[k]) { out[k] = 0.0; continue; }
+        double v = p.D * u[k];
+        if (pact(p, i - 1, j)) v += p.EW * u[k - 1];
+        if (pact(p, i + 1, j)) v += p.EW * u[k + 1];
+        if (pact(p, i, j - 1)) v += p.NS * u[k - Nx];
+        if (pact(p, i, j + 1)) v += p.NS * u[k + Nx];
+        out[k] = v;
+      }
+  };
+  // y-line Jacobi: one tridiagonal solve per column (Thomas algorithm)
+  std::vector<double> cp(Ny), dp(Ny);
+  auto precond = [&](const std::vector<double> &rr, std::vector<double> &zz) {
+    for (int i = 0; i < Nx; ++i) {
+      double cprev = 0.0, dprev = 0.0;
+      for (int j = 0; j < Ny; ++j) {
+        const size_t k = (size_t)j * Nx + i;
+        if (!p.act[k]) { cp[j] = 0.0; dp[j] = 0.0; cprev = 0.0; dprev = 0.0; continue; }
+        const double a = pact(p, i, j - 1) ? p.NS : 0.0, c = pact(p, i, j + 1) ? p.NS : 0.0;
+        const double m = p.D - a * cprev;
+        cp[j] = c / m;
+        dp[j] = (rr[k] - a * dprev) / m;
+        cprev = cp[j]; dprev = dp[j];
+      }
+      double u = 0.0;
+      for (int j = Ny - 1; j >= 0; --j) {
+        u = dp[j] - cp[j] * u;
+        zz[(size_t)j * Nx + i] = p.act[(size_t)j * Nx + i] ? u : 0.0;
+      }
+    }
+  };
+  auto dot = [&](const std::vector<double> &a, const std::vector<double> &c) {
+    double s = 0.0;
+    for (size_t k = 0; k < n; ++k) s += a[k] * c[k];
+    return s;
+  };
+  std::vector<double> u(n, 0.0);
+  for (size_t k = 0; k < n; ++k) u[k] = p.act[k] ? x[k] : 0.0;
+  apply(u, q);
+  for (size_t k = 0; k < n; ++k) r[k] = f[k] - q[k];
+  const double bn = std::sqrt(dot(f, f));
+  int it = 0;
+  double rn = std::sqrt(dot(r, r));
+  if (bn == 0.0) {
+    for (size_t k = 0; k < n; ++k) if (p.act[k]) x[k] = 0.0;
+    *relres = 0.0;
+    return 0;
+  }
+  precond(r, z);
+  d = z;
+  double rz = dot(r, z);
+  while (rn / bn > tol && it < maxit) {
+    apply(d, q);
+    const double alpha = rz / dot(d, q);
+    for (size_t k = 0; k < n; ++k) { u[k] += alpha * d[k]; r[k] -= alpha * q[k]; }
+    ++it;
+    rn = std::sqrt(dot(r, r));
+    if (rn / bn <= tol) break;
+    precond(r, z);
+    const double rz1 = dot(r, z);
+    const double beta = rz1 / rz;
+    rz = rz1;
+    for (size_t k = 0; k < n; ++k) d[k] = z[k] + beta * d[k];
+  }
+  for (size_t k = 0; k < n; ++k) if (p.act[k]) x[k] = u[k];
+  *relres = rn / bn;
+  return it;
+}
+
+// rho(R) / (eps0 gamma) on the Nx x Ny vertices (scatterQ + fillRHS).
+void poisson_rhs(const Sim &s, const std::vector<double> &X, const std::vector<double> &Y, double gamma,
+                 std::vector<double> &b) {
+  const int Nx = s.b.Nx, Ny = s.b.Ny;
+  std::vector<double> r((size_t)Nx * Ny, 0.0);
+  for (size_t k = 0; k < X.size(); ++k)
+    charge_shape(s.order, X[k], Y[k], s.q[k], 1.0, s.b.org0, s.b.org1, s.b.hr0, s.b.hr1,
+                 [&](int i, int j, double v) {
+                   if (i >= 0 && j >= 0 && i < Nx && j < Ny) r[(size_t)j * Nx + i] += v;
+                 });
+  const double cc = 1 / (EPS0 * gamma);
+  b.resize(r.size());
+  for (size_t k = 0; k < r.size(); ++k) b[k] = (r[k] / (s.b.hr0 * s.b.hr1)) * cc;
+}
+
+// copyFields static -> window interior (main.cpp:335-337), then the three
+// exchanges (:340-342).
+void copy_to_window(Sim &s) {
+  for (int j = 0; j < s.L1; ++j)
+    for (int i = 0; i < s.L0; ++i) {
+      int si = i + s.P0, sj = j + s.P1;
+      if (si < 0 || sj < 0 || si >= s.b.Nx || sj >= s.b.Ny) continue;
+      s.mEx.at(i, j) = s.Ex.at(si, sj); s.mEy.at(i, j) = s.Ey.at(si, sj);
+      s.mHx.at(i, j) = s.Hx.at(si, sj); s.mHy.at(i, j) = s.Hy.at(si, sj);
+    }
+  exchange(s, 0); exchange(s, 1); exchange(s, 2);
+}
+
 }  // namespace
 
 // ===========================================================================
@@ -1214,44 +1413,9 @@ void orc_charge_diff(int order, const double *ox, const double *oy, const double
     int a = i - i0, b = j - j0;
     if (a >= 0 && b >= 0 && a < ni && b < nj) r[(size_t)b * ni + a] += v;
   };
-  const double onesixth = 1.0 / 6.0;
   for (long k = 0; k < n; ++k) {
-    for (int pass = 0; pass < 2; ++pass) {
-      const double sg = pass == 0 ? 1.0 : -1.0;
-      const double px = pass == 0 ? x[k] : ox[k], py = pass == 0 ? y[k] : oy[k];
-      const double qq = q[k];
-      if (order == 0) {
-        double xi0 = (px - org0) / h0, xi1 = (py - org1) / h1;
-        int I = (int)std::floor(xi0), J = (int)std::floor(xi1);
-        double t0 = xi0 - I, t1 = xi1 - J;
-        add(I, J, sg * ((1.0 - t0) * (1.0 - t1) * qq));
-        add(I + 1, J, sg * (t0 * (1.0 - t1) * qq));
-        add(I, J + 1, sg * ((1.0 - t0) * t1 * qq));
-        add(I + 1, J + 1, sg * (t0 * t1 * qq));
-      } else if (order == 1) {
-        double n0 = (px - org0) / h0, n1 = (py - org1) / h1;
-        int I = (int)std::floor(n0 + 0.5), J = (int)std::floor(n1 + 0.5);
-        double a = n0 - I, b = n1 - J;
-        double sxm = qq * (0.5 - a) * (0.5 - a) * 0.5, sxp = qq * (0.5 + a) * (0.5 + a) * 0.5;
-        double sx = qq - sxm - sxp;
-        double sym = (0.5 - b) * (0.5 - b) * 0.5, syp = (0.5 + b) * (0.5 + b) * 0.5;
-        double sy = 1.0 - sym - syp;
-        double wx[3] = {sxm, sx, sxp}, wy[3] = {sym, sy, syp};
-        for (int bb = 0; bb < 3; ++bb)
-          for (int aa = 0; aa < 3; ++aa) add(I - 1 + aa, J - 1 + bb, sg * (wx[aa] * wy[bb]));
-      } else {
-        double n0 = (px - org0) / h0, n1 = (py - org1) / h1;
-        int I = (int)std::floor(n0), J = (int)std::floor(n1);
-        double a = n0 - I, b = n1 - J;
-        auto p3 = [](double v) { return v * v * v; };
-        double wx[4] = {onesixth * p3(1.0 - a), onesixth * (4.0 - 3.0 * a * a * (2.0 - a)),
-                        onesixth * (4.0 - 3.0 * (1.0 - a) * (1.0 - a) * (1.0 + a)), onesixth * p3(a)};
-        double wy[4] = {onesixth * p3(1.0 - b), onesixth * (4.0 - 3.0 * b * b * (2.0 - b)),
-                        onesixth * (4.0 - 3.0 * (1.0 - b) * (1.0 - b) * (1.0 + b)), onesixth * p3(b)};
-        for (int bb = 0; bb < 4; ++bb)
-          for (int aa = 0; aa < 4; ++aa) add(I - 1 + aa, J - 1 + bb, sg * (qq * wx[aa] * wy[bb]));
-      }
-    }
+    charge_shape(order, x[k], y[k], q[k], 1.0, org0, org1, h0, h1, add);
+    charge_shape(order, ox[k], oy[k], q[k], -1.0, org0, org1, h0, h1, add);
   }
   for (size_t k = 0; k < r.size(); ++k) rho[k] = r[k] / (h0 * h1);
 }
@@ -1350,17 +1514,90 @@ int orc_load(void *h, const double *x, const double *y, const double *px, const 
   };
   perm(s.x); perm(s.y); perm(s.px); perm(s.py); perm(s.q);
   s.ox = s.x; s.oy = s.y;
-  // copyFields static -> window (interior only), then the three exchanges.
-  for (int j = 0; j < s.L1; ++j)
-    for (int i = 0; i < s.L0; ++i) {
-      int si = i + s.P0, sj = j + s.P1;
-      if (si < 0 || sj < 0 || si >= s.b.Nx || sj >= s.b.Ny) continue;
-      s.mEx.at(i, j) = s.Ex.at(si, sj); s.mEy.at(i, j) = s.Ey.at(si, sj);
-      s.mHx.at(i, j) = s.Hx.at(si, sj); s.mHy.at(i, j) = s.Hy.at(si, sj);
-    }
-  exchange(s, 0); exchange(s, 1); exchange(s, 2);
+  copy_to_window(s);
   return 0;
 }
+
+// Initial fields of the loaded bunch (main.cpp:232-248): the three boosted
+// electrostatic solves of PoissonSolver::computeField (PoissonSolver.cpp:85-201)
+// fill Ey, Hz and Ex of the static mesh (fillFields, :441-507), then
+// SCBoundaryCondition::resetOutsideDomain and the window copy.  The first solve
+// starts from zero (the reference starts from a random vector), the others
+// from the shifted previous solution (shiftLHS, :270-303).
+// stats: gamma, then (iterations, relative residual) for each solve.
+int orc_initial_fields(void *h, double tol_first, double tol_rest, int maxit, double *stats) {
+  Sim &s = *(Sim *)h;
+  const size_t n = s.x.size();
+  if (n == 0) return -2;
+  double pm0 = 0.0, pm1 = 0.0;  // Distribution::get_pmean (Distribution.cpp:136-143)
+  for (size_t k = 0; k < n; ++k) { pm0 += s.px[k]; pm1 += s.py[k]; }
+  pm0 /= (double)n; pm1 /= (double)n;
+  const double gamma = std::sqrt((pm0 * pm0 + pm1 * pm1) + 1);
+  PoissonSys p;
+  poisson_setup(s, gamma, p);
+  const int Nx = s.b.Nx, Ny = s.b.Ny;
+  const size_t m = (size_t)Nx * Ny;
+  const double hr0 = s.b.hr0 * gamma, hr1 = s.b.hr1;
+  // positions of the three charge densities
+  std::vector<double> X1(n), Y1(n), X2(n), Y2(n);
+  const double full = (s.dt / 2) * C, back = (-s.dt / 2) * C, mv = -0.5 * hr0 / gamma;
+  for (size_t k = 0; k < n; ++k) {
+    const double r = (double)q_rsqrt((float)(1 + (s.px[k] * s.px[k] + s.py[k] * s.py[k])));
+    X1[k] = s.x[k] + full * s.px[k] * r;
+    Y1[k] = s.y[k] + full * s.py[k] * r;
+    X2[k] = (X1[k] + back * s.px[k] * r) + mv;
+    Y2[k] = (Y1[k] + back * s.py[k] * r) + 0.0;
+  }
+  std::vector<double> b, phi1(m, 0.0), phi2(m), phi3(m);
+  double rr[3];
+  int its[3];
+  poisson_rhs(s, X1, Y1, gamma, b);
+  its[0] = poisson_solve(p, b, phi1, tol_first, maxit, &rr[0]);
+  // shiftLHS(+1): phi(i) + (phi(i+1) - phi(i))
+  for (int j = 0; j < Ny; ++j)
+    for (int i = 0; i < Nx; ++i) {
+      const size_t k = (size_t)j * Nx + i;
+      const double nb = i + 1 < Nx ? phi1[k + 1] : 0.0;
+      phi2[k] = phi1[k] + (1.0 * nb - 1.0 * phi1[k]);
+    }
+  poisson_rhs(s, X2, Y2, gamma, b);
+  its[1] = poisson_solve(p, b, phi2, tol_rest, maxit, &rr[1]);
+  // shiftLHS(-0.5): phi(i) + 0.5 (phi(i-1) - phi(i))
+  for (int j = 0; j < Ny; ++j)
+    for (int i = 0; i < Nx; ++i) {
+      const size_t k = (size_t)j * Nx + i;
+      const double nb = i > 0 ? phi2[k - 1] : 0.0;
+      phi3[k] = phi2[k] + (0.5 * nb - 0.5 * phi2[k]);
+    }
+  poisson_rhs(s, s.x, s.y, gamma, b);
+  its[2] = poisson_solve(p, b, phi3, tol_rest, maxit, &rr[2]);
+  // fillFields: Ey (component 1), Hz (2), Ex (0); the guard beyond the last
+  // row / column holds zero.
+  const double bg = std::sqrt(gamma * gamma - 1);
+  const double hden = 2 * C * MU0 * hr1;
+  for (int j = 0; j < Ny; ++j)
+    for (int i = 0; i < Nx; ++i) {
+      const size_t k = (size_t)j * Nx + i;
+      const double ey0 = gamma * phi1[k] / hr1;
+      const double ey1 = j + 1 < Ny ? gamma * phi1[k + Nx] / hr1 : 0.0;
+      s.Ey.at(i, j) = ey0 - ey1;
+      const double h0v = bg * phi2[k] / hden;
+      const double h1v = j + 1 < Ny ? bg * phi2[k + Nx] / hden : 0.0;
+      s.Hx.at(i, j) = h0v - h1v;
+      s.Hy.at(i, j) = h0v - h1v;
+      const double ex0 = phi3[k] / hr0;
+      const double ex1 = i + 1 < Nx ? phi3[k + 1] / hr0 : 0.0;
+      s.Ex.at(i, j) = ex0 - ex1;
+    }
+  orc_reset_outside(h);
+  copy_to_window(s);
+  if (stats) {
+    stats[0] = gamma;
+    for (int t = 0; t < 3; ++t) { stats[1 + 2 * t] = its[t]; stats[2 + 2 * t] = rr[t]; }
+  }
+  return 0;
+}
+
 
 void orc_get_particles(void *h, double *x, double *y, double *px, double *py) {
   Sim &s = *(Sim *)h;

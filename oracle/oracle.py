@@ -71,6 +71,7 @@ def lib():
         L.orc_step.argtypes = [C.c_void_p, C.c_int]
         L.orc_wake.argtypes = [C.c_void_p] + [C.c_double] * 4 + [D]
         L.orc_moments.argtypes = [C.c_void_p, D]
+        L.orc_initial_fields.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_int, D]
         _LIB = L
     return _LIB
 
@@ -239,3 +240,12 @@ class Sim:
         out = np.zeros(max(w[2] - 4, 0))
         lib().orc_wake(self.h, rmean[0], rmean[1], pmean[0], pmean[1], _p(out))
         return out
+
+    def initial_fields(self, tol_first=1e-12, tol_rest=1e-6, maxit=500):
+        """Boosted electrostatic initial fields of the loaded bunch; returns
+        (gamma, [(iterations, relative residual)] * 3)."""
+        st = np.zeros(7)
+        rc = lib().orc_initial_fields(self.h, tol_first, tol_rest, maxit, _p(st))
+        if rc:
+            raise RuntimeError(f"oracle initial fields error {rc}")
+        return st[0], [(int(st[1 + 2 * k]), st[2 + 2 * k]) for k in range(3)]

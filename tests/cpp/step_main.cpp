@@ -1,5 +1,5 @@
-// C++ caller of the reference-shaped facade: loads a bunch, runs the
-// reference's main-loop body through TETMSolver / moveMesh, and prints the
+// C++ caller of the reference-shaped facade: loads a bunch, solves its
+// initial fields, runs the reference's main-loop body through TETMSolver / moveMesh, and prints the
 // beam centroid.  Built by tests/test_cpp_facade.py.
 #include <cmath>
 #include <cstdio>
@@ -29,6 +29,10 @@ int main(int argc, char **argv) {
       px[i] = std::sqrt(gam * gam - 1);
     }
     sim.loadBunch(x, y, px, py, q);
+    csrst::PoissonSolver poisson(sim);  // initial fields, as main.cpp:232-248
+    poisson.computeField();
+    std::printf("poisson gamma %.6f iterations %g %g %g\n", poisson.report()[0], poisson.report()[1],
+                poisson.report()[3], poisson.report()[5]);
     csrst::TETMSolver solver(sim);
     csrst::PartBunch bunch(sim);
     for (int s = 0; s < steps; ++s) {

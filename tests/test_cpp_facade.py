@@ -1,6 +1,6 @@
 """The C++ facade (include/csrst/csrst.hpp) compiles and links against the C
-ABI; on a GPU it runs the reference's loop body and agrees with the Python
-mirror of the same call sequence."""
+ABI; on a GPU it solves the initial fields, runs the reference's loop body and
+agrees with the Python mirror of the same call sequence."""
 import subprocess
 from pathlib import Path
 
@@ -28,8 +28,11 @@ def test_facade_runs_the_loop(exe):
     from csrst_b200 import Simulation, TETMSolver, moveMesh
     from csrst_b200.workloads import workload
     r = subprocess.run([str(exe), "4"], capture_output=True, text=True, check=True)
-    vals = [float(v) for v in r.stdout.split()[1:3]]
+    lines = {ln.split()[0]: ln.split()[1:] for ln in r.stdout.splitlines()}
+    vals = [float(v) for v in lines["rmean"][:2]]
     assert np.isfinite(vals).all()
+    its = [float(v) for v in lines["poisson"][3:6]]  # iterations of the three initial-field solves
+    assert all(0 < k < 50 for k in its)
     cfg, _ = workload("small-1")
     assert cfg.Nx == 512 and cfg.Ny == 104
     # the Python mirror drives the same ABI entry points

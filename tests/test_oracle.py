@@ -138,3 +138,37 @@ def test_oracle_loop_moves_window(oracle):
     assert w1[2:] == w0[2:]
     x, y, px, py = s.particles()
     assert np.isfinite(x).all() and np.isfinite(px).all()
+
+
+@pytest.mark.parametrize("order", [0, 1, 2])
+def test_oracle_initial_fields(oracle, order):
+    """The oracle's boosted electrostatic solve (PoissonSolver::computeField):
+    converges on the reference's matrix, gives a relativistic field
+    (Ey ~ Z0 Hz), leaves no field beyond the straight section it solves on
+    and zeroes E outside the pipe (resetOutsideDomain)."""
+    from csrst_b200.workloads import make_bunch, workload
+    cfg, spec = workload(f"small-{order}")
+    d = cfg.dict()
+    d["order"] = order
+    s = oracle.Sim(d)
+    s.load(*make_bunch(spec))
+    gamma, solves = s.initial_fields(1e-13, 1e-13, 2000)
+    assert gamma == pytest.approx(1000.0, rel=1e-5)
+    for it, rr in solves:
+        assert rr <= 1e-13 and it < 50
+    ex, ey, hx, hy = s.get_static()
+    assert np.array_equal(hx, hy)                 # fillFields writes both split halves
+    # Hz is solved for the bunch shifted by half a cell, so compare norms
+    assert np.linalg.norm(ey) / np.linalg.norm(hx + hy) == pytest.approx(376.73, rel=0.02)
+    assert np.abs(ex).max() < 1e-3 * np.abs(ey).max()   # longitudinal field suppressed by 1/gamma^2
+    b = oracle.bend(cfg.Nx, cfg.Ny, cfg.length_before, cfg.length_after, cfg.width, cfg.phi_deg,
+                    cfg.ekin_mev, cfg.bz)
+    max_x = int(cfg.length_before / b["hx"])    # Bend::getLengthStraightSection
+    for f in (ex, ey, hx):                       # no charge and no unknowns past the straight section
+        assert not f[:, max_x + 1:].any()
+    inside, cells = oracle.geometry(cfg.Nx, cfg.Ny, cfg.length_before, cfg.length_after, cfg.width,
+                                    cfg.phi_deg, cfg.ekin_mev, cfg.bz)
+    cut = np.zeros_like(inside)
+    cut[cells[:, 1].astype(int), cells[:, 0].astype(int)] = 1
+    outside = (inside == 0) & (cut == 0)
+    assert not ex[outside].any() and not ey[outside].any()
