@@ -135,6 +135,11 @@ def run_b200(args, world, rank, local):
     n = spec.n
     sim = Simulation(cfg)
     sim.load(*bunch)
+    # initial fields of the bunch (PoissonSolver::computeField), one-time set-up
+    # before the loop; timed on its own
+    t_if = time.perf_counter()
+    rep = sim.initial_fields(1e-12, 1e-6, 500)
+    t_if = time.perf_counter() - t_if
     stream = torch.cuda.ExternalStream(sim.stream())
     # clocks are sampled from before the warm-up to the end of the kernel
     # attribution pass: the GPU runs this workload the whole time
@@ -201,7 +206,7 @@ def run_b200(args, world, rank, local):
     out = {"metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world,
            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_step, 4),
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-           "data": "synthetic (seeded Gaussian bunch, zero initial fields)",
+           "data": "synthetic (seeded Gaussian bunch; initial fields from the GPU multigrid Poisson solve)",
            "config": {"workload": f"{args.workload}: {cfg.Nx}x{cfg.Ny} static mesh, h={1e6 * sim.info()['hx']:.3g}um,"
                                   f" {n} particles, shape order {cfg.shape_order}, CFL 0.5, FP64",
                       "Nx": cfg.Nx, "Ny": cfg.Ny, "particles": n, "shape_order": cfg.shape_order,
@@ -211,6 +216,11 @@ def run_b200(args, world, rank, local):
            "cell_updates_per_s": round(world * cells * args.steps / (ms * 1e-3), 1),
            "roofline": dominant, "roofline_other": other,
            "kernel_ms_per_step": {k: round(v, 4) for k, v in groups.items()},
+           "initial_fields": {"ms": round(1e3 * t_if, 2), "levels": rep["levels"],
+                              "iterations": [it for it, _ in rep["solves"]],
+                              "relres": [float("%.3g" % rr) for _, rr in rep["solves"]],
+                              "what": "one-time set-up, not in the timed steps: 3 MG-PCG solves on the "
+                                      f"{cfg.Nx}x{cfg.Ny} mesh incl. charge deposits and host round trips"},
            "clocks": clk}
     # launches per step: 2 pushes x (prep, push, post, bounds) + 4 sub-steps x
     # (sweep, exchange) + move
@@ -255,7 +265,8 @@ def run_e2e(args, cfg, spec, bunch, rank, world):
     sim.close()
     return {"value": round(world * n * k / el, 1), "unit": UNIT,
             "h2d_bytes_per_step": int(5 * 8 * n / k), "d2h_bytes_per_step": int(18 * 8 + 4 * 8 * n / k),
-            "steps": k, "includes": "bunch upload, window set-up and sort, steps, per-step moments, bunch download"}
+            "steps": k, "includes": "bunch upload, window set-up and sort, steps, per-step moments, bunch download "
+                                    "(zero initial fields: the solve is reported under initial_fields)"}
 
 
 def oracle_sample(cfg, spec, bunch, frac, nsteps):

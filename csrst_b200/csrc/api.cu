@@ -96,6 +96,15 @@ struct csrst_handle {
   // graph of one step
   cudaGraphExec_t graph = nullptr;
   std::string err;
+  // FP32 mode (CSRST_FLAG_FP32): FP32 static and window planes, FP32 bunch
+  bool fp32 = false;
+  int pitch32 = 0;
+  float *Exf = nullptr, *Eyf = nullptr, *Hxf = nullptr, *Hyf = nullptr;
+  float *winf = nullptr, *scratchf = nullptr;
+  Bunch32 b32{};
+  double P0 = 0, P1 = 0;      // reference momentum
+  double kh0 = 0, kh1 = 0;    // 0.5 c dt / h
+  double *d64 = nullptr;      // 4 n doubles: the bunch in FP64 for diagnostics and reads
 };
 
 namespace {
@@ -150,6 +159,30 @@ FieldArgs field_args(csrst_handle *h, int comp) {
   return a;
 }
 
+PlaneT<float> wplane32(const csrst_handle *h, int k) {
+  return PlaneT<float>{h->winf + (size_t)k * h->wpitch * (h->L1 + 2), h->wpitch};
+}
+
+// The same sub-step arguments for FP32 mode: FP32 planes, coefficients
+// computed in FP64 and rounded once.
+FieldArgsT<float> field_args32(csrst_handle *h, int comp) {
+  const FieldArgs d = field_args(h, comp);
+  FieldArgsT<float> a{};
+  a.Ex = PlaneT<float>{h->Exf, h->pitch32}; a.Ey = PlaneT<float>{h->Eyf, h->pitch32};
+  a.Hx = PlaneT<float>{h->Hxf, h->pitch32}; a.Hy = PlaneT<float>{h->Hyf, h->pitch32};
+  a.mask = d.mask; a.Nx = d.Nx; a.Ny = d.Ny;
+  if (h->winf) {
+    a.mEx = wplane32(h, 0); a.mEy = wplane32(h, 1); a.mHx = wplane32(h, 2); a.mHy = wplane32(h, 3);
+    a.mJx = wplane32(h, 4); a.mJy = wplane32(h, 5);
+  }
+  a.L0 = d.L0; a.L1 = d.L1; a.cells = d.cells; a.ncells = d.ncells; a.ws = d.ws; a.acc = d.acc;
+  a.acc_inv = d.acc_inv;
+  a.chx = (float)d.chx; a.chy = (float)d.chy; a.kex = (float)d.kex; a.key = (float)d.key;
+  a.dteps = (float)d.dteps; a.mhx = (float)d.mhx; a.mhy = (float)d.mhy; a.de = (float)d.de;
+  a.h0 = (float)d.h0; a.h1 = (float)d.h1;
+  return a;
+}
+
 // Host copy of the Bend set-up (Bend ctor and Bend::Init, Bend.cpp:60-124).
 void bend_setup(csrst_handle *h) {
   const csrst_config &c = h->cfg;
@@ -196,6 +229,11 @@ void free_particles(csrst_handle *h) {
   h->x = h->y = h->px = h->py = h->q = h->ox = h->oy = nullptr;
   cudaFree(h->win); cudaFree(h->scratch); cudaFree(h->acc);
   h->win = h->scratch = nullptr; h->acc = nullptr;
+  cudaFree(h->b32.cell); cudaFree(h->b32.ox); cudaFree(h->b32.oy); cudaFree(h->b32.dpx); cudaFree(h->b32.dpy);
+  cudaFree(h->b32.q); cudaFree(h->winf); cudaFree(h->scratchf); cudaFree(h->d64);
+  h->b32 = Bunch32{};
+  h->winf = h->scratchf = nullptr;
+  h->d64 = nullptr;
   if (h->graph) { cudaGraphExecDestroy(h->graph); h->graph = nullptr; }
   h->n = 0;
 }
@@ -235,10 +273,43 @@ PushArgs push_args(csrst_handle *h, int jcomp) {
   return a;
 }
 
+Push32Args push_args32(csrst_handle *h, int jcomp) {
+  Push32Args a{};
+  a.b = h->b32;
+  a.ws = h->ws;
+  a.mEx = wplane32(h, 0).p; a.mEy = wplane32(h, 1).p; a.mHx = wplane32(h, 2).p; a.mHy = wplane32(h, 3).p;
+  a.wpitch = h->wpitch;
+  a.acc = h->acc + (size_t)jcomp * h->L0 * h->L1;
+  a.acc_scale = h->acc_scale;
+  a.jcomp = jcomp;
+  a.pending = h->pending ? 1 : 0;
+  a.P0 = h->P0; a.P1 = h->P1;
+  a.kh0 = h->kh0; a.kh1 = h->kh1;
+  const double fact1 = h->half * h->cfg.charge_mass;
+  a.f1 = (float)fact1; a.f2 = (float)(fact1 * kC);
+  a.h0 = h->b.hr0; a.h1 = h->b.hr1; a.dt = h->dt;
+  a.org0 = h->b.org0; a.org1 = h->b.org1;
+  a.bz = h->cfg.bz; a.Lb = h->b.Lb; a.hw = 0.5 * h->b.w;
+  a.chh = h->chh; a.shh = h->shh; a.bwidth = h->bwidth;
+  a.use_smem = 1;
+  return a;
+}
+
 // PartBunch::push_particles on the device (no host synchronisation).
 int push_async(csrst_handle *h, int jcomp) {
   const bool bb_ok = h->bb == kBBValid || (h->bb == kBBValidIfPending && h->pending);
-  if (h->cfg.flags & 1) {  // keep oldR for inspection
+  if (h->fp32) {
+    if (!bb_ok) launch_bbox32(h->b32, h->P0, h->P1, h->kh0, h->kh1, h->pending ? 1 : 0, h->ws, h->s);
+    launch_prep32(h->ws, h->order, h->s);
+    launch_push32(push_args32(h, jcomp), h->order, h->L0, h->L1, h->push_grid, h->s);
+    launch_bounds32(h->ws, h->s);
+    h->pending = false;
+    h->fresh = false;
+    h->bb = kBBValidIfPending;
+    h->acc_fresh[jcomp] = true;
+    return CSRST_OK;
+  }
+  if (h->cfg.flags & CSRST_FLAG_KEEP_OLD) {  // keep oldR for inspection
     k_set_pending_old<<<(unsigned)((h->n + 255) / 256), 256, 0, h->s>>>(h->x, h->y, h->px, h->py, h->n,
                                                                        h->half, h->pending, h->ox, h->oy);
   }
@@ -253,10 +324,17 @@ int push_async(csrst_handle *h, int jcomp) {
   return CSRST_OK;
 }
 
+void drift_now(csrst_handle *h, double dt) {
+  if (h->fp32)
+    launch_drift32(h->b32, h->P0, h->P1, dt * kC / h->b.hr0, dt * kC / h->b.hr1, h->s);
+  else
+    launch_drift(h->x, h->y, h->px, h->py, h->n, dt * kC, h->s);
+}
+
 // drift(-dt/2) right after a push: defer it into the next push.
 void drift_back(csrst_handle *h) {
   if (h->pending) {  // materialise the older one first
-    launch_drift(h->x, h->y, h->px, h->py, h->n, (-0.5 * h->dt) * kC, h->s);
+    drift_now(h, -0.5 * h->dt);
     h->bb = kBBInvalid;
   }
   h->pending = true;
@@ -265,27 +343,75 @@ void drift_back(csrst_handle *h) {
 
 void materialise(csrst_handle *h) {
   if (!h->pending) return;
-  launch_drift(h->x, h->y, h->px, h->py, h->n, (-0.5 * h->dt) * kC, h->s);
+  drift_now(h, -0.5 * h->dt);
   h->pending = false;
+  if (h->fp32) h->bb = kBBInvalid;
   // the stored box of the next gather positions stays exact: R_true + h v(P)
   // has the same bits whether the drift was deferred or applied
 }
 
 void half_h_async(csrst_handle *h) {
+  if (h->fp32) {
+    FieldArgsT<float> a = field_args32(h, 0);
+    launch_half_h(a, h->s);
+    launch_exchange(a, 0, h->s);
+    return;
+  }
   FieldArgs a = field_args(h, 0);
   launch_half_h(a, h->s);
   launch_exchange(a, 0, h->s);
 }
 
 void update_e_async(csrst_handle *h, int comp) {
-  FieldArgs a = field_args(h, comp);
-  launch_update_e(a, comp, h->s);
-  launch_exchange(a, comp == 0 ? 1 : 2, h->s);
+  if (h->fp32) {
+    FieldArgsT<float> a = field_args32(h, comp);
+    launch_update_e(a, comp, h->s);
+    launch_exchange(a, comp == 0 ? 1 : 2, h->s);
+  } else {
+    FieldArgs a = field_args(h, comp);
+    launch_update_e(a, comp, h->s);
+    launch_exchange(a, comp == 0 ? 1 : 2, h->s);
+  }
   h->acc_fresh[comp] = false;
 }
 
 void move_async(csrst_handle *h) {
-  launch_move(field_args(h, 0), h->scratch, h->b.hr0, h->b.hr1, h->s);
+  if (h->fp32) launch_move(field_args32(h, 0), h->scratchf, h->b.hr0, h->b.hr1, h->s);
+  else launch_move(field_args(h, 0), h->scratch, h->b.hr0, h->b.hr1, h->s);
+}
+
+// Window fill from the static mesh (copyFields + exchangeBoundaries,
+// main.cpp:335-342) and the window-wall check.
+void fill_window(csrst_handle *h) {
+  if (h->fp32) {
+    FieldArgsT<float> fa = field_args32(h, 0);
+    launch_copy_to_window(fa, h->s);
+    launch_exchange(fa, 0, h->s);
+    launch_exchange(fa, 1, h->s);
+    launch_exchange(fa, 2, h->s);
+    launch_check_window(fa, h->s);
+  } else {
+    FieldArgs fa = field_args(h, 0);
+    launch_copy_to_window(fa, h->s);
+    launch_exchange(fa, 0, h->s);
+    launch_exchange(fa, 1, h->s);
+    launch_exchange(fa, 2, h->s);
+    launch_check_window(fa, h->s);
+  }
+}
+
+// The bunch as FP64 arrays (positions with any pending drift applied):
+// the FP64 path's own arrays, or FP32 mode's converted into d64.
+void bunch64(csrst_handle *h, const double **x, const double **y, const double **px, const double **py,
+             int *pending) {
+  if (!h->fp32) {
+    *x = h->x; *y = h->y; *px = h->px; *py = h->py; *pending = h->pending ? 1 : 0;
+    return;
+  }
+  const size_t n = (size_t)h->n;
+  launch_to64(h->b32, h->P0, h->P1, h->kh0, h->kh1, h->pending ? 1 : 0, h->b.org0, h->b.org1, h->b.hr0,
+              h->b.hr1, h->d64, h->d64 + n, h->d64 + 2 * n, h->d64 + 3 * n, h->s);
+  *x = h->d64; *y = h->d64 + n; *px = h->d64 + 2 * n; *py = h->d64 + 3 * n; *pending = 0;
 }
 
 // TETMSolver::updateField_firstStep + updateField_secondStep + moveMesh.
@@ -303,7 +429,7 @@ void step_async(csrst_handle *h) {
 
 int need_bunch(csrst_handle *h) {
   if (!h) return CSRST_E_ARG;
-  if (h->n <= 0 || !h->win) return fail(h, CSRST_E_NO_PARTICLES, "no bunch loaded");
+  if (h->n <= 0 || !(h->win || h->winf)) return fail(h, CSRST_E_NO_PARTICLES, "no bunch loaded");
   return CSRST_OK;
 }
 
@@ -316,13 +442,21 @@ int csrst_create(const csrst_config *cfg, csrst_handle **out) {
   *out = nullptr;
   if (cfg->Nx < 8 || cfg->Ny < 8 || cfg->shape_order < 0 || cfg->shape_order > 2 || !(cfg->width > 0))
     return fail(nullptr, CSRST_E_ARG, "invalid configuration");
+  if (cfg->flags & ~(CSRST_FLAG_KEEP_OLD | CSRST_FLAG_FP32)) return fail(nullptr, CSRST_E_ARG, "unknown flags");
+  if ((cfg->flags & CSRST_FLAG_FP32) && (cfg->flags & CSRST_FLAG_KEEP_OLD))
+    return fail(nullptr, CSRST_E_ARG, "CSRST_FLAG_KEEP_OLD is an FP64-path option");
+  if ((cfg->flags & CSRST_FLAG_FP32) && (cfg->Nx > 32767 || cfg->Ny > 32767))
+    return fail(nullptr, CSRST_E_ARG, "FP32 mode packs cell indices in 16 bits: Nx, Ny <= 32767");
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
     return fail(nullptr, CSRST_E_CUDA, "no CUDA device");
   csrst_handle *h = new csrst_handle;
   h->cfg = *cfg;
   h->order = cfg->shape_order;
+  h->fp32 = (cfg->flags & CSRST_FLAG_FP32) != 0;
   bend_setup(h);
+  h->kh0 = h->half / h->b.hr0;
+  h->kh1 = h->half / h->b.hr1;
   auto bad = [&](cudaError_t e, const char *w) {
     g_create_error = std::string(w) + ": " + cudaGetErrorString(e);
     csrst_destroy(h);
@@ -333,10 +467,20 @@ int csrst_create(const csrst_config *cfg, csrst_handle **out) {
   const int Nx = cfg->Nx, Ny = cfg->Ny;
   h->pitch = ((Nx + 2 + 31) / 32) * 32;
   const size_t ps = (size_t)h->pitch * (Ny + 2);
-  double **planes[4] = {&h->Ex, &h->Ey, &h->Hx, &h->Hy};
-  for (double **p : planes) {
-    if ((e = cudaMalloc(p, ps * sizeof(double))) != cudaSuccess) return bad(e, "static fields");
-    if ((e = cudaMemsetAsync(*p, 0, ps * sizeof(double), h->s)) != cudaSuccess) return bad(e, "memset");
+  if (h->fp32) {  // FP32 static planes only; FP64 copies are made on demand
+    h->pitch32 = ((Nx + 2 + 63) / 64) * 64;
+    const size_t ps32 = (size_t)h->pitch32 * (Ny + 2);
+    float **planes[4] = {&h->Exf, &h->Eyf, &h->Hxf, &h->Hyf};
+    for (float **p : planes) {
+      if ((e = cudaMalloc(p, ps32 * sizeof(float))) != cudaSuccess) return bad(e, "static fields");
+      if ((e = cudaMemsetAsync(*p, 0, ps32 * sizeof(float), h->s)) != cudaSuccess) return bad(e, "memset");
+    }
+  } else {
+    double **planes[4] = {&h->Ex, &h->Ey, &h->Hx, &h->Hy};
+    for (double **p : planes) {
+      if ((e = cudaMalloc(p, ps * sizeof(double))) != cudaSuccess) return bad(e, "static fields");
+      if ((e = cudaMemsetAsync(*p, 0, ps * sizeof(double), h->s)) != cudaSuccess) return bad(e, "memset");
+    }
   }
   if ((e = cudaMalloc(&h->mask, (size_t)Nx * Ny)) != cudaSuccess) return bad(e, "mask");
   if ((e = cudaMalloc(&h->ws, sizeof(WinState))) != cudaSuccess) return bad(e, "window state");
@@ -365,6 +509,7 @@ int csrst_destroy(csrst_handle *h) {
   if (h->s) cudaStreamSynchronize(h->s);
   free_particles(h);
   cudaFree(h->Ex); cudaFree(h->Ey); cudaFree(h->Hx); cudaFree(h->Hy);
+  cudaFree(h->Exf); cudaFree(h->Eyf); cudaFree(h->Hxf); cudaFree(h->Hyf);
   cudaFree(h->mask); cudaFree(h->cells); cudaFree(h->cutidx); cudaFree(h->ws);
   cudaFree(h->dscratch); cudaFree(h->dmean); cudaFree(h->dout);
   if (h->s) cudaStreamDestroy(h->s);
@@ -416,6 +561,21 @@ int csrst_get_geometry(csrst_handle *h, uint8_t *inside, double *cells, long max
 int csrst_set_static_fields(csrst_handle *h, const double *ex, const double *ey, const double *hzx,
                             const double *hzy) {
   if (!h) return CSRST_E_ARG;
+  if (h->fp32) {  // through an FP64 staging buffer, rounded once on the device
+    const double *src[4] = {ex, ey, hzx, hzy};
+    float *dst[4] = {h->Exf, h->Eyf, h->Hxf, h->Hyf};
+    double *tmp = nullptr;
+    CK(cudaMalloc(&tmp, (size_t)h->b.Nx * h->b.Ny * sizeof(double)));
+    for (int k = 0; k < 4; ++k) {
+      if (!src[k]) continue;
+      CK(cudaMemcpyAsync(tmp, src[k], (size_t)h->b.Nx * h->b.Ny * sizeof(double), cudaMemcpyHostToDevice, h->s));
+      launch_d2f(tmp, h->b.Nx, dst[k] + h->pitch32 + 1, h->pitch32, h->b.Ny, h->b.Nx, h->s);
+    }
+    CK(cudaStreamSynchronize(h->s));
+    cudaFree(tmp);
+    CK(cudaGetLastError());
+    return CSRST_OK;
+  }
   const double *src[4] = {ex, ey, hzx, hzy};
   double *dst[4] = {h->Ex, h->Ey, h->Hx, h->Hy};
   for (int k = 0; k < 4; ++k) {
@@ -429,6 +589,21 @@ int csrst_set_static_fields(csrst_handle *h, const double *ex, const double *ey,
 
 int csrst_get_static_fields(csrst_handle *h, double *ex, double *ey, double *hzx, double *hzy) {
   if (!h) return CSRST_E_ARG;
+  if (h->fp32) {
+    double *dst[4] = {ex, ey, hzx, hzy};
+    const float *src[4] = {h->Exf, h->Eyf, h->Hxf, h->Hyf};
+    double *tmp = nullptr;
+    CK(cudaMalloc(&tmp, (size_t)h->b.Nx * h->b.Ny * sizeof(double)));
+    for (int k = 0; k < 4; ++k) {
+      if (!dst[k]) continue;
+      launch_f2d(src[k] + h->pitch32 + 1, h->pitch32, tmp, h->b.Nx, h->b.Ny, h->b.Nx, h->s);
+      CK(cudaMemcpyAsync(dst[k], tmp, (size_t)h->b.Nx * h->b.Ny * sizeof(double), cudaMemcpyDeviceToHost, h->s));
+      CK(cudaStreamSynchronize(h->s));
+    }
+    cudaFree(tmp);
+    CK(cudaGetLastError());
+    return CSRST_OK;
+  }
   double *dst[4] = {ex, ey, hzx, hzy};
   const double *src[4] = {h->Ex, h->Ey, h->Hx, h->Hy};
   for (int k = 0; k < 4; ++k) {
@@ -442,7 +617,8 @@ int csrst_get_static_fields(csrst_handle *h, double *ex, double *ey, double *hzx
 
 int csrst_reset_outside(csrst_handle *h) {
   if (!h) return CSRST_E_ARG;
-  launch_reset_outside(field_args(h, 0), h->cutidx, h->s);
+  if (h->fp32) launch_reset_outside(field_args32(h, 0), h->cutidx, h->s);
+  else launch_reset_outside(field_args(h, 0), h->cutidx, h->s);
   CK(cudaStreamSynchronize(h->s));
   return CSRST_OK;
 }
@@ -457,6 +633,11 @@ int csrst_load_particles(csrst_handle *h, const double *x, const double *y, cons
         !std::isfinite(q[i]))
       return fail(h, CSRST_E_ARG, "non-finite particle data at index " + std::to_string(i));
     qmax = std::fmax(qmax, std::fabs(q[i]));
+    if (h->fp32) {  // FP32 mode stores 16-bit cell indices of the static mesh
+      const double a = (x[i] - h->b.org0) / h->b.hr0, b = (y[i] - h->b.org1) / h->b.hr1;
+      if (!(a >= 0 && a < h->b.Nx && b >= 0 && b < h->b.Ny))
+        return fail(h, CSRST_E_ARG, "particle outside the static mesh at index " + std::to_string(i));
+    }
   }
   CK(cudaStreamSynchronize(h->s));
   free_particles(h);
@@ -488,9 +669,15 @@ int csrst_load_particles(csrst_handle *h, const double *x, const double *y, cons
   w0.bb[0][0] = bb[0]; w0.bb[0][1] = bb[1]; w0.bb[0][2] = bb[2]; w0.bb[0][3] = bb[3];
   CK(cudaMemcpyAsync(h->ws, &w0, sizeof(WinState), cudaMemcpyHostToDevice, h->s));
   const size_t wp = (size_t)h->wpitch * (h->L1 + 2);
-  CK(cudaMalloc(&h->win, 6 * wp * sizeof(double)));
-  CK(cudaMemsetAsync(h->win, 0, 6 * wp * sizeof(double), h->s));
-  CK(cudaMalloc(&h->scratch, 6 * wp * sizeof(double)));
+  if (h->fp32) {
+    CK(cudaMalloc(&h->winf, 6 * wp * sizeof(float)));
+    CK(cudaMemsetAsync(h->winf, 0, 6 * wp * sizeof(float), h->s));
+    CK(cudaMalloc(&h->scratchf, 6 * wp * sizeof(float)));
+  } else {
+    CK(cudaMalloc(&h->win, 6 * wp * sizeof(double)));
+    CK(cudaMemsetAsync(h->win, 0, 6 * wp * sizeof(double), h->s));
+    CK(cudaMalloc(&h->scratch, 6 * wp * sizeof(double)));
+  }
   CK(cudaMalloc(&h->acc, 2 * (size_t)h->L0 * h->L1 * sizeof(unsigned long long)));
   CK(cudaMemsetAsync(h->acc, 0, 2 * (size_t)h->L0 * h->L1 * sizeof(unsigned long long), h->s));
   // PartBunch::sortParticles: y slice of the window, then x (stable radix sorts)
@@ -524,16 +711,33 @@ int csrst_load_particles(csrst_handle *h, const double *x, const double *y, cons
   const double bound = 4.0 * (double)n * (qmax > 0 ? qmax : 1e-30) * kC / (h->b.hr0 * h->b.hr1);
   h->acc_scale = std::ldexp(1.0, (int)std::floor(std::log2(std::ldexp(1.0, 62) / bound)));
   // window fill (copyFields + exchangeBoundaries, main.cpp:335-342)
-  FieldArgs fa = field_args(h, 0);
-  launch_copy_to_window(fa, h->s);
-  launch_exchange(fa, 0, h->s);
-  launch_exchange(fa, 1, h->s);
-  launch_exchange(fa, 2, h->s);
-  launch_check_window(fa, h->s);
+  fill_window(h);
   h->pending = false;
   h->bb = kBBInvalid;
   h->acc_fresh[0] = h->acc_fresh[1] = false;
-  launch_bbox_next(h->x, h->y, h->px, h->py, N, h->half, 0, h->ws, h->s);
+  if (h->fp32) {
+    // reference momentum = mean momentum; then the FP32 bunch replaces the FP64 arrays
+    double *part = nullptr, sums[2];
+    CK(cudaMalloc(&part, (2 * 296 + 2) * sizeof(double)));
+    launch_psum(h->px, h->py, N, part, part + 2 * 296, h->s);
+    CK(cudaMemcpyAsync(sums, part + 2 * 296, sizeof(sums), cudaMemcpyDeviceToHost, h->s));
+    CK(cudaStreamSynchronize(h->s));
+    cudaFree(part);
+    h->P0 = sums[0] / (double)N;
+    h->P1 = sums[1] / (double)N;
+    Bunch32 &b = h->b32;
+    b.n = N;
+    CK(cudaMalloc(&b.cell, n * sizeof(int)));
+    for (float **p : {&b.ox, &b.oy, &b.dpx, &b.dpy, &b.q}) CK(cudaMalloc(p, n * sizeof(float)));
+    CK(cudaMalloc(&h->d64, 4 * nb));
+    launch_from64(h->x, h->y, h->px, h->py, h->q, N, h->b.org0, h->b.org1, h->b.hr0, h->b.hr1, h->P0, h->P1, b,
+                  h->s);
+    CK(cudaStreamSynchronize(h->s));
+    for (double **p : {&h->x, &h->y, &h->px, &h->py, &h->q, &h->ox, &h->oy}) { cudaFree(*p); *p = nullptr; }
+    launch_bbox32(b, h->P0, h->P1, h->kh0, h->kh1, 0, h->ws, h->s);
+  } else {
+    launch_bbox_next(h->x, h->y, h->px, h->py, N, h->half, 0, h->ws, h->s);
+  }
   h->bb = kBBValid;
   h->fresh = true;
   CK(cudaStreamSynchronize(h->s));
@@ -547,24 +751,46 @@ int csrst_initial_fields(csrst_handle *h, double tol_first, double tol_rest, int
   if (!h->fresh) return fail(h, CSRST_E_ARG, "initial fields need a freshly loaded bunch (before the first push)");
   if (!(tol_first > 0) || !(tol_rest > 0) || max_iter < 1) return fail(h, CSRST_E_ARG, "invalid tolerance");
   PoissonInput in{};
-  in.x = h->x; in.y = h->y; in.px = h->px; in.py = h->py; in.q = h->q; in.n = h->n;
+  in.n = h->n;
   in.order = h->order;
   in.mask = h->mask; in.cutidx = h->cutidx; in.cells = h->cells;
   in.b = h->b; in.dt = h->dt;
-  in.Ex = plane(h->Ex, h->pitch); in.Ey = plane(h->Ey, h->pitch);
-  in.Hx = plane(h->Hx, h->pitch); in.Hy = plane(h->Hy, h->pitch);
   in.tol_first = tol_first; in.tol_rest = tol_rest; in.maxit = max_iter;
+  // FP32 mode solves in FP64 (the bunch converted, the planes staged) and
+  // rounds the fields once
+  double *qd = nullptr, *stage = nullptr;
+  const size_t ps = (size_t)h->pitch * (h->b.Ny + 2);
+  if (h->fp32) {
+    int pend = 0;
+    bunch64(h, &in.x, &in.y, &in.px, &in.py, &pend);
+    CK(cudaMalloc(&qd, (size_t)h->n * sizeof(double)));
+    launch_f2d(h->b32.q, (int)h->n, qd, (int)h->n, 1, (int)h->n, h->s);
+    in.q = qd;
+    CK(cudaMalloc(&stage, 4 * ps * sizeof(double)));
+    CK(cudaMemsetAsync(stage, 0, 4 * ps * sizeof(double), h->s));
+    in.Ex = plane(stage, h->pitch); in.Ey = plane(stage + ps, h->pitch);
+    in.Hx = plane(stage + 2 * ps, h->pitch); in.Hy = plane(stage + 3 * ps, h->pitch);
+  } else {
+    in.x = h->x; in.y = h->y; in.px = h->px; in.py = h->py; in.q = h->q;
+    in.Ex = plane(h->Ex, h->pitch); in.Ey = plane(h->Ey, h->pitch);
+    in.Hx = plane(h->Hx, h->pitch); in.Hy = plane(h->Hy, h->pitch);
+  }
   PoissonReport rep{};
   std::string msg;
   rc = poisson_initial_fields(in, &rep, h->s, &msg);
+  if (h->fp32 && rc == kOk) {
+    float *dst[4] = {h->Exf, h->Eyf, h->Hxf, h->Hyf};
+    for (int k = 0; k < 4; ++k)
+      launch_d2f(stage + k * ps, h->pitch, dst[k], h->pitch32, h->b.Ny + 2, h->b.Nx + 2, h->s);
+    cudaStreamSynchronize(h->s);
+  }
+  cudaFree(qd);
+  cudaFree(stage);
   if (rc) return fail(h, rc == kErrCuda ? CSRST_E_CUDA : CSRST_E_ARG, "initial fields: " + msg);
   // resetOutsideDomain, then copyFields + exchangeBoundaries (main.cpp:248, :335-342)
-  FieldArgs fa = field_args(h, 0);
-  launch_reset_outside(fa, h->cutidx, h->s);
-  launch_copy_to_window(fa, h->s);
-  launch_exchange(fa, 0, h->s);
-  launch_exchange(fa, 1, h->s);
-  launch_exchange(fa, 2, h->s);
+  if (h->fp32) launch_reset_outside(field_args32(h, 0), h->cutidx, h->s);
+  else launch_reset_outside(field_args(h, 0), h->cutidx, h->s);
+  fill_window(h);
   CK(cudaStreamSynchronize(h->s));
   CK(cudaGetLastError());
   if (report8) {
@@ -578,6 +804,16 @@ int csrst_initial_fields(csrst_handle *h, double tol_first, double tol_rest, int
 int csrst_get_particles(csrst_handle *h, double *x, double *y, double *px, double *py) {
   int rc = need_bunch(h);
   if (rc) return rc;
+  if (h->fp32) {  // cell origin + offset and P + deviation, formed in FP64
+    const double *src[4];
+    int pend = 0;
+    bunch64(h, &src[0], &src[1], &src[2], &src[3], &pend);
+    double *dst[4] = {x, y, px, py};
+    for (int k = 0; k < 4; ++k)
+      if (dst[k]) CK(cudaMemcpyAsync(dst[k], src[k], (size_t)h->n * sizeof(double), cudaMemcpyDeviceToHost, h->s));
+    CK(cudaStreamSynchronize(h->s));
+    return check_err(h);
+  }
   materialise(h);
   const size_t nb = (size_t)h->n * sizeof(double);
   if (x) CK(cudaMemcpyAsync(x, h->x, nb, cudaMemcpyDeviceToHost, h->s));
@@ -591,7 +827,8 @@ int csrst_get_particles(csrst_handle *h, double *x, double *y, double *px, doubl
 int csrst_get_old_positions(csrst_handle *h, double *ox, double *oy) {
   int rc = need_bunch(h);
   if (rc) return rc;
-  if (!(h->cfg.flags & 1)) return fail(h, CSRST_E_ARG, "create the handle with flags & 1 to keep oldR");
+  if (!(h->cfg.flags & CSRST_FLAG_KEEP_OLD))
+    return fail(h, CSRST_E_ARG, "create the handle with CSRST_FLAG_KEEP_OLD to keep oldR");
   const size_t nb = (size_t)h->n * sizeof(double);
   if (ox) CK(cudaMemcpyAsync(ox, h->ox, nb, cudaMemcpyDeviceToHost, h->s));
   if (oy) CK(cudaMemcpyAsync(oy, h->oy, nb, cudaMemcpyDeviceToHost, h->s));
@@ -615,6 +852,24 @@ int csrst_get_window_field(csrst_handle *h, int which, double *out) {
   int rc = need_bunch(h);
   if (rc) return rc;
   if (which < 0 || which > 5 || !out) return fail(h, CSRST_E_ARG, "which must be 0..5");
+  if (h->fp32) {
+    const size_t wp = (size_t)h->wpitch * (h->L1 + 2);
+    double *tmp = nullptr;
+    CK(cudaMalloc(&tmp, wp * sizeof(double)));
+    if (which >= 4 && h->acc_fresh[which - 4]) {  // the current before its FP32 rounding
+      CK(cudaMemsetAsync(tmp, 0, wp * sizeof(double), h->s));
+      const int c = which - 4;
+      k_acc_to_plane<<<(h->L0 * h->L1 + 255) / 256, 256, 0, h->s>>>(h->acc + (size_t)c * h->L0 * h->L1,
+                                                                  Plane{tmp, h->wpitch}, h->L0, h->L1,
+                                                                  1.0 / h->acc_scale);
+    } else {
+      launch_f2d(h->winf + (size_t)which * wp, (int)wp, tmp, (int)wp, 1, (int)wp, h->s);
+    }
+    CK(cudaMemcpyAsync(out, tmp, wp * sizeof(double), cudaMemcpyDeviceToHost, h->s));
+    CK(cudaStreamSynchronize(h->s));
+    cudaFree(tmp);
+    return CSRST_OK;
+  }
   if (which >= 4 && h->acc_fresh[which - 4]) {
     const int c = which - 4;
     k_acc_to_plane<<<(h->L0 * h->L1 + 255) / 256, 256, 0, h->s>>>(h->acc + (size_t)c * h->L0 * h->L1,
@@ -643,7 +898,7 @@ int csrst_drift(csrst_handle *h, double dt) {
     return CSRST_OK;
   }
   materialise(h);
-  launch_drift(h->x, h->y, h->px, h->py, h->n, dt * kC, h->s);
+  drift_now(h, dt);
   h->bb = kBBInvalid;
   return CSRST_OK;
 }
@@ -721,7 +976,10 @@ int csrst_diag_moments(csrst_handle *h, double *out18) {
   int rc = need_bunch(h);
   if (rc) return rc;
   if (!out18) return CSRST_E_ARG;
-  launch_moments(h->x, h->y, h->px, h->py, h->n, h->half, h->pending, h->dscratch, h->dmean, h->dout, h->s);
+  const double *x, *y, *px, *py;
+  int pend = 0;
+  bunch64(h, &x, &y, &px, &py, &pend);
+  launch_moments(x, y, px, py, h->n, h->half, pend, h->dscratch, h->dmean, h->dout, h->s);
   CK(cudaMemcpyAsync(out18, h->dout, 18 * sizeof(double), cudaMemcpyDeviceToHost, h->s));
   CK(cudaStreamSynchronize(h->s));
   return check_err(h);
@@ -731,10 +989,17 @@ int csrst_diag_wake(csrst_handle *h, double *out, int n) {
   int rc = need_bunch(h);
   if (rc) return rc;
   if (!out || n != h->L0 - 4) return fail(h, CSRST_E_ARG, "wake buffer must hold L0 - 4 values");
-  launch_moments(h->x, h->y, h->px, h->py, h->n, h->half, h->pending, h->dscratch, h->dmean, h->dout, h->s);
+  const double *x, *y, *px, *py;
+  int pend = 0;
+  bunch64(h, &x, &y, &px, &py, &pend);
+  launch_moments(x, y, px, py, h->n, h->half, pend, h->dscratch, h->dmean, h->dout, h->s);
   double *d = nullptr;
   CK(cudaMallocAsync(&d, (size_t)n * sizeof(double), h->s));
-  launch_wake(h->ws, wplane(h, 0).p, wplane(h, 1).p, h->wpitch, h->L0, h->b.hr0, h->b.hr1, h->dmean, d, h->s);
+  if (h->fp32)
+    launch_wake(h->ws, wplane32(h, 0).p, wplane32(h, 1).p, h->wpitch, h->L0, h->b.hr0, h->b.hr1, h->dmean, d,
+                h->s);
+  else
+    launch_wake(h->ws, wplane(h, 0).p, wplane(h, 1).p, h->wpitch, h->L0, h->b.hr0, h->b.hr1, h->dmean, d, h->s);
   CK(cudaMemcpyAsync(out, d, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, h->s));
   CK(cudaFreeAsync(d, h->s));
   CK(cudaStreamSynchronize(h->s));

@@ -1,10 +1,10 @@
-// Shared device definitions for the CSRST B200 kernels (FP64 path).
+// Shared device definitions for the CSRST B200 kernels.
 //
-// Layout in HBM.  Every field component is its own plane of doubles with a
-// one-cell guard ring: element (i, j), i in [-1, nx], j in [-1, ny], sits at
-// (j + 1) * pitch + (i + 1), x fastest.  The static mesh pads the pitch to a
-// multiple of 32 doubles (256 B) so every row starts on a cache-line
-// boundary; the moving window uses pitch = L0 + 2.
+// Layout in HBM.  Every field component is its own plane (doubles on the FP64
+// path, floats in FP32 mode) with a one-cell guard ring: element (i, j),
+// i in [-1, nx], j in [-1, ny], sits at (j + 1) * pitch + (i + 1), x fastest.
+// The static mesh pads the pitch so every row starts on a 256-byte boundary;
+// the moving window uses pitch = L0 + 2.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -33,11 +33,13 @@ enum : int {
   kErrWindowWall = -8,
 };
 
-struct Plane {
-  double *p;
+template <class T>
+struct PlaneT {
+  T *p;
   int pitch;
-  __host__ __device__ double &at(int i, int j) const { return p[(size_t)(j + 1) * pitch + (i + 1)]; }
+  __host__ __device__ T &at(int i, int j) const { return p[(size_t)(j + 1) * pitch + (i + 1)]; }
 };
+using Plane = PlaneT<double>;
 
 // Window state that lives on the device so that a whole time step can be
 // captured in a CUDA graph: the host never needs the window position.

@@ -141,8 +141,16 @@ __global__ void k_mom_final2(const double *part, int nb, long long n, const doub
 // momentum direction through the centroid; NaN where the sample's cell lies
 // outside the window.  The samples use the CIC edge gather of
 // ScatterGatherImpl on the window.
-__global__ void k_wake(const WinState *ws, const double *mEx, const double *mEy, int wpitch,
-                       double h0, double h1, const double *mean, double *out) {
+template <class T>
+struct WakeView {
+  const T *base;
+  int pitch;
+  __device__ __forceinline__ double operator()(int i, int j) const { return (double)base[(ptrdiff_t)j * pitch + i]; }
+};
+
+template <class T>
+__global__ void k_wake(const WinState *ws, const T *mEx, const T *mEy, int wpitch, double h0, double h1,
+                       const double *mean, double *out) {
   const int L0 = ws->L0, L1 = ws->L1;
   const int i = 2 + blockIdx.x * blockDim.x + threadIdx.x;
   if (i > L0 - 3) return;
@@ -155,7 +163,7 @@ __global__ void k_wake(const WinState *ws, const double *mEx, const double *mEy,
   const double a1 = -sP * l0 + cP * 0.0 + r1;
   const int ci = (int)floor((a0 - mo0) / h0), cj = (int)floor((a1 - mo1) / h1);
   if (ci < 0 || cj < 0 || ci >= L0 || cj >= L1) { out[i - 2] = NAN; return; }
-  const PatchView pex{mEx + wpitch + 1, wpitch}, pey{mEy + wpitch + 1, wpitch};
+  const WakeView<T> pex{mEx + wpitch + 1, wpitch}, pey{mEy + wpitch + 1, wpitch};
   const double pp0 = (a0 - mo0) * (1.0 / h0), pp1 = (a1 - mo1) * (1.0 / h1);
   const double e0 = gather_edge<0>(pex, pp0, pp1, 0), e1 = gather_edge<0>(pey, pp0, pp1, 1);
   out[i - 2] = cP * e0 + sP * e1;
@@ -196,12 +204,17 @@ void launch_moments(const double *x, const double *y, const double *px, const do
 
 size_t moments_scratch_doubles() { return (size_t)kDiagBlocks * 10; }
 
-void launch_wake(const WinState *ws, const double *mEx, const double *mEy, int wpitch, int L0, double h0,
-                 double h1, const double *mean, double *out, cudaStream_t s) {
+template <class T>
+void launch_wake(const WinState *ws, const T *mEx, const T *mEy, int wpitch, int L0, double h0, double h1,
+                 const double *mean, double *out, cudaStream_t s) {
   const int n = L0 - 4;
   if (n <= 0) return;
-  k_wake<<<(n + 127) / 128, 128, 0, s>>>(ws, mEx, mEy, wpitch, h0, h1, mean, out);
+  k_wake<T><<<(n + 127) / 128, 128, 0, s>>>(ws, mEx, mEy, wpitch, h0, h1, mean, out);
 }
+template void launch_wake<double>(const WinState *, const double *, const double *, int, int, double, double,
+                                  const double *, double *, cudaStream_t);
+template void launch_wake<float>(const WinState *, const float *, const float *, int, int, double, double,
+                                 const double *, double *, cudaStream_t);
 
 void launch_charge_diff(int order, const double *ox, const double *oy, const double *x, const double *y,
                         const double *q, long long n, double org0, double org1, double h0, double h1,

@@ -1,6 +1,8 @@
 // Field kernels: the TE/TM split Yee update on the static mesh and on the
 // moving window, the conformal cut-cell corrections, the window <-> static
-// strip exchange and the window move.
+// strip exchange and the window move.  Every kernel is a template on the
+// field type: double on the FP64 path (the reference's arithmetic, operation
+// for operation), float in FP32 mode.
 //
 // One sub-step (half-H, Ex or Ey) is one launch: the static sweep over the
 // masked regular cells, the sparse cut-cell list and the window cells are
@@ -18,33 +20,33 @@ namespace csrst {
 constexpr int kTX = 32, kTY = 8;
 
 // Half H update (first and third sub-step).
-__global__ void __launch_bounds__(256) k_half_h(FieldArgs a) {
+template <class T>
+__global__ void __launch_bounds__(256) k_half_h(FieldArgsT<T> a) {
   const int b = blockIdx.x;
-  const double zero = 0.0;
-  (void)zero;
   if (b < a.nbS) {
     const int i = (b % a.tilesX) * kTX + (threadIdx.x % kTX);
     const int j = (b / a.tilesX) * kTY + (threadIdx.x / kTX);
     if (i >= a.Nx || j >= a.Ny) return;
     if (!a.mask[(size_t)j * a.Nx + i]) return;
-    const double ey0 = a.Ey.at(i, j), ey1 = a.Ey.at(i + 1, j);
-    const double ex0 = a.Ex.at(i, j), ex1 = a.Ex.at(i, j + 1);
-    double &hx = a.Hx.at(i, j), &hy = a.Hy.at(i, j);
+    const T ey0 = a.Ey.at(i, j), ey1 = a.Ey.at(i + 1, j);
+    const T ex0 = a.Ex.at(i, j), ex1 = a.Ex.at(i, j + 1);
+    T &hx = a.Hx.at(i, j), &hy = a.Hy.at(i, j);
     hx = hx - a.chx * (ey1 - ey0);
     hy = hy + a.chy * (ex1 - ex0);
   } else if (b < a.nbS + a.nbC) {
     const int k = (b - a.nbS) * blockDim.x + threadIdx.x;
     if (k >= a.ncells) return;
     const CutCellDev c = a.cells[k];
-    const double u0 = a.mhx * (c.n1 * a.Ey.at(c.i + 1, c.j) - c.l1 * a.Ey.at(c.i, c.j)) / c.area;
-    const double u1 = a.mhy * (c.n0 * a.Ex.at(c.i, c.j + 1) - c.l0 * a.Ex.at(c.i, c.j)) / c.area;
+    const T n0 = (T)c.n0, n1 = (T)c.n1, l0 = (T)c.l0, l1 = (T)c.l1, area = (T)c.area;
+    const T u0 = a.mhx * (n1 * a.Ey.at(c.i + 1, c.j) - l1 * a.Ey.at(c.i, c.j)) / area;
+    const T u1 = a.mhy * (n0 * a.Ex.at(c.i, c.j + 1) - l0 * a.Ex.at(c.i, c.j)) / area;
     a.Hx.at(c.i, c.j) += u0;
     a.Hy.at(c.i, c.j) += u1;
   } else {
     const int k = (b - a.nbS - a.nbC) * blockDim.x + threadIdx.x;
     if (k >= a.L0 * a.L1) return;
     const int i = k % a.L0, j = k / a.L0;
-    double &hx = a.mHx.at(i, j), &hy = a.mHy.at(i, j);
+    T &hx = a.mHx.at(i, j), &hy = a.mHy.at(i, j);
     hx = hx - a.chx * (a.mEy.at(i + 1, j) - a.mEy.at(i, j));
     hy = hy + a.chy * (a.mEx.at(i, j + 1) - a.mEx.at(i, j));
   }
@@ -55,8 +57,8 @@ __global__ void __launch_bounds__(256) k_half_h(FieldArgs a) {
 // zero every step, main.cpp:388, :494), so it enters as 0.0.  The window
 // current comes from the fixed-point accumulator of the last push, which is
 // converted, stored for diagnostics and cleared for the next deposit.
-template <int COMP>
-__global__ void __launch_bounds__(256) k_update_e(FieldArgs a, double zeroJ) {
+template <class T, int COMP>
+__global__ void __launch_bounds__(256) k_update_e(FieldArgsT<T> a, T zeroJ) {
   const int b = blockIdx.x;
   if (b < a.nbS) {
     const int i = (b % a.tilesX) * kTX + (threadIdx.x % kTX);
@@ -64,10 +66,10 @@ __global__ void __launch_bounds__(256) k_update_e(FieldArgs a, double zeroJ) {
     if (i >= a.Nx || j >= a.Ny) return;
     if (!a.mask[(size_t)j * a.Nx + i]) return;
     if (COMP == 0) {
-      double &e = a.Ex.at(i, j);
+      T &e = a.Ex.at(i, j);
       e = e + (a.kex * (a.Hx.at(i, j) - a.Hx.at(i, j - 1) + a.Hy.at(i, j) - a.Hy.at(i, j - 1)) - a.dteps * zeroJ);
     } else {
-      double &e = a.Ey.at(i, j);
+      T &e = a.Ey.at(i, j);
       e = e - (a.key * (a.Hx.at(i, j) - a.Hx.at(i - 1, j) + a.Hy.at(i, j) - a.Hy.at(i - 1, j)) + a.dteps * zeroJ);
     }
   } else if (b < a.nbS + a.nbC) {
@@ -77,28 +79,28 @@ __global__ void __launch_bounds__(256) k_update_e(FieldArgs a, double zeroJ) {
     if (c.area < kMinArea) return;
     if (COMP == 0) {
       if (!(c.l0 > kSpaceEps)) return;
-      const double u0 = (a.Hx.at(c.i, c.j) - a.Hx.at(c.i, c.j - 1)) / a.h1;
-      const double u1 = (a.Hy.at(c.i, c.j) - a.Hy.at(c.i, c.j - 1)) / a.h1;
+      const T u0 = (a.Hx.at(c.i, c.j) - a.Hx.at(c.i, c.j - 1)) / a.h1;
+      const T u1 = (a.Hy.at(c.i, c.j) - a.Hy.at(c.i, c.j - 1)) / a.h1;
       a.Ex.at(c.i, c.j) += a.de * (u0 + u1 - zeroJ);
     } else {
       if (!(c.l1 > kSpaceEps)) return;
-      const double u0 = -(a.Hx.at(c.i, c.j) - a.Hx.at(c.i - 1, c.j)) / a.h0;
-      const double u1 = -(a.Hy.at(c.i, c.j) - a.Hy.at(c.i - 1, c.j)) / a.h0;
+      const T u0 = -(a.Hx.at(c.i, c.j) - a.Hx.at(c.i - 1, c.j)) / a.h0;
+      const T u1 = -(a.Hy.at(c.i, c.j) - a.Hy.at(c.i - 1, c.j)) / a.h0;
       a.Ey.at(c.i, c.j) += a.de * (u0 + u1 - zeroJ);
     }
   } else {
     const int k = (b - a.nbS - a.nbC) * blockDim.x + threadIdx.x;
     if (k >= a.L0 * a.L1) return;
     const int i = k % a.L0, j = k / a.L0;
-    const double J = (double)(long long)a.acc[k] * a.acc_inv;
+    const T J = (T)((double)(long long)a.acc[k] * a.acc_inv);
     a.acc[k] = 0ull;
     if (COMP == 0) {
       a.mJx.at(i, j) = J;
-      double &e = a.mEx.at(i, j);
+      T &e = a.mEx.at(i, j);
       e = e + (a.kex * (a.mHx.at(i, j) - a.mHx.at(i, j - 1) + a.mHy.at(i, j) - a.mHy.at(i, j - 1)) - a.dteps * J);
     } else {
       a.mJy.at(i, j) = J;
-      double &e = a.mEy.at(i, j);
+      T &e = a.mEy.at(i, j);
       e = e - (a.key * (a.mHx.at(i, j) - a.mHx.at(i - 1, j) + a.mHy.at(i, j) - a.mHy.at(i - 1, j)) + a.dteps * J);
     }
   }
@@ -112,7 +114,8 @@ __global__ void __launch_bounds__(256) k_update_e(FieldArgs a, double zeroJ) {
 //   Ex: window first row -> static; static row above the window -> window guard.
 //   Ey: window first column -> static; static column right of the window -> window guard.
 // No element is both read and written, so every thread copies one element.
-__global__ void k_exchange(FieldArgs a, int which) {
+template <class T>
+__global__ void k_exchange(FieldArgsT<T> a, int which) {
   const WinState *ws = a.ws;
   const int P0 = ws->P0, P1 = ws->P1, L0 = a.L0, L1 = a.L1;
   int k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -138,8 +141,8 @@ __global__ void k_exchange(FieldArgs a, int which) {
   if (to_window) {
     if (si < 0 || si >= a.Nx || sj < 0 || sj >= a.Ny) return;
     if (which == 0) {
-      const double v = a.Hx.at(si, sj) + a.Hy.at(si, sj);
-      a.mHx.at(wi, wj) = 0.5 * v; a.mHy.at(wi, wj) = 0.5 * v;
+      const T v = a.Hx.at(si, sj) + a.Hy.at(si, sj);
+      a.mHx.at(wi, wj) = T(0.5) * v; a.mHy.at(wi, wj) = T(0.5) * v;
     } else if (which == 1) {
       a.mEx.at(wi, wj) = a.Ex.at(si, sj);
     } else {
@@ -148,8 +151,8 @@ __global__ void k_exchange(FieldArgs a, int which) {
   } else {
     if (si < -1 || si > a.Nx || sj < -1 || sj > a.Ny) return;
     if (which == 0) {
-      const double v = a.mHx.at(wi, wj) + a.mHy.at(wi, wj);
-      a.Hx.at(si, sj) = 0.5 * v; a.Hy.at(si, sj) = 0.5 * v;
+      const T v = a.mHx.at(wi, wj) + a.mHy.at(wi, wj);
+      a.Hx.at(si, sj) = T(0.5) * v; a.Hy.at(si, sj) = T(0.5) * v;
     } else if (which == 1) {
       a.Ex.at(si, sj) = a.mEx.at(wi, wj);
     } else {
@@ -160,7 +163,8 @@ __global__ void k_exchange(FieldArgs a, int which) {
 
 // Copy the static fields into the window interior (Communicator::copy via
 // copyFields, main.cpp:335-337).
-__global__ void k_copy_to_window(FieldArgs a) {
+template <class T>
+__global__ void k_copy_to_window(FieldArgsT<T> a) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= a.L0 * a.L1) return;
   const int i = k % a.L0, j = k / a.L0;
@@ -173,7 +177,8 @@ __global__ void k_copy_to_window(FieldArgs a) {
 // Set err if the window or its one-cell ring touches a cell that is not a
 // regular inside cell: the fused sub-step launches assume the strip exchange
 // and the cut-cell corrections never meet.
-__device__ void check_window_clear(const FieldArgs &a, WinState *ws) {
+template <class T>
+__device__ void check_window_clear(const FieldArgsT<T> &a, WinState *ws) {
   const int P0 = ws->P0, P1 = ws->P1;
   const int per = 2 * (a.L0 + 2) + 2 * a.L1;
   for (int k = threadIdx.x; k < per; k += blockDim.x) {
@@ -188,20 +193,23 @@ __device__ void check_window_clear(const FieldArgs &a, WinState *ws) {
   }
 }
 
-__global__ void k_check_window(FieldArgs a) { check_window_clear(a, a.ws); }
+template <class T>
+__global__ void k_check_window(FieldArgsT<T> a) { check_window_clear(a, a.ws); }
 
 // Window move (moveMesh, main.cpp:562-652, and exchangeBoundariesMovingMesh,
 // Communicator.cpp:123-642).  One CTA: reads the last deposit's particle
 // bounds, shifts the window by whole cells through a scratch copy, updates
 // the window position and origin, then refreshes the strips.
+template <class T>
 struct MoveArgs {
-  FieldArgs f;
-  double *scratch;      // 6 window planes
+  FieldArgsT<T> f;
+  T *scratch;           // 6 window planes
   double h0, h1;
 };
 
-__global__ void __launch_bounds__(1024) k_move(MoveArgs m) {
-  FieldArgs &a = m.f;
+template <class T>
+__global__ void __launch_bounds__(1024) k_move(MoveArgs<T> m) {
+  FieldArgsT<T> &a = m.f;
   WinState *ws = a.ws;
   if (ws->err) return;
   const int L[2] = {a.L0, a.L1};
@@ -230,7 +238,7 @@ __global__ void __launch_bounds__(1024) k_move(MoveArgs m) {
   const int moveI = s_move[1], m1 = s_move[2];
   if (moveI == 0 && m1 == 0) return;
   const int W0 = a.L0 + 2, W1 = a.L1 + 2, np = W0 * W1;
-  Plane *pl[6] = {&a.mEx, &a.mEy, &a.mHx, &a.mHy, &a.mJx, &a.mJy};
+  PlaneT<T> *pl[6] = {&a.mEx, &a.mEy, &a.mHx, &a.mHy, &a.mJx, &a.mJy};
   // phase A: snapshot
   for (int k = threadIdx.x; k < 6 * np; k += blockDim.x) {
     const int f = k / np, r = k % np;
@@ -309,14 +317,14 @@ __global__ void __launch_bounds__(1024) k_move(MoveArgs m) {
     beg[l + 1] = beg[l] + c;
   }
   const int total = beg[nl];
-  double *vals = m.scratch;  // the snapshot is no longer needed
+  T *vals = m.scratch;  // the snapshot is no longer needed
   for (int k = threadIdx.x; k < total; k += blockDim.x) {
     int l = 0;
     while (k >= beg[l + 1]) ++l;
     const int *y = lay[l];
     const int w = y[2] - y[1] + 1, r = k - beg[l];
     const int i = y[1] + r % w, j = y[3] + r / w;
-    double v;
+    T v;
     switch (y[0]) {
       case 0: v = a.mHx.at(i, j) + a.mHy.at(i, j); break;
       case 1: v = a.mEx.at(i, j); break;
@@ -334,12 +342,12 @@ __global__ void __launch_bounds__(1024) k_move(MoveArgs m) {
     const int *y = lay[l];
     const int w = y[2] - y[1] + 1, r = k - beg[l];
     const int i = y[1] + r % w, j = y[3] + r / w;
-    const double v = vals[k];
+    const T v = vals[k];
     switch (y[0]) {
-      case 0: a.Hx.at(i + P0, j + P1) = 0.5 * v; a.Hy.at(i + P0, j + P1) = 0.5 * v; break;
+      case 0: a.Hx.at(i + P0, j + P1) = T(0.5) * v; a.Hy.at(i + P0, j + P1) = T(0.5) * v; break;
       case 1: a.Ex.at(i + P0, j + P1) = v; break;
       case 2: a.Ey.at(i + P0, j + P1) = v; break;
-      case 3: a.mHx.at(i - P0, j - P1) = 0.5 * v; a.mHy.at(i - P0, j - P1) = 0.5 * v; break;
+      case 3: a.mHx.at(i - P0, j - P1) = T(0.5) * v; a.mHy.at(i - P0, j - P1) = T(0.5) * v; break;
       case 4: a.mEx.at(i - P0, j - P1) = v; break;
       default: a.mEy.at(i - P0, j - P1) = v; break;
     }
@@ -351,22 +359,24 @@ __global__ void __launch_bounds__(1024) k_move(MoveArgs m) {
 // SCBoundaryCondition::resetOutsideDomain (SCBoundaryCondition.hh:163-195):
 // E = 0 on cells that are neither inside nor a kept cut cell, and on cut
 // cells per component.  cutidx maps a cell to its cut-cell entry or -1.
-__global__ void k_reset_outside(FieldArgs a, const int *cutidx) {
+template <class T>
+__global__ void k_reset_outside(FieldArgsT<T> a, const int *cutidx) {
   const long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (k >= (long long)a.Nx * a.Ny) return;
   if (a.mask[k]) return;
   const int i = (int)(k % a.Nx), j = (int)(k / a.Nx);
   const int c = cutidx[k];
-  if (c < 0) { a.Ex.at(i, j) = 0.0; a.Ey.at(i, j) = 0.0; return; }
+  if (c < 0) { a.Ex.at(i, j) = T(0); a.Ey.at(i, j) = T(0); return; }
   const CutCellDev cc = a.cells[c];
-  if (cc.l0 < kSpaceEps) a.Ex.at(i, j) = 0.0;
-  if (cc.l1 < kSpaceEps) a.Ey.at(i, j) = 0.0;
-  if (cc.area < kMinArea) { a.Ex.at(i, j) = 0.0; a.Ey.at(i, j) = 0.0; }
+  if (cc.l0 < kSpaceEps) a.Ex.at(i, j) = T(0);
+  if (cc.l1 < kSpaceEps) a.Ey.at(i, j) = T(0);
+  if (cc.area < kMinArea) { a.Ex.at(i, j) = T(0); a.Ey.at(i, j) = T(0); }
 }
 
 // --- host launchers -----------------------------------------------------------
 
-static int sub_grid(FieldArgs &a) {
+template <class T>
+static int sub_grid(FieldArgsT<T> &a) {
   a.tilesX = (a.Nx + kTX - 1) / kTX;
   a.nbS = a.tilesX * ((a.Ny + kTY - 1) / kTY);
   a.nbC = (a.ncells + 255) / 256;
@@ -374,36 +384,54 @@ static int sub_grid(FieldArgs &a) {
   return a.nbS + a.nbC + nbM;
 }
 
-void launch_half_h(FieldArgs a, cudaStream_t s) {
+template <class T>
+void launch_half_h(FieldArgsT<T> a, cudaStream_t s) {
   const int g = sub_grid(a);
-  k_half_h<<<g, 256, 0, s>>>(a);
+  k_half_h<T><<<g, 256, 0, s>>>(a);
 }
 
-void launch_update_e(FieldArgs a, int comp, cudaStream_t s) {
+template <class T>
+void launch_update_e(FieldArgsT<T> a, int comp, cudaStream_t s) {
   const int g = sub_grid(a);
-  if (comp == 0) k_update_e<0><<<g, 256, 0, s>>>(a, 0.0);
-  else k_update_e<1><<<g, 256, 0, s>>>(a, 0.0);
+  if (comp == 0) k_update_e<T, 0><<<g, 256, 0, s>>>(a, T(0));
+  else k_update_e<T, 1><<<g, 256, 0, s>>>(a, T(0));
 }
 
-void launch_exchange(FieldArgs a, int which, cudaStream_t s) {
+template <class T>
+void launch_exchange(FieldArgsT<T> a, int which, cudaStream_t s) {
   const int n = which == 0 ? 2 * (a.L0 + a.L1) + 4 : which == 1 ? 2 * a.L0 + 2 : 2 * a.L1 + 2;
-  k_exchange<<<(n + 127) / 128, 128, 0, s>>>(a, which);
+  k_exchange<T><<<(n + 127) / 128, 128, 0, s>>>(a, which);
 }
 
-void launch_copy_to_window(FieldArgs a, cudaStream_t s) {
-  k_copy_to_window<<<(a.L0 * a.L1 + 255) / 256, 256, 0, s>>>(a);
+template <class T>
+void launch_copy_to_window(FieldArgsT<T> a, cudaStream_t s) {
+  k_copy_to_window<T><<<(a.L0 * a.L1 + 255) / 256, 256, 0, s>>>(a);
 }
 
-void launch_check_window(FieldArgs a, cudaStream_t s) { k_check_window<<<1, 256, 0, s>>>(a); }
+template <class T>
+void launch_check_window(FieldArgsT<T> a, cudaStream_t s) { k_check_window<T><<<1, 256, 0, s>>>(a); }
 
-void launch_move(FieldArgs a, double *scratch, double h0, double h1, cudaStream_t s) {
-  MoveArgs m{a, scratch, h0, h1};
-  k_move<<<1, 1024, 0, s>>>(m);
+template <class T>
+void launch_move(FieldArgsT<T> a, T *scratch, double h0, double h1, cudaStream_t s) {
+  MoveArgs<T> m{a, scratch, h0, h1};
+  k_move<T><<<1, 1024, 0, s>>>(m);
 }
 
-void launch_reset_outside(FieldArgs a, const int *cutidx, cudaStream_t s) {
+template <class T>
+void launch_reset_outside(FieldArgsT<T> a, const int *cutidx, cudaStream_t s) {
   const long long n = (long long)a.Nx * a.Ny;
-  k_reset_outside<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(a, cutidx);
+  k_reset_outside<T><<<(unsigned)((n + 255) / 256), 256, 0, s>>>(a, cutidx);
 }
+
+#define CSRST_FIELDS_INSTANTIATE(T)                                                         \
+  template void launch_half_h<T>(FieldArgsT<T>, cudaStream_t);                              \
+  template void launch_update_e<T>(FieldArgsT<T>, int, cudaStream_t);                       \
+  template void launch_exchange<T>(FieldArgsT<T>, int, cudaStream_t);                       \
+  template void launch_copy_to_window<T>(FieldArgsT<T>, cudaStream_t);                      \
+  template void launch_check_window<T>(FieldArgsT<T>, cudaStream_t);                        \
+  template void launch_move<T>(FieldArgsT<T>, T *, double, double, cudaStream_t);           \
+  template void launch_reset_outside<T>(FieldArgsT<T>, const int *, cudaStream_t);
+CSRST_FIELDS_INSTANTIATE(double)
+CSRST_FIELDS_INSTANTIATE(float)
 
 }  // namespace csrst

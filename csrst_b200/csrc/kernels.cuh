@@ -28,11 +28,13 @@ struct PushArgs {
 };
 
 // One field sub-step over the static mesh, the cut cells and the window.
-struct FieldArgs {
-  Plane Ex, Ey, Hx, Hy;            // static mesh
+// T is the field type: double on the FP64 path, float in FP32 mode.
+template <class T>
+struct FieldArgsT {
+  PlaneT<T> Ex, Ey, Hx, Hy;        // static mesh
   const uint8_t *mask;             // inside mask, Nx * Ny, x fastest
   int Nx, Ny;
-  Plane mEx, mEy, mHx, mHy, mJx, mJy;  // window
+  PlaneT<T> mEx, mEy, mHx, mHy, mJx, mJy;  // window
   int L0, L1;
   const CutCellDev *cells;
   int ncells;
@@ -40,15 +42,16 @@ struct FieldArgs {
   unsigned long long *acc;         // fixed-point window current of the E sub-step
   double acc_inv;
   // regular-cell coefficients (TETMSolver.hh:121-125)
-  double chx, chy;                 // 0.5 * eta_x / Z0, 0.5 * eta_y / Z0
-  double kex, key;                 // eta_y * Z0, eta_x * Z0
-  double dteps;                    // c dt Z0
+  T chx, chy;                      // 0.5 * eta_x / Z0, 0.5 * eta_y / Z0
+  T kex, key;                      // eta_y * Z0, eta_x * Z0
+  T dteps;                         // c dt Z0
   // cut-cell coefficients (TETMSolver.cpp:87-127)
-  double mhx, mhy;                 // -0.5 dt / (hx mu0), +0.5 dt / (hy mu0)
-  double de;                       // dt / eps0
-  double h0, h1;
+  T mhx, mhy;                      // -0.5 dt / (hx mu0), +0.5 dt / (hy mu0)
+  T de;                            // dt / eps0
+  T h0, h1;
   int nbS, nbC, tilesX;            // block ranges: static tiles, cut-cell blocks
 };
+using FieldArgs = FieldArgsT<double>;
 
 // Bend parameters (Bend ctor and Bend::Init, Bend.cpp:60-124).
 struct BendDev {
@@ -73,14 +76,14 @@ void launch_deposit(int order, int comp, const double *ox, const double *oy, con
                     double scale, int *err, cudaStream_t s);
 void launch_fixed_to_double(const unsigned long long *acc, double *out, long long n, double inv,
                             cudaStream_t s);
-// fields.cu
-void launch_half_h(FieldArgs a, cudaStream_t s);
-void launch_update_e(FieldArgs a, int comp, cudaStream_t s);
-void launch_exchange(FieldArgs a, int which, cudaStream_t s);
-void launch_copy_to_window(FieldArgs a, cudaStream_t s);
-void launch_check_window(FieldArgs a, cudaStream_t s);
-void launch_move(FieldArgs a, double *scratch, double h0, double h1, cudaStream_t s);
-void launch_reset_outside(FieldArgs a, const int *cutidx, cudaStream_t s);
+// fields.cu (instantiated for T = double and T = float)
+template <class T> void launch_half_h(FieldArgsT<T> a, cudaStream_t s);
+template <class T> void launch_update_e(FieldArgsT<T> a, int comp, cudaStream_t s);
+template <class T> void launch_exchange(FieldArgsT<T> a, int which, cudaStream_t s);
+template <class T> void launch_copy_to_window(FieldArgsT<T> a, cudaStream_t s);
+template <class T> void launch_check_window(FieldArgsT<T> a, cudaStream_t s);
+template <class T> void launch_move(FieldArgsT<T> a, T *scratch, double h0, double h1, cudaStream_t s);
+template <class T> void launch_reset_outside(FieldArgsT<T> a, const int *cutidx, cudaStream_t s);
 // geometry.cu
 int build_geometry(const BendDev &b, uint8_t *d_mask, CutCellDev **d_cells, int *ncells, int **d_cutidx,
                    cudaStream_t s);
@@ -88,8 +91,9 @@ int build_geometry(const BendDev &b, uint8_t *d_mask, CutCellDev **d_cells, int 
 void launch_moments(const double *x, const double *y, const double *px, const double *py, long long n,
                     double half, int pending, double *part, double *mean, double *out, cudaStream_t s);
 size_t moments_scratch_doubles();
-void launch_wake(const WinState *ws, const double *mEx, const double *mEy, int wpitch, int L0, double h0,
-                 double h1, const double *mean, double *out, cudaStream_t s);
+template <class T>
+void launch_wake(const WinState *ws, const T *mEx, const T *mEy, int wpitch, int L0, double h0, double h1,
+                 const double *mean, double *out, cudaStream_t s);
 void launch_charge_diff(int order, const double *ox, const double *oy, const double *x, const double *y,
                         const double *q, long long n, double org0, double org1, double h0, double h1,
                         int i0, int j0, int ni, int nj, unsigned long long *acc, double scale,
@@ -116,5 +120,55 @@ struct PoissonReport {
   int levels;
 };
 int poisson_initial_fields(const PoissonInput &in, PoissonReport *rep, cudaStream_t s, std::string *msg);
+
+// --- FP32 mode (particles32.cu) -------------------------------------------
+// Positions are FP32 offsets from an FP64 cell origin: the static-mesh cell
+// (i, j) packed as i | j << 16 and the offset inside it in cells, [0, 1).
+// Momenta are FP32 deviations from an FP64 reference momentum P (the mean
+// at load): at gamma ~ 1000 a bare FP32 momentum has an ulp of 6e-5, above
+// the per-step kicks, while the deviations stay below ~1.
+struct Bunch32 {
+  int *cell;
+  float *ox, *oy;
+  float *dpx, *dpy;
+  float *q;
+  long long n;
+};
+
+struct Push32Args {
+  Bunch32 b;
+  WinState *ws;
+  const float *mEx, *mEy, *mHx, *mHy;  // window planes, pitch wpitch
+  int wpitch;
+  unsigned long long *acc;             // L0 * L1 fixed-point current for jcomp
+  double acc_scale;
+  int jcomp, pending;
+  double P0, P1;                       // reference momentum
+  double kh0, kh1;                     // 0.5 c dt / h: cells per half step per unit beta
+  float f1, f2;                        // 0.5 c dt q/m and f1 c
+  double h0, h1, dt;                   // spacing and time step (current scale)
+  double org0, org1;                   // static mesh origin (dipole position)
+  double bz, Lb, hw, chh, shh, bwidth; // hard-edge dipole
+  int use_smem;
+};
+
+int launch_push32(const Push32Args &a, int order, int L0, int L1, int grid, cudaStream_t s);
+void launch_prep32(WinState *ws, int order, cudaStream_t s);
+void launch_bounds32(WinState *ws, cudaStream_t s);
+void launch_bbox32(const Bunch32 &b, double P0, double P1, double kh0, double kh1, int pending, WinState *ws,
+                   cudaStream_t s);
+void launch_drift32(const Bunch32 &b, double P0, double P1, double kd0, double kd1, cudaStream_t s);
+void launch_from64(const double *x, const double *y, const double *px, const double *py, const double *q,
+                   long long n, double org0, double org1, double h0, double h1, double P0, double P1,
+                   const Bunch32 &b, cudaStream_t s);
+// pending > 0: the stored positions still owe the drift by -kh (cells)
+void launch_to64(const Bunch32 &b, double P0, double P1, double kh0, double kh1, int pending, double org0,
+                 double org1, double h0, double h1, double *x, double *y, double *px, double *py,
+                 cudaStream_t s);
+void launch_psum(const double *px, const double *py, long long n, double *part, double *out2,
+                 cudaStream_t s);
+// Plane copies between FP64 and FP32 (rows x cols elements, pitches in elements).
+void launch_d2f(const double *src, int spitch, float *dst, int dpitch, int rows, int cols, cudaStream_t s);
+void launch_f2d(const float *src, int spitch, double *dst, int dpitch, int rows, int cols, cudaStream_t s);
 
 }  // namespace csrst

@@ -44,7 +44,7 @@ __global__ void k_noalloc_deposit(int comp, const double *ox, const double *oy, 
       const bool in = a >= 0 && b >= 0 && a < ni && b < nj;
       warp_add(acc, in ? b * ni + a : -1, __double2ll_rn(v * scale));
     };
-    if (!deposit_particle<ORDER>(comp, q[i], ox[i], oy[i], x[i], y[i], org0, org1, h0, h1, dt, sink))
+    if (!deposit_particle<ORDER>(comp, q[i], ox[i], oy[i], x[i], y[i], org0, org1, h0, h1, h0, h1, dt, sink))
       g_noalloc_err = kErrCrossings;
   }
 }

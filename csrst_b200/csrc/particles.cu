@@ -16,48 +16,12 @@
 // shared-memory copy of the window per CTA, then into the global window.
 // Integer addition is exact and associative, so the result is bitwise the
 // same for any launch shape, CTA count or scheduling order.
+#include "accum.cuh"
+#include "bbox.cuh"
 #include "kernels.cuh"
 #include "shapes.cuh"
 
 namespace csrst {
-
-__device__ __forceinline__ void warp_bbox(double &mn0, double &mn1, double &mx0, double &mx1) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    mn0 = fmin(mn0, __shfl_xor_sync(0xffffffffu, mn0, o));
-    mn1 = fmin(mn1, __shfl_xor_sync(0xffffffffu, mn1, o));
-    mx0 = fmax(mx0, __shfl_xor_sync(0xffffffffu, mx0, o));
-    mx1 = fmax(mx1, __shfl_xor_sync(0xffffffffu, mx1, o));
-  }
-}
-
-// Reduce a per-thread box over the CTA and merge it into dst[4] with atomics.
-__device__ void block_bbox(double mn0, double mn1, double mx0, double mx1, long long *dst) {
-  __shared__ double sb[4][32];
-  warp_bbox(mn0, mn1, mx0, mx1);
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
-  if (lane == 0) { sb[0][w] = mn0; sb[1][w] = mn1; sb[2][w] = mx0; sb[3][w] = mx1; }
-  __syncthreads();
-  if (w == 0) {
-    mn0 = lane < nw ? sb[0][lane] : INFINITY;
-    mn1 = lane < nw ? sb[1][lane] : INFINITY;
-    mx0 = lane < nw ? sb[2][lane] : -INFINITY;
-    mx1 = lane < nw ? sb[3][lane] : -INFINITY;
-    warp_bbox(mn0, mn1, mx0, mx1);
-    if (lane == 0 && mn0 <= mx0) {
-      atomicMin(&dst[0], dbl_ord(mn0));
-      atomicMin(&dst[1], dbl_ord(mn1));
-      atomicMax(&dst[2], dbl_ord(mx0));
-      atomicMax(&dst[3], dbl_ord(mx1));
-    }
-  }
-  __syncthreads();
-}
-
-__device__ __forceinline__ void bbox_reset(long long *b) {
-  b[0] = dbl_ord(INFINITY); b[1] = dbl_ord(INFINITY);
-  b[2] = dbl_ord(-INFINITY); b[3] = dbl_ord(-INFINITY);
-}
 
 // Positions R1 = R0 + h v(P) of the next push; fills slot `cur` of the window
 // state.  pending: the stored R still owes the -dt/2 drift.
@@ -120,6 +84,7 @@ __global__ void k_push_post(WinState *ws) {
   if (threadIdx.x == 0) ws->cur = 1 - ws->cur;
 }
 
+// Dynamic shared memory: [window accumulator (SMEM only)][per-thread deposit tiles].
 template <int ORDER, bool SMEM>
 __global__ void __launch_bounds__(256, 2) k_push(PushArgs a) {
   extern __shared__ unsigned long long sacc[];
@@ -131,11 +96,16 @@ __global__ void __launch_bounds__(256, 2) k_push(PushArgs a) {
   if (s_err) return;  // the whole CTA leaves together
   const int L0 = ws->L0, L1 = ws->L1;
   const int ncell = L0 * L1;
-  if (SMEM) {
+  using Tile = typename TileFor<ORDER>::T;
+  unsigned long long *win = SMEM ? sacc : a.acc;
+  unsigned long long *tmem = SMEM ? sacc + ncell : sacc;
+  if (SMEM)
     for (int k = threadIdx.x; k < ncell; k += blockDim.x) sacc[k] = 0ull;
-    if (threadIdx.x == 0) { tb[0] = L0; tb[1] = L1; tb[2] = -1; tb[3] = -1; }
-    __syncthreads();
-  }
+  for (int k = threadIdx.x; k < Tile::kSize * (int)blockDim.x; k += blockDim.x) tmem[k] = 0ull;
+  if (threadIdx.x == 0) { tb[0] = L0; tb[1] = L1; tb[2] = -1; tb[3] = -1; }
+  __syncthreads();
+  Tile tile;
+  tile.init(tmem, L0, L1);
   const double mo0 = ws->mo0, mo1 = ws->mo1;
   const double h0 = a.h0, h1 = a.h1;
   const double ood0 = 1.0 / h0, ood1 = 1.0 / h1;
@@ -153,72 +123,78 @@ __global__ void __launch_bounds__(256, 2) k_push(PushArgs a) {
   double bmn0 = INFINITY, bmn1 = INFINITY, bmx0 = -INFINITY, bmx1 = -INFINITY;  // next R1
   bool overflow = false;
   const double scale = a.acc_scale;
-  int ti0 = L0, tj0 = L1, ti1 = -1, tj1 = -1;  // cells this thread touched
-  auto sink = [&](int i, int j, double v) {
-    const bool in = i >= 0 && j >= 0 && i < L0 && j < L1;
-    const long long iv = __double2ll_rn(v * scale);
-    if (SMEM) {
-      if (in) { ti0 = min(ti0, i); tj0 = min(tj0, j); ti1 = max(ti1, i); tj1 = max(tj1, j); }
-      warp_add(sacc, in ? j * L0 + i : -1, iv);
-    } else {
-      warp_add(a.acc, in ? j * L0 + i : -1, iv);
-    }
-  };
+  auto sink = [&](int i, int j, double v) { tile.template add<SMEM>(i, j, __double2ll_rn(v * scale), win, L0, L1); };
 
-  // Each CTA owns a contiguous slice of the (cell-ordered) particles.
+  // Each CTA owns a contiguous slice of the (cell-ordered) particles.  The
+  // rounds are the same for every lane, so that the warp re-bases its
+  // deposit tile together.
   const long long per = (a.n + gridDim.x - 1) / gridDim.x;
   const long long beg = (long long)blockIdx.x * per;
   const long long end = beg + per < a.n ? beg + per : a.n;
-  for (long long i = beg + threadIdx.x; i < end; i += blockDim.x) {
-    double x = a.x[i], y = a.y[i];
-    double p0 = a.px[i], p1 = a.py[i];
-    const double q = a.q[i];
-    if (!(isfinite(x) && isfinite(y) && isfinite(p0) && isfinite(p1))) {
-      set_err(ws, kErrWindowFit);
-      continue;
+  const long long rounds = end > beg ? (end - beg + blockDim.x - 1) / blockDim.x : 0;
+  for (long long it = 0; it < rounds; ++it) {
+    const long long i = beg + it * blockDim.x + threadIdx.x;
+    bool ok = i < end;
+    double x = 0.0, y = 0.0, p0 = 0.0, p1 = 0.0, q = 0.0, r0x = 0.0, r0y = 0.0, w0 = 0.0, w1 = 0.0;
+    if (ok) {
+      x = a.x[i]; y = a.y[i]; p0 = a.px[i]; p1 = a.py[i]; q = a.q[i];
+      if (!(isfinite(x) && isfinite(y) && isfinite(p0) && isfinite(p1))) {
+        set_err(ws, kErrWindowFit);
+        ok = false;
+      }
     }
-    double r = inv_gamma(p0, p1);
-    double w0 = a.half * p0 * r, w1 = a.half * p1 * r;
-    if (a.pending) { x = x + (-w0); y = y + (-w1); }          // drift_particles(-dt/2)
-    const double r0x = x, r0y = y;                             // oldR
-    x = x + w0; y = y + w1;                                    // R1
-    // gather (FieldPatch::gather x3; Hz = Hzx + Hzy on the fly)
-    const double E0 = gather_edge<ORDER>(pex, (x - exo0) * ood0, (y - exo1) * ood1, 0);
-    const double E1 = gather_edge<ORDER>(pey, (x - eyo0) * ood0, (y - eyo1) * ood1, 1);
-    const double hpp0 = (x - hzo0) * ood0, hpp1 = (y - hzo1) * ood1;
-    const double Hf = gather_cell<ORDER>(SumView{phx, phy}, hpp0, hpp1);
-    // hard-edge dipole
-    const double D0 = x - a.Lb, D1 = y - a.hw;
-    const double dist = a.chh * D0 - a.shh * D1;
-    const double bext = (dist > 0.0 && dist < a.bwidth) ? a.bz : 0.0;
-    const double B = kMu0 * Hf + 0.5 * bext;
-    // kick + rotation (PartBunch.cpp:366-383)
-    const double k0 = a.fact1 * E0, k1 = a.fact1 * E1;
-    double u0 = p0 + k0, u1 = p1 + k1;
-    const double aa = a.fact2 * B * inv_gamma(u0, u1);
-    const double s0 = u0 + aa * u1, s1 = u1 + aa * (-u0);
-    const double tmp = 1.0 + aa * aa;
-    u0 = ((1.0 + aa * aa) * s0 + aa * s1) / tmp;
-    u1 = ((1.0 + aa * aa) * s1 - aa * s0) / tmp;
-    p0 = u0 + k0; p1 = u1 + k1;
-    r = inv_gamma(p0, p1);
-    w0 = a.half * p0 * r; w1 = a.half * p1 * r;
-    x = x + w0; y = y + w1;                                    // R2
-    a.x[i] = x; a.y[i] = y; a.px[i] = p0; a.py[i] = p1;
-    // current deposit R0 -> R2 in window coordinates
-    if (!deposit_particle<ORDER>(a.jcomp, q, r0x, r0y, x, y, mo0, mo1, h0, h1, a.dt, sink))
-      overflow = true;
-    amn0 = fmin(amn0, fmin(x, r0x)); amn1 = fmin(amn1, fmin(y, r0y));
-    amx0 = fmax(amx0, fmax(x, r0x)); amx1 = fmax(amx1, fmax(y, r0y));
-    // next push gathers at (R2 - h v) + h v
-    const double nx = (x + (-w0)) + w0, ny = (y + (-w1)) + w1;
-    bmn0 = fmin(bmn0, nx); bmn1 = fmin(bmn1, ny); bmx0 = fmax(bmx0, nx); bmx1 = fmax(bmx1, ny);
+    if (ok) {
+      double r = inv_gamma(p0, p1);
+      w0 = a.half * p0 * r; w1 = a.half * p1 * r;
+      if (a.pending) { x = x + (-w0); y = y + (-w1); }          // drift_particles(-dt/2)
+      r0x = x; r0y = y;                                          // oldR
+      x = x + w0; y = y + w1;                                    // R1
+      // gather (FieldPatch::gather x3; Hz = Hzx + Hzy on the fly)
+      const double E0 = gather_edge<ORDER>(pex, (x - exo0) * ood0, (y - exo1) * ood1, 0);
+      const double E1 = gather_edge<ORDER>(pey, (x - eyo0) * ood0, (y - eyo1) * ood1, 1);
+      const double hpp0 = (x - hzo0) * ood0, hpp1 = (y - hzo1) * ood1;
+      const double Hf = gather_cell<ORDER>(SumView{phx, phy}, hpp0, hpp1);
+      // hard-edge dipole
+      const double D0 = x - a.Lb, D1 = y - a.hw;
+      const double dist = a.chh * D0 - a.shh * D1;
+      const double bext = (dist > 0.0 && dist < a.bwidth) ? a.bz : 0.0;
+      const double B = kMu0 * Hf + 0.5 * bext;
+      // kick + rotation (PartBunch.cpp:366-383)
+      const double k0 = a.fact1 * E0, k1 = a.fact1 * E1;
+      double u0 = p0 + k0, u1 = p1 + k1;
+      const double aa = a.fact2 * B * inv_gamma(u0, u1);
+      const double s0 = u0 + aa * u1, s1 = u1 + aa * (-u0);
+      const double tmp = 1.0 + aa * aa;
+      u0 = ((1.0 + aa * aa) * s0 + aa * s1) / tmp;
+      u1 = ((1.0 + aa * aa) * s1 - aa * s0) / tmp;
+      p0 = u0 + k0; p1 = u1 + k1;
+      r = inv_gamma(p0, p1);
+      w0 = a.half * p0 * r; w1 = a.half * p1 * r;
+      x = x + w0; y = y + w1;                                    // R2
+      a.x[i] = x; a.y[i] = y; a.px[i] = p0; a.py[i] = p1;
+    }
+    // current deposit R0 -> R2 in window coordinates, summed in the warp's tile
+    tile.template rebase<SMEM>(ok, ok ? (int)floor((r0x - mo0) * ood0) : 0, ok ? (int)floor((r0y - mo1) * ood1) : 0,
+                               win, L0, L1);
+    if (ok) {
+      if (!deposit_particle<ORDER>(a.jcomp, q, r0x, r0y, x, y, mo0, mo1, h0, h1, h0, h1, a.dt, sink))
+        overflow = true;
+      amn0 = fmin(amn0, fmin(x, r0x)); amn1 = fmin(amn1, fmin(y, r0y));
+      amx0 = fmax(amx0, fmax(x, r0x)); amx1 = fmax(amx1, fmax(y, r0y));
+      // next push gathers at (R2 - h v) + h v
+      const double nx = (x + (-w0)) + w0, ny = (y + (-w1)) + w1;
+      bmn0 = fmin(bmn0, nx); bmn1 = fmin(bmn1, ny); bmx0 = fmax(bmx0, nx); bmx1 = fmax(bmx1, ny);
+    }
   }
+  tile.template flush<SMEM>(win, L0, L1);
   if (overflow) set_err(ws, kErrCrossings);
   block_bbox(amn0, amn1, amx0, amx1, ws->bball);
   block_bbox(bmn0, bmn1, bmx0, bmx1, ws->bb[1 - ws->cur]);
   if (SMEM) {
-    if (ti1 >= 0) { atomicMin(&tb[0], ti0); atomicMin(&tb[1], tj0); atomicMax(&tb[2], ti1); atomicMax(&tb[3], tj1); }
+    if (tile.ti1 >= 0) {
+      atomicMin(&tb[0], tile.ti0); atomicMin(&tb[1], tile.tj0);
+      atomicMax(&tb[2], tile.ti1); atomicMax(&tb[3], tile.tj1);
+    }
     __syncthreads();
     const int i0 = tb[0], j0 = tb[1], i1 = tb[2], j1 = tb[3];
     if (i1 >= i0) {
@@ -285,7 +261,7 @@ __global__ void k_deposit(int comp, const double *ox, const double *oy, const do
       const bool in = a >= 0 && b >= 0 && a < ni && b < nj;
       warp_add(acc, in ? b * ni + a : -1, __double2ll_rn(v * scale));
     };
-    if (!deposit_particle<ORDER>(comp, q[i], ox[i], oy[i], x[i], y[i], org0, org1, h0, h1, dt, sink))
+    if (!deposit_particle<ORDER>(comp, q[i], ox[i], oy[i], x[i], y[i], org0, org1, h0, h1, h0, h1, dt, sink))
       atomicExch(err, kErrCrossings);
   }
 }
@@ -335,11 +311,12 @@ static long long push_smem_limit() {
 
 template <int ORDER>
 static void push_order(const PushArgs &a, int L0, int L1, int grid, cudaStream_t s) {
-  const size_t sm = (size_t)L0 * L1 * sizeof(unsigned long long);
+  const size_t tiles = (size_t)TileFor<ORDER>::T::kSize * 256 * sizeof(unsigned long long);
+  const size_t sm = (size_t)L0 * L1 * sizeof(unsigned long long) + tiles;
   if (a.use_smem && (long long)sm <= push_smem_limit<ORDER>()) {
     k_push<ORDER, true><<<grid, 256, sm, s>>>(a);
   } else {
-    k_push<ORDER, false><<<grid, 256, 0, s>>>(a);
+    k_push<ORDER, false><<<grid, 256, tiles, s>>>(a);
   }
 }
 

@@ -1,0 +1,436 @@
+// FP32 mode particle kernels: the same fused push as particles.cu
+// (PartBunch::push_particles, PartBunch.cpp:215-519) on a bunch stored as
+// FP32 offsets from FP64 cell origins and FP32 momentum deviations from an
+// FP64 reference momentum.
+//
+// Precision split (what stays FP64 and why):
+//   - 1/gamma: the reference's float Q_rsqrt of 1 + |P|^2 formed in FP64, so
+//     velocities match the FP64 path's (utils.hh:491-504);
+//   - positions during the push: cell-relative doubles built exactly from
+//     the stored offsets, so no precision is lost to the distance from the
+//     mesh origin; the stored offset is rounded to FP32 once per push;
+//   - the current deposit: FP64 weights on those exact positions, so the
+//     discrete continuity equation holds to FP64 rounding;
+//   - the hard-edge dipole test: absolute position in FP64 (the bend frame).
+// The field gather (27 taps for TSC) and the kick/rotation run in FP32; the
+// gather is anchored at the particle's own window cell, so its coordinates
+// are offsets of magnitude < 2 and keep FP32's full resolution.
+// This file is built with FMA contraction on: FP32 mode is checked against
+// the FP64 path to a tolerance, not bit for bit.
+#include "accum.cuh"
+#include "bbox.cuh"
+#include "kernels.cuh"
+#include "shapes.cuh"
+
+namespace csrst {
+namespace {
+
+__device__ __forceinline__ long long gtid() { return blockIdx.x * (long long)blockDim.x + threadIdx.x; }
+
+struct View32 {
+  const float *base;  // window element of the particle's cell
+  int pitch;
+  __device__ __forceinline__ float operator()(int i, int j) const { return __ldg(base + (ptrdiff_t)j * pitch + i); }
+};
+struct SumView32 {
+  View32 a, b;
+  __device__ __forceinline__ float operator()(int i, int j) const { return a(i, j) + b(i, j); }
+};
+
+__device__ __forceinline__ void unpack(int c, int &i, int &j) {
+  i = c & 0xffff;
+  j = (int)((unsigned)c >> 16);
+}
+
+// Position arithmetic uses explicitly rounded operations: the push, the box
+// of the next push's positions and the drift must produce the same bits for
+// the same inputs wherever they are computed, whatever the compiler fuses.
+__device__ __forceinline__ double dmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double dadd(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double dsub(double a, double b) { return __dsub_rn(a, b); }
+
+// 1/gamma as the FP64 path computes it, from the full momentum P + d.
+__device__ __forceinline__ float rgam(double P0, double P1, float d0, float d1, double &p0, double &p1) {
+  p0 = dadd(P0, (double)d0);
+  p1 = dadd(P1, (double)d1);
+  return q_rsqrt((float)dadd(1.0, dadd(dmul(p0, p0), dmul(p1, p1))));
+}
+
+// Drift of one half step in cells: kh * p * (1/gamma).
+__device__ __forceinline__ double half_drift(double kh, double p, float r) { return dmul(dmul(kh, p), (double)r); }
+
+// Cell of the cell-relative coordinate t of cell c, as c' + 0.5 (exact).
+__device__ __forceinline__ double cellc(int c, double t) { return (double)(c + (int)floor(t)) + 0.5; }
+
+// Store a cell-relative position t (cells) of cell (ci, cj) as cell + offset.
+__device__ __forceinline__ void store_pos(double t0, double t1, int ci, int cj, int &cell, float &o0, float &o1) {
+  double f0 = floor(t0), f1 = floor(t1);
+  float a0 = (float)(t0 - f0), a1 = (float)(t1 - f1);
+  if (a0 >= 1.0f) { a0 = 0.0f; f0 += 1.0; }  // rounded up to the next cell
+  if (a1 >= 1.0f) { a1 = 0.0f; f1 += 1.0; }
+  cell = ((ci + (int)f0) & 0xffff) | ((cj + (int)f1) << 16);
+  o0 = a0; o1 = a1;
+}
+
+template <int ORDER, bool SMEM>
+__global__ void __launch_bounds__(256, 2) k_push32(Push32Args a) {
+  extern __shared__ unsigned long long sacc[];
+  __shared__ int tb[4];
+  __shared__ int s_err;
+  WinState *ws = a.ws;
+  if (threadIdx.x == 0) s_err = *(volatile int *)&ws->err;
+  __syncthreads();
+  if (s_err) return;  // the whole CTA leaves together
+  const int L0 = ws->L0, L1 = ws->L1, WP0 = ws->P0, WP1 = ws->P1;
+  using Tile = typename TileFor<ORDER>::T;
+  unsigned long long *win = SMEM ? sacc : a.acc;
+  unsigned long long *tmem = SMEM ? sacc + L0 * L1 : sacc;
+  if (SMEM)
+    for (int k = threadIdx.x; k < L0 * L1; k += blockDim.x) sacc[k] = 0ull;
+  for (int k = threadIdx.x; k < Tile::kSize * (int)blockDim.x; k += blockDim.x) tmem[k] = 0ull;
+  if (threadIdx.x == 0) { tb[0] = L0; tb[1] = L1; tb[2] = -1; tb[3] = -1; }
+  __syncthreads();
+  Tile tile;
+  tile.init(tmem, L0, L1);
+  const int wp = a.wpitch;
+  const double scale = a.acc_scale;
+  double amn0 = INFINITY, amn1 = INFINITY, amx0 = -INFINITY, amx1 = -INFINITY;  // R0 u R2 (cells)
+  double bmn0 = INFINITY, bmn1 = INFINITY, bmx0 = -INFINITY, bmx1 = -INFINITY;  // next R1 (cells)
+  bool overflow = false;
+  int wi = 0, wj = 0;  // window cell of the particle being deposited
+  auto sink = [&](int i, int j, double v) {
+    tile.template add<SMEM>(i + wi, j + wj, __double2ll_rn(v * scale), win, L0, L1);
+  };
+  const double P0 = a.P0, P1 = a.P1;
+  const float Pf0 = (float)P0, Pf1 = (float)P1;
+  const long long per = (a.b.n + gridDim.x - 1) / gridDim.x;
+  const long long beg = (long long)blockIdx.x * per;
+  const long long end = beg + per < a.b.n ? beg + per : a.b.n;
+  const long long rounds = end > beg ? (end - beg + blockDim.x - 1) / blockDim.x : 0;
+  for (long long it = 0; it < rounds; ++it) {  // the same rounds for every lane
+    const long long n = beg + it * blockDim.x + threadIdx.x;
+    bool ok = n < end;
+    int ci = 0, cj = 0;
+    double s0 = 0.0, s1 = 0.0, q = 0.0;
+    float d0 = 0.0f, d1 = 0.0f;
+    if (ok) {
+      unpack(a.b.cell[n], ci, cj);
+      s0 = a.b.ox[n]; s1 = a.b.oy[n];
+      d0 = a.b.dpx[n]; d1 = a.b.dpy[n];
+      q = a.b.q[n];
+      if (!(isfinite(d0) && isfinite(d1) && s0 >= 0.0 && s0 < 1.0 && s1 >= 0.0 && s1 < 1.0)) {
+        set_err(ws, kErrWindowFit);
+        ok = false;
+      }
+    }
+    double p0 = 0.0, p1 = 0.0, w0 = 0.0, w1 = 0.0, r00 = 0.0, r01 = 0.0, x0 = 0.0, x1 = 0.0;
+    if (ok) {
+      const float r = rgam(P0, P1, d0, d1, p0, p1);
+      w0 = half_drift(a.kh0, p0, r); w1 = half_drift(a.kh1, p1, r);
+      r00 = s0; r01 = s1;
+      if (a.pending) { r00 = dsub(s0, w0); r01 = dsub(s1, w1); }  // drift_particles(-dt/2)
+      x0 = dadd(r00, w0); x1 = dadd(r01, w1);                     // R1, cells from (ci, cj)
+      wi = ci - WP0; wj = cj - WP1;
+      // gather (FieldPatch::gather x3) anchored at the window cell of R1; the
+      // offset inside it is clamped below 1 so that FP32 rounding cannot move
+      // the stencil to the next cell (the window-fit check counts cells in FP64)
+      const double c0 = floor(x0), c1 = floor(x1);
+      const int ai = wi + (int)c0, aj = wj + (int)c1;
+      if (ai - 2 < -1 || ai + 2 > L0 || aj - 2 < -1 || aj + 2 > L1) {  // stencil outside the window planes
+        set_err(ws, kErrWindowFit);
+        ok = false;
+      } else {
+        const float g0 = fminf((float)(x0 - c0), 0x1.fffffep-1f), g1 = fminf((float)(x1 - c1), 0x1.fffffep-1f);
+        const size_t o = (size_t)(aj + 1) * wp + (ai + 1);
+        const View32 vex{a.mEx + o, wp}, vey{a.mEy + o, wp}, vhx{a.mHx + o, wp}, vhy{a.mHy + o, wp};
+        const float E0 = gather_edge<ORDER>(vex, g0, g1, 0);
+        const float E1 = gather_edge<ORDER>(vey, g0, g1, 1);
+        const float Hf = gather_cell<ORDER>(SumView32{vhx, vhy}, g0, g1);
+        // hard-edge dipole at the absolute position of R1
+        const double X = a.org0 + ((double)ci + x0) * a.h0, Y = a.org1 + ((double)cj + x1) * a.h1;
+        const double dist = a.chh * (X - a.Lb) - a.shh * (Y - a.hw);
+        const float bext = (dist > 0.0 && dist < a.bwidth) ? (float)a.bz : 0.0f;
+        const float B = (float)kMu0 * Hf + 0.5f * bext;
+        // kick + rotation (PartBunch.cpp:366-383) on u - P
+        const float k0 = a.f1 * E0, k1 = a.f1 * E1;
+        const float du0 = d0 + k0, du1 = d1 + k1;
+        double U0, U1;
+        const float ru = rgam(P0, P1, du0, du1, U0, U1);
+        const float aa = a.f2 * B * ru;
+        const float sv0 = du0 + aa * (Pf1 + du1), sv1 = du1 - aa * (Pf0 + du0);  // s - P
+        const float cf = aa / (1.0f + aa * aa);
+        d0 = (sv0 + cf * (Pf1 + sv1)) + k0;
+        d1 = (sv1 - cf * (Pf0 + sv0)) + k1;
+        a.b.dpx[n] = d0; a.b.dpy[n] = d1;
+      }
+    }
+    int ni = 0, nj = 0;
+    double e0 = 0.0, e1 = 0.0;
+    float o0 = 0.0f, o1 = 0.0f;
+    if (ok) {
+      const float r = rgam(P0, P1, d0, d1, p0, p1);
+      w0 = half_drift(a.kh0, p0, r); w1 = half_drift(a.kh1, p1, r);
+      int nc;
+      store_pos(dadd(x0, w0), dadd(x1, w1), ci, cj, nc, o0, o1);  // R2
+      a.b.cell[n] = nc; a.b.ox[n] = o0; a.b.oy[n] = o1;
+      // the move ends at the stored (FP32-rounded) position, so that every
+      // move's current conserves charge for the positions the bunch holds
+      unpack(nc, ni, nj);
+      e0 = (double)(ni - ci) + (double)o0; e1 = (double)(nj - cj) + (double)o1;
+    }
+    // current deposit R0 -> R2 in cells from (ci, cj), FP64 weights, summed in
+    // the warp's tile
+    tile.template rebase<SMEM>(ok, ok ? wi + (int)floor(r00) : 0, ok ? wj + (int)floor(r01) : 0, win, L0, L1);
+    if (ok) {
+      if (!deposit_particle<ORDER>(a.jcomp, q, r00, r01, e0, e1, 0.0, 0.0, 1.0, 1.0, a.h0, a.h1, a.dt, sink))
+        overflow = true;
+      // boxes hold cell index + 0.5: only the cells are used, and a cell-relative
+      // coordinate added to a large index could round across a cell border
+      amn0 = fmin(amn0, cellc(ci, fmin(r00, e0))); amn1 = fmin(amn1, cellc(cj, fmin(r01, e1)));
+      amx0 = fmax(amx0, cellc(ci, fmax(r00, e0))); amx1 = fmax(amx1, cellc(cj, fmax(r01, e1)));
+      // next push gathers at (stored R2 - w) + w
+      const double n0 = cellc(ni, dadd(dsub((double)o0, w0), w0)), n1 = cellc(nj, dadd(dsub((double)o1, w1), w1));
+      bmn0 = fmin(bmn0, n0); bmn1 = fmin(bmn1, n1); bmx0 = fmax(bmx0, n0); bmx1 = fmax(bmx1, n1);
+    }
+  }
+  tile.template flush<SMEM>(win, L0, L1);
+  if (overflow) set_err(ws, kErrCrossings);
+  block_bbox(amn0, amn1, amx0, amx1, ws->bball);
+  block_bbox(bmn0, bmn1, bmx0, bmx1, ws->bb[1 - ws->cur]);
+  if (SMEM) {
+    if (tile.ti1 >= 0) {
+      atomicMin(&tb[0], tile.ti0); atomicMin(&tb[1], tile.tj0);
+      atomicMax(&tb[2], tile.ti1); atomicMax(&tb[3], tile.tj1);
+    }
+    __syncthreads();
+    const int i0 = tb[0], j0 = tb[1], i1 = tb[2], j1 = tb[3];
+    if (i1 >= i0) {
+      const int w = i1 - i0 + 1, cnt = w * (j1 - j0 + 1);
+      for (int k = threadIdx.x; k < cnt; k += blockDim.x) {
+        const int i = i0 + k % w, j = j0 + k / w;
+        const unsigned long long v = sacc[j * L0 + i];
+        if (v) atomicAdd(&a.acc[j * L0 + i], v);
+      }
+    }
+  }
+}
+
+// Gather-patch set-up and the window-fit check from the box of the next
+// push's gather positions (cells of the static mesh).
+__global__ void k_prep32(WinState *ws, int reach) {
+  if (threadIdx.x != 0) return;
+  const int c = ws->cur;
+  const double mn0 = ord_dbl(ws->bb[c][0]), mn1 = ord_dbl(ws->bb[c][1]);
+  const double mx0 = ord_dbl(ws->bb[c][2]), mx1 = ord_dbl(ws->bb[c][3]);
+  if (mn0 <= mx0) {
+    const int lp[4] = {(int)floor(mn0) - ws->P0, (int)floor(mx0) - ws->P0, (int)floor(mn1) - ws->P1,
+                       (int)floor(mx1) - ws->P1};
+    for (int k = 0; k < 4; ++k) ws->lp[k] = lp[k];
+    // every gather tap lies within [lp - reach, lp + reach]
+    if (lp[0] - reach < -1 || lp[1] + reach > ws->L0 || lp[2] - reach < -1 || lp[3] + reach > ws->L1)
+      set_err(ws, kErrWindowFit);
+  }
+  bbox_reset(ws->bb[1 - c]);
+  bbox_reset(ws->bball);
+}
+
+// Deposit bounds in window cells (PartBunch::getLocalPDomainInclOld).
+__global__ void k_bounds32(WinState *ws) {
+  if (threadIdx.x != 0) return;
+  const double mn0 = ord_dbl(ws->bball[0]), mn1 = ord_dbl(ws->bball[1]);
+  const double mx0 = ord_dbl(ws->bball[2]), mx1 = ord_dbl(ws->bball[3]);
+  if (!(mn0 <= mx0)) { ws->gb[0] = 0; ws->gb[1] = -1; ws->gb[2] = 0; ws->gb[3] = -1; return; }
+  ws->gb[0] = (int)floor(mn0) - ws->P0; ws->gb[1] = (int)floor(mx0) - ws->P0;
+  ws->gb[2] = (int)floor(mn1) - ws->P1; ws->gb[3] = (int)floor(mx1) - ws->P1;
+}
+
+__global__ void k_post32(WinState *ws) {
+  if (threadIdx.x == 0) ws->cur = 1 - ws->cur;
+}
+
+__global__ void k_bbox32_clear(WinState *ws) {
+  if (threadIdx.x == 0) bbox_reset(ws->bb[ws->cur]);
+}
+
+// Box of the next push's gather positions R1 = (R - w) + w or R + w.
+__global__ void k_bbox32(Bunch32 b, double P0, double P1, double kh0, double kh1, int pending, WinState *ws) {
+  double mn0 = INFINITY, mn1 = INFINITY, mx0 = -INFINITY, mx1 = -INFINITY;
+  for (long long n = gtid(); n < b.n; n += (long long)gridDim.x * blockDim.x) {
+    int ci, cj;
+    unpack(b.cell[n], ci, cj);
+    double p0, p1;
+    const float r = rgam(P0, P1, b.dpx[n], b.dpy[n], p0, p1);
+    const double w0 = half_drift(kh0, p0, r), w1 = half_drift(kh1, p1, r);
+    double s0 = b.ox[n], s1 = b.oy[n];
+    if (pending) { s0 = dsub(s0, w0); s1 = dsub(s1, w1); }
+    const double x0 = cellc(ci, dadd(s0, w0)), x1 = cellc(cj, dadd(s1, w1));
+    mn0 = fmin(mn0, x0); mn1 = fmin(mn1, x1); mx0 = fmax(mx0, x0); mx1 = fmax(mx1, x1);
+  }
+  block_bbox(mn0, mn1, mx0, mx1, ws->bb[ws->cur]);
+}
+
+// R += kd * v (cells), kd = dt c / h (PartBunch::drift_particles).
+__global__ void k_drift32(Bunch32 b, double P0, double P1, double kd0, double kd1) {
+  for (long long n = gtid(); n < b.n; n += (long long)gridDim.x * blockDim.x) {
+    int ci, cj;
+    unpack(b.cell[n], ci, cj);
+    double p0, p1;
+    const float r = rgam(P0, P1, b.dpx[n], b.dpy[n], p0, p1);
+    int nc;
+    float o0, o1;
+    store_pos(dadd((double)b.ox[n], half_drift(kd0, p0, r)), dadd((double)b.oy[n], half_drift(kd1, p1, r)), ci, cj,
+              nc, o0, o1);
+    b.cell[n] = nc; b.ox[n] = o0; b.oy[n] = o1;
+  }
+}
+
+__global__ void k_from64(const double *x, const double *y, const double *px, const double *py, const double *q,
+                         long long nn, double org0, double org1, double h0, double h1, double P0, double P1,
+                         Bunch32 b) {
+  for (long long n = gtid(); n < nn; n += (long long)gridDim.x * blockDim.x) {
+    int c;
+    float o0, o1;
+    store_pos((x[n] - org0) / h0, (y[n] - org1) / h1, 0, 0, c, o0, o1);
+    b.cell[n] = c; b.ox[n] = o0; b.oy[n] = o1;
+    b.dpx[n] = (float)(px[n] - P0);
+    b.dpy[n] = (float)(py[n] - P1);
+    b.q[n] = (float)q[n];
+  }
+}
+
+__global__ void k_to64(Bunch32 b, double P0, double P1, double kh0, double kh1, int pending, double org0,
+                       double org1, double h0, double h1, double *x, double *y, double *px, double *py) {
+  for (long long n = gtid(); n < b.n; n += (long long)gridDim.x * blockDim.x) {
+    int ci, cj;
+    unpack(b.cell[n], ci, cj);
+    double p0, p1;
+    const float r = rgam(P0, P1, b.dpx[n], b.dpy[n], p0, p1);
+    double s0 = b.ox[n], s1 = b.oy[n];
+    if (pending) { s0 = dsub(s0, half_drift(kh0, p0, r)); s1 = dsub(s1, half_drift(kh1, p1, r)); }
+    if (x) x[n] = org0 + ((double)ci + s0) * h0;
+    if (y) y[n] = org1 + ((double)cj + s1) * h1;
+    if (px) px[n] = p0;
+    if (py) py[n] = p1;
+  }
+}
+
+__global__ void k_psum2(const double *px, const double *py, long long n, double *part) {
+  __shared__ double sh[2][256];
+  double a = 0.0, c = 0.0;
+  for (long long k = blockIdx.x * 256ll + threadIdx.x; k < n; k += (long long)gridDim.x * 256) {
+    a += px[k]; c += py[k];
+  }
+  sh[0][threadIdx.x] = a; sh[1][threadIdx.x] = c;
+  __syncthreads();
+  for (int w = 128; w > 0; w >>= 1) {
+    if (threadIdx.x < w) { sh[0][threadIdx.x] += sh[0][threadIdx.x + w]; sh[1][threadIdx.x] += sh[1][threadIdx.x + w]; }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) { part[2 * blockIdx.x] = sh[0][0]; part[2 * blockIdx.x + 1] = sh[1][0]; }
+}
+
+__global__ void k_psum2_final(const double *part, int np, double *out) {
+  if (threadIdx.x != 0) return;
+  double a = 0.0, c = 0.0;
+  for (int k = 0; k < np; ++k) { a += part[2 * k]; c += part[2 * k + 1]; }
+  out[0] = a; out[1] = c;
+}
+
+template <class S, class D>
+__global__ void k_plane_copy(const S *src, int spitch, D *dst, int dpitch, int rows, int cols) {
+  const long long k = gtid();
+  if (k >= (long long)rows * cols) return;
+  const int r = (int)(k / cols), c = (int)(k % cols);
+  dst[(size_t)r * dpitch + c] = (D)src[(size_t)r * spitch + c];
+}
+
+inline unsigned grid_for(long long n, unsigned cap = 4096) {
+  const long long g = (n + 255) / 256;
+  return (unsigned)(g < 1 ? 1 : (g > cap ? cap : g));
+}
+
+template <int ORDER>
+long long smem_limit32() {
+  static long long lim = -1;
+  if (lim < 0) {
+    int dev = 0, v = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    cudaFuncAttributes fa{};
+    cudaFuncGetAttributes(&fa, k_push32<ORDER, true>);
+    lim = (long long)v - (long long)fa.sharedSizeBytes;
+    if (cudaFuncSetAttribute(k_push32<ORDER, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lim) !=
+        cudaSuccess)
+      lim = 0;
+    cudaGetLastError();
+  }
+  return lim;
+}
+
+template <int ORDER>
+void push32_order(const Push32Args &a, int L0, int L1, int grid, cudaStream_t s) {
+  const size_t tiles = (size_t)TileFor<ORDER>::T::kSize * 256 * sizeof(unsigned long long);
+  const size_t sm = (size_t)L0 * L1 * sizeof(unsigned long long) + tiles;
+  if (a.use_smem && (long long)sm <= smem_limit32<ORDER>())
+    k_push32<ORDER, true><<<grid, 256, sm, s>>>(a);
+  else
+    k_push32<ORDER, false><<<grid, 256, tiles, s>>>(a);
+}
+
+}  // namespace
+
+int launch_push32(const Push32Args &a, int order, int L0, int L1, int grid, cudaStream_t s) {
+  if (order == 0) push32_order<0>(a, L0, L1, grid, s);
+  else if (order == 1) push32_order<1>(a, L0, L1, grid, s);
+  else push32_order<2>(a, L0, L1, grid, s);
+  k_post32<<<1, 32, 0, s>>>(a.ws);
+  return 0;
+}
+
+void launch_prep32(WinState *ws, int order, cudaStream_t s) {
+  (void)order;
+  k_prep32<<<1, 32, 0, s>>>(ws, 2);
+}
+
+void launch_bounds32(WinState *ws, cudaStream_t s) { k_bounds32<<<1, 32, 0, s>>>(ws); }
+
+void launch_bbox32(const Bunch32 &b, double P0, double P1, double kh0, double kh1, int pending, WinState *ws,
+                   cudaStream_t s) {
+  k_bbox32_clear<<<1, 32, 0, s>>>(ws);
+  k_bbox32<<<grid_for(b.n, 1184), 256, 0, s>>>(b, P0, P1, kh0, kh1, pending, ws);
+}
+
+void launch_drift32(const Bunch32 &b, double P0, double P1, double kd0, double kd1, cudaStream_t s) {
+  if (b.n > 0) k_drift32<<<grid_for(b.n), 256, 0, s>>>(b, P0, P1, kd0, kd1);
+}
+
+void launch_from64(const double *x, const double *y, const double *px, const double *py, const double *q,
+                   long long n, double org0, double org1, double h0, double h1, double P0, double P1,
+                   const Bunch32 &b, cudaStream_t s) {
+  if (n > 0) k_from64<<<grid_for(n), 256, 0, s>>>(x, y, px, py, q, n, org0, org1, h0, h1, P0, P1, b);
+}
+
+void launch_to64(const Bunch32 &b, double P0, double P1, double kh0, double kh1, int pending, double org0,
+                 double org1, double h0, double h1, double *x, double *y, double *px, double *py,
+                 cudaStream_t s) {
+  if (b.n > 0)
+    k_to64<<<grid_for(b.n), 256, 0, s>>>(b, P0, P1, kh0, kh1, pending, org0, org1, h0, h1, x, y, px, py);
+}
+
+// Mean-momentum sums: part holds 2 x 296 doubles, out2 receives the two sums.
+void launch_psum(const double *px, const double *py, long long n, double *part, double *out2, cudaStream_t s) {
+  k_psum2<<<296, 256, 0, s>>>(px, py, n, part);
+  k_psum2_final<<<1, 32, 0, s>>>(part, 296, out2);
+}
+
+void launch_d2f(const double *src, int spitch, float *dst, int dpitch, int rows, int cols, cudaStream_t s) {
+  k_plane_copy<double, float><<<grid_for((long long)rows * cols, 1u << 30), 256, 0, s>>>(src, spitch, dst, dpitch,
+                                                                                        rows, cols);
+}
+
+void launch_f2d(const float *src, int spitch, double *dst, int dpitch, int rows, int cols, cudaStream_t s) {
+  k_plane_copy<float, double><<<grid_for((long long)rows * cols, 1u << 30), 256, 0, s>>>(src, spitch, dst, dpitch,
+                                                                                        rows, cols);
+}
+
+}  // namespace csrst

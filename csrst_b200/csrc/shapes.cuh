@@ -31,44 +31,47 @@ struct SumView {
 // --- gather -----------------------------------------------------------------
 
 // Edge component `comp` at patch coordinates (pp0, pp1) = (R - origin) / h.
-// ScatterGatherImpl.hh:69-104 (CIC), :201-253 (S1), :406-468 (S2).
-template <int ORDER, class F>
-__device__ __forceinline__ double gather_edge(const F &f, double pp0, double pp1, int comp) {
+// ScatterGatherImpl.hh:69-104 (CIC), :201-253 (S1), :406-468 (S2).  S is the
+// arithmetic type: double reproduces the reference bit for bit, float is the
+// FP32 mode's gather.
+template <int ORDER, class F, class S>
+__device__ __forceinline__ S gather_edge(const F &f, S pp0, S pp1, int comp) {
+  const S one = S(1), half = S(0.5), zero = S(0);
   if (ORDER == 0) {
-    long l0 = (long)floor(pp0 + (comp == 0 ? 0.5 : 0.0));
-    long l1 = (long)floor(pp1 + (comp == 1 ? 0.5 : 0.0));
+    long l0 = (long)floor(pp0 + (comp == 0 ? half : zero));
+    long l1 = (long)floor(pp1 + (comp == 1 ? half : zero));
     if (comp == 0) l0 -= 1; else l1 -= 1;
-    double g0 = (double)l0, g1 = (double)l1;
-    if (comp == 0) g0 += 0.5; else g1 += 0.5;
-    const double d0 = pp0 - g0, d1 = pp1 - g1;
+    S g0 = (S)l0, g1 = (S)l1;
+    if (comp == 0) g0 += half; else g1 += half;
+    const S d0 = pp0 - g0, d1 = pp1 - g1;
     const int I = (int)l0, J = (int)l1;
-    return ((1 - d1) * ((1 - d0) * f(I, J) + d0 * f(I + 1, J)) +
-            d1 * ((1 - d0) * f(I, J + 1) + d0 * f(I + 1, J + 1)));
+    return ((one - d1) * ((one - d0) * f(I, J) + d0 * f(I + 1, J)) +
+            d1 * ((one - d0) * f(I, J + 1) + d0 * f(I + 1, J + 1)));
   } else if (ORDER == 1) {
-    long l0 = (long)floor(pp0 + (comp == 0 ? 0.0 : 0.5));
-    long l1 = (long)floor(pp1 + (comp == 1 ? 0.0 : 0.5));
-    double g0 = (double)l0, g1 = (double)l1;
-    if (comp == 0) g0 += 0.5; else g1 += 0.5;
-    const double d0 = pp0 - g0, d1 = pp1 - g1;
-    const double bx = 0.75 - d0 * d0, cx = 0.5 * (0.5 + d0) * (0.5 + d0), ax = 1.0 - (bx + cx);
-    const double by = 0.75 - d1 * d1, cy = 0.5 * (0.5 + d1) * (0.5 + d1), ay = 1.0 - (by + cy);
+    long l0 = (long)floor(pp0 + (comp == 0 ? zero : half));
+    long l1 = (long)floor(pp1 + (comp == 1 ? zero : half));
+    S g0 = (S)l0, g1 = (S)l1;
+    if (comp == 0) g0 += half; else g1 += half;
+    const S d0 = pp0 - g0, d1 = pp1 - g1;
+    const S bx = S(0.75) - d0 * d0, cx = half * (half + d0) * (half + d0), ax = one - (bx + cx);
+    const S by = S(0.75) - d1 * d1, cy = half * (half + d1) * (half + d1), ay = one - (by + cy);
     const int I = (int)l0, J = (int)l1;
     return (ay * (ax * f(I - 1, J - 1) + bx * f(I, J - 1) + cx * f(I + 1, J - 1)) +
             by * (ax * f(I - 1, J) + bx * f(I, J) + cx * f(I + 1, J)) +
             cy * (ax * f(I - 1, J + 1) + bx * f(I, J + 1) + cx * f(I + 1, J + 1)));
   } else {
-    long l0 = (long)floor(pp0 + (comp == 0 ? 0.5 : 0.0));
-    long l1 = (long)floor(pp1 + (comp == 1 ? 0.5 : 0.0));
+    long l0 = (long)floor(pp0 + (comp == 0 ? half : zero));
+    long l1 = (long)floor(pp1 + (comp == 1 ? half : zero));
     if (comp == 0) l0 -= 1; else l1 -= 1;
-    double g0 = (double)l0, g1 = (double)l1;
-    if (comp == 0) g0 += 0.5; else g1 += 0.5;
-    const double d0 = pp0 - g0, d1 = pp1 - g1;
-    const double q0 = d0 * d0, q1 = d1 * d1;
-    const double t23 = 2.0 / 3.0, t16 = 1.0 / 6.0;
-    const double bx = t23 - q0 * (1 - 0.5 * d0), cx = t23 - 0.5 * (1 - d0) * (1 - q0), ex = t16 * q0 * d0;
-    const double ax = 1.0 - (bx + cx + ex);
-    const double by = t23 - q1 * (1 - 0.5 * d1), cy = t23 - 0.5 * (1 - d1) * (1 - q1), ey = t16 * q1 * d1;
-    const double ay = 1.0 - (by + cy + ey);
+    S g0 = (S)l0, g1 = (S)l1;
+    if (comp == 0) g0 += half; else g1 += half;
+    const S d0 = pp0 - g0, d1 = pp1 - g1;
+    const S q0 = d0 * d0, q1 = d1 * d1;
+    const S t23 = S(2.0 / 3.0), t16 = S(1.0 / 6.0);
+    const S bx = t23 - q0 * (one - half * d0), cx = t23 - half * (one - d0) * (one - q0), ex = t16 * q0 * d0;
+    const S ax = one - (bx + cx + ex);
+    const S by = t23 - q1 * (one - half * d1), cy = t23 - half * (one - d1) * (one - q1), ey = t16 * q1 * d1;
+    const S ay = one - (by + cy + ey);
     const int I = (int)l0, J = (int)l1;
     // The last term reads (I+1, J+2), as the reference does (ScatterGatherImpl.hh:467).
     return (ay * (ax * f(I - 1, J - 1) + bx * f(I, J - 1) + cx * f(I + 1, J - 1) + ex * f(I + 2, J - 1)) +
@@ -79,32 +82,33 @@ __device__ __forceinline__ double gather_edge(const F &f, double pp0, double pp1
 }
 
 // Cell-centred field.  ScatterGatherImpl.hh:106-134, :255-301, :470-527.
-template <int ORDER, class F>
-__device__ __forceinline__ double gather_cell(const F &f, double pp0, double pp1) {
+template <int ORDER, class F, class S>
+__device__ __forceinline__ S gather_cell(const F &f, S pp0, S pp1) {
+  const S one = S(1), half = S(0.5);
   if (ORDER == 0) {
-    const long l0 = (long)floor(pp0 - 0.5), l1 = (long)floor(pp1 - 0.5);
-    const double d0 = pp0 - (l0 + 0.5), d1 = pp1 - (l1 + 0.5);
+    const long l0 = (long)floor(pp0 - half), l1 = (long)floor(pp1 - half);
+    const S d0 = pp0 - ((S)l0 + half), d1 = pp1 - ((S)l1 + half);
     const int I = (int)l0, J = (int)l1;
-    return ((1 - d1) * ((1 - d0) * f(I, J) + d0 * f(I + 1, J)) +
-            d1 * ((1 - d0) * f(I, J + 1) + d0 * f(I + 1, J + 1)));
+    return ((one - d1) * ((one - d0) * f(I, J) + d0 * f(I + 1, J)) +
+            d1 * ((one - d0) * f(I, J + 1) + d0 * f(I + 1, J + 1)));
   } else if (ORDER == 1) {
     const long l0 = (long)floor(pp0), l1 = (long)floor(pp1);
-    const double d0 = pp0 - (l0 + 0.5), d1 = pp1 - (l1 + 0.5);
-    const double bx = 0.75 - d0 * d0, cx = 0.5 * (0.5 + d0) * (0.5 + d0), ax = 1.0 - (bx + cx);
-    const double by = 0.75 - d1 * d1, cy = 0.5 * (0.5 + d1) * (0.5 + d1), ay = 1.0 - (by + cy);
+    const S d0 = pp0 - ((S)l0 + half), d1 = pp1 - ((S)l1 + half);
+    const S bx = S(0.75) - d0 * d0, cx = half * (half + d0) * (half + d0), ax = one - (bx + cx);
+    const S by = S(0.75) - d1 * d1, cy = half * (half + d1) * (half + d1), ay = one - (by + cy);
     const int I = (int)l0, J = (int)l1;
     return (ay * (ax * f(I - 1, J - 1) + bx * f(I, J - 1) + cx * f(I + 1, J - 1)) +
             by * (ax * f(I - 1, J) + bx * f(I, J) + cx * f(I + 1, J)) +
             cy * (ax * f(I - 1, J + 1) + bx * f(I, J + 1) + cx * f(I + 1, J + 1)));
   } else {
-    const long l0 = (long)floor(pp0 - 0.5), l1 = (long)floor(pp1 - 0.5);
-    const double d0 = pp0 - (l0 + 0.5), d1 = pp1 - (l1 + 0.5);
-    const double q0 = d0 * d0, q1 = d1 * d1;
-    const double t23 = 2.0 / 3.0, t16 = 1.0 / 6.0;
-    const double bx = t23 - q0 * (1 - 0.5 * d0), cx = t23 - 0.5 * (1 - d0) * (1 - q0), ex = t16 * q0 * d0;
-    const double ax = 1.0 - (bx + cx + ex);
-    const double by = t23 - q1 * (1 - 0.5 * d1), cy = t23 - 0.5 * (1 - d1) * (1 - q1), ey = t16 * q1 * d1;
-    const double ay = 1.0 - (by + cy + ey);
+    const long l0 = (long)floor(pp0 - half), l1 = (long)floor(pp1 - half);
+    const S d0 = pp0 - ((S)l0 + half), d1 = pp1 - ((S)l1 + half);
+    const S q0 = d0 * d0, q1 = d1 * d1;
+    const S t23 = S(2.0 / 3.0), t16 = S(1.0 / 6.0);
+    const S bx = t23 - q0 * (one - half * d0), cx = t23 - half * (one - d0) * (one - q0), ex = t16 * q0 * d0;
+    const S ax = one - (bx + cx + ex);
+    const S by = t23 - q1 * (one - half * d1), cy = t23 - half * (one - d1) * (one - q1), ey = t16 * q1 * d1;
+    const S ay = one - (by + cy + ey);
     const int I = (int)l0, J = (int)l1;
     return (ay * (ax * f(I - 1, J - 1) + bx * f(I, J - 1) + cx * f(I + 1, J - 1) + ex * f(I + 2, J - 1)) +
             by * (ax * f(I - 1, J) + bx * f(I, J) + cx * f(I + 1, J) + ex * f(I + 2, J)) +
@@ -357,23 +361,28 @@ __device__ __forceinline__ bool segments_fast(double o0, double o1, double n0, d
 
 // Calls sink(i, j, value) for every current contribution of one particle
 // moving old -> new (absolute positions; the mesh origin is org; indices are
-// mesh cells).  Returns false on a crossing overflow.
+// mesh cells).  Returns false on a crossing overflow.  (h0, h1) is the
+// spacing of the coordinates given; (jh0, jh1) the physical spacing that
+// scales the current.  The FP64 path passes physical positions with
+// jh = h; FP32 mode passes positions in cells (h = 1).  Ratios of lengths
+// along one straight move do not depend on the units, so both give the
+// same current up to rounding.
 template <int ORDER, class Sink>
 __device__ __forceinline__ bool deposit_particle(int comp, double q, double ao0, double ao1, double an0,
                                                  double an1, double org0, double org1, double h0, double h1,
-                                                 double dt, Sink &&sink) {
+                                                 double jh0, double jh1, double dt, Sink &&sink) {
   // crossings are taken relative to the mesh origin (utils.hh:435-436)
   const double o0 = ao0 - org0, o1 = ao1 - org1, n0 = an0 - org0, n1 = an1 - org1;
   const double ood0 = 1.0 / h0, ood1 = 1.0 / h1;
   double oodt0, oodt1, dl0 = 0.0, dl1 = 0.0, cov = 0.0;
   if (ORDER == 0) {
-    oodt0 = 1.0 / (h1 * dt); oodt1 = 1.0 / (h0 * dt);
+    oodt0 = 1.0 / (jh1 * dt); oodt1 = 1.0 / (jh0 * dt);
   } else {
     // the full displacement uses the absolute positions (R - oldR)
     const double Dx0 = an0 - ao0, Dx1 = an1 - ao1;
     cov = sqrt(Dx0 * Dx0 + Dx1 * Dx1);
     if (cov == 0.0) return true;  // a particle that does not move carries no current
-    oodt0 = ood0 / dt; oodt1 = ood1 / dt;
+    oodt0 = (1.0 / jh0) / dt; oodt1 = (1.0 / jh1) / dt;
     dl0 = Dx0 * ood0; dl1 = Dx1 * ood1;
   }
   auto seg = [&](double a0, double a1, double b0, double b1) {

@@ -25,12 +25,20 @@ IntCIC, IntS1, IntS2 = 0, 1, 2
 class Simulation:
     """Owns one csrst handle: static mesh, moving window and bunch."""
 
-    def __init__(self, cfg, keep_old=False):
+    FLAG_KEEP_OLD = 1
+    FLAG_FP32 = 2
+
+    def __init__(self, cfg, keep_old=False, fp32=False):
+        """fp32: FP32 mode (FP32 fields, gather and kick; positions as FP32
+        offsets from FP64 cell origins; FP64 current deposit)."""
         c = Config()
         for k, v in cfg.dict().items():
             setattr(c, k, v)
         if keep_old:
-            c.flags |= 1
+            c.flags |= self.FLAG_KEEP_OLD
+        if fp32:
+            c.flags |= self.FLAG_FP32
+        self.fp32 = bool(c.flags & self.FLAG_FP32)
         self.cfg = cfg
         h = C.c_void_p()
         check(lib().csrst_create(C.byref(c), C.byref(h)))

@@ -37,13 +37,20 @@ extern "C" {
 
 typedef struct csrst_handle csrst_handle;
 
+/* csrst_config.flags */
+#define CSRST_FLAG_KEEP_OLD 1  /* keep oldR of every push for csrst_get_old_positions (FP64 only) */
+#define CSRST_FLAG_FP32 2      /* FP32 mode: FP32 fields, gather and kick; positions as FP32 offsets
+                                * from FP64 cell origins, momenta as FP32 deviations from an FP64
+                                * reference momentum; FP64 current deposit.  No reference
+                                * counterpart; checked against the FP64 path to a tolerance. */
+
 /* Run set-up.  Mirrors the command line of src/main.cpp:111-136 for the
  * parts the time step uses.  shape_order: 0 = IntCIC (ZerothOrderShapeFunction),
  * 1 = IntS1 / TSC (FirstOrderShapeFunction), 2 = IntS2 (SecondOrderShapeFunction). */
 typedef struct {
   int Nx, Ny;                 /* static mesh vertices per direction (-x, -y) */
   int shape_order;
-  int flags;                  /* reserved, 0 */
+  int flags;                  /* CSRST_FLAG_* bits, 0 = the FP64 path */
   double length_before;       /* drift before the bend [m] (--lengthbefore) */
   double length_after;        /* drift after the bend [m] (-l) */
   double width;               /* pipe width [m] (-w) */

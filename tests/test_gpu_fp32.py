@@ -1,0 +1,130 @@
+"""FP32 mode (CSRST_FLAG_FP32) against the FP64 GPU path, which is itself
+bit-exact to the oracle.
+
+FP32 mode has no reference counterpart.  Its bar: the longitudinal wake on
+the bunch within 1e-3 of the FP64 path's (relative to the wake's maximum);
+the current it deposits equal to the FP64 deposit of the same moves; the
+discrete continuity equation satisfied to 1e-10 relative, checked in FP64."""
+import numpy as np
+import pytest
+
+from csrst_b200 import ShapeFunction, Simulation, TETMSolver, moveMesh
+from csrst_b200.workloads import make_bunch, workload
+
+pytestmark = pytest.mark.gpu
+
+WAKE_TOL = 1e-3
+
+
+def run(name, fp32, steps, fields=True):
+    cfg, spec = workload(name)
+    s = Simulation(cfg, fp32=fp32)
+    s.load(*make_bunch(spec))
+    if fields:
+        s.initial_fields()
+    s.step(steps)
+    return s
+
+
+def wake_err(a, b):
+    ok = np.isfinite(a) & np.isfinite(b)
+    assert ok.sum() > 10
+    return np.abs(a[ok] - b[ok]).max() / np.abs(b[ok]).max()
+
+
+@pytest.mark.parametrize("name", ["small-0", "small-1", "small-2", "small-1-bend"])
+def test_fp32_wake_and_bunch_vs_fp64(gpu_lib, name):
+    steps = 60
+    # the initial-field solve covers the straight section before the bend
+    # (PoissonSolver::cutoffStencil): a bunch that starts in the dipole runs
+    # from zero fields
+    fields = "bend" not in name
+    s64, s32 = run(name, False, steps, fields), run(name, True, steps, fields)
+    assert s64.window()[0] == s32.window()[0]
+    err = wake_err(s32.wake(), s64.wake())
+    assert err <= WAKE_TOL, err
+    h = s64.info()["hx"]
+    p64, p32 = s64.particles(), s32.particles()
+    assert np.abs(p32[0] - p64[0]).max() < 1e-3 * h     # positions within 1e-3 cells
+    assert np.abs(p32[1] - p64[1]).max() < 1e-3 * h
+    m64, m32 = s64.moments(), s32.moments()
+    assert m32[14] == pytest.approx(m64[14], rel=1e-9)  # kinetic energy
+    assert abs(m32[15] - m64[15]) <= 1e-3 * abs(m64[15])  # energy spread
+    s64.close(); s32.close()
+
+
+def test_fp32_initial_fields_match_fp64(gpu_lib):
+    """FP32 mode solves in FP64 for its FP32-stored bunch and rounds the
+    fields once: they agree with the FP64 path's to FP32 precision."""
+    s64, s32 = run("small-1", False, 0), run("small-1", True, 0)
+    for a, b in zip(s32.get_static(), s64.get_static()):
+        assert np.abs(a - b).max() <= 1e-6 * np.abs(b).max()
+    s64.close(); s32.close()
+
+
+@pytest.mark.parametrize("order", [0, 1, 2])
+def test_fp32_deposit_matches_fp64_and_conserves_charge(gpu_lib, order):
+    """One FP32-mode push: its current equals the FP64 stand-alone deposit of
+    the same move (positions read back as FP64), and that move satisfies
+    rho_new - rho_old + dt div J = 0 to 1e-10 relative."""
+    name = f"small-{order}"
+    cfg, spec = workload(name)
+    s = run(name, True, 3)
+    info = s.info()
+    h, dt = (info["hx"], info["hy"]), info["dt"]
+    xo, yo, _, _ = s.particles()
+    s.push(0)
+    xn, yn, _, _ = s.particles()
+    w, org, _ = s.window()
+    L0, L1 = w[2], w[3]
+    jx_sim = s.window_field(4)[1:L1 + 1, 1:L0 + 1]
+    q = np.full(len(xo), np.float32(spec.charge / spec.n), dtype=np.float64)
+    sf = ShapeFunction(order)
+    scale = info["fixed_scale"]
+    jx = sf.getCurrentDensityBase(0, xo, yo, xn, yn, q, org, h, dt, 0, 0, L0, L1, scale)
+    jy = sf.getCurrentDensityBase(1, xo, yo, xn, yn, q, org, h, dt, 0, 0, L0, L1, scale)
+    assert np.abs(jx_sim - jx).max() <= 1e-9 * np.abs(jx).max()
+    qs = 2.0 ** np.floor(np.log2(2.0 ** 62 / (4 * np.abs(q).sum())))
+    rho = sf.getChargeDensityDiff(xo, yo, xn, yn, q, org, h, 0, 0, L0, L1, qs)
+    res = rho[1:, 1:] / dt + (jx[1:, 1:] - jx[1:, :-1]) / h[0] + (jy[1:, 1:] - jy[:-1, 1:]) / h[1]
+    assert np.abs(res).max() <= 1e-10 * np.abs(rho / dt).max()
+    s.close()
+
+
+def test_fp32_graph_matches_eager_and_reruns(gpu_lib):
+    cfg, spec = workload("small-1")
+    b = make_bunch(spec)
+    out = []
+    for eager in (False, True, False):
+        s = Simulation(cfg, fp32=True)
+        s.load(*b)
+        if eager:
+            solver = TETMSolver(s)
+            for _ in range(6):
+                solver.updateField_firstStep()
+                solver.updateField_secondStep()
+                moveMesh(s)
+        else:
+            s.step(6)
+        out.append(s.particles() + [s.window_field(k) for k in range(6)])
+        s.close()
+    for a, c, d in zip(*out):
+        assert np.array_equal(a, c) and np.array_equal(a, d)
+
+
+def test_fp32_full_size_c2(gpu_lib):
+    """The 8192 x 1024 / 4e6-particle TSC workload: FP32 wake within 1e-3 of
+    FP64 after 20 steps."""
+    s64, s32 = run("c2", False, 20), run("c2", True, 20)
+    assert wake_err(s32.wake(), s64.wake()) <= WAKE_TOL
+    s64.close(); s32.close()
+
+
+def test_fp32_rejects_keep_old_and_large_meshes(gpu_lib):
+    cfg, _ = workload("small-0")
+    with pytest.raises(Exception):
+        Simulation(cfg, fp32=True, keep_old=True)
+    big = workload("small-0")[0]
+    big.Nx = 40000
+    with pytest.raises(Exception):
+        Simulation(big, fp32=True)
