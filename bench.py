@@ -8,9 +8,12 @@ TE/TM field sub-steps on the static mesh, the cut cells and the moving
 window, their strip exchanges and the window move.
 
 Default workload: 8192 x 1024 static mesh at 5 um, 4e6 macro-particles,
-TSC (IntS1 gather + first-order deposit), CFL 0.5, FP64 (the plain FP64 GPU
-path).  Synthetic seeded bunch (Gaussian, sigma_s 50 um, sigma_x 20 um,
-energy spread 1e-4, 1 nC); zero initial fields.
+TSC (IntS1 gather + first-order deposit), CFL 0.5, in FP32 mode (FP32
+fields, gather and kick on FP32 offsets from FP64 cell origins, FP64
+deposit), with the plain FP64 GPU path timed beside it and the FP32 result
+checked against it (CSR wake, energy change per slice, continuity).
+Synthetic seeded bunch (Gaussian, sigma_s 50 um, sigma_x 20 um, energy
+spread 1e-4, 1 nC); initial fields from the GPU multigrid Poisson solve.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
 
@@ -37,11 +40,12 @@ if str(ROOT) not in sys.path:
 
 METRIC = "particle-steps/s, Yee cell-updates/s; FP32 vs FP64 GPU at ≤1e-3 CSR-wake err"
 UNIT = "particle-steps/s"
-# algorithmic bytes per unit (FP64): the fused Yee update reads and writes
-# Ex, Ey, Hzx, Hzy and reads a 1-byte mask per cell-step; a push streams
-# position and momentum in and out per particle.
-YEE_BYTES = 65
-PUSH_BYTES = 64
+# algorithmic bytes per unit: the fused Yee update reads and writes Ex, Ey,
+# Hzx, Hzy and reads a 1-byte mask per cell-step; a push streams position and
+# momentum in and out per particle (FP32 mode: 4-byte cell + two FP32 offsets
+# + two FP32 momentum deviations).
+YEE_BYTES = {"fp64": 65, "fp32": 33}
+PUSH_BYTES = {"fp64": 64, "fp32": 40}
 
 
 def parse():
@@ -53,6 +57,9 @@ def parse():
     p.add_argument("--workload", default="c2")
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--precision", default="fp32", choices=["fp32", "fp64"],
+                   help="mode of the headline value; the other mode is timed beside it")
+    p.add_argument("--no-compare", action="store_true", help="skip the other precision and the accuracy check")
     return p.parse_args()
 
 
@@ -123,32 +130,22 @@ class Clocks:
                 "sm_max_mhz": max(mx) if mx else None, "reasons": reasons, "samples": len(rows)}
 
 
-def run_b200(args, world, rank, local):
+def time_mode(args, cfg, bunch, world, fp32, clocks):
+    """One precision mode: initial fields, warm-up, the timed graph-captured
+    steps (max over ranks) and a per-group kernel attribution pass."""
     import torch
     from csrst_b200 import Simulation
-    from csrst_b200.workloads import make_bunch, workload
-
-    torch.cuda.set_device(local)
-    cfg, spec = workload(args.workload)
-    spec.seed += rank
-    bunch = make_bunch(spec)
-    n = spec.n
-    sim = Simulation(cfg)
+    sim = Simulation(cfg, fp32=fp32)
     sim.load(*bunch)
-    # initial fields of the bunch (PoissonSolver::computeField), one-time set-up
-    # before the loop; timed on its own
+    # initial fields of the bunch (PoissonSolver::computeField): one-time set-up, timed on its own
     t_if = time.perf_counter()
     rep = sim.initial_fields(1e-12, 1e-6, 500)
     t_if = time.perf_counter() - t_if
     stream = torch.cuda.ExternalStream(sim.stream())
-    # clocks are sampled from before the warm-up to the end of the kernel
-    # attribution pass: the GPU runs this workload the whole time
-    clocks = Clocks(local) if rank == 0 else None
     sim.step(args.warmup)
     sim.sync()
     if clocks:
         clocks.soak(sim)
-
     # ---- timed region: graph-captured steps, inputs resident in HBM ----
     if world > 1:
         torch.distributed.barrier()
@@ -165,16 +162,11 @@ def run_b200(args, world, rank, local):
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         ms = float(t.item())
         torch.distributed.barrier()
-    ms_step = ms / args.steps
-    value = world * n * args.steps / (ms * 1e-3)
-    cells = cfg.Nx * cfg.Ny
-
     # ---- kernel attribution: the same steps launched group by group ----
     groups = {"push": 0.0, "yee": 0.0, "move": 0.0}
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(8)]
     dt = sim.info()["dt"]
     ksteps = min(args.steps, 10)
-    sim.sync()
     for _ in range(ksteps):
         ev[0].record(stream); sim.push(0); ev[1].record(stream)
         sim.half_h(); sim.update_e(0); sim.half_h(); ev[2].record(stream)
@@ -189,52 +181,146 @@ def run_b200(args, world, rank, local):
         groups["move"] += ev[6].elapsed_time(ev[7])
     for k in groups:
         groups[k] /= ksteps
+    window = sim.window()[0][2:]
+    hx = sim.info()["hx"]
+    sim.close()
+    return {"ms": ms, "groups": groups, "window": window, "hx": hx,
+            "initial_fields": {"ms": round(1e3 * t_if, 2), "levels": rep["levels"],
+                               "iterations": [it for it, _ in rep["solves"]],
+                               "relres": [float("%.3g" % rr) for _, rr in rep["solves"]]}}
+
+
+def accuracy(cfg, spec, bunch, steps=50):
+    """FP32 mode against the FP64 path on identical inputs: the longitudinal
+    wake on the bunch axis, the energy change per slice, and the continuity
+    residual of one FP32-mode push (its Jx, the FP64 deposit's Jy of the same
+    move and the charge difference, in FP64)."""
+    from csrst_b200 import ShapeFunction, Simulation
+    res, sims = {}, {}
+    for fp32 in (False, True):
+        s = Simulation(cfg, fp32=fp32)
+        s.load(*bunch)
+        s.initial_fields(1e-12, 1e-6, 500)
+        g0 = np.sqrt(1 + s.particles()[2] ** 2 + s.particles()[3] ** 2)
+        s.step(steps)
+        x, y, px, py = s.particles()
+        m = s.moments()
+        res[fp32] = {"wake": s.wake(), "x": x, "y": y, "dg": np.sqrt(1 + px * px + py * py) - g0, "m": m}
+        sims[fp32] = s
+    a, b = res[True], res[False]
+    ok = np.isfinite(a["wake"]) & np.isfinite(b["wake"])
+    wake_err = float(np.abs(a["wake"][ok] - b["wake"][ok]).max() / np.abs(b["wake"][ok]).max())
+    # energy change per slice along the bunch axis (32 slices over +-3 sigma, FP64 positions)
+    m = b["m"]
+    c, sn = m[2] / math.hypot(m[2], m[3]), m[3] / math.hypot(m[2], m[3])
+    sl = (b["x"] - m[0]) * c + (b["y"] - m[1]) * sn
+    edges = np.linspace(-3 * spec.sigma_s, 3 * spec.sigma_s, 33)
+    idx = np.clip(np.digitize(sl, edges) - 1, 0, 31)
+    cnt = np.bincount(idx, minlength=32)
+    de64 = np.bincount(idx, b["dg"], minlength=32) / np.maximum(cnt, 1)
+    de32 = np.bincount(idx, a["dg"], minlength=32) / np.maximum(cnt, 1)
+    slice_err = float(np.abs(de32 - de64).max() / max(np.abs(de64).max(), 1e-300))
+    # continuity residual of one FP32-mode push
+    s = sims[True]
+    info = s.info()
+    h, dt = (info["hx"], info["hy"]), info["dt"]
+    xo, yo, _, _ = s.particles()
+    s.push(0)
+    xn, yn, _, _ = s.particles()
+    w, org, _ = s.window()
+    L0, L1 = w[2], w[3]
+    jx = s.window_field(4)[1:L1 + 1, 1:L0 + 1]
+    q = np.full(len(xo), np.float32(spec.charge / spec.n), dtype=np.float64)
+    sf = ShapeFunction(cfg.shape_order)
+    jy = sf.getCurrentDensityBase(1, xo, yo, xn, yn, q, org, h, dt, 0, 0, L0, L1, info["fixed_scale"])
+    qs = 2.0 ** np.floor(np.log2(2.0 ** 62 / (4 * np.abs(q).sum())))
+    rho = sf.getChargeDensityDiff(xo, yo, xn, yn, q, org, h, 0, 0, L0, L1, qs)
+    r = rho[1:, 1:] / dt + (jx[1:, 1:] - jx[1:, :-1]) / h[0] + (jy[1:, 1:] - jy[:-1, 1:]) / h[1]
+    cont = float(np.abs(r).max() / np.abs(rho / dt).max())
+    for v in sims.values():
+        v.close()
+    return {"steps": steps, "wake_rel_err": float("%.3g" % wake_err),
+            "energy_change_per_slice_rel_err": float("%.3g" % slice_err),
+            "energy_change_per_slice_mev_fp64": [float("%.4g" % (0.511 * v)) for v in de64[8:24]],
+            "continuity_residual_rel": float("%.3g" % cont),
+            "bar": "wake <= 1e-3 of the FP64 path's maximum; continuity <= 1e-10 (FP64 check)"}
+
+
+def run_b200(args, world, rank, local):
+    import torch
+    from csrst_b200.workloads import make_bunch, workload
+
+    torch.cuda.set_device(local)
+    cfg, spec = workload(args.workload)
+    spec.seed += rank
+    bunch = make_bunch(spec)
+    n = spec.n
+    cells = cfg.Nx * cfg.Ny
+    head = args.precision
+    # clocks are sampled from before the first warm-up to the end of the last
+    # attribution pass: the GPU runs this workload the whole time
+    clocks = Clocks(local) if rank == 0 else None
+    runs = {head: time_mode(args, cfg, bunch, world, head == "fp32", clocks)}
+    other = "fp64" if head == "fp32" else "fp32"
+    if not args.no_compare:
+        runs[other] = time_mode(args, cfg, bunch, world, other == "fp32", clocks)
     clk = clocks.stop() if clocks else None
     hbm, src = peaks()
 
-    def roof(key, bytes_step, ms_):
+    def roof(key, prec, bytes_step, ms_):
         ach = bytes_step / (ms_ * 1e-3) / 1e9
-        tr = profile_traffic(f"{key},{args.workload},fp64")
+        tr = profile_traffic(f"{key},{args.workload},{prec}")
         return {"kernel": key, "bound": "hbm", "achieved": round(ach, 1), "peak": hbm, "unit": "GB/s",
                 "frac": round(ach / hbm, 4), "traffic": tr, "peak_source": f"{src} hbm_gbs",
                 "algorithmic_bytes_per_step": bytes_step, "ms_per_step": round(ms_, 4)}
 
-    r_yee = roof("yee", YEE_BYTES * cells, groups["yee"])
-    r_push = roof("push", 2 * PUSH_BYTES * n, groups["push"])
-    dominant, other = (r_yee, r_push) if groups["yee"] >= groups["push"] else (r_push, r_yee)
+    def summary(prec):
+        r = runs[prec]
+        g = r["groups"]
+        r_yee = roof("yee", prec, YEE_BYTES[prec] * cells, g["yee"])
+        r_push = roof("push", prec, 2 * PUSH_BYTES[prec] * n, g["push"])
+        dom, oth = (r_yee, r_push) if g["yee"] >= g["push"] else (r_push, r_yee)
+        return {"value": round(world * n * args.steps / (r["ms"] * 1e-3), 1),
+                "ms_per_step": round(r["ms"] / args.steps, 4),
+                "cell_updates_per_s": round(world * cells * args.steps / (r["ms"] * 1e-3), 1),
+                "roofline": dom, "roofline_other": oth,
+                "kernel_ms_per_step": {k: round(v, 4) for k, v in g.items()},
+                "initial_fields": dict(r["initial_fields"],
+                                       what="one-time set-up, not in the timed steps: 3 MG-PCG solves on the "
+                                            f"{cfg.Nx}x{cfg.Ny} mesh incl. charge deposits and host round trips")}
 
-    out = {"metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world,
-           "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_step, 4),
-           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+    hs = summary(head)
+    dtype = "f32 (fields, gather, kick) + f64 (deposit)" if head == "fp32" else "f64"
+    out = {"metric": METRIC, "value": hs["value"], "unit": UNIT, "n_gpus": world,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": hs["ms_per_step"],
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": dtype,
            "data": "synthetic (seeded Gaussian bunch; initial fields from the GPU multigrid Poisson solve)",
-           "config": {"workload": f"{args.workload}: {cfg.Nx}x{cfg.Ny} static mesh, h={1e6 * sim.info()['hx']:.3g}um,"
-                                  f" {n} particles, shape order {cfg.shape_order}, CFL 0.5, FP64",
+           "config": {"workload": f"{args.workload}: {cfg.Nx}x{cfg.Ny} static mesh, h={1e6 * runs[head]['hx']:.3g}um,"
+                                  f" {n} particles, shape order {cfg.shape_order}, CFL 0.5, {head.upper()}",
                       "Nx": cfg.Nx, "Ny": cfg.Ny, "particles": n, "shape_order": cfg.shape_order,
-                      "window": sim.window()[0][2:], "precision": "fp64", "parallelism": f"replicas x{world}",
-                      "l2": "inputs larger than L2 (fields 4 x %.0f MB, particles %.0f MB)" % (
-                          cells * 8 / 1e6, n * 40 / 1e6)},
-           "cell_updates_per_s": round(world * cells * args.steps / (ms * 1e-3), 1),
-           "roofline": dominant, "roofline_other": other,
-           "kernel_ms_per_step": {k: round(v, 4) for k, v in groups.items()},
-           "initial_fields": {"ms": round(1e3 * t_if, 2), "levels": rep["levels"],
-                              "iterations": [it for it, _ in rep["solves"]],
-                              "relres": [float("%.3g" % rr) for _, rr in rep["solves"]],
-                              "what": "one-time set-up, not in the timed steps: 3 MG-PCG solves on the "
-                                      f"{cfg.Nx}x{cfg.Ny} mesh incl. charge deposits and host round trips"},
+                      "window": runs[head]["window"], "precision": head, "parallelism": f"replicas x{world}",
+                      "l2": "inputs larger than L2 (static fields 4 x %.0f MB, particles %.0f MB)" % (
+                          cells * (4 if head == "fp32" else 8) / 1e6, n * (24 if head == "fp32" else 40) / 1e6)},
+           "cell_updates_per_s": hs["cell_updates_per_s"],
+           "roofline": hs["roofline"], "roofline_other": hs["roofline_other"],
+           "kernel_ms_per_step": hs["kernel_ms_per_step"], "initial_fields": hs["initial_fields"],
            "clocks": clk}
+    if other in runs:
+        out[other] = summary(other)
+        out[f"{head}_over_{other}"] = round(hs["value"] / out[other]["value"], 3)
     # launches per step: 2 pushes x (prep, push, post, bounds) + 4 sub-steps x
     # (sweep, exchange) + move
     out["gpu_launches"] = args.steps * (2 * 4 + 4 * 2 + 1)
-    sim.close()
-
+    if rank == 0 and not args.no_compare:
+        out["accuracy_fp32_vs_fp64"] = accuracy(cfg, spec, bunch)
     if not args.no_e2e:
-        out["e2e"] = run_e2e(args, cfg, spec, bunch, rank, world)
+        out["e2e"] = run_e2e(args, cfg, spec, bunch, rank, world, head == "fp32")
     if rank == 0 and world == 1 and not args.no_cpu:
         out["cpu_baseline"] = cpu_baseline(cfg, spec, bunch)
     return out if rank == 0 else None
 
 
-def run_e2e(args, cfg, spec, bunch, rank, world):
+def run_e2e(args, cfg, spec, bunch, rank, world, fp32):
     """The same metric through the C ABI with host buffers: the bunch goes
     up from pinned host memory, every step returns the beam moments to the
     host, and the bunch comes back at the end."""
@@ -243,8 +329,7 @@ def run_e2e(args, cfg, spec, bunch, rank, world):
     n = spec.n
     pinned = [torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy() for a in bunch]
     outp = [torch.empty(n, dtype=torch.float64).pin_memory().numpy() for _ in range(4)]
-    sim = Simulation(cfg)
-    stream = torch.cuda.ExternalStream(sim.stream())
+    sim = Simulation(cfg, fp32=fp32)
     if world > 1:
         torch.distributed.barrier()
     torch.cuda.synchronize()
