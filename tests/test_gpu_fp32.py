@@ -128,3 +128,30 @@ def test_fp32_rejects_keep_old_and_large_meshes(gpu_lib):
     big.Nx = 40000
     with pytest.raises(Exception):
         Simulation(big, fp32=True)
+
+
+def test_fp32_energy_change_per_slice_in_the_dipole(gpu_lib):
+    """A bunch entering the dipole loses energy to CSR; FP32 mode's energy
+    change per slice stays within 1e-3 of the FP64 path's after 200 steps."""
+    cfg, spec = workload("small-1-bend")
+    b = make_bunch(spec)
+    dg, pos = {}, None
+    for fp32 in (False, True):
+        s = Simulation(cfg, fp32=fp32)
+        s.load(*b)
+        _, _, px, py = s.particles()
+        g0 = np.sqrt(1 + px * px + py * py)
+        s.step(200)
+        x, y, px, py = s.particles()
+        dg[fp32] = np.sqrt(1 + px * px + py * py) - g0
+        if not fp32:
+            pos = (x, s.moments())
+        s.close()
+    x, m = pos
+    edges = np.linspace(m[0] - 3 * spec.sigma_s, m[0] + 3 * spec.sigma_s, 17)
+    idx = np.clip(np.digitize(x, edges) - 1, 0, 15)
+    cnt = np.maximum(np.bincount(idx, minlength=16), 1)
+    e64 = np.bincount(idx, dg[False], minlength=16) / cnt
+    e32 = np.bincount(idx, dg[True], minlength=16) / cnt
+    assert np.abs(e64).max() > 0
+    assert np.abs(e32 - e64).max() <= 1e-3 * np.abs(e64).max()
