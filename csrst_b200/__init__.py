@@ -5,6 +5,6 @@ the C ABI of include/csrst.h; this package is the host-side mirror of the
 reference's TETMSolver / PartBunch / ScatterGatherImpl interfaces.
 """
 from ._lib import CsrstError, lib  # noqa: F401
-from .pic import (IntCIC, IntS1, IntS2, PartBunch, ScatterGatherImpl, ShapeFunction,  # noqa: F401
+from .pic import (Ensemble, IntCIC, IntS1, IntS2, PartBunch, ScatterGatherImpl, ShapeFunction,  # noqa: F401
                   PoissonSolver, Simulation, TETMSolver, moveMesh)
 from .workloads import BunchSpec, RunConfig, bend_config, make_bunch, workload  # noqa: F401

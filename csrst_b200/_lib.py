@@ -60,6 +60,14 @@ def lib():
         "csrst_reset_outside": ([P], C.c_int),
         "csrst_load_particles": ([P, D, D, D, D, D, C.c_size_t], C.c_int),
         "csrst_initial_fields": ([P, C.c_double, C.c_double, C.c_int, D], C.c_int),
+        "csrst_ensemble_create": ([C.POINTER(P), C.c_int, C.POINTER(P)], C.c_int),
+        "csrst_ensemble_destroy": ([P], C.c_int),
+        "csrst_ensemble_get_error": ([P, C.c_char_p, C.c_size_t], C.c_int),
+        "csrst_ensemble_stream": ([P], C.c_void_p),
+        "csrst_ensemble_step": ([P, C.c_int], C.c_int),
+        "csrst_ensemble_sync": ([P, I], C.c_int),
+        "csrst_ensemble_set_shape": ([P, C.c_int, C.c_int, C.c_int], C.c_int),
+        "csrst_ensemble_tune": ([P, C.c_int, D, C.c_int, I], C.c_int),
         "csrst_get_particles": ([P, D, D, D, D], C.c_int),
         "csrst_get_old_positions": ([P, D, D], C.c_int),
         "csrst_get_window": ([P, I, D, I], C.c_int),

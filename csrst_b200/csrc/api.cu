@@ -107,6 +107,36 @@ struct csrst_handle {
   double *d64 = nullptr;      // 4 n doubles: the bunch in FP64 for diagnostics and reads
 };
 
+// A batch of members stepped together: per-member argument tables in device
+// memory, one launch per phase of the time step for all members, and the
+// whole step captured as one CUDA graph.
+struct csrst_ensemble {
+  std::vector<csrst_handle *> mem;
+  int m = 0;
+  bool fp32 = false;
+  cudaStream_t s = nullptr;
+  cudaEvent_t done = nullptr;
+  // device tables (one entry per member)
+  PushArgs *push64[2] = {nullptr, nullptr};
+  Push32Args *push32[2] = {nullptr, nullptr};
+  FieldArgs *f64[2] = {nullptr, nullptr};
+  FieldArgsT<float> *f32[2] = {nullptr, nullptr};
+  MoveArgs<double> *mv64 = nullptr;
+  MoveArgs<float> *mv32 = nullptr;
+  PrepArgs *prep = nullptr;
+  int *order = nullptr;
+  unsigned char *smem_ok = nullptr;
+  long long *ppre = nullptr;
+  int *bpre_sub = nullptr, *bpre_ex[3] = {nullptr, nullptr, nullptr};
+  int nsub = 0, nex[3] = {0, 0, 0};
+  long long total = 0;
+  size_t push_smem = 0;
+  // launch shapes (set by csrst_ensemble_tune)
+  int push_grid = 0, tx = 32, ty = 8;
+  cudaGraphExec_t graph = nullptr;
+  std::string err;
+};
+
 namespace {
 
 int fail(csrst_handle *h, int code, const std::string &msg) {
@@ -1004,6 +1034,344 @@ int csrst_diag_wake(csrst_handle *h, double *out, int n) {
   CK(cudaFreeAsync(d, h->s));
   CK(cudaStreamSynchronize(h->s));
   return check_err(h);
+}
+
+// ---- batched ensemble ----
+
+}  // extern "C"
+
+namespace {
+
+template <class T>
+T *dev_copy(const std::vector<T> &v, cudaError_t &e) {
+  T *p = nullptr;
+  if (e == cudaSuccess) e = cudaMalloc(&p, (v.empty() ? 1 : v.size()) * sizeof(T));
+  if (e == cudaSuccess && !v.empty()) e = cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice);
+  return p;
+}
+
+void ensemble_free_tables(csrst_ensemble *e) {
+  for (int k = 0; k < 2; ++k) {
+    cudaFree(e->push64[k]); cudaFree(e->push32[k]); cudaFree(e->f64[k]); cudaFree(e->f32[k]);
+    e->push64[k] = nullptr; e->push32[k] = nullptr; e->f64[k] = nullptr; e->f32[k] = nullptr;
+  }
+  cudaFree(e->mv64); cudaFree(e->mv32); cudaFree(e->prep); cudaFree(e->order); cudaFree(e->smem_ok);
+  cudaFree(e->ppre); cudaFree(e->bpre_sub);
+  for (int k = 0; k < 3; ++k) { cudaFree(e->bpre_ex[k]); e->bpre_ex[k] = nullptr; }
+  e->mv64 = nullptr; e->mv32 = nullptr; e->prep = nullptr; e->order = nullptr; e->smem_ok = nullptr;
+  e->ppre = nullptr; e->bpre_sub = nullptr;
+  if (e->graph) { cudaGraphExecDestroy(e->graph); e->graph = nullptr; }
+}
+
+int efail(csrst_ensemble *e, int code, const std::string &msg) {
+  if (e) e->err = msg;
+  else g_create_error = msg;
+  return code;
+}
+
+// Argument tables of the steady-state step (pending drift, current boxes).
+int ensemble_build(csrst_ensemble *e) {
+  ensemble_free_tables(e);
+  const int m = e->m;
+  std::vector<PushArgs> p64[2];
+  std::vector<Push32Args> p32[2];
+  std::vector<FieldArgs> a64[2];
+  std::vector<FieldArgsT<float>> a32[2];
+  std::vector<MoveArgs<double>> mv64;
+  std::vector<MoveArgs<float>> mv32;
+  std::vector<PrepArgs> prep;
+  std::vector<int> order, bsub(1, 0), bex[3];
+  std::vector<unsigned char> ok;
+  std::vector<long long> ppre(1, 0);
+  for (int k = 0; k < 3; ++k) bex[k].assign(1, 0);
+  const long long cap = e->fp32 ? push32_batch_smem_limit() : push_batch_smem_limit();
+  size_t smem = 0;
+  for (csrst_handle *h : e->mem) {
+    order.push_back(h->order);
+    prep.push_back(prep_args(h->ws, h->b.hr0, h->b.hr1, h->order));
+    ppre.push_back(ppre.back() + h->n);
+    const size_t tiles = push_tile_bytes(h->order);
+    const size_t need = (size_t)h->L0 * h->L1 * sizeof(unsigned long long) + tiles;
+    const bool fits = (long long)need <= cap;
+    ok.push_back(fits ? 1 : 0);
+    smem = std::max(smem, fits ? need : tiles);
+    int nb = 0;
+    for (int c = 0; c < 2; ++c) {
+      if (e->fp32) {
+        FieldArgsT<float> a = field_args32(h, c);
+        a.tx = e->tx; a.ty = e->ty;
+        nb = sub_grid(a);
+        a32[c].push_back(a);
+        Push32Args pa = push_args32(h, c);
+        pa.pending = 1;
+        p32[c].push_back(pa);
+      } else {
+        FieldArgs a = field_args(h, c);
+        a.tx = e->tx; a.ty = e->ty;
+        nb = sub_grid(a);
+        a64[c].push_back(a);
+        PushArgs pa = push_args(h, c);
+        pa.pending = 1;
+        p64[c].push_back(pa);
+      }
+    }
+    if (e->fp32) mv32.push_back(MoveArgs<float>{a32[0].back(), h->scratchf, h->b.hr0, h->b.hr1});
+    else mv64.push_back(MoveArgs<double>{a64[0].back(), h->scratch, h->b.hr0, h->b.hr1});
+    bsub.push_back(bsub.back() + nb);
+    for (int k = 0; k < 3; ++k) bex[k].push_back(bex[k].back() + (exchange_count(h->L0, h->L1, k) + 127) / 128);
+  }
+  cudaError_t err = cudaSuccess;
+  for (int c = 0; c < 2; ++c) {
+    if (e->fp32) { e->push32[c] = dev_copy(p32[c], err); e->f32[c] = dev_copy(a32[c], err); }
+    else { e->push64[c] = dev_copy(p64[c], err); e->f64[c] = dev_copy(a64[c], err); }
+  }
+  if (e->fp32) e->mv32 = dev_copy(mv32, err);
+  else e->mv64 = dev_copy(mv64, err);
+  e->prep = dev_copy(prep, err);
+  e->order = dev_copy(order, err);
+  e->smem_ok = dev_copy(ok, err);
+  e->ppre = dev_copy(ppre, err);
+  e->bpre_sub = dev_copy(bsub, err);
+  for (int k = 0; k < 3; ++k) { e->bpre_ex[k] = dev_copy(bex[k], err); e->nex[k] = bex[k].back(); }
+  if (err != cudaSuccess) return efail(e, CSRST_E_CUDA, std::string("ensemble tables: ") + cudaGetErrorString(err));
+  e->nsub = bsub.back();
+  e->total = ppre.back();
+  e->push_smem = smem;
+  if (e->push_grid <= 0) {
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    e->push_grid = 2 * sms;
+  }
+  return CSRST_OK;
+}
+
+void ensemble_push(csrst_ensemble *e, int jcomp) {
+  if (e->fp32)
+    launch_push32_batch(e->push32[jcomp], e->order, e->smem_ok, e->ppre, e->m, e->total, e->push_grid,
+                        e->push_smem, e->prep, e->s);
+  else
+    launch_push_batch(e->push64[jcomp], e->order, e->smem_ok, e->ppre, e->m, e->total, e->push_grid, e->push_smem,
+                      e->prep, e->s);
+}
+
+template <class T>
+void ensemble_fields(csrst_ensemble *e, const FieldArgsT<T> *a0, const FieldArgsT<T> *a1, const MoveArgs<T> *mv,
+                     int part) {
+  if (part == 0) {  // half H, Ex, half H (after the first push)
+    launch_half_h_batch(a0, e->bpre_sub, e->m, e->nsub, e->s);
+    launch_exchange_batch(a0, e->bpre_ex[0], e->m, e->nex[0], 0, e->s);
+    launch_update_e_batch(a0, e->bpre_sub, e->m, e->nsub, 0, e->s);
+    launch_exchange_batch(a0, e->bpre_ex[1], e->m, e->nex[1], 1, e->s);
+    launch_half_h_batch(a0, e->bpre_sub, e->m, e->nsub, e->s);
+    launch_exchange_batch(a0, e->bpre_ex[0], e->m, e->nex[0], 0, e->s);
+  } else {          // Ey (after the second push), then the window move
+    launch_update_e_batch(a1, e->bpre_sub, e->m, e->nsub, 1, e->s);
+    launch_exchange_batch(a1, e->bpre_ex[2], e->m, e->nex[2], 2, e->s);
+    launch_move_batch(mv, e->m, e->s);
+  }
+}
+
+// One steady-state time step of every member (main.cpp:390-506).
+void ensemble_step_async(csrst_ensemble *e) {
+  ensemble_push(e, 0);
+  if (e->fp32) ensemble_fields(e, e->f32[0], e->f32[1], e->mv32, 0);
+  else ensemble_fields(e, e->f64[0], e->f64[1], e->mv64, 0);
+  ensemble_push(e, 1);
+  if (e->fp32) ensemble_fields(e, e->f32[0], e->f32[1], e->mv32, 1);
+  else ensemble_fields(e, e->f64[0], e->f64[1], e->mv64, 1);
+}
+
+// Brings every member to the steady state of the loop (the stored positions
+// owe the trailing drift, the box of the next gather positions is current)
+// with single-member steps, then hands the members to the ensemble stream.
+int ensemble_steady(csrst_ensemble *e, int &nsteps) {
+  while (nsteps > 0) {
+    bool all = true;
+    for (csrst_handle *h : e->mem) all = all && h->pending && h->bb == kBBValid;
+    if (all) break;
+    for (csrst_handle *h : e->mem) step_async(h);
+    --nsteps;
+  }
+  for (csrst_handle *h : e->mem) {
+    cudaError_t c = cudaStreamSynchronize(h->s);
+    if (c != cudaSuccess) return efail(e, CSRST_E_CUDA, std::string("member stream: ") + cudaGetErrorString(c));
+  }
+  return CSRST_OK;
+}
+
+void ensemble_mark(csrst_ensemble *e) {
+  for (csrst_handle *h : e->mem) {
+    h->pending = true;
+    h->bb = kBBValid;
+    h->fresh = false;
+    h->acc_fresh[0] = h->acc_fresh[1] = false;
+  }
+}
+
+// Member streams wait for the ensemble's work before anything else.
+int ensemble_release(csrst_ensemble *e) {
+  cudaError_t c = cudaEventRecord(e->done, e->s);
+  for (csrst_handle *h : e->mem)
+    if (c == cudaSuccess) c = cudaStreamWaitEvent(h->s, e->done, 0);
+  if (c != cudaSuccess) return efail(e, CSRST_E_CUDA, std::string("ensemble release: ") + cudaGetErrorString(c));
+  return CSRST_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int csrst_ensemble_create(csrst_handle *const *members, int m, csrst_ensemble **out) {
+  if (!out || !members || m <= 0) return efail(nullptr, CSRST_E_ARG, "ensemble: no members");
+  *out = nullptr;
+  csrst_ensemble *e = new csrst_ensemble;
+  e->m = m;
+  for (int k = 0; k < m; ++k) {
+    csrst_handle *h = members[k];
+    if (!h || h->n <= 0 || !(h->win || h->winf)) {
+      delete e;
+      return efail(nullptr, CSRST_E_NO_PARTICLES, "ensemble: member " + std::to_string(k) + " has no bunch");
+    }
+    if (k > 0 && h->fp32 != e->fp32) {
+      delete e;
+      return efail(nullptr, CSRST_E_ARG, "ensemble: members must share one precision mode");
+    }
+    if (h->cfg.flags & CSRST_FLAG_KEEP_OLD) {
+      delete e;
+      return efail(nullptr, CSRST_E_ARG, "ensemble: CSRST_FLAG_KEEP_OLD members cannot be batched");
+    }
+    e->fp32 = h->fp32;
+    e->mem.push_back(h);
+  }
+  if (cudaStreamCreateWithFlags(&e->s, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&e->done, cudaEventDisableTiming) != cudaSuccess) {
+    csrst_ensemble_destroy(e);
+    return efail(nullptr, CSRST_E_CUDA, "ensemble: stream");
+  }
+  const int rc = ensemble_build(e);
+  if (rc) {
+    g_create_error = e->err;
+    csrst_ensemble_destroy(e);
+    return rc;
+  }
+  *out = e;
+  return CSRST_OK;
+}
+
+int csrst_ensemble_destroy(csrst_ensemble *e) {
+  if (!e) return CSRST_OK;
+  if (e->s) cudaStreamSynchronize(e->s);
+  ensemble_free_tables(e);
+  if (e->done) cudaEventDestroy(e->done);
+  if (e->s) cudaStreamDestroy(e->s);
+  delete e;
+  return CSRST_OK;
+}
+
+int csrst_ensemble_get_error(const csrst_ensemble *e, char *buf, size_t len) {
+  if (!buf || len == 0) return CSRST_E_ARG;
+  std::snprintf(buf, len, "%s", (e ? e->err : g_create_error).c_str());
+  return CSRST_OK;
+}
+
+void *csrst_ensemble_stream(csrst_ensemble *e) { return e ? (void *)e->s : nullptr; }
+
+int csrst_ensemble_step(csrst_ensemble *e, int nsteps) {
+  if (!e || nsteps < 0) return efail(e, CSRST_E_ARG, "ensemble step: invalid arguments");
+  int rc = ensemble_steady(e, nsteps);
+  if (rc) return rc;
+  if (nsteps > 0) {
+    if (!e->graph) {
+      cudaGraph_t g;
+      if (cudaStreamBeginCapture(e->s, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+        return efail(e, CSRST_E_CUDA, "ensemble graph capture");
+      ensemble_step_async(e);
+      if (cudaStreamEndCapture(e->s, &g) != cudaSuccess) return efail(e, CSRST_E_CUDA, "ensemble graph capture");
+      const cudaError_t c = cudaGraphInstantiate(&e->graph, g, 0);
+      cudaGraphDestroy(g);
+      if (c != cudaSuccess) return efail(e, CSRST_E_CUDA, std::string("ensemble graph: ") + cudaGetErrorString(c));
+    }
+    for (int k = 0; k < nsteps; ++k)
+      if (cudaGraphLaunch(e->graph, e->s) != cudaSuccess) return efail(e, CSRST_E_CUDA, "ensemble graph launch");
+    ensemble_mark(e);
+  }
+  return ensemble_release(e);
+}
+
+// Sticky device errors of all members: the first member with one, or 0.
+int csrst_ensemble_sync(csrst_ensemble *e, int *bad_member) {
+  if (!e) return CSRST_E_ARG;
+  if (bad_member) *bad_member = -1;
+  if (cudaStreamSynchronize(e->s) != cudaSuccess) return efail(e, CSRST_E_CUDA, "ensemble stream");
+  for (int k = 0; k < e->m; ++k) {
+    const int rc = csrst_sync(e->mem[k]);
+    if (rc) {
+      if (bad_member) *bad_member = k;
+      return efail(e, rc, "member " + std::to_string(k) + ": " + e->mem[k]->err);
+    }
+  }
+  return CSRST_OK;
+}
+
+// Launch shapes: CTAs of the batched push (0 = 2 per SM) and the static-sweep
+// tile (tx * ty = 256).  Results do not depend on them.
+int csrst_ensemble_set_shape(csrst_ensemble *e, int push_ctas, int tx, int ty) {
+  if (!e || push_ctas < 0 || tx <= 0 || ty <= 0 || tx * ty != 256) return efail(e, CSRST_E_ARG, "invalid shape");
+  if (cudaStreamSynchronize(e->s) != cudaSuccess) return efail(e, CSRST_E_CUDA, "ensemble stream");
+  e->push_grid = push_ctas;
+  e->tx = tx; e->ty = ty;
+  return ensemble_build(e);
+}
+
+// The autotuner: times `steps` steady-state steps (events on the ensemble
+// stream, launched eagerly) for each candidate shape and keeps the fastest.
+// The timed steps are real steps of the members.  report: rows of
+// (push_ctas, tx, ty, ms per step), ncand rows at most; returns the count
+// through *nrows.
+int csrst_ensemble_tune(csrst_ensemble *e, int steps, double *report, int max_rows, int *nrows) {
+  if (!e || steps < 1) return efail(e, CSRST_E_ARG, "tune: invalid arguments");
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  int warm = 1;
+  int rc = ensemble_steady(e, warm);
+  if (rc) return rc;
+  const int ctas[4] = {sms, 2 * sms, 4 * sms, 8 * sms};
+  const int tiles[3][2] = {{32, 8}, {64, 4}, {128, 2}};
+  cudaEvent_t t0, t1;
+  cudaEventCreate(&t0);
+  cudaEventCreate(&t1);
+  float best = 1e30f;
+  int bc = 2 * sms, bt = 0, rows = 0;
+  for (int a = 0; a < 4; ++a)
+    for (int b = 0; b < 3; ++b) {
+      e->push_grid = ctas[a];
+      e->tx = tiles[b][0]; e->ty = tiles[b][1];
+      if ((rc = ensemble_build(e))) return rc;
+      ensemble_step_async(e);  // untimed warm-up of this shape
+      cudaEventRecord(t0, e->s);
+      for (int k = 0; k < steps; ++k) ensemble_step_async(e);
+      cudaEventRecord(t1, e->s);
+      if (cudaEventSynchronize(t1) != cudaSuccess) return efail(e, CSRST_E_CUDA, "tune: timing");
+      float ms = 0;
+      cudaEventElapsedTime(&ms, t0, t1);
+      ms /= steps;
+      if (report && rows < max_rows) {
+        report[4 * rows] = ctas[a]; report[4 * rows + 1] = tiles[b][0];
+        report[4 * rows + 2] = tiles[b][1]; report[4 * rows + 3] = ms;
+      }
+      ++rows;
+      if (ms < best) { best = ms; bc = ctas[a]; bt = b; }
+    }
+  cudaEventDestroy(t0);
+  cudaEventDestroy(t1);
+  ensemble_mark(e);
+  e->push_grid = bc;
+  e->tx = tiles[bt][0]; e->ty = tiles[bt][1];
+  if (nrows) *nrows = rows < max_rows ? rows : max_rows;
+  if ((rc = ensemble_build(e))) return rc;
+  return ensemble_release(e);
 }
 
 // ---- stand-alone ScatterGatherImpl / ShapeFunction entry points ----

@@ -17,15 +17,14 @@
 
 namespace csrst {
 
-constexpr int kTX = 32, kTY = 8;
-
-// Half H update (first and third sub-step).
+// Half H update (first and third sub-step), block b of the sub-step grid.
+// The static sweep covers the mesh in tiles of tx x ty cells (tx * ty = 256
+// threads; the shape is a tuning parameter).
 template <class T>
-__global__ void __launch_bounds__(256) k_half_h(FieldArgsT<T> a) {
-  const int b = blockIdx.x;
+__device__ __forceinline__ void half_h_body(const FieldArgsT<T> &a, int b) {
   if (b < a.nbS) {
-    const int i = (b % a.tilesX) * kTX + (threadIdx.x % kTX);
-    const int j = (b / a.tilesX) * kTY + (threadIdx.x / kTX);
+    const int i = (b % a.tilesX) * a.tx + (threadIdx.x % a.tx);
+    const int j = (b / a.tilesX) * a.ty + (threadIdx.x / a.tx);
     if (i >= a.Nx || j >= a.Ny) return;
     if (!a.mask[(size_t)j * a.Nx + i]) return;
     const T ey0 = a.Ey.at(i, j), ey1 = a.Ey.at(i + 1, j);
@@ -58,11 +57,10 @@ __global__ void __launch_bounds__(256) k_half_h(FieldArgsT<T> a) {
 // current comes from the fixed-point accumulator of the last push, which is
 // converted, stored for diagnostics and cleared for the next deposit.
 template <class T, int COMP>
-__global__ void __launch_bounds__(256) k_update_e(FieldArgsT<T> a, T zeroJ) {
-  const int b = blockIdx.x;
+__device__ __forceinline__ void update_e_body(const FieldArgsT<T> &a, int b, T zeroJ) {
   if (b < a.nbS) {
-    const int i = (b % a.tilesX) * kTX + (threadIdx.x % kTX);
-    const int j = (b / a.tilesX) * kTY + (threadIdx.x / kTX);
+    const int i = (b % a.tilesX) * a.tx + (threadIdx.x % a.tx);
+    const int j = (b / a.tilesX) * a.ty + (threadIdx.x / a.tx);
     if (i >= a.Nx || j >= a.Ny) return;
     if (!a.mask[(size_t)j * a.Nx + i]) return;
     if (COMP == 0) {
@@ -115,10 +113,9 @@ __global__ void __launch_bounds__(256) k_update_e(FieldArgsT<T> a, T zeroJ) {
 //   Ey: window first column -> static; static column right of the window -> window guard.
 // No element is both read and written, so every thread copies one element.
 template <class T>
-__global__ void k_exchange(FieldArgsT<T> a, int which) {
+__device__ __forceinline__ void exchange_body(const FieldArgsT<T> &a, int which, int k) {
   const WinState *ws = a.ws;
   const int P0 = ws->P0, P1 = ws->P1, L0 = a.L0, L1 = a.L1;
-  int k = blockIdx.x * blockDim.x + threadIdx.x;
   // segment table: (to_window, count)
   int si, sj, wi, wj;  // static and window coordinates of the element
   bool to_window;
@@ -200,16 +197,10 @@ __global__ void k_check_window(FieldArgsT<T> a) { check_window_clear(a, a.ws); }
 // Communicator.cpp:123-642).  One CTA: reads the last deposit's particle
 // bounds, shifts the window by whole cells through a scratch copy, updates
 // the window position and origin, then refreshes the strips.
-template <class T>
-struct MoveArgs {
-  FieldArgsT<T> f;
-  T *scratch;           // 6 window planes
-  double h0, h1;
-};
 
 template <class T>
-__global__ void __launch_bounds__(1024) k_move(MoveArgs<T> m) {
-  FieldArgsT<T> &a = m.f;
+__device__ __forceinline__ void move_body(const MoveArgs<T> &m) {
+  const FieldArgsT<T> &a = m.f;
   WinState *ws = a.ws;
   if (ws->err) return;
   const int L[2] = {a.L0, a.L1};
@@ -238,7 +229,7 @@ __global__ void __launch_bounds__(1024) k_move(MoveArgs<T> m) {
   const int moveI = s_move[1], m1 = s_move[2];
   if (moveI == 0 && m1 == 0) return;
   const int W0 = a.L0 + 2, W1 = a.L1 + 2, np = W0 * W1;
-  PlaneT<T> *pl[6] = {&a.mEx, &a.mEy, &a.mHx, &a.mHy, &a.mJx, &a.mJy};
+  const PlaneT<T> *pl[6] = {&a.mEx, &a.mEy, &a.mHx, &a.mHy, &a.mJx, &a.mJy};
   // phase A: snapshot
   for (int k = threadIdx.x; k < 6 * np; k += blockDim.x) {
     const int f = k / np, r = k % np;
@@ -356,6 +347,69 @@ __global__ void __launch_bounds__(1024) k_move(MoveArgs<T> m) {
   check_window_clear(a, ws);
 }
 
+// --- kernels: one member, and a batch of members in one launch --------------
+
+template <class T>
+__global__ void __launch_bounds__(256) k_half_h(FieldArgsT<T> a) { half_h_body(a, blockIdx.x); }
+
+template <class T, int COMP>
+__global__ void __launch_bounds__(256) k_update_e(FieldArgsT<T> a, T zeroJ) { update_e_body<T, COMP>(a, blockIdx.x, zeroJ); }
+
+template <class T>
+__global__ void k_exchange(FieldArgsT<T> a, int which) { exchange_body(a, which, blockIdx.x * blockDim.x + threadIdx.x); }
+
+template <class T>
+__global__ void __launch_bounds__(1024) k_move(MoveArgs<T> m) { move_body(m); }
+
+// Member of global block b: bpre holds the first block of every member (m + 1
+// entries).  The member's arguments are copied to shared memory, which the
+// kernels' global stores cannot alias.
+__device__ __forceinline__ int batch_member(const int *bpre, int m, int b) {
+  int lo = 0, hi = m - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (__ldg(bpre + mid) <= b) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
+template <class T>
+__device__ __forceinline__ const FieldArgsT<T> &batch_args(const FieldArgsT<T> *args, int mm) {
+  __shared__ FieldArgsT<T> sa;
+  if (threadIdx.x == 0) sa = args[mm];
+  __syncthreads();
+  return sa;
+}
+
+template <class T>
+__global__ void __launch_bounds__(256) k_half_h_batch(const FieldArgsT<T> *args, const int *bpre, int m) {
+  const int mm = batch_member(bpre, m, blockIdx.x);
+  const FieldArgsT<T> &a = batch_args(args, mm);
+  half_h_body(a, blockIdx.x - bpre[mm]);
+}
+
+template <class T, int COMP>
+__global__ void __launch_bounds__(256) k_update_e_batch(const FieldArgsT<T> *args, const int *bpre, int m) {
+  const int mm = batch_member(bpre, m, blockIdx.x);
+  const FieldArgsT<T> &a = batch_args(args, mm);
+  update_e_body<T, COMP>(a, blockIdx.x - bpre[mm], T(0));
+}
+
+template <class T>
+__global__ void k_exchange_batch(const FieldArgsT<T> *args, const int *bpre, int m, int which) {
+  const int mm = batch_member(bpre, m, blockIdx.x);
+  const FieldArgsT<T> &a = batch_args(args, mm);
+  exchange_body(a, which, (blockIdx.x - bpre[mm]) * blockDim.x + threadIdx.x);
+}
+
+template <class T>
+__global__ void __launch_bounds__(1024) k_move_batch(const MoveArgs<T> *args) {
+  __shared__ MoveArgs<T> sm;
+  if (threadIdx.x == 0) sm = args[blockIdx.x];
+  __syncthreads();
+  move_body(sm);
+}
+
 // SCBoundaryCondition::resetOutsideDomain (SCBoundaryCondition.hh:163-195):
 // E = 0 on cells that are neither inside nor a kept cut cell, and on cut
 // cells per component.  cutidx maps a cell to its cut-cell entry or -1.
@@ -375,10 +429,15 @@ __global__ void k_reset_outside(FieldArgsT<T> a, const int *cutidx) {
 
 // --- host launchers -----------------------------------------------------------
 
+int exchange_count(int L0, int L1, int which) {
+  return which == 0 ? 2 * (L0 + L1) + 4 : which == 1 ? 2 * L0 + 2 : 2 * L1 + 2;
+}
+
 template <class T>
-static int sub_grid(FieldArgsT<T> &a) {
-  a.tilesX = (a.Nx + kTX - 1) / kTX;
-  a.nbS = a.tilesX * ((a.Ny + kTY - 1) / kTY);
+int sub_grid(FieldArgsT<T> &a) {
+  if (a.tx <= 0 || a.ty <= 0 || a.tx * a.ty != 256) { a.tx = 32; a.ty = 8; }
+  a.tilesX = (a.Nx + a.tx - 1) / a.tx;
+  a.nbS = a.tilesX * ((a.Ny + a.ty - 1) / a.ty);
   a.nbC = (a.ncells + 255) / 256;
   const int nbM = (a.L0 * a.L1 + 255) / 256;
   return a.nbS + a.nbC + nbM;
@@ -399,7 +458,7 @@ void launch_update_e(FieldArgsT<T> a, int comp, cudaStream_t s) {
 
 template <class T>
 void launch_exchange(FieldArgsT<T> a, int which, cudaStream_t s) {
-  const int n = which == 0 ? 2 * (a.L0 + a.L1) + 4 : which == 1 ? 2 * a.L0 + 2 : 2 * a.L1 + 2;
+  const int n = exchange_count(a.L0, a.L1, which);
   k_exchange<T><<<(n + 127) / 128, 128, 0, s>>>(a, which);
 }
 
@@ -417,6 +476,31 @@ void launch_move(FieldArgsT<T> a, T *scratch, double h0, double h1, cudaStream_t
   k_move<T><<<1, 1024, 0, s>>>(m);
 }
 
+// Batched sub-steps over m members: args and bpre are device arrays (bpre:
+// first block of each member, m + 1 entries, built from sub_grid / exchange
+// counts); nblocks = bpre[m].
+template <class T>
+void launch_half_h_batch(const FieldArgsT<T> *args, const int *bpre, int m, int nblocks, cudaStream_t s) {
+  if (nblocks > 0) k_half_h_batch<T><<<nblocks, 256, 0, s>>>(args, bpre, m);
+}
+template <class T>
+void launch_update_e_batch(const FieldArgsT<T> *args, const int *bpre, int m, int nblocks, int comp,
+                           cudaStream_t s) {
+  if (nblocks <= 0) return;
+  if (comp == 0) k_update_e_batch<T, 0><<<nblocks, 256, 0, s>>>(args, bpre, m);
+  else k_update_e_batch<T, 1><<<nblocks, 256, 0, s>>>(args, bpre, m);
+}
+template <class T>
+void launch_exchange_batch(const FieldArgsT<T> *args, const int *bpre, int m, int nblocks, int which,
+                           cudaStream_t s) {
+  if (nblocks > 0) k_exchange_batch<T><<<nblocks, 128, 0, s>>>(args, bpre, m, which);
+}
+template <class T>
+void launch_move_batch(const MoveArgs<T> *args, int m, cudaStream_t s) {
+  if (m > 0) k_move_batch<T><<<m, 1024, 0, s>>>(args);
+}
+
+
 template <class T>
 void launch_reset_outside(FieldArgsT<T> a, const int *cutidx, cudaStream_t s) {
   const long long n = (long long)a.Nx * a.Ny;
@@ -430,7 +514,12 @@ void launch_reset_outside(FieldArgsT<T> a, const int *cutidx, cudaStream_t s) {
   template void launch_copy_to_window<T>(FieldArgsT<T>, cudaStream_t);                      \
   template void launch_check_window<T>(FieldArgsT<T>, cudaStream_t);                        \
   template void launch_move<T>(FieldArgsT<T>, T *, double, double, cudaStream_t);           \
-  template void launch_reset_outside<T>(FieldArgsT<T>, const int *, cudaStream_t);
+  template void launch_reset_outside<T>(FieldArgsT<T>, const int *, cudaStream_t);                \
+  template int sub_grid<T>(FieldArgsT<T> &);                                                \
+  template void launch_half_h_batch<T>(const FieldArgsT<T> *, const int *, int, int, cudaStream_t); \
+  template void launch_update_e_batch<T>(const FieldArgsT<T> *, const int *, int, int, int, cudaStream_t); \
+  template void launch_exchange_batch<T>(const FieldArgsT<T> *, const int *, int, int, int, cudaStream_t); \
+  template void launch_move_batch<T>(const MoveArgs<T> *, int, cudaStream_t);
 CSRST_FIELDS_INSTANTIATE(double)
 CSRST_FIELDS_INSTANTIATE(float)
 

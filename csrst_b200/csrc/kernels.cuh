@@ -50,8 +50,17 @@ struct FieldArgsT {
   T de;                            // dt / eps0
   T h0, h1;
   int nbS, nbC, tilesX;            // block ranges: static tiles, cut-cell blocks
+  int tx, ty;                      // static-sweep tile (tx * ty = 256; 0 = 32 x 8)
 };
 using FieldArgs = FieldArgsT<double>;
+
+// Window move of one member (fields.cu).
+template <class T>
+struct MoveArgs {
+  FieldArgsT<T> f;
+  T *scratch;           // 6 window planes
+  double h0, h1;
+};
 
 // Bend parameters (Bend ctor and Bend::Init, Bend.cpp:60-124).
 struct BendDev {
@@ -60,7 +69,20 @@ struct BendDev {
   double hr0, hr1, org0, org1, cen0, cen1;
 };
 
+// Per-member arguments of the small bookkeeping kernels around a push.
+struct PrepArgs {
+  WinState *ws;
+  double h0, h1;
+  int em0, em2, cm0;  // gather-patch margins of the shape order
+};
+
 // particles.cu
+PrepArgs prep_args(WinState *ws, double h0, double h1, int order);
+size_t push_tile_bytes(int order);
+long long push_batch_smem_limit();
+// prep + push + post + bounds of a batch of FP64 members (device arrays)
+void launch_push_batch(const PushArgs *args, const int *order, const unsigned char *smem_ok, const long long *ppre,
+                       int m, long long total, int grid, size_t smem, const PrepArgs *prep, cudaStream_t s);
 void launch_bbox_next(const double *x, const double *y, const double *px, const double *py, long long n,
                       double half, int pending, WinState *ws, cudaStream_t s);
 void launch_push_prep(WinState *ws, double h0, double h1, int order, cudaStream_t s);
@@ -84,6 +106,18 @@ template <class T> void launch_copy_to_window(FieldArgsT<T> a, cudaStream_t s);
 template <class T> void launch_check_window(FieldArgsT<T> a, cudaStream_t s);
 template <class T> void launch_move(FieldArgsT<T> a, T *scratch, double h0, double h1, cudaStream_t s);
 template <class T> void launch_reset_outside(FieldArgsT<T> a, const int *cutidx, cudaStream_t s);
+// sets the block ranges of a sub-step; returns its block count
+template <class T> int sub_grid(FieldArgsT<T> &a);
+int exchange_count(int L0, int L1, int which);
+template <class T>
+void launch_half_h_batch(const FieldArgsT<T> *args, const int *bpre, int m, int nblocks, cudaStream_t s);
+template <class T>
+void launch_update_e_batch(const FieldArgsT<T> *args, const int *bpre, int m, int nblocks, int comp,
+                           cudaStream_t s);
+template <class T>
+void launch_exchange_batch(const FieldArgsT<T> *args, const int *bpre, int m, int nblocks, int which,
+                           cudaStream_t s);
+template <class T> void launch_move_batch(const MoveArgs<T> *args, int m, cudaStream_t s);
 // geometry.cu
 int build_geometry(const BendDev &b, uint8_t *d_mask, CutCellDev **d_cells, int *ncells, int **d_cutidx,
                    cudaStream_t s);
@@ -153,6 +187,10 @@ struct Push32Args {
 };
 
 int launch_push32(const Push32Args &a, int order, int L0, int L1, int grid, cudaStream_t s);
+long long push32_batch_smem_limit();
+void launch_push32_batch(const Push32Args *args, const int *order, const unsigned char *smem_ok,
+                         const long long *ppre, int m, long long total, int grid, size_t smem,
+                         const PrepArgs *prep, cudaStream_t s);
 void launch_prep32(WinState *ws, int order, cudaStream_t s);
 void launch_bounds32(WinState *ws, cudaStream_t s);
 void launch_bbox32(const Bunch32 &b, double P0, double P1, double kh0, double kh1, int pending, WinState *ws,

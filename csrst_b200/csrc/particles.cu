@@ -49,8 +49,7 @@ __global__ void k_bbox_clear(WinState *ws, int slot) {
 // positions the push will gather at (PartBunch::getLocalPDomain and
 // getFields), and reset the accumulators the push will fill.
 // em: getExtraMarginEdge (x first, x last, y first, y last); cm: getExtraMarginCell.
-__global__ void k_push_prep(WinState *ws, double h0, double h1, int em0, int em2, int cm0) {
-  if (threadIdx.x != 0) return;
+__device__ __forceinline__ void push_prep_body(WinState *ws, double h0, double h1, int em0, int em2, int cm0) {
   const int c = ws->cur;
   const double mn0 = ord_dbl(ws->bb[c][0]), mn1 = ord_dbl(ws->bb[c][1]);
   const double mx0 = ord_dbl(ws->bb[c][2]), mx1 = ord_dbl(ws->bb[c][3]);
@@ -79,15 +78,22 @@ __global__ void k_push_prep(WinState *ws, double h0, double h1, int em0, int em2
   bbox_reset(ws->bball);
 }
 
+__global__ void k_push_prep(WinState *ws, double h0, double h1, int em0, int em2, int cm0) {
+  if (threadIdx.x == 0) push_prep_body(ws, h0, h1, em0, em2, cm0);
+}
+
 // After a push: flip the bbox slot.
 __global__ void k_push_post(WinState *ws) {
   if (threadIdx.x == 0) ws->cur = 1 - ws->cur;
 }
 
 // Dynamic shared memory: [window accumulator (SMEM only)][per-thread deposit tiles].
+// One CTA's share [beg, end) of one push.  All threads of the CTA call it
+// together; it ends with a barrier, so a CTA can run it for several members
+// in turn.
 template <int ORDER, bool SMEM>
-__global__ void __launch_bounds__(256, 2) k_push(PushArgs a) {
-  extern __shared__ unsigned long long sacc[];
+__device__ __forceinline__ void push_body(const PushArgs &a, long long beg, long long end,
+                                          unsigned long long *sacc) {
   __shared__ int tb[4];  // touched box of this CTA (window cells)
   WinState *ws = a.ws;
   __shared__ int s_err;
@@ -125,12 +131,9 @@ __global__ void __launch_bounds__(256, 2) k_push(PushArgs a) {
   const double scale = a.acc_scale;
   auto sink = [&](int i, int j, double v) { tile.template add<SMEM>(i, j, __double2ll_rn(v * scale), win, L0, L1); };
 
-  // Each CTA owns a contiguous slice of the (cell-ordered) particles.  The
+  // The CTA owns a contiguous slice of the (cell-ordered) particles.  The
   // rounds are the same for every lane, so that the warp re-bases its
   // deposit tile together.
-  const long long per = (a.n + gridDim.x - 1) / gridDim.x;
-  const long long beg = (long long)blockIdx.x * per;
-  const long long end = beg + per < a.n ? beg + per : a.n;
   const long long rounds = end > beg ? (end - beg + blockDim.x - 1) / blockDim.x : 0;
   for (long long it = 0; it < rounds; ++it) {
     const long long i = beg + it * blockDim.x + threadIdx.x;
@@ -206,12 +209,63 @@ __global__ void __launch_bounds__(256, 2) k_push(PushArgs a) {
       }
     }
   }
+  __syncthreads();
+}
+
+template <int ORDER, bool SMEM>
+__global__ void __launch_bounds__(256, 2) k_push(PushArgs a) {
+  extern __shared__ unsigned long long sacc[];
+  const long long per = (a.n + gridDim.x - 1) / gridDim.x;
+  const long long beg = (long long)blockIdx.x * per;
+  const long long end = beg + per < a.n ? beg + per : a.n;
+  push_body<ORDER, SMEM>(a, beg, end, sacc);
+}
+
+// One push over a batch of members: the members' particles form one index
+// range (ppre: first particle of each member, m + 1 entries) that is cut into
+// equal contiguous shares, one per CTA; a CTA runs the push of every member
+// its share overlaps, with that member's shape order and accumulator.
+__global__ void __launch_bounds__(256, 2) k_push_batch(const PushArgs *args, const int *order,
+                                                       const unsigned char *smem_ok, const long long *ppre,
+                                                       int m, long long per) {
+  extern __shared__ unsigned long long sacc[];
+  __shared__ PushArgs sa;
+  const long long total = ppre[m];
+  const long long g0 = (long long)blockIdx.x * per;
+  const long long g1 = g0 + per < total ? g0 + per : total;
+  for (int mm = 0; mm < m; ++mm) {
+    const long long b0 = ppre[mm], b1 = ppre[mm + 1];
+    if (b1 <= g0 || b0 >= g1) continue;
+    const long long lb = (g0 > b0 ? g0 : b0) - b0, le = (g1 < b1 ? g1 : b1) - b0;
+    __syncthreads();
+    if (threadIdx.x == 0) sa = args[mm];
+    __syncthreads();
+    const int o = order[mm];
+    if (smem_ok[mm]) {
+      if (o == 0) push_body<0, true>(sa, lb, le, sacc);
+      else if (o == 1) push_body<1, true>(sa, lb, le, sacc);
+      else push_body<2, true>(sa, lb, le, sacc);
+    } else {
+      if (o == 0) push_body<0, false>(sa, lb, le, sacc);
+      else if (o == 1) push_body<1, false>(sa, lb, le, sacc);
+      else push_body<2, false>(sa, lb, le, sacc);
+    }
+  }
+}
+
+// Per-member bookkeeping of a batched push, one thread per member.
+__global__ void k_push_prep_batch(const PrepArgs *p, int m) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < m) push_prep_body(p[k].ws, p[k].h0, p[k].h1, p[k].em0, p[k].em2, p[k].cm0);
+}
+__global__ void k_push_post_batch(const PrepArgs *p, int m) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < m) p[k].ws->cur = 1 - p[k].ws->cur;
 }
 
 // After the last push of a step: the deposit's particle bounds relative to
 // the window (PartBunch::getLocalPDomainInclOld -> setGlobalBounds).
-__global__ void k_global_bounds(WinState *ws, double h0, double h1) {
-  if (threadIdx.x != 0) return;
+__device__ __forceinline__ void global_bounds_body(WinState *ws, double h0, double h1) {
   const double mn0 = ord_dbl(ws->bball[0]), mn1 = ord_dbl(ws->bball[1]);
   const double mx0 = ord_dbl(ws->bball[2]), mx1 = ord_dbl(ws->bball[3]);
   if (!(mn0 <= mx0)) { ws->gb[0] = 0; ws->gb[1] = -1; ws->gb[2] = 0; ws->gb[3] = -1; return; }
@@ -219,6 +273,14 @@ __global__ void k_global_bounds(WinState *ws, double h0, double h1) {
   ws->gb[1] = (int)floor((mx0 - ws->mo0) / h0);
   ws->gb[2] = (int)floor((mn1 - ws->mo1) / h1);
   ws->gb[3] = (int)floor((mx1 - ws->mo1) / h1);
+}
+
+__global__ void k_global_bounds(WinState *ws, double h0, double h1) {
+  if (threadIdx.x == 0) global_bounds_body(ws, h0, h1);
+}
+__global__ void k_global_bounds_batch(const PrepArgs *p, int m) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < m) global_bounds_body(p[k].ws, p[k].h0, p[k].h1);
 }
 
 // Stand-alone drift (PartBunch::drift_particles, PartBunch.cpp:179-187).
@@ -281,12 +343,50 @@ void launch_bbox_next(const double *x, const double *y, const double *px, const 
   k_bbox_next<<<blocks, 256, 0, s>>>(x, y, px, py, n, half, pending, ws);
 }
 
+PrepArgs prep_args(WinState *ws, double h0, double h1, int order) {
+  PrepArgs p{ws, h0, h1, 0, 0, 0};
+  if (order == 0) { p.em0 = -1; p.em2 = 0; p.cm0 = -1; }
+  else if (order == 1) { p.em0 = -1; p.em2 = -1; p.cm0 = -1; }
+  else { p.em0 = -2; p.em2 = -1; p.cm0 = -2; }
+  return p;
+}
+
 void launch_push_prep(WinState *ws, double h0, double h1, int order, cudaStream_t s) {
-  int em0, em2, cm0;
-  if (order == 0) { em0 = -1; em2 = 0; cm0 = -1; }
-  else if (order == 1) { em0 = -1; em2 = -1; cm0 = -1; }
-  else { em0 = -2; em2 = -1; cm0 = -2; }
-  k_push_prep<<<1, 32, 0, s>>>(ws, h0, h1, em0, em2, cm0);
+  const PrepArgs p = prep_args(ws, h0, h1, order);
+  k_push_prep<<<1, 32, 0, s>>>(ws, h0, h1, p.em0, p.em2, p.cm0);
+}
+
+size_t push_tile_bytes(int order) {
+  const int k = order == 0 ? TileFor<0>::T::kSize : order == 1 ? TileFor<1>::T::kSize : TileFor<2>::T::kSize;
+  return (size_t)k * 256 * sizeof(unsigned long long);
+}
+
+long long push_batch_smem_limit() {
+  static long long lim = -1;
+  if (lim < 0) {
+    int dev = 0, v = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    cudaFuncAttributes fa{};
+    cudaFuncGetAttributes(&fa, k_push_batch);
+    lim = (long long)v - (long long)fa.sharedSizeBytes;
+    if (cudaFuncSetAttribute(k_push_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lim) != cudaSuccess)
+      lim = 0;
+    cudaGetLastError();
+  }
+  return lim;
+}
+
+void launch_push_batch(const PushArgs *args, const int *order, const unsigned char *smem_ok, const long long *ppre,
+                       int m, long long total, int grid, size_t smem, const PrepArgs *prep, cudaStream_t s) {
+  const int tb = (m + 127) / 128;
+  k_push_prep_batch<<<tb, 128, 0, s>>>(prep, m);
+  if (total > 0 && grid > 0) {
+    const long long per = (total + grid - 1) / grid;
+    k_push_batch<<<grid, 256, smem, s>>>(args, order, smem_ok, ppre, m, per);
+  }
+  k_push_post_batch<<<tb, 128, 0, s>>>(prep, m);
+  k_global_bounds_batch<<<tb, 128, 0, s>>>(prep, m);
 }
 
 // Largest dynamic shared memory the window accumulator may use for this

@@ -72,9 +72,11 @@ __device__ __forceinline__ void store_pos(double t0, double t1, int ci, int cj, 
   o0 = a0; o1 = a1;
 }
 
+// One CTA's share [beg, end) of one push; called by all threads of the CTA,
+// ends with a barrier (a CTA may run it for several members in turn).
 template <int ORDER, bool SMEM>
-__global__ void __launch_bounds__(256, 2) k_push32(Push32Args a) {
-  extern __shared__ unsigned long long sacc[];
+__device__ __forceinline__ void push32_body(const Push32Args &a, long long beg, long long end,
+                                            unsigned long long *sacc) {
   __shared__ int tb[4];
   __shared__ int s_err;
   WinState *ws = a.ws;
@@ -103,9 +105,6 @@ __global__ void __launch_bounds__(256, 2) k_push32(Push32Args a) {
   };
   const double P0 = a.P0, P1 = a.P1;
   const float Pf0 = (float)P0, Pf1 = (float)P1;
-  const long long per = (a.b.n + gridDim.x - 1) / gridDim.x;
-  const long long beg = (long long)blockIdx.x * per;
-  const long long end = beg + per < a.b.n ? beg + per : a.b.n;
   const long long rounds = end > beg ? (end - beg + blockDim.x - 1) / blockDim.x : 0;
   for (long long it = 0; it < rounds; ++it) {  // the same rounds for every lane
     const long long n = beg + it * blockDim.x + threadIdx.x;
@@ -213,12 +212,50 @@ __global__ void __launch_bounds__(256, 2) k_push32(Push32Args a) {
       }
     }
   }
+  __syncthreads();
+}
+
+template <int ORDER, bool SMEM>
+__global__ void __launch_bounds__(256, 2) k_push32(Push32Args a) {
+  extern __shared__ unsigned long long sacc[];
+  const long long per = (a.b.n + gridDim.x - 1) / gridDim.x;
+  const long long beg = (long long)blockIdx.x * per;
+  const long long end = beg + per < a.b.n ? beg + per : a.b.n;
+  push32_body<ORDER, SMEM>(a, beg, end, sacc);
+}
+
+// One push over a batch of FP32-mode members (see k_push_batch).
+__global__ void __launch_bounds__(256, 2) k_push32_batch(const Push32Args *args, const int *order,
+                                                         const unsigned char *smem_ok, const long long *ppre,
+                                                         int m, long long per) {
+  extern __shared__ unsigned long long sacc[];
+  __shared__ Push32Args sa;
+  const long long total = ppre[m];
+  const long long g0 = (long long)blockIdx.x * per;
+  const long long g1 = g0 + per < total ? g0 + per : total;
+  for (int mm = 0; mm < m; ++mm) {
+    const long long b0 = ppre[mm], b1 = ppre[mm + 1];
+    if (b1 <= g0 || b0 >= g1) continue;
+    const long long lb = (g0 > b0 ? g0 : b0) - b0, le = (g1 < b1 ? g1 : b1) - b0;
+    __syncthreads();
+    if (threadIdx.x == 0) sa = args[mm];
+    __syncthreads();
+    const int o = order[mm];
+    if (smem_ok[mm]) {
+      if (o == 0) push32_body<0, true>(sa, lb, le, sacc);
+      else if (o == 1) push32_body<1, true>(sa, lb, le, sacc);
+      else push32_body<2, true>(sa, lb, le, sacc);
+    } else {
+      if (o == 0) push32_body<0, false>(sa, lb, le, sacc);
+      else if (o == 1) push32_body<1, false>(sa, lb, le, sacc);
+      else push32_body<2, false>(sa, lb, le, sacc);
+    }
+  }
 }
 
 // Gather-patch set-up and the window-fit check from the box of the next
 // push's gather positions (cells of the static mesh).
-__global__ void k_prep32(WinState *ws, int reach) {
-  if (threadIdx.x != 0) return;
+__device__ __forceinline__ void prep32_body(WinState *ws, int reach) {
   const int c = ws->cur;
   const double mn0 = ord_dbl(ws->bb[c][0]), mn1 = ord_dbl(ws->bb[c][1]);
   const double mx0 = ord_dbl(ws->bb[c][2]), mx1 = ord_dbl(ws->bb[c][3]);
@@ -234,14 +271,34 @@ __global__ void k_prep32(WinState *ws, int reach) {
   bbox_reset(ws->bball);
 }
 
+__global__ void k_prep32(WinState *ws, int reach) {
+  if (threadIdx.x == 0) prep32_body(ws, reach);
+}
+
 // Deposit bounds in window cells (PartBunch::getLocalPDomainInclOld).
-__global__ void k_bounds32(WinState *ws) {
-  if (threadIdx.x != 0) return;
+__device__ __forceinline__ void bounds32_body(WinState *ws) {
   const double mn0 = ord_dbl(ws->bball[0]), mn1 = ord_dbl(ws->bball[1]);
   const double mx0 = ord_dbl(ws->bball[2]), mx1 = ord_dbl(ws->bball[3]);
   if (!(mn0 <= mx0)) { ws->gb[0] = 0; ws->gb[1] = -1; ws->gb[2] = 0; ws->gb[3] = -1; return; }
   ws->gb[0] = (int)floor(mn0) - ws->P0; ws->gb[1] = (int)floor(mx0) - ws->P0;
   ws->gb[2] = (int)floor(mn1) - ws->P1; ws->gb[3] = (int)floor(mx1) - ws->P1;
+}
+
+__global__ void k_bounds32(WinState *ws) {
+  if (threadIdx.x == 0) bounds32_body(ws);
+}
+
+__global__ void k_prep32_batch(const PrepArgs *p, int m) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < m) prep32_body(p[k].ws, 2);
+}
+__global__ void k_post32_batch(const PrepArgs *p, int m) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < m) p[k].ws->cur = 1 - p[k].ws->cur;
+}
+__global__ void k_bounds32_batch(const PrepArgs *p, int m) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < m) bounds32_body(p[k].ws);
 }
 
 __global__ void k_post32(WinState *ws) {
@@ -385,6 +442,36 @@ int launch_push32(const Push32Args &a, int order, int L0, int L1, int grid, cuda
   else push32_order<2>(a, L0, L1, grid, s);
   k_post32<<<1, 32, 0, s>>>(a.ws);
   return 0;
+}
+
+long long push32_batch_smem_limit() {
+  static long long lim = -1;
+  if (lim < 0) {
+    int dev = 0, v = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    cudaFuncAttributes fa{};
+    cudaFuncGetAttributes(&fa, k_push32_batch);
+    lim = (long long)v - (long long)fa.sharedSizeBytes;
+    if (cudaFuncSetAttribute(k_push32_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lim) !=
+        cudaSuccess)
+      lim = 0;
+    cudaGetLastError();
+  }
+  return lim;
+}
+
+void launch_push32_batch(const Push32Args *args, const int *order, const unsigned char *smem_ok,
+                         const long long *ppre, int m, long long total, int grid, size_t smem,
+                         const PrepArgs *prep, cudaStream_t s) {
+  const int tb = (m + 127) / 128;
+  k_prep32_batch<<<tb, 128, 0, s>>>(prep, m);
+  if (total > 0 && grid > 0) {
+    const long long per = (total + grid - 1) / grid;
+    k_push32_batch<<<grid, 256, smem, s>>>(args, order, smem_ok, ppre, m, per);
+  }
+  k_post32_batch<<<tb, 128, 0, s>>>(prep, m);
+  k_bounds32_batch<<<tb, 128, 0, s>>>(prep, m);
 }
 
 void launch_prep32(WinState *ws, int order, cudaStream_t s) {

@@ -17,7 +17,7 @@ import ctypes as C
 
 import numpy as np
 
-from ._lib import Config, check, f64, lib, ptr, D
+from ._lib import Config, CsrstError, check, f64, lib, ptr, D
 
 IntCIC, IntS1, IntS2 = 0, 1, 2
 
@@ -166,6 +166,62 @@ class Simulation:
         out = np.zeros(max(w[2] - 4, 0))
         self._ck(lib().csrst_diag_wake(self.h, ptr(out), len(out)))
         return out
+
+
+class Ensemble:
+    """Independent members stepped together: one launch per phase of the time
+    step for all members, the step captured as one CUDA graph.  Members are
+    loaded Simulations in one precision mode; each ends every step bitwise in
+    the state its own step() would give."""
+
+    def __init__(self, sims):
+        self.sims = list(sims)
+        arr = (C.c_void_p * len(self.sims))(*[s.h.value for s in self.sims])
+        e = C.c_void_p()
+        rc = lib().csrst_ensemble_create(arr, len(self.sims), C.byref(e))
+        if rc:
+            buf = C.create_string_buffer(512)
+            lib().csrst_ensemble_get_error(None, buf, 512)
+            raise CsrstError(rc, buf.value.decode(errors="replace"))
+        self._e = e
+
+    def _ck(self, rc):
+        if rc:
+            buf = C.create_string_buffer(512)
+            lib().csrst_ensemble_get_error(self._e, buf, 512)
+            raise CsrstError(rc, buf.value.decode(errors="replace"))
+
+    def step(self, n=1):
+        self._ck(lib().csrst_ensemble_step(self._e, int(n)))
+
+    def sync(self):
+        bad = C.c_int(-1)
+        self._ck(lib().csrst_ensemble_sync(self._e, C.byref(bad)))
+
+    def stream(self):
+        return lib().csrst_ensemble_stream(self._e)
+
+    def set_shape(self, push_ctas, tx=32, ty=8):
+        self._ck(lib().csrst_ensemble_set_shape(self._e, int(push_ctas), int(tx), int(ty)))
+
+    def tune(self, steps=3):
+        """Autotunes the launch shapes on real steps; returns the timing table
+        [(push_ctas, tx, ty, ms_per_step)] and leaves the fastest selected."""
+        rows = np.zeros(4 * 64)
+        n = C.c_int(0)
+        self._ck(lib().csrst_ensemble_tune(self._e, int(steps), ptr(rows), 64, C.byref(n)))
+        return [tuple(rows[4 * k:4 * k + 4]) for k in range(n.value)]
+
+    def close(self):
+        if getattr(self, "_e", None) is not None:
+            lib().csrst_ensemble_destroy(self._e)
+            self._e = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class PartBunch:

@@ -127,3 +127,82 @@ def workload(name):
     else:
         raise KeyError(name)
     return cfg, spec
+
+
+def bend_config_fit(Nx, Ny, h, R, width, gamma, lb_min, shape_order=0, cfl=0.5, length_after=None):
+    """A bend on an Nx x Ny mesh of square cells h with a drift of at least
+    lb_min before it: the bend angle is the largest that fits both the mesh
+    height with a pipe of `width` and the mesh length; when the length limits
+    it, the pipe is widened until the bend fills the mesh height again."""
+    if length_after is None:
+        length_after = 50 * h
+    ekin_mev = (gamma - 1.0) * MASS_EV * 1e-6
+    ekin = ekin_mev * 1e6
+    bz = math.sqrt(ekin * ekin + 2.0 * ekin * MASS_EV) / (C_LIGHT * R)
+    dom_l, dom_w = (Nx - 2) * h, (Ny - 2) * h
+    if dom_w <= width or dom_l <= lb_min + length_after:
+        raise ValueError("mesh too small for this bend")
+
+    def width_of(phi, w):
+        return (R - 0.5 * w) * (1 - math.cos(phi)) + w + length_after * math.sin(phi)
+
+    def length_of(phi, w):
+        return lb_min + length_after * math.cos(phi) + (R + 0.5 * w) * math.sin(phi)
+
+    def fill(phi):  # pipe width that makes the bounding box exactly (Ny - 2) h tall
+        c, sn = math.cos(phi), math.sin(phi)
+        return (dom_w - R * (1 - c) - length_after * sn) / (1 - 0.5 * (1 - c))
+
+    lo, hi = 0.0, 0.5 * math.pi
+    for _ in range(200):  # largest angle the height allows with the narrowest pipe
+        mid = 0.5 * (lo + hi)
+        lo, hi = (mid, hi) if width_of(mid, width) < dom_w else (lo, mid)
+    lo, hi = 0.0, lo
+    for _ in range(200):  # then the largest that also fits the length with the filling pipe
+        mid = 0.5 * (lo + hi)
+        lo, hi = (mid, hi) if length_of(mid, fill(mid)) < dom_l else (lo, mid)
+    phi = lo
+    c, sn = math.cos(phi), math.sin(phi)
+    width = fill(phi)
+    lb = dom_l - length_after * c - (R + 0.5 * width) * sn
+    if lb < lb_min or width > 0.75 * dom_w:
+        raise ValueError("mesh too small for this bend")
+    return RunConfig(Nx=Nx, Ny=Ny, length_before=lb, length_after=length_after, width=width,
+                     phi_deg=math.degrees(phi), ekin_mev=ekin_mev, bz=bz, shape_order=shape_order,
+                     dt=cfl * h / C_LIGHT)
+
+
+def ensemble_members(m=64, seed=2024):
+    """The batched-ensemble workload: m independent bunches with uneven
+    meshes and bunch sizes.  Nx ~ U[1024, 8192], Ny ~ U[256, 1024],
+    sigma_s log-uniform in [20, 200] um, sigma_x = sigma_s / 2.5, gamma ~
+    U[200, 2000], bend radius ~ U[0.5, 5] m, 5e4 - 1e6 particles, CIC and TSC
+    alternating, CFL 0.5.  Cells are sigma_s / 10, made coarser in steps of
+    1.25 until the bend fits the drawn mesh (bend_config_fit; the pipe is 60 -
+    85 % of the mesh height)."""
+    g = np.random.Generator(np.random.Philox(seed))
+    out = []
+    while len(out) < m:
+        k = len(out)
+        Nx = int(g.integers(1024, 8193))
+        Ny = int(g.integers(256, 1025))
+        sigma_s = float(np.exp(g.uniform(np.log(20e-6), np.log(200e-6))))
+        gamma = float(g.uniform(200.0, 2000.0))
+        R = float(g.uniform(0.5, 5.0))
+        n = int(g.integers(50_000, 1_000_001))
+        cfg = None
+        for t in range(12):  # cells of sigma_s / 10, coarser until the bend fits the mesh
+            h = sigma_s / 10 * 1.25 ** t
+            width = 0.6 * (Ny - 2) * h
+            x0 = 50 * h + 6 * sigma_s
+            try:
+                cfg = bend_config_fit(Nx, Ny, h, R, width, gamma, x0 + 30 * sigma_s, shape_order=k % 2)
+                break
+            except ValueError:
+                continue
+        if cfg is None:
+            continue
+        spec = BunchSpec(n=n, gamma=gamma, sigma_s=sigma_s, sigma_x=sigma_s / 2.5, energy_spread=1e-4,
+                         charge=-1e-9, x0=x0, y0=0.5 * width, seed=1000 + k)
+        out.append((cfg, spec))
+    return out

@@ -131,6 +131,31 @@ int csrst_step_second(csrst_handle *h);
  * second step, window move.  Captured once as a CUDA graph and replayed. */
 int csrst_step(csrst_handle *h, int nsteps);
 
+/* Batched ensemble (no reference counterpart: the reference runs one bunch
+ * per job).  Independent members, each a loaded handle with its own mesh,
+ * window, shape order and bunch size, all in the same precision mode, are
+ * stepped together: every phase of the time step is one launch over all
+ * members and the whole step is one CUDA graph.  Each member's state after a
+ * batched step is bitwise the state its own csrst_step would give.  The
+ * member handles stay valid for reads between ensemble steps; reloading a
+ * member invalidates the ensemble. */
+typedef struct csrst_ensemble csrst_ensemble;
+int csrst_ensemble_create(csrst_handle *const *members, int m, csrst_ensemble **out);
+int csrst_ensemble_destroy(csrst_ensemble *e);
+int csrst_ensemble_get_error(const csrst_ensemble *e, char *buf, size_t len);
+/* CUDA stream of the ensemble (a cudaStream_t). */
+void *csrst_ensemble_stream(csrst_ensemble *e);
+int csrst_ensemble_step(csrst_ensemble *e, int nsteps);
+/* Waits for the ensemble; returns the first member's sticky error (its index in *bad_member). */
+int csrst_ensemble_sync(csrst_ensemble *e, int *bad_member);
+/* Launch shapes: CTAs of the batched push (0 = two per SM) and the static-sweep
+ * tile tx x ty (tx * ty = 256).  Results do not depend on them. */
+int csrst_ensemble_set_shape(csrst_ensemble *e, int push_ctas, int tx, int ty);
+/* Autotuner: times `steps` steps for each candidate shape and keeps the
+ * fastest; the timed steps are real steps of the members.  report: rows of
+ * (push_ctas, tx, ty, ms per step). */
+int csrst_ensemble_tune(csrst_ensemble *e, int steps, double *report, int max_rows, int *nrows);
+
 /* Beam moments (PartBunch::calcBeamParameters, PartBunch.cpp:584-657):
  * out18 = rmean2, pmean2, rrms2, prms2, eps_norm2, rmin2, rmax2, Ekin[MeV], dE, 0, 0. */
 int csrst_diag_moments(csrst_handle *h, double *out18);
