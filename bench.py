@@ -60,6 +60,7 @@ def parse():
     p.add_argument("--precision", default="fp32", choices=["fp32", "fp64"],
                    help="mode of the headline value; the other mode is timed beside it")
     p.add_argument("--no-compare", action="store_true", help="skip the other precision and the accuracy check")
+    p.add_argument("--no-ensemble", action="store_true", help="skip the 64-member batched-ensemble workload")
     return p.parse_args()
 
 
@@ -267,6 +268,94 @@ def accuracy(cfg, spec, bunch, steps=50):
             "bar": "wake <= 1e-3 of the FP64 path's maximum; continuity <= 1e-10 (FP64 check)"}
 
 
+def run_ensemble(args, rank, members=64):
+    """The batched-ensemble workload: `members` independent bunches (uneven
+    meshes 1024-8192 x 256-1024, 5e4-1e6 particles, CIC/TSC) stepped as one
+    batch in FP32 mode after the autotuner picked the launch shapes, against
+    the same members run one after another on the plain FP64 path (each
+    member its own handle, stream and CUDA graph) and on FP32 unbatched."""
+    import torch
+    from csrst_b200 import Ensemble, Simulation
+    from csrst_b200.workloads import ensemble_members, make_bunch
+    ms = ensemble_members(members, seed=2024 + rank)
+    total = sum(spec.n for _, spec in ms)
+    cells = sum(cfg.Nx * cfg.Ny for cfg, _ in ms)
+    K, W = max(args.steps // 2, 5), max(args.warmup, 3)
+    out = {"members": members, "particles": total, "cells": cells, "steps": K, "warmup": W}
+
+    def build(fp32):
+        sims = []
+        t = time.perf_counter()
+        for cfg, spec in ms:
+            sm = Simulation(cfg, fp32=fp32)
+            sm.load(*make_bunch(spec))
+            sm.initial_fields(1e-12, 1e-6, 500)
+            sims.append(sm)
+        return sims, time.perf_counter() - t
+
+    def time_streams(sims):
+        # members one after another, each on its own stream, device-timed fork/join
+        side = torch.cuda.Stream()
+        start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        for sm in sims:
+            sm.step(W)
+            sm.sync()
+        torch.cuda.synchronize()
+        start.record(side)
+        ends = []
+        for sm in sims:
+            st = torch.cuda.ExternalStream(sm.stream())
+            st.wait_event(start)
+            sm.step(K)
+            e = torch.cuda.Event()
+            e.record(st)
+            ends.append(e)
+        for e in ends:
+            side.wait_event(e)
+        stop.record(side)
+        torch.cuda.synchronize()
+        return start.elapsed_time(stop)
+
+    # plain FP64 path, unbatched
+    sims, setup = build(False)
+    ms64 = time_streams(sims)
+    for sm in sims:
+        sm.close()
+    out["fp64_unbatched"] = {"value": round(total * K / (ms64 * 1e-3), 1), "ms_per_step": round(ms64 / K, 3),
+                             "setup_s": round(setup, 1)}
+    # FP32 mode, unbatched
+    sims, _ = build(True)
+    ms32 = time_streams(sims)
+    out["fp32_unbatched"] = {"value": round(total * K / (ms32 * 1e-3), 1), "ms_per_step": round(ms32 / K, 3)}
+    # FP32 mode, batched + graph, autotuned
+    ens = Ensemble(sims)
+    rows = ens.tune(steps=2)
+    best = min(rows, key=lambda r: r[4])
+    ens.step(W)
+    ens.sync()
+    st = torch.cuda.ExternalStream(ens.stream())
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    t0.record(st)
+    ens.step(K)
+    t1.record(st)
+    ens.sync()
+    torch.cuda.synchronize()
+    msb = t0.elapsed_time(t1)
+    ens.close()
+    for sm in sims:
+        sm.close()
+    out["fp32_batched"] = {"value": round(total * K / (msb * 1e-3), 1), "ms_per_step": round(msb / K, 3),
+                           "launches_per_step": 4 * 2 + 2 * 4 + 2 + 1,
+                           "tuned_shape": {"push_ctas": int(best[0]), "tile": [int(best[1]), int(best[2])],
+                                           "parts": int(best[3])},
+                           "tuning_table_ms": [[int(r[0]), int(r[1]), int(r[2]), int(r[3]), round(r[4], 3)]
+                                               for r in rows]}
+    out["fp32_batched_over_fp64_unbatched"] = round(ms64 / msb, 2)
+    out["fp32_batched_over_fp32_unbatched"] = round(ms32 / msb, 2)
+    return out
+
+
 def run_b200(args, world, rank, local):
     import torch
     from csrst_b200.workloads import make_bunch, workload
@@ -334,6 +423,8 @@ def run_b200(args, world, rank, local):
     out["gpu_launches"] = args.steps * (2 * 4 + 4 * 2 + 1)
     if rank == 0 and not args.no_compare:
         out["accuracy_fp32_vs_fp64"] = accuracy(cfg, spec, bunch)
+    if not args.no_ensemble:
+        out["batched_ensemble"] = run_ensemble(args, rank)
     if not args.no_e2e:
         out["e2e"] = run_e2e(args, cfg, spec, bunch, rank, world, head == "fp32")
     if rank == 0 and world == 1 and not args.no_cpu:

@@ -66,7 +66,7 @@ def lib():
         "csrst_ensemble_stream": ([P], C.c_void_p),
         "csrst_ensemble_step": ([P, C.c_int], C.c_int),
         "csrst_ensemble_sync": ([P, I], C.c_int),
-        "csrst_ensemble_set_shape": ([P, C.c_int, C.c_int, C.c_int], C.c_int),
+        "csrst_ensemble_set_shape": ([P, C.c_int, C.c_int, C.c_int, C.c_int], C.c_int),
         "csrst_ensemble_tune": ([P, C.c_int, D, C.c_int, I], C.c_int),
         "csrst_get_particles": ([P, D, D, D, D], C.c_int),
         "csrst_get_old_positions": ([P, D, D], C.c_int),

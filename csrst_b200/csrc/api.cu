@@ -2,6 +2,7 @@
 // memory, the order of kernel launches for one time step and its CUDA graph.
 #include <cub/cub.cuh>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -107,32 +108,40 @@ struct csrst_handle {
   double *d64 = nullptr;      // 4 n doubles: the bunch in FP64 for diagnostics and reads
 };
 
-// A batch of members stepped together: per-member argument tables in device
-// memory, one launch per phase of the time step for all members, and the
-// whole step captured as one CUDA graph.
-struct csrst_ensemble {
+// One part of a batch: its members' argument tables in device memory and the
+// streams its launches go to (the two shape-order groups of a push run side
+// by side on s and s2).
+struct EnsPart {
   std::vector<csrst_handle *> mem;
   int m = 0;
-  bool fp32 = false;
-  cudaStream_t s = nullptr;
-  cudaEvent_t done = nullptr;
-  // device tables (one entry per member)
-  PushArgs *push64[2] = {nullptr, nullptr};
-  Push32Args *push32[2] = {nullptr, nullptr};
+  long long particles = 0;
+  cudaStream_t s = nullptr, s2 = nullptr;
+  cudaEvent_t fork = nullptr, join = nullptr, end = nullptr;
+  std::vector<PushGroup> groups[2];  // [jcomp], one per shape order
+  std::vector<void *> blocks;        // device allocations of the push groups
   FieldArgs *f64[2] = {nullptr, nullptr};
   FieldArgsT<float> *f32[2] = {nullptr, nullptr};
   MoveArgs<double> *mv64 = nullptr;
   MoveArgs<float> *mv32 = nullptr;
   PrepArgs *prep = nullptr;
-  int *order = nullptr;
-  unsigned char *smem_ok = nullptr;
-  long long *ppre = nullptr;
   int *bpre_sub = nullptr, *bpre_ex[3] = {nullptr, nullptr, nullptr};
   int nsub = 0, nex[3] = {0, 0, 0};
-  long long total = 0;
-  size_t push_smem = 0;
-  // launch shapes (set by csrst_ensemble_tune)
-  int push_grid = 0, tx = 32, ty = 8;
+  int push_grid = 0;
+};
+
+// A batch of members stepped together: every phase of the time step is one
+// launch per part for all its members; the parts run side by side on their
+// own streams (so that one part's pushes overlap another's field sweeps),
+// and the whole step is captured as one CUDA graph.
+struct csrst_ensemble {
+  std::vector<csrst_handle *> mem;
+  int m = 0;
+  bool fp32 = false;
+  cudaStream_t s = nullptr;  // the ensemble's stream (graph launches, ordering with the members)
+  cudaEvent_t done = nullptr, fork = nullptr;
+  std::vector<EnsPart> parts;
+  // launch shapes (set by csrst_ensemble_set_shape / csrst_ensemble_tune)
+  int push_grid = 0, tx = 32, ty = 8, nparts = 1;
   cudaGraphExec_t graph = nullptr;
   std::string err;
 };
@@ -1050,16 +1059,30 @@ T *dev_copy(const std::vector<T> &v, cudaError_t &e) {
   return p;
 }
 
-void ensemble_free_tables(csrst_ensemble *e) {
+void part_free(EnsPart &P) {
   for (int k = 0; k < 2; ++k) {
-    cudaFree(e->push64[k]); cudaFree(e->push32[k]); cudaFree(e->f64[k]); cudaFree(e->f32[k]);
-    e->push64[k] = nullptr; e->push32[k] = nullptr; e->f64[k] = nullptr; e->f32[k] = nullptr;
+    cudaFree(P.f64[k]); cudaFree(P.f32[k]);
+    P.f64[k] = nullptr; P.f32[k] = nullptr;
+    P.groups[k].clear();
   }
-  cudaFree(e->mv64); cudaFree(e->mv32); cudaFree(e->prep); cudaFree(e->order); cudaFree(e->smem_ok);
-  cudaFree(e->ppre); cudaFree(e->bpre_sub);
-  for (int k = 0; k < 3; ++k) { cudaFree(e->bpre_ex[k]); e->bpre_ex[k] = nullptr; }
-  e->mv64 = nullptr; e->mv32 = nullptr; e->prep = nullptr; e->order = nullptr; e->smem_ok = nullptr;
-  e->ppre = nullptr; e->bpre_sub = nullptr;
+  for (void *p : P.blocks) cudaFree(p);
+  P.blocks.clear();
+  cudaFree(P.mv64); cudaFree(P.mv32); cudaFree(P.prep); cudaFree(P.bpre_sub);
+  for (int k = 0; k < 3; ++k) { cudaFree(P.bpre_ex[k]); P.bpre_ex[k] = nullptr; }
+  P.mv64 = nullptr; P.mv32 = nullptr; P.prep = nullptr; P.bpre_sub = nullptr;
+  if (P.fork) cudaEventDestroy(P.fork);
+  if (P.join) cudaEventDestroy(P.join);
+  if (P.end) cudaEventDestroy(P.end);
+  if (P.s2) cudaStreamDestroy(P.s2);
+  if (P.s) cudaStreamDestroy(P.s);
+  P.fork = P.join = P.end = nullptr;
+  P.s = P.s2 = nullptr;
+}
+
+void ensemble_free_tables(csrst_ensemble *e) {
+  if (e->s) cudaStreamSynchronize(e->s);
+  for (EnsPart &P : e->parts) part_free(P);
+  e->parts.clear();
   if (e->graph) { cudaGraphExecDestroy(e->graph); e->graph = nullptr; }
 }
 
@@ -1069,32 +1092,36 @@ int efail(csrst_ensemble *e, int code, const std::string &msg) {
   return code;
 }
 
-// Argument tables of the steady-state step (pending drift, current boxes).
-int ensemble_build(csrst_ensemble *e) {
-  ensemble_free_tables(e);
-  const int m = e->m;
-  std::vector<PushArgs> p64[2];
-  std::vector<Push32Args> p32[2];
+// Argument tables of the steady-state step (pending drift, current boxes) of
+// one part.
+cudaError_t part_build(csrst_ensemble *e, EnsPart &P) {
   std::vector<FieldArgs> a64[2];
   std::vector<FieldArgsT<float>> a32[2];
   std::vector<MoveArgs<double>> mv64;
   std::vector<MoveArgs<float>> mv32;
   std::vector<PrepArgs> prep;
-  std::vector<int> order, bsub(1, 0), bex[3];
-  std::vector<unsigned char> ok;
-  std::vector<long long> ppre(1, 0);
+  std::vector<int> bsub(1, 0), bex[3];
   for (int k = 0; k < 3; ++k) bex[k].assign(1, 0);
   const long long cap = e->fp32 ? push32_batch_smem_limit() : push_batch_smem_limit();
-  size_t smem = 0;
-  for (csrst_handle *h : e->mem) {
-    order.push_back(h->order);
+  // per shape order: members, their push arguments, shared-memory fit, particle prefix
+  struct Group {
+    std::vector<PushArgs> p64[2];
+    std::vector<Push32Args> p32[2];
+    std::vector<unsigned char> ok;
+    std::vector<long long> ppre{0};
+    size_t smem = 0;
+  } grp[3];
+  P.particles = 0;
+  for (csrst_handle *h : P.mem) {
     prep.push_back(prep_args(h->ws, h->b.hr0, h->b.hr1, h->order));
-    ppre.push_back(ppre.back() + h->n);
+    Group &G = grp[h->order];
+    G.ppre.push_back(G.ppre.back() + h->n);
+    P.particles += h->n;
     const size_t tiles = push_tile_bytes(h->order);
     const size_t need = (size_t)h->L0 * h->L1 * sizeof(unsigned long long) + tiles;
     const bool fits = (long long)need <= cap;
-    ok.push_back(fits ? 1 : 0);
-    smem = std::max(smem, fits ? need : tiles);
+    G.ok.push_back(fits ? 1 : 0);
+    G.smem = std::max(G.smem, fits ? need : tiles);
     int nb = 0;
     for (int c = 0; c < 2; ++c) {
       if (e->fp32) {
@@ -1104,7 +1131,7 @@ int ensemble_build(csrst_ensemble *e) {
         a32[c].push_back(a);
         Push32Args pa = push_args32(h, c);
         pa.pending = 1;
-        p32[c].push_back(pa);
+        G.p32[c].push_back(pa);
       } else {
         FieldArgs a = field_args(h, c);
         a.tx = e->tx; a.ty = e->ty;
@@ -1112,7 +1139,7 @@ int ensemble_build(csrst_ensemble *e) {
         a64[c].push_back(a);
         PushArgs pa = push_args(h, c);
         pa.pending = 1;
-        p64[c].push_back(pa);
+        G.p64[c].push_back(pa);
       }
     }
     if (e->fp32) mv32.push_back(MoveArgs<float>{a32[0].back(), h->scratchf, h->b.hr0, h->b.hr1});
@@ -1121,65 +1148,130 @@ int ensemble_build(csrst_ensemble *e) {
     for (int k = 0; k < 3; ++k) bex[k].push_back(bex[k].back() + (exchange_count(h->L0, h->L1, k) + 127) / 128);
   }
   cudaError_t err = cudaSuccess;
-  for (int c = 0; c < 2; ++c) {
-    if (e->fp32) { e->push32[c] = dev_copy(p32[c], err); e->f32[c] = dev_copy(a32[c], err); }
-    else { e->push64[c] = dev_copy(p64[c], err); e->f64[c] = dev_copy(a64[c], err); }
+  for (int o = 0; o < 3; ++o) {
+    Group &G = grp[o];
+    const int gm = (int)G.ok.size();
+    if (gm == 0) continue;
+    unsigned char *ok = dev_copy(G.ok, err);
+    long long *pp = dev_copy(G.ppre, err);
+    P.blocks.push_back(ok);
+    P.blocks.push_back(pp);
+    for (int c = 0; c < 2; ++c) {
+      void *args = e->fp32 ? (void *)dev_copy(G.p32[c], err) : (void *)dev_copy(G.p64[c], err);
+      P.blocks.push_back(args);
+      P.groups[c].push_back(PushGroup{o, gm, args, ok, pp, G.ppre.back(), 0, G.smem});
+    }
   }
-  if (e->fp32) e->mv32 = dev_copy(mv32, err);
-  else e->mv64 = dev_copy(mv64, err);
-  e->prep = dev_copy(prep, err);
-  e->order = dev_copy(order, err);
-  e->smem_ok = dev_copy(ok, err);
-  e->ppre = dev_copy(ppre, err);
-  e->bpre_sub = dev_copy(bsub, err);
-  for (int k = 0; k < 3; ++k) { e->bpre_ex[k] = dev_copy(bex[k], err); e->nex[k] = bex[k].back(); }
-  if (err != cudaSuccess) return efail(e, CSRST_E_CUDA, std::string("ensemble tables: ") + cudaGetErrorString(err));
-  e->nsub = bsub.back();
-  e->total = ppre.back();
-  e->push_smem = smem;
+  for (int c = 0; c < 2; ++c) {
+    if (e->fp32) P.f32[c] = dev_copy(a32[c], err);
+    else P.f64[c] = dev_copy(a64[c], err);
+  }
+  if (e->fp32) P.mv32 = dev_copy(mv32, err);
+  else P.mv64 = dev_copy(mv64, err);
+  P.prep = dev_copy(prep, err);
+  P.bpre_sub = dev_copy(bsub, err);
+  for (int k = 0; k < 3; ++k) { P.bpre_ex[k] = dev_copy(bex[k], err); P.nex[k] = bex[k].back(); }
+  P.nsub = bsub.back();
+  if (err == cudaSuccess) err = cudaStreamCreateWithFlags(&P.s, cudaStreamNonBlocking);
+  if (err == cudaSuccess) err = cudaStreamCreateWithFlags(&P.s2, cudaStreamNonBlocking);
+  if (err == cudaSuccess) err = cudaEventCreateWithFlags(&P.fork, cudaEventDisableTiming);
+  if (err == cudaSuccess) err = cudaEventCreateWithFlags(&P.join, cudaEventDisableTiming);
+  if (err == cudaSuccess) err = cudaEventCreateWithFlags(&P.end, cudaEventDisableTiming);
+  return err;
+}
+
+// Splits the members into parts of about equal particle counts (largest
+// first, each to the lightest part) and builds their tables.
+int ensemble_build(csrst_ensemble *e) {
+  ensemble_free_tables(e);
   if (e->push_grid <= 0) {
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     e->push_grid = 2 * sms;
   }
+  const int np = std::max(1, std::min(e->nparts, e->m));
+  e->parts.resize(np);
+  std::vector<int> idx(e->m);
+  for (int k = 0; k < e->m; ++k) idx[k] = k;
+  std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) { return e->mem[a]->n > e->mem[b]->n; });
+  std::vector<long long> load(np, 0);
+  std::vector<std::vector<int>> pick(np);
+  for (int k : idx) {
+    const int p = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+    pick[p].push_back(k);
+    load[p] += e->mem[k]->n;
+  }
+  long long all = 0;
+  for (int p = 0; p < np; ++p) {
+    std::sort(pick[p].begin(), pick[p].end());  // members in their given order
+    for (int k : pick[p]) e->parts[p].mem.push_back(e->mem[k]);
+    e->parts[p].m = (int)pick[p].size();
+    all += load[p];
+  }
+  for (EnsPart &P : e->parts) {
+    const cudaError_t c = part_build(e, P);
+    if (c != cudaSuccess) return efail(e, CSRST_E_CUDA, std::string("ensemble tables: ") + cudaGetErrorString(c));
+    P.push_grid = std::max(1, (int)((long long)e->push_grid * P.particles / (all > 0 ? all : 1)));
+    for (int c = 0; c < 2; ++c)
+      for (PushGroup &G : P.groups[c]) G.all = P.particles;
+  }
   return CSRST_OK;
 }
 
-void ensemble_push(csrst_ensemble *e, int jcomp) {
-  if (e->fp32)
-    launch_push32_batch(e->push32[jcomp], e->order, e->smem_ok, e->ppre, e->m, e->total, e->push_grid,
-                        e->push_smem, e->prep, e->s);
-  else
-    launch_push_batch(e->push64[jcomp], e->order, e->smem_ok, e->ppre, e->m, e->total, e->push_grid, e->push_smem,
-                      e->prep, e->s);
+// The push of every member of a part: the shape-order groups run side by side
+// on two streams, after the per-member preparation and before the bounds.
+void part_push(csrst_ensemble *e, EnsPart &P, int jcomp) {
+  const std::vector<PushGroup> &G = P.groups[jcomp];
+  const int ng = (int)G.size();
+  auto batch = [&](const PushGroup *g, int n, int grid, const PrepArgs *prep, cudaStream_t st, int parts) {
+    if (e->fp32) launch_push32_batch(g, n, P.m, grid, prep, st, parts);
+    else launch_push_batch(g, n, P.m, grid, prep, st, parts);
+  };
+  if (ng <= 1) {
+    batch(G.data(), ng, P.push_grid, P.prep, P.s, 3);
+    return;
+  }
+  batch(nullptr, 0, 0, P.prep, P.s, 1);
+  cudaEventRecord(P.fork, P.s);
+  cudaStreamWaitEvent(P.s2, P.fork, 0);
+  for (int g = 0; g < ng; ++g) batch(&G[g], 1, P.push_grid, nullptr, (g & 1) ? P.s2 : P.s, 0);
+  cudaEventRecord(P.join, P.s2);
+  cudaStreamWaitEvent(P.s, P.join, 0);
+  batch(nullptr, 0, 0, P.prep, P.s, 2);
 }
 
 template <class T>
-void ensemble_fields(csrst_ensemble *e, const FieldArgsT<T> *a0, const FieldArgsT<T> *a1, const MoveArgs<T> *mv,
-                     int part) {
-  if (part == 0) {  // half H, Ex, half H (after the first push)
-    launch_half_h_batch(a0, e->bpre_sub, e->m, e->nsub, e->s);
-    launch_exchange_batch(a0, e->bpre_ex[0], e->m, e->nex[0], 0, e->s);
-    launch_update_e_batch(a0, e->bpre_sub, e->m, e->nsub, 0, e->s);
-    launch_exchange_batch(a0, e->bpre_ex[1], e->m, e->nex[1], 1, e->s);
-    launch_half_h_batch(a0, e->bpre_sub, e->m, e->nsub, e->s);
-    launch_exchange_batch(a0, e->bpre_ex[0], e->m, e->nex[0], 0, e->s);
+void part_fields(EnsPart &P, const FieldArgsT<T> *a0, const FieldArgsT<T> *a1, const MoveArgs<T> *mv, int half) {
+  if (half == 0) {  // half H, Ex, half H (after the first push)
+    launch_half_h_batch(a0, P.bpre_sub, P.m, P.nsub, P.s);
+    launch_exchange_batch(a0, P.bpre_ex[0], P.m, P.nex[0], 0, P.s);
+    launch_update_e_batch(a0, P.bpre_sub, P.m, P.nsub, 0, P.s);
+    launch_exchange_batch(a0, P.bpre_ex[1], P.m, P.nex[1], 1, P.s);
+    launch_half_h_batch(a0, P.bpre_sub, P.m, P.nsub, P.s);
+    launch_exchange_batch(a0, P.bpre_ex[0], P.m, P.nex[0], 0, P.s);
   } else {          // Ey (after the second push), then the window move
-    launch_update_e_batch(a1, e->bpre_sub, e->m, e->nsub, 1, e->s);
-    launch_exchange_batch(a1, e->bpre_ex[2], e->m, e->nex[2], 2, e->s);
-    launch_move_batch(mv, e->m, e->s);
+    launch_update_e_batch(a1, P.bpre_sub, P.m, P.nsub, 1, P.s);
+    launch_exchange_batch(a1, P.bpre_ex[2], P.m, P.nex[2], 2, P.s);
+    launch_move_batch(mv, P.m, P.s);
   }
 }
 
-// One steady-state time step of every member (main.cpp:390-506).
+// One steady-state time step of every member (main.cpp:390-506), all parts
+// side by side, joined back on the ensemble stream.
 void ensemble_step_async(csrst_ensemble *e) {
-  ensemble_push(e, 0);
-  if (e->fp32) ensemble_fields(e, e->f32[0], e->f32[1], e->mv32, 0);
-  else ensemble_fields(e, e->f64[0], e->f64[1], e->mv64, 0);
-  ensemble_push(e, 1);
-  if (e->fp32) ensemble_fields(e, e->f32[0], e->f32[1], e->mv32, 1);
-  else ensemble_fields(e, e->f64[0], e->f64[1], e->mv64, 1);
+  cudaEventRecord(e->fork, e->s);
+  for (EnsPart &P : e->parts) {
+    cudaStreamWaitEvent(P.s, e->fork, 0);
+    part_push(e, P, 0);
+    if (e->fp32) part_fields(P, P.f32[0], P.f32[1], P.mv32, 0);
+    else part_fields(P, P.f64[0], P.f64[1], P.mv64, 0);
+    part_push(e, P, 1);
+    if (e->fp32) part_fields(P, P.f32[0], P.f32[1], P.mv32, 1);
+    else part_fields(P, P.f64[0], P.f64[1], P.mv64, 1);
+    cudaEventRecord(P.end, P.s);
+    cudaStreamWaitEvent(e->s, P.end, 0);
+  }
 }
 
 // Brings every member to the steady state of the loop (the stored positions
@@ -1245,7 +1337,8 @@ int csrst_ensemble_create(csrst_handle *const *members, int m, csrst_ensemble **
     e->mem.push_back(h);
   }
   if (cudaStreamCreateWithFlags(&e->s, cudaStreamNonBlocking) != cudaSuccess ||
-      cudaEventCreateWithFlags(&e->done, cudaEventDisableTiming) != cudaSuccess) {
+      cudaEventCreateWithFlags(&e->done, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&e->fork, cudaEventDisableTiming) != cudaSuccess) {
     csrst_ensemble_destroy(e);
     return efail(nullptr, CSRST_E_CUDA, "ensemble: stream");
   }
@@ -1261,9 +1354,9 @@ int csrst_ensemble_create(csrst_handle *const *members, int m, csrst_ensemble **
 
 int csrst_ensemble_destroy(csrst_ensemble *e) {
   if (!e) return CSRST_OK;
-  if (e->s) cudaStreamSynchronize(e->s);
   ensemble_free_tables(e);
   if (e->done) cudaEventDestroy(e->done);
+  if (e->fork) cudaEventDestroy(e->fork);
   if (e->s) cudaStreamDestroy(e->s);
   delete e;
   return CSRST_OK;
@@ -1314,21 +1407,23 @@ int csrst_ensemble_sync(csrst_ensemble *e, int *bad_member) {
   return CSRST_OK;
 }
 
-// Launch shapes: CTAs of the batched push (0 = 2 per SM) and the static-sweep
-// tile (tx * ty = 256).  Results do not depend on them.
-int csrst_ensemble_set_shape(csrst_ensemble *e, int push_ctas, int tx, int ty) {
-  if (!e || push_ctas < 0 || tx <= 0 || ty <= 0 || tx * ty != 256) return efail(e, CSRST_E_ARG, "invalid shape");
+// Launch shapes: CTAs of the batched push over all parts (0 = two per SM),
+// the static-sweep tile (tx * ty = 256) and the number of parts that run side
+// by side.  Results do not depend on them.
+int csrst_ensemble_set_shape(csrst_ensemble *e, int push_ctas, int tx, int ty, int parts) {
+  if (!e || push_ctas < 0 || tx <= 0 || ty <= 0 || tx * ty != 256 || parts < 1)
+    return efail(e, CSRST_E_ARG, "invalid shape");
   if (cudaStreamSynchronize(e->s) != cudaSuccess) return efail(e, CSRST_E_CUDA, "ensemble stream");
   e->push_grid = push_ctas;
   e->tx = tx; e->ty = ty;
+  e->nparts = parts;
   return ensemble_build(e);
 }
 
 // The autotuner: times `steps` steady-state steps (events on the ensemble
 // stream, launched eagerly) for each candidate shape and keeps the fastest.
 // The timed steps are real steps of the members.  report: rows of
-// (push_ctas, tx, ty, ms per step), ncand rows at most; returns the count
-// through *nrows.
+// (push_ctas, tx, ty, parts, ms per step); *nrows receives the row count.
 int csrst_ensemble_tune(csrst_ensemble *e, int steps, double *report, int max_rows, int *nrows) {
   if (!e || steps < 1) return efail(e, CSRST_E_ARG, "tune: invalid arguments");
   int dev = 0, sms = 148;
@@ -1337,38 +1432,42 @@ int csrst_ensemble_tune(csrst_ensemble *e, int steps, double *report, int max_ro
   int warm = 1;
   int rc = ensemble_steady(e, warm);
   if (rc) return rc;
-  const int ctas[4] = {sms, 2 * sms, 4 * sms, 8 * sms};
-  const int tiles[3][2] = {{32, 8}, {64, 4}, {128, 2}};
+  const int ctas[3] = {4 * sms, 16 * sms, 32 * sms};
+  const int tiles[2][2] = {{32, 8}, {128, 2}};
+  const int parts[3] = {1, 2, 4};
   cudaEvent_t t0, t1;
   cudaEventCreate(&t0);
   cudaEventCreate(&t1);
   float best = 1e30f;
-  int bc = 2 * sms, bt = 0, rows = 0;
-  for (int a = 0; a < 4; ++a)
-    for (int b = 0; b < 3; ++b) {
-      e->push_grid = ctas[a];
-      e->tx = tiles[b][0]; e->ty = tiles[b][1];
-      if ((rc = ensemble_build(e))) return rc;
-      ensemble_step_async(e);  // untimed warm-up of this shape
-      cudaEventRecord(t0, e->s);
-      for (int k = 0; k < steps; ++k) ensemble_step_async(e);
-      cudaEventRecord(t1, e->s);
-      if (cudaEventSynchronize(t1) != cudaSuccess) return efail(e, CSRST_E_CUDA, "tune: timing");
-      float ms = 0;
-      cudaEventElapsedTime(&ms, t0, t1);
-      ms /= steps;
-      if (report && rows < max_rows) {
-        report[4 * rows] = ctas[a]; report[4 * rows + 1] = tiles[b][0];
-        report[4 * rows + 2] = tiles[b][1]; report[4 * rows + 3] = ms;
+  int bc = 2 * sms, bt = 0, bp = 1, rows = 0;
+  for (int pa = 0; pa < 3; ++pa)
+    for (int a = 0; a < 3; ++a)
+      for (int b = 0; b < 2; ++b) {
+        e->push_grid = ctas[a];
+        e->tx = tiles[b][0]; e->ty = tiles[b][1];
+        e->nparts = parts[pa];
+        if ((rc = ensemble_build(e))) return rc;
+        ensemble_step_async(e);  // untimed warm-up of this shape
+        cudaEventRecord(t0, e->s);
+        for (int k = 0; k < steps; ++k) ensemble_step_async(e);
+        cudaEventRecord(t1, e->s);
+        if (cudaEventSynchronize(t1) != cudaSuccess) return efail(e, CSRST_E_CUDA, "tune: timing");
+        float ms = 0;
+        cudaEventElapsedTime(&ms, t0, t1);
+        ms /= steps;
+        if (report && rows < max_rows) {
+          double *r = report + 5 * rows;
+          r[0] = ctas[a]; r[1] = tiles[b][0]; r[2] = tiles[b][1]; r[3] = parts[pa]; r[4] = ms;
+        }
+        ++rows;
+        if (ms < best) { best = ms; bc = ctas[a]; bt = b; bp = parts[pa]; }
       }
-      ++rows;
-      if (ms < best) { best = ms; bc = ctas[a]; bt = b; }
-    }
   cudaEventDestroy(t0);
   cudaEventDestroy(t1);
   ensemble_mark(e);
   e->push_grid = bc;
   e->tx = tiles[bt][0]; e->ty = tiles[bt][1];
+  e->nparts = bp;
   if (nrows) *nrows = rows < max_rows ? rows : max_rows;
   if ((rc = ensemble_build(e))) return rc;
   return ensemble_release(e);

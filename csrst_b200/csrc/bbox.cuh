@@ -16,9 +16,10 @@ __device__ __forceinline__ void warp_bbox(double &mn0, double &mn1, double &mx0,
   }
 }
 
-// Reduce a per-thread box over the CTA and merge it into dst[4] with atomics.
-__device__ __forceinline__ void block_bbox(double mn0, double mn1, double mx0, double mx1, long long *dst) {
-  __shared__ double sb[4][32];
+// Reduce a per-thread box over the CTA and merge it into dst[4] with atomics;
+// sb is shared scratch of 4 x 32 doubles.
+__device__ __forceinline__ void block_bbox(double mn0, double mn1, double mx0, double mx1, long long *dst,
+                                           double (*sb)[32]) {
   warp_bbox(mn0, mn1, mx0, mx1);
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
   if (lane == 0) { sb[0][w] = mn0; sb[1][w] = mn1; sb[2][w] = mx0; sb[3][w] = mx1; }
@@ -38,6 +39,14 @@ __device__ __forceinline__ void block_bbox(double mn0, double mn1, double mx0, d
   }
   __syncthreads();
 }
+
+// Shared scratch of one push CTA, declared once per kernel so that a kernel
+// that inlines several push variants does not hold one copy per variant.
+struct PushShared {
+  double sb[4][32];  // block_bbox
+  int tb[4];         // touched box of the CTA (window cells)
+  int err;           // the member's sticky error at entry
+};
 
 __device__ __forceinline__ void bbox_reset(long long *b) {
   b[0] = dbl_ord(INFINITY); b[1] = dbl_ord(INFINITY);

@@ -362,8 +362,7 @@ template <class T>
 __global__ void __launch_bounds__(1024) k_move(MoveArgs<T> m) { move_body(m); }
 
 // Member of global block b: bpre holds the first block of every member (m + 1
-// entries).  The member's arguments are copied to shared memory, which the
-// kernels' global stores cannot alias.
+// entries).
 __device__ __forceinline__ int batch_member(const int *bpre, int m, int b) {
   int lo = 0, hi = m - 1;
   while (lo < hi) {
@@ -373,12 +372,11 @@ __device__ __forceinline__ int batch_member(const int *bpre, int m, int b) {
   return lo;
 }
 
+// The member's arguments are read in place: every thread of a block reads the
+// same words, which the L1 cache serves after the first.
 template <class T>
 __device__ __forceinline__ const FieldArgsT<T> &batch_args(const FieldArgsT<T> *args, int mm) {
-  __shared__ FieldArgsT<T> sa;
-  if (threadIdx.x == 0) sa = args[mm];
-  __syncthreads();
-  return sa;
+  return args[mm];
 }
 
 template <class T>

@@ -76,13 +76,26 @@ struct PrepArgs {
   int em0, em2, cm0;  // gather-patch margins of the shape order
 };
 
+// The members of one shape order in a batched push (device arrays of m
+// entries; ppre: first particle of each member, m + 1 entries).
+struct PushGroup {
+  int order, m;
+  const void *args;                 // PushArgs or Push32Args
+  const unsigned char *smem_ok;     // the member's window accumulator fits in shared memory
+  const long long *ppre;
+  long long total, all;             // particles of the group, of the whole batch
+  size_t smem;                      // dynamic shared memory of the group's launch
+};
+
 // particles.cu
 PrepArgs prep_args(WinState *ws, double h0, double h1, int order);
 size_t push_tile_bytes(int order);
 long long push_batch_smem_limit();
-// prep + push + post + bounds of a batch of FP64 members (device arrays)
-void launch_push_batch(const PushArgs *args, const int *order, const unsigned char *smem_ok, const long long *ppre,
-                       int m, long long total, int grid, size_t smem, const PrepArgs *prep, cudaStream_t s);
+// prep + push + post + bounds of a batch of FP64 members: one push launch per
+// shape order present, the CTAs (grid in total) shared out by particle count.
+// parts: 1 = the per-member preparation, 2 = the per-member bookkeeping after.
+void launch_push_batch(const PushGroup *groups, int ngroups, int m, int grid, const PrepArgs *prep, cudaStream_t s,
+                       int parts = 3);
 void launch_bbox_next(const double *x, const double *y, const double *px, const double *py, long long n,
                       double half, int pending, WinState *ws, cudaStream_t s);
 void launch_push_prep(WinState *ws, double h0, double h1, int order, cudaStream_t s);
@@ -188,9 +201,8 @@ struct Push32Args {
 
 int launch_push32(const Push32Args &a, int order, int L0, int L1, int grid, cudaStream_t s);
 long long push32_batch_smem_limit();
-void launch_push32_batch(const Push32Args *args, const int *order, const unsigned char *smem_ok,
-                         const long long *ppre, int m, long long total, int grid, size_t smem,
-                         const PrepArgs *prep, cudaStream_t s);
+void launch_push32_batch(const PushGroup *groups, int ngroups, int m, int grid, const PrepArgs *prep,
+                         cudaStream_t s, int parts = 3);
 void launch_prep32(WinState *ws, int order, cudaStream_t s);
 void launch_bounds32(WinState *ws, cudaStream_t s);
 void launch_bbox32(const Bunch32 &b, double P0, double P1, double kh0, double kh1, int pending, WinState *ws,

@@ -38,7 +38,8 @@ __global__ void k_bbox_next(const double *x, const double *y, const double *px, 
     a0 = a0 + w0; a1 = a1 + w1;
     mn0 = fmin(mn0, a0); mn1 = fmin(mn1, a1); mx0 = fmax(mx0, a0); mx1 = fmax(mx1, a1);
   }
-  block_bbox(mn0, mn1, mx0, mx1, ws->bb[ws->cur]);
+  __shared__ double sb[4][32];
+  block_bbox(mn0, mn1, mx0, mx1, ws->bb[ws->cur], sb);
 }
 
 __global__ void k_bbox_clear(WinState *ws, int slot) {
@@ -92,14 +93,13 @@ __global__ void k_push_post(WinState *ws) {
 // together; it ends with a barrier, so a CTA can run it for several members
 // in turn.
 template <int ORDER, bool SMEM>
-__device__ __forceinline__ void push_body(const PushArgs &a, long long beg, long long end,
+__device__ __forceinline__ void push_body(const PushArgs &a, long long beg, long long end, PushShared &sh,
                                           unsigned long long *sacc) {
-  __shared__ int tb[4];  // touched box of this CTA (window cells)
+  int *tb = sh.tb;  // touched box of this CTA (window cells)
   WinState *ws = a.ws;
-  __shared__ int s_err;
-  if (threadIdx.x == 0) s_err = *(volatile int *)&ws->err;
+  if (threadIdx.x == 0) sh.err = *(volatile int *)&ws->err;
   __syncthreads();
-  if (s_err) return;  // the whole CTA leaves together
+  if (sh.err) return;  // the whole CTA leaves together
   const int L0 = ws->L0, L1 = ws->L1;
   const int ncell = L0 * L1;
   using Tile = typename TileFor<ORDER>::T;
@@ -191,8 +191,8 @@ __device__ __forceinline__ void push_body(const PushArgs &a, long long beg, long
   }
   tile.template flush<SMEM>(win, L0, L1);
   if (overflow) set_err(ws, kErrCrossings);
-  block_bbox(amn0, amn1, amx0, amx1, ws->bball);
-  block_bbox(bmn0, bmn1, bmx0, bmx1, ws->bb[1 - ws->cur]);
+  block_bbox(amn0, amn1, amx0, amx1, ws->bball, sh.sb);
+  block_bbox(bmn0, bmn1, bmx0, bmx1, ws->bb[1 - ws->cur], sh.sb);
   if (SMEM) {
     if (tile.ti1 >= 0) {
       atomicMin(&tb[0], tile.ti0); atomicMin(&tb[1], tile.tj0);
@@ -215,20 +215,22 @@ __device__ __forceinline__ void push_body(const PushArgs &a, long long beg, long
 template <int ORDER, bool SMEM>
 __global__ void __launch_bounds__(256, 2) k_push(PushArgs a) {
   extern __shared__ unsigned long long sacc[];
+  __shared__ PushShared sh;
   const long long per = (a.n + gridDim.x - 1) / gridDim.x;
   const long long beg = (long long)blockIdx.x * per;
   const long long end = beg + per < a.n ? beg + per : a.n;
-  push_body<ORDER, SMEM>(a, beg, end, sacc);
+  push_body<ORDER, SMEM>(a, beg, end, sh, sacc);
 }
 
 // One push over a batch of members: the members' particles form one index
 // range (ppre: first particle of each member, m + 1 entries) that is cut into
 // equal contiguous shares, one per CTA; a CTA runs the push of every member
 // its share overlaps, with that member's shape order and accumulator.
-__global__ void __launch_bounds__(256, 2) k_push_batch(const PushArgs *args, const int *order,
-                                                       const unsigned char *smem_ok, const long long *ppre,
-                                                       int m, long long per) {
+template <int ORDER>
+__global__ void __launch_bounds__(256, 2) k_push_batch(const PushArgs *args, const unsigned char *smem_ok,
+                                                       const long long *ppre, int m, long long per) {
   extern __shared__ unsigned long long sacc[];
+  __shared__ PushShared sh;
   __shared__ PushArgs sa;
   const long long total = ppre[m];
   const long long g0 = (long long)blockIdx.x * per;
@@ -240,16 +242,8 @@ __global__ void __launch_bounds__(256, 2) k_push_batch(const PushArgs *args, con
     __syncthreads();
     if (threadIdx.x == 0) sa = args[mm];
     __syncthreads();
-    const int o = order[mm];
-    if (smem_ok[mm]) {
-      if (o == 0) push_body<0, true>(sa, lb, le, sacc);
-      else if (o == 1) push_body<1, true>(sa, lb, le, sacc);
-      else push_body<2, true>(sa, lb, le, sacc);
-    } else {
-      if (o == 0) push_body<0, false>(sa, lb, le, sacc);
-      else if (o == 1) push_body<1, false>(sa, lb, le, sacc);
-      else push_body<2, false>(sa, lb, le, sacc);
-    }
+    if (smem_ok[mm]) push_body<ORDER, true>(sa, lb, le, sh, sacc);
+    else push_body<ORDER, false>(sa, lb, le, sh, sacc);
   }
 }
 
@@ -368,25 +362,41 @@ long long push_batch_smem_limit() {
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
     cudaFuncAttributes fa{};
-    cudaFuncGetAttributes(&fa, k_push_batch);
+    cudaFuncGetAttributes(&fa, k_push_batch<1>);
     lim = (long long)v - (long long)fa.sharedSizeBytes;
-    if (cudaFuncSetAttribute(k_push_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lim) != cudaSuccess)
+    // keep two CTAs per SM: half the SM's shared memory less the static part
+    // and the 1 KB the runtime reserves per CTA
+    int per_sm = 0;
+    cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+    const long long two = (long long)per_sm / 2 - (long long)fa.sharedSizeBytes - 1024;
+    if (two > 0 && two < lim) lim = two;
+    if (cudaFuncSetAttribute(k_push_batch<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lim) != cudaSuccess ||
+        cudaFuncSetAttribute(k_push_batch<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lim) != cudaSuccess ||
+        cudaFuncSetAttribute(k_push_batch<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lim) != cudaSuccess)
       lim = 0;
     cudaGetLastError();
   }
   return lim;
 }
 
-void launch_push_batch(const PushArgs *args, const int *order, const unsigned char *smem_ok, const long long *ppre,
-                       int m, long long total, int grid, size_t smem, const PrepArgs *prep, cudaStream_t s) {
+void launch_push_batch(const PushGroup *groups, int ngroups, int m, int grid, const PrepArgs *prep, cudaStream_t s,
+            int parts) {
   const int tb = (m + 127) / 128;
-  k_push_prep_batch<<<tb, 128, 0, s>>>(prep, m);
-  if (total > 0 && grid > 0) {
-    const long long per = (total + grid - 1) / grid;
-    k_push_batch<<<grid, 256, smem, s>>>(args, order, smem_ok, ppre, m, per);
+  if (parts & 1) k_push_prep_batch<<<tb, 128, 0, s>>>(prep, m);
+  for (int g = 0; g < ngroups; ++g) {
+    const PushGroup &G = groups[g];
+    if (G.total <= 0) continue;
+    const int ctas = (int)((long long)grid * G.total / (G.all > 0 ? G.all : G.total)) + 1;
+    const long long per = (G.total + ctas - 1) / ctas;
+    const PushArgs *args = static_cast<const PushArgs *>(G.args);
+    if (G.order == 0) k_push_batch<0><<<ctas, 256, G.smem, s>>>(args, G.smem_ok, G.ppre, G.m, per);
+    else if (G.order == 1) k_push_batch<1><<<ctas, 256, G.smem, s>>>(args, G.smem_ok, G.ppre, G.m, per);
+    else k_push_batch<2><<<ctas, 256, G.smem, s>>>(args, G.smem_ok, G.ppre, G.m, per);
   }
-  k_push_post_batch<<<tb, 128, 0, s>>>(prep, m);
-  k_global_bounds_batch<<<tb, 128, 0, s>>>(prep, m);
+  if (parts & 2) {
+    k_push_post_batch<<<tb, 128, 0, s>>>(prep, m);
+    k_global_bounds_batch<<<tb, 128, 0, s>>>(prep, m);
+  }
 }
 
 // Largest dynamic shared memory the window accumulator may use for this

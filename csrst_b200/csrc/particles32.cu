@@ -75,14 +75,13 @@ __device__ __forceinline__ void store_pos(double t0, double t1, int ci, int cj, 
 // One CTA's share [beg, end) of one push; called by all threads of the CTA,
 // ends with a barrier (a CTA may run it for several members in turn).
 template <int ORDER, bool SMEM>
-__device__ __forceinline__ void push32_body(const Push32Args &a, long long beg, long long end,
+__device__ __forceinline__ void push32_body(const Push32Args &a, long long beg, long long end, PushShared &sh,
                                             unsigned long long *sacc) {
-  __shared__ int tb[4];
-  __shared__ int s_err;
+  int *tb = sh.tb;
   WinState *ws = a.ws;
-  if (threadIdx.x == 0) s_err = *(volatile int *)&ws->err;
+  if (threadIdx.x == 0) sh.err = *(volatile int *)&ws->err;
   __syncthreads();
-  if (s_err) return;  // the whole CTA leaves together
+  if (sh.err) return;  // the whole CTA leaves together
   const int L0 = ws->L0, L1 = ws->L1, WP0 = ws->P0, WP1 = ws->P1;
   using Tile = typename TileFor<ORDER>::T;
   unsigned long long *win = SMEM ? sacc : a.acc;
@@ -194,8 +193,8 @@ __device__ __forceinline__ void push32_body(const Push32Args &a, long long beg, 
   }
   tile.template flush<SMEM>(win, L0, L1);
   if (overflow) set_err(ws, kErrCrossings);
-  block_bbox(amn0, amn1, amx0, amx1, ws->bball);
-  block_bbox(bmn0, bmn1, bmx0, bmx1, ws->bb[1 - ws->cur]);
+  block_bbox(amn0, amn1, amx0, amx1, ws->bball, sh.sb);
+  block_bbox(bmn0, bmn1, bmx0, bmx1, ws->bb[1 - ws->cur], sh.sb);
   if (SMEM) {
     if (tile.ti1 >= 0) {
       atomicMin(&tb[0], tile.ti0); atomicMin(&tb[1], tile.tj0);
@@ -218,17 +217,19 @@ __device__ __forceinline__ void push32_body(const Push32Args &a, long long beg, 
 template <int ORDER, bool SMEM>
 __global__ void __launch_bounds__(256, 2) k_push32(Push32Args a) {
   extern __shared__ unsigned long long sacc[];
+  __shared__ PushShared sh;
   const long long per = (a.b.n + gridDim.x - 1) / gridDim.x;
   const long long beg = (long long)blockIdx.x * per;
   const long long end = beg + per < a.b.n ? beg + per : a.b.n;
-  push32_body<ORDER, SMEM>(a, beg, end, sacc);
+  push32_body<ORDER, SMEM>(a, beg, end, sh, sacc);
 }
 
 // One push over a batch of FP32-mode members (see k_push_batch).
-__global__ void __launch_bounds__(256, 2) k_push32_batch(const Push32Args *args, const int *order,
-                                                         const unsigned char *smem_ok, const long long *ppre,
-                                                         int m, long long per) {
+template <int ORDER>
+__global__ void __launch_bounds__(256, 2) k_push32_batch(const Push32Args *args, const unsigned char *smem_ok,
+                                                       const long long *ppre, int m, long long per) {
   extern __shared__ unsigned long long sacc[];
+  __shared__ PushShared sh;
   __shared__ Push32Args sa;
   const long long total = ppre[m];
   const long long g0 = (long long)blockIdx.x * per;
@@ -240,16 +241,8 @@ __global__ void __launch_bounds__(256, 2) k_push32_batch(const Push32Args *args,
     __syncthreads();
     if (threadIdx.x == 0) sa = args[mm];
     __syncthreads();
-    const int o = order[mm];
-    if (smem_ok[mm]) {
-      if (o == 0) push32_body<0, true>(sa, lb, le, sacc);
-      else if (o == 1) push32_body<1, true>(sa, lb, le, sacc);
-      else push32_body<2, true>(sa, lb, le, sacc);
-    } else {
-      if (o == 0) push32_body<0, false>(sa, lb, le, sacc);
-      else if (o == 1) push32_body<1, false>(sa, lb, le, sacc);
-      else push32_body<2, false>(sa, lb, le, sacc);
-    }
+    if (smem_ok[mm]) push32_body<ORDER, true>(sa, lb, le, sh, sacc);
+    else push32_body<ORDER, false>(sa, lb, le, sh, sacc);
   }
 }
 
@@ -323,7 +316,8 @@ __global__ void k_bbox32(Bunch32 b, double P0, double P1, double kh0, double kh1
     const double x0 = cellc(ci, dadd(s0, w0)), x1 = cellc(cj, dadd(s1, w1));
     mn0 = fmin(mn0, x0); mn1 = fmin(mn1, x1); mx0 = fmax(mx0, x0); mx1 = fmax(mx1, x1);
   }
-  block_bbox(mn0, mn1, mx0, mx1, ws->bb[ws->cur]);
+  __shared__ double sb[4][32];
+  block_bbox(mn0, mn1, mx0, mx1, ws->bb[ws->cur], sb);
 }
 
 // R += kd * v (cells), kd = dt c / h (PartBunch::drift_particles).
@@ -451,9 +445,17 @@ long long push32_batch_smem_limit() {
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
     cudaFuncAttributes fa{};
-    cudaFuncGetAttributes(&fa, k_push32_batch);
+    cudaFuncGetAttributes(&fa, k_push32_batch<1>);
     lim = (long long)v - (long long)fa.sharedSizeBytes;
-    if (cudaFuncSetAttribute(k_push32_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lim) !=
+    // keep two CTAs per SM: half the SM's shared memory less the static part
+    // and the 1 KB the runtime reserves per CTA
+    int per_sm = 0;
+    cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+    const long long two = (long long)per_sm / 2 - (long long)fa.sharedSizeBytes - 1024;
+    if (two > 0 && two < lim) lim = two;
+    if (cudaFuncSetAttribute(k_push32_batch<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lim) != cudaSuccess ||
+        cudaFuncSetAttribute(k_push32_batch<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lim) != cudaSuccess ||
+        cudaFuncSetAttribute(k_push32_batch<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lim) !=
         cudaSuccess)
       lim = 0;
     cudaGetLastError();
@@ -461,17 +463,24 @@ long long push32_batch_smem_limit() {
   return lim;
 }
 
-void launch_push32_batch(const Push32Args *args, const int *order, const unsigned char *smem_ok,
-                         const long long *ppre, int m, long long total, int grid, size_t smem,
-                         const PrepArgs *prep, cudaStream_t s) {
+void launch_push32_batch(const PushGroup *groups, int ngroups, int m, int grid, const PrepArgs *prep, cudaStream_t s,
+            int parts) {
   const int tb = (m + 127) / 128;
-  k_prep32_batch<<<tb, 128, 0, s>>>(prep, m);
-  if (total > 0 && grid > 0) {
-    const long long per = (total + grid - 1) / grid;
-    k_push32_batch<<<grid, 256, smem, s>>>(args, order, smem_ok, ppre, m, per);
+  if (parts & 1) k_prep32_batch<<<tb, 128, 0, s>>>(prep, m);
+  for (int g = 0; g < ngroups; ++g) {
+    const PushGroup &G = groups[g];
+    if (G.total <= 0) continue;
+    const int ctas = (int)((long long)grid * G.total / (G.all > 0 ? G.all : G.total)) + 1;
+    const long long per = (G.total + ctas - 1) / ctas;
+    const Push32Args *args = static_cast<const Push32Args *>(G.args);
+    if (G.order == 0) k_push32_batch<0><<<ctas, 256, G.smem, s>>>(args, G.smem_ok, G.ppre, G.m, per);
+    else if (G.order == 1) k_push32_batch<1><<<ctas, 256, G.smem, s>>>(args, G.smem_ok, G.ppre, G.m, per);
+    else k_push32_batch<2><<<ctas, 256, G.smem, s>>>(args, G.smem_ok, G.ppre, G.m, per);
   }
-  k_post32_batch<<<tb, 128, 0, s>>>(prep, m);
-  k_bounds32_batch<<<tb, 128, 0, s>>>(prep, m);
+  if (parts & 2) {
+    k_post32_batch<<<tb, 128, 0, s>>>(prep, m);
+    k_bounds32_batch<<<tb, 128, 0, s>>>(prep, m);
+  }
 }
 
 void launch_prep32(WinState *ws, int order, cudaStream_t s) {

@@ -201,16 +201,16 @@ class Ensemble:
     def stream(self):
         return lib().csrst_ensemble_stream(self._e)
 
-    def set_shape(self, push_ctas, tx=32, ty=8):
-        self._ck(lib().csrst_ensemble_set_shape(self._e, int(push_ctas), int(tx), int(ty)))
+    def set_shape(self, push_ctas, tx=32, ty=8, parts=1):
+        self._ck(lib().csrst_ensemble_set_shape(self._e, int(push_ctas), int(tx), int(ty), int(parts)))
 
     def tune(self, steps=3):
         """Autotunes the launch shapes on real steps; returns the timing table
-        [(push_ctas, tx, ty, ms_per_step)] and leaves the fastest selected."""
-        rows = np.zeros(4 * 64)
+        [(push_ctas, tx, ty, parts, ms_per_step)] and leaves the fastest selected."""
+        rows = np.zeros(5 * 64)
         n = C.c_int(0)
         self._ck(lib().csrst_ensemble_tune(self._e, int(steps), ptr(rows), 64, C.byref(n)))
-        return [tuple(rows[4 * k:4 * k + 4]) for k in range(n.value)]
+        return [tuple(rows[5 * k:5 * k + 5]) for k in range(n.value)]
 
     def close(self):
         if getattr(self, "_e", None) is not None:

@@ -148,12 +148,14 @@ void *csrst_ensemble_stream(csrst_ensemble *e);
 int csrst_ensemble_step(csrst_ensemble *e, int nsteps);
 /* Waits for the ensemble; returns the first member's sticky error (its index in *bad_member). */
 int csrst_ensemble_sync(csrst_ensemble *e, int *bad_member);
-/* Launch shapes: CTAs of the batched push (0 = two per SM) and the static-sweep
- * tile tx x ty (tx * ty = 256).  Results do not depend on them. */
-int csrst_ensemble_set_shape(csrst_ensemble *e, int push_ctas, int tx, int ty);
+/* Launch shapes: CTAs of the batched push (0 = two per SM), the static-sweep
+ * tile tx x ty (tx * ty = 256) and the number of parts the members are split
+ * into, which step side by side on their own streams.  Results do not depend
+ * on them. */
+int csrst_ensemble_set_shape(csrst_ensemble *e, int push_ctas, int tx, int ty, int parts);
 /* Autotuner: times `steps` steps for each candidate shape and keeps the
  * fastest; the timed steps are real steps of the members.  report: rows of
- * (push_ctas, tx, ty, ms per step). */
+ * (push_ctas, tx, ty, parts, ms per step). */
 int csrst_ensemble_tune(csrst_ensemble *e, int steps, double *report, int max_rows, int *nrows);
 
 /* Beam moments (PartBunch::calcBeamParameters, PartBunch.cpp:584-657):

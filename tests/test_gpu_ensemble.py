@@ -54,7 +54,7 @@ def test_ensemble_matches_single_runs(gpu_lib, fp32):
 
 def test_launch_shapes_do_not_change_results(gpu_lib):
     runs = []
-    for shape in ((148, 32, 8), (1184, 128, 2)):
+    for shape in ((148, 32, 8, 1), (1184, 128, 2, 3)):
         sims = members(True, NAMES[:4])
         ens = Ensemble(sims)
         ens.set_shape(*shape)
@@ -71,12 +71,12 @@ def test_autotuner_steps_are_real_steps(gpu_lib):
     sims, ref = members(False, NAMES[:3]), members(False, NAMES[:3])
     ens = Ensemble(sims)
     rows = ens.tune(steps=1)
-    assert len(rows) == 12 and all(r[3] > 0 for r in rows)
+    assert len(rows) == 18 and all(r[4] > 0 for r in rows)
     ens.step(2)
     ens.sync()
-    # one step to reach the loop's steady state, then 12 shapes x (1 warm-up + 1 timed), then 2
+    # one step to reach the steady state of the loop, then 18 shapes x (1 warm-up + 1 timed), then 2
     for s in ref:
-        s.step(1 + 12 * 2 + 2)
+        s.step(1 + 18 * 2 + 2)
     for a, b in zip(sims, ref):
         assert_same(a, b)
     ens.close()
