@@ -268,7 +268,7 @@ def accuracy(cfg, spec, bunch, steps=50):
             "bar": "wake <= 1e-3 of the FP64 path's maximum; continuity <= 1e-10 (FP64 check)"}
 
 
-def run_ensemble(args, rank, members=64):
+def run_ensemble(args, rank, members=64, ms=None, fields=True):
     """The batched-ensemble workload: `members` independent bunches (uneven
     meshes 1024-8192 x 256-1024, 5e4-1e6 particles, CIC/TSC) stepped as one
     batch in FP32 mode after the autotuner picked the launch shapes, against
@@ -277,7 +277,9 @@ def run_ensemble(args, rank, members=64):
     import torch
     from csrst_b200 import Ensemble, Simulation
     from csrst_b200.workloads import ensemble_members, make_bunch
-    ms = ensemble_members(members, seed=2024 + rank)
+    if ms is None:
+        ms = ensemble_members(members, seed=2024 + rank)
+    members = len(ms)
     total = sum(spec.n for _, spec in ms)
     cells = sum(cfg.Nx * cfg.Ny for cfg, _ in ms)
     K, W = max(args.steps // 2, 5), max(args.warmup, 3)
@@ -289,7 +291,8 @@ def run_ensemble(args, rank, members=64):
         for cfg, spec in ms:
             sm = Simulation(cfg, fp32=fp32)
             sm.load(*make_bunch(spec))
-            sm.initial_fields(1e-12, 1e-6, 500)
+            if fields:
+                sm.initial_fields(1e-12, 1e-6, 500)
             sims.append(sm)
         return sims, time.perf_counter() - t
 
@@ -425,6 +428,16 @@ def run_b200(args, world, rank, local):
         out["accuracy_fp32_vs_fp64"] = accuracy(cfg, spec, bunch)
     if not args.no_ensemble:
         out["batched_ensemble"] = run_ensemble(args, rank)
+        # many small members: the regime where the batch's few launches per step matter
+        from csrst_b200.workloads import workload as wl
+        small = []
+        for k in range(256):
+            c, sp = wl(f"small-{k % 3}")
+            sp.seed = 500 + k
+            small.append((c, sp))
+        out["batched_ensemble_small"] = dict(run_ensemble(args, rank, ms=small, fields=False),
+                                             what="256 members of 512x104 meshes at 20 um with 4000 particles "
+                                                  "each, CIC/TSC/cubic, zero initial fields")
     if not args.no_e2e:
         out["e2e"] = run_e2e(args, cfg, spec, bunch, rank, world, head == "fp32")
     if rank == 0 and world == 1 and not args.no_cpu:

@@ -68,6 +68,8 @@ def lib():
         "csrst_ensemble_sync": ([P, I], C.c_int),
         "csrst_ensemble_set_shape": ([P, C.c_int, C.c_int, C.c_int, C.c_int], C.c_int),
         "csrst_ensemble_tune": ([P, C.c_int, D, C.c_int, I], C.c_int),
+        "csrst_gemm_bf16": ([P, C.c_longlong, C.c_longlong, P, C.c_longlong, C.c_longlong, C.c_int, C.c_int,
+                             C.c_int, C.c_int, P, P, P], C.c_int),
         "csrst_get_particles": ([P, D, D, D, D], C.c_int),
         "csrst_get_old_positions": ([P, D, D], C.c_int),
         "csrst_get_window": ([P, I, D, I], C.c_int),

@@ -1,0 +1,261 @@
+// BF16 tensor-core GEMM on the 5th-generation tensor cores (tcgen05) for the
+// surrogate network: C[M, N] = A[M, K] . B[N, K]^T with FP32 accumulation, both
+// operands K-major (rows contiguous along K), batched over blockIdx.z.
+//
+// One CTA of 128 threads computes a 128 x BN tile:
+//   - the A and B tiles of 64 K-columns are copied to shared memory with
+//     cp.async in two stages, in the tensor core's canonical K-major layout
+//     without swizzle: 8-row x 16-byte core matrices, the 8-row groups 128 B
+//     apart (SBO) and the 8-element K chunks a whole tile column apart (LBO);
+//   - one thread issues four tcgen05.mma (M = 128, N = BN, K = 16 each) per
+//     stage into an FP32 accumulator in tensor memory (TMEM) and commits them
+//     to the stage's mbarrier, which frees the stage for the next copy;
+//   - the epilogue reads the accumulator with tcgen05.ld (warp w owns TMEM
+//     lanes 32w .. 32w + 31, i.e. rows) and writes FP32 and/or BF16 through an
+//     affine index map, so that transposed and mode-major layouts come out
+//     directly.
+// Waits on mbarriers are bounded; a wait that gives up sets *err, skips the
+// epilogue and still frees the TMEM.
+#include <cuda_bf16.h>
+#include <stdint.h>
+
+#include "../../include/csrst.h"
+
+namespace csrst {
+namespace {
+
+constexpr int kBM = 128, kBK = 64, kThreads = 128;
+constexpr long long kSpin = 1ll << 24;  // mbarrier polls before a wait gives up
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, int count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+
+__device__ __forceinline__ bool mbar_try(uint64_t *bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// Bounded wait for completion `parity` of an mbarrier.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
+  for (long long k = 0; k < kSpin; ++k)
+    if (mbar_try(bar, parity)) return true;
+  return false;
+}
+
+__device__ __forceinline__ void cp_async16(void *dst, const void *src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+// Shared-memory matrix descriptor, K-major, no swizzle (version 1 for sm_100).
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+  uint64_t d = 0;
+  d |= (uint64_t)((addr >> 4) & 0x3FFF);
+  d |= (uint64_t)((lbo >> 4) & 0x3FFF) << 16;
+  d |= (uint64_t)((sbo >> 4) & 0x3FFF) << 32;
+  d |= (uint64_t)1 << 46;  // descriptor version
+  return d;                // base offset 0, legacy LBO mode, layout type 0 (no swizzle)
+}
+
+// Instruction descriptor of kind::f16: FP32 accumulator, BF16 A and B, both
+// K-major, M = 128, N = BN.
+template <int BN>
+__device__ __forceinline__ uint32_t instr_desc() {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(kBM >> 4) << 24);
+}
+
+__device__ __forceinline__ void mma_bf16(uint32_t tmem, uint64_t da, uint64_t db, uint32_t idesc, uint32_t acc) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
+      :
+      : "r"(tmem), "l"(da), "l"(db), "r"(idesc), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+}
+
+__device__ __forceinline__ void mma_commit(uint64_t *bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+               : "memory");
+}
+
+__device__ __forceinline__ float gelu(float x) { return 0.5f * x * (1.0f + erff(x * 0.70710678118654752f)); }
+
+// Copies rows [r0, r0 + R) x K-columns [k0, k0 + 64) of a K-major matrix into
+// the canonical layout: element (r, k) at ((k / 8) * (R / 8) + r / 8) * 128 +
+// (r % 8) * 16 + (k % 8) * 2 bytes.  Rows at or beyond `rows` are zero.
+template <int R>
+__device__ __forceinline__ void load_tile(uint8_t *dst, const __nv_bfloat16 *src, long long ld, int r0, int rows,
+                                          int k0) {
+  constexpr int chunks = R * (kBK / 8);  // 16-byte pieces
+#pragma unroll
+  for (int c = threadIdx.x; c < chunks; c += kThreads) {
+    const int r = c % 8 + 8 * ((c / 8) % (R / 8));  // row: 8 consecutive threads take one core matrix column
+    const int kc = c / R;                           // K chunk
+    uint8_t *d = dst + ((kc * (R / 8) + r / 8) * 128 + (r % 8) * 16);
+    if (r0 + r < rows) {
+      cp_async16(d, src + (long long)(r0 + r) * ld + k0 + kc * 8);
+    } else {
+      *reinterpret_cast<uint4 *>(d) = make_uint4(0, 0, 0, 0);
+    }
+  }
+}
+
+template <int BN>
+__global__ void __launch_bounds__(kThreads) k_gemm(const __nv_bfloat16 *A, long long lda, long long sA,
+                                                   const __nv_bfloat16 *B, long long ldb, long long sB, int M,
+                                                   int N, int K, csrst_gemm_epilogue ep, int *err) {
+  extern __shared__ __align__(1024) uint8_t smem[];
+  __shared__ uint64_t bar[2];
+  __shared__ uint32_t tmem_base;
+  __shared__ int s_fail;
+  constexpr int kA = kBM * kBK * 2, kB = BN * kBK * 2, kStage = kA + kB;
+  uint8_t *base = smem + ((1024 - (smem_u32(smem) & 1023)) & 1023);
+  const int z = blockIdx.z, m0 = blockIdx.y * kBM, n0 = blockIdx.x * BN;
+  A += (long long)z * sA;
+  B += (long long)z * sB;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+
+  if (warp == 0) {  // TMEM: BN FP32 columns x 128 lanes
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base)),
+                 "r"(BN));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  if (threadIdx.x == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    s_fail = 0;
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;");
+  const uint32_t tmem = tmem_base;
+  const int nk = K / kBK;
+
+  load_tile<kBM>(base, A, lda, m0, M, 0);
+  load_tile<BN>(base + kA, B, ldb, n0, N, 0);
+  cp_async_commit();
+  for (int kt = 0; kt < nk; ++kt) {
+    const int s = kt & 1;
+    if (kt + 1 < nk) {
+      const int s1 = (kt + 1) & 1;
+      if (kt >= 1) {  // the MMAs of tile kt - 1 still read stage s1
+        if (threadIdx.x == 0 && !mbar_wait(&bar[s1], ((kt - 1) >> 1) & 1)) s_fail = 1;
+        __syncthreads();
+        if (s_fail) break;
+      }
+      load_tile<kBM>(base + s1 * kStage, A, lda, m0, M, (kt + 1) * kBK);
+      load_tile<BN>(base + s1 * kStage + kA, B, ldb, n0, N, (kt + 1) * kBK);
+      cp_async_commit();
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // copies visible to the tensor core
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      asm volatile("tcgen05.fence::after_thread_sync;");
+      const uint32_t a0 = smem_u32(base + s * kStage), b0 = a0 + kA;
+#pragma unroll
+      for (int kk = 0; kk < kBK / 16; ++kk) {
+        // K = 16 is two 8-element chunks: advance by two chunk strides (LBO)
+        const uint64_t da = smem_desc(a0 + kk * 2 * (kBM / 8) * 128, (kBM / 8) * 128, 128);
+        const uint64_t db = smem_desc(b0 + kk * 2 * (BN / 8) * 128, (BN / 8) * 128, 128);
+        mma_bf16(tmem, da, db, instr_desc<BN>(), (kt > 0 || kk > 0) ? 1u : 0u);
+      }
+      mma_commit(&bar[s]);
+    }
+  }
+  // the last commit covers every MMA issued before it
+  if (threadIdx.x == 0 && !s_fail && nk > 0 && !mbar_wait(&bar[(nk - 1) & 1], ((nk - 1) >> 1) & 1)) s_fail = 1;
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;");
+  if (s_fail) {
+    if (threadIdx.x == 0) atomicExch(err, 1);
+  } else {
+    const int m = m0 + warp * 32 + lane;
+    for (int c0 = 0; c0 < BN; c0 += 16) {
+      uint32_t v[16];
+      const uint32_t ta = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0;
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+          "%15}, [%16];"
+          : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+            "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+          : "r"(ta));
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      if (m >= M) continue;
+#pragma unroll
+      for (int j = 0; j < 16; ++j) {
+        const int n = n0 + c0 + j;
+        if (n >= N) continue;
+        float x = ep.alpha * __uint_as_float(v[j]);
+        if (ep.bias) x += ep.bias[n];
+        const long long o = (long long)z * ep.sb + (long long)(m / ep.md) * ep.sm0 + (long long)(m % ep.md) * ep.sm1 +
+                            (long long)(n / ep.nd) * ep.sn0 + (long long)(n % ep.nd) * ep.sn1;
+        if (ep.res) x += ep.res[o];
+        if (ep.pre) ep.pre[o] = x;
+        if (ep.act == 1) x = gelu(x);
+        if (ep.out32) ep.out32[o] = ep.accumulate ? ep.out32[o] + x : x;
+        if (ep.out16) reinterpret_cast<__nv_bfloat16 *>(ep.out16)[o] = __float2bfloat16(x);
+        if (ep.out16t) {
+          const long long t = (long long)z * ep.tb + (long long)(m / ep.tmd) * ep.tm0 +
+                              (long long)(m % ep.tmd) * ep.tm1 + (long long)(n / ep.tnd) * ep.tn0 +
+                              (long long)(n % ep.tnd) * ep.tn1;
+          reinterpret_cast<__nv_bfloat16 *>(ep.out16t)[t] = __float2bfloat16(x);
+        }
+      }
+    }
+  }
+  cp_async_wait<0>();  // nothing still landing in shared memory (an early exit leaves copies in flight)
+  asm volatile("tcgen05.fence::before_thread_sync;");
+  __syncthreads();
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(BN));
+}
+
+template <int BN>
+int launch_gemm(const void *A, long long lda, long long sA, const void *B, long long ldb, long long sB, int M, int N,
+                int K, int batch, const csrst_gemm_epilogue &ep, int *err, cudaStream_t s) {
+  const int smem = 2 * (kBM * kBK * 2 + BN * kBK * 2) + 1024;
+  static bool attr = false;
+  if (!attr) {
+    if (cudaFuncSetAttribute(k_gemm<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess)
+      return CSRST_E_CUDA;
+    attr = true;
+  }
+  dim3 grid((N + BN - 1) / BN, (M + kBM - 1) / kBM, batch);
+  k_gemm<BN><<<grid, kThreads, smem, s>>>(static_cast<const __nv_bfloat16 *>(A), lda, sA,
+                                          static_cast<const __nv_bfloat16 *>(B), ldb, sB, M, N, K, ep, err);
+  return cudaGetLastError() == cudaSuccess ? CSRST_OK : CSRST_E_CUDA;
+}
+
+}  // namespace
+}  // namespace csrst
+
+extern "C" int csrst_gemm_bf16(const void *A, long long lda, long long stride_a, const void *B, long long ldb,
+                               long long stride_b, int M, int N, int K, int batch, const csrst_gemm_epilogue *ep,
+                               int *err, void *stream) {
+  using namespace csrst;
+  if (!A || !B || !ep || !err || M <= 0 || N <= 0 || K <= 0 || batch <= 0 || K % kBK != 0 || N % 16 != 0 ||
+      lda % 8 != 0 || ldb % 8 != 0 || lda < K || ldb < K || ep->md <= 0 || ep->nd <= 0 || (ep->out16t && (ep->tmd <= 0 || ep->tnd <= 0)) ||
+      ((uintptr_t)A & 15) || ((uintptr_t)B & 15) || (stride_a % 8) || (stride_b % 8))
+    return CSRST_E_ARG;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (N % 128 == 0) return launch_gemm<128>(A, lda, stride_a, B, ldb, stride_b, M, N, K, batch, *ep, err, s);
+  if (N % 64 == 0) return launch_gemm<64>(A, lda, stride_a, B, ldb, stride_b, M, N, K, batch, *ep, err, s);
+  return launch_gemm<32>(A, lda, stride_a, B, ldb, stride_b, M, N, K, batch, *ep, err, s);
+}

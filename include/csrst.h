@@ -158,6 +158,32 @@ int csrst_ensemble_set_shape(csrst_ensemble *e, int push_ctas, int tx, int ty, i
  * (push_ctas, tx, ty, parts, ms per step). */
 int csrst_ensemble_tune(csrst_ensemble *e, int steps, double *report, int max_rows, int *nrows);
 
+/* BF16 tensor-core GEMM of the wake surrogate (no reference counterpart):
+ * C[M, N] = alpha * A[M, K] . B[N, K]^T with FP32 accumulation, A and B
+ * K-major BF16 device matrices (leading dimensions lda, ldb in elements,
+ * multiples of 8; K a multiple of 64; N a multiple of 16), `batch` of them
+ * stride_a / stride_b apart.  The epilogue adds bias[n] and the residual,
+ * keeps the pre-activation, applies GELU and writes FP32 and/or BF16 through
+ * the index map below.  *err (device int) is set if a tensor-core wait gave up. */
+typedef struct {
+  float alpha;
+  int act;                            /* 0 none, 1 GELU (erf form), after bias and residual */
+  int accumulate;                     /* out32 += value */
+  int md, nd;                         /* index-map divisors */
+  long long sb, sm0, sm1, sn0, sn1;   /* index = z*sb + (m/md)*sm0 + (m%md)*sm1 + (n/nd)*sn0 + (n%nd)*sn1 */
+  const float *bias;                  /* per column n, or NULL */
+  const float *res;                   /* residual under the index map, or NULL */
+  float *pre;                         /* pre-activation (FP32) under the index map, or NULL */
+  float *out32;                       /* FP32 output, or NULL */
+  void *out16;                        /* BF16 output, or NULL */
+  void *out16t;                       /* second BF16 output under its own map, or NULL */
+  int tmd, tnd;
+  long long tb, tm0, tm1, tn0, tn1;
+} csrst_gemm_epilogue;
+int csrst_gemm_bf16(const void *A, long long lda, long long stride_a, const void *B, long long ldb,
+                    long long stride_b, int M, int N, int K, int batch, const csrst_gemm_epilogue *ep, int *err,
+                    void *stream);
+
 /* Beam moments (PartBunch::calcBeamParameters, PartBunch.cpp:584-657):
  * out18 = rmean2, pmean2, rrms2, prms2, eps_norm2, rmin2, rmax2, Ekin[MeV], dE, 0, 0. */
 int csrst_diag_moments(csrst_handle *h, double *out18);

@@ -1,0 +1,56 @@
+"""The surrogate's BF16 tensor-core GEMM (tcgen05, FP32 accumulation) against
+an FP64 product of the same BF16 values on the CPU."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def bf16(rng, shape):
+    import torch
+    return torch.from_numpy(rng.standard_normal(shape).astype(np.float32)).to(torch.bfloat16)
+
+
+def ref(a, b):
+    return a.float().double().numpy() @ b.float().double().numpy().T
+
+
+@pytest.mark.parametrize("M,N,K", [(128, 128, 64), (256, 128, 192), (200, 64, 64), (130, 48, 128), (384, 256, 256)])
+def test_gemm_matches_cpu(gpu_lib, M, N, K):
+    import torch
+    from csrst_b200.tensor import check_errors, gemm
+    rng = np.random.default_rng(M * 7 + N + K)
+    a, b = bf16(rng, (M, K)), bf16(rng, (N, K))
+    out = torch.zeros(M, N, dtype=torch.float32, device="cuda")
+    gemm(a.cuda(), b.cuda(), M, N, K, out32=out)
+    torch.cuda.synchronize()
+    check_errors()
+    r = ref(a, b)
+    assert np.abs(out.cpu().numpy() - r).max() <= 1e-4 * np.abs(r).max()
+
+
+def test_gemm_epilogue_and_batches(gpu_lib):
+    """bias, residual, GELU, pre-activation, BF16 copy in a transposed layout,
+    accumulation, and a batch of three products."""
+    import torch
+    from csrst_b200.tensor import check_errors, gemm
+    rng = np.random.default_rng(5)
+    M, N, K, Z = 256, 64, 128, 3
+    a, b = bf16(rng, (Z, M, K)), bf16(rng, (Z, N, K))
+    bias = torch.from_numpy(rng.standard_normal(N).astype(np.float32))
+    res = torch.from_numpy(rng.standard_normal((Z, M, N)).astype(np.float32))
+    pre = torch.zeros(Z, M, N, device="cuda")
+    o32 = torch.full((Z, M, N), 2.0, device="cuda")
+    o16t = torch.zeros(Z, N, M, dtype=torch.bfloat16, device="cuda")
+    gemm(a.cuda(), b.cuda(), M, N, K, batch=Z, stride_a=M * K, stride_b=N * K, alpha=0.5, bias=bias.cuda(),
+         res=res.cuda(), pre=pre, out32=o32, act=1, accumulate=True, sb=M * N, out16t=o16t,
+         tmap=dict(md=1, nd=1, sm0=1, sm1=0, sn0=M, sn1=0), tb=N * M)
+    torch.cuda.synchronize()
+    check_errors()
+    for z in range(Z):
+        h = 0.5 * ref(a[z], b[z]) + bias.double().numpy() + res[z].double().numpy()
+        g = 0.5 * h * (1 + np.vectorize(__import__("math").erf)(h / np.sqrt(2)))
+        assert np.abs(pre[z].cpu().numpy() - h).max() <= 1e-4 * np.abs(h).max()
+        assert np.abs(o32[z].cpu().numpy() - (2.0 + g)).max() <= 1e-4 * np.abs(g).max()
+        t = o16t[z].float().cpu().numpy()
+        assert np.abs(t - g.T).max() <= 1e-2 * np.abs(g).max()
