@@ -70,6 +70,15 @@ def lib():
         "csrst_ensemble_tune": ([P, C.c_int, D, C.c_int, I], C.c_int),
         "csrst_gemm_bf16": ([P, C.c_longlong, C.c_longlong, P, C.c_longlong, C.c_longlong, C.c_int, C.c_int,
                              C.c_int, C.c_int, P, P, P], C.c_int),
+        "csrst_nn_transpose_bf16": ([P, P, C.c_int, C.c_int, C.c_int, C.c_int, P], C.c_int),
+        "csrst_nn_gelu_bwd": ([P, P, P, P, C.c_longlong, P], C.c_int),
+        "csrst_nn_cast_bf16": ([P, P, C.c_longlong, P], C.c_int),
+        "csrst_nn_colsum": ([P, C.c_int, C.c_int, P, P, C.c_int, P], C.c_int),
+        "csrst_nn_mse": ([P, P, C.c_longlong, P, C.c_int, C.c_longlong, C.c_longlong, P, P, P], C.c_int),
+        "csrst_nn_adam_tick": ([P, P, C.c_float, C.c_float, C.c_int, C.c_float, C.c_float, P], C.c_int),
+        "csrst_nn_adam": ([P, P, P, P, C.c_longlong, P, C.c_float, C.c_float, C.c_float, P], C.c_int),
+        "csrst_nn_spectral_pack": ([P, P, C.c_int, C.c_int, P, P, P], C.c_int),
+        "csrst_nn_spectral_unpack": ([P, C.c_int, C.c_int, P, P, P], C.c_int),
         "csrst_get_particles": ([P, D, D, D, D], C.c_int),
         "csrst_get_old_positions": ([P, D, D], C.c_int),
         "csrst_get_window": ([P, I, D, I], C.c_int),

@@ -13,8 +13,8 @@ from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
 SRC = ["api.cu", "geometry.cu", "particles.cu", "particles32.cu", "fields.cu", "diag.cu", "poisson.cu",
-       "gemm.cu", "noalloc.cu"]
-FMA_ON = {"particles32.cu", "gemm.cu"}
+       "gemm.cu", "nn.cu", "noalloc.cu"]
+FMA_ON = {"particles32.cu", "gemm.cu", "nn.cu"}
 OUT = HERE / "libcsrst_gpu.so"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "--fmad=false", "-lineinfo", "-Xcompiler", "-fPIC",

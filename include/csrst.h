@@ -184,6 +184,28 @@ int csrst_gemm_bf16(const void *A, long long lda, long long stride_a, const void
                     long long stride_b, int M, int N, int K, int batch, const csrst_gemm_epilogue *ep, int *err,
                     void *stream);
 
+/* Element-wise and reduction kernels of the surrogate's training and inference
+ * (device pointers; BF16 arrays as void *).  No reference counterpart. */
+/* [batch][rows][cols] -> [batch][cols][ldd] (ldd >= rows; columns rows .. ldd - 1 untouched) */
+int csrst_nn_transpose_bf16(const void *src, void *dst, int batch, int rows, int cols, int ldd, void *stream);
+/* dx = dy * GELU'(pre) (erf form); dx32 and/or dx16 */
+int csrst_nn_gelu_bwd(const float *dy, const float *pre, float *dx32, void *dx16, long long n, void *stream);
+int csrst_nn_cast_bf16(const float *x, void *y, long long n, void *stream);
+/* out[c] (+)= sum over rows of x[r][c] in a fixed order; part: ceil(rows/256)*cols floats of scratch */
+int csrst_nn_colsum(const float *x, int rows, int cols, float *part, float *out, int accumulate, void *stream);
+/* loss = mean (pred - target)^2; grad[(i/gd)*g0 + (i%gd)*g1] = 2 (pred_i - target_i) / n (grad may be NULL);
+ * part: 256 doubles of scratch; loss: one device double */
+int csrst_nn_mse(const float *pred, const float *target, long long n, float *grad, int gd, long long g0, long long g1,
+                 double *part, double *loss, void *stream);
+/* Adam with bias correction; the step counter *t and coef = {lr_t, 1 - b1^t, 1 - b2^t} live on the device:
+ * adam_tick advances t and writes coef (cosine schedule from lr0 to lr_min over `total` steps) */
+int csrst_nn_adam_tick(int *t, float *coef, float lr0, float lr_min, int total, float b1, float b2, void *stream);
+int csrst_nn_adam(float *w, const float *g, float *m, float *v, long long n, const float *coef, float b1, float b2,
+                  float eps, void *stream);
+/* complex spectral weights Wr + i Wi [modes][ch][ch] -> real blocks Mk [modes][2ch][2ch] and their transposes */
+int csrst_nn_spectral_pack(const float *wr, const float *wi, int modes, int ch, void *mk, void *mkt, void *stream);
+int csrst_nn_spectral_unpack(const float *dmk, int modes, int ch, float *dwr, float *dwi, void *stream);
+
 /* Beam moments (PartBunch::calcBeamParameters, PartBunch.cpp:584-657):
  * out18 = rmean2, pmean2, rrms2, prms2, eps_norm2, rmin2, rmax2, Ekin[MeV], dE, 0, 0. */
 int csrst_diag_moments(csrst_handle *h, double *out18);

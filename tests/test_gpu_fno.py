@@ -1,0 +1,122 @@
+"""The surrogate network on the GPU (tensor-core GEMMs + nn.cu kernels)
+against its CPU oracle: forward output, loss and every parameter gradient.
+
+Tolerances: against the oracle's BF16 restatement (same rounding points, FP64
+arithmetic) 2e-3 relative L2 for the output and 5e-3 for each gradient, the
+spectral weights of a layer taken together as one complex tensor (Wr, Wi):
+what is left is FP32 accumulation order and the BF16 rounding flips it causes.
+The oracle itself, with FP32 instead of FP64 arithmetic between the same
+rounding points, moves by up to 2.2e-3 (P) and 1.4e-3 (Wr0 + Wi0) on this
+case; the imaginary parts alone carry 100x less gradient and move by 4.5e-3
+(checked at 2e-2).  Against the exact FP64 FFT restatement: 3e-2 (BF16
+activations and weights)."""
+import numpy as np
+import pytest
+
+from oracle.fno_oracle import FNO as OracleFNO, NBINS, NFEAT, init_params
+
+pytestmark = pytest.mark.gpu
+
+
+def problem(B=64, seed=1, nout=32):
+    g = np.random.default_rng(seed)
+    X = np.zeros((B, NBINS, NFEAT), dtype=np.float32)
+    s = np.linspace(-1, 1, NBINS)
+    X[..., 0] = np.exp(-0.5 * (s[None, :] / g.uniform(0.1, 0.4, (B, 1))) ** 2)
+    X[..., 1] = s[None, :]
+    X[..., 2:6] = g.uniform(-1, 1, (B, 1, 4))
+    T = g.standard_normal((B, NBINS, nout)).astype(np.float32) * 0.5
+    p = init_params(seed)
+    for k in p:
+        if p[k].ndim == 1 and k != "pad":
+            p[k] = 0.05 * g.standard_normal(p[k].shape)
+    return X, T, p
+
+
+def rel(a, b):
+    return np.linalg.norm(np.asarray(a) - np.asarray(b)) / max(np.linalg.norm(np.asarray(b)), 1e-30)
+
+
+@pytest.fixture(scope="module")
+def case(gpu_lib):
+    import torch
+    from csrst_b200.surrogate import FNO
+    X, T, p = problem()
+    net = FNO(params=p)
+    Xd = torch.from_numpy(X).cuda().to(torch.bfloat16)
+    Td = torch.from_numpy(T).cuda()
+    loss = float(net.loss_and_grad(Xd, Td).item())
+    torch.cuda.synchronize()
+    net.check()
+    out = net._bufs[(64, True)].out.view(64, NBINS, 32).cpu().numpy()
+    return dict(X=X, T=T, p=p, net=net, Xd=Xd, loss=loss, out=out, grads=net.grads())
+
+
+def test_forward_and_gradients_match_bf16_oracle(case):
+    ref = OracleFNO(case["p"], bf16=True)
+    out, _ = ref.forward(case["X"])
+    assert rel(case["out"], out) <= 2e-3
+    loss, g = ref.backward(case["X"], case["T"])
+    assert abs(case["loss"] - loss) <= 1e-4 * loss
+    gg = case["grads"]
+    for k, v in g.items():
+        if k.startswith("Wr"):
+            l = k[2:]
+            a = np.concatenate([gg["Wr" + l].ravel(), gg["Wi" + l].ravel()])
+            b = np.concatenate([v.ravel(), g["Wi" + l].ravel()])
+            assert rel(a, b) <= 5e-3, (k, rel(a, b))
+        elif k.startswith("Wi"):
+            assert rel(gg[k], v) <= 2e-2, (k, rel(gg[k], v))
+        else:
+            assert rel(gg[k], v) <= 5e-3, (k, rel(gg[k], v))
+
+
+def test_gradients_close_to_fp64_fft_oracle(case):
+    loss, g = OracleFNO(case["p"]).backward(case["X"], case["T"])
+    assert abs(case["loss"] - loss) <= 1e-2 * loss
+    gg = case["grads"]
+    for k, v in g.items():
+        if k.startswith("Wr"):
+            l = k[2:]
+            a = np.concatenate([gg["Wr" + l].ravel(), gg["Wi" + l].ravel()])
+            b = np.concatenate([v.ravel(), g["Wi" + l].ravel()])
+            assert rel(a, b) <= 3e-2, (k, rel(a, b))
+        elif np.any(v) and not k.startswith("Wi"):
+            assert rel(gg[k], v) <= 3e-2, (k, rel(gg[k], v))
+
+
+def test_inference_path_matches_training_forward(case):
+    pred = case["net"].predict(case["Xd"], chunk=32).cpu().numpy()
+    assert np.array_equal(pred, case["out"])
+
+
+def test_training_reduces_loss_and_repeats_bitwise(gpu_lib):
+    """Adam on a small regression (the wake of a smoothing kernel): the loss
+    falls by 10x in 300 steps, and a second run from the same start ends in
+    bitwise the same weights."""
+    import torch
+    from csrst_b200.surrogate import FNO
+    X, _, p = problem(B=128, seed=4)
+    # target: per-station smoothing of the profile, scaled by one of the scalar features
+    k = np.exp(-0.5 * (np.arange(-20, 21) / 6.0) ** 2)
+    T = np.stack([np.convolve(x, k * (1 + 0.02 * st), "same") for x in X[..., 0] for st in range(32)])
+    T = (T.reshape(128, 32, NBINS).transpose(0, 2, 1) * (1 + 0.3 * X[:, :1, 2:3])).astype(np.float32)
+    T /= T.std()
+    Xd = torch.from_numpy(X).cuda().to(torch.bfloat16)
+    Td = torch.from_numpy(T).cuda()
+    finals, losses = [], []
+    for _ in range(2):
+        net = FNO(params=p)
+        first = None
+        for it in range(300):
+            loss = net.loss_and_grad(Xd, Td)
+            if first is None:
+                first = float(loss.item())
+            net.adam(lr0=2e-3, lr_min=1e-4, total=300)
+        last = float(net.loss_and_grad(Xd, Td).item())
+        torch.cuda.synchronize()
+        net.check()
+        finals.append(net.w.cpu().numpy())
+        losses.append((first, last))
+    assert losses[0][1] < 0.1 * losses[0][0], losses
+    assert np.array_equal(finals[0], finals[1])
