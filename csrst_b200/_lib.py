@@ -93,6 +93,7 @@ def lib():
         "csrst_step": ([P, C.c_int], C.c_int),
         "csrst_diag_moments": ([P, D], C.c_int),
         "csrst_diag_wake": ([P, D, C.c_int], C.c_int),
+        "csrst_diag_wake_async": ([P, P, C.c_int, P], C.c_int),
         "csrst_gather": ([C.c_int, C.c_int, D, C.c_int, C.c_int, D, D, D, D, C.c_size_t, D], C.c_int),
         "csrst_deposit": ([C.c_int, C.c_int, D, D, D, D, D, C.c_size_t, D, D, C.c_double, C.c_int,
                            C.c_int, C.c_int, C.c_int, C.c_double, D], C.c_int),

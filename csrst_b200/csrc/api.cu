@@ -1045,6 +1045,24 @@ int csrst_diag_wake(csrst_handle *h, double *out, int n) {
   return check_err(h);
 }
 
+int csrst_diag_wake_async(csrst_handle *h, double *out_dev, int n, double *meta_dev) {
+  int rc = need_bunch(h);
+  if (rc) return rc;
+  if (!out_dev || !meta_dev || n != h->L0 - 4) return fail(h, CSRST_E_ARG, "wake buffer must hold L0 - 4 values");
+  const double *x, *y, *px, *py;
+  int pend = 0;
+  bunch64(h, &x, &y, &px, &py, &pend);
+  launch_moments(x, y, px, py, h->n, h->half, pend, h->dscratch, h->dmean, h->dout, h->s);
+  if (h->fp32)
+    launch_wake(h->ws, wplane32(h, 0).p, wplane32(h, 1).p, h->wpitch, h->L0, h->b.hr0, h->b.hr1, h->dmean, out_dev,
+                h->s);
+  else
+    launch_wake(h->ws, wplane(h, 0).p, wplane(h, 1).p, h->wpitch, h->L0, h->b.hr0, h->b.hr1, h->dmean, out_dev, h->s);
+  CK(cudaMemcpyAsync(meta_dev, &h->ws->mo0, 2 * sizeof(double), cudaMemcpyDeviceToDevice, h->s));
+  CK(cudaMemcpyAsync(meta_dev + 2, h->dmean, 2 * sizeof(double), cudaMemcpyDeviceToDevice, h->s));
+  return CSRST_OK;
+}
+
 // ---- batched ensemble ----
 
 }  // extern "C"

@@ -201,7 +201,7 @@ class FNO:
         return self._bufs[key]
 
     # ---- forward ----
-    def _forward(self, bf, B, X16):
+    def _forward(self, bf, B, X16, out=None):
         w, m, L, R = self.width, self.modes, self.layers, B * NBINS
         tr = bf.train
         w16 = lambda n: self.view(n, self.w16)
@@ -229,7 +229,7 @@ class FNO:
         Vl = bf.V16[L if tr else L & 1]
         gemm(Vl, w16("Q1"), R, w, w, bias=self.view("q1"), act=1, pre=bf.A1pre if tr else None, out16=bf.A1_16,
              out16t=bf.A1t16 if tr else None, tmap=dict(md=1, nd=1, sm0=1, sm1=0, sn0=R, sn1=0))
-        gemm(bf.A1_16, w16("Q2"), R, self.nout, w, bias=self.view("q2"), out32=bf.out)
+        gemm(bf.A1_16, w16("Q2"), R, self.nout, w, bias=self.view("q2"), out32=bf.out if out is None else out)
 
     def predict(self, X, chunk=4096):
         """X: [N][256][64] BF16 (device) -> wake [N][256][nout] FP32 (device), in chunks of members."""
@@ -238,8 +238,7 @@ class FNO:
         for a in range(0, N, chunk):
             B = min(chunk, N - a)
             bf = self._buf(B, False)
-            self._forward(bf, B, X[a:a + B].reshape(B * NBINS, NFEAT))
-            out[a:a + B].copy_(bf.out.view(B, NBINS, self.nout))
+            self._forward(bf, B, X[a:a + B].reshape(B * NBINS, NFEAT), out[a:a + B])
         return out
 
     # ---- backward ----

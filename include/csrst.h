@@ -213,6 +213,10 @@ int csrst_diag_moments(csrst_handle *h, double *out18);
  * (IntegrateElongCommand::execute, IntegrateElong.cpp:38-89); NaN where the
  * sample lies outside the window.  n must be L0 - 4. */
 int csrst_diag_wake(csrst_handle *h, double *out, int n);
+/* The same into device memory, enqueued on the handle's stream without
+ * waiting (for many members read at once): out_dev receives the L0 - 4
+ * samples, meta_dev the window origin (x, y) and the bunch centroid (x, y). */
+int csrst_diag_wake_async(csrst_handle *h, double *out_dev, int n, double *meta_dev);
 
 /* ScatterGatherImpl<IntOp>::gather (ScatterGatherImpl.hh:27-47) on a dense
  * host patch (nx * ny, x fastest) with origin o and spacing hh; comp 0/1 =
