@@ -74,7 +74,7 @@ def lib():
         "csrst_nn_gelu_bwd": ([P, P, P, P, C.c_longlong, P], C.c_int),
         "csrst_nn_cast_bf16": ([P, P, C.c_longlong, P], C.c_int),
         "csrst_nn_colsum": ([P, C.c_int, C.c_int, P, P, C.c_int, P], C.c_int),
-        "csrst_nn_mse": ([P, P, C.c_longlong, P, C.c_int, C.c_longlong, C.c_longlong, P, P, P], C.c_int),
+        "csrst_nn_mse": ([P, P, P, C.c_longlong, P, C.c_int, C.c_longlong, C.c_longlong, P, P, P], C.c_int),
         "csrst_nn_adam_tick": ([P, P, C.c_float, C.c_float, C.c_int, C.c_float, C.c_float, P], C.c_int),
         "csrst_nn_adam": ([P, P, P, P, C.c_longlong, P, C.c_float, C.c_float, C.c_float, P], C.c_int),
         "csrst_nn_spectral_pack": ([P, P, C.c_int, C.c_int, P, P, P], C.c_int),

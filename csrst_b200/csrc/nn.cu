@@ -63,17 +63,18 @@ __global__ void k_colsum_final(const float *part, int slabs, int cols, float *ou
   out[c] = accumulate ? out[c] + s : s;
 }
 
-// Mean squared error: grad = 2 (pred - target) / n (written through gmap:
+// Mean squared error, optionally weighted per output (a 0/1 weight leaves
+// an output out): grad = 2 w^2 (pred - target) / n (written through gmap:
 // index (i / gd) * g0 + (i % gd) * g1, so that the gradient lands in the layout
 // of the last product), partial sums per block, then the total in order.
-__global__ void k_mse(const float *pred, const float *target, long long n, float *grad, int gd, long long g0,
-                      long long g1, double *part) {
+__global__ void k_mse(const float *pred, const float *target, const float *weight, long long n, float *grad, int gd,
+                      long long g0, long long g1, double *part) {
   __shared__ double sh[256];
   double s = 0.0;
   for (long long i = gtid(); i < n; i += (long long)gridDim.x * blockDim.x) {
-    const float e = pred[i] - target[i];
+    const float e = weight ? (pred[i] - target[i]) * weight[i] : pred[i] - target[i];
     s += (double)e * e;
-    if (grad) grad[(i / gd) * g0 + (i % gd) * g1] = 2.0f * e / (float)n;
+    if (grad) grad[(i / gd) * g0 + (i % gd) * g1] = 2.0f * (weight ? weight[i] : 1.0f) * e / (float)n;
   }
   sh[threadIdx.x] = s;
   __syncthreads();
@@ -184,10 +185,10 @@ int csrst_nn_colsum(const float *x, int rows, int cols, float *part, float *out,
   return cudaGetLastError() == cudaSuccess ? CSRST_OK : CSRST_E_CUDA;
 }
 
-int csrst_nn_mse(const float *pred, const float *target, long long n, float *grad, int gd, long long g0, long long g1,
-                 double *part, double *loss, void *stream) {
+int csrst_nn_mse(const float *pred, const float *target, const float *weight, long long n, float *grad, int gd,
+                 long long g0, long long g1, double *part, double *loss, void *stream) {
   if (!pred || !target || !part || !loss || n <= 0 || gd <= 0) return CSRST_E_ARG;
-  k_mse<<<256, 256, 0, (cudaStream_t)stream>>>(pred, target, n, grad, gd, g0, g1, part);
+  k_mse<<<256, 256, 0, (cudaStream_t)stream>>>(pred, target, weight, n, grad, gd, g0, g1, part);
   k_sum_final<<<1, 32, 0, (cudaStream_t)stream>>>(part, 256, n, loss);
   return cudaGetLastError() == cudaSuccess ? CSRST_OK : CSRST_E_CUDA;
 }

@@ -255,14 +255,14 @@ class FNO:
         _ck(lib().csrst_nn_colsum(_p(x), rows, cols, _p(bf.cpart), _p(out), 1 if accumulate else 0, _stream()),
             "colsum")
 
-    def _backward(self, bf, B, X16, T):
+    def _backward(self, bf, B, X16, T, Wt=None):
         w, m, L, R, nout = self.width, self.modes, self.layers, B * NBINS, self.nout
         s = _stream()
         lb = lib()
         w16 = lambda n: self.view(n, self.w16)
         # loss and dLoss/dout into the first nout columns of a 64-column buffer
-        _ck(lb.csrst_nn_mse(_p(bf.out), _p(T), R * nout, _p(bf.dOut), nout, 64, 1, _p(bf.lpart), _p(bf.loss), s),
-            "mse")
+        _ck(lb.csrst_nn_mse(_p(bf.out), _p(T), _p(Wt), R * nout, _p(bf.dOut), nout, 64, 1, _p(bf.lpart),
+                            _p(bf.loss), s), "mse")
         _ck(lb.csrst_nn_cast_bf16(_p(bf.dOut), _p(bf.dOut16), R * 64, s), "cast")
         _ck(lb.csrst_nn_transpose_bf16(_p(bf.dOut16), _p(bf.dOutT16), 1, R, 64, R, s), "transpose")
         self._wgrad(bf, bf.dOutT16, bf.A1t16, nout, w, R, "Q2")
@@ -307,16 +307,19 @@ class FNO:
         self._wgrad(bf, bf.dHt16, bf.Xt16, w, NFEAT, R, "P")
         self._colsum(bf, dV, R, w, self.view("p", self.g))
 
-    def loss_and_grad(self, X, T):
+    def loss_and_grad(self, X, T, weight=None):
         """X: [B][256][64] BF16, T: [B][256][nout] FP32 (device, B a multiple
-        of 64).  Fills the gradient buffer; returns the loss as a device scalar."""
+        of 64), weight: optional FP32 per-output weights of the squared error
+        (0 leaves an output out).  Fills the gradient buffer; returns the loss
+        as a device scalar."""
         B = X.shape[0]
         if B % 64:
             raise ValueError("training batches must be a multiple of 64 members")
         bf = self._buf(B, True)
         X16 = X.reshape(B * NBINS, NFEAT)
         self._forward(bf, B, X16)
-        self._backward(bf, B, X16, T.reshape(B * NBINS, self.nout))
+        self._backward(bf, B, X16, T.reshape(B * NBINS, self.nout),
+                       None if weight is None else weight.reshape(B * NBINS, self.nout))
         return bf.loss
 
     def adam(self, lr0=1e-3, lr_min=1e-5, total=10000, b1=0.9, b2=0.999, eps=1e-8):

@@ -12,6 +12,7 @@ size.  The held-out cases (the last 10 % of the seeded draw) are judged
 against their PIC wakes on the bins the PIC window sampled:
   error = || E_surrogate - E_PIC ||_2 / || E_PIC ||_2 over 256 bins x 32 stations.
 """
+import dataclasses
 import json
 import math
 import time
@@ -99,9 +100,11 @@ def train(d, steps=20000, batch=64, lr0=1e-3, lr_min=1e-5, seed=0, width=128, mo
     dev = net.device
     Xd = torch.from_numpy(pad_features(X6)).to(dev).to(torch.bfloat16)
     Td = torch.from_numpy(Tn).to(dev)
+    Md = torch.from_numpy(M.astype(np.float32)).to(dev)    # bins outside the PIC window carry no target
     N = len(tr)
     Xs = torch.empty(batch, NBINS, NFEAT, dtype=torch.bfloat16, device=dev)
     Ts = torch.empty(batch, NBINS, Tn.shape[2], dtype=torch.float32, device=dev)
+    Ms = torch.empty(batch, NBINS, Tn.shape[2], dtype=torch.float32, device=dev)
     gen = torch.Generator(device=dev)
     gen.manual_seed(seed)
     per_epoch = N // batch
@@ -114,9 +117,10 @@ def train(d, steps=20000, batch=64, lr0=1e-3, lr_min=1e-5, seed=0, width=128, mo
         state["pos"] += 1
         torch.index_select(Xd, 0, idx, out=Xs)
         torch.index_select(Td, 0, idx, out=Ts)
+        torch.index_select(Md, 0, idx, out=Ms)
 
     def one():
-        loss = net.loss_and_grad(Xs, Ts)
+        loss = net.loss_and_grad(Xs, Ts, Ms)
         net.adam(lr0=lr0, lr_min=lr_min, total=steps)
         return loss
 
@@ -151,13 +155,40 @@ def train(d, steps=20000, batch=64, lr0=1e-3, lr_min=1e-5, seed=0, width=128, mo
                                         "train_cases": int(N), "params": int(net.n)}
 
 
-def evaluate(model, d, log=print):
+SHIFTS = (0.0, 0.25, 0.5, 0.75)
+
+
+def pic_reference(cases, n_particles=50_000, batch=256, log=print):
+    """The alignment-averaged PIC wake of each case: the case run with its
+    bunch shifted by 0, 1/4, 1/2 and 3/4 of a cell, averaged.  A single run
+    depends on where sub-cell features (horns, sharp edges) fall on the mesh:
+    half a cell moves a double-horn wake by 6 - 9 %, a flat top's by 1 - 4 %,
+    a Gaussian's by about 1 %; the average over the cell is what a
+    resolution-limited PIC determines.  Returns (mean wake, mask of bins every
+    run sampled, per-shift wakes)."""
+    from . import wakeset
+    runs, masks = [], []
+    for sh in SHIFTS:
+        w, m, _ = wakeset.run_cases(cases, n_particles=n_particles, batch=batch, log=log, shift=sh)
+        runs.append(w)
+        masks.append(m)
+    runs = np.array(runs)
+    return runs.mean(0), np.logical_and.reduce(masks), runs
+
+
+def evaluate(model, d, log=print, ref=None):
     """Held-out errors against PIC, and the same for two baselines without
     the network: the amplitude law times the mean normalised training wake,
     and the nearest training case (in the standardised inputs) rescaled by the
-    amplitude law."""
+    amplitude law.  ref = (wakes, masks) of the held-out cases from
+    pic_reference() makes the alignment-averaged PIC wake the judge and adds
+    the single runs' own scatter about it."""
     tr, te = split(len(d["X"]))
-    X6, W, M = d["X"], d["W"], d["M"]
+    X6, W, M = d["X"], d["W"].copy(), d["M"].copy()
+    single = None
+    if ref is not None:
+        single = rel_errors(W[te], ref[0], ref[1])
+        W[te], M[te] = ref[0], ref[1]
     P = model.predict(X6[te])
     err = rel_errors(P, W[te], M[te])
     s_tr = model.scale(X6[tr])
@@ -175,9 +206,14 @@ def evaluate(model, d, log=print):
                 "max": float(e.max()), "frac_le_2pct": float(np.mean(e <= 0.02))}
 
     kinds = np.array([c.kind for c in d["cases"]])[te]
-    out = {"held_out": int(len(te)), "surrogate": summary(err),
-           "by_family": {name: summary(err[kinds == k]) for k, name in enumerate(("gaussian", "flat_top", "double_horn"))},
+    fam = ("gaussian", "flat_top", "double_horn")
+    out = {"held_out": int(len(te)), "judge": "alignment-averaged PIC" if ref is not None else "single PIC run",
+           "surrogate": summary(err),
+           "by_family": {name: summary(err[kinds == k]) for k, name in enumerate(fam)},
            "baseline_mean_shape": summary(err_mean), "baseline_nearest_case": summary(err_nn)}
+    if single is not None:
+        out["single_pic_run_vs_average"] = summary(single)
+        out["single_pic_run_by_family"] = {name: summary(single[kinds == k]) for k, name in enumerate(fam)}
     if log:
         log(json.dumps(out))
     return out, err
@@ -206,6 +242,136 @@ def _flops_per_profile(net):
     w, m, L, no = net.width, net.modes, net.layers, net.nout
     per_layer = 2 * NBINS * w * w + 2 * w * 2 * m * NBINS * 2 + 2 * m * (2 * w) * (2 * w)
     return 2 * NBINS * NFEAT * w + L * per_layer + 2 * NBINS * w * w + 2 * NBINS * w * no
+
+
+# ---- production: surrogate prescreen of profile variants, PIC reruns, the large run ----
+
+C5_HALF_LENGTH = 50e-6      # flat top of 100 um
+C5_GAMMA, C5_R = 2000.0, 2.0
+
+
+def c5_variants(n, seed=5):
+    """n double-horn variants of the production bunch (flat top of 100 um;
+    horns at +-horn_pos x 50 um of rms width horn_w x 50 um), drawn over the
+    training ranges of the double-horn family, at gamma = 2000, R = 2 m and a
+    pipe of 80 sigma_s.  Variant 0 is the nominal profile: horns of 5 um at
+    +-40 um, sharp edges, no tilt."""
+    from . import wakeset
+    g = np.random.Generator(np.random.Philox(seed))
+    out = []
+    for k in range(n):
+        if k == 0:
+            e, t, hp, hw, a, b = 0.05, 0.0, 0.8, 0.1, 1.5, 1.5
+        else:
+            e, t = g.uniform(0.05, 0.3), g.uniform(-0.3, 0.3)
+            hp, hw = g.uniform(0.7, 0.95), g.uniform(0.04, 0.12)
+            a, b = g.uniform(0.5, 2.5), g.uniform(0.5, 2.5)
+        out.append(wakeset.WakeCase(kind=2, edge=float(e), tilt=float(t), horn_pos=float(hp), horn_w=float(hw),
+                                    horn_a=float(a), horn_b=float(b), sigma_s=1.0, gamma=C5_GAMMA, R=C5_R,
+                                    width_sigma=80.0, seed=int(g.integers(1, 2 ** 31))))
+    rms = wakeset.moments_batch(out)[2]
+    return [dataclasses.replace(c, sigma_s=float(r * C5_HALF_LENGTH)) for c, r in zip(out, rms)]
+
+
+def objective(X6, W):
+    """Charge-weighted rms of the wake over the bunch at the last station
+    (the correlated energy-spread rate the bend imprints); lower is better."""
+    lam = np.maximum(X6[:, :, 0].astype(np.float64), 0)
+    e = W[:, :, -1].astype(np.float64)
+    wsum = lam.sum(1)
+    mean = (lam * e).sum(1) / wsum
+    return np.sqrt((lam * (e - mean[:, None]) ** 2).sum(1) / wsum)
+
+
+def prescreen(models, cases, top=16, unc_limit=0.02, max_reruns=256, chunk=8192, log=print):
+    """Objective of every variant under each model of an ensemble; returns
+    the variants to rerun in PIC (the `top` best by the ensemble mean, then
+    every variant whose ensemble spread exceeds unc_limit of its mean, most
+    uncertain first, up to max_reruns in all), with the screen's timing."""
+    from . import wakeset
+    t = time.perf_counter()
+    X6 = wakeset.features(cases)
+    t_feat = time.perf_counter() - t
+    J = []
+    sync = torch.cuda.synchronize if torch.cuda.is_available() else (lambda: None)
+    sync()
+    t = time.perf_counter()
+    for m in models:
+        X = torch.from_numpy(pad_features(X6)).to(m.net.device).to(torch.bfloat16)
+        W = m.net.predict(X, chunk=chunk)[:, :, -1:].cpu().numpy()
+        J.append(objective(X6, W * m.scale(X6)[:, None, None]))
+    sync()
+    t_net = time.perf_counter() - t
+    J = np.array(J)
+    mean, unc = J.mean(0), J.std(0) / J.mean(0)
+    best = np.argsort(mean)[:top]
+    bset = set(best.tolist())
+    risky = [k for k in np.argsort(-unc) if unc[k] > unc_limit and k not in bset]
+    rerun = list(best) + risky[:max(0, max_reruns - top)]
+    rec = {"variants": len(cases), "models": len(models), "features_s": t_feat, "network_s": t_net,
+           "over_unc_limit": int(np.sum(unc > unc_limit)), "reruns": len(rerun),
+           "unc_median": float(np.median(unc)), "unc_p99": float(np.quantile(unc, 0.99))}
+    if log:
+        log(json.dumps(rec))
+    return np.array(rerun), best, mean, unc, rec
+
+
+def production_config(nx=16384, ny=2048, h=2.5e-6, width=5e-3, cfl=0.4):
+    """The large production mesh: 16384 x 2048 cells of 2.5 um, R = 2 m,
+    gamma = 2000, TSC.  At CFL 0.4 a bunch at c crosses 16000 cells in 40000
+    steps, which fits the mesh; at CFL 0.5 it would reach the end wall after
+    about 32000."""
+    from .workloads import bend_config
+    return bend_config(nx, ny, h, C5_R, width, C5_GAMMA, shape_order=1, cfl=cfl)
+
+
+def production_run(case, n=32_000_000, steps=40_000, stations=32, cfg=None, log=print):
+    """The production run for one profile: quiet-start bunch of n particles
+    50 cells plus 6 sigma_s from the mesh start, FP32 mode, stepped as a
+    one-member ensemble (the batched path, one CUDA graph per step).  Records
+    the wake on the 256 bins every steps/stations steps; returns the wakes and
+    the timing (device time of the stepping; the station reads excluded)."""
+    from scipy.special import ndtri
+    from . import wakeset
+    from .pic import Ensemble, Simulation
+    cfg = cfg or production_config()
+    sim = Simulation(cfg, fp32=True)
+    hx = sim.info()["hx"]
+    g = np.random.Generator(np.random.Philox(case.seed))
+    x = 50 * hx + 6 * case.sigma_s + wakeset.quiet_offsets(case, n)
+    q = np.clip(np.mod(g.uniform() + wakeset.GOLDEN * np.arange(n), 1.0), 0.5 / n, 1 - 0.5 / n)
+    y = 0.5 * cfg.width + case.sigma_s / 2.5 * ndtri(q)
+    gam = case.gamma * (1.0 + 1e-4 * g.standard_normal(n))
+    sim.load(x, y, np.sqrt(gam * gam - 1.0), np.zeros(n), np.full(n, wakeset.CHARGE / n))
+    del x, y, gam, q
+    t = time.perf_counter()
+    rep = sim.initial_fields()
+    t_poisson = time.perf_counter() - t
+    ens = Ensemble([sim])
+    reader = wakeset._WakeReader([sim], [case.sigma_s])
+    every = steps // stations
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    st = torch.cuda.ExternalStream(ens.stream())
+    W, dev_ms = [], 0.0
+    t = time.perf_counter()
+    for j in range(stations):
+        a.record(st)
+        ens.step(every)
+        b.record(st)
+        ens.sync()
+        dev_ms += a.elapsed_time(b)
+        w, _ = reader.read()
+        W.append(w[0])
+        if log and (j % 8 == 7 or j == stations - 1):
+            log("production: %d steps, %.2f ms/step" % ((j + 1) * every, dev_ms / ((j + 1) * every)))
+    wall = time.perf_counter() - t
+    mom = sim.moments()
+    ens.close()
+    sim.close()
+    return np.array(W).T, {"particles": n, "steps": every * stations, "cells": cfg.Nx * cfg.Ny,
+                           "ms_per_step": dev_ms / (every * stations), "wall_s": wall,
+                           "particle_steps_per_s": n * every * stations / (dev_ms / 1e3),
+                           "poisson_s": t_poisson, "poisson": rep["solves"], "final_moments": mom[:8].tolist()}
 
 
 def pic_seconds_per_case(d):

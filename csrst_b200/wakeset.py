@@ -147,15 +147,16 @@ def case_config(case):
 GOLDEN = 0.6180339887498949
 
 
-def case_bunch(case, cfg, lb, n):
+def case_bunch(case, cfg, lb, n, shift=0.0):
     """Two-dimensional quiet start: particle k sits at the (k + 1/2)/n
     quantile of the profile in s and at the quantile frac(u0 + k * 0.618...)
     of the transverse Gaussian (a rank-1 lattice; u0 drawn from the case
-    seed, so that seeds give independent realisations); gamma spread drawn."""
+    seed, so that seeds give independent realisations); gamma spread drawn.
+    shift moves the bunch by that fraction of a cell in s."""
     from scipy.special import ndtri
     g = np.random.Generator(np.random.Philox(case.seed))
     u0 = g.uniform()
-    x = lb - 6 * case.sigma_s + quiet_offsets(case, n)
+    x = lb - 6 * case.sigma_s + shift * case.sigma_s / CELLS_PER_SIGMA + quiet_offsets(case, n)
     q = np.mod(u0 + GOLDEN * np.arange(n), 1.0)
     q = np.clip(q, 0.5 / n, 1.0 - 0.5 / n)
     y = 0.5 * cfg.width + case.sigma_s / 2.5 * ndtri(q)
@@ -174,22 +175,71 @@ def station_steps():
 NFEATURES = 7
 
 
-def features(cases):
+def _params(cases):
+    """Shape parameters of many cases as arrays [N, 1]."""
+    f = lambda name: np.array([getattr(c, name) for c in cases], dtype=np.float64)[:, None]
+    return {k: f(k) for k in ("kind", "edge", "tilt", "horn_pos", "horn_w", "horn_a", "horn_b")}
+
+
+def shape_batch(P, z, kind):
+    """shape() for many cases of one family at once: P from _params, z [N, m]."""
+    if kind == 0:
+        return np.exp(-0.5 * z * z)
+    e = P["edge"] * math.sqrt(2.0)
+    ft = np.maximum(0.5 * (erf((z + 1.0) / e) - erf((z - 1.0) / e)) * (1.0 + P["tilt"] * z), 0.0)
+    if kind == 1:
+        return ft
+    hw = 2.0 * P["horn_w"] ** 2
+    return ft + P["horn_a"] * np.exp(-(z + P["horn_pos"]) ** 2 / hw) + P["horn_b"] * np.exp(-(z - P["horn_pos"]) ** 2 / hw)
+
+
+def moments_batch(cases, fine=512):
+    """(mass, centroid, rms) of the families' shapes, vectorised per family
+    (a Gaussian analytically; the flat-top families, whose support lies
+    within +-3 of their scale, by the trapezoid rule on a fine grid)."""
+    z = np.linspace(-3.0, 3.0, fine)
+    dz = z[1] - z[0]
+    wq = np.full(fine, dz)
+    wq[0] = wq[-1] = 0.5 * dz
+    kinds = np.array([c.kind for c in cases])
+    mass, mu, rms = np.full(len(cases), math.sqrt(2 * math.pi)), np.zeros(len(cases)), np.ones(len(cases))
+    for kind in (1, 2):
+        idx = np.nonzero(kinds == kind)[0]
+        for a in range(0, len(idx), 4096):
+            sel = idx[a:a + 4096]
+            d = shape_batch(_params([cases[k] for k in sel]), z[None, :], kind)
+            mass[sel] = d @ wq
+            mu[sel] = (d * z) @ wq / mass[sel]
+            rms[sel] = np.sqrt((d * (z[None, :] - mu[sel, None]) ** 2) @ wq / mass[sel])
+    return mass, mu, rms
+
+
+def features(cases, chunk=4096):
     """[N][256][7] float32: line density per sigma_s, bin position / SPAN,
     log-scaled gamma, R, sigma_s, pipe width / sigma_s (each about [-1, 1]
     over the drawn ranges), and the slope of the line density (per sigma_s^2,
-    / 4)."""
-    s = bin_centres() / SPAN
-    out = np.zeros((len(cases), NBINS, NFEATURES), dtype=np.float32)
-    for k, c in enumerate(cases):
-        cfg, _ = case_config(c)
-        out[k, :, 0] = line_density(c)
-        out[k, :, 1] = s
-        out[k, :, 2] = (math.log(c.gamma) - math.log(632.5)) / 1.152
-        out[k, :, 3] = (math.log(c.R) - math.log(1.581)) / 1.152
-        out[k, :, 4] = (math.log(c.sigma_s) - math.log(63.25e-6)) / 1.152
-        out[k, :, 5] = (cfg.width / c.sigma_s - 80.0) / 16.0
-        out[k, :, 6] = np.gradient(out[k, :, 0], 2 * SPAN / NBINS) / 4.0
+    / 4).  Vectorised per family over chunks of cases: a Gaussian is centred
+    with unit rms; the flat-top families (support within +-3 of their scale)
+    take centroid and rms from a fine grid; the density at the bins comes
+    from the shape itself."""
+    N = len(cases)
+    out = np.zeros((N, NBINS, NFEATURES), dtype=np.float32)
+    sb = bin_centres()
+    mass_all, mu_all, rms_all = moments_batch(cases)
+    kinds = np.array([c.kind for c in cases])
+    for kind in (0, 1, 2):
+        idx = np.nonzero(kinds == kind)[0]
+        for a in range(0, len(idx), chunk):
+            sel = idx[a:a + chunk]
+            P = _params([cases[k] for k in sel])
+            mass, mu, rms = mass_all[sel], mu_all[sel], rms_all[sel]
+            lam = shape_batch(P, mu[:, None] + sb[None, :] * rms[:, None], kind) / mass[:, None] * rms[:, None]
+            out[sel, :, 0] = lam
+            out[sel, :, 6] = np.gradient(lam, 2 * SPAN / NBINS, axis=1) / 4.0
+    out[:, :, 1] = sb[None, :] / SPAN
+    for j, (name, ref) in enumerate((("gamma", 632.5), ("R", 1.581), ("sigma_s", 63.25e-6))):
+        out[:, :, 2 + j] = ((np.log([getattr(c, name) for c in cases]) - math.log(ref)) / 1.152)[:, None]
+    out[:, :, 5] = ((np.array([case_config(c)[0].width / c.sigma_s for c in cases]) - 80.0) / 16.0)[:, None]
     return out
 
 
@@ -244,7 +294,7 @@ class _WakeReader:
         return out, ok
 
 
-def run_cases(cases, n_particles=50_000, batch=256, fp32=True, log=None):
+def run_cases(cases, n_particles=50_000, batch=256, fp32=True, log=None, shift=0.0):
     """Runs every case in batches of `batch` members (one Ensemble each) and
     returns wakes [N][256][32] (float32, V/m), the mask of bins inside the
     sampled window columns (same shape) and per-batch run facts (the stepping
@@ -270,7 +320,7 @@ def run_cases(cases, n_particles=50_000, batch=256, fp32=True, log=None):
                     log("case %d skipped: %s" % (a + k, e))
                 wakes[a + k] = np.nan
                 continue
-            s.load(*case_bunch(c, cfg, lb, n_particles))
+            s.load(*case_bunch(c, cfg, lb, n_particles, shift))
             s.initial_fields()
             sims.append(s)
             keep.append(k)

@@ -193,10 +193,10 @@ int csrst_nn_gelu_bwd(const float *dy, const float *pre, float *dx32, void *dx16
 int csrst_nn_cast_bf16(const float *x, void *y, long long n, void *stream);
 /* out[c] (+)= sum over rows of x[r][c] in a fixed order; part: ceil(rows/256)*cols floats of scratch */
 int csrst_nn_colsum(const float *x, int rows, int cols, float *part, float *out, int accumulate, void *stream);
-/* loss = mean (pred - target)^2; grad[(i/gd)*g0 + (i%gd)*g1] = 2 (pred_i - target_i) / n (grad may be NULL);
- * part: 256 doubles of scratch; loss: one device double */
-int csrst_nn_mse(const float *pred, const float *target, long long n, float *grad, int gd, long long g0, long long g1,
-                 double *part, double *loss, void *stream);
+/* loss = mean (w_i (pred_i - target_i))^2 (w = 1 when weight is NULL); grad[(i/gd)*g0 + (i%gd)*g1] =
+ * 2 w_i^2 (pred_i - target_i) / n (grad may be NULL); part: 256 doubles of scratch; loss: one device double */
+int csrst_nn_mse(const float *pred, const float *target, const float *weight, long long n, float *grad, int gd,
+                 long long g0, long long g1, double *part, double *loss, void *stream);
 /* Adam with bias correction; the step counter *t and coef = {lr_t, 1 - b1^t, 1 - b2^t} live on the device:
  * adam_tick advances t and writes coef (cosine schedule from lr0 to lr_min over `total` steps) */
 int csrst_nn_adam_tick(int *t, float *coef, float lr0, float lr_min, int total, float b1, float b2, void *stream);

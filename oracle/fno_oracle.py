@@ -143,14 +143,16 @@ class FNO:
         out, _ = self.forward(X)
         return float(np.mean((out - T) ** 2))
 
-    def backward(self, X, T):
-        """Loss and gradient dict for mean-squared error against T [B][256][nout]."""
+    def backward(self, X, T, weight=None):
+        """Loss and gradient dict for the mean squared error against T
+        [B][256][nout], each output's error multiplied by weight (default 1)."""
         p, r = self.p, self.r
         out, st = self.forward(X)
         n = out.size
         g = {}
-        dOut = 2.0 * (out - T) / n
-        loss = float(np.mean((out - T) ** 2))
+        w = 1.0 if weight is None else np.asarray(weight, dtype=np.float64)
+        dOut = 2.0 * w * w * (out - T) / n
+        loss = float(np.mean((w * (out - T)) ** 2))
         dO16 = r(dOut)
         g["Q2"] = np.einsum("bns,bnc->sc", dO16, st["A1"])
         g["q2"] = dOut.sum(axis=(0, 1))

@@ -85,6 +85,23 @@ def test_gradients_close_to_fp64_fft_oracle(case):
             assert rel(gg[k], v) <= 3e-2, (k, rel(gg[k], v))
 
 
+def test_weighted_loss_matches_oracle(case):
+    """Outputs with weight 0 (bins the PIC did not sample) drop out of the
+    loss and of every gradient."""
+    import torch
+    g = np.random.default_rng(9)
+    wt = (g.random(case["T"].shape) < 0.8).astype(np.float32)
+    net = case["net"]
+    loss = float(net.loss_and_grad(case["Xd"], torch.from_numpy(case["T"]).cuda(), torch.from_numpy(wt).cuda()).item())
+    torch.cuda.synchronize()
+    net.check()
+    ref_loss, ref = OracleFNO(case["p"], bf16=True).backward(case["X"], case["T"], wt)
+    assert abs(loss - ref_loss) <= 1e-4 * ref_loss
+    got = net.grads()
+    for k in ("Q2", "q2", "W3", "b0", "P"):
+        assert rel(got[k], ref[k]) <= 5e-3, k
+
+
 def test_inference_path_matches_training_forward(case):
     pred = case["net"].predict(case["Xd"], chunk=32).cpu().numpy()
     assert np.array_equal(pred, case["out"])
