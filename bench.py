@@ -61,6 +61,7 @@ def parse():
                    help="mode of the headline value; the other mode is timed beside it")
     p.add_argument("--no-compare", action="store_true", help="skip the other precision and the accuracy check")
     p.add_argument("--no-ensemble", action="store_true", help="skip the 64-member batched-ensemble workload")
+    p.add_argument("--no-surrogate", action="store_true", help="skip the wake-surrogate measurements")
     return p.parse_args()
 
 
@@ -71,11 +72,17 @@ def dist_setup():
     return world, rank, local
 
 
-def peaks():
+def peaks(bf16=False):
+    """HBM GB/s (and, with bf16=True, (hbm, dense BF16 TFLOP/s burst, source))
+    from MEASURED_PEAKS.json, else the pool's fallback figures."""
     f = ROOT / "MEASURED_PEAKS.json"
     if f.exists():
         d = json.loads(f.read_text())
+        if bf16:
+            return float(d["hbm_gbs"]), float(d.get("bf16_tflops", 1590.0)), "measured bf16_tflops"
         return float(d["hbm_gbs"]), "measured"
+    if bf16:
+        return 6650.0, 1590.0, "fallback bf16 (no MEASURED_PEAKS.json)"
     return 6650.0, "fallback"
 
 
@@ -359,6 +366,98 @@ def run_ensemble(args, rank, members=64, ms=None, fields=True):
     return out
 
 
+def run_surrogate(args):
+    """The learned part, measured live.  (1) Inference of the wake surrogate
+    (1D FNO: width 128, 32 modes, 4 layers; every product on the tcgen05
+    GEMM) at a batch of 65536 profiles resident on the device, with the
+    weights as initialised (the time does not depend on their values), and
+    its tensor roofline.  (2) Training steps per second (batch 64, the step
+    captured as one CUDA graph).  (3) What the surrogate replaces: the batched
+    FP32 PIC's cost per data-set case (256 cases stepped as one ensemble for
+    256 steps, scaled to a case's 2144 steps; set-up reported apart), and the
+    screening speed-up.  Its accuracy against PIC needs the 4096-run data set
+    and a trained model: profiles/surrogate_wake.md."""
+    import torch
+    from csrst_b200 import wakescreen, wakeset
+    from csrst_b200.pic import Ensemble, Simulation
+    from csrst_b200.surrogate import FNO
+    out = {}
+    cases = wakeset.draw_cases(256, seed=99)
+    X6 = wakeset.features(cases)
+    net = FNO(seed=0)
+    model = wakescreen.WakeModel(net, np.zeros(7), 1.0)
+    inf = wakescreen.time_inference(model, X6, n=65536, chunk=8192)
+    _, tf_peak, src = peaks(bf16=True)
+    t0 = time.perf_counter()
+    feats = wakeset.features(wakescreen.c5_variants(20000))
+    feat_s = (time.perf_counter() - t0) / 20000
+    out["inference"] = dict(inf, roofline={"kernel": "k_gemm (all products of the forward pass)", "bound": "tensor",
+                                           "achieved": round(inf["tflops"], 2), "peak": tf_peak, "unit": "TFLOP/s",
+                                           "frac": round(inf["tflops"] / tf_peak, 4), "peak_source": src},
+                            host_features_s_per_profile=round(feat_s, 7))
+    # training steps
+    B = 64
+    Xs = torch.from_numpy(wakescreen.pad_features(np.repeat(X6[:B], 1, axis=0))).cuda().to(torch.bfloat16)
+    Ts = torch.randn(B, wakeset.NBINS, 32, device="cuda")
+    Ms = torch.ones_like(Ts)
+    net.loss_and_grad(Xs, Ts, Ms)
+    net.adam(total=1000)
+    side = torch.cuda.Stream()
+    side.wait_stream(torch.cuda.current_stream())
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g, stream=side):
+        net.loss_and_grad(Xs, Ts, Ms)
+        net.adam(total=1000)
+    for _ in range(3):
+        g.replay()
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(200):
+        g.replay()
+    b.record()
+    torch.cuda.synchronize()
+    net.check()
+    out["training"] = {"batch": B, "ms_per_step": round(a.elapsed_time(b) / 200, 4),
+                       "library_calls_per_step": 106,
+                       "what": "forward, hand-written backward and Adam, captured as one CUDA graph"}
+    del g
+    # the PIC it replaces: 256 data-set cases as one ensemble
+    t0 = time.perf_counter()
+    sims = []
+    for c in cases:
+        cfg, lb = wakeset.case_config(c)
+        try:
+            s = Simulation(cfg, fp32=True)
+        except Exception:
+            continue
+        s.load(*wakeset.case_bunch(c, cfg, lb, 50_000))
+        s.initial_fields()
+        sims.append(s)
+    ens = Ensemble(sims)
+    ens.sync()
+    setup = (time.perf_counter() - t0) / len(sims)
+    ens.step(8)
+    ens.sync()
+    st = torch.cuda.ExternalStream(ens.stream())
+    a.record(st)
+    ens.step(256)
+    b.record(st)
+    ens.sync()
+    ms = a.elapsed_time(b) / 256
+    ens.close()
+    for s in sims:
+        s.close()
+    per_case = ms * 1e-3 * wakeset.station_steps()[-1] / len(sims)
+    sur = inf["seconds"] / inf["profiles"]
+    out["pic_per_case"] = {"members": len(sims), "ms_per_ensemble_step": round(ms, 3),
+                           "stepping_s_per_case": round(per_case, 5), "setup_s_per_case": round(setup, 4),
+                           "what": "50k-particle TSC cases, 2144 steps, FP32 batched ensemble of 256"}
+    out["screening_speedup"] = {"network_only": round(per_case / sur), "with_host_features": round(per_case / (sur + feat_s)),
+                                "bar": ">= 1000x faster than PIC"}
+    return out
+
+
 def run_b200(args, world, rank, local):
     import torch
     from csrst_b200.workloads import make_bunch, workload
@@ -438,6 +537,8 @@ def run_b200(args, world, rank, local):
         out["batched_ensemble_small"] = dict(run_ensemble(args, rank, ms=small, fields=False),
                                              what="256 members of 512x104 meshes at 20 um with 4000 particles "
                                                   "each, CIC/TSC/cubic, zero initial fields")
+    if rank == 0 and not args.no_surrogate:
+        out["surrogate"] = run_surrogate(args)
     if not args.no_e2e:
         out["e2e"] = run_e2e(args, cfg, spec, bunch, rank, world, head == "fp32")
     if rank == 0 and world == 1 and not args.no_cpu:

@@ -71,6 +71,7 @@ def lib():
         "csrst_gemm_bf16": ([P, C.c_longlong, C.c_longlong, P, C.c_longlong, C.c_longlong, C.c_int, C.c_int,
                              C.c_int, C.c_int, P, P, P], C.c_int),
         "csrst_nn_transpose_bf16": ([P, P, C.c_int, C.c_int, C.c_int, C.c_int, P], C.c_int),
+        "csrst_nn_transpose_b32": ([P, P, C.c_int, C.c_int, C.c_int, C.c_int, P], C.c_int),
         "csrst_nn_gelu_bwd": ([P, P, P, P, C.c_longlong, P], C.c_int),
         "csrst_nn_cast_bf16": ([P, P, C.c_longlong, P], C.c_int),
         "csrst_nn_colsum": ([P, C.c_int, C.c_int, P, P, C.c_int, P], C.c_int),

@@ -11,9 +11,11 @@
 //     stage into an FP32 accumulator in tensor memory (TMEM) and commits them
 //     to the stage's mbarrier, which frees the stage for the next copy;
 //   - the epilogue reads the accumulator with tcgen05.ld (warp w owns TMEM
-//     lanes 32w .. 32w + 31, i.e. rows) and writes FP32 and/or BF16 through an
-//     affine index map, so that transposed and mode-major layouts come out
-//     directly.
+//     lanes 32w .. 32w + 31, i.e. rows) into an FP32 staging tile in the
+//     freed operand stages, then writes FP32 and/or BF16 outputs through
+//     affine index maps (transposed and mode-major layouts come out
+//     directly), each swept in the order - along rows or along columns -
+//     that puts a warp's stores next to each other under its map.
 // Waits on mbarriers are bounded; a wait that gives up sets *err, skips the
 // epilogue and still frees the TMEM.
 #include <cuda_bf16.h>
@@ -114,10 +116,32 @@ __device__ __forceinline__ void load_tile(uint8_t *dst, const __nv_bfloat16 *src
   }
 }
 
+// Affine output index of tile element (m, n) of batch z under a map.
+__device__ __forceinline__ long long map_index(long long zb, int m, int n, int md, int nd, long long s0, long long s1,
+                                               long long t0, long long t1) {
+  return zb + (long long)(m / md) * s0 + (long long)(m % md) * s1 + (long long)(n / nd) * t0 +
+         (long long)(n % nd) * t1;
+}
+
+// Visits the tile's (row, column) pairs so that the 32 lanes of a warp take
+// consecutive columns (m_fast == 0) or consecutive rows (m_fast == 1): the
+// order in which the output map puts neighbouring lanes next to each other.
+template <int BN, class F>
+__device__ __forceinline__ void tile_order(int m_fast, F &&f) {
+  if (m_fast) {
+    for (int c = 0; c < BN; ++c) f(threadIdx.x, c);
+  } else {
+    constexpr int kRows = kThreads / BN;  // rows per sweep of the block
+    const int c = threadIdx.x % BN;
+    for (int r = threadIdx.x / BN; r < kBM; r += kRows) f(r, c);
+  }
+}
+
 template <int BN>
 __global__ void __launch_bounds__(kThreads) k_gemm(const __nv_bfloat16 *A, long long lda, long long sA,
                                                    const __nv_bfloat16 *B, long long ldb, long long sB, int M,
-                                                   int N, int K, csrst_gemm_epilogue ep, int *err) {
+                                                   int N, int K, csrst_gemm_epilogue ep, int *err, int o_mfast,
+                                                   int t_mfast) {
   extern __shared__ __align__(1024) uint8_t smem[];
   __shared__ uint64_t bar[2];
   __shared__ uint32_t tmem_base;
@@ -187,7 +211,12 @@ __global__ void __launch_bounds__(kThreads) k_gemm(const __nv_bfloat16 *A, long 
   if (s_fail) {
     if (threadIdx.x == 0) atomicExch(err, 1);
   } else {
-    const int m = m0 + warp * 32 + lane;
+    // The MMAs have completed and every copy has landed: the operand stages
+    // become an FP32 staging tile [128][BN + 1] (the +1 keeps both row- and
+    // column-wise sweeps free of bank conflicts).
+    constexpr int LD = BN + 1;
+    float *tile = reinterpret_cast<float *>(base);
+    const int r = warp * 32 + lane;
     for (int c0 = 0; c0 < BN; c0 += 16) {
       uint32_t v[16];
       const uint32_t ta = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0;
@@ -198,27 +227,33 @@ __global__ void __launch_bounds__(kThreads) k_gemm(const __nv_bfloat16 *A, long 
             "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
           : "r"(ta));
       asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-      if (m >= M) continue;
 #pragma unroll
-      for (int j = 0; j < 16; ++j) {
-        const int n = n0 + c0 + j;
-        if (n >= N) continue;
-        float x = ep.alpha * __uint_as_float(v[j]);
-        if (ep.bias) x += ep.bias[n];
-        const long long o = (long long)z * ep.sb + (long long)(m / ep.md) * ep.sm0 + (long long)(m % ep.md) * ep.sm1 +
-                            (long long)(n / ep.nd) * ep.sn0 + (long long)(n % ep.nd) * ep.sn1;
-        if (ep.res) x += ep.res[o];
-        if (ep.pre) ep.pre[o] = x;
-        if (ep.act == 1) x = gelu(x);
-        if (ep.out32) ep.out32[o] = ep.accumulate ? ep.out32[o] + x : x;
-        if (ep.out16) reinterpret_cast<__nv_bfloat16 *>(ep.out16)[o] = __float2bfloat16(x);
-        if (ep.out16t) {
-          const long long t = (long long)z * ep.tb + (long long)(m / ep.tmd) * ep.tm0 +
-                              (long long)(m % ep.tmd) * ep.tm1 + (long long)(n / ep.tnd) * ep.tn0 +
-                              (long long)(n % ep.tnd) * ep.tn1;
-          reinterpret_cast<__nv_bfloat16 *>(ep.out16t)[t] = __float2bfloat16(x);
-        }
-      }
+      for (int j = 0; j < 16; ++j) tile[r * LD + c0 + j] = __uint_as_float(v[j]);
+    }
+    __syncthreads();
+    const long long zo = (long long)z * ep.sb, zt = (long long)z * ep.tb;
+    // outputs through the primary map, in the order that map makes contiguous
+    tile_order<BN>(o_mfast, [&](int rr, int cc) {
+      const int m = m0 + rr, n = n0 + cc;
+      if (m >= M || n >= N) return;
+      float x = ep.alpha * tile[rr * LD + cc];
+      if (ep.bias) x += ep.bias[n];
+      const long long o = map_index(zo, m, n, ep.md, ep.nd, ep.sm0, ep.sm1, ep.sn0, ep.sn1);
+      if (ep.res) x += ep.res[o];
+      if (ep.pre) ep.pre[o] = x;
+      if (ep.act == 1) x = gelu(x);
+      if (ep.out32) ep.out32[o] = ep.accumulate ? ep.out32[o] + x : x;
+      if (ep.out16) reinterpret_cast<__nv_bfloat16 *>(ep.out16)[o] = __float2bfloat16(x);
+      tile[rr * LD + cc] = x;
+    });
+    if (ep.out16t) {  // the second BF16 copy through its own map and order
+      __syncthreads();
+      tile_order<BN>(t_mfast, [&](int rr, int cc) {
+        const int m = m0 + rr, n = n0 + cc;
+        if (m >= M || n >= N) return;
+        const long long t = map_index(zt, m, n, ep.tmd, ep.tnd, ep.tm0, ep.tm1, ep.tn0, ep.tn1);
+        reinterpret_cast<__nv_bfloat16 *>(ep.out16t)[t] = __float2bfloat16(tile[rr * LD + cc]);
+      });
     }
   }
   cp_async_wait<0>();  // nothing still landing in shared memory (an early exit leaves copies in flight)
@@ -227,10 +262,37 @@ __global__ void __launch_bounds__(kThreads) k_gemm(const __nv_bfloat16 *A, long 
   if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(BN));
 }
 
+// 32-byte sectors one warp's 32 stores touch under a map when its lanes take
+// 32 consecutive rows (m_fast) or 32 consecutive columns of a tile at the
+// origin, for elements of `bytes` bytes.
+int warp_sectors(int md, int nd, long long sm0, long long sm1, long long sn0, long long sn1, int m_fast,
+                 int bytes) {
+  long long sec[32];
+  int k = 0;
+  for (int i = 0; i < 32; ++i) {
+    const int m = m_fast ? i : 0, n = m_fast ? 0 : i;
+    const long long a = ((long long)(m / md) * sm0 + (long long)(m % md) * sm1 + (long long)(n / nd) * sn0 +
+                         (long long)(n % nd) * sn1) * bytes;
+    const long long s = a >= 0 ? a / 32 : -((-a + 31) / 32);
+    bool seen = false;
+    for (int j = 0; j < k; ++j) seen |= sec[j] == s;
+    if (!seen) sec[k++] = s;
+  }
+  return k;
+}
+
+// 1 when a warp's stores touch fewer sectors with its lanes on consecutive
+// rows than on consecutive columns: the epilogue then sweeps the tile by rows.
+int rows_fast(int md, int nd, long long sm0, long long sm1, long long sn0, long long sn1, int bytes) {
+  return warp_sectors(md, nd, sm0, sm1, sn0, sn1, 1, bytes) < warp_sectors(md, nd, sm0, sm1, sn0, sn1, 0, bytes);
+}
+
 template <int BN>
 int launch_gemm(const void *A, long long lda, long long sA, const void *B, long long ldb, long long sB, int M, int N,
                 int K, int batch, const csrst_gemm_epilogue &ep, int *err, cudaStream_t s) {
-  const int smem = 2 * (kBM * kBK * 2 + BN * kBK * 2) + 1024;
+  // operand stages, or the FP32 staging tile of the epilogue if larger, plus alignment slack
+  const int stages = 2 * (kBM * kBK * 2 + BN * kBK * 2), staging = kBM * (BN + 1) * 4;
+  const int smem = (stages > staging ? stages : staging) + 1024;
   static bool attr = false;
   if (!attr) {
     if (cudaFuncSetAttribute(k_gemm<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess)
@@ -238,8 +300,12 @@ int launch_gemm(const void *A, long long lda, long long sA, const void *B, long 
     attr = true;
   }
   dim3 grid((N + BN - 1) / BN, (M + kBM - 1) / kBM, batch);
+  const int o_bytes = (ep.out32 || ep.res || ep.pre) ? 4 : 2;
+  const int o_mfast = rows_fast(ep.md, ep.nd, ep.sm0, ep.sm1, ep.sn0, ep.sn1, o_bytes);
+  const int t_mfast = ep.out16t ? rows_fast(ep.tmd, ep.tnd, ep.tm0, ep.tm1, ep.tn0, ep.tn1, 2) : 0;
   k_gemm<BN><<<grid, kThreads, smem, s>>>(static_cast<const __nv_bfloat16 *>(A), lda, sA,
-                                          static_cast<const __nv_bfloat16 *>(B), ldb, sB, M, N, K, ep, err);
+                                          static_cast<const __nv_bfloat16 *>(B), ldb, sB, M, N, K, ep, err, o_mfast,
+                                          t_mfast);
   return cudaGetLastError() == cudaSuccess ? CSRST_OK : CSRST_E_CUDA;
 }
 

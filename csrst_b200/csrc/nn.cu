@@ -12,9 +12,11 @@ namespace {
 __device__ __forceinline__ long long gtid() { return blockIdx.x * (long long)blockDim.x + threadIdx.x; }
 inline unsigned grid_of(long long n) { return (unsigned)((n + 255) / 256 < 65535 * 16 ? (n + 255) / 256 : 65535 * 16); }
 
-// [z][r][c] -> [z][c][r] (dst rows ldd apart) through 32 x 32 shared-memory tiles.
-__global__ void k_transpose(const __nv_bfloat16 *src, __nv_bfloat16 *dst, int rows, int cols, int ldd) {
-  __shared__ __nv_bfloat16 t[32][33];
+// [z][r][c] -> [z][c][r] (dst rows ldd apart) through 32 x 32 shared-memory
+// tiles; T is a BF16 value or a 32-bit pair of them.
+template <class T>
+__global__ void k_transpose(const T *src, T *dst, int rows, int cols, int ldd) {
+  __shared__ T t[32][33];
   const long long z = blockIdx.z;
   src += z * (long long)rows * cols;
   dst += z * (long long)ldd * cols;
@@ -160,8 +162,18 @@ int csrst_nn_transpose_bf16(const void *src, void *dst, int batch, int rows, int
       (rows + 31) / 32 > 65535)
     return CSRST_E_ARG;
   dim3 g((cols + 31) / 32, (rows + 31) / 32, batch);
-  k_transpose<<<g, dim3(32, 8), 0, (cudaStream_t)stream>>>((const __nv_bfloat16 *)src, (__nv_bfloat16 *)dst, rows,
-                                                           cols, ldd);
+  k_transpose<__nv_bfloat16><<<g, dim3(32, 8), 0, (cudaStream_t)stream>>>((const __nv_bfloat16 *)src,
+                                                                         (__nv_bfloat16 *)dst, rows, cols, ldd);
+  return cudaGetLastError() == cudaSuccess ? CSRST_OK : CSRST_E_CUDA;
+}
+
+int csrst_nn_transpose_b32(const void *src, void *dst, int batch, int rows, int cols, int ldd, void *stream) {
+  if (!src || !dst || batch <= 0 || rows <= 0 || cols <= 0 || batch > 65535 || ldd < rows ||
+      (rows + 31) / 32 > 65535 || ((uintptr_t)src & 3) || ((uintptr_t)dst & 3))
+    return CSRST_E_ARG;
+  dim3 g((cols + 31) / 32, (rows + 31) / 32, batch);
+  k_transpose<uint32_t><<<g, dim3(32, 8), 0, (cudaStream_t)stream>>>((const uint32_t *)src, (uint32_t *)dst, rows,
+                                                                     cols, ldd);
   return cudaGetLastError() == cudaSuccess ? CSRST_OK : CSRST_E_CUDA;
 }
 

@@ -77,7 +77,16 @@ def _ck(rc, what):
 
 class _Buffers:
     """Activations and scratch of one batch size (training keeps every
-    layer's input for the backward pass; inference ping-pongs two)."""
+    layer's input for the backward pass; inference ping-pongs two).
+
+    Layouts (b member, n bin, c channel, k mode, ri real/imaginary):
+      V16  [b][n][c]      rows of the pointwise products
+      Tv16 [b][c][n]      rows (b, c) of 256 bins: the forward DFT's operand
+      Vg16 [c][b][n]      every bin of a channel in one row: weight gradients
+      U16  [k][b][2c+ri]  spectra, the mode mixing's operand
+      Z16  [k][b][2o+p]   mixed spectra; Zp16 [b][o][2k+p] the inverse DFT's operand
+    Every product writes its large outputs in a layout its epilogue can store
+    contiguously; the others come from transposes."""
 
     def __init__(self, net, B, train):
         w, m, L, dev = net.width, net.modes, net.layers, net.device
@@ -85,15 +94,17 @@ class _Buffers:
         bf, f32 = dict(dtype=torch.bfloat16, device=dev), dict(dtype=torch.float32, device=dev)
         nkeep = L + 1 if train else 2
         self.V16 = [torch.empty(R, w, **bf) for _ in range(nkeep)]
-        self.Vt16 = [torch.empty(w, R, **bf) for _ in range(nkeep)]
+        self.Tv16 = [torch.empty(B * w, NBINS, **bf) for _ in range(nkeep)]
         self.Hp = torch.empty(R, w, **f32)
         self.U16 = torch.empty(m, B, 2 * w, **bf)
+        self.Z16 = torch.empty(m, B, 2 * w, **bf)
         self.Zp16 = torch.empty(B * w, 2 * m, **bf)
         self.A1_16 = torch.empty(R, w, **bf)
         self.out = torch.empty(R, net.nout, **f32)
         self.train = train
         if not train:
             return
+        self.Vg16 = [torch.empty(w, R, **bf) for _ in range(L + 1)]
         self.Ut16 = [torch.empty(m, 2 * w, B, **bf) for _ in range(L)]
         self.Hfull = [torch.empty(R, w, **f32) for _ in range(L - 1)]
         self.A1pre = torch.empty(R, w, **f32)
@@ -110,7 +121,8 @@ class _Buffers:
         self.dVn = torch.empty(R, w, **f32)
         self.dZ16 = torch.empty(m, B, 2 * w, **bf)
         self.dZt16 = torch.empty(m, 2 * w, B, **bf)
-        self.dS16 = torch.empty(w * B, 2 * m, **bf)
+        self.dSk16 = torch.empty(m, B, 2 * w, **bf)
+        self.dS16 = torch.empty(B * w, 2 * m, **bf)
         self.dMk = torch.empty(m, 2 * w, 2 * w, **f32)
         self.part = torch.empty(max(R // KSPLIT, 1) * max(w * w, w * NFEAT), **f32)
         # column-sum scratch: ceil(rows / 256) * cols floats for every column sum of the backward pass
@@ -201,32 +213,45 @@ class FNO:
         return self._bufs[key]
 
     # ---- forward ----
+    def _tr16(self, src, dst, batch, rows, cols, ldd=None):
+        _ck(lib().csrst_nn_transpose_bf16(_p(src), _p(dst), batch, rows, cols, ldd or rows, _stream()), "transpose")
+
+    def _tr32(self, src, dst, rows, cols):
+        _ck(lib().csrst_nn_transpose_b32(_p(src), _p(dst), 1, rows, cols, rows, _stream()), "transpose")
+
     def _forward(self, bf, B, X16, out=None):
         w, m, L, R = self.width, self.modes, self.layers, B * NBINS
         tr = bf.train
         w16 = lambda n: self.view(n, self.w16)
-        gemm(X16, w16("P"), R, w, NFEAT, bias=self.view("p"), out16=bf.V16[0], out16t=bf.Vt16[0],
-             tmap=dict(md=1, nd=1, sm0=1, sm1=0, sn0=R, sn1=0))
+        # lift: V0 in rows and in per-member channel rows
+        gemm(X16, w16("P"), R, w, NFEAT, bias=self.view("p"), out16=bf.V16[0], out16t=bf.Tv16[0],
+             tmap=dict(md=NBINS, nd=1, sm0=w * NBINS, sm1=1, sn0=NBINS, sn1=0))
         for l in range(L):
             i, o = (l, l + 1) if tr else (l & 1, (l + 1) & 1)
-            V, Vt = bf.V16[i], bf.Vt16[i]
-            gemm(V, w16("W%d" % l), R, w, w, bias=self.view("b%d" % l), out32=bf.Hp)
-            # forward DFT over the bins: rows (channel c, member b) of Vt -> U[k][b][2c + ri]
-            gemm(Vt, self.F16, w * B, 2 * m, NBINS, out16=bf.U16,
-                 omap=dict(md=B, nd=2, sm0=2, sm1=2 * w, sn0=2 * w * B, sn1=1),
-                 out16t=bf.Ut16[l] if tr else None, tmap=dict(md=B, nd=2, sm0=2 * B, sm1=1, sn0=2 * w * B, sn1=B))
-            # mode mixing: per mode k, Z[b][2o + p] = sum U[b][2c + q] Mk[2o + p][2c + q] -> Zp[(b, o)][2k + p]
+            if tr:
+                self._tr16(bf.V16[i], bf.Vg16[i], 1, R, w)
+            gemm(bf.V16[i], w16("W%d" % l), R, w, w, bias=self.view("b%d" % l), out32=bf.Hp)
+            # forward DFT over the bins: rows (member b, channel c) -> U[k][b][2c + ri]
+            gemm(bf.Tv16[i], self.F16, B * w, 2 * m, NBINS, out16=bf.U16,
+                 omap=dict(md=w, nd=2, sm0=2 * w, sm1=2, sn0=2 * w * B, sn1=1))
+            if tr:
+                self._tr16(bf.U16, bf.Ut16[l], m, B, 2 * w)
+            # mode mixing: per mode k, Z[b][2o + p] = sum U[b][2c + q] Mk[2o + p][2c + q]
             gemm(bf.U16, self.Mk16[l], B, 2 * w, 2 * w, batch=m, stride_a=2 * w * B, stride_b=4 * w * w,
-                 out16=bf.Zp16, omap=dict(md=1, nd=2, sm0=2 * m * w, sm1=0, sn0=2 * m, sn1=1), sb=2)
-            # truncated inverse DFT + pointwise product + bias -> H; activation; V (rows) and V^T (channels)
+                 out16=bf.Z16, omap=rowmap(2 * w), sb=2 * w * B)
+            # (mode, (member, channel)) pairs -> ((member, channel), mode) pairs: Zp[(b, o)][2k + p]
+            self._tr32(bf.Z16, bf.Zp16, m, B * w)
+            # truncated inverse DFT + pointwise product + bias -> H; activation; V in both layouts
             act = l < L - 1
             last = l == L - 1
-            gemm(bf.Zp16, self.G16, w * B, NBINS, 2 * m, res=bf.Hp, pre=bf.Hfull[l] if (tr and act) else None,
+            gemm(bf.Zp16, self.G16, B * w, NBINS, 2 * m, res=bf.Hp, pre=bf.Hfull[l] if (tr and act) else None,
                  act=1 if act else 0, out16=bf.V16[o],
                  omap=dict(md=w, nd=1, sm0=NBINS * w, sm1=1, sn0=w, sn1=0),
-                 out16t=None if (last and not tr) else bf.Vt16[o],
-                 tmap=dict(md=w, nd=1, sm0=NBINS, sm1=R, sn0=1, sn1=0))
+                 out16t=None if last else bf.Tv16[o],
+                 tmap=dict(md=w, nd=1, sm0=w * NBINS, sm1=NBINS, sn0=1, sn1=0))
         Vl = bf.V16[L if tr else L & 1]
+        if tr:
+            self._tr16(Vl, bf.Vg16[L], 1, R, w)
         gemm(Vl, w16("Q1"), R, w, w, bias=self.view("q1"), act=1, pre=bf.A1pre if tr else None, out16=bf.A1_16,
              out16t=bf.A1t16 if tr else None, tmap=dict(md=1, nd=1, sm0=1, sm1=0, sn0=R, sn1=0))
         gemm(bf.A1_16, w16("Q2"), R, self.nout, w, bias=self.view("q2"), out32=bf.out if out is None else out)
@@ -270,7 +295,7 @@ class FNO:
         gemm(bf.dOut16, self.Q2T16, R, w, 64, out32=bf.dA1)
         _ck(lb.csrst_nn_gelu_bwd(_p(bf.dA1), _p(bf.A1pre), _p(bf.dH), _p(bf.dH16), R * w, s), "gelu")
         _ck(lb.csrst_nn_transpose_bf16(_p(bf.dH16), _p(bf.dHt16), 1, R, w, R, s), "transpose")
-        self._wgrad(bf, bf.dHt16, bf.Vt16[L], w, w, R, "Q1")
+        self._wgrad(bf, bf.dHt16, bf.Vg16[L], w, w, R, "Q1")
         self._colsum(bf, bf.dH, R, w, self.view("q1", self.g))
         gemm(bf.dH16, self.Q1T16, R, w, w, out32=bf.dV)
         dV, dVn = bf.dV, bf.dVn
@@ -282,24 +307,25 @@ class FNO:
                 _ck(lb.csrst_nn_cast_bf16(_p(dV), _p(bf.dH16), R * w, s), "cast")
                 dH = dV
             _ck(lb.csrst_nn_transpose_bf16(_p(bf.dH16), _p(bf.dHt16), 1, R, w, R, s), "transpose")
-            self._wgrad(bf, bf.dHt16, bf.Vt16[l], w, w, R, "W%d" % l)
+            self._wgrad(bf, bf.dHt16, bf.Vg16[l], w, w, R, "W%d" % l)
             self._colsum(bf, dH, R, w, self.view("b%d" % l, self.g))
-            # adjoint of the inverse DFT: dZ[(o, b)][2k + ri] = sum_n dH[b][n][o] G[n][2k + ri]
-            gemm(bf.dHt16, self.GT16, w * B, 2 * m, NBINS, out16=bf.dZ16,
-                 omap=dict(md=B, nd=2, sm0=2, sm1=2 * w, sn0=2 * w * B, sn1=1),
-                 out16t=bf.dZt16, tmap=dict(md=B, nd=2, sm0=2 * B, sm1=1, sn0=2 * w * B, sn1=B))
+            # adjoint of the inverse DFT: dZ[k][(o, ri)][b] = sum_n dH[b][n][o] G[n][2k + ri] (rows (o, b) of dH^T)
+            gemm(bf.dHt16, self.GT16, w * B, 2 * m, NBINS, out16=bf.dZt16,
+                 omap=dict(md=B, nd=2, sm0=2 * B, sm1=1, sn0=2 * w * B, sn1=B))
+            self._tr16(bf.dZt16, bf.dZ16, m, 2 * w, B)
             # mode-mixing weights: dMk[k] = dZ_k^T U_k, then back to (dWr, dWi)
             gemm(bf.dZt16, bf.Ut16[l], 2 * w, 2 * w, B, batch=m, stride_a=2 * w * B, stride_b=2 * w * B,
                  out32=bf.dMk, omap=rowmap(2 * w), sb=4 * w * w)
             _ck(lb.csrst_nn_spectral_unpack(_p(bf.dMk), m, w, _p(self.view("Wr%d" % l, self.g)),
                                             _p(self.view("Wi%d" % l, self.g)), s), "spectral unpack")
-            # dU_k = dZ_k Mk -> dS[(c, b)][2k + q]
+            # dU_k = dZ_k Mk -> dSk[k][b][2c + q] -> dS[(b, c)][2k + q]
             gemm(bf.dZ16, self.MkT16[l], B, 2 * w, 2 * w, batch=m, stride_a=2 * w * B, stride_b=4 * w * w,
-                 out16=bf.dS16, omap=dict(md=1, nd=2, sm0=2 * m, sm1=0, sn0=2 * m * B, sn1=1), sb=2)
+                 out16=bf.dSk16, omap=rowmap(2 * w), sb=2 * w * B)
+            self._tr32(bf.dSk16, bf.dS16, m, B * w)
             # input gradient: pointwise part, then the adjoint of the forward DFT added on
             gemm(bf.dH16, self.WT16[l], R, w, w, out32=dVn)
-            gemm(bf.dS16, self.FT16, w * B, NBINS, 2 * m, out32=dVn, accumulate=True,
-                 omap=dict(md=B, nd=1, sm0=1, sm1=NBINS * w, sn0=w, sn1=0))
+            gemm(bf.dS16, self.FT16, B * w, NBINS, 2 * m, out32=dVn, accumulate=True,
+                 omap=dict(md=w, nd=1, sm0=NBINS * w, sm1=1, sn0=w, sn1=0))
             dV, dVn = dVn, dV
         _ck(lb.csrst_nn_cast_bf16(_p(dV), _p(bf.dH16), R * w, s), "cast")
         _ck(lb.csrst_nn_transpose_bf16(_p(bf.dH16), _p(bf.dHt16), 1, R, w, R, s), "transpose")

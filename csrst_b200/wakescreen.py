@@ -2,6 +2,7 @@
 
   python -m csrst_b200.wakescreen train --data wakes.npz --out model.npz
   python -m csrst_b200.wakescreen evaluate --data wakes.npz --model model.npz
+  python -m csrst_b200.wakescreen time --n 65536          (inference throughput)
 
 A model is the network's parameters plus the output normalisation: each case's
 wake is divided by an amplitude law exp(a . phi(x)) fitted by least squares on
@@ -374,6 +375,86 @@ def production_run(case, n=32_000_000, steps=40_000, stations=32, cfg=None, log=
                            "poisson_s": t_poisson, "poisson": rep["solves"], "final_moments": mom[:8].tolist()}
 
 
+def _summary(e):
+    e = np.asarray(e, dtype=np.float64)
+    e = e[np.isfinite(e)]
+    return {"n": int(e.size), "mean": float(e.mean()), "median": float(np.median(e)),
+            "p90": float(np.quantile(e, 0.9)), "max": float(e.max()), "frac_le_2pct": float(np.mean(e <= 0.02))}
+
+
+def study(d, models=4, steps=40000, variants=100000, top=16, out=None, log=print):
+    """The whole workflow on a data set: train `models` networks (seeds 0..),
+    judge each and their mean on the held-out cases against the
+    alignment-averaged PIC (with the single PIC runs' own scatter beside it),
+    time inference at 65536 profiles, prescreen `variants` production
+    profiles, rerun the selected ones in PIC (alignment-averaged) and compare.
+    Writes a JSON record to `out` after every stage."""
+    from . import wakeset
+    R = {}
+
+    def dump():
+        if out:
+            with open(out, "w") as f:
+                json.dump(R, f, indent=1)
+
+    facts = d["facts"]
+    R["data"] = {"cases": len(d["cases"]), "skipped": d.get("skipped", 0),
+                 "pic_s_per_case_stepping": pic_seconds_per_case(d),
+                 "pic_s_per_case_setup": sum(f["setup_s"] for f in facts) / sum(f["members"] for f in facts)}
+    nets = []
+    for k in range(models):
+        m, rec = train(d, steps=steps, seed=k, log=None)
+        rec.pop("losses")
+        R["train%d" % k] = rec
+        nets.append(m)
+        dump()
+    R["inference"] = time_inference(nets[0], d["X"][:64], n=65536, chunk=8192)
+    tr, te = split(len(d["X"]))
+    held = [d["cases"][k] for k in te]
+    mean, mask, runs = pic_reference(held, log=None)
+    R["eval"] = [evaluate(m, d, ref=(mean, mask), log=None)[0] for m in nets]
+    R["eval_single_pic_judge"] = evaluate(nets[0], d, log=None)[0]
+    P = np.mean([m.predict(d["X"][te]) for m in nets], axis=0)
+    err = rel_errors(P, mean, mask)
+    kinds = np.array([c.kind for c in held])
+    R["ensemble_mean_eval"] = {"all": _summary(err), **{n: _summary(err[kinds == i]) for i, n in
+                                                        enumerate(("gaussian", "flat_top", "double_horn"))}}
+    dump()
+    t = time.perf_counter()
+    var = c5_variants(variants)
+    t_var = time.perf_counter() - t
+    rerun, best, J, unc, rec = prescreen(nets, var, top=top, log=None)
+    rec["variants_s"] = t_var
+    R["prescreen"] = rec
+    dump()
+    sel = [var[k] for k in rerun]
+    t = time.perf_counter()
+    pm, pmask, _ = pic_reference(sel, log=None)
+    t_pic = time.perf_counter() - t
+    Xs = wakeset.features(sel)
+    Ps = np.mean([m.predict(Xs) for m in nets], axis=0)
+    ran = np.all(np.isfinite(pm.reshape(len(sel), -1)), axis=1)     # the reference's geometry asserts for a few
+    e_sel = np.full(len(sel), np.nan)
+    e_sel[ran] = rel_errors(Ps[ran], pm[ran], pmask[ran])
+    Jp, Js = np.full(len(sel), np.nan), objective(Xs, Ps)
+    Jp[ran] = objective(Xs[ran], pm[ran])
+    rank = lambda a: np.argsort(np.argsort(a))
+    istop = np.arange(len(sel)) < len(best)
+    b = int(np.argmin(np.where(ran, Jp, np.inf)))
+    R["reruns"] = {"count": len(sel), "ran": int(ran.sum()), "pic_seconds_4_shifts": t_pic,
+                   "wake_err": _summary(e_sel), "wake_err_top": _summary(e_sel[istop]),
+                   "wake_err_uncertain": _summary(e_sel[~istop]),
+                   "objective_err": _summary(np.abs(Js - Jp) / Jp),
+                   "objective_err_top": _summary((np.abs(Js - Jp) / Jp)[istop]),
+                   "spearman_all": float(np.corrcoef(rank(Jp[ran]), rank(Js[ran]))[0, 1]),
+                   "spearman_top": float(np.corrcoef(rank(Jp[ran & istop]), rank(Js[ran & istop]))[0, 1]),
+                   "pic_best": {"variant": int(rerun[b]), "in_surrogate_top": bool(istop[b]),
+                                "surrogate_rank_among_reruns": int(np.sum(Js[ran] < Js[b])),
+                                "J_pic": float(Jp[b]), "J_surrogate": float(Js[b])}}
+    dump()
+    return R, nets
+
+
 def pic_seconds_per_case(d):
     f = d["facts"]
     return sum(x["seconds"] for x in f) / sum(x["members"] for x in f)
@@ -383,8 +464,14 @@ if __name__ == "__main__":
     import argparse
     from . import wakeset
     ap = argparse.ArgumentParser(description="train / evaluate the wake surrogate")
-    ap.add_argument("cmd", choices=["train", "evaluate"])
-    ap.add_argument("--data", required=True, help="data files, comma-separated")
+    ap.add_argument("cmd", choices=["train", "evaluate", "time", "study", "production"])
+    ap.add_argument("--variant", type=int, default=0, help="production variant index (production)")
+    ap.add_argument("--particles", type=int, default=32_000_000, help="production bunch size (production)")
+    ap.add_argument("--models", type=int, default=4, help="networks in the ensemble (study)")
+    ap.add_argument("--variants", type=int, default=100000, help="production variants to screen (study)")
+    ap.add_argument("--json", default=None, help="where study writes its record")
+    ap.add_argument("--n", type=int, default=65536, help="profiles per inference batch (time)")
+    ap.add_argument("--data", default=None, help="data files, comma-separated")
     ap.add_argument("--model", default=None)
     ap.add_argument("--out", default=None)
     ap.add_argument("--steps", type=int, default=20000)
@@ -392,7 +479,29 @@ if __name__ == "__main__":
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--seed", type=int, default=0)
     a = ap.parse_args()
+    if a.cmd == "production":  # the 16384 x 2048 run of one screened variant (no data needed)
+        v = c5_variants(a.variant + 1)[a.variant]
+        W, rec = production_run(v, n=a.particles, steps=a.steps)
+        rec["variant"], rec["variant_index"] = v.dict(), a.variant
+        if a.json:
+            with open(a.json, "w") as f:
+                json.dump(rec, f, indent=1)
+        if a.out:
+            np.savez_compressed(a.out, W=W.astype(np.float32))
+        print(json.dumps(rec))
+        raise SystemExit(0)
+    if a.cmd == "time":  # inference throughput with the weights as initialised (no data needed)
+        cases = wakeset.draw_cases(64, seed=99)
+        m = WakeModel(FNO(seed=a.seed), np.zeros(7), 1.0)
+        print(json.dumps(time_inference(m, wakeset.features(cases), n=a.n, chunk=min(a.n, 8192))))
+        raise SystemExit(0)
     d = wakeset.load(*a.data.split(","))
+    if a.cmd == "study":
+        R, nets = study(d, models=a.models, steps=a.steps, variants=a.variants, out=a.json)
+        if a.out:
+            nets[0].save(a.out)
+        print(json.dumps(R))
+        raise SystemExit(0)
     if a.cmd == "train":
         m, rec = train(d, steps=a.steps, batch=a.batch, lr0=a.lr, seed=a.seed)
         print(json.dumps(rec))

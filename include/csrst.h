@@ -188,6 +188,8 @@ int csrst_gemm_bf16(const void *A, long long lda, long long stride_a, const void
  * (device pointers; BF16 arrays as void *).  No reference counterpart. */
 /* [batch][rows][cols] -> [batch][cols][ldd] (ldd >= rows; columns rows .. ldd - 1 untouched) */
 int csrst_nn_transpose_bf16(const void *src, void *dst, int batch, int rows, int cols, int ldd, void *stream);
+/* the same for 32-bit elements (pairs of BF16 values kept together); 4-byte aligned pointers */
+int csrst_nn_transpose_b32(const void *src, void *dst, int batch, int rows, int cols, int ldd, void *stream);
 /* dx = dy * GELU'(pre) (erf form); dx32 and/or dx16 */
 int csrst_nn_gelu_bwd(const float *dy, const float *pre, float *dx32, void *dx16, long long n, void *stream);
 int csrst_nn_cast_bf16(const float *x, void *y, long long n, void *stream);
