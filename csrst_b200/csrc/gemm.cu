@@ -230,15 +230,28 @@ __global__ void __launch_bounds__(kThreads) k_gemm(const __nv_bfloat16 *A, long 
 #pragma unroll
       for (int j = 0; j < 16; ++j) tile[r * LD + c0 + j] = __uint_as_float(v[j]);
     }
+    // Each map's address is a row part plus a column part: both computed once
+    // per tile (128 + BN divisions instead of two per element).
+    __shared__ long long s_row[2][kBM], s_col[2][BN];
+    {
+      const int m = m0 + threadIdx.x;
+      s_row[0][threadIdx.x] = (long long)z * ep.sb + map_index(0, m, 0, ep.md, ep.nd, ep.sm0, ep.sm1, 0, 0);
+      if (ep.out16t)
+        s_row[1][threadIdx.x] = (long long)z * ep.tb + map_index(0, m, 0, ep.tmd, ep.tnd, ep.tm0, ep.tm1, 0, 0);
+      if (threadIdx.x < BN) {
+        const int n = n0 + threadIdx.x;
+        s_col[0][threadIdx.x] = map_index(0, 0, n, 1, ep.nd, 0, 0, ep.sn0, ep.sn1);
+        if (ep.out16t) s_col[1][threadIdx.x] = map_index(0, 0, n, 1, ep.tnd, 0, 0, ep.tn0, ep.tn1);
+      }
+    }
     __syncthreads();
-    const long long zo = (long long)z * ep.sb, zt = (long long)z * ep.tb;
     // outputs through the primary map, in the order that map makes contiguous
     tile_order<BN>(o_mfast, [&](int rr, int cc) {
       const int m = m0 + rr, n = n0 + cc;
       if (m >= M || n >= N) return;
       float x = ep.alpha * tile[rr * LD + cc];
       if (ep.bias) x += ep.bias[n];
-      const long long o = map_index(zo, m, n, ep.md, ep.nd, ep.sm0, ep.sm1, ep.sn0, ep.sn1);
+      const long long o = s_row[0][rr] + s_col[0][cc];
       if (ep.res) x += ep.res[o];
       if (ep.pre) ep.pre[o] = x;
       if (ep.act == 1) x = gelu(x);
@@ -251,7 +264,7 @@ __global__ void __launch_bounds__(kThreads) k_gemm(const __nv_bfloat16 *A, long 
       tile_order<BN>(t_mfast, [&](int rr, int cc) {
         const int m = m0 + rr, n = n0 + cc;
         if (m >= M || n >= N) return;
-        const long long t = map_index(zt, m, n, ep.tmd, ep.tnd, ep.tm0, ep.tm1, ep.tn0, ep.tn1);
+        const long long t = s_row[1][rr] + s_col[1][cc];
         reinterpret_cast<__nv_bfloat16 *>(ep.out16t)[t] = __float2bfloat16(tile[rr * LD + cc]);
       });
     }
