@@ -123,17 +123,29 @@ __device__ __forceinline__ long long map_index(long long zb, int m, int n, int m
          (long long)(n % nd) * t1;
 }
 
-// Visits the tile's (row, column) pairs so that the 32 lanes of a warp take
-// consecutive columns (m_fast == 0) or consecutive rows (m_fast == 1): the
-// order in which the output map puts neighbouring lanes next to each other.
+// Visits the tile's (row, column) pairs in groups of eight per thread, so
+// that the 32 lanes of a warp take consecutive columns (m_fast == 0) or
+// consecutive rows (m_fast == 1): the order in which the output map puts
+// neighbouring lanes next to each other.  A group's reads of global memory
+// (residual, accumulated output) are all issued before its first store.
+constexpr int kGroup = 8;
 template <int BN, class F>
 __device__ __forceinline__ void tile_order(int m_fast, F &&f) {
+  int rr[kGroup], cc[kGroup];
   if (m_fast) {
-    for (int c = 0; c < BN; ++c) f(threadIdx.x, c);
+    for (int c = 0; c < BN; c += kGroup) {
+#pragma unroll
+      for (int j = 0; j < kGroup; ++j) rr[j] = threadIdx.x, cc[j] = c + j;
+      f(rr, cc);
+    }
   } else {
     constexpr int kRows = kThreads / BN;  // rows per sweep of the block
     const int c = threadIdx.x % BN;
-    for (int r = threadIdx.x / BN; r < kBM; r += kRows) f(r, c);
+    for (int r = threadIdx.x / BN; r < kBM; r += kGroup * kRows) {
+#pragma unroll
+      for (int j = 0; j < kGroup; ++j) rr[j] = r + j * kRows, cc[j] = c;
+      f(rr, cc);
+    }
   }
 }
 
@@ -246,26 +258,42 @@ __global__ void __launch_bounds__(kThreads) k_gemm(const __nv_bfloat16 *A, long 
     }
     __syncthreads();
     // outputs through the primary map, in the order that map makes contiguous
-    tile_order<BN>(o_mfast, [&](int rr, int cc) {
-      const int m = m0 + rr, n = n0 + cc;
-      if (m >= M || n >= N) return;
-      float x = ep.alpha * tile[rr * LD + cc];
-      if (ep.bias) x += ep.bias[n];
-      const long long o = s_row[0][rr] + s_col[0][cc];
-      if (ep.res) x += ep.res[o];
-      if (ep.pre) ep.pre[o] = x;
-      if (ep.act == 1) x = gelu(x);
-      if (ep.out32) ep.out32[o] = ep.accumulate ? ep.out32[o] + x : x;
-      if (ep.out16) reinterpret_cast<__nv_bfloat16 *>(ep.out16)[o] = __float2bfloat16(x);
-      tile[rr * LD + cc] = x;
+    tile_order<BN>(o_mfast, [&](const int *rr, const int *cc) {
+      long long o[kGroup];
+      bool ok[kGroup];
+      float rv[kGroup], ov[kGroup];
+#pragma unroll
+      for (int j = 0; j < kGroup; ++j) {
+        ok[j] = m0 + rr[j] < M && n0 + cc[j] < N;
+        o[j] = s_row[0][rr[j]] + s_col[0][cc[j]];
+      }
+#pragma unroll
+      for (int j = 0; j < kGroup; ++j) {
+        rv[j] = (ok[j] && ep.res) ? ep.res[o[j]] : 0.0f;
+        ov[j] = (ok[j] && ep.out32 && ep.accumulate) ? ep.out32[o[j]] : 0.0f;
+      }
+#pragma unroll
+      for (int j = 0; j < kGroup; ++j) {
+        if (!ok[j]) continue;
+        float x = ep.alpha * tile[rr[j] * LD + cc[j]];
+        if (ep.bias) x += ep.bias[n0 + cc[j]];
+        if (ep.res) x += rv[j];
+        if (ep.pre) ep.pre[o[j]] = x;
+        if (ep.act == 1) x = gelu(x);
+        if (ep.out32) ep.out32[o[j]] = ep.accumulate ? ov[j] + x : x;
+        if (ep.out16) reinterpret_cast<__nv_bfloat16 *>(ep.out16)[o[j]] = __float2bfloat16(x);
+        tile[rr[j] * LD + cc[j]] = x;
+      }
     });
     if (ep.out16t) {  // the second BF16 copy through its own map and order
       __syncthreads();
-      tile_order<BN>(t_mfast, [&](int rr, int cc) {
-        const int m = m0 + rr, n = n0 + cc;
-        if (m >= M || n >= N) return;
-        const long long t = s_row[1][rr] + s_col[1][cc];
-        reinterpret_cast<__nv_bfloat16 *>(ep.out16t)[t] = __float2bfloat16(tile[rr * LD + cc]);
+      tile_order<BN>(t_mfast, [&](const int *rr, const int *cc) {
+#pragma unroll
+        for (int j = 0; j < kGroup; ++j) {
+          if (m0 + rr[j] >= M || n0 + cc[j] >= N) continue;
+          reinterpret_cast<__nv_bfloat16 *>(ep.out16t)[s_row[1][rr[j]] + s_col[1][cc[j]]] =
+              __float2bfloat16(tile[rr[j] * LD + cc[j]]);
+        }
       });
     }
   }
