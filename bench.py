@@ -62,6 +62,9 @@ def parse():
     p.add_argument("--no-compare", action="store_true", help="skip the other precision and the accuracy check")
     p.add_argument("--no-ensemble", action="store_true", help="skip the 64-member batched-ensemble workload")
     p.add_argument("--no-surrogate", action="store_true", help="skip the wake-surrogate measurements")
+    p.add_argument("--ensemble-only", default=None, choices=["c3", "small"],
+                   help="time only the batched FP32 ensemble (c3: 64 uneven members; small: 256 512x104 members)")
+    p.add_argument("--shape", default=None, help="push_ctas,tx,ty,parts for --ensemble-only instead of the autotuner")
     return p.parse_args()
 
 
@@ -366,6 +369,54 @@ def run_ensemble(args, rank, members=64, ms=None, fields=True):
     return out
 
 
+def small_members():
+    """256 members of 512 x 104 meshes at 20 um with 4000 particles each,
+    CIC / TSC / cubic in turn."""
+    from csrst_b200.workloads import workload as wl
+    small = []
+    for k in range(256):
+        c, sp = wl(f"small-{k % 3}")
+        sp.seed = 500 + k
+        small.append((c, sp))
+    return small
+
+
+def ensemble_only(args):
+    """The batched FP32 ensemble alone (for profiling): build, tune or set
+    the launch shape, warm up, time `steps` steps on the device."""
+    import torch
+    from csrst_b200 import Ensemble, Simulation
+    from csrst_b200.workloads import ensemble_members, make_bunch
+    ms = small_members() if args.ensemble_only == "small" else ensemble_members(64, seed=2024)
+    sims = []
+    for cfg, spec in ms:
+        sm = Simulation(cfg, fp32=True)
+        sm.load(*make_bunch(spec))
+        if args.ensemble_only == "c3":
+            sm.initial_fields(1e-12, 1e-6, 500)
+        sims.append(sm)
+    ens = Ensemble(sims)
+    if args.shape:
+        ens.set_shape(*(int(v) for v in args.shape.split(",")))
+    else:
+        ens.tune(steps=2)
+    ens.step(args.warmup)
+    ens.sync()
+    st = torch.cuda.ExternalStream(ens.stream())
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0.record(st)
+    ens.step(args.steps)
+    t1.record(st)
+    ens.sync()
+    ms_ = t0.elapsed_time(t1) / args.steps
+    total = sum(spec.n for _, spec in ms)
+    ens.close()
+    for sm in sims:
+        sm.close()
+    return {"ensemble": args.ensemble_only, "members": len(ms), "particles": total, "ms_per_step": round(ms_, 4),
+            "particle_steps_per_s": round(total / (ms_ * 1e-3), 1), "shape": args.shape or "tuned"}
+
+
 def run_surrogate(args):
     """The learned part, measured live.  (1) Inference of the wake surrogate
     (1D FNO: width 128, 32 modes, 4 layers; every product on the tcgen05
@@ -529,12 +580,7 @@ def run_b200(args, world, rank, local):
     if not args.no_ensemble:
         out["batched_ensemble"] = run_ensemble(args, rank)
         # many small members: the regime where the batch's few launches per step matter
-        from csrst_b200.workloads import workload as wl
-        small = []
-        for k in range(256):
-            c, sp = wl(f"small-{k % 3}")
-            sp.seed = 500 + k
-            small.append((c, sp))
+        small = small_members()
         out["batched_ensemble_small"] = dict(run_ensemble(args, rank, ms=small, fields=False),
                                              what="256 members of 512x104 meshes at 20 um with 4000 particles "
                                                   "each, CIC/TSC/cubic, zero initial fields")
@@ -661,7 +707,12 @@ def main():
         torch.cuda.set_device(local)
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     try:
-        out = run_reference(args, world, rank) if args.impl == "reference" else run_b200(args, world, rank, local)
+        if args.ensemble_only and args.impl != "reference":
+            import torch
+            torch.cuda.set_device(local)
+            out = ensemble_only(args) if rank == 0 else None
+        else:
+            out = run_reference(args, world, rank) if args.impl == "reference" else run_b200(args, world, rank, local)
     finally:
         if world > 1:
             import torch

@@ -70,6 +70,9 @@ def lib():
         "csrst_ensemble_tune": ([P, C.c_int, D, C.c_int, I], C.c_int),
         "csrst_gemm_bf16": ([P, C.c_longlong, C.c_longlong, P, C.c_longlong, C.c_longlong, C.c_int, C.c_int,
                              C.c_int, C.c_int, P, P, P], C.c_int),
+        "csrst_gemm_bf16_dual": ([P, C.c_longlong, C.c_longlong, P, C.c_longlong, C.c_longlong, C.c_int, P,
+                                  C.c_longlong, C.c_longlong, P, C.c_longlong, C.c_longlong, C.c_int, C.c_int,
+                                  C.c_int, C.c_int, P, P, P], C.c_int),
         "csrst_nn_transpose_bf16": ([P, P, C.c_int, C.c_int, C.c_int, C.c_int, P], C.c_int),
         "csrst_nn_transpose_b32": ([P, P, C.c_int, C.c_int, C.c_int, C.c_int, P], C.c_int),
         "csrst_nn_gelu_bwd": ([P, P, P, P, C.c_longlong, P], C.c_int),

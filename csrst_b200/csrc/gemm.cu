@@ -149,11 +149,21 @@ __device__ __forceinline__ void tile_order(int m_fast, F &&f) {
   }
 }
 
+// One K segment of a product: A[M, Kseg] and B[N, Kseg], K-major, batch
+// strides sA / sB, nk tiles of 64 K-columns.  A product runs over the K
+// tiles of its first segment and then of its second (nk = 0 when absent):
+// C = A1 B1^T + A2 B2^T in one accumulator.
+struct Seg {
+  const __nv_bfloat16 *A;
+  long long lda, sA;
+  const __nv_bfloat16 *B;
+  long long ldb, sB;
+  int nk;
+};
+
 template <int BN>
-__global__ void __launch_bounds__(kThreads) k_gemm(const __nv_bfloat16 *A, long long lda, long long sA,
-                                                   const __nv_bfloat16 *B, long long ldb, long long sB, int M,
-                                                   int N, int K, csrst_gemm_epilogue ep, int *err, int o_mfast,
-                                                   int t_mfast) {
+__global__ void __launch_bounds__(kThreads) k_gemm(Seg g0, Seg g1, int M, int N, csrst_gemm_epilogue ep, int *err,
+                                                   int o_mfast, int t_mfast) {
   extern __shared__ __align__(1024) uint8_t smem[];
   __shared__ uint64_t bar[2];
   __shared__ uint32_t tmem_base;
@@ -161,8 +171,19 @@ __global__ void __launch_bounds__(kThreads) k_gemm(const __nv_bfloat16 *A, long 
   constexpr int kA = kBM * kBK * 2, kB = BN * kBK * 2, kStage = kA + kB;
   uint8_t *base = smem + ((1024 - (smem_u32(smem) & 1023)) & 1023);
   const int z = blockIdx.z, m0 = blockIdx.y * kBM, n0 = blockIdx.x * BN;
-  A += (long long)z * sA;
-  B += (long long)z * sB;
+  g0.A += (long long)z * g0.sA;
+  g0.B += (long long)z * g0.sB;
+  if (g1.nk) {
+    g1.A += (long long)z * g1.sA;
+    g1.B += (long long)z * g1.sB;
+  }
+  // copies K tile kt (of either segment) into a stage
+  auto load_k = [&](uint8_t *stage, int kt) {
+    const Seg &g = kt < g0.nk ? g0 : g1;
+    const int k0 = (kt < g0.nk ? kt : kt - g0.nk) * kBK;
+    load_tile<kBM>(stage, g.A, g.lda, m0, M, k0);
+    load_tile<BN>(stage + kBM * kBK * 2, g.B, g.ldb, n0, N, k0);
+  };
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
   if (warp == 0) {  // TMEM: BN FP32 columns x 128 lanes
@@ -180,10 +201,9 @@ __global__ void __launch_bounds__(kThreads) k_gemm(const __nv_bfloat16 *A, long 
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;");
   const uint32_t tmem = tmem_base;
-  const int nk = K / kBK;
+  const int nk = g0.nk + g1.nk;
 
-  load_tile<kBM>(base, A, lda, m0, M, 0);
-  load_tile<BN>(base + kA, B, ldb, n0, N, 0);
+  load_k(base, 0);
   cp_async_commit();
   for (int kt = 0; kt < nk; ++kt) {
     const int s = kt & 1;
@@ -194,8 +214,7 @@ __global__ void __launch_bounds__(kThreads) k_gemm(const __nv_bfloat16 *A, long 
         __syncthreads();
         if (s_fail) break;
       }
-      load_tile<kBM>(base + s1 * kStage, A, lda, m0, M, (kt + 1) * kBK);
-      load_tile<BN>(base + s1 * kStage + kA, B, ldb, n0, N, (kt + 1) * kBK);
+      load_k(base + s1 * kStage, kt + 1);
       cp_async_commit();
       cp_async_wait<1>();
     } else {
@@ -277,6 +296,7 @@ __global__ void __launch_bounds__(kThreads) k_gemm(const __nv_bfloat16 *A, long 
         if (!ok[j]) continue;
         float x = ep.alpha * tile[rr[j] * LD + cc[j]];
         if (ep.bias) x += ep.bias[n0 + cc[j]];
+        if (ep.bias_m) x += ep.bias_m[m0 + rr[j]];
         if (ep.res) x += rv[j];
         if (ep.pre) ep.pre[o[j]] = x;
         if (ep.act == 1) x = gelu(x);
@@ -329,8 +349,8 @@ int rows_fast(int md, int nd, long long sm0, long long sm1, long long sn0, long 
 }
 
 template <int BN>
-int launch_gemm(const void *A, long long lda, long long sA, const void *B, long long ldb, long long sB, int M, int N,
-                int K, int batch, const csrst_gemm_epilogue &ep, int *err, cudaStream_t s) {
+int launch_gemm(const Seg &g0, const Seg &g1, int M, int N, int batch, const csrst_gemm_epilogue &ep, int *err,
+                cudaStream_t s) {
   // operand stages, or the FP32 staging tile of the epilogue if larger, plus alignment slack
   const int stages = 2 * (kBM * kBK * 2 + BN * kBK * 2), staging = kBM * (BN + 1) * 4;
   const int smem = (stages > staging ? stages : staging) + 1024;
@@ -344,10 +364,24 @@ int launch_gemm(const void *A, long long lda, long long sA, const void *B, long 
   const int o_bytes = (ep.out32 || ep.res || ep.pre) ? 4 : 2;
   const int o_mfast = rows_fast(ep.md, ep.nd, ep.sm0, ep.sm1, ep.sn0, ep.sn1, o_bytes);
   const int t_mfast = ep.out16t ? rows_fast(ep.tmd, ep.tnd, ep.tm0, ep.tm1, ep.tn0, ep.tn1, 2) : 0;
-  k_gemm<BN><<<grid, kThreads, smem, s>>>(static_cast<const __nv_bfloat16 *>(A), lda, sA,
-                                          static_cast<const __nv_bfloat16 *>(B), ldb, sB, M, N, K, ep, err, o_mfast,
-                                          t_mfast);
+  k_gemm<BN><<<grid, kThreads, smem, s>>>(g0, g1, M, N, ep, err, o_mfast, t_mfast);
   return cudaGetLastError() == cudaSuccess ? CSRST_OK : CSRST_E_CUDA;
+}
+
+bool seg_ok(const void *A, long long lda, long long sa, const void *B, long long ldb, long long sb, int K) {
+  return A && B && K > 0 && K % kBK == 0 && lda % 8 == 0 && ldb % 8 == 0 && lda >= K && ldb >= K &&
+         !((uintptr_t)A & 15) && !((uintptr_t)B & 15) && sa % 8 == 0 && sb % 8 == 0;
+}
+
+int gemm_dispatch(const Seg &g0, const Seg &g1, int M, int N, int batch, const csrst_gemm_epilogue *ep, int *err,
+                  void *stream) {
+  if (!ep || !err || M <= 0 || N <= 0 || batch <= 0 || N % 16 != 0 || ep->md <= 0 || ep->nd <= 0 ||
+      (ep->out16t && (ep->tmd <= 0 || ep->tnd <= 0)))
+    return CSRST_E_ARG;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (N % 128 == 0) return launch_gemm<128>(g0, g1, M, N, batch, *ep, err, s);
+  if (N % 64 == 0) return launch_gemm<64>(g0, g1, M, N, batch, *ep, err, s);
+  return launch_gemm<32>(g0, g1, M, N, batch, *ep, err, s);
 }
 
 }  // namespace
@@ -357,12 +391,23 @@ extern "C" int csrst_gemm_bf16(const void *A, long long lda, long long stride_a,
                                long long stride_b, int M, int N, int K, int batch, const csrst_gemm_epilogue *ep,
                                int *err, void *stream) {
   using namespace csrst;
-  if (!A || !B || !ep || !err || M <= 0 || N <= 0 || K <= 0 || batch <= 0 || K % kBK != 0 || N % 16 != 0 ||
-      lda % 8 != 0 || ldb % 8 != 0 || lda < K || ldb < K || ep->md <= 0 || ep->nd <= 0 || (ep->out16t && (ep->tmd <= 0 || ep->tnd <= 0)) ||
-      ((uintptr_t)A & 15) || ((uintptr_t)B & 15) || (stride_a % 8) || (stride_b % 8))
+  if (!seg_ok(A, lda, stride_a, B, ldb, stride_b, K)) return CSRST_E_ARG;
+  const Seg g0{static_cast<const __nv_bfloat16 *>(A), lda, stride_a, static_cast<const __nv_bfloat16 *>(B), ldb,
+               stride_b, K / kBK};
+  const Seg g1{nullptr, 0, 0, nullptr, 0, 0, 0};
+  return gemm_dispatch(g0, g1, M, N, batch, ep, err, stream);
+}
+
+extern "C" int csrst_gemm_bf16_dual(const void *A1, long long lda1, long long stride_a1, const void *B1,
+                                    long long ldb1, long long stride_b1, int K1, const void *A2, long long lda2,
+                                    long long stride_a2, const void *B2, long long ldb2, long long stride_b2, int K2,
+                                    int M, int N, int batch, const csrst_gemm_epilogue *ep, int *err, void *stream) {
+  using namespace csrst;
+  if (!seg_ok(A1, lda1, stride_a1, B1, ldb1, stride_b1, K1) || !seg_ok(A2, lda2, stride_a2, B2, ldb2, stride_b2, K2))
     return CSRST_E_ARG;
-  cudaStream_t s = static_cast<cudaStream_t>(stream);
-  if (N % 128 == 0) return launch_gemm<128>(A, lda, stride_a, B, ldb, stride_b, M, N, K, batch, *ep, err, s);
-  if (N % 64 == 0) return launch_gemm<64>(A, lda, stride_a, B, ldb, stride_b, M, N, K, batch, *ep, err, s);
-  return launch_gemm<32>(A, lda, stride_a, B, ldb, stride_b, M, N, K, batch, *ep, err, s);
+  const Seg g0{static_cast<const __nv_bfloat16 *>(A1), lda1, stride_a1, static_cast<const __nv_bfloat16 *>(B1), ldb1,
+               stride_b1, K1 / kBK};
+  const Seg g1{static_cast<const __nv_bfloat16 *>(A2), lda2, stride_a2, static_cast<const __nv_bfloat16 *>(B2), ldb2,
+               stride_b2, K2 / kBK};
+  return gemm_dispatch(g0, g1, M, N, batch, ep, err, stream);
 }

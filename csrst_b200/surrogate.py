@@ -14,11 +14,12 @@ Network (width w = 128, 32 Fourier modes, 4 layers, 32 outputs per bin):
   V_{l+1} = gelu(H_l) (l < 3), V_4 = H_3
   out     = gelu(V_4 Q1^T + q1) Q2^T + q2
 The spectral product is three GEMMs per layer: the forward DFT as a product
-with a [64 x 256] matrix of cosines and sines (rows in (channel, member)
+with a [64 x 256] matrix of cosines and sines (rows in (member, channel)
 order, output written mode-major), the mode mixing as a batch of 32 real
 [2w x 2w] block matrices (one per mode: [[Wr, -Wi], [Wi, Wr]] interleaved),
-and the truncated inverse DFT with the layer's pointwise product, bias,
-activation, BF16 copies and a transposed copy fused into its epilogue.
+and, per member, the truncated inverse DFT with the layer's pointwise product
+as a second K segment of the same accumulator, and bias, activation, the
+BF16 copies and a transposed copy fused into its epilogue.
 
 Activations are BF16 between products (FP32 accumulation inside them); the
 loss, gradients of biases and the Adam state are FP32.  Reductions are in a
@@ -31,7 +32,7 @@ import numpy as np
 import torch
 
 from ._lib import CsrstError, lib
-from .tensor import check_errors, gemm, rowmap
+from .tensor import check_errors, gemm, gemm_dual, rowmap
 
 NBINS, NFEAT = 256, 64
 KSPLIT = 256          # K-columns per partial product of a weight gradient
@@ -85,6 +86,9 @@ class _Buffers:
       Vg16 [c][b][n]      every bin of a channel in one row: weight gradients
       U16  [k][b][2c+ri]  spectra, the mode mixing's operand
       Z16  [k][b][2o+p]   mixed spectra; Zp16 [b][o][2k+p] the inverse DFT's operand
+    The pointwise product rides in the inverse DFT's accumulator as a second
+    K segment, so the layer's FP32 pre-activation sum never goes to memory
+    (it is kept only for training, for the activation's backward pass).
     Every product writes its large outputs in a layout its epilogue can store
     contiguously; the others come from transposes."""
 
@@ -95,7 +99,6 @@ class _Buffers:
         nkeep = L + 1 if train else 2
         self.V16 = [torch.empty(R, w, **bf) for _ in range(nkeep)]
         self.Tv16 = [torch.empty(B * w, NBINS, **bf) for _ in range(nkeep)]
-        self.Hp = torch.empty(R, w, **f32)
         self.U16 = torch.empty(m, B, 2 * w, **bf)
         self.Z16 = torch.empty(m, B, 2 * w, **bf)
         self.Zp16 = torch.empty(B * w, 2 * m, **bf)
@@ -230,7 +233,6 @@ class FNO:
             i, o = (l, l + 1) if tr else (l & 1, (l + 1) & 1)
             if tr:
                 self._tr16(bf.V16[i], bf.Vg16[i], 1, R, w)
-            gemm(bf.V16[i], w16("W%d" % l), R, w, w, bias=self.view("b%d" % l), out32=bf.Hp)
             # forward DFT over the bins: rows (member b, channel c) -> U[k][b][2c + ri]
             gemm(bf.Tv16[i], self.F16, B * w, 2 * m, NBINS, out16=bf.U16,
                  omap=dict(md=w, nd=2, sm0=2 * w, sm1=2, sn0=2 * w * B, sn1=1))
@@ -241,14 +243,17 @@ class FNO:
                  out16=bf.Z16, omap=rowmap(2 * w), sb=2 * w * B)
             # (mode, (member, channel)) pairs -> ((member, channel), mode) pairs: Zp[(b, o)][2k + p]
             self._tr32(bf.Z16, bf.Zp16, m, B * w)
-            # truncated inverse DFT + pointwise product + bias -> H; activation; V in both layouts
+            # per member b, one accumulator: H_b[o][n] = sum_j Zp[(b, o)][j] G[n][j]   (truncated inverse DFT)
+            #                                          + sum_c W[o][c] V[b][n][c]    (pointwise product)
+            # + bias[o]; pre-activation, activation, V in rows and in per-member channel rows
             act = l < L - 1
             last = l == L - 1
-            gemm(bf.Zp16, self.G16, B * w, NBINS, 2 * m, res=bf.Hp, pre=bf.Hfull[l] if (tr and act) else None,
-                 act=1 if act else 0, out16=bf.V16[o],
-                 omap=dict(md=w, nd=1, sm0=NBINS * w, sm1=1, sn0=w, sn1=0),
-                 out16t=None if last else bf.Tv16[o],
-                 tmap=dict(md=w, nd=1, sm0=w * NBINS, sm1=NBINS, sn0=1, sn1=0))
+            gemm_dual(bf.Zp16, self.G16, 2 * m, w16("W%d" % l), bf.V16[i], w, w, NBINS, stride_a1=2 * m * w,
+                      stride_b2=NBINS * w, batch=B, bias_m=self.view("b%d" % l),
+                      pre=bf.Hfull[l] if (tr and act) else None, act=1 if act else 0, out16=bf.V16[o],
+                      omap=dict(md=1, nd=1, sm0=1, sm1=0, sn0=w, sn1=0), sb=NBINS * w,
+                      out16t=None if last else bf.Tv16[o],
+                      tmap=dict(md=1, nd=1, sm0=NBINS, sm1=0, sn0=1, sn1=0), tb=w * NBINS)
         Vl = bf.V16[L if tr else L & 1]
         if tr:
             self._tr16(Vl, bf.Vg16[L], 1, R, w)

@@ -18,7 +18,7 @@ class Epilogue(C.Structure):
                 ("sn1", C.c_longlong), ("bias", C.c_void_p), ("res", C.c_void_p), ("pre", C.c_void_p),
                 ("out32", C.c_void_p), ("out16", C.c_void_p), ("out16t", C.c_void_p), ("tmd", C.c_int),
                 ("tnd", C.c_int), ("tb", C.c_longlong), ("tm0", C.c_longlong), ("tm1", C.c_longlong),
-                ("tn0", C.c_longlong), ("tn1", C.c_longlong)]
+                ("tn0", C.c_longlong), ("tn1", C.c_longlong), ("bias_m", C.c_void_p)]
 
 
 def _ptr(t):
@@ -36,27 +36,51 @@ def rowmap(ld):
     return dict(md=1, nd=1, sm0=ld, sm1=0, sn0=1, sn1=0)
 
 
-def gemm(A, B, M, N, K, *, lda=None, ldb=None, batch=1, stride_a=0, stride_b=0, alpha=1.0, bias=None, res=None,
-         pre=None, out32=None, out16=None, out16t=None, act=0, accumulate=False, omap=None, tmap=None, sb=0, tb=0):
-    """C[M, N] = alpha A[M, K] B[N, K]^T (+ bias[n] + res) on the tensor cores,
-    batched over `batch`; outputs through the index maps omap / tmap
-    (dicts of md, nd, sm0, sm1, sn0, sn1, default row-major N)."""
-    assert A.dtype == torch.bfloat16 and B.dtype == torch.bfloat16
+def _epilogue(N, alpha, bias, bias_m, res, pre, out32, out16, out16t, act, accumulate, omap, tmap, sb, tb):
     omap = omap or rowmap(N)
     ep = Epilogue()
     ep.alpha, ep.act, ep.accumulate = alpha, act, 1 if accumulate else 0
     ep.md, ep.nd, ep.sm0, ep.sm1, ep.sn0, ep.sn1 = (omap[k] for k in ("md", "nd", "sm0", "sm1", "sn0", "sn1"))
     ep.sb = sb
     ep.bias, ep.res, ep.pre, ep.out32, ep.out16 = _ptr(bias), _ptr(res), _ptr(pre), _ptr(out32), _ptr(out16)
+    ep.bias_m = _ptr(bias_m)
     if out16t is not None:
         ep.out16t = _ptr(out16t)
         ep.tmd, ep.tnd, ep.tm0, ep.tm1, ep.tn0, ep.tn1 = (tmap[k] for k in ("md", "nd", "sm0", "sm1", "sn0", "sn1"))
         ep.tb = tb
+    return ep
+
+
+def gemm(A, B, M, N, K, *, lda=None, ldb=None, batch=1, stride_a=0, stride_b=0, alpha=1.0, bias=None, bias_m=None,
+         res=None, pre=None, out32=None, out16=None, out16t=None, act=0, accumulate=False, omap=None, tmap=None, sb=0,
+         tb=0):
+    """C[M, N] = alpha A[M, K] B[N, K]^T (+ bias[n] + bias_m[m] + res) on the
+    tensor cores, batched over `batch`; outputs through the index maps omap /
+    tmap (dicts of md, nd, sm0, sm1, sn0, sn1, default row-major N)."""
+    assert A.dtype == torch.bfloat16 and B.dtype == torch.bfloat16
+    ep = _epilogue(N, alpha, bias, bias_m, res, pre, out32, out16, out16t, act, accumulate, omap, tmap, sb, tb)
     err = _err(A.device)
     rc = lib().csrst_gemm_bf16(_ptr(A), lda or K, stride_a, _ptr(B), ldb or K, stride_b, M, N, K, batch,
                                C.byref(ep), _ptr(err), C.c_void_p(torch.cuda.current_stream().cuda_stream))
     if rc:
         raise CsrstError(rc, "csrst_gemm_bf16: invalid arguments or launch failure")
+
+
+def gemm_dual(A1, B1, K1, A2, B2, K2, M, N, *, lda1=None, ldb1=None, stride_a1=0, stride_b1=0, lda2=None,
+              ldb2=None, stride_a2=0, stride_b2=0, batch=1, alpha=1.0, bias=None, bias_m=None, res=None, pre=None,
+              out32=None, out16=None, out16t=None, act=0, accumulate=False, omap=None, tmap=None, sb=0, tb=0):
+    """C = alpha (A1[M, K1] B1[N, K1]^T + A2[M, K2] B2[N, K2]^T) (+ epilogue
+    terms as in gemm) in one accumulator; each segment has its own leading
+    dimensions and batch strides (0: the operand is shared by the batch)."""
+    for t in (A1, B1, A2, B2):
+        assert t.dtype == torch.bfloat16
+    ep = _epilogue(N, alpha, bias, bias_m, res, pre, out32, out16, out16t, act, accumulate, omap, tmap, sb, tb)
+    err = _err(A1.device)
+    rc = lib().csrst_gemm_bf16_dual(_ptr(A1), lda1 or K1, stride_a1, _ptr(B1), ldb1 or K1, stride_b1, K1, _ptr(A2),
+                                    lda2 or K2, stride_a2, _ptr(B2), ldb2 or K2, stride_b2, K2, M, N, batch,
+                                    C.byref(ep), _ptr(err), C.c_void_p(torch.cuda.current_stream().cuda_stream))
+    if rc:
+        raise CsrstError(rc, "csrst_gemm_bf16_dual: invalid arguments or launch failure")
 
 
 def check_errors(device="cuda"):

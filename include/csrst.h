@@ -179,10 +179,17 @@ typedef struct {
   void *out16t;                       /* second BF16 output under its own map, or NULL */
   int tmd, tnd;
   long long tb, tm0, tm1, tn0, tn1;
+  const float *bias_m;                /* per row m, or NULL (added after bias[n]) */
 } csrst_gemm_epilogue;
 int csrst_gemm_bf16(const void *A, long long lda, long long stride_a, const void *B, long long ldb,
                     long long stride_b, int M, int N, int K, int batch, const csrst_gemm_epilogue *ep, int *err,
                     void *stream);
+/* The same over two K segments into one accumulator: C = A1 B1^T + A2 B2^T (K1, K2 multiples of 64), each
+ * segment with its own pointers, leading dimensions and batch strides (a stride may be 0: shared operand). */
+int csrst_gemm_bf16_dual(const void *A1, long long lda1, long long stride_a1, const void *B1, long long ldb1,
+                         long long stride_b1, int K1, const void *A2, long long lda2, long long stride_a2,
+                         const void *B2, long long ldb2, long long stride_b2, int K2, int M, int N, int batch,
+                         const csrst_gemm_epilogue *ep, int *err, void *stream);
 
 /* Element-wise and reduction kernels of the surrogate's training and inference
  * (device pointers; BF16 arrays as void *).  No reference counterpart. */
