@@ -54,3 +54,23 @@ def test_gemm_epilogue_and_batches(gpu_lib):
         assert np.abs(o32[z].cpu().numpy() - (2.0 + g)).max() <= 1e-4 * np.abs(g).max()
         t = o16t[z].float().cpu().numpy()
         assert np.abs(t - g.T).max() <= 1e-2 * np.abs(g).max()
+
+
+def test_gemm_dual_segments_and_row_bias(gpu_lib):
+    """C_z = A1_z B1^T + A2 B2_z^T + bias_m[m]: two K segments in one
+    accumulator, each with its own strides (B1 and A2 shared by the batch)."""
+    import torch
+    from csrst_b200.tensor import check_errors, gemm_dual
+    rng = np.random.default_rng(11)
+    M, N, K1, K2, Z = 128, 256, 64, 128, 3
+    a1, b1 = bf16(rng, (Z, M, K1)), bf16(rng, (N, K1))
+    a2, b2 = bf16(rng, (M, K2)), bf16(rng, (Z, N, K2))
+    bm = torch.from_numpy(rng.standard_normal(M).astype(np.float32))
+    out = torch.zeros(Z, M, N, device="cuda")
+    gemm_dual(a1.cuda(), b1.cuda(), K1, a2.cuda(), b2.cuda(), K2, M, N, stride_a1=M * K1, stride_b2=N * K2,
+              batch=Z, bias_m=bm.cuda(), out32=out, sb=M * N)
+    torch.cuda.synchronize()
+    check_errors()
+    for z in range(Z):
+        r = ref(a1[z], b1) + ref(a2, b2[z]) + bm.double().numpy()[:, None]
+        assert np.abs(out[z].cpu().numpy() - r).max() <= 1e-4 * np.abs(r).max()
