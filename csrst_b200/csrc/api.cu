@@ -1563,3 +1563,172 @@ int csrst_charge_diff(int order, const double *ox, const double *oy, const doubl
 }
 
 }  // extern "C"
+
+// ---- checkpoint / restart ----
+
+namespace {
+
+constexpr char kCkMagic[8] = {'C', 'S', 'R', 'S', 'T', 'C', 'K', '1'};
+constexpr char kCkEnd[8] = {'C', 'S', 'R', 'S', 'T', 'E', 'N', 'D'};
+constexpr uint32_t kCkVersion = 1;
+
+bool ck_put(FILE *f, const void *p, size_t n) { return n == 0 || std::fwrite(p, 1, n, f) == n; }
+bool ck_get(FILE *f, void *p, size_t n) { return n == 0 || std::fread(p, 1, n, f) == n; }
+
+bool ck_put_dev(FILE *f, const void *d, size_t n, std::vector<unsigned char> &buf, cudaStream_t s) {
+  if (n == 0) return true;
+  buf.resize(n);
+  if (cudaMemcpyAsync(buf.data(), d, n, cudaMemcpyDeviceToHost, s) != cudaSuccess) return false;
+  if (cudaStreamSynchronize(s) != cudaSuccess) return false;
+  return ck_put(f, buf.data(), n);
+}
+
+bool ck_get_dev(FILE *f, void *d, size_t n, std::vector<unsigned char> &buf, cudaStream_t s) {
+  if (n == 0) return true;
+  buf.resize(n);
+  if (!ck_get(f, buf.data(), n)) return false;
+  if (cudaMemcpyAsync(d, buf.data(), n, cudaMemcpyHostToDevice, s) != cudaSuccess) return false;
+  return cudaStreamSynchronize(s) == cudaSuccess;
+}
+
+// The state a time step reads and writes, as (device pointer, bytes) in file order.
+struct CkPlan {
+  std::vector<std::pair<void *, size_t>> planes, window, bunch;
+};
+
+CkPlan ck_plan(csrst_handle *h) {
+  CkPlan P;
+  const size_t ny = (size_t)h->cfg.Ny + 2;
+  if (h->fp32) {
+    for (float *p : {h->Exf, h->Eyf, h->Hxf, h->Hyf}) P.planes.push_back({p, (size_t)h->pitch32 * ny * 4});
+  } else {
+    for (double *p : {h->Ex, h->Ey, h->Hx, h->Hy}) P.planes.push_back({p, (size_t)h->pitch * ny * 8});
+  }
+  const size_t wp = (size_t)h->wpitch * (h->L1 + 2);
+  P.window.push_back({h->ws, sizeof(WinState)});
+  P.window.push_back({h->fp32 ? (void *)h->winf : (void *)h->win, 6 * wp * (h->fp32 ? 4 : 8)});
+  P.window.push_back({h->acc, 2 * (size_t)h->L0 * h->L1 * sizeof(unsigned long long)});
+  const size_t n = (size_t)h->n;
+  if (h->fp32) {
+    P.bunch.push_back({h->b32.cell, n * 4});
+    for (float *p : {h->b32.ox, h->b32.oy, h->b32.dpx, h->b32.dpy, h->b32.q}) P.bunch.push_back({p, n * 4});
+  } else {
+    for (double *p : {h->x, h->y, h->px, h->py, h->q, h->ox, h->oy}) P.bunch.push_back({p, n * 8});
+  }
+  return P;
+}
+
+}  // namespace
+
+extern "C" {
+
+int csrst_get_num_particles(csrst_handle *h, long long *n) {
+  if (!h || !n) return CSRST_E_ARG;
+  *n = h->n;
+  return CSRST_OK;
+}
+
+int csrst_checkpoint_write(csrst_handle *h, const char *path, long long step, double time) {
+  int rc = need_bunch(h);
+  if (rc) return rc;
+  if (!path) return fail(h, CSRST_E_ARG, "checkpoint: no path");
+  CK(cudaStreamSynchronize(h->s));
+  if ((rc = check_err(h))) return rc;  // a run that stopped on a device error is not saved
+  FILE *f = std::fopen(path, "wb");
+  if (!f) return fail(h, CSRST_E_IO, std::string("checkpoint: cannot open ") + path);
+  std::vector<unsigned char> buf;
+  const CkPlan P = ck_plan(h);
+  const uint32_t head[2] = {kCkVersion, h->fp32 ? 1u : 0u};
+  const int32_t win[3] = {h->L0, h->L1, h->wpitch};
+  const uint8_t flags[4] = {(uint8_t)h->pending, (uint8_t)h->fresh, (uint8_t)h->acc_fresh[0],
+                            (uint8_t)h->acc_fresh[1]};
+  const int32_t bb = (int32_t)h->bb;
+  const double mom[2] = {h->P0, h->P1};
+  bool ok = ck_put(f, kCkMagic, 8) && ck_put(f, head, sizeof(head)) && ck_put(f, &h->cfg, sizeof(csrst_config)) &&
+            ck_put(f, &step, 8) && ck_put(f, &time, 8);
+  for (auto &pl : P.planes) ok = ok && ck_put_dev(f, pl.first, pl.second, buf, h->s);
+  ok = ok && ck_put(f, win, sizeof(win)) && ck_put(f, &h->acc_scale, 8);
+  for (auto &pl : P.window) ok = ok && ck_put_dev(f, pl.first, pl.second, buf, h->s);
+  ok = ok && ck_put(f, &h->n, 8) && ck_put(f, flags, sizeof(flags)) && ck_put(f, &bb, 4) && ck_put(f, mom, 16);
+  for (auto &pl : P.bunch) ok = ok && ck_put_dev(f, pl.first, pl.second, buf, h->s);
+  ok = ok && ck_put(f, kCkEnd, 8);
+  ok = (std::fclose(f) == 0) && ok;
+  return ok ? CSRST_OK : fail(h, CSRST_E_IO, std::string("checkpoint: writing ") + path + " failed");
+}
+
+int csrst_checkpoint_read(csrst_handle *h, const char *path, long long *step, double *time) {
+  if (!h || !path) return CSRST_E_ARG;
+  FILE *f = std::fopen(path, "rb");
+  if (!f) return fail(h, CSRST_E_IO, std::string("restart: cannot open ") + path);
+  auto bad = [&](int code, const std::string &why) {
+    std::fclose(f);
+    return fail(h, code, "restart: " + why);
+  };
+  char magic[8];
+  uint32_t head[2];
+  csrst_config cfg{};
+  long long st = 0;
+  double tm = 0;
+  if (!ck_get(f, magic, 8) || std::memcmp(magic, kCkMagic, 8) != 0) return bad(CSRST_E_IO, "not a checkpoint file");
+  if (!ck_get(f, head, sizeof(head)) || head[0] != kCkVersion) return bad(CSRST_E_IO, "unknown checkpoint version");
+  if (!ck_get(f, &cfg, sizeof(cfg)) || std::memcmp(&cfg, &h->cfg, sizeof(cfg)) != 0 || (head[1] != 0) != h->fp32)
+    return bad(CSRST_E_ARG, "the checkpoint was written for another configuration");
+  if (!ck_get(f, &st, 8) || !ck_get(f, &tm, 8)) return bad(CSRST_E_IO, "truncated file");
+  CK(cudaStreamSynchronize(h->s));
+  free_particles(h);  // window, bunch and the captured step go; the handle is rebuilt from the file
+  std::vector<unsigned char> buf;
+  CkPlan P = ck_plan(h);
+  for (auto &pl : P.planes)
+    if (!ck_get_dev(f, pl.first, pl.second, buf, h->s)) return bad(CSRST_E_IO, "truncated file (static fields)");
+  int32_t win[3];
+  if (!ck_get(f, win, sizeof(win)) || !ck_get(f, &h->acc_scale, 8)) return bad(CSRST_E_IO, "truncated file");
+  if (win[0] <= 0 || win[1] <= 0 || win[2] != win[0] + 2) return bad(CSRST_E_IO, "corrupt window size");
+  h->L0 = win[0]; h->L1 = win[1]; h->wpitch = win[2];
+  const size_t wp = (size_t)h->wpitch * (h->L1 + 2);
+  const size_t es = h->fp32 ? 4 : 8;
+  if (h->fp32) {
+    CK(cudaMalloc(&h->winf, 6 * wp * es));
+    CK(cudaMalloc(&h->scratchf, 6 * wp * es));
+  } else {
+    CK(cudaMalloc(&h->win, 6 * wp * es));
+    CK(cudaMalloc(&h->scratch, 6 * wp * es));
+  }
+  CK(cudaMalloc(&h->acc, 2 * (size_t)h->L0 * h->L1 * sizeof(unsigned long long)));
+  P = ck_plan(h);
+  for (auto &pl : P.window)
+    if (!ck_get_dev(f, pl.first, pl.second, buf, h->s)) return bad(CSRST_E_IO, "truncated file (window)");
+  long long n = 0;
+  uint8_t flags[4];
+  int32_t bb = 0;
+  double mom[2];
+  if (!ck_get(f, &n, 8) || n <= 0 || !ck_get(f, flags, 4) || !ck_get(f, &bb, 4) || !ck_get(f, mom, 16))
+    return bad(CSRST_E_IO, "truncated file (bunch)");
+  const size_t nb = (size_t)n * 8;
+  h->n = n;
+  if (h->fp32) {
+    Bunch32 &b = h->b32;
+    b.n = n;
+    CK(cudaMalloc(&b.cell, (size_t)n * sizeof(int)));
+    for (float **p : {&b.ox, &b.oy, &b.dpx, &b.dpy, &b.q}) CK(cudaMalloc(p, (size_t)n * sizeof(float)));
+    CK(cudaMalloc(&h->d64, 4 * nb));
+  } else {
+    for (double **p : {&h->x, &h->y, &h->px, &h->py, &h->q, &h->ox, &h->oy}) CK(cudaMalloc(p, nb));
+  }
+  P = ck_plan(h);
+  for (auto &pl : P.bunch)
+    if (!ck_get_dev(f, pl.first, pl.second, buf, h->s)) return bad(CSRST_E_IO, "truncated file (bunch)");
+  if (!ck_get(f, magic, 8) || std::memcmp(magic, kCkEnd, 8) != 0) return bad(CSRST_E_IO, "corrupt end of file");
+  std::fclose(f);
+  h->pending = flags[0] != 0;
+  h->fresh = flags[1] != 0;
+  h->acc_fresh[0] = flags[2] != 0;
+  h->acc_fresh[1] = flags[3] != 0;
+  h->bb = (BBoxState)bb;
+  h->P0 = mom[0];
+  h->P1 = mom[1];
+  if (step) *step = st;
+  if (time) *time = tm;
+  return CSRST_OK;
+}
+
+}  // extern "C"

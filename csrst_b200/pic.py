@@ -156,6 +156,23 @@ class Simulation:
     def stream(self):
         return lib().csrst_stream(self.h)
 
+    # -- checkpoint / restart (the restart dump of LoadH5Part, LoadH5Part.cpp:60-321) --
+    def checkpoint(self, path, step=0, time=0.0):
+        """Writes everything a time step reads (fields, window, bunch) with the
+        step count and time; a handle of the same configuration restored from
+        the file continues bit for bit."""
+        self._ck(lib().csrst_checkpoint_write(self.h, str(path).encode(), int(step), float(time)))
+
+    def restore(self, path):
+        """Replaces the state with a checkpoint written for this configuration;
+        returns (step, time)."""
+        st, tm = C.c_longlong(), C.c_double()
+        self._ck(lib().csrst_checkpoint_read(self.h, str(path).encode(), C.byref(st), C.byref(tm)))
+        n = C.c_longlong()
+        self._ck(lib().csrst_get_num_particles(self.h, C.byref(n)))
+        self.n = n.value
+        return st.value, tm.value
+
     def moments(self):
         out = np.zeros(18)
         self._ck(lib().csrst_diag_moments(self.h, ptr(out)))

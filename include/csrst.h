@@ -34,6 +34,7 @@ extern "C" {
 #define CSRST_E_WINDOW_MOVE (-6)   /* window would move by other than 0/1 cell in x, -1..1 in y */
 #define CSRST_E_CROSSINGS (-7)     /* a particle crossed more cell borders than one push allows */
 #define CSRST_E_WINDOW_WALL (-8)   /* window or its ring touches a non-inside cell */
+#define CSRST_E_IO (-9)            /* checkpoint file could not be written or read */
 
 typedef struct csrst_handle csrst_handle;
 
@@ -190,6 +191,18 @@ int csrst_gemm_bf16_dual(const void *A1, long long lda1, long long stride_a1, co
                          long long stride_b1, int K1, const void *A2, long long lda2, long long stride_a2,
                          const void *B2, long long ldb2, long long stride_b2, int K2, int M, int N, int batch,
                          const csrst_gemm_epilogue *ep, int *err, void *stream);
+
+/* Checkpoint and restart (the restart dump read by LoadH5Part, src/Commands/LoadH5Part.cpp:60-321:
+ * run attributes, fields, bunch R / oldR / P / Q), as a dependency-free binary file that holds
+ * everything a time step reads: the configuration, step and time, the static-mesh planes, the
+ * moving window (position, size, bookkeeping, its fields and fixed-point current) and the bunch in
+ * the handle's own form (FP64 arrays, or the FP32 mode's offsets and momentum deviations).  A run
+ * restored into a handle created with the same configuration continues bit for bit.  Files are
+ * host-endian; the layout is versioned. */
+int csrst_checkpoint_write(csrst_handle *h, const char *path, long long step, double time);
+/* Particles of the loaded (or restored) bunch. */
+int csrst_get_num_particles(csrst_handle *h, long long *n);
+int csrst_checkpoint_read(csrst_handle *h, const char *path, long long *step, double *time);
 
 /* Element-wise and reduction kernels of the surrogate's training and inference
  * (device pointers; BF16 arrays as void *).  No reference counterpart. */

@@ -59,6 +59,17 @@ class Simulation {
   size_t size() const { return n_; }
   void step(int n) { check(csrst_step(h_, n), h_); }
   void sync() { check(csrst_sync(h_), h_); }
+  // Restart dump (LoadH5Part, src/Commands/LoadH5Part.cpp:60-321): everything a step reads, so
+  // that a Simulation of the same configuration restored from the file continues bit for bit.
+  void checkpoint(const std::string &path, long long step, double time) {
+    check(csrst_checkpoint_write(h_, path.c_str(), step, time), h_);
+  }
+  void restore(const std::string &path, long long &step, double &time) {
+    check(csrst_checkpoint_read(h_, path.c_str(), &step, &time), h_);
+    long long n = 0;
+    check(csrst_get_num_particles(h_, &n), h_);
+    n_ = (size_t)n;
+  }
 
  private:
   csrst_config cfg_;
