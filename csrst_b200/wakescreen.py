@@ -348,28 +348,40 @@ def production_config(nx=16384, ny=2048, h=2.5e-6, width=5e-3, cfl=0.4):
     return bend_config(nx, ny, h, C5_R, width, C5_GAMMA, shape_order=1, cfl=cfl)
 
 
-def production_run(case, n=32_000_000, steps=40_000, stations=32, cfg=None, log=print):
+def production_run(case, n=32_000_000, steps=40_000, stations=32, cfg=None, log=print, checkpoint=None,
+                   resume=None):
     """The production run for one profile: quiet-start bunch of n particles
     50 cells plus 6 sigma_s from the mesh start, FP32 mode, stepped as a
     one-member ensemble (the batched path, one CUDA graph per step).  Records
     the wake on the 256 bins every steps/stations steps; returns the wakes and
-    the timing (device time of the stepping; the station reads excluded)."""
+    the timing (device time of the stepping; the station reads excluded).
+    checkpoint: a file rewritten at every station; resume: a checkpoint of the
+    same run to continue from (its stations before the saved step are left
+    out of the returned wakes)."""
     from scipy.special import ndtri
     from . import wakeset
     from .pic import Ensemble, Simulation
     cfg = cfg or production_config()
     sim = Simulation(cfg, fp32=True)
-    hx = sim.info()["hx"]
-    g = np.random.Generator(np.random.Philox(case.seed))
-    x = 50 * hx + 6 * case.sigma_s + wakeset.quiet_offsets(case, n)
-    q = np.clip(np.mod(g.uniform() + wakeset.GOLDEN * np.arange(n), 1.0), 0.5 / n, 1 - 0.5 / n)
-    y = 0.5 * cfg.width + case.sigma_s / 2.5 * ndtri(q)
-    gam = case.gamma * (1.0 + 1e-4 * g.standard_normal(n))
-    sim.load(x, y, np.sqrt(gam * gam - 1.0), np.zeros(n), np.full(n, wakeset.CHARGE / n))
-    del x, y, gam, q
-    t = time.perf_counter()
-    rep = sim.initial_fields()
-    t_poisson = time.perf_counter() - t
+    first, rep, t_poisson = 0, {"solves": None}, 0.0
+    if resume:  # the file holds fields, window and bunch: nothing to load or solve
+        done, _ = sim.restore(resume)
+        first = int(done) // (steps // stations)
+        n = sim.n
+        if log:
+            log("production: resumed at step %d" % done)
+    else:
+        hx = sim.info()["hx"]
+        g = np.random.Generator(np.random.Philox(case.seed))
+        x = 50 * hx + 6 * case.sigma_s + wakeset.quiet_offsets(case, n)
+        q = np.clip(np.mod(g.uniform() + wakeset.GOLDEN * np.arange(n), 1.0), 0.5 / n, 1 - 0.5 / n)
+        y = 0.5 * cfg.width + case.sigma_s / 2.5 * ndtri(q)
+        gam = case.gamma * (1.0 + 1e-4 * g.standard_normal(n))
+        sim.load(x, y, np.sqrt(gam * gam - 1.0), np.zeros(n), np.full(n, wakeset.CHARGE / n))
+        del x, y, gam, q
+        t = time.perf_counter()
+        rep = sim.initial_fields()
+        t_poisson = time.perf_counter() - t
     ens = Ensemble([sim])
     reader = wakeset._WakeReader([sim], [case.sigma_s])
     every = steps // stations
@@ -377,7 +389,7 @@ def production_run(case, n=32_000_000, steps=40_000, stations=32, cfg=None, log=
     st = torch.cuda.ExternalStream(ens.stream())
     W, dev_ms = [], 0.0
     t = time.perf_counter()
-    for j in range(stations):
+    for j in range(first, stations):
         a.record(st)
         ens.step(every)
         b.record(st)
@@ -385,15 +397,18 @@ def production_run(case, n=32_000_000, steps=40_000, stations=32, cfg=None, log=
         dev_ms += a.elapsed_time(b)
         w, _ = reader.read()
         W.append(w[0])
+        if checkpoint:
+            sim.checkpoint(checkpoint, step=(j + 1) * every, time=(j + 1) * every * sim.info()["dt"])
         if log and (j % 8 == 7 or j == stations - 1):
-            log("production: %d steps, %.2f ms/step" % ((j + 1) * every, dev_ms / ((j + 1) * every)))
+            log("production: %d steps, %.2f ms/step" % ((j + 1) * every, dev_ms / ((j + 1 - first) * every)))
     wall = time.perf_counter() - t
     mom = sim.moments()
     ens.close()
     sim.close()
-    return np.array(W).T, {"particles": n, "steps": every * stations, "cells": cfg.Nx * cfg.Ny,
-                           "ms_per_step": dev_ms / (every * stations), "wall_s": wall,
-                           "particle_steps_per_s": n * every * stations / (dev_ms / 1e3),
+    ran = every * (stations - first)
+    return np.array(W).T, {"particles": n, "steps": ran, "first_step": first * every, "cells": cfg.Nx * cfg.Ny,
+                           "ms_per_step": dev_ms / ran, "wall_s": wall,
+                           "particle_steps_per_s": n * ran / (dev_ms / 1e3),
                            "poisson_s": t_poisson, "poisson": rep["solves"], "final_moments": mom[:8].tolist()}
 
 
@@ -489,6 +504,8 @@ if __name__ == "__main__":
     ap.add_argument("cmd", choices=["train", "evaluate", "time", "study", "production"])
     ap.add_argument("--variant", type=int, default=0, help="production variant index (production)")
     ap.add_argument("--particles", type=int, default=32_000_000, help="production bunch size (production)")
+    ap.add_argument("--checkpoint", default=None, help="checkpoint file rewritten at every station (production)")
+    ap.add_argument("--resume", default=None, help="checkpoint to continue from (production)")
     ap.add_argument("--models", type=int, default=4, help="networks in the ensemble (study)")
     ap.add_argument("--variants", type=int, default=100000, help="production variants to screen (study)")
     ap.add_argument("--json", default=None, help="where study writes its record")
@@ -503,7 +520,7 @@ if __name__ == "__main__":
     a = ap.parse_args()
     if a.cmd == "production":  # the 16384 x 2048 run of one screened variant (no data needed)
         v = c5_variants(a.variant + 1)[a.variant]
-        W, rec = production_run(v, n=a.particles, steps=a.steps)
+        W, rec = production_run(v, n=a.particles, steps=a.steps, checkpoint=a.checkpoint, resume=a.resume)
         rec["variant"], rec["variant_index"] = v.dict(), a.variant
         if a.json:
             with open(a.json, "w") as f:
