@@ -1045,6 +1045,25 @@ int csrst_diag_wake(csrst_handle *h, double *out, int n) {
   return check_err(h);
 }
 
+int csrst_diag_field_energy(csrst_handle *h, int with_window, double *out2) {
+  if (!h || !out2) return CSRST_E_ARG;
+  if (with_window) {
+    const int rc = need_bunch(h);
+    if (rc) return rc;
+  }
+  const double area = h->b.hr0 * h->b.hr1;
+  if (h->fp32)
+    launch_field_energy(h->Exf, h->Eyf, h->Hxf, h->Hyf, h->pitch32, h->cfg.Nx, h->cfg.Ny, h->winf, h->wpitch, h->ws,
+                        with_window, area, h->dscratch, h->dout, h->s);
+  else
+    launch_field_energy(h->Ex, h->Ey, h->Hx, h->Hy, h->pitch, h->cfg.Nx, h->cfg.Ny, h->win, h->wpitch, h->ws,
+                        with_window, area, h->dscratch, h->dout, h->s);
+  CK(cudaMemcpyAsync(out2, h->dout, 2 * sizeof(double), cudaMemcpyDeviceToHost, h->s));
+  CK(cudaStreamSynchronize(h->s));
+  CK(cudaGetLastError());
+  return CSRST_OK;
+}
+
 int csrst_diag_wake_async(csrst_handle *h, double *out_dev, int n, double *meta_dev) {
   int rc = need_bunch(h);
   if (rc) return rc;

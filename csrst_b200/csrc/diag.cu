@@ -75,13 +75,15 @@ __global__ void __launch_bounds__(256) k_mom1(const double *x, const double *y, 
 // with 1e-4 energy spread; here px' is centred on |<p>| first and the
 // identity sum(px'^2) - N m^2 = sum((px'-m)^2) + 2 m sum(px'-m) restores the
 // same quantity without the cancellation.  Sums: q0^2, q2^2, (q1-m)^2, q3^2,
-// q0 (q1-m), q0, q2 q3, (q1-m).
+// q0 (q1-m), q0, q2 q3, (q1-m), and for the dispersion terms q2 (q1-m), q2,
+// q3 (q1-m), q3 (the reference's moments(2,1) and (3,1) pair y' and py' with
+// the uncentred px' = (q1-m) + m).
 __global__ void __launch_bounds__(256) k_mom2(const double *x, const double *y, const double *px,
                                               const double *py, long long n, double half,
                                               int pending, const double *mean, double *part) {
   const double aR0 = mean[0], aR1 = mean[1], aP0 = mean[2], aP1 = mean[3];
   const double am = sqrt(aP0 * aP0 + aP1 * aP1), cph = aP0 / am, sph = aP1 / am;
-  double v[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  double v[12] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x) {
     double a = x[i], b = y[i];
@@ -94,8 +96,9 @@ __global__ void __launch_bounds__(256) k_mom2(const double *x, const double *y, 
     const double q2 = -sph * d0 + cph * d2;
     v[0] += q0 * q0; v[1] += q2 * q2; v[2] += q1 * q1; v[3] += q3 * q3;
     v[4] += q0 * q1; v[5] += q0; v[6] += q2 * q3; v[7] += q1;
+    v[8] += q2 * q1; v[9] += q2; v[10] += q3 * q1; v[11] += q3;
   }
-  block_sum<8>(v, part + blockIdx.x * 10);
+  block_sum<12>(v, part + blockIdx.x * 12);
 }
 
 // Final reduction and the derived quantities; out[18] as the oracle's layout:
@@ -115,9 +118,9 @@ __global__ void k_mom_final1(const double *part, int nb, long long n, double *me
 
 __global__ void k_mom_final2(const double *part, int nb, long long n, const double *mean, double *out) {
   if (threadIdx.x != 0) return;
-  double M[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  double M[12] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
   for (int b = 0; b < nb; ++b)
-    for (int k = 0; k < 8; ++k) M[k] += part[b * 10 + k];
+    for (int k = 0; k < 12; ++k) M[k] += part[b * 12 + k];
   const double N = (double)n;
   const double am = sqrt(mean[2] * mean[2] + mean[3] * mean[3]);
   const double rsq[2] = {M[0], M[1]};
@@ -134,7 +137,8 @@ __global__ void k_mom_final2(const double *part, int nb, long long n, const doub
   const double ek = (mean[4] - 1.0) * m0;
   out[14] = ek;
   out[15] = out[6] * sqrt(ek * (ek + 2. * m0) / (1. + ek * (ek + 2. * m0) / (m0 * m0)));
-  out[16] = 0.0; out[17] = 0.0;
+  out[16] = (M[8] + am * M[9]) / N;   // Dy  = moments(2, 1) / N (PartBunch.cpp:643)
+  out[17] = (M[10] + am * M[11]) / N;  // DDy = moments(3, 1) / N (PartBunch.cpp:644)
 }
 
 // E_s = cos(p) Ex + sin(p) Ey sampled at i = 2 .. L0-3 along the mean
@@ -192,6 +196,48 @@ __global__ void k_charge_diff(const double *ox, const double *oy, const double *
   }
 }
 
+// Field energy sums (CalcEnergyCommand::execute, CalcEnergy.cpp:41-120): the
+// sum of Ex^2 + Ey^2 and of (Hzx + Hzy)^2 over the static mesh's Nx x Ny
+// points and, with the window, over the window's L0 x L1 points, which replace
+// the static points they cover.  One partial pair per block, summed in order.
+template <class T>
+__global__ void __launch_bounds__(256) k_energy(const T *Ex, const T *Ey, const T *Hx, const T *Hy, int pitch,
+                                                int Nx, int Ny, const T *win, int wpitch, const WinState *ws,
+                                                int with_window, double *part) {
+  double v[2] = {0.0, 0.0};
+  int P0 = 0, P1 = 0, L0 = 0, L1 = 0;
+  if (with_window) { P0 = ws->P0; P1 = ws->P1; L0 = ws->L0; L1 = ws->L1; }
+  const long long st = (long long)gridDim.x * blockDim.x;
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < (long long)Nx * Ny; k += st) {
+    const int i = (int)(k % Nx), j = (int)(k / Nx);
+    if (with_window && i >= P0 && i < P0 + L0 && j >= P1 && j < P1 + L1) continue;
+    const size_t o = (size_t)(j + 1) * pitch + (i + 1);
+    const double ex = (double)Ex[o], ey = (double)Ey[o], hz = (double)Hx[o] + (double)Hy[o];
+    v[0] += ex * ex + ey * ey;
+    v[1] += hz * hz;
+  }
+  if (with_window) {
+    const size_t wp = (size_t)wpitch * (L1 + 2);
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < (long long)L0 * L1; k += st) {
+      const int i = (int)(k % L0), j = (int)(k / L0);
+      const size_t o = (size_t)(j + 1) * wpitch + (i + 1);
+      const double ex = (double)win[o], ey = (double)win[wp + o];
+      const double hz = (double)win[2 * wp + o] + (double)win[3 * wp + o];
+      v[0] += ex * ex + ey * ey;
+      v[1] += hz * hz;
+    }
+  }
+  block_sum<2>(v, part + blockIdx.x * 2);
+}
+
+__global__ void k_energy_final(const double *part, int nb, double area, double *out) {
+  if (threadIdx.x != 0) return;
+  double s0 = 0.0, s1 = 0.0;
+  for (int b = 0; b < nb; ++b) { s0 += part[2 * b]; s1 += part[2 * b + 1]; }
+  out[0] = s0 * area;
+  out[1] = s1 * area;
+}
+
 // --- host launchers -----------------------------------------------------------
 
 void launch_moments(const double *x, const double *y, const double *px, const double *py, long long n,
@@ -202,7 +248,21 @@ void launch_moments(const double *x, const double *y, const double *px, const do
   k_mom_final2<<<1, 32, 0, s>>>(part, kDiagBlocks, n, mean, out);
 }
 
-size_t moments_scratch_doubles() { return (size_t)kDiagBlocks * 10; }
+size_t moments_scratch_doubles() { return (size_t)kDiagBlocks * 12; }
+
+template <class T>
+void launch_field_energy(const T *Ex, const T *Ey, const T *Hx, const T *Hy, int pitch, int Nx, int Ny,
+                         const T *win, int wpitch, const WinState *ws, int with_window, double area, double *part,
+                         double *out, cudaStream_t s) {
+  k_energy<T><<<kDiagBlocks, 256, 0, s>>>(Ex, Ey, Hx, Hy, pitch, Nx, Ny, win, wpitch, ws, with_window, part);
+  k_energy_final<<<1, 32, 0, s>>>(part, kDiagBlocks, area, out);
+}
+template void launch_field_energy<double>(const double *, const double *, const double *, const double *, int, int,
+                                          int, const double *, int, const WinState *, int, double, double *,
+                                          double *, cudaStream_t);
+template void launch_field_energy<float>(const float *, const float *, const float *, const float *, int, int, int,
+                                         const float *, int, const WinState *, int, double, double *, double *,
+                                         cudaStream_t);
 
 template <class T>
 void launch_wake(const WinState *ws, const T *mEx, const T *mEy, int wpitch, int L0, double h0, double h1,

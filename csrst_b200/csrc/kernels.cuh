@@ -137,6 +137,13 @@ int build_geometry(const BendDev &b, uint8_t *d_mask, CutCellDev **d_cells, int 
 // diag.cu
 void launch_moments(const double *x, const double *y, const double *px, const double *py, long long n,
                     double half, int pending, double *part, double *mean, double *out, cudaStream_t s);
+// Field energy sums over the static mesh (and the window, replacing the points
+// it covers): out2 = {sum(Ex^2 + Ey^2), sum((Hzx + Hzy)^2)} x area; part holds
+// 2 doubles per block of the moments grid.
+template <class T>
+void launch_field_energy(const T *Ex, const T *Ey, const T *Hx, const T *Hy, int pitch, int Nx, int Ny,
+                         const T *win, int wpitch, const WinState *ws, int with_window, double area, double *part,
+                         double *out, cudaStream_t s);
 size_t moments_scratch_doubles();
 template <class T>
 void launch_wake(const WinState *ws, const T *mEx, const T *mEy, int wpitch, int L0, double h0, double h1,

@@ -178,6 +178,13 @@ class Simulation:
         self._ck(lib().csrst_diag_moments(self.h, ptr(out)))
         return out
 
+    def field_energy(self, with_window=True):
+        """{sum(Ex^2 + Ey^2), sum((Hzx + Hzy)^2)} x cell area over the static
+        mesh, the window replacing the points it covers (CalcEnergy.cpp:41-120)."""
+        out = np.zeros(2)
+        self._ck(lib().csrst_diag_field_energy(self.h, 1 if with_window else 0, ptr(out)))
+        return out
+
     def wake(self):
         w, _, _ = self.window()
         out = np.zeros(max(w[2] - 4, 0))

@@ -229,8 +229,13 @@ int csrst_nn_spectral_pack(const float *wr, const float *wi, int modes, int ch, 
 int csrst_nn_spectral_unpack(const float *dmk, int modes, int ch, float *dwr, float *dwi, void *stream);
 
 /* Beam moments (PartBunch::calcBeamParameters, PartBunch.cpp:584-657):
- * out18 = rmean2, pmean2, rrms2, prms2, eps_norm2, rmin2, rmax2, Ekin[MeV], dE, 0, 0. */
+ * out18 = rmean2, pmean2, rrms2, prms2, eps_norm2, rmin2, rmax2, Ekin[MeV], dE, Dy, DDy. */
 int csrst_diag_moments(csrst_handle *h, double *out18);
+/* Field energy sums (CalcEnergyCommand, src/Commands/CalcEnergy.cpp:41-120): out2 = {sum of
+ * Ex^2 + Ey^2, sum of (Hzx + Hzy)^2} over the static mesh's points times the cell area, with the
+ * window's points replacing the ones they cover when with_window is set (needs a loaded bunch).
+ * The reference's energy is 0.25 eps0 (E_now + E_last) + 0.5 mu0 H (csrst_b200.diagnostics). */
+int csrst_diag_field_energy(csrst_handle *h, int with_window, double *out2);
 /* Longitudinal field along the bunch axis at window columns 2 .. L0-3
  * (IntegrateElongCommand::execute, IntegrateElong.cpp:38-89); NaN where the
  * sample lies outside the window.  n must be L0 - 4. */

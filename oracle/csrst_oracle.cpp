@@ -1676,8 +1676,35 @@ void orc_wake(void *h, double r0, double r1, double p0, double p1, double *out) 
   }
 }
 
+// CalcEnergyCommand::execute (src/Commands/CalcEnergy.cpp:41-120) before its time
+// averaging, in the reference's order: every static point, plus every mini-mesh
+// point, minus the static points the mini mesh covers; times the cell area.
+void orc_field_energy(void *h, int with_window, double *out2) {
+  Sim &s = *(Sim *)h;
+  double ee = 0.0, hh = 0.0;
+  auto add = [&](const Grid &ex, const Grid &ey, const Grid &hx, const Grid &hy, int i, int j, double sg) {
+    const double a = ex.at(i, j), b = ey.at(i, j), c = hx.at(i, j) + hy.at(i, j);
+    ee += sg * (a * a + b * b);
+    hh += sg * c * c;
+  };
+  for (int j = 0; j < s.b.Ny; ++j)
+    for (int i = 0; i < s.b.Nx; ++i) add(s.Ex, s.Ey, s.Hx, s.Hy, i, j, 1.0);
+  if (with_window) {
+    for (int j = 0; j < s.L1; ++j)
+      for (int i = 0; i < s.L0; ++i) add(s.mEx, s.mEy, s.mHx, s.mHy, i, j, 1.0);
+    const int i0 = std::max(0, s.P0), i1 = std::min(s.b.Nx - 1, s.P0 + s.L0 - 1);
+    const int j0 = std::max(0, s.P1), j1 = std::min(s.b.Ny - 1, s.P1 + s.L1 - 1);
+    for (int j = j0; j <= j1; ++j)
+      for (int i = i0; i <= i1; ++i) add(s.Ex, s.Ey, s.Hx, s.Hy, i, j, -1.0);
+  }
+  const double area = s.b.hr0 * s.b.hr1;
+  out2[0] = ee * area;
+  out2[1] = hh * area;
+}
+
 // PartBunch::calcBeamParameters / calcMoments (PartBunch.cpp:584-767) with
-// long-double Kahan sums.  out: rmean2, pmean2, rrms2, prms2, eps2, rmin2, rmax2, Ekin, dE.
+// long-double Kahan sums.  out: rmean2, pmean2, rrms2, prms2, eps2, rmin2, rmax2, Ekin, dE,
+// Dy, DDy (moments (2, 1) and (3, 1) over N, PartBunch.cpp:643-644).
 void orc_moments(void *h, double *out) {
   Sim &s = *(Sim *)h;
   const size_t n = s.x.size();
@@ -1737,7 +1764,8 @@ void orc_moments(void *h, double *out) {
   double ek = (gam - 1.0) * m0;
   double dE = prms[0] * std::sqrt(ek * (ek + 2. * m0) / (1. + ek * (ek + 2. * m0) / (m0 * m0)));
   double o[18] = {rmean[0], rmean[1], pmean[0], pmean[1], rrms[0], rrms[1], prms[0], prms[1],
-                  eps[0], eps[1], lim[0], lim[1], lim[2], lim[3], ek, dE, 0, 0};
+                  eps[0], eps[1], lim[0], lim[1], lim[2], lim[3], ek, dE,
+                  (double)(M[2 * 4 + 1] / (long double)N), (double)(M[3 * 4 + 1] / (long double)N)};
   std::memcpy(out, o, sizeof(o));
 }
 

@@ -71,6 +71,7 @@ def lib():
         L.orc_step.argtypes = [C.c_void_p, C.c_int]
         L.orc_wake.argtypes = [C.c_void_p] + [C.c_double] * 4 + [D]
         L.orc_moments.argtypes = [C.c_void_p, D]
+        L.orc_field_energy.argtypes = [C.c_void_p, C.c_int, D]
         L.orc_initial_fields.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_int, D]
         _LIB = L
     return _LIB
@@ -233,6 +234,11 @@ class Sim:
     def moments(self):
         out = np.zeros(18)
         lib().orc_moments(self.h, _p(out))
+        return out
+
+    def field_energy(self, with_window=True):
+        out = np.zeros(2)
+        lib().orc_field_energy(self.h, 1 if with_window else 0, _p(out))
         return out
 
     def wake(self, rmean, pmean):

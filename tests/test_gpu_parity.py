@@ -221,6 +221,14 @@ def test_moments_and_wake(gpu_lib, oracle):
                       (10, 12, 1e-9), (12, 14, 1e-9), (14, 15, 1e-9), (15, 16, 1e-7)):
         scale = np.abs(mo[a:b]).max()
         assert np.abs(mg[a:b] - mo[a:b]).max() <= tol * scale, (a, mg[a:b], mo[a:b])
+    # dispersion terms Dy, DDy (PartBunch.cpp:643-644): the reference pairs y' and py'
+    # with the uncentred px' ~ |<p>|; the GPU with the centred one plus |<p>| sum(y')
+    scale = np.abs(mo[16:18]).max()
+    assert scale > 0 and np.abs(mg[16:18] - mo[16:18]).max() <= 1e-6 * scale, (mg[16:18], mo[16:18])
+    # field energy sums (CalcEnergy.cpp:41-120), static mesh alone and with the window
+    for win in (False, True):
+        eg, eo = g.field_energy(win), o.field_energy(win)
+        assert np.all(eo > 0) and np.all(np.abs(eg - eo) <= 1e-12 * np.abs(eo)), (win, eg, eo)
     wg = g.wake()
     wo = o.wake(mo[:2], mo[2:4])
     assert np.array_equal(np.isnan(wg), np.isnan(wo))
