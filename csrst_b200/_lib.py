@@ -99,6 +99,7 @@ def lib():
         "csrst_diag_wake": ([P, D, C.c_int], C.c_int),
         "csrst_diag_wake_async": ([P, P, C.c_int, P], C.c_int),
         "csrst_diag_field_energy": ([P, C.c_int, D], C.c_int),
+        "csrst_diag_line_fields": ([P, C.c_int, D, C.c_int, C.POINTER(C.c_int)], C.c_int),
         "csrst_get_num_particles": ([P, C.POINTER(C.c_longlong)], C.c_int),
         "csrst_checkpoint_write": ([P, C.c_char_p, C.c_longlong, C.c_double], C.c_int),
         "csrst_checkpoint_read": ([P, C.c_char_p, C.POINTER(C.c_longlong), C.POINTER(C.c_double)], C.c_int),

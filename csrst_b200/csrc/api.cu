@@ -1045,6 +1045,41 @@ int csrst_diag_wake(csrst_handle *h, double *out, int n) {
   return check_err(h);
 }
 
+int csrst_diag_line_fields(csrst_handle *h, int with_current, double *out, int cap, int *count) {
+  int rc = need_bunch(h);
+  if (rc) return rc;
+  if (!count) return fail(h, CSRST_E_ARG, "line fields: count pointer missing");
+  const double *x, *y, *px, *py;
+  int pend = 0;
+  bunch64(h, &x, &y, &px, &py, &pend);
+  launch_moments(x, y, px, py, h->n, h->half, pend, h->dscratch, h->dmean, h->dout, h->s);
+  double m[18];
+  CK(cudaMemcpyAsync(m, h->dout, sizeof(m), cudaMemcpyDeviceToHost, h->s));
+  CK(cudaStreamSynchronize(h->s));
+  // samples from 1.5 g0 - 0.5 g1 to 2 g1 - g0, g0 / g1 the static cells holding rmin / rmax
+  // (SaveEMFields.cpp:59-76)
+  const double g0 = std::floor((m[10] - h->b.org0) / h->b.hr0), g1 = std::floor((m[12] - h->b.org0) / h->b.hr0);
+  const double l0 = std::floor(1.5 * g0 - 0.5 * g1), u0 = 2 * g1 - g0;
+  const long long i0 = (long long)l0;
+  const int n = (int)std::floor(u0 - l0 + 0.5) + 1;
+  *count = n;
+  if (!out) return CSRST_OK;
+  if (cap < n) return fail(h, CSRST_E_ARG, "line fields: output holds fewer than count samples");
+  double *d = nullptr;
+  CK(cudaMallocAsync(&d, (size_t)n * 7 * sizeof(double), h->s));
+  if (h->fp32)
+    launch_line_fields(h->order, h->Exf, h->Eyf, h->Hxf, h->Hyf, h->pitch32, h->cfg.Nx, h->cfg.Ny, h->winf,
+                       h->wpitch, h->ws, with_current, h->b.org0, h->b.org1, h->b.hr0, h->b.hr1, h->dmean, i0, n, d,
+                       h->s);
+  else
+    launch_line_fields(h->order, h->Ex, h->Ey, h->Hx, h->Hy, h->pitch, h->cfg.Nx, h->cfg.Ny, h->win, h->wpitch,
+                       h->ws, with_current, h->b.org0, h->b.org1, h->b.hr0, h->b.hr1, h->dmean, i0, n, d, h->s);
+  CK(cudaMemcpyAsync(out, d, (size_t)n * 7 * sizeof(double), cudaMemcpyDeviceToHost, h->s));
+  CK(cudaFreeAsync(d, h->s));
+  CK(cudaStreamSynchronize(h->s));
+  return check_err(h);
+}
+
 int csrst_diag_field_energy(csrst_handle *h, int with_window, double *out2) {
   if (!h || !out2) return CSRST_E_ARG;
   if (with_window) {

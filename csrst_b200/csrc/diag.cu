@@ -238,6 +238,72 @@ __global__ void k_energy_final(const double *part, int nb, double area, double *
   out[1] = s1 * area;
 }
 
+// The static mesh with the window's values over the points it covers (the
+// state copyFields leaves before SaveEMFieldsCommand, main.cpp:468-476):
+// up to two planes summed (the split Hz); outside the static planes' guard
+// ring, and for the static current (zero in the loop), the value is 0.
+template <class T>
+struct OverlayView {
+  const T *s1, *s2;           // static planes (NULL: zero), interior (0, 0) at s + pitch + 1
+  int pitch, Nx, Ny;
+  const T *w1, *w2;           // window planes (NULL: no window)
+  int wpitch, P0, P1, L0, L1;
+  __device__ __forceinline__ double operator()(int i, int j) const {
+    const int a = i - P0, b = j - P1;
+    if (w1 && a >= 0 && a < L0 && b >= 0 && b < L1) {
+      const ptrdiff_t o = (ptrdiff_t)(b + 1) * wpitch + a + 1;
+      return (double)w1[o] + (w2 ? (double)w2[o] : 0.0);
+    }
+    if (!s1 || i < -1 || j < -1 || i > Nx || j > Ny) return 0.0;
+    const ptrdiff_t o = (ptrdiff_t)(j + 1) * pitch + i + 1;
+    return (double)s1[o] + (s2 ? (double)s2[o] : 0.0);
+  }
+};
+
+// SaveEMFieldsCommand::execute (src/Commands/SaveEMFields.cpp:34-189): the
+// fields along the line through the centroid in the direction of the mean
+// momentum, one sample per static column i0 .. i0 + n - 1, gathered with the
+// run's shape order from the overlaid mesh.  out[7 k ..]: signed distance from
+// the centroid, E along and across the momentum, Hz, J along it, x, y; samples
+// off the static mesh keep their position and zero fields.
+template <int ORDER, class T>
+__global__ void k_line_fields(const T *Ex, const T *Ey, const T *Hx, const T *Hy, int pitch, int Nx, int Ny,
+                              const T *win, int wpitch, const WinState *ws, int with_current, double org0,
+                              double org1, double h0, double h1, const double *mean, long long i0, int n,
+                              double *out) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const double R0 = mean[0], R1 = mean[1], P0 = mean[2], P1 = mean[3];
+  const long long i = i0 + k;
+  const double dx = (org0 + (double)i * h0) - R0;
+  const double dy = dx / P0 * P1;
+  double *o = out + 7 * (size_t)k;
+  o[0] = sqrt(dx * dx + dy * dy) * (dx > 0 ? 1.0 : -1.0);
+  o[5] = dx + R0;
+  o[6] = dy + R1;
+  const double x = org0 + (double)i * h0, y = R1 + (x - R0) / P0 * P1;
+  const double pp0 = (x - org0) * (1.0 / h0), pp1 = (y - org1) * (1.0 / h1);
+  const long long cy = (long long)floor(pp1);
+  if (i < 0 || i >= Nx || cy < 0 || cy >= Ny) { o[1] = o[2] = o[3] = o[4] = 0.0; return; }
+  const size_t wp = (size_t)wpitch * (ws->L1 + 2);
+  const int WP0 = ws->P0, WP1 = ws->P1, L0 = ws->L0, L1 = ws->L1;
+  const OverlayView<T> vEx{Ex, nullptr, pitch, Nx, Ny, win, nullptr, wpitch, WP0, WP1, L0, L1};
+  const OverlayView<T> vEy{Ey, nullptr, pitch, Nx, Ny, win + wp, nullptr, wpitch, WP0, WP1, L0, L1};
+  const OverlayView<T> vH{Hx, Hy, pitch, Nx, Ny, win + 2 * wp, win + 3 * wp, wpitch, WP0, WP1, L0, L1};
+  const OverlayView<T> vJx{nullptr, nullptr, pitch, Nx, Ny, with_current ? win + 4 * wp : nullptr, nullptr, wpitch,
+                           WP0, WP1, L0, L1};
+  const OverlayView<T> vJy{nullptr, nullptr, pitch, Nx, Ny, with_current ? win + 5 * wp : nullptr, nullptr, wpitch,
+                           WP0, WP1, L0, L1};
+  const double e0 = gather_edge<ORDER>(vEx, pp0, pp1, 0), e1 = gather_edge<ORDER>(vEy, pp0, pp1, 1);
+  const double hz = gather_cell<ORDER>(vH, pp0, pp1);
+  const double j0 = gather_edge<ORDER>(vJx, pp0, pp1, 0), j1 = gather_edge<ORDER>(vJy, pp0, pp1, 1);
+  const double lenP = sqrt(P0 * P0 + P1 * P1), cP = P0 / lenP, sP = P1 / lenP;
+  o[1] = cP * e0 + sP * e1;
+  o[2] = -sP * e0 + cP * e1;
+  o[3] = hz;
+  o[4] = cP * j0 + sP * j1;
+}
+
 // --- host launchers -----------------------------------------------------------
 
 void launch_moments(const double *x, const double *y, const double *px, const double *py, long long n,
@@ -249,6 +315,28 @@ void launch_moments(const double *x, const double *y, const double *px, const do
 }
 
 size_t moments_scratch_doubles() { return (size_t)kDiagBlocks * 12; }
+
+template <class T>
+void launch_line_fields(int order, const T *Ex, const T *Ey, const T *Hx, const T *Hy, int pitch, int Nx, int Ny,
+                        const T *win, int wpitch, const WinState *ws, int with_current, double org0, double org1,
+                        double h0, double h1, const double *mean, long long i0, int n, double *out, cudaStream_t s) {
+  const int g = (n + 127) / 128;
+  if (order == 0)
+    k_line_fields<0, T><<<g, 128, 0, s>>>(Ex, Ey, Hx, Hy, pitch, Nx, Ny, win, wpitch, ws, with_current, org0, org1,
+                                          h0, h1, mean, i0, n, out);
+  else if (order == 1)
+    k_line_fields<1, T><<<g, 128, 0, s>>>(Ex, Ey, Hx, Hy, pitch, Nx, Ny, win, wpitch, ws, with_current, org0, org1,
+                                          h0, h1, mean, i0, n, out);
+  else
+    k_line_fields<2, T><<<g, 128, 0, s>>>(Ex, Ey, Hx, Hy, pitch, Nx, Ny, win, wpitch, ws, with_current, org0, org1,
+                                          h0, h1, mean, i0, n, out);
+}
+template void launch_line_fields<double>(int, const double *, const double *, const double *, const double *, int,
+                                         int, int, const double *, int, const WinState *, int, double, double,
+                                         double, double, const double *, long long, int, double *, cudaStream_t);
+template void launch_line_fields<float>(int, const float *, const float *, const float *, const float *, int, int,
+                                        int, const float *, int, const WinState *, int, double, double, double,
+                                        double, const double *, long long, int, double *, cudaStream_t);
 
 template <class T>
 void launch_field_energy(const T *Ex, const T *Ey, const T *Hx, const T *Hy, int pitch, int Nx, int Ny,

@@ -140,6 +140,11 @@ void launch_moments(const double *x, const double *y, const double *px, const do
 // Field energy sums over the static mesh (and the window, replacing the points
 // it covers): out2 = {sum(Ex^2 + Ey^2), sum((Hzx + Hzy)^2)} x area; part holds
 // 2 doubles per block of the moments grid.
+// Fields along the centroid line over static columns i0 .. i0 + n - 1 (7 values per sample).
+template <class T>
+void launch_line_fields(int order, const T *Ex, const T *Ey, const T *Hx, const T *Hy, int pitch, int Nx, int Ny,
+                        const T *win, int wpitch, const WinState *ws, int with_current, double org0, double org1,
+                        double h0, double h1, const double *mean, long long i0, int n, double *out, cudaStream_t s);
 template <class T>
 void launch_field_energy(const T *Ex, const T *Ey, const T *Hx, const T *Hy, int pitch, int Nx, int Ny,
                          const T *win, int wpitch, const WinState *ws, int with_window, double area, double *part,

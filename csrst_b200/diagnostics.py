@@ -1,4 +1,4 @@
-"""Run statistics in the reference's file format.
+"""Run statistics and field dumps in the reference's file formats.
 
 DataSink writes the SDDS1 ASCII statistics file of DataSinkCommand
 (src/Commands/DataSink.cpp:22-149): the reference's header, then one row per
@@ -90,6 +90,28 @@ class DataSink:
 
     def __exit__(self, *exc):
         self.close()
+
+
+class LineFieldSink:
+    """SaveEMFieldsCommand (src/Commands/SaveEMFields.cpp:34-189): each
+    execute() writes Data/FieldOnLine_NNNN.dat with one tab-separated line per
+    sample (signed distance from the centroid, E along and across the mean
+    momentum, Hz, J along it, x, y) in the default 6-digit C++ stream format,
+    numbering the files from 0.  with_current=True takes J from the window
+    (the reference does on plot steps; otherwise its column is 0)."""
+
+    def __init__(self, sim, directory="Data", with_current=False):
+        self.sim, self.dir, self.with_current, self.iteration = sim, directory, with_current, 0
+        os.makedirs(directory, exist_ok=True)
+
+    def execute(self):
+        rows = self.sim.line_fields(self.with_current)
+        path = os.path.join(self.dir, "FieldOnLine_%04d.dat" % self.iteration)
+        with open(path, "w") as f:
+            for r in rows:
+                f.write("\t".join("%g" % v for v in r) + "\n")
+        self.iteration += 1
+        return path, rows
 
 
 def read_sdds(path):

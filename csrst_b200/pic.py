@@ -178,6 +178,15 @@ class Simulation:
         self._ck(lib().csrst_diag_moments(self.h, ptr(out)))
         return out
 
+    def line_fields(self, with_current=False):
+        """[n][7] samples along the centroid line (SaveEMFields.cpp:34-189):
+        signed distance, E along / across the momentum, Hz, J along, x, y."""
+        cnt = C.c_int()
+        self._ck(lib().csrst_diag_line_fields(self.h, 1 if with_current else 0, None, 0, C.byref(cnt)))
+        out = np.zeros((cnt.value, 7))
+        self._ck(lib().csrst_diag_line_fields(self.h, 1 if with_current else 0, ptr(out), cnt.value, C.byref(cnt)))
+        return out
+
     def field_energy(self, with_window=True):
         """{sum(Ex^2 + Ey^2), sum((Hzx + Hzy)^2)} x cell area over the static
         mesh, the window replacing the points it covers (CalcEnergy.cpp:41-120)."""

@@ -236,6 +236,15 @@ int csrst_diag_moments(csrst_handle *h, double *out18);
  * window's points replacing the ones they cover when with_window is set (needs a loaded bunch).
  * The reference's energy is 0.25 eps0 (E_now + E_last) + 0.5 mu0 H (csrst_b200.diagnostics). */
 int csrst_diag_field_energy(csrst_handle *h, int with_window, double *out2);
+/* Fields along the line through the bunch centroid in the direction of its mean momentum
+ * (SaveEMFieldsCommand, src/Commands/SaveEMFields.cpp:34-189): one sample per static column from
+ * 1.5 g0 - 0.5 g1 to 2 g1 - g0 (g0, g1 the columns holding the bunch's extremes), gathered with the
+ * run's shape order from the static mesh with the window's values over the points it covers.
+ * out[7 k ..] = signed distance from the centroid, E along and across the momentum, Hz, J along
+ * the momentum, x, y.  with_current: J from the window (the reference copies it on plot steps
+ * only; otherwise its static J, zero in the loop, gives 0).  *count receives the number of
+ * samples; out = NULL returns only the count; cap < count is an error. */
+int csrst_diag_line_fields(csrst_handle *h, int with_current, double *out, int cap, int *count);
 /* Longitudinal field along the bunch axis at window columns 2 .. L0-3
  * (IntegrateElongCommand::execute, IntegrateElong.cpp:38-89); NaN where the
  * sample lies outside the window.  n must be L0 - 4. */

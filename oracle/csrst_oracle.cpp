@@ -1676,6 +1676,63 @@ void orc_wake(void *h, double r0, double r1, double p0, double p1, double *out) 
   }
 }
 
+// SaveEMFieldsCommand::execute (src/Commands/SaveEMFields.cpp:34-189) after copyFields
+// (main.cpp:468-476): the static mesh with the mini mesh's values over the points it covers
+// (the current only with with_current; the loop's static current is zero), gathered with the
+// run's shape order at one point per static column on the line through the centroid along the
+// mean momentum.  Points beyond the static guard ring read zero.  out: 7 values per sample.
+void orc_moments(void *h, double *out);
+void orc_line_fields(void *h, int with_current, double *out, int cap, int *count) {
+  Sim &s = *(Sim *)h;
+  double m[18];
+  orc_moments(h, m);
+  const double org0 = s.b.org0, org1 = s.b.org1, h0 = s.b.hr0, h1 = s.b.hr1;
+  const double g0 = std::floor((m[10] - org0) / h0), g1 = std::floor((m[12] - org0) / h0);
+  const double l0 = std::floor(1.5 * g0 - 0.5 * g1), u0 = 2 * g1 - g0;
+  const long i0 = (long)l0;
+  const int n = (int)std::floor(u0 - l0 + 0.5) + 1;
+  *count = n;
+  if (!out || cap < n) return;
+  const int Nx = s.b.Nx, Ny = s.b.Ny, M = 2, W = Nx + 2 * M;
+  // dense overlaid copies with a 2-point margin; index (0, 0) = static point (0, 0)
+  std::vector<double> ex((size_t)W * (Ny + 2 * M), 0.0), ey(ex.size(), 0.0), hz(ex.size(), 0.0),
+      jx(ex.size(), 0.0), jy(ex.size(), 0.0);
+  auto at = [&](std::vector<double> &v, int i, int j) -> double & { return v[(size_t)(j + M) * W + i + M]; };
+  for (int j = -1; j <= Ny; ++j)
+    for (int i = -1; i <= Nx; ++i) {
+      const int a = i - s.P0, b = j - s.P1;
+      if (a >= 0 && a < s.L0 && b >= 0 && b < s.L1) {
+        at(ex, i, j) = s.mEx.at(a, b); at(ey, i, j) = s.mEy.at(a, b);
+        at(hz, i, j) = s.mHx.at(a, b) + s.mHy.at(a, b);
+        if (with_current) { at(jx, i, j) = s.mJx.at(a, b); at(jy, i, j) = s.mJy.at(a, b); }
+      } else {
+        at(ex, i, j) = s.Ex.at(i, j); at(ey, i, j) = s.Ey.at(i, j);
+        at(hz, i, j) = s.Hx.at(i, j) + s.Hy.at(i, j);
+      }
+    }
+  auto patch = [&](std::vector<double> &v) { return Patch{v.data() + (size_t)M * W + M, W, Ny + 2 * M, org0, org1, h0, h1}; };
+  const Patch pex = patch(ex), pey = patch(ey), phz = patch(hz), pjx = patch(jx), pjy = patch(jy);
+  const double R0 = m[0], R1 = m[1], P0 = m[2], P1 = m[3];
+  const double lenP = std::sqrt(P0 * P0 + P1 * P1), cP = P0 / lenP, sP = P1 / lenP;
+  for (int k = 0; k < n; ++k) {
+    const long i = i0 + k;
+    const double dx = (org0 + (double)i * h0) - R0, dy = dx / P0 * P1;
+    double *o = out + 7 * (size_t)k;
+    o[0] = std::sqrt(dx * dx + dy * dy) * (dx > 0 ? 1.0 : -1.0);
+    o[5] = dx + R0;
+    o[6] = dy + R1;
+    const double x = org0 + (double)i * h0, y = R1 + (x - R0) / P0 * P1;
+    const long cy = (long)std::floor((y - org1) * (1.0 / h1));
+    if (i < 0 || i >= Nx || cy < 0 || cy >= Ny) { o[1] = o[2] = o[3] = o[4] = 0.0; continue; }
+    const double e0 = gather_edge(s.order, pex, x, y, 0), e1 = gather_edge(s.order, pey, x, y, 1);
+    const double j0 = gather_edge(s.order, pjx, x, y, 0), j1 = gather_edge(s.order, pjy, x, y, 1);
+    o[1] = cP * e0 + sP * e1;
+    o[2] = -sP * e0 + cP * e1;
+    o[3] = gather_cell(s.order, phz, x, y);
+    o[4] = cP * j0 + sP * j1;
+  }
+}
+
 // CalcEnergyCommand::execute (src/Commands/CalcEnergy.cpp:41-120) before its time
 // averaging, in the reference's order: every static point, plus every mini-mesh
 // point, minus the static points the mini mesh covers; times the cell area.

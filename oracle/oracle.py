@@ -72,6 +72,7 @@ def lib():
         L.orc_wake.argtypes = [C.c_void_p] + [C.c_double] * 4 + [D]
         L.orc_moments.argtypes = [C.c_void_p, D]
         L.orc_field_energy.argtypes = [C.c_void_p, C.c_int, D]
+        L.orc_line_fields.argtypes = [C.c_void_p, C.c_int, D, C.c_int, C.POINTER(C.c_int)]
         L.orc_initial_fields.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_int, D]
         _LIB = L
     return _LIB
@@ -234,6 +235,13 @@ class Sim:
     def moments(self):
         out = np.zeros(18)
         lib().orc_moments(self.h, _p(out))
+        return out
+
+    def line_fields(self, with_current=False):
+        cnt = C.c_int()
+        lib().orc_line_fields(self.h, 1 if with_current else 0, None, 0, C.byref(cnt))
+        out = np.zeros((cnt.value, 7))
+        lib().orc_line_fields(self.h, 1 if with_current else 0, _p(out), cnt.value, C.byref(cnt))
         return out
 
     def field_energy(self, with_window=True):

@@ -38,3 +38,20 @@ def test_header_rows_and_energy(tmp_path):
     e2 = 0.25 * EPSILON_0 * (4.0 + 3.0) + 0.5 * MU_0 * 6.0      # then the previous call's E
     assert np.isclose(rows[0][15], e1 * 1e9, rtol=1e-13) and np.isclose(rows[1][15], e2 * 1e9, rtol=1e-13)
     assert all(len(ln) == 25 * 16 for ln in text[-2:])
+
+
+def test_line_field_files(tmp_path):
+    """FieldOnLine_NNNN.dat: numbered from 0, one tab-separated line of 7
+    values per sample in the default stream format."""
+    from csrst_b200.diagnostics import LineFieldSink
+
+    class _S:
+        def line_fields(self, with_current):
+            return np.array([[-1.5e-4, 1.25, -2.0, 3.0, 0.0 if not with_current else 4.0, 1e-3, 2e-3]] * 3)
+
+    ls = LineFieldSink(_S(), str(tmp_path / "Data"))
+    p0, _ = ls.execute()
+    p1, _ = ls.execute()
+    assert p0.endswith("FieldOnLine_0000.dat") and p1.endswith("FieldOnLine_0001.dat")
+    lines = open(p0).read().splitlines()
+    assert len(lines) == 3 and lines[0] == "-0.00015\t1.25\t-2\t3\t0\t0.001\t0.002"

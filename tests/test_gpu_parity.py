@@ -292,3 +292,26 @@ def test_error_paths(gpu_lib):
     with pytest.raises(CsrstError) as e:
         s.load(x, y, px, py, q)
     assert e.value.code == -1
+
+
+@pytest.mark.parametrize("name", ["small-0", "small-1", "small-2", "small-1-bend"])
+def test_line_fields(gpu_lib, oracle, name):
+    """SaveEMFieldsCommand's line samples (SaveEMFields.cpp:34-189) on the
+    overlaid static mesh, for every shape order, with and without the window's
+    current: positions (built from the centroid and mean momentum, whose FP64
+    and long-double Kahan sums round differently) within 1e-12, fields within
+    1e-12 of their magnitude."""
+    cfg, g, o = pair(name, oracle)
+    g.step(5)
+    o.step(5)
+    for cur in (False, True):
+        lg, lo = g.line_fields(cur), o.line_fields(cur)
+        assert lg.shape == lo.shape and lg.shape[0] > 10
+        for c in (0, 5, 6):
+            assert np.abs(lg[:, c] - lo[:, c]).max() <= 1e-12 * np.abs(lo[:, c]).max(), c
+        for c in (1, 2, 3, 4):
+            scale = np.abs(lo[:, c]).max()
+            if c == 4 and not cur:
+                assert scale == 0 and np.all(lg[:, c] == 0)
+                continue
+            assert scale > 0 and np.abs(lg[:, c] - lo[:, c]).max() <= 1e-12 * scale, (cur, c)
