@@ -114,6 +114,164 @@ class LineFieldSink:
         return path, rows
 
 
+def overlaid_fields(sim, with_current=True):
+    """The static mesh's fields [Ny][Nx] with the window's values over the
+    points it covers, as copyFields leaves them on a plot step (main.cpp:54-66,
+    called at :417 with copyCurrent true): Ex, Ey, Hz = Hzx + Hzy, Jx, Jy (the
+    current only from the window, and only with_current)."""
+    import numpy as np
+    ex, ey, hx, hy = sim.get_static()
+    jx, jy = np.zeros_like(ex), np.zeros_like(ex)
+    (P0, P1, L0, L1), _, _ = sim.window()
+    win = [sim.window_field(k)[1:L1 + 1, 1:L0 + 1] for k in range(6)]
+    j0, j1 = max(P1, 0), min(P1 + L1, sim.Ny)
+    i0, i1 = max(P0, 0), min(P0 + L0, sim.Nx)
+    sl = (slice(j0, j1), slice(i0, i1))
+    ws = (slice(j0 - P1, j1 - P1), slice(i0 - P0, i1 - P0))
+    for dst, k in ((ex, 0), (ey, 1), (hx, 2), (hy, 3)):
+        dst[sl] = win[k][ws]
+    if with_current:
+        jx[sl], jy[sl] = win[4][ws], win[5][ws]
+    return ex, ey, hx + hy, jx, jy
+
+
+def window_fields(sim):
+    """The window's own fields [L1][L0] (its interior) and its origin: Ex, Ey,
+    Hzx + Hzy, Jx, Jy."""
+    (_, _, L0, L1), origin, _ = sim.window()
+    w = [sim.window_field(k)[1:L1 + 1, 1:L0 + 1] for k in range(6)]
+    return (w[0], w[1], w[2] + w[3], w[4], w[5]), origin
+
+
+class VtkSink:
+    """PlotBinaryVTKCommand (src/Commands/PlotBinaryVTK.cpp:29-88, with the
+    collection of PlotBinaryVTK.hh:58-80) and its writer BinaryVtkFile
+    (src/Commands/BinaryVTKFile.cpp:25-78, BinaryVTKFile.hh:102-380).
+
+    The run writes two series (main.cpp:358-359): base "c", the static mesh
+    with the window copied over it, and base "mm", the window alone
+    (source="window").  Each execute(t) writes, for the i-th call,
+    <dir>/<base>_NNNN_node00000.vtr: an XML RectilinearGrid with raw appended
+    little-endian Float32 data, every array preceded by its byte count as a
+    32-bit unsigned integer: X/Y/Z_COORDINATES (i h + origin; z one 0), then
+    E-Field and J-Field (3 components, z 0) and H-Field (Hzx + Hzy), x fastest;
+    <dir>/<base>_NNNN.pvtr, the parallel header naming that piece; and
+    <dir>/<base>_collection.pvd, the time series so far (the reference writes it
+    at closeFile; writing it at every step keeps it whole if a run stops).  A
+    collection already on disk is read first and numbering continues after it
+    (PlotBinaryVTK.cpp:90-119), so a resumed run extends its series."""
+
+    def __init__(self, sim, base="c", directory="Data", source="static", with_current=True):
+        import re
+        if source not in ("static", "window"):
+            raise ValueError("source must be 'static' or 'window'")
+        self.sim, self.base, self.dir, self.source = sim, base, directory, source
+        self.with_current = with_current
+        os.makedirs(directory, exist_ok=True)
+        self.times = []
+        col = self._collection()
+        if os.path.exists(col):
+            for line in open(col):
+                m = re.search(r'<DataSet timestep="(.*?)"', line)
+                if m:
+                    self.times.append(float(m.group(1)))
+
+    def _collection(self):
+        return os.path.join(self.dir, self.base + "_collection.pvd")
+
+    def _fields(self):
+        info = self.sim.info()
+        if self.source == "static":
+            f = overlaid_fields(self.sim, self.with_current)
+            origin = (info["ox"], info["oy"])
+        else:
+            f, origin = window_fields(self.sim)
+        return f, origin, (info["hx"], info["hy"])
+
+    def execute(self, t):
+        import numpy as np
+        (ex, ey, hz, jx, jy), origin, h = self._fields()
+        ny, nx = ex.shape
+        stem = os.path.join(self.dir, "%s_%04d" % (self.base, len(self.times)))
+        blocks, arrays = [], []
+
+        def add(kind, name, values, comps):
+            arrays.append((kind, name, comps, sum(4 + b.nbytes for b in blocks)))
+            blocks.append(np.ascontiguousarray(values, dtype="<f4"))
+
+        add("coord", "X_COORDINATES", np.arange(nx) * h[0] + origin[0], 1)
+        add("coord", "Y_COORDINATES", np.arange(ny) * h[1] + origin[1], 1)
+        add("coord", "Z_COORDINATES", np.zeros(1), 1)
+        zero = np.zeros_like(ex)
+        add("point", "E-Field", np.stack([ex, ey, zero], axis=-1), 3)
+        add("point", "J-Field", np.stack([jx, jy, zero], axis=-1), 3)
+        add("point", "H-Field", hz, 1)
+        ext = '"0 %d 0 %d 1 1"' % (nx - 1, ny - 1)
+        head = ('<?xml version="1.0"?>\n<VTKFile type="RectilinearGrid" version="0.1" '
+                'byte_order="LittleEndian">\n  <RectilinearGrid WholeExtent=%s>\n    <Piece Extent=%s>\n'
+                '      <PointData Scalars="H-Field" Vectors="E-Field, J-Field">\n' % (ext, ext))
+        for kind, name, comps, off in arrays:
+            if kind == "point":
+                head += ('        <DataArray type="Float32" Name="%s" NumberOfComponents="%d" '
+                         'format="appended" offset="%d"/>\n' % (name, comps, off))
+        head += '      </PointData>\n      <Coordinates>\n'
+        for kind, name, comps, off in arrays:
+            if kind == "coord":
+                head += ('        <DataArray type="Float32" name="%s" NumberOfComponents="%d" '
+                         'format="appended" offset="%d"/>\n' % (name, comps, off))
+        head += ('      </Coordinates>\n    </Piece>\n  </RectilinearGrid>\n'
+                 '  <AppendedData encoding="raw">\n    _')
+        piece = stem + "_node00000.vtr"
+        with open(piece, "wb") as f:
+            f.write(head.encode())
+            for b in blocks:
+                f.write(np.uint32(b.nbytes).tobytes())
+                f.write(b.tobytes())
+            f.write(b"\n  </AppendedData>\n</VTKFile>\n")
+        with open(stem + ".pvtr", "w") as f:
+            f.write('<?xml version="1.0"?>\n<VTKFile type="PRectilinearGrid" version="0.1" '
+                    'byte_order="LittleEndian">\n  <PRectilinearGrid WholeExtent=%s GhostLevel="1">\n' % ext)
+            f.write('    <PPointData Scalars="H-Field" Vectors="E-Field, J-Field">\n')
+            for kind, name, comps, _ in arrays:
+                if kind == "point":
+                    f.write('      <PDataArray type="Float32" Name="%s" NumberOfComponents="%d"/>\n'
+                            % (name, comps))
+            f.write('    </PPointData>\n    <PCoordinates>\n')
+            for name in ("X_COORDINATES", "Y_COORDINATES", "Z_COORDINATES"):
+                f.write('      <PDataArray type="Float32" name="%s" NumberOfComponents="1"/>\n' % name)
+            f.write('    </PCoordinates>\n    <Piece Extent=%s Source="%s"/>\n'
+                    % (ext, os.path.basename(piece)))
+            f.write('  </PRectilinearGrid>\n</VTKFile>\n')
+        self.times.append(t)
+        self.close()
+        return piece
+
+    def close(self):
+        with open(self._collection(), "w") as f:
+            f.write('<?xml version="1.0"?>\n<VTKFile type="Collection" version="0.1" '
+                    'byte_order="LittleEndian">\n  <Collection>\n')
+            for i, t in enumerate(self.times):
+                f.write('    <DataSet timestep="%g" group="" part="0" file="%s_%04d.pvtr"/>\n'
+                        % (t, self.base, i))
+            f.write('  </Collection>\n</VTKFile>\n')
+
+
+def read_vtr(path):
+    """{name: float32 array} of a piece written by VtkSink (appended raw data)."""
+    import re
+    import numpy as np
+    raw = open(path, "rb").read()
+    head, _, rest = raw.partition(b"<AppendedData encoding=\"raw\">")
+    data = rest[rest.index(b"_") + 1:]
+    out = {}
+    for m in re.finditer(rb'<DataArray type="Float32" [Nn]ame="([^"]+)" NumberOfComponents="(\d)" '
+                         rb'format="appended" offset="(\d+)"/>', head):
+        off = int(m.group(3))
+        n = int(np.frombuffer(data[off:off + 4], dtype="<u4")[0])
+        out[m.group(1).decode()] = np.frombuffer(data[off + 4:off + 4 + n], dtype="<f4")
+    return out
+
+
 def read_sdds(path):
     """(column names, rows) of an ASCII statistics file written by DataSink."""
     import numpy as np

@@ -206,3 +206,50 @@ def ensemble_members(m=64, seed=2024):
                          charge=-1e-9, x0=x0, y0=0.5 * width, seed=1000 + k)
         out.append((cfg, spec))
     return out
+
+
+# ---- the reference's own initial distribution (src/Distribution.cpp:55-163) ----
+
+M_E_MEV = M_E_GEV * 1e3       # Distribution.cpp:26: MASS = Physics::m_e * 1e3
+
+
+def radical_inverse(n, base):
+    """Van der Corput radical inverse of the integers n in `base` (the
+    published Halton construction): digits of n mirrored about the point,
+    accumulated most significant first as v /= base; r += v * digit."""
+    x = np.asarray(n, dtype=np.int64).copy()
+    r = np.zeros(x.shape)
+    v = np.ones(x.shape)
+    while np.any(x > 0):
+        m = x > 0
+        v[m] /= base
+        r[m] += v[m] * (x[m] % base)
+        x[m] //= base
+    return r
+
+
+def halton_bunch(n=50000, mean_rx=0.05, mean_ry=0.0, sigma_x=0.01, ekin_mev=250.0, sigma_p=1.0, qtotal_nc=-1.0,
+                 origin=(0.0, 0.0), spacing=(1.0, 1.0)):
+    """The bunch the reference builds from its command line (Distribution.cpp:55-131;
+    defaults from main.cpp:126-133): point k (k = 1 .. n) of the 2D Halton
+    sequence (bases 2, 3) becomes a round Gaussian sample by Box-Muller,
+    sigma sqrt(-2 ln v0) (cos, sin)(2 pi v1).  Positions and momentum offsets
+    come from two generators of the same sequence, so they are proportional
+    point by point; momenta are (sqrt(gamma^2 - 1), 0) + offset with gamma =
+    Ekin / m_e + 1; charges -Qtotal 1e-9 / n each.  Then the positions alone
+    are sorted by mesh row (truncated, Utils::XFirst, utils.hh:116-142) and x
+    — which, as in the reference, unpairs them from the momenta.  Returns
+    (x, y, px, py, q).  GSL is not available here: the sequence is the
+    published construction, checked against scipy's, not against GSL itself."""
+    k = np.arange(1, n + 1)
+    v0, v1 = radical_inverse(k, 2), radical_inverse(k, 3)
+    r = np.sqrt(-2.0 * np.log(v0))
+    a = 2.0 * math.pi * v1
+    c, s_ = np.cos(a), np.sin(a)
+    x, y = mean_rx + sigma_x * r * c, mean_ry + sigma_x * r * s_
+    gamma = ekin_mev / M_E_MEV + 1.0
+    px, py = math.sqrt(gamma * gamma - 1.0) + sigma_p * r * c, sigma_p * r * s_
+    row = np.trunc((y - origin[1]) / spacing[1]).astype(np.int64)
+    order = np.lexsort((x, row))
+    q = np.full(n, -qtotal_nc * 1e-9 / n)
+    return x[order], y[order], px, py, q

@@ -55,3 +55,59 @@ def test_line_field_files(tmp_path):
     assert p0.endswith("FieldOnLine_0000.dat") and p1.endswith("FieldOnLine_0001.dat")
     lines = open(p0).read().splitlines()
     assert len(lines) == 3 and lines[0] == "-0.00015\t1.25\t-2\t3\t0\t0.001\t0.002"
+
+
+def test_vtk_piece_header_and_collection(tmp_path):
+    """VtkSink steps of both series: the static piece's appended arrays read
+    back equal to the overlaid fields (window over static, J from the window),
+    the window piece to the window's interior at its origin; the parallel
+    header names its piece, the collection lists each time step, and a new
+    sink on the same directory continues the numbering."""
+    from csrst_b200.diagnostics import VtkSink, read_vtr
+
+    class _S:
+        Nx, Ny = 12, 8
+
+        def info(self):
+            return {"hx": 0.5, "hy": 0.25, "ox": -1.0, "oy": 2.0}
+
+        def get_static(self):
+            g = np.arange(96, dtype=float).reshape(8, 12)
+            return [g, g + 1000, g * 2, g * 3]
+
+        def window(self):
+            return [3, 2, 4, 3], np.array([0.5, 2.5]), None
+
+        def window_field(self, k):
+            w = np.full((5, 6), 10000.0 * (k + 1))
+            w[2, 2] += 1
+            return w
+
+    d = str(tmp_path / "Data")
+    vs = VtkSink(_S(), directory=d)
+    piece = vs.execute(1e-12)
+    vs.execute(2e-12)
+    a = read_vtr(piece)
+    assert np.allclose(a["X_COORDINATES"], np.arange(12) * 0.5 - 1.0)
+    assert np.allclose(a["Y_COORDINATES"], np.arange(8) * 0.25 + 2.0)
+    E = a["E-Field"].reshape(8, 12, 3)
+    g = np.arange(96, dtype=float).reshape(8, 12)
+    ex = g.copy()
+    ex[2:5, 3:7] = 10000.0
+    ex[3, 4] += 1
+    assert np.array_equal(E[..., 0], ex.astype(np.float32)) and np.all(E[..., 2] == 0)
+    H = a["H-Field"].reshape(8, 12)
+    hz = g * 5
+    hz[2:5, 3:7] = 30000.0 + 40000.0
+    hz[3, 4] += 2
+    assert np.array_equal(H, hz.astype(np.float32))
+    J = a["J-Field"].reshape(8, 12, 3)
+    assert J[3, 4, 0] == 50001.0 and J[0, 0, 0] == 0.0
+    assert 'Source="c_0000_node00000.vtr"' in open(d + "/c_0000.pvtr").read()
+    col = open(d + "/c_collection.pvd").read()
+    assert col.count("<DataSet") == 2 and 'timestep="2e-12"' in col and 'file="c_0001.pvtr"' in col
+    assert len(VtkSink(_S(), directory=d).times) == 2           # a resumed run continues the series
+    w = read_vtr(VtkSink(_S(), base="mm", directory=d, source="window").execute(0.0))
+    assert np.allclose(w["X_COORDINATES"], np.arange(4) * 0.5 + 0.5)
+    Ew = w["E-Field"].reshape(3, 4, 3)
+    assert Ew.shape == (3, 4, 3) and Ew[1, 1, 0] == 10001.0 and Ew[0, 0, 1] == 20000.0

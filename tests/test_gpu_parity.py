@@ -315,3 +315,54 @@ def test_line_fields(gpu_lib, oracle, name):
                 assert scale == 0 and np.all(lg[:, c] == 0)
                 continue
             assert scale > 0 and np.abs(lg[:, c] - lo[:, c]).max() <= 1e-12 * scale, (cur, c)
+
+
+def test_halton_bunch_steps(gpu_lib, oracle):
+    """The reference's command-line bunch (Distribution.cpp:55-163, the Halton
+    round Gaussian), placed and sized for the 512 x 104 mesh, runs through the
+    loop bit-identically to the oracle."""
+    from csrst_b200.workloads import halton_bunch
+    cfg, spec = workload("small-1")
+    g = Simulation(cfg)
+    info = g.info()
+    bunch = halton_bunch(3000, mean_rx=spec.x0, mean_ry=spec.y0, sigma_x=40e-6, ekin_mev=cfg.ekin_mev,
+                         sigma_p=1.0, qtotal_nc=1.0, origin=(info["ox"], info["oy"]), spacing=(info["hx"], info["hy"]))
+    f = smooth_fields(cfg, 3)
+    g.set_static(*f)
+    g.load(*bunch)
+    d = cfg.dict()
+    d["order"] = cfg.shape_order
+    d["fixed_scale"] = g.info()["fixed_scale"]
+    o = oracle.Sim(d)
+    o.set_static(*f)
+    o.load(*bunch)
+    g.step(6)
+    o.step(6)
+    assert_same_state(g, o)
+
+
+def test_vtk_fields_match_oracle(gpu_lib, oracle, tmp_path):
+    """PlotBinaryVTKCommand's two series (main.cpp:358-365) from a GPU run:
+    the static piece holds the oracle's overlaid fields rounded to Float32
+    (the current, whose FP64 sums may differ in the last bits, within one
+    Float32 step), the window piece the oracle's window interior."""
+    from csrst_b200.diagnostics import VtkSink, overlaid_fields, read_vtr, window_fields
+    cfg, g, o = pair("small-1", oracle)
+    g.step(5)
+    o.step(5)
+    d = str(tmp_path / "Data")
+    a = read_vtr(VtkSink(g, directory=d).execute(1.0))
+    w = read_vtr(VtkSink(g, base="mm", directory=d, source="window").execute(1.0))
+    ex, ey, hz, jx, jy = overlaid_fields(o)
+    (wx, wy, wh, wjx, wjy), _ = window_fields(o)
+    f32 = lambda v: np.asarray(v, dtype=np.float32)
+    E = a["E-Field"].reshape(cfg.Ny, cfg.Nx, 3)
+    J = a["J-Field"].reshape(cfg.Ny, cfg.Nx, 3)
+    assert np.array_equal(E[..., 0], f32(ex)) and np.array_equal(E[..., 1], f32(ey))
+    for got, ref in ((J[..., 0], jx), (J[..., 1], jy)):         # the current: one Float32 rounding step
+        assert np.abs(got - ref).max() <= 2.4e-7 * np.abs(ref).max()
+    assert np.array_equal(a["H-Field"].reshape(cfg.Ny, cfg.Nx), f32(hz))
+    assert np.abs(jx).max() > 0
+    L1, L0 = wx.shape
+    assert np.array_equal(w["E-Field"].reshape(L1, L0, 3)[..., 0], f32(wx))
+    assert np.array_equal(w["H-Field"].reshape(L1, L0), f32(wh))
