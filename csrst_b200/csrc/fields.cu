@@ -17,21 +17,100 @@
 
 namespace csrst {
 
+// The static sweep works on 16-byte vectors of a plane row: a thread holds
+// storage columns c .. c + V - 1 of row j (V = 4 floats or 2 doubles), which
+// are the cells i = c - 1 .. c + V - 2 (storage column 0 is the left guard).
+// Plane rows start 256-byte aligned (pitch rounded up), so every vector load
+// is aligned.  A warp lies in one row segment of 32 consecutive vectors (tx is
+// a multiple of 32): the one element a cell needs from the next or previous
+// vector comes from the neighbouring lane by shuffle, the warp's end lanes
+// load it.  Vectors with c <= Nx + 1 are loaded (the right guard column is
+// read); cells 0 <= i < Nx on the inside mask are updated with the same
+// arithmetic as one cell per thread, and written back as a vector when all
+// of a vector's cells are, else element by element (the cut-cell blocks of
+// the same launch update the cells off the mask).
+template <class T>
+struct alignas(16) Vec16 {
+  static constexpr int N = 16 / sizeof(T);
+  T v[N];
+};
+template <class T>
+__device__ __forceinline__ Vec16<T> ld16(const T *p) { return *reinterpret_cast<const Vec16<T> *>(p); }
+template <class T>
+__device__ __forceinline__ void st16(T *p, const Vec16<T> &r) { *reinterpret_cast<Vec16<T> *>(p) = r; }
+
+// Storage column c and row j of thread t in static block b; false: no row.
+template <class T>
+__device__ __forceinline__ bool static_vec(const FieldArgsT<T> &a, int b, int &c, int &j) {
+  constexpr int V = Vec16<T>::N;
+  c = (b % a.tilesX) * a.tx * V + (threadIdx.x % a.tx) * V;
+  j = (b / a.tilesX) * a.ty + threadIdx.x / a.tx;
+  return j < a.Ny;  // uniform over the warp
+}
+
+// Inside-mask bits of the cells i = c - 1 + e of row j that are on the mesh.
+template <class T>
+__device__ __forceinline__ unsigned static_mask(const FieldArgsT<T> &a, int c, int j) {
+  constexpr int V = Vec16<T>::N;
+  unsigned m = 0;
+  const uint8_t *row = a.mask + (size_t)j * a.Nx;
+#pragma unroll
+  for (int e = 0; e < V; ++e) {
+    const int i = c - 1 + e;
+    if (i >= 0 && i < a.Nx && row[i]) m |= 1u << e;
+  }
+  return m;
+}
+
+template <class T>
+__device__ __forceinline__ void store_masked(T *p, const Vec16<T> &r, unsigned m) {
+  constexpr int V = Vec16<T>::N;
+  if (m == (1u << V) - 1) {
+    st16(p, r);
+  } else {
+#pragma unroll
+    for (int e = 0; e < V; ++e)
+      if (m >> e & 1u) p[e] = r.v[e];
+  }
+}
+
+template <class T>
+__device__ __forceinline__ void half_h_static(const FieldArgsT<T> &a, int b) {
+  constexpr int V = Vec16<T>::N;
+  int c, j;
+  if (!static_vec(a, b, c, j)) return;
+  const bool live = c <= a.Nx + 1;
+  T *hxp = &a.Hx.at(c - 1, j), *hyp = &a.Hy.at(c - 1, j);
+  Vec16<T> ey{}, ex0{}, ex1{}, hx{}, hy{};
+  if (live) {
+    ey = ld16(&a.Ey.at(c - 1, j));
+    ex0 = ld16(&a.Ex.at(c - 1, j));
+    ex1 = ld16(&a.Ex.at(c - 1, j + 1));
+    hx = ld16(hxp);
+    hy = ld16(hyp);
+  }
+  T eyn = __shfl_down_sync(0xffffffffu, ey.v[0], 1);
+  if (!live) return;
+  const unsigned m = static_mask(a, c, j);
+  if (!m) return;
+  if ((threadIdx.x & 31) == 31 && c + V <= a.Nx + 1) eyn = a.Ey.at(c + V - 1, j);
+#pragma unroll
+  for (int e = 0; e < V; ++e) {
+    const T ey1 = e + 1 < V ? ey.v[e + 1 < V ? e + 1 : 0] : eyn;
+    hx.v[e] = hx.v[e] - a.chx * (ey1 - ey.v[e]);
+    hy.v[e] = hy.v[e] + a.chy * (ex1.v[e] - ex0.v[e]);
+  }
+  store_masked(hxp, hx, m);
+  store_masked(hyp, hy, m);
+}
+
 // Half H update (first and third sub-step), block b of the sub-step grid.
-// The static sweep covers the mesh in tiles of tx x ty cells (tx * ty = 256
-// threads; the shape is a tuning parameter).
+// Static blocks cover the mesh in tiles of tx x ty vectors (tx * ty = 256
+// threads, tx a multiple of 32; the shape is a tuning parameter).
 template <class T>
 __device__ __forceinline__ void half_h_body(const FieldArgsT<T> &a, int b) {
   if (b < a.nbS) {
-    const int i = (b % a.tilesX) * a.tx + (threadIdx.x % a.tx);
-    const int j = (b / a.tilesX) * a.ty + (threadIdx.x / a.tx);
-    if (i >= a.Nx || j >= a.Ny) return;
-    if (!a.mask[(size_t)j * a.Nx + i]) return;
-    const T ey0 = a.Ey.at(i, j), ey1 = a.Ey.at(i + 1, j);
-    const T ex0 = a.Ex.at(i, j), ex1 = a.Ex.at(i, j + 1);
-    T &hx = a.Hx.at(i, j), &hy = a.Hy.at(i, j);
-    hx = hx - a.chx * (ey1 - ey0);
-    hy = hy + a.chy * (ex1 - ex0);
+    half_h_static(a, b);
   } else if (b < a.nbS + a.nbC) {
     const int k = (b - a.nbS) * blockDim.x + threadIdx.x;
     if (k >= a.ncells) return;
@@ -57,19 +136,55 @@ __device__ __forceinline__ void half_h_body(const FieldArgsT<T> &a, int b) {
 // current comes from the fixed-point accumulator of the last push, which is
 // converted, stored for diagnostics and cleared for the next deposit.
 template <class T, int COMP>
+__device__ __forceinline__ void update_e_static(const FieldArgsT<T> &a, int b, T zeroJ) {
+  constexpr int V = Vec16<T>::N;
+  int c, j;
+  if (!static_vec(a, b, c, j)) return;
+  const bool live = c <= a.Nx + 1;
+  T *ep = COMP == 0 ? &a.Ex.at(c - 1, j) : &a.Ey.at(c - 1, j);
+  Vec16<T> e{}, hx{}, hy{}, hxm{}, hym{};
+  if (live) {
+    e = ld16(ep);
+    hx = ld16(&a.Hx.at(c - 1, j));
+    hy = ld16(&a.Hy.at(c - 1, j));
+    if (COMP == 0) {
+      hxm = ld16(&a.Hx.at(c - 1, j - 1));
+      hym = ld16(&a.Hy.at(c - 1, j - 1));
+    }
+  }
+  T hxp = T(0), hyp = T(0);  // Ey: H of the cell left of the vector
+  if (COMP == 1) {
+    hxp = __shfl_up_sync(0xffffffffu, hx.v[V - 1], 1);
+    hyp = __shfl_up_sync(0xffffffffu, hy.v[V - 1], 1);
+  }
+  if (!live) return;
+  const unsigned m = static_mask(a, c, j);
+  if (!m) return;
+  if (COMP == 1 && (threadIdx.x & 31) == 0 && c >= 1) {
+    hxp = a.Hx.at(c - 2, j);
+    hyp = a.Hy.at(c - 2, j);
+  }
+#pragma unroll
+  for (int k = 0; k < V; ++k) {
+    if (COMP == 0) {
+      e.v[k] = e.v[k] + (a.kex * (hx.v[k] - hxm.v[k] + hy.v[k] - hym.v[k]) - a.dteps * zeroJ);
+    } else {
+      const T hxl = k > 0 ? hx.v[k > 0 ? k - 1 : 0] : hxp, hyl = k > 0 ? hy.v[k > 0 ? k - 1 : 0] : hyp;
+      e.v[k] = e.v[k] - (a.key * (hx.v[k] - hxl + hy.v[k] - hyl) + a.dteps * zeroJ);
+    }
+  }
+  store_masked(ep, e, m);
+}
+
+// E update: comp 0 = Ex (TETMSolver.hh:165-172), comp 1 = Ey (:241-249).  The
+// static mesh carries no current in the reference loop (its J is reset to
+// zero every step, main.cpp:388, :494), so it enters as 0.0.  The window
+// current comes from the fixed-point accumulator of the last push, which is
+// converted, stored for diagnostics and cleared for the next deposit.
+template <class T, int COMP>
 __device__ __forceinline__ void update_e_body(const FieldArgsT<T> &a, int b, T zeroJ) {
   if (b < a.nbS) {
-    const int i = (b % a.tilesX) * a.tx + (threadIdx.x % a.tx);
-    const int j = (b / a.tilesX) * a.ty + (threadIdx.x / a.tx);
-    if (i >= a.Nx || j >= a.Ny) return;
-    if (!a.mask[(size_t)j * a.Nx + i]) return;
-    if (COMP == 0) {
-      T &e = a.Ex.at(i, j);
-      e = e + (a.kex * (a.Hx.at(i, j) - a.Hx.at(i, j - 1) + a.Hy.at(i, j) - a.Hy.at(i, j - 1)) - a.dteps * zeroJ);
-    } else {
-      T &e = a.Ey.at(i, j);
-      e = e - (a.key * (a.Hx.at(i, j) - a.Hx.at(i - 1, j) + a.Hy.at(i, j) - a.Hy.at(i - 1, j)) + a.dteps * zeroJ);
-    }
+    update_e_static<T, COMP>(a, b, zeroJ);
   } else if (b < a.nbS + a.nbC) {
     const int k = (b - a.nbS) * blockDim.x + threadIdx.x;
     if (k >= a.ncells) return;
@@ -433,8 +548,8 @@ int exchange_count(int L0, int L1, int which) {
 
 template <class T>
 int sub_grid(FieldArgsT<T> &a) {
-  if (a.tx <= 0 || a.ty <= 0 || a.tx * a.ty != 256) { a.tx = 32; a.ty = 8; }
-  a.tilesX = (a.Nx + a.tx - 1) / a.tx;
+  if (a.tx <= 0 || a.ty <= 0 || a.tx * a.ty != 256 || a.tx % 32) { a.tx = 32; a.ty = 8; }
+  a.tilesX = (a.Nx + 2 + a.tx * (16 / (int)sizeof(T)) - 1) / (a.tx * (16 / (int)sizeof(T)));
   a.nbS = a.tilesX * ((a.Ny + a.ty - 1) / a.ty);
   a.nbC = (a.ncells + 255) / 256;
   const int nbM = (a.L0 * a.L1 + 255) / 256;
