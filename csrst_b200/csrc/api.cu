@@ -308,7 +308,6 @@ PushArgs push_args(csrst_handle *h, int jcomp) {
   a.h0 = h->b.hr0; a.h1 = h->b.hr1; a.dt = h->dt;
   a.bz = h->cfg.bz; a.Lb = h->b.Lb; a.hw = 0.5 * h->b.w;
   a.chh = h->chh; a.shh = h->shh; a.bwidth = h->bwidth;
-  a.use_smem = 1;
   return a;
 }
 
@@ -330,7 +329,10 @@ Push32Args push_args32(csrst_handle *h, int jcomp) {
   a.org0 = h->b.org0; a.org1 = h->b.org1;
   a.bz = h->cfg.bz; a.Lb = h->b.Lb; a.hw = 0.5 * h->b.w;
   a.chh = h->chh; a.shh = h->shh; a.bwidth = h->bwidth;
-  a.use_smem = 1;
+  // the FP64 bunch copy (diagnostics scratch, 4 n doubles) carries the
+  // move -> deposit hand-over inside a push
+  a.dep_r0 = h->d64;
+  a.dep_cell = reinterpret_cast<int *>(h->d64 + 2 * (size_t)h->n);
   return a;
 }
 
@@ -340,7 +342,7 @@ int push_async(csrst_handle *h, int jcomp) {
   if (h->fp32) {
     if (!bb_ok) launch_bbox32(h->b32, h->P0, h->P1, h->kh0, h->kh1, h->pending ? 1 : 0, h->ws, h->s);
     launch_prep32(h->ws, h->order, h->s);
-    launch_push32(push_args32(h, jcomp), h->order, h->L0, h->L1, h->push_grid, h->s);
+    launch_push32(push_args32(h, jcomp), h->order, h->s);
     launch_bounds32(h->ws, h->s);
     h->pending = false;
     h->fresh = false;
@@ -354,7 +356,7 @@ int push_async(csrst_handle *h, int jcomp) {
   }
   if (!bb_ok) launch_bbox_next(h->x, h->y, h->px, h->py, h->n, h->half, h->pending, h->ws, h->s);
   launch_push_prep(h->ws, h->b.hr0, h->b.hr1, h->order, h->s);
-  launch_push(push_args(h, jcomp), h->order, h->L0, h->L1, h->push_grid, h->s);
+  launch_push(push_args(h, jcomp), h->order, h->push_grid, h->s);
   launch_global_bounds(h->ws, h->b.hr0, h->b.hr1, h->s);
   h->pending = false;
   h->fresh = false;
@@ -538,7 +540,7 @@ int csrst_create(const csrst_config *cfg, csrst_handle **out) {
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  h->push_grid = 2 * sms;
+  h->push_grid = 3 * sms;  // single-member FP64 push: three CTAs per SM
   *out = h;
   return CSRST_OK;
 }

@@ -80,6 +80,7 @@ __device__ __forceinline__ void half_h_static(const FieldArgsT<T> &a, int b) {
   int c, j;
   if (!static_vec(a, b, c, j)) return;
   const bool live = c <= a.Nx + 1;
+  const unsigned m = live ? static_mask(a, c, j) : 0u;  // in flight with the plane loads
   T *hxp = &a.Hx.at(c - 1, j), *hyp = &a.Hy.at(c - 1, j);
   Vec16<T> ey{}, ex0{}, ex1{}, hx{}, hy{};
   if (live) {
@@ -90,8 +91,6 @@ __device__ __forceinline__ void half_h_static(const FieldArgsT<T> &a, int b) {
     hy = ld16(hyp);
   }
   T eyn = __shfl_down_sync(0xffffffffu, ey.v[0], 1);
-  if (!live) return;
-  const unsigned m = static_mask(a, c, j);
   if (!m) return;
   if ((threadIdx.x & 31) == 31 && c + V <= a.Nx + 1) eyn = a.Ey.at(c + V - 1, j);
 #pragma unroll
@@ -141,6 +140,7 @@ __device__ __forceinline__ void update_e_static(const FieldArgsT<T> &a, int b, T
   int c, j;
   if (!static_vec(a, b, c, j)) return;
   const bool live = c <= a.Nx + 1;
+  const unsigned m = live ? static_mask(a, c, j) : 0u;  // in flight with the plane loads
   T *ep = COMP == 0 ? &a.Ex.at(c - 1, j) : &a.Ey.at(c - 1, j);
   Vec16<T> e{}, hx{}, hy{}, hxm{}, hym{};
   if (live) {
@@ -157,8 +157,6 @@ __device__ __forceinline__ void update_e_static(const FieldArgsT<T> &a, int b, T
     hxp = __shfl_up_sync(0xffffffffu, hx.v[V - 1], 1);
     hyp = __shfl_up_sync(0xffffffffu, hy.v[V - 1], 1);
   }
-  if (!live) return;
-  const unsigned m = static_mask(a, c, j);
   if (!m) return;
   if (COMP == 1 && (threadIdx.x & 31) == 0 && c >= 1) {
     hxp = a.Hx.at(c - 2, j);

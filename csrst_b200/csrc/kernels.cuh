@@ -24,7 +24,6 @@ struct PushArgs {
   double h0, h1, dt;
   // hard-edge dipole (Bend::getExternalField, Bend.cpp:865-907)
   double bz, Lb, hw, chh, shh, bwidth;
-  int use_smem;
 };
 
 // One field sub-step over the static mesh, the cut cells and the window.
@@ -99,7 +98,7 @@ void launch_push_batch(const PushGroup *groups, int ngroups, int m, int grid, co
 void launch_bbox_next(const double *x, const double *y, const double *px, const double *py, long long n,
                       double half, int pending, WinState *ws, cudaStream_t s);
 void launch_push_prep(WinState *ws, double h0, double h1, int order, cudaStream_t s);
-void launch_push(const PushArgs &a, int order, int L0, int L1, int grid, cudaStream_t s);
+void launch_push(const PushArgs &a, int order, int grid, cudaStream_t s);
 void launch_global_bounds(WinState *ws, double h0, double h1, cudaStream_t s);
 void launch_drift(double *x, double *y, const double *px, const double *py, long long n, double full,
                   cudaStream_t s);
@@ -208,10 +207,13 @@ struct Push32Args {
   double h0, h1, dt;                   // spacing and time step (current scale)
   double org0, org1;                   // static mesh origin (dipole position)
   double bz, Lb, hw, chh, shh, bwidth; // hard-edge dipole
-  int use_smem;
+  // single-member push: the move's hand-over to the deposit, n entries each
+  // (deposit start R0 in cells from the old cell, NaN if not moved; old cell)
+  double *dep_r0;                      // 2 n
+  int *dep_cell;                       // n
 };
 
-int launch_push32(const Push32Args &a, int order, int L0, int L1, int grid, cudaStream_t s);
+int launch_push32(const Push32Args &a, int order, cudaStream_t s);
 long long push32_batch_smem_limit();
 void launch_push32_batch(const PushGroup *groups, int ngroups, int m, int grid, const PrepArgs *prep,
                          cudaStream_t s, int parts = 3);

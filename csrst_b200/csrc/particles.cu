@@ -212,14 +212,21 @@ __device__ __forceinline__ void push_body(const PushArgs &a, long long beg, long
   __syncthreads();
 }
 
-template <int ORDER, bool SMEM>
-__global__ void __launch_bounds__(256, 2) k_push(PushArgs a) {
+// The single-member push: warp tiles in dynamic shared memory, the window
+// accumulator in global memory, three CTAs per SM.  The push is bound by the
+// latency of dependent FP64 chains; a CTA copy of the accumulator in shared
+// memory held the SM to two CTAs and cost more to zero and flush than the
+// global adds it saved (4e6-particle TSC bunch, 8192 x 1024 mesh: 0.55 ->
+// 0.44 ms per push).  Integer sums: the result does not depend on where
+// they are added.
+template <int ORDER>
+__global__ void __launch_bounds__(256, 3) k_push(PushArgs a) {
   extern __shared__ unsigned long long sacc[];
   __shared__ PushShared sh;
   const long long per = (a.n + gridDim.x - 1) / gridDim.x;
   const long long beg = (long long)blockIdx.x * per;
   const long long end = beg + per < a.n ? beg + per : a.n;
-  push_body<ORDER, SMEM>(a, beg, end, sh, sacc);
+  push_body<ORDER, false>(a, beg, end, sh, sacc);
 }
 
 // One push over a batch of members: the members' particles form one index
@@ -399,41 +406,24 @@ void launch_push_batch(const PushGroup *groups, int ngroups, int m, int grid, co
   }
 }
 
-// Largest dynamic shared memory the window accumulator may use for this
-// kernel: the opt-in per-block limit minus the kernel's static shared memory.
+// Dynamic shared memory of the single-member push: its warp tiles (48-56 KB,
+// above the 48 KB a launch gets without opting in).
 template <int ORDER>
-static long long push_smem_limit() {
-  static long long lim = -1;
-  if (lim < 0) {
-    int dev = 0, v = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-    cudaFuncAttributes fa{};
-    cudaFuncGetAttributes(&fa, k_push<ORDER, true>);
-    lim = (long long)v - (long long)fa.sharedSizeBytes;
-    if (cudaFuncSetAttribute(k_push<ORDER, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lim) !=
-        cudaSuccess)
-      lim = 0;  // use the global-atomic variant
-    cudaGetLastError();
-  }
-  return lim;
-}
-
-template <int ORDER>
-static void push_order(const PushArgs &a, int L0, int L1, int grid, cudaStream_t s) {
+static size_t push_smem() {
+  static int set = 0;
   const size_t tiles = (size_t)TileFor<ORDER>::T::kSize * 256 * sizeof(unsigned long long);
-  const size_t sm = (size_t)L0 * L1 * sizeof(unsigned long long) + tiles;
-  if (a.use_smem && (long long)sm <= push_smem_limit<ORDER>()) {
-    k_push<ORDER, true><<<grid, 256, sm, s>>>(a);
-  } else {
-    k_push<ORDER, false><<<grid, 256, tiles, s>>>(a);
+  if (!set) {
+    cudaFuncSetAttribute(k_push<ORDER>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tiles);
+    cudaGetLastError();
+    set = 1;
   }
+  return tiles;
 }
 
-void launch_push(const PushArgs &a, int order, int L0, int L1, int grid, cudaStream_t s) {
-  if (order == 0) push_order<0>(a, L0, L1, grid, s);
-  else if (order == 1) push_order<1>(a, L0, L1, grid, s);
-  else push_order<2>(a, L0, L1, grid, s);
+void launch_push(const PushArgs &a, int order, int grid, cudaStream_t s) {
+  if (order == 0) k_push<0><<<grid, 256, push_smem<0>(), s>>>(a);
+  else if (order == 1) k_push<1><<<grid, 256, push_smem<1>(), s>>>(a);
+  else k_push<2><<<grid, 256, push_smem<2>(), s>>>(a);
   k_push_post<<<1, 32, 0, s>>>(a.ws);
 }
 

@@ -72,156 +72,298 @@ __device__ __forceinline__ void store_pos(double t0, double t1, int ci, int cj, 
   o0 = a0; o1 = a1;
 }
 
-// One CTA's share [beg, end) of one push; called by all threads of the CTA,
-// ends with a barrier (a CTA may run it for several members in turn).
+// One particle's move: gather at R1, kick + rotation, drift to R2, R2 stored
+// (cell + FP32 offset) and the new momentum deviation stored.  On return,
+// when ok: r0 = R0 (deposit start) and e = R2 (end, as stored) in cells from
+// the old cell (ci, cj); (ni, nj) the new cell and w the half drift of the
+// new momentum.  Particles that fail the window-fit checks set the member's
+// error and come back with ok false, unchanged.
+struct Move32 {
+  bool ok;
+  int ci, cj, ni, nj;
+  double r00, r01, e0, e1, w0, w1, q;
+  float o0, o1;
+};
+
+template <int ORDER_OF_PUSH>
+__device__ __forceinline__ void move32(const Push32Args &a, long long n, bool ok, int L0, int L1, int WP0, int WP1,
+                                       Move32 &m) {
+  WinState *ws = a.ws;
+  const int wp = a.wpitch;
+  const double P0 = a.P0, P1 = a.P1;
+  const float Pf0 = (float)P0, Pf1 = (float)P1;
+  int ci = 0, cj = 0;
+  double s0 = 0.0, s1 = 0.0, q = 0.0;
+  float d0 = 0.0f, d1 = 0.0f;
+  if (ok) {
+    unpack(a.b.cell[n], ci, cj);
+    s0 = a.b.ox[n]; s1 = a.b.oy[n];
+    d0 = a.b.dpx[n]; d1 = a.b.dpy[n];
+    q = a.b.q[n];
+    if (!(isfinite(d0) && isfinite(d1) && s0 >= 0.0 && s0 < 1.0 && s1 >= 0.0 && s1 < 1.0)) {
+      set_err(ws, kErrWindowFit);
+      ok = false;
+    }
+  }
+  double p0 = 0.0, p1 = 0.0, w0 = 0.0, w1 = 0.0, r00 = 0.0, r01 = 0.0, x0 = 0.0, x1 = 0.0;
+  if (ok) {
+    const float r = rgam(P0, P1, d0, d1, p0, p1);
+    w0 = half_drift(a.kh0, p0, r); w1 = half_drift(a.kh1, p1, r);
+    r00 = s0; r01 = s1;
+    if (a.pending) { r00 = dsub(s0, w0); r01 = dsub(s1, w1); }  // drift_particles(-dt/2)
+    x0 = dadd(r00, w0); x1 = dadd(r01, w1);                     // R1, cells from (ci, cj)
+    const int wi = ci - WP0, wj = cj - WP1;
+    // gather (FieldPatch::gather x3) anchored at the window cell of R1; the
+    // offset inside it is clamped below 1 so that FP32 rounding cannot move
+    // the stencil to the next cell (the window-fit check counts cells in FP64)
+    const double c0 = floor(x0), c1 = floor(x1);
+    const int ai = wi + (int)c0, aj = wj + (int)c1;
+    if (ai - 2 < -1 || ai + 2 > L0 || aj - 2 < -1 || aj + 2 > L1) {  // stencil outside the window planes
+      set_err(ws, kErrWindowFit);
+      ok = false;
+    } else {
+      const float g0 = fminf((float)(x0 - c0), 0x1.fffffep-1f), g1 = fminf((float)(x1 - c1), 0x1.fffffep-1f);
+      const size_t o = (size_t)(aj + 1) * wp + (ai + 1);
+      const View32 vex{a.mEx + o, wp}, vey{a.mEy + o, wp}, vhx{a.mHx + o, wp}, vhy{a.mHy + o, wp};
+      const float E0 = gather_edge<ORDER_OF_PUSH>(vex, g0, g1, 0);
+      const float E1 = gather_edge<ORDER_OF_PUSH>(vey, g0, g1, 1);
+      const float Hf = gather_cell<ORDER_OF_PUSH>(SumView32{vhx, vhy}, g0, g1);
+      // hard-edge dipole at the absolute position of R1
+      const double X = a.org0 + ((double)ci + x0) * a.h0, Y = a.org1 + ((double)cj + x1) * a.h1;
+      const double dist = a.chh * (X - a.Lb) - a.shh * (Y - a.hw);
+      const float bext = (dist > 0.0 && dist < a.bwidth) ? (float)a.bz : 0.0f;
+      const float B = (float)kMu0 * Hf + 0.5f * bext;
+      // kick + rotation (PartBunch.cpp:366-383) on u - P
+      const float k0 = a.f1 * E0, k1 = a.f1 * E1;
+      const float du0 = d0 + k0, du1 = d1 + k1;
+      double U0, U1;
+      const float ru = rgam(P0, P1, du0, du1, U0, U1);
+      const float aa = a.f2 * B * ru;
+      const float sv0 = du0 + aa * (Pf1 + du1), sv1 = du1 - aa * (Pf0 + du0);  // s - P
+      const float cf = aa / (1.0f + aa * aa);
+      d0 = (sv0 + cf * (Pf1 + sv1)) + k0;
+      d1 = (sv1 - cf * (Pf0 + sv0)) + k1;
+      a.b.dpx[n] = d0; a.b.dpy[n] = d1;
+    }
+  }
+  m.ok = ok;
+  m.ci = ci; m.cj = cj; m.r00 = r00; m.r01 = r01; m.q = q;
+  m.ni = 0; m.nj = 0; m.e0 = 0.0; m.e1 = 0.0; m.o0 = 0.0f; m.o1 = 0.0f; m.w0 = 0.0; m.w1 = 0.0;
+  if (ok) {
+    const float r = rgam(P0, P1, d0, d1, p0, p1);
+    w0 = half_drift(a.kh0, p0, r); w1 = half_drift(a.kh1, p1, r);
+    int nc;
+    float o0, o1;
+    store_pos(dadd(x0, w0), dadd(x1, w1), ci, cj, nc, o0, o1);  // R2
+    a.b.cell[n] = nc; a.b.ox[n] = o0; a.b.oy[n] = o1;
+    // the move ends at the stored (FP32-rounded) position, so that every
+    // move's current conserves charge for the positions the bunch holds
+    unpack(nc, m.ni, m.nj);
+    m.e0 = (double)(m.ni - ci) + (double)o0; m.e1 = (double)(m.nj - cj) + (double)o1;
+    m.o0 = o0; m.o1 = o1; m.w0 = w0; m.w1 = w1;
+  }
+}
+
+// Boxes of one moved particle: R0 u R2 (the deposit bounds) and the next
+// push's gather position.  Boxes hold cell index + 0.5: only the cells are
+// used, and a cell-relative coordinate added to a large index could round
+// across a cell border.
+struct Boxes32 {
+  double amn0 = INFINITY, amn1 = INFINITY, amx0 = -INFINITY, amx1 = -INFINITY;  // R0 u R2 (cells)
+  double bmn0 = INFINITY, bmn1 = INFINITY, bmx0 = -INFINITY, bmx1 = -INFINITY;  // next R1 (cells)
+  __device__ __forceinline__ void add(const Move32 &m) {
+    amn0 = fmin(amn0, cellc(m.ci, fmin(m.r00, m.e0))); amn1 = fmin(amn1, cellc(m.cj, fmin(m.r01, m.e1)));
+    amx0 = fmax(amx0, cellc(m.ci, fmax(m.r00, m.e0))); amx1 = fmax(amx1, cellc(m.cj, fmax(m.r01, m.e1)));
+    // next push gathers at (stored R2 - w) + w
+    const double n0 = cellc(m.ni, dadd(dsub((double)m.o0, m.w0), m.w0));
+    const double n1 = cellc(m.nj, dadd(dsub((double)m.o1, m.w1), m.w1));
+    bmn0 = fmin(bmn0, n0); bmn1 = fmin(bmn1, n1); bmx0 = fmax(bmx0, n0); bmx1 = fmax(bmx1, n1);
+  }
+  __device__ __forceinline__ void store(WinState *ws, PushShared &sh) {
+    block_bbox(amn0, amn1, amx0, amx1, ws->bball, sh.sb);
+    block_bbox(bmn0, bmn1, bmx0, bmx1, ws->bb[1 - ws->cur], sh.sb);
+  }
+};
+
+// Deposit state of one CTA: the warp tiles and, with SMEM, the CTA's copy of
+// the window accumulator (flushed into the member's at the end).
+template <int ORDER, bool SMEM>
+struct Depositor32 {
+  using Tile = typename TileFor<ORDER>::T;
+  Tile tile;
+  unsigned long long *win, *sacc;
+  int L0, L1;
+  double scale;
+  bool overflow = false;
+
+  // Called by all threads of the CTA; ends with a barrier.
+  __device__ __forceinline__ void begin(const Push32Args &a, unsigned long long *sm, PushShared &sh, int l0,
+                                        int l1) {
+    L0 = l0; L1 = l1; sacc = sm; scale = a.acc_scale;
+    win = SMEM ? sm : a.acc;
+    unsigned long long *tmem = SMEM ? sm + L0 * L1 : sm;
+    if (SMEM)
+      for (int k = threadIdx.x; k < L0 * L1; k += blockDim.x) sm[k] = 0ull;
+    for (int k = threadIdx.x; k < Tile::kSize * (int)blockDim.x; k += blockDim.x) tmem[k] = 0ull;
+    if (threadIdx.x == 0) { sh.tb[0] = L0; sh.tb[1] = L1; sh.tb[2] = -1; sh.tb[3] = -1; }
+    __syncthreads();
+    tile.init(tmem, L0, L1);
+  }
+
+  // Current of one move R0 -> R2 (cells from the old cell, whose window cell
+  // is (wi, wj)), FP64 weights summed in the warp's tile.  Called by all
+  // lanes of the warp together (has: this lane has a particle).
+  __device__ __forceinline__ void particle(const Push32Args &a, bool has, int wi, int wj, double q, double r00,
+                                           double r01, double e0, double e1) {
+    tile.template rebase<SMEM>(has, has ? wi + (int)floor(r00) : 0, has ? wj + (int)floor(r01) : 0, win, L0, L1);
+    if (has) {
+      auto sink = [&](int i, int j, double v) {
+        tile.template add<SMEM>(i + wi, j + wj, __double2ll_rn(v * scale), win, L0, L1);
+      };
+      if (!deposit_particle<ORDER>(a.jcomp, q, r00, r01, e0, e1, 0.0, 0.0, 1.0, 1.0, a.h0, a.h1, a.dt, sink))
+        overflow = true;
+    }
+  }
+
+  // Called by all threads of the CTA (after their last particle(), before
+  // any other use of sh.sb); ends with a barrier.
+  __device__ __forceinline__ void end(const Push32Args &a, PushShared &sh) {
+    tile.template flush<SMEM>(win, L0, L1);
+    if (overflow) set_err(a.ws, kErrCrossings);
+    if (SMEM) {
+      if (tile.ti1 >= 0) {
+        atomicMin(&sh.tb[0], tile.ti0); atomicMin(&sh.tb[1], tile.tj0);
+        atomicMax(&sh.tb[2], tile.ti1); atomicMax(&sh.tb[3], tile.tj1);
+      }
+      __syncthreads();
+      const int i0 = sh.tb[0], j0 = sh.tb[1], i1 = sh.tb[2], j1 = sh.tb[3];
+      if (i1 >= i0) {
+        const int w = i1 - i0 + 1, cnt = w * (j1 - j0 + 1);
+        for (int k = threadIdx.x; k < cnt; k += blockDim.x) {
+          const int i = i0 + k % w, j = j0 + k / w;
+          const unsigned long long v = sacc[j * L0 + i];
+          if (v) atomicAdd(&a.acc[j * L0 + i], v);
+        }
+      }
+    }
+    __syncthreads();
+  }
+};
+
+// The member's sticky error at entry, read by one thread for the CTA; a CTA
+// that sees one leaves as a whole.
+__device__ __forceinline__ bool entry_error(WinState *ws, PushShared &sh) {
+  if (threadIdx.x == 0) sh.err = *(volatile int *)&ws->err;
+  __syncthreads();
+  return sh.err != 0;
+}
+
+// One CTA's share [beg, end) of one fused push (move + deposit); called by
+// all threads of the CTA, ends with a barrier (a CTA may run it for several
+// members in turn).
 template <int ORDER, bool SMEM>
 __device__ __forceinline__ void push32_body(const Push32Args &a, long long beg, long long end, PushShared &sh,
                                             unsigned long long *sacc) {
-  int *tb = sh.tb;
+  if (entry_error(a.ws, sh)) return;  // the whole CTA leaves together
   WinState *ws = a.ws;
-  if (threadIdx.x == 0) sh.err = *(volatile int *)&ws->err;
-  __syncthreads();
-  if (sh.err) return;  // the whole CTA leaves together
   const int L0 = ws->L0, L1 = ws->L1, WP0 = ws->P0, WP1 = ws->P1;
-  using Tile = typename TileFor<ORDER>::T;
-  unsigned long long *win = SMEM ? sacc : a.acc;
-  unsigned long long *tmem = SMEM ? sacc + L0 * L1 : sacc;
-  if (SMEM)
-    for (int k = threadIdx.x; k < L0 * L1; k += blockDim.x) sacc[k] = 0ull;
-  for (int k = threadIdx.x; k < Tile::kSize * (int)blockDim.x; k += blockDim.x) tmem[k] = 0ull;
-  if (threadIdx.x == 0) { tb[0] = L0; tb[1] = L1; tb[2] = -1; tb[3] = -1; }
-  __syncthreads();
-  Tile tile;
-  tile.init(tmem, L0, L1);
-  const int wp = a.wpitch;
-  const double scale = a.acc_scale;
-  double amn0 = INFINITY, amn1 = INFINITY, amx0 = -INFINITY, amx1 = -INFINITY;  // R0 u R2 (cells)
-  double bmn0 = INFINITY, bmn1 = INFINITY, bmx0 = -INFINITY, bmx1 = -INFINITY;  // next R1 (cells)
-  bool overflow = false;
-  int wi = 0, wj = 0;  // window cell of the particle being deposited
-  auto sink = [&](int i, int j, double v) {
-    tile.template add<SMEM>(i + wi, j + wj, __double2ll_rn(v * scale), win, L0, L1);
-  };
-  const double P0 = a.P0, P1 = a.P1;
-  const float Pf0 = (float)P0, Pf1 = (float)P1;
+  Depositor32<ORDER, SMEM> dep;
+  dep.begin(a, sacc, sh, L0, L1);
+  Boxes32 box;
   const long long rounds = end > beg ? (end - beg + blockDim.x - 1) / blockDim.x : 0;
   for (long long it = 0; it < rounds; ++it) {  // the same rounds for every lane
     const long long n = beg + it * blockDim.x + threadIdx.x;
-    bool ok = n < end;
-    int ci = 0, cj = 0;
-    double s0 = 0.0, s1 = 0.0, q = 0.0;
-    float d0 = 0.0f, d1 = 0.0f;
-    if (ok) {
-      unpack(a.b.cell[n], ci, cj);
-      s0 = a.b.ox[n]; s1 = a.b.oy[n];
-      d0 = a.b.dpx[n]; d1 = a.b.dpy[n];
-      q = a.b.q[n];
-      if (!(isfinite(d0) && isfinite(d1) && s0 >= 0.0 && s0 < 1.0 && s1 >= 0.0 && s1 < 1.0)) {
-        set_err(ws, kErrWindowFit);
-        ok = false;
-      }
-    }
-    double p0 = 0.0, p1 = 0.0, w0 = 0.0, w1 = 0.0, r00 = 0.0, r01 = 0.0, x0 = 0.0, x1 = 0.0;
-    if (ok) {
-      const float r = rgam(P0, P1, d0, d1, p0, p1);
-      w0 = half_drift(a.kh0, p0, r); w1 = half_drift(a.kh1, p1, r);
-      r00 = s0; r01 = s1;
-      if (a.pending) { r00 = dsub(s0, w0); r01 = dsub(s1, w1); }  // drift_particles(-dt/2)
-      x0 = dadd(r00, w0); x1 = dadd(r01, w1);                     // R1, cells from (ci, cj)
-      wi = ci - WP0; wj = cj - WP1;
-      // gather (FieldPatch::gather x3) anchored at the window cell of R1; the
-      // offset inside it is clamped below 1 so that FP32 rounding cannot move
-      // the stencil to the next cell (the window-fit check counts cells in FP64)
-      const double c0 = floor(x0), c1 = floor(x1);
-      const int ai = wi + (int)c0, aj = wj + (int)c1;
-      if (ai - 2 < -1 || ai + 2 > L0 || aj - 2 < -1 || aj + 2 > L1) {  // stencil outside the window planes
-        set_err(ws, kErrWindowFit);
-        ok = false;
-      } else {
-        const float g0 = fminf((float)(x0 - c0), 0x1.fffffep-1f), g1 = fminf((float)(x1 - c1), 0x1.fffffep-1f);
-        const size_t o = (size_t)(aj + 1) * wp + (ai + 1);
-        const View32 vex{a.mEx + o, wp}, vey{a.mEy + o, wp}, vhx{a.mHx + o, wp}, vhy{a.mHy + o, wp};
-        const float E0 = gather_edge<ORDER>(vex, g0, g1, 0);
-        const float E1 = gather_edge<ORDER>(vey, g0, g1, 1);
-        const float Hf = gather_cell<ORDER>(SumView32{vhx, vhy}, g0, g1);
-        // hard-edge dipole at the absolute position of R1
-        const double X = a.org0 + ((double)ci + x0) * a.h0, Y = a.org1 + ((double)cj + x1) * a.h1;
-        const double dist = a.chh * (X - a.Lb) - a.shh * (Y - a.hw);
-        const float bext = (dist > 0.0 && dist < a.bwidth) ? (float)a.bz : 0.0f;
-        const float B = (float)kMu0 * Hf + 0.5f * bext;
-        // kick + rotation (PartBunch.cpp:366-383) on u - P
-        const float k0 = a.f1 * E0, k1 = a.f1 * E1;
-        const float du0 = d0 + k0, du1 = d1 + k1;
-        double U0, U1;
-        const float ru = rgam(P0, P1, du0, du1, U0, U1);
-        const float aa = a.f2 * B * ru;
-        const float sv0 = du0 + aa * (Pf1 + du1), sv1 = du1 - aa * (Pf0 + du0);  // s - P
-        const float cf = aa / (1.0f + aa * aa);
-        d0 = (sv0 + cf * (Pf1 + sv1)) + k0;
-        d1 = (sv1 - cf * (Pf0 + sv0)) + k1;
-        a.b.dpx[n] = d0; a.b.dpy[n] = d1;
-      }
-    }
-    int ni = 0, nj = 0;
-    double e0 = 0.0, e1 = 0.0;
-    float o0 = 0.0f, o1 = 0.0f;
-    if (ok) {
-      const float r = rgam(P0, P1, d0, d1, p0, p1);
-      w0 = half_drift(a.kh0, p0, r); w1 = half_drift(a.kh1, p1, r);
-      int nc;
-      store_pos(dadd(x0, w0), dadd(x1, w1), ci, cj, nc, o0, o1);  // R2
-      a.b.cell[n] = nc; a.b.ox[n] = o0; a.b.oy[n] = o1;
-      // the move ends at the stored (FP32-rounded) position, so that every
-      // move's current conserves charge for the positions the bunch holds
-      unpack(nc, ni, nj);
-      e0 = (double)(ni - ci) + (double)o0; e1 = (double)(nj - cj) + (double)o1;
-    }
-    // current deposit R0 -> R2 in cells from (ci, cj), FP64 weights, summed in
-    // the warp's tile
-    tile.template rebase<SMEM>(ok, ok ? wi + (int)floor(r00) : 0, ok ? wj + (int)floor(r01) : 0, win, L0, L1);
-    if (ok) {
-      if (!deposit_particle<ORDER>(a.jcomp, q, r00, r01, e0, e1, 0.0, 0.0, 1.0, 1.0, a.h0, a.h1, a.dt, sink))
-        overflow = true;
-      // boxes hold cell index + 0.5: only the cells are used, and a cell-relative
-      // coordinate added to a large index could round across a cell border
-      amn0 = fmin(amn0, cellc(ci, fmin(r00, e0))); amn1 = fmin(amn1, cellc(cj, fmin(r01, e1)));
-      amx0 = fmax(amx0, cellc(ci, fmax(r00, e0))); amx1 = fmax(amx1, cellc(cj, fmax(r01, e1)));
-      // next push gathers at (stored R2 - w) + w
-      const double n0 = cellc(ni, dadd(dsub((double)o0, w0), w0)), n1 = cellc(nj, dadd(dsub((double)o1, w1), w1));
-      bmn0 = fmin(bmn0, n0); bmn1 = fmin(bmn1, n1); bmx0 = fmax(bmx0, n0); bmx1 = fmax(bmx1, n1);
-    }
+    Move32 m;
+    move32<ORDER>(a, n, n < end, L0, L1, WP0, WP1, m);
+    dep.particle(a, m.ok, m.ci - WP0, m.cj - WP1, m.q, m.r00, m.r01, m.e0, m.e1);
+    if (m.ok) box.add(m);
   }
-  tile.template flush<SMEM>(win, L0, L1);
-  if (overflow) set_err(ws, kErrCrossings);
-  block_bbox(amn0, amn1, amx0, amx1, ws->bball, sh.sb);
-  block_bbox(bmn0, bmn1, bmx0, bmx1, ws->bb[1 - ws->cur], sh.sb);
-  if (SMEM) {
-    if (tile.ti1 >= 0) {
-      atomicMin(&tb[0], tile.ti0); atomicMin(&tb[1], tile.tj0);
-      atomicMax(&tb[2], tile.ti1); atomicMax(&tb[3], tile.tj1);
-    }
-    __syncthreads();
-    const int i0 = tb[0], j0 = tb[1], i1 = tb[2], j1 = tb[3];
-    if (i1 >= i0) {
-      const int w = i1 - i0 + 1, cnt = w * (j1 - j0 + 1);
-      for (int k = threadIdx.x; k < cnt; k += blockDim.x) {
-        const int i = i0 + k % w, j = j0 + k / w;
-        const unsigned long long v = sacc[j * L0 + i];
-        if (v) atomicAdd(&a.acc[j * L0 + i], v);
-      }
-    }
-  }
+  dep.end(a, sh);
+  box.store(ws, sh);
   __syncthreads();
 }
 
-template <int ORDER, bool SMEM>
-__global__ void __launch_bounds__(256, 2) k_push32(Push32Args a) {
+// The single-member FP32 push in two launches.  k_push32_move moves every
+// particle (gather, kick, drift, stores, boxes) with no shared memory at
+// three CTAs per SM, and leaves for the deposit each particle's start R0
+// and old cell in a.dep_r0 / a.dep_cell (NaN for a particle it did not
+// move).  k_push32_dep then adds the current of every move R0 -> R2 exactly
+// as the fused push does, CTA by CTA over contiguous (cell-sorted) ranges,
+// also at three CTAs per SM.  Both are bound by the latency of dependent
+// FP64 chains, not by bytes: split, each runs at 24 warps per SM where the
+// fused push's registers and shared memory allowed 16 (4e6-particle TSC
+// bunch, 8192 x 1024 mesh: 0.50 -> 0.41 ms per push).  The extra traffic is
+// 20 bytes written and 36 read per particle.
+template <int ORDER>
+__global__ void __launch_bounds__(256, 3) k_push32_move(Push32Args a) {
+  __shared__ PushShared sh;
+  if (entry_error(a.ws, sh)) return;
+  WinState *ws = a.ws;
+  const int L0 = ws->L0, L1 = ws->L1, WP0 = ws->P0, WP1 = ws->P1;
+  Boxes32 box;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  const long long rounds = (a.b.n + stride - 1) / stride;
+  for (long long it = 0; it < rounds; ++it) {
+    const long long n = it * stride + blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (n >= a.b.n) continue;
+    Move32 m;
+    move32<ORDER>(a, n, true, L0, L1, WP0, WP1, m);
+    a.dep_r0[2 * n] = m.ok ? m.r00 : NAN;
+    a.dep_r0[2 * n + 1] = m.r01;
+    a.dep_cell[n] = (m.ci & 0xffff) | (m.cj << 16);
+    if (m.ok) box.add(m);
+  }
+  box.store(ws, sh);
+}
+
+template <int ORDER>
+__global__ void __launch_bounds__(256, 3) k_push32_dep(Push32Args a) {
+  constexpr bool SMEM = false;
   extern __shared__ unsigned long long sacc[];
   __shared__ PushShared sh;
+  if (entry_error(a.ws, sh)) return;
+  WinState *ws = a.ws;
+  const int L0 = ws->L0, L1 = ws->L1, WP0 = ws->P0, WP1 = ws->P1;
   const long long per = (a.b.n + gridDim.x - 1) / gridDim.x;
   const long long beg = (long long)blockIdx.x * per;
   const long long end = beg + per < a.b.n ? beg + per : a.b.n;
-  push32_body<ORDER, SMEM>(a, beg, end, sh, sacc);
+  Depositor32<ORDER, SMEM> dep;
+  dep.begin(a, sacc, sh, L0, L1);
+  // a round's inputs are loaded together, one round ahead, so that their
+  // latency overlaps the deposit of the round before
+  struct In {
+    double2 r0;
+    int c0, c1;
+    float o0, o1, q;
+  };
+  auto load = [&](long long n, In &v) {
+    if (n < end) {
+      v.r0 = reinterpret_cast<const double2 *>(a.dep_r0)[n];
+      v.c0 = a.dep_cell[n]; v.c1 = a.b.cell[n];
+      v.o0 = a.b.ox[n]; v.o1 = a.b.oy[n]; v.q = a.b.q[n];
+    } else {
+      v.r0.x = NAN; v.r0.y = 0.0; v.c0 = v.c1 = 0; v.o0 = v.o1 = v.q = 0.0f;
+    }
+  };
+  const long long rounds = end > beg ? (end - beg + blockDim.x - 1) / blockDim.x : 0;
+  In cur, nxt;
+  load(beg + threadIdx.x, cur);
+  for (long long it = 0; it < rounds; ++it) {
+    if (it + 1 < rounds) load(beg + (it + 1) * blockDim.x + threadIdx.x, nxt);
+    const bool has = !isnan(cur.r0.x);
+    double e0 = 0.0, e1 = 0.0;
+    int ci = 0, cj = 0;
+    if (has) {
+      unpack(cur.c0, ci, cj);
+      int ni, nj;
+      unpack(cur.c1, ni, nj);
+      e0 = (double)(ni - ci) + (double)cur.o0;
+      e1 = (double)(nj - cj) + (double)cur.o1;
+    }
+    dep.particle(a, has, ci - WP0, cj - WP1, (double)cur.q, cur.r0.x, cur.r0.y, e0, e1);
+    cur = nxt;
+  }
+  dep.end(a, sh);
 }
 
 // One push over a batch of FP32-mode members (see k_push_batch).
@@ -400,40 +542,48 @@ inline unsigned grid_for(long long n, unsigned cap = 4096) {
   return (unsigned)(g < 1 ? 1 : (g > cap ? cap : g));
 }
 
+// The deposit launch keeps only the warp tiles in dynamic shared memory
+// (48-56 KB, above the 48 KB a launch gets without opting in) and adds into
+// the window accumulator in global memory: measured on the 4e6-particle TSC
+// bunch, a CTA copy of the accumulator in shared memory cost more (zeroing,
+// flushing its touched box) than the global adds it saves, and its size kept
+// the SM to two CTAs.
 template <int ORDER>
-long long smem_limit32() {
-  static long long lim = -1;
-  if (lim < 0) {
-    int dev = 0, v = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-    cudaFuncAttributes fa{};
-    cudaFuncGetAttributes(&fa, k_push32<ORDER, true>);
-    lim = (long long)v - (long long)fa.sharedSizeBytes;
-    if (cudaFuncSetAttribute(k_push32<ORDER, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lim) !=
-        cudaSuccess)
-      lim = 0;
+size_t dep_smem32() {
+  static int set = 0;
+  const size_t tiles = (size_t)TileFor<ORDER>::T::kSize * 256 * sizeof(unsigned long long);
+  if (!set) {
+    cudaFuncSetAttribute(k_push32_dep<ORDER>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tiles);
     cudaGetLastError();
+    set = 1;
   }
-  return lim;
+  return tiles;
+}
+
+// CTAs of the move and deposit launches: three per SM.
+int push_grid32() {
+  static int g = 0;
+  if (!g) {
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    g = 3 * (sms > 0 ? sms : 148);
+  }
+  return g;
 }
 
 template <int ORDER>
-void push32_order(const Push32Args &a, int L0, int L1, int grid, cudaStream_t s) {
-  const size_t tiles = (size_t)TileFor<ORDER>::T::kSize * 256 * sizeof(unsigned long long);
-  const size_t sm = (size_t)L0 * L1 * sizeof(unsigned long long) + tiles;
-  if (a.use_smem && (long long)sm <= smem_limit32<ORDER>())
-    k_push32<ORDER, true><<<grid, 256, sm, s>>>(a);
-  else
-    k_push32<ORDER, false><<<grid, 256, tiles, s>>>(a);
+void push32_order(const Push32Args &a, cudaStream_t s) {
+  k_push32_move<ORDER><<<push_grid32(), 256, 0, s>>>(a);
+  k_push32_dep<ORDER><<<push_grid32(), 256, dep_smem32<ORDER>(), s>>>(a);
 }
 
 }  // namespace
 
-int launch_push32(const Push32Args &a, int order, int L0, int L1, int grid, cudaStream_t s) {
-  if (order == 0) push32_order<0>(a, L0, L1, grid, s);
-  else if (order == 1) push32_order<1>(a, L0, L1, grid, s);
-  else push32_order<2>(a, L0, L1, grid, s);
+int launch_push32(const Push32Args &a, int order, cudaStream_t s) {
+  if (order == 0) push32_order<0>(a, s);
+  else if (order == 1) push32_order<1>(a, s);
+  else push32_order<2>(a, s);
   k_post32<<<1, 32, 0, s>>>(a.ws);
   return 0;
 }
