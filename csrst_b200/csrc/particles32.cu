@@ -185,29 +185,24 @@ struct Boxes32 {
   }
 };
 
-// Deposit state of one CTA: the warp tiles and, with SMEM, the CTA's copy of
-// the window accumulator (flushed into the member's at the end).
-template <int ORDER, bool SMEM>
+// Deposit state of one CTA: the warp tiles (dynamic shared memory) over the
+// member's window accumulator in global memory.
+template <int ORDER>
 struct Depositor32 {
   using Tile = typename TileFor<ORDER>::T;
   Tile tile;
-  unsigned long long *win, *sacc;
+  unsigned long long *win;
   int L0, L1;
   double scale;
   bool overflow = false;
 
   // Called by all threads of the CTA; ends with a barrier.
-  __device__ __forceinline__ void begin(const Push32Args &a, unsigned long long *sm, PushShared &sh, int l0,
-                                        int l1) {
-    L0 = l0; L1 = l1; sacc = sm; scale = a.acc_scale;
-    win = SMEM ? sm : a.acc;
-    unsigned long long *tmem = SMEM ? sm + L0 * L1 : sm;
-    if (SMEM)
-      for (int k = threadIdx.x; k < L0 * L1; k += blockDim.x) sm[k] = 0ull;
-    for (int k = threadIdx.x; k < Tile::kSize * (int)blockDim.x; k += blockDim.x) tmem[k] = 0ull;
-    if (threadIdx.x == 0) { sh.tb[0] = L0; sh.tb[1] = L1; sh.tb[2] = -1; sh.tb[3] = -1; }
+  __device__ __forceinline__ void begin(const Push32Args &a, unsigned long long *sm, int l0, int l1) {
+    L0 = l0; L1 = l1; scale = a.acc_scale;
+    win = a.acc;
+    for (int k = threadIdx.x; k < Tile::kSize * (int)blockDim.x; k += blockDim.x) sm[k] = 0ull;
     __syncthreads();
-    tile.init(tmem, L0, L1);
+    tile.init(sm, L0, L1);
   }
 
   // Current of one move R0 -> R2 (cells from the old cell, whose window cell
@@ -215,37 +210,21 @@ struct Depositor32 {
   // lanes of the warp together (has: this lane has a particle).
   __device__ __forceinline__ void particle(const Push32Args &a, bool has, int wi, int wj, double q, double r00,
                                            double r01, double e0, double e1) {
-    tile.template rebase<SMEM>(has, has ? wi + (int)floor(r00) : 0, has ? wj + (int)floor(r01) : 0, win, L0, L1);
+    tile.template rebase<false>(has, has ? wi + (int)floor(r00) : 0, has ? wj + (int)floor(r01) : 0, win, L0, L1);
     if (has) {
       auto sink = [&](int i, int j, double v) {
-        tile.template add<SMEM>(i + wi, j + wj, __double2ll_rn(v * scale), win, L0, L1);
+        tile.template add<false>(i + wi, j + wj, __double2ll_rn(v * scale), win, L0, L1);
       };
       if (!deposit_particle<ORDER>(a.jcomp, q, r00, r01, e0, e1, 0.0, 0.0, 1.0, 1.0, a.h0, a.h1, a.dt, sink))
         overflow = true;
     }
   }
 
-  // Called by all threads of the CTA (after their last particle(), before
-  // any other use of sh.sb); ends with a barrier.
-  __device__ __forceinline__ void end(const Push32Args &a, PushShared &sh) {
-    tile.template flush<SMEM>(win, L0, L1);
+  // Called by all threads of the CTA after their last particle(); ends with
+  // a barrier.
+  __device__ __forceinline__ void end(const Push32Args &a) {
+    tile.template flush<false>(win, L0, L1);
     if (overflow) set_err(a.ws, kErrCrossings);
-    if (SMEM) {
-      if (tile.ti1 >= 0) {
-        atomicMin(&sh.tb[0], tile.ti0); atomicMin(&sh.tb[1], tile.tj0);
-        atomicMax(&sh.tb[2], tile.ti1); atomicMax(&sh.tb[3], tile.tj1);
-      }
-      __syncthreads();
-      const int i0 = sh.tb[0], j0 = sh.tb[1], i1 = sh.tb[2], j1 = sh.tb[3];
-      if (i1 >= i0) {
-        const int w = i1 - i0 + 1, cnt = w * (j1 - j0 + 1);
-        for (int k = threadIdx.x; k < cnt; k += blockDim.x) {
-          const int i = i0 + k % w, j = j0 + k / w;
-          const unsigned long long v = sacc[j * L0 + i];
-          if (v) atomicAdd(&a.acc[j * L0 + i], v);
-        }
-      }
-    }
     __syncthreads();
   }
 };
@@ -258,54 +237,16 @@ __device__ __forceinline__ bool entry_error(WinState *ws, PushShared &sh) {
   return sh.err != 0;
 }
 
-// One CTA's share [beg, end) of one fused push (move + deposit); called by
-// all threads of the CTA, ends with a barrier (a CTA may run it for several
-// members in turn).
-template <int ORDER, bool SMEM>
-__device__ __forceinline__ void push32_body(const Push32Args &a, long long beg, long long end, PushShared &sh,
-                                            unsigned long long *sacc) {
+// Move and deposit of one CTA's share [beg, end) of one member; called by
+// all threads of the CTA, each ends with a barrier, so that a CTA may run
+// them for several members in turn.
+template <int ORDER>
+__device__ __forceinline__ void move32_range(const Push32Args &a, long long beg, long long end, PushShared &sh) {
   if (entry_error(a.ws, sh)) return;  // the whole CTA leaves together
   WinState *ws = a.ws;
   const int L0 = ws->L0, L1 = ws->L1, WP0 = ws->P0, WP1 = ws->P1;
-  Depositor32<ORDER, SMEM> dep;
-  dep.begin(a, sacc, sh, L0, L1);
   Boxes32 box;
-  const long long rounds = end > beg ? (end - beg + blockDim.x - 1) / blockDim.x : 0;
-  for (long long it = 0; it < rounds; ++it) {  // the same rounds for every lane
-    const long long n = beg + it * blockDim.x + threadIdx.x;
-    Move32 m;
-    move32<ORDER>(a, n, n < end, L0, L1, WP0, WP1, m);
-    dep.particle(a, m.ok, m.ci - WP0, m.cj - WP1, m.q, m.r00, m.r01, m.e0, m.e1);
-    if (m.ok) box.add(m);
-  }
-  dep.end(a, sh);
-  box.store(ws, sh);
-  __syncthreads();
-}
-
-// The single-member FP32 push in two launches.  k_push32_move moves every
-// particle (gather, kick, drift, stores, boxes) with no shared memory at
-// three CTAs per SM, and leaves for the deposit each particle's start R0
-// and old cell in a.dep_r0 / a.dep_cell (NaN for a particle it did not
-// move).  k_push32_dep then adds the current of every move R0 -> R2 exactly
-// as the fused push does, CTA by CTA over contiguous (cell-sorted) ranges,
-// also at three CTAs per SM.  Both are bound by the latency of dependent
-// FP64 chains, not by bytes: split, each runs at 24 warps per SM where the
-// fused push's registers and shared memory allowed 16 (4e6-particle TSC
-// bunch, 8192 x 1024 mesh: 0.50 -> 0.41 ms per push).  The extra traffic is
-// 20 bytes written and 36 read per particle.
-template <int ORDER>
-__global__ void __launch_bounds__(256, 3) k_push32_move(Push32Args a) {
-  __shared__ PushShared sh;
-  if (entry_error(a.ws, sh)) return;
-  WinState *ws = a.ws;
-  const int L0 = ws->L0, L1 = ws->L1, WP0 = ws->P0, WP1 = ws->P1;
-  Boxes32 box;
-  const long long stride = (long long)gridDim.x * blockDim.x;
-  const long long rounds = (a.b.n + stride - 1) / stride;
-  for (long long it = 0; it < rounds; ++it) {
-    const long long n = it * stride + blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (n >= a.b.n) continue;
+  for (long long n = beg + threadIdx.x; n < end; n += blockDim.x) {
     Move32 m;
     move32<ORDER>(a, n, true, L0, L1, WP0, WP1, m);
     a.dep_r0[2 * n] = m.ok ? m.r00 : NAN;
@@ -314,21 +255,17 @@ __global__ void __launch_bounds__(256, 3) k_push32_move(Push32Args a) {
     if (m.ok) box.add(m);
   }
   box.store(ws, sh);
+  __syncthreads();
 }
 
 template <int ORDER>
-__global__ void __launch_bounds__(256, 3) k_push32_dep(Push32Args a) {
-  constexpr bool SMEM = false;
-  extern __shared__ unsigned long long sacc[];
-  __shared__ PushShared sh;
+__device__ __forceinline__ void dep32_range(const Push32Args &a, long long beg, long long end, PushShared &sh,
+                                            unsigned long long *sacc) {
   if (entry_error(a.ws, sh)) return;
   WinState *ws = a.ws;
   const int L0 = ws->L0, L1 = ws->L1, WP0 = ws->P0, WP1 = ws->P1;
-  const long long per = (a.b.n + gridDim.x - 1) / gridDim.x;
-  const long long beg = (long long)blockIdx.x * per;
-  const long long end = beg + per < a.b.n ? beg + per : a.b.n;
-  Depositor32<ORDER, SMEM> dep;
-  dep.begin(a, sacc, sh, L0, L1);
+  Depositor32<ORDER> dep;
+  dep.begin(a, sacc, L0, L1);
   // a round's inputs are loaded together, one round ahead, so that their
   // latency overlaps the deposit of the round before
   struct In {
@@ -348,7 +285,7 @@ __global__ void __launch_bounds__(256, 3) k_push32_dep(Push32Args a) {
   const long long rounds = end > beg ? (end - beg + blockDim.x - 1) / blockDim.x : 0;
   In cur, nxt;
   load(beg + threadIdx.x, cur);
-  for (long long it = 0; it < rounds; ++it) {
+  for (long long it = 0; it < rounds; ++it) {  // the same rounds for every lane
     if (it + 1 < rounds) load(beg + (it + 1) * blockDim.x + threadIdx.x, nxt);
     const bool has = !isnan(cur.r0.x);
     double e0 = 0.0, e1 = 0.0;
@@ -363,13 +300,64 @@ __global__ void __launch_bounds__(256, 3) k_push32_dep(Push32Args a) {
     dep.particle(a, has, ci - WP0, cj - WP1, (double)cur.q, cur.r0.x, cur.r0.y, e0, e1);
     cur = nxt;
   }
-  dep.end(a, sh);
+  dep.end(a);
 }
 
-// One push over a batch of FP32-mode members (see k_push_batch).
+// The FP32 push in two launches.  The move launch moves every particle
+// (gather, kick, drift, stores, boxes) with no shared memory and leaves for
+// the deposit each particle's start R0 and old cell in a.dep_r0 / a.dep_cell
+// (NaN for a particle it did not move); the deposit launch then adds the
+// current of every move R0 -> R2, CTA by CTA over contiguous (cell-sorted)
+// ranges.  Both run at three CTAs per SM and are bound by the latency of
+// dependent FP64 chains, not by bytes: split, each runs at 24 warps per SM
+// where the fused push's 128 registers and 98 KB of shared memory (window
+// accumulator copy + tiles) allowed 16 (4e6-particle TSC bunch, 8192 x 1024
+// mesh: 0.50 -> 0.40 ms per push).  The extra traffic is 20 bytes written
+// and 36 read per particle.
 template <int ORDER>
-__global__ void __launch_bounds__(256, 2) k_push32_batch(const Push32Args *args, const unsigned char *smem_ok,
-                                                       const long long *ppre, int m, long long per) {
+__global__ void __launch_bounds__(256, 3) k_push32_move(Push32Args a) {
+  __shared__ PushShared sh;
+  const long long per = (a.b.n + gridDim.x - 1) / gridDim.x;
+  const long long beg = (long long)blockIdx.x * per;
+  move32_range<ORDER>(a, beg, beg + per < a.b.n ? beg + per : a.b.n, sh);
+}
+
+template <int ORDER>
+__global__ void __launch_bounds__(256, 3) k_push32_dep(Push32Args a) {
+  extern __shared__ unsigned long long sacc[];
+  __shared__ PushShared sh;
+  const long long per = (a.b.n + gridDim.x - 1) / gridDim.x;
+  const long long beg = (long long)blockIdx.x * per;
+  dep32_range<ORDER>(a, beg, beg + per < a.b.n ? beg + per : a.b.n, sh, sacc);
+}
+
+// One push over a batch of FP32-mode members in two launches, as for one
+// member: the members' particles form one index range (ppre: first particle
+// of each member, m + 1 entries) cut into equal contiguous shares, one per
+// CTA; a CTA runs the move (then, in the second launch, the deposit) of every
+// member its share overlaps.
+template <int ORDER>
+__global__ void __launch_bounds__(256, 3) k_push32_batch_move(const Push32Args *args, const long long *ppre, int m,
+                                                            long long per) {
+  __shared__ PushShared sh;
+  __shared__ Push32Args sa;
+  const long long total = ppre[m];
+  const long long g0 = (long long)blockIdx.x * per;
+  const long long g1 = g0 + per < total ? g0 + per : total;
+  for (int mm = 0; mm < m; ++mm) {
+    const long long b0 = ppre[mm], b1 = ppre[mm + 1];
+    if (b1 <= g0 || b0 >= g1) continue;
+    const long long lb = (g0 > b0 ? g0 : b0) - b0, le = (g1 < b1 ? g1 : b1) - b0;
+    __syncthreads();
+    if (threadIdx.x == 0) sa = args[mm];
+    __syncthreads();
+    move32_range<ORDER>(sa, lb, le, sh);
+  }
+}
+
+template <int ORDER>
+__global__ void __launch_bounds__(256, 3) k_push32_batch_dep(const Push32Args *args, const long long *ppre, int m,
+                                                           long long per) {
   extern __shared__ unsigned long long sacc[];
   __shared__ PushShared sh;
   __shared__ Push32Args sa;
@@ -383,8 +371,7 @@ __global__ void __launch_bounds__(256, 2) k_push32_batch(const Push32Args *args,
     __syncthreads();
     if (threadIdx.x == 0) sa = args[mm];
     __syncthreads();
-    if (smem_ok[mm]) push32_body<ORDER, true>(sa, lb, le, sh, sacc);
-    else push32_body<ORDER, false>(sa, lb, le, sh, sacc);
+    dep32_range<ORDER>(sa, lb, le, sh, sacc);
   }
 }
 
@@ -588,29 +575,21 @@ int launch_push32(const Push32Args &a, int order, cudaStream_t s) {
   return 0;
 }
 
+// The batched FP32 push keeps no window copy in shared memory (0: no member
+// "fits"); its deposit launch takes the warp tiles of the largest shape order.
 long long push32_batch_smem_limit() {
-  static long long lim = -1;
-  if (lim < 0) {
-    int dev = 0, v = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-    cudaFuncAttributes fa{};
-    cudaFuncGetAttributes(&fa, k_push32_batch<1>);
-    lim = (long long)v - (long long)fa.sharedSizeBytes;
-    // keep two CTAs per SM: half the SM's shared memory less the static part
-    // and the 1 KB the runtime reserves per CTA
-    int per_sm = 0;
-    cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
-    const long long two = (long long)per_sm / 2 - (long long)fa.sharedSizeBytes - 1024;
-    if (two > 0 && two < lim) lim = two;
-    if (cudaFuncSetAttribute(k_push32_batch<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lim) != cudaSuccess ||
-        cudaFuncSetAttribute(k_push32_batch<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lim) != cudaSuccess ||
-        cudaFuncSetAttribute(k_push32_batch<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lim) !=
-        cudaSuccess)
-      lim = 0;
+  static int set = 0;
+  if (!set) {
+    cudaFuncSetAttribute(k_push32_batch_dep<0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)(TileFor<0>::T::kSize * 256 * sizeof(unsigned long long)));
+    cudaFuncSetAttribute(k_push32_batch_dep<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)(TileFor<1>::T::kSize * 256 * sizeof(unsigned long long)));
+    cudaFuncSetAttribute(k_push32_batch_dep<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)(TileFor<2>::T::kSize * 256 * sizeof(unsigned long long)));
     cudaGetLastError();
+    set = 1;
   }
-  return lim;
+  return 0;
 }
 
 void launch_push32_batch(const PushGroup *groups, int ngroups, int m, int grid, const PrepArgs *prep, cudaStream_t s,
@@ -623,9 +602,18 @@ void launch_push32_batch(const PushGroup *groups, int ngroups, int m, int grid, 
     const int ctas = (int)((long long)grid * G.total / (G.all > 0 ? G.all : G.total)) + 1;
     const long long per = (G.total + ctas - 1) / ctas;
     const Push32Args *args = static_cast<const Push32Args *>(G.args);
-    if (G.order == 0) k_push32_batch<0><<<ctas, 256, G.smem, s>>>(args, G.smem_ok, G.ppre, G.m, per);
-    else if (G.order == 1) k_push32_batch<1><<<ctas, 256, G.smem, s>>>(args, G.smem_ok, G.ppre, G.m, per);
-    else k_push32_batch<2><<<ctas, 256, G.smem, s>>>(args, G.smem_ok, G.ppre, G.m, per);
+    push32_batch_smem_limit();
+    const size_t tiles = push_tile_bytes(G.order);
+    if (G.order == 0) {
+      k_push32_batch_move<0><<<ctas, 256, 0, s>>>(args, G.ppre, G.m, per);
+      k_push32_batch_dep<0><<<ctas, 256, tiles, s>>>(args, G.ppre, G.m, per);
+    } else if (G.order == 1) {
+      k_push32_batch_move<1><<<ctas, 256, 0, s>>>(args, G.ppre, G.m, per);
+      k_push32_batch_dep<1><<<ctas, 256, tiles, s>>>(args, G.ppre, G.m, per);
+    } else {
+      k_push32_batch_move<2><<<ctas, 256, 0, s>>>(args, G.ppre, G.m, per);
+      k_push32_batch_dep<2><<<ctas, 256, tiles, s>>>(args, G.ppre, G.m, per);
+    }
   }
   if (parts & 2) {
     k_post32_batch<<<tb, 128, 0, s>>>(prep, m);
