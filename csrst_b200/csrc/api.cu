@@ -10,6 +10,7 @@
 #include <vector>
 
 #include "../../include/csrst.h"
+#include "bunch32.cuh"
 #include "kernels.cuh"
 
 namespace csrst {
@@ -33,6 +34,35 @@ __global__ void k_slice_keys(const double *y, const long long *idx, long long n,
   const double mn1 = ord_dbl(ws->bb[ws->cur][1]);
   const int lp2 = (int)floor((mn1 - ws->mo1) / h1);
   ks[i] = (unsigned int)((int)floor((y[idx[i]] - ws->mo1) / h1) - lp2);
+}
+inline double bits_to_double(unsigned long long b) {
+  double d;
+  std::memcpy(&d, &b, sizeof d);
+  return d;
+}
+// Input check of a bunch on the device: out[0] = the first index whose
+// values are not all finite or (in FP32 mode, whose cells are 16-bit static
+// mesh indices) whose position lies off the static mesh, ~0 if none; out[1] =
+// max |q| as the bits of a non-negative double.  out starts as {~0, 0}.
+__global__ void k_check_bunch(const double *x, const double *y, const double *px, const double *py,
+                              const double *q, long long n, int on_mesh, double org0, double org1, double h0,
+                              double h1, int Nx, int Ny, unsigned long long *out) {
+  unsigned long long bad = ~0ull, qm = 0ull;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    bool ok = isfinite(x[i]) && isfinite(y[i]) && isfinite(px[i]) && isfinite(py[i]) && isfinite(q[i]);
+    if (ok) {
+      const unsigned long long b = (unsigned long long)__double_as_longlong(fabs(q[i]));
+      qm = b > qm ? b : qm;
+      if (on_mesh) {
+        const double a = (x[i] - org0) / h0, c = (y[i] - org1) / h1;
+        ok = a >= 0 && a < Nx && c >= 0 && c < Ny;
+      }
+    }
+    if (!ok && (unsigned long long)i < bad) bad = (unsigned long long)i;
+  }
+  if (bad != ~0ull) atomicMin(&out[0], bad);
+  if (qm) atomicMax(&out[1], qm);
 }
 __global__ void k_acc_to_plane(const unsigned long long *acc, Plane p, int L0, int L1, double inv) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -455,6 +485,19 @@ void bunch64(csrst_handle *h, const double **x, const double **y, const double *
   *x = h->d64; *y = h->d64 + n; *px = h->d64 + 2 * n; *py = h->d64 + 3 * n; *pending = 0;
 }
 
+// Beam moments of the current bunch into dout (out[18]) and dmean, without a
+// host synchronisation; FP32 mode reads its bunch in place.
+void moments_async(csrst_handle *h) {
+  if (h->fp32) {
+    launch_moments32(Bunch32View{h->b32, h->P0, h->P1, h->kh0, h->kh1, h->pending ? 1 : 0, h->b.org0, h->b.org1,
+                                 h->b.hr0, h->b.hr1},
+                     h->dscratch, h->dmean, h->dout, h->s);
+    return;
+  }
+  launch_moments(h->x, h->y, h->px, h->py, h->n, h->half, h->pending ? 1 : 0, h->dscratch, h->dmean, h->dout,
+                 h->s);
+}
+
 // TETMSolver::updateField_firstStep + updateField_secondStep + moveMesh.
 void step_async(csrst_handle *h) {
   push_async(h, 0);
@@ -668,28 +711,53 @@ int csrst_load_particles(csrst_handle *h, const double *x, const double *y, cons
                          const double *py, const double *q, size_t n) {
   if (!h || (n > 0 && (!x || !y || !px || !py || !q))) return CSRST_E_ARG;
   if (n == 0) return fail(h, CSRST_E_NO_PARTICLES, "empty bunch");
-  double qmax = 0.0;
-  for (size_t i = 0; i < n; ++i) {
+  CK(cudaStreamSynchronize(h->s));
+  const long long N = (long long)n;
+  const size_t nb = n * sizeof(double);
+  // the bunch goes up and is checked on the device before the handle's
+  // current bunch is released, so that a rejected bunch leaves it intact
+  double *tmp[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+  unsigned long long *chk = nullptr;
+  auto drop = [&]() {
+    for (int k = 0; k < 5; ++k) cudaFree(tmp[k]);
+    cudaFree(chk);
+  };
+  for (int k = 0; k < 5; ++k)
+    if (cudaMalloc(&tmp[k], nb) != cudaSuccess) { drop(); return fail(h, CSRST_E_CUDA, "bunch upload: out of memory"); }
+  if (cudaMalloc(&chk, 2 * sizeof(unsigned long long)) != cudaSuccess) {
+    drop();
+    return fail(h, CSRST_E_CUDA, "bunch upload: out of memory");
+  }
+  const double *src[5] = {x, y, px, py, q};
+  for (int k = 0; k < 5; ++k) CK(cudaMemcpyAsync(tmp[k], src[k], nb, cudaMemcpyHostToDevice, h->s));
+  unsigned long long hchk[2] = {~0ull, 0ull};
+  CK(cudaMemcpyAsync(chk, hchk, sizeof(hchk), cudaMemcpyHostToDevice, h->s));
+  {
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const long long want = (N + 255) / 256, cap = 8LL * sms;
+    k_check_bunch<<<(unsigned)(want < cap ? want : cap), 256, 0, h->s>>>(
+        tmp[0], tmp[1], tmp[2], tmp[3], tmp[4], N, h->fp32 ? 1 : 0, h->b.org0, h->b.org1, h->b.hr0, h->b.hr1,
+        h->b.Nx, h->b.Ny, chk);
+  }
+  CK(cudaMemcpyAsync(hchk, chk, sizeof(hchk), cudaMemcpyDeviceToHost, h->s));
+  CK(cudaStreamSynchronize(h->s));
+  if (hchk[0] < (unsigned long long)n) {  // the first rejected particle, with its reason
+    const size_t i = (size_t)hchk[0];
+    drop();
     if (!std::isfinite(x[i]) || !std::isfinite(y[i]) || !std::isfinite(px[i]) || !std::isfinite(py[i]) ||
         !std::isfinite(q[i]))
       return fail(h, CSRST_E_ARG, "non-finite particle data at index " + std::to_string(i));
-    qmax = std::fmax(qmax, std::fabs(q[i]));
-    if (h->fp32) {  // FP32 mode stores 16-bit cell indices of the static mesh
-      const double a = (x[i] - h->b.org0) / h->b.hr0, b = (y[i] - h->b.org1) / h->b.hr1;
-      if (!(a >= 0 && a < h->b.Nx && b >= 0 && b < h->b.Ny))
-        return fail(h, CSRST_E_ARG, "particle outside the static mesh at index " + std::to_string(i));
-    }
+    // FP32 mode stores 16-bit cell indices of the static mesh
+    return fail(h, CSRST_E_ARG, "particle outside the static mesh at index " + std::to_string(i));
   }
-  CK(cudaStreamSynchronize(h->s));
+  const double qmax = bits_to_double(hchk[1]);
+  cudaFree(chk);
+  chk = nullptr;
   free_particles(h);
-  const long long N = (long long)n;
   h->n = N;
-  const size_t nb = n * sizeof(double);
-  double *tmp[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
   for (double **p : {&h->x, &h->y, &h->px, &h->py, &h->q, &h->ox, &h->oy}) CK(cudaMalloc(p, nb));
-  for (int k = 0; k < 5; ++k) CK(cudaMalloc(&tmp[k], nb));
-  const double *src[5] = {x, y, px, py, q};
-  for (int k = 0; k < 5; ++k) CK(cudaMemcpyAsync(tmp[k], src[k], nb, cudaMemcpyHostToDevice, h->s));
   // particle box on the static mesh -> window +-5 cells (main.cpp:198-217)
   WinState w0{};
   w0.cur = 0;
@@ -1017,23 +1085,16 @@ int csrst_diag_moments(csrst_handle *h, double *out18) {
   int rc = need_bunch(h);
   if (rc) return rc;
   if (!out18) return CSRST_E_ARG;
-  const double *x, *y, *px, *py;
-  int pend = 0;
-  bunch64(h, &x, &y, &px, &py, &pend);
-  launch_moments(x, y, px, py, h->n, h->half, pend, h->dscratch, h->dmean, h->dout, h->s);
+  moments_async(h);
   CK(cudaMemcpyAsync(out18, h->dout, 18 * sizeof(double), cudaMemcpyDeviceToHost, h->s));
-  CK(cudaStreamSynchronize(h->s));
-  return check_err(h);
+  return check_err(h);  // one synchronisation for both copies
 }
 
 int csrst_diag_wake(csrst_handle *h, double *out, int n) {
   int rc = need_bunch(h);
   if (rc) return rc;
   if (!out || n != h->L0 - 4) return fail(h, CSRST_E_ARG, "wake buffer must hold L0 - 4 values");
-  const double *x, *y, *px, *py;
-  int pend = 0;
-  bunch64(h, &x, &y, &px, &py, &pend);
-  launch_moments(x, y, px, py, h->n, h->half, pend, h->dscratch, h->dmean, h->dout, h->s);
+  moments_async(h);
   double *d = nullptr;
   CK(cudaMallocAsync(&d, (size_t)n * sizeof(double), h->s));
   if (h->fp32)
@@ -1051,10 +1112,7 @@ int csrst_diag_line_fields(csrst_handle *h, int with_current, double *out, int c
   int rc = need_bunch(h);
   if (rc) return rc;
   if (!count) return fail(h, CSRST_E_ARG, "line fields: count pointer missing");
-  const double *x, *y, *px, *py;
-  int pend = 0;
-  bunch64(h, &x, &y, &px, &py, &pend);
-  launch_moments(x, y, px, py, h->n, h->half, pend, h->dscratch, h->dmean, h->dout, h->s);
+  moments_async(h);
   double m[18];
   CK(cudaMemcpyAsync(m, h->dout, sizeof(m), cudaMemcpyDeviceToHost, h->s));
   CK(cudaStreamSynchronize(h->s));
@@ -1105,10 +1163,7 @@ int csrst_diag_wake_async(csrst_handle *h, double *out_dev, int n, double *meta_
   int rc = need_bunch(h);
   if (rc) return rc;
   if (!out_dev || !meta_dev || n != h->L0 - 4) return fail(h, CSRST_E_ARG, "wake buffer must hold L0 - 4 values");
-  const double *x, *y, *px, *py;
-  int pend = 0;
-  bunch64(h, &x, &y, &px, &py, &pend);
-  launch_moments(x, y, px, py, h->n, h->half, pend, h->dscratch, h->dmean, h->dout, h->s);
+  moments_async(h);
   if (h->fp32)
     launch_wake(h->ws, wplane32(h, 0).p, wplane32(h, 1).p, h->wpitch, h->L0, h->b.hr0, h->b.hr1, h->dmean, out_dev,
                 h->s);

@@ -4,6 +4,7 @@
 // IntegrateElong.cpp:38-89) and the charge difference used by the FP64
 // continuity check.  All reductions run in FP64 with a fixed order (per-CTA
 // partials reduced by one CTA), so they are reproducible run to run.
+#include "bunch32.cuh"
 #include "kernels.cuh"
 #include "shapes.cuh"
 
@@ -38,17 +39,27 @@ __device__ void block_sum(double (&v)[NV], double *out) {
   __syncthreads();
 }
 
+// Particle sources of the moment passes: the FP64 arrays (positions with a
+// pending trailing half drift undone), or the FP32-mode bunch read in place.
+struct Bunch64View {
+  const double *x, *y, *px, *py;
+  double half;
+  int pending;
+  __device__ __forceinline__ void operator()(long long i, double &a, double &b, double &p0, double &p1) const {
+    a = x[i]; b = y[i]; p0 = px[i]; p1 = py[i];
+    true_pos(a, b, p0, p1, half, pending);
+  }
+};
+
 // pass 1: sum x, px, y, py, gamma; min/max x, y.  part[b * 9 + k]
-__global__ void __launch_bounds__(256) k_mom1(const double *x, const double *y, const double *px,
-                                              const double *py, long long n, double half,
-                                              int pending, double *part) {
+template <class Src>
+__global__ void __launch_bounds__(256) k_mom1(Src src, long long n, double *part) {
   double v[5] = {0, 0, 0, 0, 0};
   double mn0 = INFINITY, mn1 = INFINITY, mx0 = -INFINITY, mx1 = -INFINITY;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x) {
-    double a = x[i], b = y[i];
-    const double p0 = px[i], p1 = py[i];
-    true_pos(a, b, p0, p1, half, pending);
+    double a, b, p0, p1;
+    src(i, a, b, p0, p1);
     v[0] += a; v[1] += p0; v[2] += b; v[3] += p1;
     v[4] += sqrt(1.0 + (p0 * p0 + p1 * p1));
     mn0 = fmin(mn0, a); mn1 = fmin(mn1, b); mx0 = fmax(mx0, a); mx1 = fmax(mx1, b);
@@ -78,17 +89,15 @@ __global__ void __launch_bounds__(256) k_mom1(const double *x, const double *y, 
 // q0 (q1-m), q0, q2 q3, (q1-m), and for the dispersion terms q2 (q1-m), q2,
 // q3 (q1-m), q3 (the reference's moments(2,1) and (3,1) pair y' and py' with
 // the uncentred px' = (q1-m) + m).
-__global__ void __launch_bounds__(256) k_mom2(const double *x, const double *y, const double *px,
-                                              const double *py, long long n, double half,
-                                              int pending, const double *mean, double *part) {
+template <class Src>
+__global__ void __launch_bounds__(256) k_mom2(Src src, long long n, const double *mean, double *part) {
   const double aR0 = mean[0], aR1 = mean[1], aP0 = mean[2], aP1 = mean[3];
   const double am = sqrt(aP0 * aP0 + aP1 * aP1), cph = aP0 / am, sph = aP1 / am;
   double v[12] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x) {
-    double a = x[i], b = y[i];
-    const double p0 = px[i], p1 = py[i];
-    true_pos(a, b, p0, p1, half, pending);
+    double a, b, p0, p1;
+    src(i, a, b, p0, p1);
     const double q1 = cph * p0 + sph * p1 - am;
     const double q3 = -sph * p0 + cph * p1;
     const double d0 = a - aR0, d2 = b - aR1;
@@ -103,13 +112,27 @@ __global__ void __launch_bounds__(256) k_mom2(const double *x, const double *y, 
 
 // Final reduction and the derived quantities; out[18] as the oracle's layout:
 // rmean2 pmean2 rrms2 prms2 eps2 rmin2 rmax2 Ekin dE, pad.
+// The final reductions run on one warp in a fixed order: lane t sums the
+// block partials t, t + 32, ... in turn, then the lanes combine in a fixed
+// shuffle tree, so the result does not depend on scheduling.  (One thread
+// walking all partials waited on a dependent chain of a few thousand loads.)
+template <int K>
+__device__ __forceinline__ void warp_fixed_sums(const double *part, int nb, int stride, int k0, double (&v)[K]) {
+  for (int k = 0; k < K; ++k) v[k] = 0.0;
+  for (int b = threadIdx.x; b < nb; b += 32)
+    for (int k = 0; k < K; ++k) v[k] += part[b * stride + k0 + k];
+  for (int k = 0; k < K; ++k)
+    for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_down_sync(0xffffffffu, v[k], o);
+}
+
 __global__ void k_mom_final1(const double *part, int nb, long long n, double *mean, double *out) {
-  if (threadIdx.x != 0) return;
-  double s[5] = {0, 0, 0, 0, 0}, m[4] = {INFINITY, INFINITY, INFINITY, INFINITY};
-  for (int b = 0; b < nb; ++b) {
-    for (int k = 0; k < 5; ++k) s[k] += part[b * 9 + k];
+  double s[5], m[4] = {INFINITY, INFINITY, INFINITY, INFINITY};
+  warp_fixed_sums<5>(part, nb, 9, 0, s);
+  for (int b = threadIdx.x; b < nb; b += 32)
     for (int k = 0; k < 4; ++k) m[k] = fmin(m[k], part[b * 9 + 5 + k]);
-  }
+  for (int k = 0; k < 4; ++k)
+    for (int o = 16; o > 0; o >>= 1) m[k] = fmin(m[k], __shfl_down_sync(0xffffffffu, m[k], o));
+  if (threadIdx.x != 0) return;
   const double N = (double)n;
   mean[0] = s[0] / N; mean[1] = s[2] / N; mean[2] = s[1] / N; mean[3] = s[3] / N; mean[4] = s[4] / N;
   out[0] = mean[0]; out[1] = mean[1]; out[2] = mean[2]; out[3] = mean[3];
@@ -117,10 +140,9 @@ __global__ void k_mom_final1(const double *part, int nb, long long n, double *me
 }
 
 __global__ void k_mom_final2(const double *part, int nb, long long n, const double *mean, double *out) {
+  double M[12];
+  warp_fixed_sums<12>(part, nb, 12, 0, M);
   if (threadIdx.x != 0) return;
-  double M[12] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
-  for (int b = 0; b < nb; ++b)
-    for (int k = 0; k < 12; ++k) M[k] += part[b * 12 + k];
   const double N = (double)n;
   const double am = sqrt(mean[2] * mean[2] + mean[3] * mean[3]);
   const double rsq[2] = {M[0], M[1]};
@@ -231,11 +253,11 @@ __global__ void __launch_bounds__(256) k_energy(const T *Ex, const T *Ey, const 
 }
 
 __global__ void k_energy_final(const double *part, int nb, double area, double *out) {
+  double v[2];
+  warp_fixed_sums<2>(part, nb, 2, 0, v);
   if (threadIdx.x != 0) return;
-  double s0 = 0.0, s1 = 0.0;
-  for (int b = 0; b < nb; ++b) { s0 += part[2 * b]; s1 += part[2 * b + 1]; }
-  out[0] = s0 * area;
-  out[1] = s1 * area;
+  out[0] = v[0] * area;
+  out[1] = v[1] * area;
 }
 
 // The static mesh with the window's values over the points it covers (the
@@ -306,12 +328,23 @@ __global__ void k_line_fields(const T *Ex, const T *Ey, const T *Hx, const T *Hy
 
 // --- host launchers -----------------------------------------------------------
 
+template <class Src>
+static void moments_of(const Src &src, long long n, double *part, double *mean, double *out, cudaStream_t s) {
+  k_mom1<<<kDiagBlocks, 256, 0, s>>>(src, n, part);
+  k_mom_final1<<<1, 32, 0, s>>>(part, kDiagBlocks, n, mean, out);
+  k_mom2<<<kDiagBlocks, 256, 0, s>>>(src, n, mean, part);
+  k_mom_final2<<<1, 32, 0, s>>>(part, kDiagBlocks, n, mean, out);
+}
+
 void launch_moments(const double *x, const double *y, const double *px, const double *py, long long n,
                     double half, int pending, double *part, double *mean, double *out, cudaStream_t s) {
-  k_mom1<<<kDiagBlocks, 256, 0, s>>>(x, y, px, py, n, half, pending, part);
-  k_mom_final1<<<1, 32, 0, s>>>(part, kDiagBlocks, n, mean, out);
-  k_mom2<<<kDiagBlocks, 256, 0, s>>>(x, y, px, py, n, half, pending, mean, part);
-  k_mom_final2<<<1, 32, 0, s>>>(part, kDiagBlocks, n, mean, out);
+  moments_of(Bunch64View{x, y, px, py, half, pending}, n, part, mean, out, s);
+}
+
+// FP32 mode: the moments of the bunch read in place (the FP64 copy it would
+// otherwise be converted into first holds the same values).
+void launch_moments32(const Bunch32View &v, double *part, double *mean, double *out, cudaStream_t s) {
+  moments_of(v, v.b.n, part, mean, out, s);
 }
 
 size_t moments_scratch_doubles() { return (size_t)kDiagBlocks * 12; }

@@ -19,6 +19,7 @@
 // the FP64 path to a tolerance, not bit for bit.
 #include "accum.cuh"
 #include "bbox.cuh"
+#include "bunch32.cuh"
 #include "kernels.cuh"
 #include "shapes.cuh"
 
@@ -36,28 +37,6 @@ struct SumView32 {
   View32 a, b;
   __device__ __forceinline__ float operator()(int i, int j) const { return a(i, j) + b(i, j); }
 };
-
-__device__ __forceinline__ void unpack(int c, int &i, int &j) {
-  i = c & 0xffff;
-  j = (int)((unsigned)c >> 16);
-}
-
-// Position arithmetic uses explicitly rounded operations: the push, the box
-// of the next push's positions and the drift must produce the same bits for
-// the same inputs wherever they are computed, whatever the compiler fuses.
-__device__ __forceinline__ double dmul(double a, double b) { return __dmul_rn(a, b); }
-__device__ __forceinline__ double dadd(double a, double b) { return __dadd_rn(a, b); }
-__device__ __forceinline__ double dsub(double a, double b) { return __dsub_rn(a, b); }
-
-// 1/gamma as the FP64 path computes it, from the full momentum P + d.
-__device__ __forceinline__ float rgam(double P0, double P1, float d0, float d1, double &p0, double &p1) {
-  p0 = dadd(P0, (double)d0);
-  p1 = dadd(P1, (double)d1);
-  return q_rsqrt((float)dadd(1.0, dadd(dmul(p0, p0), dmul(p1, p1))));
-}
-
-// Drift of one half step in cells: kh * p * (1/gamma).
-__device__ __forceinline__ double half_drift(double kh, double p, float r) { return dmul(dmul(kh, p), (double)r); }
 
 // Cell of the cell-relative coordinate t of cell c, as c' + 0.5 (exact).
 __device__ __forceinline__ double cellc(int c, double t) { return (double)(c + (int)floor(t)) + 0.5; }
@@ -478,17 +457,12 @@ __global__ void k_from64(const double *x, const double *y, const double *px, con
   }
 }
 
-__global__ void k_to64(Bunch32 b, double P0, double P1, double kh0, double kh1, int pending, double org0,
-                       double org1, double h0, double h1, double *x, double *y, double *px, double *py) {
-  for (long long n = gtid(); n < b.n; n += (long long)gridDim.x * blockDim.x) {
-    int ci, cj;
-    unpack(b.cell[n], ci, cj);
-    double p0, p1;
-    const float r = rgam(P0, P1, b.dpx[n], b.dpy[n], p0, p1);
-    double s0 = b.ox[n], s1 = b.oy[n];
-    if (pending) { s0 = dsub(s0, half_drift(kh0, p0, r)); s1 = dsub(s1, half_drift(kh1, p1, r)); }
-    if (x) x[n] = org0 + ((double)ci + s0) * h0;
-    if (y) y[n] = org1 + ((double)cj + s1) * h1;
+__global__ void k_to64(Bunch32View v, double *x, double *y, double *px, double *py) {
+  for (long long n = gtid(); n < v.b.n; n += (long long)gridDim.x * blockDim.x) {
+    double a, c, p0, p1;
+    v(n, a, c, p0, p1);
+    if (x) x[n] = a;
+    if (y) y[n] = c;
     if (px) px[n] = p0;
     if (py) py[n] = p1;
   }
@@ -648,7 +622,8 @@ void launch_to64(const Bunch32 &b, double P0, double P1, double kh0, double kh1,
                  double org1, double h0, double h1, double *x, double *y, double *px, double *py,
                  cudaStream_t s) {
   if (b.n > 0)
-    k_to64<<<grid_for(b.n), 256, 0, s>>>(b, P0, P1, kh0, kh1, pending, org0, org1, h0, h1, x, y, px, py);
+    k_to64<<<grid_for(b.n), 256, 0, s>>>(Bunch32View{b, P0, P1, kh0, kh1, pending, org0, org1, h0, h1}, x, y, px,
+                                         py);
 }
 
 // Mean-momentum sums: part holds 2 x 296 doubles, out2 receives the two sums.
