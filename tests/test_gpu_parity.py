@@ -294,6 +294,40 @@ def test_error_paths(gpu_lib):
     assert e.value.code == -1
 
 
+@pytest.mark.parametrize("fp32", [False, True])
+def test_rejected_bunch_keeps_the_loaded_one(gpu_lib, fp32):
+    """The bunch is checked on the device after the upload: the error names
+    the first rejected particle and why (non-finite values; in FP32 mode also
+    a position off the static mesh), and the bunch already loaded stays in
+    place and keeps stepping."""
+    cfg, spec = workload("small-1")
+    s = Simulation(cfg, fp32=fp32)
+    bunch = make_bunch(spec)
+    s.load(*bunch)
+    s.step(2)
+    before = s.particles()
+    x, y, px, py, q = (a.copy() for a in bunch)
+    q[40] = np.inf
+    py[11] = np.nan
+    x[25] = -1.0                      # off the static mesh
+    with pytest.raises(CsrstError) as e:
+        s.load(x, y, px, py, q)
+    assert e.value.code == -1 and "non-finite particle data at index 11" in str(e.value)
+    py[11] = 0.0
+    with pytest.raises(CsrstError) as e:
+        s.load(x, y, px, py, q)
+    assert e.value.code == -1
+    if fp32:
+        assert "outside the static mesh at index 25" in str(e.value)
+    else:
+        assert "non-finite particle data at index 40" in str(e.value)
+    for a, b in zip(s.particles(), before):
+        assert np.array_equal(a, b)
+    s.step(1)
+    s.sync()
+    s.close()
+
+
 @pytest.mark.parametrize("name", ["small-0", "small-1", "small-2", "small-1-bend"])
 def test_line_fields(gpu_lib, oracle, name):
     """SaveEMFieldsCommand's line samples (SaveEMFields.cpp:34-189) on the
