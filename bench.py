@@ -577,9 +577,9 @@ def run_b200(args, world, rank, local):
     if other in runs:
         out[other] = summary(other)
         out[f"{head}_over_{other}"] = round(hs["value"] / out[other]["value"], 3)
-    # launches per step: 2 pushes x (prep, push, post, bounds) + 4 sub-steps x
-    # (sweep, exchange) + move
-    out["gpu_launches"] = args.steps * (2 * 4 + 4 * 2 + 1)
+    # launches per step: 2 pushes x (prep, push, post, bounds; FP32 mode's push
+    # is two launches, move and deposit) + 4 sub-steps x (sweep, exchange) + move
+    out["gpu_launches"] = args.steps * (2 * (5 if head == "fp32" else 4) + 4 * 2 + 1)
     if rank == 0 and not args.no_compare:
         out["accuracy_fp32_vs_fp64"] = accuracy(cfg, spec, bunch)
     if not args.no_ensemble:
