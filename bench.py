@@ -75,6 +75,17 @@ def dist_setup():
     return world, rank, local
 
 
+def max_over_ranks(value, world, device="cuda"):
+    """The largest of every rank's value (each rank calls this with its own
+    measurement): a multi-GPU time is the slowest replica's."""
+    if world <= 1:
+        return value
+    import torch
+    t = torch.tensor([value], device=device, dtype=torch.float64)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
 def peaks(bf16=False):
     """HBM GB/s (and, with bf16=True, (hbm, dense BF16 TFLOP/s burst, source))
     from MEASURED_PEAKS.json, else the pool's fallback figures."""
@@ -167,11 +178,8 @@ def time_mode(args, cfg, bunch, world, fp32, clocks):
     t1.record(stream)
     sim.sync()
     torch.cuda.synchronize()
-    ms = t0.elapsed_time(t1)
+    ms = max_over_ranks(t0.elapsed_time(t1), world)
     if world > 1:
-        t = torch.tensor([ms], device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms = float(t.item())
         torch.distributed.barrier()
     # ---- kernel attribution: the same steps launched group by group ----
     groups = {"push": 0.0, "yee": 0.0, "move": 0.0}
@@ -619,11 +627,7 @@ def run_e2e(args, cfg, spec, bunch, rank, world, fp32):
     from csrst_b200._lib import lib, ptr
     lib().csrst_get_particles(sim.h, *map(ptr, outp))
     torch.cuda.synchronize()
-    el = time.perf_counter() - t
-    if world > 1:
-        tt = torch.tensor([el], device="cuda")
-        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
-        el = float(tt.item())
+    el = max_over_ranks(time.perf_counter() - t, world)
     k = args.warmup + args.steps
     sim.close()
     return {"value": round(world * n * k / el, 1), "unit": UNIT,
