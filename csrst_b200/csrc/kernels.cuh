@@ -207,7 +207,7 @@ struct Push32Args {
   double h0, h1, dt;                   // spacing and time step (current scale)
   double org0, org1;                   // static mesh origin (dipole position)
   double bz, Lb, hw, chh, shh, bwidth; // hard-edge dipole
-  // single-member push: the move's hand-over to the deposit, n entries each
+  // the move launch's hand-over to the deposit launch, n entries each
   // (deposit start R0 in cells from the old cell, NaN if not moved; old cell)
   double *dep_r0;                      // 2 n
   int *dep_cell;                       // n
