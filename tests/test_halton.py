@@ -35,3 +35,21 @@ def test_bunch_moments_charges_and_order():
     k = np.arange(1, n + 1)
     r = np.sqrt(-2 * np.log(radical_inverse(k, 2)))
     assert np.allclose(py, 0.5 * r * np.sin(2 * np.pi * radical_inverse(k, 3)), rtol=0, atol=1e-15)
+
+
+def test_cpp_distribution_matches_python(tmp_path):
+    """include/csrst/distribution.hpp builds the same bunch as the Python
+    restatement: the same row-and-x order, values equal to a few ulps (the two
+    sides' log, sqrt, cos and sin libraries may round differently)."""
+    import subprocess
+    from pathlib import Path
+    root = Path(__file__).resolve().parents[1]
+    exe, out = tmp_path / "halton_main", tmp_path / "bunch.bin"
+    subprocess.run(["g++", "-std=c++17", "-O2", "-I", str(root / "include"), str(root / "tests/cpp/halton_main.cpp"),
+                    "-o", str(exe)], check=True)
+    subprocess.run([str(exe), str(out)], check=True)
+    got = np.fromfile(out, dtype=np.float64).reshape(5, 3000)
+    ref = halton_bunch(3000, mean_rx=1.7e-3, mean_ry=1.0e-3, sigma_x=40e-6, ekin_mev=510.489, sigma_p=1.0,
+                       qtotal_nc=1.0, origin=(-20e-6, -20e-6), spacing=(20e-6, 20e-6))
+    for a, b in zip(got, ref):
+        assert np.allclose(a, b, rtol=4e-16 * 8, atol=0), np.abs(a - b).max()
