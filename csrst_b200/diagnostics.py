@@ -256,6 +256,111 @@ class VtkSink:
             f.write('  </Collection>\n</VTKFile>\n')
 
 
+def bend_frame(cfg):
+    """(center0, center1, phi) of the bend as the reference sets it up
+    (Bend ctor and Bend::Init, Bend.cpp:60-124): cfg has bz [T], ekin_mev,
+    phi_deg, length_before and width [m]."""
+    import math
+    mass, ekin = 0.511e6, cfg.ekin_mev * 1e6
+    if abs(cfg.bz) > 1e-8:
+        R = math.sqrt(ekin * ekin + 2. * ekin * mass) / (299792458.0 * abs(cfg.bz))
+        phi = -cfg.bz / abs(cfg.bz) * abs(cfg.phi_deg) * math.pi / 180.
+    else:
+        R, phi = 9999999.9, 0.0
+    c1 = 0.5 * cfg.width - R if cfg.bz <= 0.0 else 0.5 * cfg.width + R
+    return cfg.length_before, c1, phi
+
+
+def inside_bend(frame, r):
+    """Bend::isInsideBend (Bend.hh:308-322): r between the entrance plane and
+    the exit plane of the bend, measured from its center."""
+    import math
+    c0, c1, phi = frame
+    d0, d1 = r[0] - c0, r[1] - c1
+    rot0 = math.cos(phi) * d0 + (-math.sin(phi)) * d1
+    if d0 < 0.0 or rot0 > 0.0:
+        return False
+    return d0 > 0.0 and rot0 < 0.0
+
+
+class IntegrateElong:
+    """IntegrateElongCommand (src/Commands/IntegrateElong.cpp:14-125): at each
+    execute() the longitudinal field E_s sampled on the bunch axis at window
+    columns 2 .. L0-3 (csrst_diag_wake: along the mean momentum through the
+    centroid; NaN where the sample's cell is off the window) is added to a
+    per-sample Kahan sum in long double (Utils::KahanSum, utils.hh:513-521);
+    write(fname) puts one line per sample, "position from the centroid <tab>
+    -dt_sample x sum" in the default 6-digit stream format, the position being
+    window origin + column h - current centroid x.  dt_sample is the time
+    between calls (the reference passes statmodulus x dt, main.cpp:370)."""
+
+    def __init__(self, sim, dt_sample):
+        import numpy as np
+        self.sim, self.dt = sim, float(dt_sample)
+        self.n = sim.window()[0][2] - 4
+        self.sum = np.zeros(self.n, dtype=np.longdouble)
+        self.corr = np.zeros(self.n, dtype=np.longdouble)
+
+    def reset(self):
+        self.sum[:] = 0
+        self.corr[:] = 0
+
+    def execute(self):
+        import numpy as np
+        e = np.asarray(self.sim.wake(), dtype=np.float64)
+        ok = ~np.isnan(e)
+        y = e[ok].astype(np.longdouble) - self.corr[ok]
+        t = self.sum[ok] + y
+        self.corr[ok] = (t - self.sum[ok]) - y
+        self.sum[ok] = t
+
+    def write(self, fname):
+        import numpy as np
+        d = os.path.dirname(fname)
+        if d:
+            os.makedirs(d, exist_ok=True)
+        _, origin, _ = self.sim.window()
+        r0 = float(self.sim.moments()[0])
+        h0 = float(self.sim.info()["hx"])
+        line = self.sum.astype(np.float64)
+        with open(fname, "w") as f:
+            for i in range(self.n):
+                pos = float(origin[0]) + (2 + i) * h0 - r0
+                f.write("%g\t%g\n" % (pos, -self.dt * float(line[i])))
+
+
+class EnergyChange:
+    """The reference loop's energy-change files (main.cpp:370, :445-465,
+    :517): an IntegrateElong over the statistics steps, written to
+    energyChangeBefore.dat when the bunch's front (rmax) first enters the
+    bend, to energyChangeInBend.dat when front and back (rmin) have both
+    left it, and to energyChangeAfter.dat at finish(); the sum restarts after
+    each file.  Call execute() on every statistics step, after the
+    statistics row (the reference reads the same step's moments)."""
+
+    def __init__(self, sim, cfg, stat_modulus, directory="Data"):
+        self.sim, self.dir = sim, directory
+        self.ielc = IntegrateElong(sim, stat_modulus * sim.info()["dt"])
+        self.frame = bend_frame(cfg)
+        self.before, self.in_bend = True, False
+
+    def execute(self):
+        m = self.sim.moments()
+        rmin, rmax = m[10:12], m[12:14]
+        if self.before and inside_bend(self.frame, rmax):
+            self.ielc.write(os.path.join(self.dir, "energyChangeBefore.dat"))
+            self.ielc.reset()
+            self.before, self.in_bend = False, True
+        if self.in_bend and not inside_bend(self.frame, rmax) and not inside_bend(self.frame, rmin):
+            self.ielc.write(os.path.join(self.dir, "energyChangeInBend.dat"))
+            self.ielc.reset()
+            self.in_bend = False
+        self.ielc.execute()
+
+    def finish(self):
+        self.ielc.write(os.path.join(self.dir, "energyChangeAfter.dat"))
+
+
 def read_vtr(path):
     """{name: float32 array} of a piece written by VtkSink (appended raw data)."""
     import re

@@ -5,6 +5,7 @@
 //   SaveEMFieldsCommand  FieldOnLine_NNNN.dat     (src/Commands/SaveEMFields.cpp:34-189)
 //   PlotBinaryVTKCommand XML RectilinearGrid      (src/Commands/PlotBinaryVTK.cpp:29-119,
 //                        series + collection       src/Commands/BinaryVTKFile.cpp:25-78)
+//   IntegrateElongCommand energyChange*.dat       (src/Commands/IntegrateElong.cpp:14-125)
 // The GPU supplies the numbers (moments, field-energy sums, line samples,
 // field read-back); the files are written here on the host, byte for byte as
 // csrst_b200/diagnostics.py writes them.  The functions in `format` take
@@ -12,6 +13,7 @@
 #pragma once
 
 #include <array>
+#include <cmath>
 #include <cstdint>
 #include <cstdio>
 #include <fstream>
@@ -236,7 +238,95 @@ inline std::vector<double> read_vtk_collection(const std::string &dir, const std
   return t;
 }
 
+// Kahan sums in long double (Utils::KahanSum, src/utils.hh:513-521) of the
+// finite samples e[k] into sum[k], corr[k].
+inline void kahan_add(std::vector<long double> &sum, std::vector<long double> &corr, const double *e) {
+  for (size_t k = 0; k < sum.size(); ++k) {
+    if (e[k] != e[k]) continue;  // NaN: the sample's cell is off the window
+    const long double y = (long double)e[k] - corr[k];
+    const long double t = sum[k] + y;
+    corr[k] = (t - sum[k]) - y;
+    sum[k] = t;
+  }
+}
+
+// IntegrateElongCommand::write (IntegrateElong.cpp:91-125): per sample at
+// window column 2 + k, "origin0 + column h0 - rmean0 <tab> -dt x sum" in the
+// default stream format.
+inline void energy_change_file(const std::string &path, double origin0, double h0, double rmean0, double dt,
+                               const std::vector<long double> &sum) {
+  std::FILE *f = std::fopen(path.c_str(), "w");
+  if (!f) throw Error(CSRST_E_IO, "cannot write " + path);
+  for (size_t k = 0; k < sum.size(); ++k) {
+    const double pos = origin0 + (double)(2 + (long long)k) * h0 - rmean0;
+    std::fprintf(f, "%g\t%g\n", pos, -dt * (double)sum[k]);
+  }
+  std::fclose(f);
+}
+
 }  // namespace format
+
+// The bend's frame as the reference sets it up (Bend ctor and Bend::Init,
+// src/Bend.cpp:60-124): center and deflection angle.
+struct BendFrame {
+  double c0, c1, phi;
+};
+
+inline BendFrame bend_frame(const csrst_config &c) {
+  const double mass = 0.511e6, ekin = c.ekin_mev * 1e6;
+  double R = 9999999.9, phi = 0.0;
+  if (std::abs(c.bz) > 1e-8) {
+    R = std::sqrt(ekin * ekin + 2. * ekin * mass) / (299792458.0 * std::abs(c.bz));
+    phi = -c.bz / std::abs(c.bz) * std::abs(c.phi_deg) * 3.14159265358979323846 / 180.;
+  }
+  return {c.length_before, c.bz <= 0.0 ? 0.5 * c.width - R : 0.5 * c.width + R, phi};
+}
+
+// Bend::isInsideBend (src/Bend.hh:308-322).
+inline bool inside_bend(const BendFrame &b, double r0, double r1) {
+  const double d0 = r0 - b.c0, d1 = r1 - b.c1;
+  const double rot0 = std::cos(b.phi) * d0 + (-std::sin(b.phi)) * d1;
+  if (d0 < 0.0 || rot0 > 0.0) return false;
+  return d0 > 0.0 && rot0 < 0.0;
+}
+
+// IntegrateElongCommand (src/Commands/IntegrateElong.cpp:14-125): E_s on the
+// bunch axis at window columns 2 .. L0-3 (csrst_diag_wake) summed over the
+// calls; dt_sample is the time between calls (statmodulus x dt, main.cpp:370).
+class IntegrateElongCommand {
+ public:
+  IntegrateElongCommand(Simulation &s, double dt_sample) : s_(s), dt_(dt_sample) {
+    int w[4], gb[4];
+    double o[2];
+    check(csrst_get_window(s.handle(), w, o, gb), s.handle());
+    n_ = w[2] - 4;
+    sum_.assign((size_t)n_, 0.0L);
+    corr_.assign((size_t)n_, 0.0L);
+  }
+  void execute() {
+    std::vector<double> e((size_t)n_);
+    check(csrst_diag_wake(s_.handle(), e.data(), n_), s_.handle());
+    format::kahan_add(sum_, corr_, e.data());
+  }
+  void write(const std::string &path) const {
+    int w[4], gb[4];
+    double o[2], m[18], info[8];
+    check(csrst_get_window(s_.handle(), w, o, gb), s_.handle());
+    check(csrst_diag_moments(s_.handle(), m), s_.handle());
+    check(csrst_get_info(s_.handle(), info), s_.handle());
+    format::energy_change_file(path, o[0], info[0], m[0], dt_, sum_);
+  }
+  void reset() {
+    sum_.assign((size_t)n_, 0.0L);
+    corr_.assign((size_t)n_, 0.0L);
+  }
+
+ private:
+  Simulation &s_;
+  double dt_;
+  int n_ = 0;
+  std::vector<long double> sum_, corr_;
+};
 
 // CalcEnergyCommand over a Simulation: the total field energy [J] per call.
 class CalcEnergyCommand {

@@ -10,6 +10,10 @@ void run(csrst::Simulation &s) {
   csrst::PlotBinaryVTKCommand plot(s), mini(s, "mm", ".", true);
   plot.execute(0.0);
   mini.execute(0.0);
+  csrst::IntegrateElongCommand ielc(s, 1e-12);
+  ielc.execute();
+  if (csrst::inside_bend(csrst::bend_frame(s.config()), 0.0, 0.0)) ielc.write("energyChangeBefore.dat");
+  ielc.reset();
 }
 
 int main(int argc, char **) { return argc > 99 ? (run(*(csrst::Simulation *)nullptr), 0) : 0; }

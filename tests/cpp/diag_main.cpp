@@ -1,6 +1,7 @@
 // Writes the statistics, line-field and VTK files of include/csrst/diagnostics.hpp
 // from fixed host arrays (no GPU) into the directory argv[1], for comparison
 // with the Python writers on the same values.
+#include <cmath>
 #include <cstdio>
 #include <string>
 #include <vector>
@@ -57,6 +58,16 @@ int main(int argc, char **argv) {
   for (int n = 0; n < L0 * L1; ++n) w.hz[n] = wp[2][n] + wp[3][n];
   csrst::format::vtk_step(dir, "mm", 0, w);
   csrst::format::vtk_collection(dir, "mm", {0.0});
+  // energy change: Kahan sums of three sample sets (NaN where off the window)
+  std::vector<long double> sum(8, 0.0L), corr(8, 0.0L);
+  for (int k = 0; k < 3; ++k) {
+    double e[8];
+    for (int i = 0; i < 8; ++i) e[i] = (double)((k * 7 + i * 13) % 17 - 8) * 1.5e4;
+    e[0] = std::nan("");
+    if (k % 2) e[7] = std::nan("");
+    csrst::format::kahan_add(sum, corr, e);
+  }
+  csrst::format::energy_change_file(dir + "/energyChange.dat", 0.5e-3, 0.25e-3, 0.75e-3, 5e-12, sum);
   const std::vector<double> back = csrst::format::read_vtk_collection(dir, "c");
   std::printf("collection %zu %g %g\n", back.size(), back.size() > 1 ? back[1] : -1.0, back.empty() ? -1.0 : back[0]);
   return 0;

@@ -55,6 +55,33 @@ class _FakeSim:
         return w
 
 
+class _ElongSim:
+    """What IntegrateElong reads: a 12-column window, three wake sample sets,
+    the centroid at x = 0.75 mm."""
+
+    def __init__(self):
+        self.k = 0
+
+    def window(self):
+        return [3, 2, 12, 5], np.array([0.5e-3, 2.5e-3]), None
+
+    def info(self):
+        return {"hx": 0.25e-3, "hy": 0.25e-3, "dt": 1e-12}
+
+    def wake(self):
+        e = np.array([((self.k * 7 + i * 13) % 17 - 8) * 1.5e4 for i in range(8)], dtype=float)
+        e[0] = np.nan
+        if self.k % 2:
+            e[7] = np.nan
+        self.k += 1
+        return e
+
+    def moments(self):
+        m = np.zeros(18)
+        m[0] = 0.75e-3
+        return m
+
+
 def test_cpp_writers_match_python(tmp_path):
     exe = tmp_path / "diag_main"
     subprocess.run(["g++", "-std=c++17", "-O2", "-I", str(ROOT / "include"), str(ROOT / "tests/cpp/diag_main.cpp"),
@@ -72,8 +99,14 @@ def test_cpp_writers_match_python(tmp_path):
     vs.execute(1e-12)
     vs.execute(2e-12)
     VtkSink(sim, base="mm", directory=str(pdir), source="window").execute(0.0)
+    from csrst_b200.diagnostics import IntegrateElong
+    ie = IntegrateElong(_ElongSim(), 5e-12)
+    for _ in range(3):
+        ie.execute()
+    ie.write(str(pdir / "energyChange.dat"))
     names = ["stats.stat", "FieldOnLine_0000.dat", "c_0000_node00000.vtr", "c_0001_node00000.vtr", "c_0000.pvtr",
-             "c_0001.pvtr", "c_collection.pvd", "mm_0000_node00000.vtr", "mm_0000.pvtr", "mm_collection.pvd"]
+             "c_0001.pvtr", "c_collection.pvd", "mm_0000_node00000.vtr", "mm_0000.pvtr", "mm_collection.pvd",
+             "energyChange.dat"]
     for n in names:
         assert filecmp.cmp(cdir / n, pdir / n, shallow=False), n
 

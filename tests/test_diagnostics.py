@@ -2,6 +2,9 @@
 supplies moments and field sums): the reference's SDDS1 header with its 16
 columns, the row layout, and the field energy's time average
 0.25 eps0 (E_now + E_last) + 0.5 mu0 H (CalcEnergy.cpp)."""
+import math
+import os
+
 import numpy as np
 
 from csrst_b200.diagnostics import COLUMNS, EPSILON_0, MU_0, DataSink, read_sdds
@@ -111,3 +114,88 @@ def test_vtk_piece_header_and_collection(tmp_path):
     assert np.allclose(w["X_COORDINATES"], np.arange(4) * 0.5 + 0.5)
     Ew = w["E-Field"].reshape(3, 4, 3)
     assert Ew.shape == (3, 4, 3) and Ew[1, 1, 0] == 10001.0 and Ew[0, 0, 1] == 20000.0
+
+
+class _ElongSim:
+    """A Simulation stand-in for IntegrateElong / EnergyChange: a 12-column
+    window (8 samples), wake samples with NaN where off the window, and a
+    centroid that moves along x by 1 mm per moments() call."""
+
+    def __init__(self):
+        self.calls = 0
+        self.k = 0
+
+    def window(self):
+        return [3, 2, 12, 5], np.array([0.5e-3, 2.5e-3]), None
+
+    def info(self):
+        return {"hx": 0.25e-3, "hy": 0.25e-3, "dt": 1e-12}
+
+    def wake(self):
+        e = np.array([((self.k * 7 + i * 13) % 17 - 8) * 1.5e4 for i in range(8)], dtype=float)
+        e[0] = np.nan
+        if self.k % 2:
+            e[-1] = np.nan
+        self.k += 1
+        return e
+
+    def moments(self):
+        m = np.zeros(18)
+        x = 1e-3 * self.calls
+        self.calls += 1
+        m[0] = x
+        m[10], m[11], m[12], m[13] = x - 0.2e-3, 1e-3, x + 0.2e-3, 1.2e-3
+        return m
+
+
+def elong_samples(k):
+    e = np.array([((k * 7 + i * 13) % 17 - 8) * 1.5e4 for i in range(8)], dtype=float)
+    e[0] = np.nan
+    if k % 2:
+        e[-1] = np.nan
+    return e
+
+
+def test_integrate_elong_kahan_sum_and_file(tmp_path):
+    """IntegrateElongCommand: long-double Kahan sums of the finite samples,
+    written as (position from the centroid, -dt x sum) per sample."""
+    from csrst_b200.diagnostics import IntegrateElong
+    sim = _ElongSim()
+    ie = IntegrateElong(sim, 5e-12)
+    for _ in range(3):
+        ie.execute()
+    ref = np.nansum(np.stack([elong_samples(k) for k in range(3)]), axis=0)
+    assert np.allclose(ie.sum.astype(float), ref, rtol=1e-15, atol=0)
+    p = tmp_path / "ec.dat"
+    ie.write(str(p))
+    rows = np.loadtxt(p)
+    assert rows.shape == (8, 2)
+    assert np.allclose(rows[:, 0], 0.5e-3 + (2 + np.arange(8)) * 0.25e-3 - 0.0, rtol=1e-5)
+    assert np.allclose(rows[:, 1], -5e-12 * ref, rtol=1e-5)
+    ie.reset()
+    assert not ie.sum.any()
+
+
+def test_energy_change_files_follow_the_bend():
+    """The loop's three energy-change files: before the bend until the front
+    enters it, in the bend until the back has left it, after at the end."""
+    import tempfile
+    from types import SimpleNamespace
+    from csrst_b200.diagnostics import EnergyChange, bend_frame, inside_bend
+    # a bend of 4.7 mm radius (1 MeV, 1 T) starting at x = 3 mm, 30 degrees; bz < 0
+    # puts the center below the pipe and deflects by +30 degrees
+    cfg = SimpleNamespace(bz=-1.0, ekin_mev=1.0, phi_deg=30.0, length_before=3e-3, width=4e-3)
+    fr = bend_frame(cfg)
+    assert fr[0] == 3e-3 and fr[1] < 0 and abs(fr[2] - math.pi / 6) < 1e-15
+    assert not inside_bend(fr, (2e-3, 1e-3)) and inside_bend(fr, (4e-3, 1e-3))
+    with tempfile.TemporaryDirectory() as d:
+        sim = _ElongSim()
+        ec = EnergyChange(sim, cfg, 5, directory=d)
+        written = []
+        for _ in range(12):
+            before = set(os.listdir(d))
+            ec.execute()
+            written += sorted(set(os.listdir(d)) - before)
+        ec.finish()
+        assert written == ["energyChangeBefore.dat", "energyChangeInBend.dat"]
+        assert "energyChangeAfter.dat" in os.listdir(d)
