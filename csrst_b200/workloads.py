@@ -230,7 +230,7 @@ def radical_inverse(n, base):
 
 def halton_bunch(n=50000, mean_rx=0.05, mean_ry=0.0, sigma_x=0.01, ekin_mev=250.0, sigma_p=1.0, qtotal_nc=-1.0,
                  origin=(0.0, 0.0), spacing=(1.0, 1.0)):
-    """The bunch the reference builds from its command line (Distribution.cpp:55-131;
+    """The bunch the reference builds from its command line (Distribution.cpp:55-131 and gaussian2DSample :145-153;
     defaults from main.cpp:126-133): point k (k = 1 .. n) of the 2D Halton
     sequence (bases 2, 3) becomes a round Gaussian sample by Box-Muller,
     sigma sqrt(-2 ln v0) (cos, sin)(2 pi v1).  Positions and momentum offsets
