@@ -147,6 +147,14 @@ class Simulation:
     def move(self):
         self._ck(lib().csrst_move_window(self.h))
 
+    def step_first(self):
+        """TETMSolver::updateField_firstStep: push(Jx), half H, Ex, half H, back drift."""
+        self._ck(lib().csrst_step_first(self.h))
+
+    def step_second(self):
+        """TETMSolver::updateField_secondStep: push(Jy), Ey, back drift."""
+        self._ck(lib().csrst_step_second(self.h))
+
     def step(self, n=1):
         self._ck(lib().csrst_step(self.h, n))
 
@@ -290,10 +298,10 @@ class TETMSolver:
         return self.sim.info()["dt"]
 
     def updateField_firstStep(self):
-        check(lib().csrst_step_first(self.sim.h), self.sim.h)
+        self.sim.step_first()
 
     def updateField_secondStep(self):
-        check(lib().csrst_step_second(self.sim.h), self.sim.h)
+        self.sim.step_second()
 
 
 def moveMesh(sim: Simulation):
