@@ -385,11 +385,13 @@ class SaveEMFieldsCommand {
  public:
   explicit SaveEMFieldsCommand(Simulation &s, const std::string &dir = "Data", bool with_current = false)
       : s_(s), dir_(dir), with_current_(with_current) {}
-  std::string execute() {
+  std::string execute() { return execute(with_current_); }
+  // with_current for this file only (the reference's plot steps copy the current)
+  std::string execute(bool with_current) {
     int n = 0;
-    check(csrst_diag_line_fields(s_.handle(), with_current_ ? 1 : 0, nullptr, 0, &n), s_.handle());
+    check(csrst_diag_line_fields(s_.handle(), with_current ? 1 : 0, nullptr, 0, &n), s_.handle());
     std::vector<double> rows((size_t)7 * n);
-    check(csrst_diag_line_fields(s_.handle(), with_current_ ? 1 : 0, rows.data(), n, &n), s_.handle());
+    check(csrst_diag_line_fields(s_.handle(), with_current ? 1 : 0, rows.data(), n, &n), s_.handle());
     char name[32];
     std::snprintf(name, sizeof name, "/FieldOnLine_%04d.dat", iteration_++);
     const std::string path = dir_ + name;

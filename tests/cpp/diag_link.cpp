@@ -7,6 +7,7 @@ void run(csrst::Simulation &s) {
   ds.execute(0.0);
   csrst::SaveEMFieldsCommand sf(s, ".", true);
   sf.execute();
+  sf.execute(false);
   csrst::PlotBinaryVTKCommand plot(s), mini(s, "mm", ".", true);
   plot.execute(0.0);
   mini.execute(0.0);
