@@ -9,7 +9,7 @@ wake is divided by an amplitude law exp(a . phi(x)) fitted by least squares on
 the training cases (phi: the four log-scaled scalars, the log of the peak line
 density and of its mean squared slope), then by one global rms, so that the
 network fits O(1) values whose squared error weighs each case by its own
-size.  The held-out cases (the last 10 % of the seeded draw) are judged
+size.  The held-out cases (the last 10 % of the seeded draw) are checked
 against their PIC wakes on the bins the PIC window sampled:
   error = || E_surrogate - E_PIC ||_2 / || E_PIC ||_2 over 256 bins x 32 stations.
 """
@@ -182,7 +182,7 @@ def evaluate(model, d, log=print, ref=None):
     the network: the amplitude law times the mean normalised training wake,
     and the nearest training case (in the standardised inputs) rescaled by the
     amplitude law.  ref = (wakes, masks) of the held-out cases from
-    pic_reference() makes the alignment-averaged PIC wake the judge and adds
+    pic_reference() makes the alignment-averaged PIC wake the reference and adds
     the single runs' own scatter about it."""
     tr, te = split(len(d["X"]))
     X6, W, M = d["X"], d["W"].copy(), d["M"].copy()
@@ -208,7 +208,7 @@ def evaluate(model, d, log=print, ref=None):
 
     kinds = np.array([c.kind for c in d["cases"]])[te]
     fam = ("gaussian", "flat_top", "double_horn")
-    out = {"held_out": int(len(te)), "judge": "alignment-averaged PIC" if ref is not None else "single PIC run",
+    out = {"held_out": int(len(te)), "checked_against": "alignment-averaged PIC" if ref is not None else "single PIC run",
            "surrogate": summary(err),
            "by_family": {name: summary(err[kinds == k]) for k, name in enumerate(fam)},
            "baseline_mean_shape": summary(err_mean), "baseline_nearest_case": summary(err_nn)}
@@ -421,7 +421,7 @@ def _summary(e):
 
 def study(d, models=4, steps=40000, variants=100000, top=16, out=None, log=print):
     """The whole workflow on a data set: train `models` networks (seeds 0..),
-    judge each and their mean on the held-out cases against the
+    check each and their mean on the held-out cases against the
     alignment-averaged PIC (with the single PIC runs' own scatter beside it),
     time inference at 65536 profiles, prescreen `variants` production
     profiles, rerun the selected ones in PIC (alignment-averaged) and compare.
@@ -450,7 +450,7 @@ def study(d, models=4, steps=40000, variants=100000, top=16, out=None, log=print
     held = [d["cases"][k] for k in te]
     mean, mask, runs = pic_reference(held, log=None)
     R["eval"] = [evaluate(m, d, ref=(mean, mask), log=None)[0] for m in nets]
-    R["eval_single_pic_judge"] = evaluate(nets[0], d, log=None)[0]
+    R["eval_against_single_pic"] = evaluate(nets[0], d, log=None)[0]
     P = np.mean([m.predict(d["X"][te]) for m in nets], axis=0)
     err = rel_errors(P, mean, mask)
     kinds = np.array([c.kind for c in held])

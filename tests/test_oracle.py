@@ -4,7 +4,7 @@ test/scattergather.cpp tabulates the IntCIC / IntS1 / IntS2 scatter weights
 of one particle at (3.3, 3.2) (golden file tests/golden/scattergather.json);
 test/calcCurrent.cpp and test/calcCurrentS1.cpp check that the deposited
 current satisfies the discrete continuity equation against the matching
-charge shape.  These pin the oracle before it is used to judge the GPU.
+charge shape.  These pin the oracle before the GPU is checked against it.
 """
 import json
 from pathlib import Path
