@@ -523,6 +523,19 @@ def run_surrogate(args):
     return out
 
 
+DATA = "synthetic (seeded Gaussian bunch; initial fields from the GPU multigrid Poisson solve)"
+
+
+def run_config(args, cfg, spec, world, window, h):
+    """The workload as both arms name it (the precision is the line's dtype)."""
+    return {"workload": f"{args.workload}: {cfg.Nx}x{cfg.Ny} static mesh, h={1e6 * h:.3g}um, "
+                        f"{spec.n} particles, shape order {cfg.shape_order}, CFL 0.5",
+            "Nx": cfg.Nx, "Ny": cfg.Ny, "particles": spec.n, "shape_order": cfg.shape_order,
+            "window": [int(v) for v in window], "parallelism": f"replicas x{world}",
+            "l2": "inputs larger than L2 (126 MB): 4 static planes of %.3g M cells, %.3g M particles" % (
+                cfg.Nx * cfg.Ny / 1e6, spec.n / 1e6)}
+
+
 def run_b200(args, world, rank, local):
     import torch
     from csrst_b200.workloads import make_bunch, workload
@@ -571,13 +584,8 @@ def run_b200(args, world, rank, local):
     out = {"metric": METRIC, "value": hs["value"], "unit": UNIT, "n_gpus": world,
            "steps": args.steps, "warmup": args.warmup, "ms_per_step": hs["ms_per_step"],
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": dtype,
-           "data": "synthetic (seeded Gaussian bunch; initial fields from the GPU multigrid Poisson solve)",
-           "config": {"workload": f"{args.workload}: {cfg.Nx}x{cfg.Ny} static mesh, h={1e6 * runs[head]['hx']:.3g}um,"
-                                  f" {n} particles, shape order {cfg.shape_order}, CFL 0.5, {head.upper()}",
-                      "Nx": cfg.Nx, "Ny": cfg.Ny, "particles": n, "shape_order": cfg.shape_order,
-                      "window": runs[head]["window"], "precision": head, "parallelism": f"replicas x{world}",
-                      "l2": "inputs larger than L2 (static fields 4 x %.0f MB, particles %.0f MB)" % (
-                          cells * (4 if head == "fp32" else 8) / 1e6, n * (24 if head == "fp32" else 40) / 1e6)},
+           "data": DATA,
+           "config": run_config(args, cfg, spec, world, runs[head]["window"], runs[head]["hx"]),
            "cell_updates_per_s": hs["cell_updates_per_s"],
            "roofline": hs["roofline"], "roofline_other": hs["roofline_other"],
            "kernel_ms_per_step": hs["kernel_ms_per_step"], "initial_fields": hs["initial_fields"],
@@ -636,74 +644,84 @@ def run_e2e(args, cfg, spec, bunch, rank, world, fp32):
                                     "(zero initial fields: the solve is reported under initial_fields)"}
 
 
-def oracle_sample(cfg, spec, bunch, frac, nsteps):
-    """Times the oracle on the full static mesh with a particle sample; the
-    full-workload step time is fields + (N / sample) x particles."""
+def oracle_steps(cfg, bunch, warmup, steps):
+    """The oracle (the CPU restatement of the reference loop, plain FP64 sums
+    in the reference's order) on the full workload: load, `warmup` untimed
+    steps, then `steps` timed steps.  Returns (seconds per step, window size,
+    mesh spacing hx)."""
     from oracle import oracle as O
     d = cfg.dict()
     d["order"] = cfg.shape_order
     s = O.Sim(d)
-    ns = max(1000, int(spec.n * frac))
-    idx = np.linspace(0, spec.n - 1, ns).astype(np.int64)
-    s.load(*[a[idx] for a in bunch])
-    tf = tp = tm = 0.0
-    for _ in range(nsteps):
-        a = time.perf_counter(); s.push(0); b = time.perf_counter()
-        s.half_h(); s.update_e(0); s.half_h(); c = time.perf_counter()
-        s.drift(-0.5 * s.dt); s.push(1); e = time.perf_counter()
-        s.update_e(1); f = time.perf_counter()
-        s.drift(-0.5 * s.dt); s.move(); g = time.perf_counter()
-        tp += (b - a) + (e - c)
-        tf += (c - b) + (f - e)
-        tm += g - f
-    tp, tf, tm = tp / nsteps, tf / nsteps, tm / nsteps
-    full = tf + tm + tp * spec.n / ns
-    return full, tf, tp, ns
+    s.load(*bunch)
+    s.step(warmup)
+    t = time.perf_counter()
+    s.step(steps)
+    el = time.perf_counter() - t
+    hx = O.bend(cfg.Nx, cfg.Ny, cfg.length_before, cfg.length_after, cfg.width, cfg.phi_deg, cfg.ekin_mev,
+                cfg.bz)["hx"]
+    return el / max(steps, 1), list(s.window()[0][2:]), hx
 
 
-def cpu_baseline(cfg, spec, bunch):
-    full, tf, tp, ns = oracle_sample(cfg, spec, bunch, 1 / 16, 2)
-    return {"value": round(spec.n / full, 1), "unit": UNIT, "cores": 1, "kind": "port",
-            "sample": f"oracle (C++ restatement, -O2 -ffp-contract=off), 1 thread: 2 steps on the full "
-                      f"{cfg.Nx}x{cfg.Ny} mesh with {ns} of {spec.n} particles; step time = fields "
-                      f"{tf:.3f}s + particles {tp:.3f}s x {spec.n / ns:.0f}"}
+def cpu_baseline(cfg, spec, bunch, steps=2):
+    sec, _, _ = oracle_steps(cfg, bunch, 0, steps)
+    return {"value": round(spec.n / sec, 1), "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"oracle (C++ restatement of the reference loop, -O2 -ffp-contract=off), 1 thread: "
+                      f"{steps} full steps of the whole workload ({cfg.Nx}x{cfg.Ny} mesh, {spec.n} particles), "
+                      f"{sec:.2f} s per step, nothing extrapolated"}
 
 
 def _ref_worker(args):
-    name, frac, nsteps, seed = args
+    name, seed, warmup, steps = args
     from csrst_b200.workloads import make_bunch, workload
     cfg, spec = workload(name)
     spec.seed = seed
-    return oracle_sample(cfg, spec, make_bunch(spec), frac, nsteps)
+    return oracle_steps(cfg, make_bunch(spec), warmup, steps)
+
+
+def ref_cores():
+    """Host cores the reference arm uses: all it may run on, capped by the
+    memory one full-workload replica needs (about 0.8 GB)."""
+    try:
+        n = len(os.sched_getaffinity(0))
+    except AttributeError:
+        n = os.cpu_count() or 1
+    try:
+        avail = os.sysconf("SC_AVPHYS_PAGES") * os.sysconf("SC_PAGE_SIZE")
+        n = min(n, max(1, int(avail * 0.5 / 0.8e9)))
+    except (ValueError, OSError):
+        pass
+    return max(1, min(n, 64))
 
 
 def run_reference(args, world, rank):
     """The reference arm: the CPU restatement of the reference loop on the
-    box's host cores (independent replicas, one per core), same workload."""
+    box's host cores, one full-workload replica per core (the loop does not
+    shard; replicas are its only parallelism on the host), each running the
+    declared warm-up and timed steps in full.  value = all replicas'
+    particle-steps / the slowest replica's timed seconds."""
     if rank != 0:
         return None
     import multiprocessing as mp
     from csrst_b200.workloads import workload
     cfg, spec = workload(args.workload)
-    cores = max(1, min(os.cpu_count() or 1, 32))
-    # bounded: each replica runs (warmup + steps) sample steps of ~1/64 of the bunch
-    nsteps = max(1, min(args.steps + args.warmup, 4))
+    cores = ref_cores()
     t = time.perf_counter()
     with mp.get_context("spawn").Pool(cores) as pool:
-        res = pool.map(_ref_worker, [(args.workload, 1 / 64, nsteps, 100 + k) for k in range(cores)])
+        res = pool.map(_ref_worker, [(args.workload, spec.seed + k, args.warmup, args.steps) for k in range(cores)])
     wall = time.perf_counter() - t
-    fulls = [r[0] for r in res]
-    value = sum(spec.n / f for f in fulls)
-    ms = 1e3 * float(np.mean(fulls))
+    sec = max(r[0] for r in res)
+    value = cores * spec.n / sec
     return {"impl": "reference", "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": args.workload, "Nx": cfg.Nx, "Ny": cfg.Ny, "particles": spec.n,
-                       "shape_order": cfg.shape_order},
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1e3 * sec, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (the same seeded Gaussian bunch generator; zero initial fields: a step's work does "
+                    "not depend on the field values)",
+            "config": run_config(args, cfg, spec, world, res[0][1], res[0][2]),
             "cpu_baseline": {"value": round(value, 1), "unit": UNIT, "cores": cores, "kind": "port",
-                             "sample": f"{cores} replica processes of the oracle, each {nsteps} steps on the full "
-                                       f"mesh with 1/64 of the bunch, particle time scaled to the full bunch; "
-                                       f"wall {wall:.1f}s"},
+                             "sample": f"{cores} replica processes of the oracle (C++ restatement of the reference "
+                                       f"loop), each the whole workload for {args.warmup} warm-up + {args.steps} "
+                                       f"timed steps; slowest replica {sec:.2f} s per step; wall {wall:.1f} s"},
             "e2e": {"value": round(value, 1), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 

@@ -26,7 +26,7 @@ class Config(C.Structure):
 
 ERRORS = {0: "ok", -1: "invalid argument", -2: "CUDA error", -3: "geometry",
           -4: "no particles", -5: "window fit", -6: "window move", -7: "crossings",
-          -8: "window wall"}
+          -8: "window wall", -9: "i/o", 1: "outside the patch"}
 
 
 class CsrstError(RuntimeError):
@@ -133,8 +133,19 @@ def f64(a):
     return np.ascontiguousarray(a, dtype=np.float64)
 
 
+class CsrstWarning(UserWarning):
+    """A call that succeeded with a positive CSRST_W_* status."""
+
+
 def check(code, handle=None):
+    """Raises CsrstError on a negative status; a positive one (the call
+    succeeded, e.g. CSRST_W_OUTSIDE) is issued as a CsrstWarning."""
     if code != 0:
         buf = C.create_string_buffer(512)
         lib().csrst_get_error(handle, buf, 512)
-        raise CsrstError(code, buf.value.decode(errors="replace"))
+        msg = buf.value.decode(errors="replace")
+        if code > 0:
+            import warnings
+            warnings.warn(f"csrst warning {code} ({ERRORS.get(code, '?')}): {msg}", CsrstWarning, stacklevel=3)
+            return
+        raise CsrstError(code, msg)

@@ -184,6 +184,12 @@ int fail(csrst_handle *h, int code, const std::string &msg) {
   return code;
 }
 
+}  // namespace
+
+int csrst::set_global_error(int code, const char *msg) { return fail(nullptr, code, msg); }
+
+namespace {
+
 int cuda_fail(csrst_handle *h, cudaError_t e, const char *where) {
   return fail(h, CSRST_E_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
 }
@@ -1632,9 +1638,9 @@ static int run_fixed(int kind, int order, int comp, const double *ox, const doub
   const size_t m = (size_t)ni * nj;
   unsigned long long *acc;
   double *dJ;
-  int *derr;
-  CK(cudaMalloc(&acc, m * 8)); CK(cudaMalloc(&dJ, m * 8)); CK(cudaMalloc(&derr, 4));
-  CK(cudaMemset(acc, 0, m * 8)); CK(cudaMemset(derr, 0, 4));
+  int *derr;  // crossing overflow, dropped contribution
+  CK(cudaMalloc(&acc, m * 8)); CK(cudaMalloc(&dJ, m * 8)); CK(cudaMalloc(&derr, 8));
+  CK(cudaMemset(acc, 0, m * 8)); CK(cudaMemset(derr, 0, 8));
   double *d[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
   const double *s[5] = {ox, oy, x, y, q};
   if (n > 0)
@@ -1647,17 +1653,22 @@ static int run_fixed(int kind, int order, int comp, const double *ox, const doub
                    i0, j0, ni, nj, acc, scale, derr, 0);
   else
     launch_charge_diff(order, d[0], d[1], d[2], d[3], d[4], (long long)n, o2[0], o2[1], hh2[0], hh2[1], i0, j0,
-                       ni, nj, acc, scale, 0);
+                       ni, nj, acc, scale, derr + 1, 0);
   launch_fixed_to_double(acc, dJ, (long long)m, 1.0 / scale, 0);
-  int e = 0;
+  int e[2] = {0, 0};
   CK(cudaMemcpy(J, dJ, m * 8, cudaMemcpyDeviceToHost));
-  CK(cudaMemcpy(&e, derr, 4, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(e, derr, 8, cudaMemcpyDeviceToHost));
   if (kind == 1)
     for (size_t k = 0; k < m; ++k) J[k] = J[k] / (hh2[0] * hh2[1]);
   cudaFree(acc); cudaFree(dJ); cudaFree(derr);
   for (double *p : d) cudaFree(p);
   CK(cudaGetLastError());
-  return e ? fail(h, e, "too many cell-border crossings") : CSRST_OK;
+  if (e[0]) return fail(h, e[0], "too many cell-border crossings");
+  if (e[1]) {
+    fail(h, CSRST_W_OUTSIDE, "contributions outside the patch were dropped");
+    return CSRST_W_OUTSIDE;
+  }
+  return CSRST_OK;
 }
 
 int csrst_deposit(int order, int comp, const double *ox, const double *oy, const double *x, const double *y,

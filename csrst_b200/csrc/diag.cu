@@ -201,7 +201,7 @@ template <int ORDER>
 __global__ void k_charge_diff(const double *ox, const double *oy, const double *x, const double *y,
                               const double *q, long long n, double org0, double org1, double h0,
                               double h1, int i0, int j0, int ni, int nj, unsigned long long *acc,
-                              double scale) {
+                              double scale, int *dropped) {
   for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n;
        k += (long long)gridDim.x * blockDim.x) {
     const double qq = q[k];
@@ -210,8 +210,12 @@ __global__ void k_charge_diff(const double *ox, const double *oy, const double *
       const double X = pass == 0 ? x[k] : ox[k], Y = pass == 0 ? y[k] : oy[k];
       auto add = [&](int i, int j, double v) {
         i -= i0; j -= j0;
-        if (i < 0 || j < 0 || i >= ni || j >= nj) return;
-        atomicAdd(&acc[(size_t)j * ni + i], (unsigned long long)__double2ll_rn(sg * v * scale));
+        const long long iv = __double2ll_rn(sg * v * scale);
+        if (i < 0 || j < 0 || i >= ni || j >= nj) {
+          if (iv != 0) *dropped = 1;
+          return;
+        }
+        atomicAdd(&acc[(size_t)j * ni + i], (unsigned long long)iv);
       };
       charge_shape<ORDER>(X, Y, qq, org0, org1, h0, h1, add);
     }
@@ -400,15 +404,15 @@ template void launch_wake<float>(const WinState *, const float *, const float *,
 void launch_charge_diff(int order, const double *ox, const double *oy, const double *x, const double *y,
                         const double *q, long long n, double org0, double org1, double h0, double h1,
                         int i0, int j0, int ni, int nj, unsigned long long *acc, double scale,
-                        cudaStream_t s) {
+                        int *dropped, cudaStream_t s) {
   if (n <= 0) return;
   const int blocks = (int)((n + 255) / 256 < 4096 ? (n + 255) / 256 : 4096);
   if (order == 0)
-    k_charge_diff<0><<<blocks, 256, 0, s>>>(ox, oy, x, y, q, n, org0, org1, h0, h1, i0, j0, ni, nj, acc, scale);
+    k_charge_diff<0><<<blocks, 256, 0, s>>>(ox, oy, x, y, q, n, org0, org1, h0, h1, i0, j0, ni, nj, acc, scale, dropped);
   else if (order == 1)
-    k_charge_diff<1><<<blocks, 256, 0, s>>>(ox, oy, x, y, q, n, org0, org1, h0, h1, i0, j0, ni, nj, acc, scale);
+    k_charge_diff<1><<<blocks, 256, 0, s>>>(ox, oy, x, y, q, n, org0, org1, h0, h1, i0, j0, ni, nj, acc, scale, dropped);
   else
-    k_charge_diff<2><<<blocks, 256, 0, s>>>(ox, oy, x, y, q, n, org0, org1, h0, h1, i0, j0, ni, nj, acc, scale);
+    k_charge_diff<2><<<blocks, 256, 0, s>>>(ox, oy, x, y, q, n, org0, org1, h0, h1, i0, j0, ni, nj, acc, scale, dropped);
 }
 
 }  // namespace csrst

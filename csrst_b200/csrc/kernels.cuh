@@ -86,6 +86,10 @@ struct PushGroup {
   size_t smem;                      // dynamic shared memory of the group's launch
 };
 
+// api.cu: records the message csrst_get_error(NULL) returns and returns code
+// (for entry points that take no handle).
+int set_global_error(int code, const char *msg);
+
 // particles.cu
 PrepArgs prep_args(WinState *ws, double h0, double h1, int order);
 size_t push_tile_bytes(int order);
@@ -107,7 +111,7 @@ void launch_gather(int order, int comp, const double *patch, int nx, double o0, 
 void launch_deposit(int order, int comp, const double *ox, const double *oy, const double *x,
                     const double *y, const double *q, long long n, double org0, double org1, double h0,
                     double h1, double dt, int i0, int j0, int ni, int nj, unsigned long long *acc,
-                    double scale, int *err, cudaStream_t s);
+                    double scale, int *err, cudaStream_t s);  // err: 2 ints (crossings, dropped)
 void launch_fixed_to_double(const unsigned long long *acc, double *out, long long n, double inv,
                             cudaStream_t s);
 // fields.cu (instantiated for T = double and T = float)
@@ -155,7 +159,7 @@ void launch_wake(const WinState *ws, const T *mEx, const T *mEy, int wpitch, int
 void launch_charge_diff(int order, const double *ox, const double *oy, const double *x, const double *y,
                         const double *q, long long n, double org0, double org1, double h0, double h1,
                         int i0, int j0, int ni, int nj, unsigned long long *acc, double scale,
-                        cudaStream_t s);
+                        int *dropped, cudaStream_t s);
 
 // poisson.cu: initial fields of the bunch (PoissonSolver::computeField)
 struct PoissonInput {

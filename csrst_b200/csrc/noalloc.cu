@@ -23,13 +23,14 @@ namespace csrst {
 constexpr long long kNoAllocMaxCells = 1ll << 20;
 
 static __device__ __align__(256) unsigned long long g_noalloc_acc[kNoAllocMaxCells];
-static __device__ int g_noalloc_err;
+// [0]: crossing overflow, [1]: a non-zero contribution fell outside the patch
+static __device__ int g_noalloc_err[2];
 
 __global__ void k_noalloc_clear(unsigned long long *acc, long long m) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < m;
        i += (long long)gridDim.x * blockDim.x)
     acc[i] = 0ull;
-  if (blockIdx.x == 0 && threadIdx.x == 0) g_noalloc_err = 0;
+  if (blockIdx.x == 0 && threadIdx.x == 0) { g_noalloc_err[0] = 0; g_noalloc_err[1] = 0; }
 }
 
 template <int ORDER>
@@ -39,13 +40,17 @@ __global__ void k_noalloc_deposit(int comp, const double *ox, const double *oy, 
                                   unsigned long long *acc, double scale) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x) {
+    bool dropped = false;
     auto sink = [&](int a, int b, double v) {
       a -= i0; b -= j0;
       const bool in = a >= 0 && b >= 0 && a < ni && b < nj;
-      warp_add(acc, in ? b * ni + a : -1, __double2ll_rn(v * scale));
+      const long long iv = __double2ll_rn(v * scale);
+      if (!in && iv != 0) dropped = true;
+      warp_add(acc, in ? b * ni + a : -1, iv);
     };
     if (!deposit_particle<ORDER>(comp, q[i], ox[i], oy[i], x[i], y[i], org0, org1, h0, h1, h0, h1, dt, sink))
-      g_noalloc_err = kErrCrossings;
+      g_noalloc_err[0] = kErrCrossings;
+    if (dropped) g_noalloc_err[1] = 1;
   }
 }
 
@@ -80,11 +85,15 @@ extern "C" int csrst_deposit_noalloc(int order, int comp, const double *ox, cons
   using namespace csrst;
   if (order < 0 || order > 2 || (comp != 0 && comp != 1) || ni <= 0 || nj <= 0 || !o2 || !hh2 || !J ||
       !(scale > 0) || (n > 0 && (!ox || !oy || !x || !y || !q)))
-    return CSRST_E_ARG;
+    return set_global_error(CSRST_E_ARG, "invalid deposit arguments");
   const long long m = (long long)ni * nj;
-  if (m > kNoAllocMaxCells) return CSRST_E_ARG;  // patch larger than the static accumulator
+  if (m > kNoAllocMaxCells)
+    return set_global_error(CSRST_E_ARG, "patch larger than the 2^20-cell accumulator of the allocation-free deposit");
   unsigned long long *acc = nullptr;
-  if (noalloc_scratch(&acc) != kOk) return CSRST_E_CUDA;
+  if (noalloc_scratch(&acc) != kOk) return set_global_error(CSRST_E_CUDA, "cudaGetSymbolAddress failed");
+  // drop an error left by earlier, unrelated work, so that the checks below
+  // see only this call's launches
+  (void)cudaGetLastError();
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   const int gm = (int)((m + 255) / 256 < 2048 ? (m + 255) / 256 : 2048);
   k_noalloc_clear<<<gm, 256, 0, s>>>(acc, m);
@@ -101,9 +110,14 @@ extern "C" int csrst_deposit_noalloc(int order, int comp, const double *ox, cons
                                               dt, i0, j0, ni, nj, acc, scale);
   }
   k_noalloc_out<<<gm, 256, 0, s>>>(acc, J, m, 1.0 / scale);
-  if (cudaGetLastError() != cudaSuccess) return CSRST_E_CUDA;
-  if (cudaStreamSynchronize(s) != cudaSuccess) return CSRST_E_CUDA;
-  int e = 0;
-  if (cudaMemcpyFromSymbol(&e, g_noalloc_err, sizeof(int)) != cudaSuccess) return CSRST_E_CUDA;
-  return e ? CSRST_E_CROSSINGS : CSRST_OK;
+  cudaError_t ce = cudaGetLastError();
+  if (ce != cudaSuccess) return set_global_error(CSRST_E_CUDA, cudaGetErrorString(ce));
+  // the flags come back in stream order, so only this stream is waited for
+  int e[2] = {0, 0};
+  ce = cudaMemcpyFromSymbolAsync(e, g_noalloc_err, sizeof e, 0, cudaMemcpyDeviceToHost, s);
+  if (ce == cudaSuccess) ce = cudaStreamSynchronize(s);
+  if (ce != cudaSuccess) return set_global_error(CSRST_E_CUDA, cudaGetErrorString(ce));
+  if (e[0]) return set_global_error(CSRST_E_CROSSINGS, "too many cell-border crossings");
+  if (e[1]) return set_global_error(CSRST_W_OUTSIDE, "contributions outside the patch were dropped");
+  return CSRST_OK;
 }

@@ -317,15 +317,20 @@ __global__ void k_deposit(int comp, const double *ox, const double *oy, const do
                           const double *y, const double *q, long long n, double org0, double org1,
                           double h0, double h1, double dt, int i0, int j0, int ni, int nj,
                           unsigned long long *acc, double scale, int *err) {
+  // err[0]: crossing overflow; err[1]: a non-zero contribution fell outside the patch
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x) {
+    bool dropped = false;
     auto sink = [&](int a, int b, double v) {
       a -= i0; b -= j0;
       const bool in = a >= 0 && b >= 0 && a < ni && b < nj;
-      warp_add(acc, in ? b * ni + a : -1, __double2ll_rn(v * scale));
+      const long long iv = __double2ll_rn(v * scale);
+      if (!in && iv != 0) dropped = true;
+      warp_add(acc, in ? b * ni + a : -1, iv);
     };
     if (!deposit_particle<ORDER>(comp, q[i], ox[i], oy[i], x[i], y[i], org0, org1, h0, h1, h0, h1, dt, sink))
-      atomicExch(err, kErrCrossings);
+      atomicExch(&err[0], kErrCrossings);
+    if (dropped) atomicExch(&err[1], 1);
   }
 }
 

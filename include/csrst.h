@@ -7,7 +7,9 @@
  *
  * Conventions
  *  - Every call returns an int status: 0 on success, a negative CSRST_E_*
- *    code on failure; csrst_get_error() returns the message of the last one.
+ *    code on failure, a positive CSRST_W_* code when the call succeeded with
+ *    a warning; csrst_get_error() returns the message of the last failure or
+ *    warning.
  *  - Host buffers are copied; device memory is owned by the handle.
  *  - One handle per thread.  A handle is bound to one device and one CUDA
  *    stream; calls are asynchronous on that stream except the ones that
@@ -35,6 +37,7 @@ extern "C" {
 #define CSRST_E_CROSSINGS (-7)     /* a particle crossed more cell borders than one push allows */
 #define CSRST_E_WINDOW_WALL (-8)   /* window or its ring touches a non-inside cell */
 #define CSRST_E_IO (-9)            /* checkpoint file could not be written or read */
+#define CSRST_W_OUTSIDE 1          /* warning: contributions outside the caller's patch were dropped */
 
 typedef struct csrst_handle csrst_handle;
 
@@ -262,7 +265,11 @@ int csrst_gather(int order, int comp, const double *patch, int nx, int ny, const
 /* ShapeFunction<IntOp>::getCurrentDensityBase{X,Y} (ShapeFunction.hh:173-204):
  * current of particles moving old -> new on a mesh with origin o2, spacing
  * hh2, into a dense (ni x nj) patch whose element (0,0) is mesh index
- * (i0, j0).  Accumulated in 64-bit fixed point with the given scale. */
+ * (i0, j0).  Accumulated in 64-bit fixed point with the given scale.  The
+ * reference sizes its patch to hold every contribution (the particle box plus
+ * getExtraMarginCurrent); here the caller chooses the patch, and a non-zero
+ * contribution that falls outside it is dropped and reported by the return
+ * value CSRST_W_OUTSIDE (J is still written).  csrst_charge_diff does the same. */
 int csrst_deposit(int order, int comp, const double *ox, const double *oy, const double *x,
                   const double *y, const double *q, size_t n, const double *o2, const double *hh2,
                   double dt, int i0, int j0, int ni, int nj, double scale, double *J);
@@ -286,10 +293,16 @@ int csrst_charge_diff(int order, const double *ox, const double *oy, const doubl
  *    ni * nj above 2^20 is rejected with CSRST_E_ARG.  Nothing is allocated
  *    or freed (no cudaMalloc, cudaFree or allocating library call).
  *  - The first call on a device looks up the array's device address
- *    (cudaGetSymbolAddress) and should come before any stream capture.
- *  - Runs on `stream` (a cudaStream_t, NULL = default stream) and returns
- *    after it has finished.  All calls share the one array per device, so
- *    calls that overlap on the GPU (other threads or streams) race. */
+ *    (cudaGetSymbolAddress) and keeps it for the life of the process; make
+ *    that first call before any stream capture begins.  After
+ *    cudaDeviceReset the kept address is stale: calls after a reset are not
+ *    supported.
+ *  - Runs on `stream` (a cudaStream_t, NULL = default stream) and waits for
+ *    that stream before it returns, because it reads the crossing and
+ *    dropped-contribution flags back.  All calls share the one array per
+ *    device, so calls that overlap on the GPU (other threads or streams) race.
+ *  - Same return values as csrst_deposit (CSRST_E_CROSSINGS, CSRST_W_OUTSIDE);
+ *    csrst_get_error(NULL) gives the message of a failure or warning. */
 int csrst_deposit_noalloc(int order, int comp, const double *ox, const double *oy, const double *x,
                           const double *y, const double *q, size_t n, const double *o2,
                           const double *hh2, double dt, int i0, int j0, int ni, int nj, double scale,

@@ -25,8 +25,10 @@ struct Error : std::runtime_error {
   Error(int c, const std::string &m) : std::runtime_error(m), code(c) {}
 };
 
-inline void check(int code, const csrst_handle *h = nullptr) {
-  if (code == CSRST_OK) return;
+// Throws on a failure (negative status); a warning (positive status, the
+// call succeeded) is returned to the caller.
+inline int check(int code, const csrst_handle *h = nullptr) {
+  if (code >= CSRST_OK) return code;
   char buf[512];
   csrst_get_error(h, buf, sizeof(buf));
   throw Error(code, "csrst error " + std::to_string(code) + ": " + buf);

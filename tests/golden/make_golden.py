@@ -5,14 +5,16 @@ The reference test places one particle at (3.3, 3.2) on a unit-spacing patch
 with origin 0 and tabulates the scatter weights of IntCIC, IntS1 and IntS2
 for the edge components (Vcheck: i, j, (ex, ey)) and the cell field (Scheck:
 i, j, bz); gathers of a field that is 1 on the support must return 1.
-Usage: python tests/golden/make_golden.py [path to the reference checkout]
+Usage: python tests/golden/make_golden.py <path to the reference checkout>
 """
+import argparse
 import json
 import re
-import sys
 from pathlib import Path
 
-ref = Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+ap.add_argument("reference", type=Path, help="root of the reference checkout (holds test/scattergather.cpp)")
+ref = ap.parse_args().reference
 src = (ref / "test" / "scattergather.cpp").read_text()
 
 sections = re.split(r"// CHECK (CIC|S1|S2)", src)

@@ -244,6 +244,20 @@ def test_c1_full_size_bit_exact(gpu_lib, oracle):
     assert_same_state(g, o)
 
 
+def test_c2_full_size_bit_exact(gpu_lib, oracle):
+    """The headline workload on the FP64 path: 8192 x 1024 static mesh at
+    5 um, the full 4e6-particle TSC bunch, smooth random static fields so that
+    every gather reads non-zero values, 2 steps (4 pushes, 8 field sub-steps,
+    2 window moves) against the oracle: particles, window, static and window
+    fields bit-identical."""
+    cfg, g, o = pair("c2", oracle, fields=True, seed=11)
+    assert len(g.particles()[0]) == 4_000_000
+    g.step(2)
+    o.step(2)
+    assert_same_state(g, o)
+    g.close()
+
+
 def test_continuity_full_size(gpu_lib):
     """Deposit + charge difference of 4e6 particles (the TSC workload's
     bunch) moving for one step: residual <= 1e-10 relative."""
