@@ -233,18 +233,47 @@ def slice_energy_change(cfg, spec, bunch, steps):
     return e64, e32
 
 
+def continuity32(sim, sf):
+    """Continuity of one FP32-mode push (a keep_old handle): the current of
+    its moves from the stand-alone FP32 deposit (csrst_flux32; the push's own
+    window current equals it bit for bit, tests/test_gpu_fp32.py), both
+    components, against (a) the integer charge it assigns, exactly, and (b)
+    the FP64 charge shape (PartBunch's getChargeDensityDiff) in FP64.
+    Returns (max |integer residual|, FP64 residual relative to max |rho/dt|)."""
+    info = sim.info()
+    h, dt, scale = (info["hx"], info["hy"]), info["dt"], info["fixed_scale"]
+    sim.push(0)
+    c1, b0, b1, _, _, q = sim.bunch32(0)
+    c0, a0, a1 = sim.bunch32(1)
+    w, org, _ = sim.window()
+    P0, P1, L0, L1 = w
+    fx, drho = sf.flux32(0, c0, a0, a1, c1, b0, b1, q, scale, P0, P1, L0, L1, with_charge=True)
+    fy = sf.flux32(1, c0, a0, a1, c1, b0, b1, q, scale, P0, P1, L0, L1)
+    exact = int(np.abs(drho[1:, 1:] + (fx[1:, 1:] - fx[1:, :-1]) + (fy[1:, 1:] - fy[:-1, 1:])).max())
+    unpack = lambda c: ((c & 0xFFFF).astype(np.int64), (c.astype(np.uint32) >> 16).astype(np.int64))
+    ci, cj = unpack(c0)
+    ni, nj = unpack(c1)
+    ox, oy = info["ox"] + (ci + a0.astype(np.float64)) * h[0], info["oy"] + (cj + a1.astype(np.float64)) * h[1]
+    x, y = info["ox"] + (ni + b0.astype(np.float64)) * h[0], info["oy"] + (nj + b1.astype(np.float64)) * h[1]
+    q64 = q.astype(np.float64)
+    qs = 2.0 ** np.floor(np.log2(2.0 ** 62 / (4 * np.abs(q64).sum())))
+    rho = sf.getChargeDensityDiff(ox, oy, x, y, q64, org, h, 0, 0, L0, L1, qs)
+    jx, jy = fx / (scale * dt * h[1]), fy / (scale * dt * h[0])
+    r = rho[1:, 1:] / dt + (jx[1:, 1:] - jx[1:, :-1]) / h[0] + (jy[1:, 1:] - jy[:-1, 1:]) / h[1]
+    return exact, float(np.abs(r).max() / np.abs(rho / dt).max())
+
+
 def accuracy(cfg, spec, bunch, steps=50):
     """FP32 mode against the FP64 path on identical inputs: the longitudinal
     wake on the bunch axis, the energy change per slice, and the continuity
-    residual of one FP32-mode push (its Jx, the FP64 deposit's Jy of the same
-    move and the charge difference, in FP64).  The energy change per slice
-    is taken where it is physical: a bunch entering the dipole (the small
-    bend workload, 300 steps); over the workload's own 50 steps in the
-    straight section it is ~1e-8 MeV and numerically noise."""
+    residual of one FP32-mode push.  The energy change per slice is taken
+    where it is physical: a bunch entering the dipole (the small bend
+    workload, 300 steps); over the workload's own 50 steps in the straight
+    section it is ~1e-8 MeV and numerically noise."""
     from csrst_b200 import ShapeFunction, Simulation
     res, sims = {}, {}
     for fp32 in (False, True):
-        s = Simulation(cfg, fp32=fp32)
+        s = Simulation(cfg, fp32=fp32, keep_old=fp32)
         s.load(*bunch)
         s.initial_fields(1e-12, 1e-6, 500)
         s.step(steps)
@@ -258,23 +287,7 @@ def accuracy(cfg, spec, bunch, steps=50):
     bcfg, bspec = workload("small-1-bend")
     de64, de32 = slice_energy_change(bcfg, bspec, make_bunch(bspec), 300)
     slice_err = float(np.abs(de32 - de64).max() / np.abs(de64).max())
-    # continuity residual of one FP32-mode push
-    s = sims[True]
-    info = s.info()
-    h, dt = (info["hx"], info["hy"]), info["dt"]
-    xo, yo, _, _ = s.particles()
-    s.push(0)
-    xn, yn, _, _ = s.particles()
-    w, org, _ = s.window()
-    L0, L1 = w[2], w[3]
-    jx = s.window_field(4)[1:L1 + 1, 1:L0 + 1]
-    q = np.full(len(xo), np.float32(spec.charge / spec.n), dtype=np.float64)
-    sf = ShapeFunction(cfg.shape_order)
-    jy = sf.getCurrentDensityBase(1, xo, yo, xn, yn, q, org, h, dt, 0, 0, L0, L1, info["fixed_scale"])
-    qs = 2.0 ** np.floor(np.log2(2.0 ** 62 / (4 * np.abs(q).sum())))
-    rho = sf.getChargeDensityDiff(xo, yo, xn, yn, q, org, h, 0, 0, L0, L1, qs)
-    r = rho[1:, 1:] / dt + (jx[1:, 1:] - jx[1:, :-1]) / h[0] + (jy[1:, 1:] - jy[:-1, 1:]) / h[1]
-    cont = float(np.abs(r).max() / np.abs(rho / dt).max())
+    exact, cont = continuity32(sims[True], ShapeFunction(cfg.shape_order))
     for v in sims.values():
         v.close()
     return {"steps": steps, "wake_rel_err": float("%.3g" % wake_err),
@@ -283,7 +296,9 @@ def accuracy(cfg, spec, bunch, steps=50):
                                         "rel_err": float("%.3g" % slice_err),
                                         "fp64_mev": [float("%.4g" % v) for v in de64]},
             "continuity_residual_rel": float("%.3g" % cont),
-            "bar": "wake <= 1e-3 of the FP64 path's maximum; continuity <= 1e-10 (FP64 check)"}
+            "continuity_integer_residual": exact,
+            "bar": "wake <= 1e-3 of the FP64 path's maximum; continuity <= 1e-10 (FP64 check against the FP64 "
+                   "charge shape); the integer residual against the charge the deposit assigns is exactly 0"}
 
 
 def run_ensemble(args, rank, members=64, ms=None, fields=True):
@@ -580,7 +595,8 @@ def run_b200(args, world, rank, local):
                                             f"{cfg.Nx}x{cfg.Ny} mesh incl. charge deposits and host round trips")}
 
     hs = summary(head)
-    dtype = "f32 (fields, gather, kick) + f64 (deposit)" if head == "fp32" else "f64"
+    dtype = ("f32 (fields, gather, kick, drifts, positions, current path integral) + f64 (bend frame, end-point "
+             "charge weights) + i64 (fixed-point current)") if head == "fp32" else "f64"
     out = {"metric": METRIC, "value": hs["value"], "unit": UNIT, "n_gpus": world,
            "steps": args.steps, "warmup": args.warmup, "ms_per_step": hs["ms_per_step"],
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": dtype,
@@ -593,9 +609,9 @@ def run_b200(args, world, rank, local):
     if other in runs:
         out[other] = summary(other)
         out[f"{head}_over_{other}"] = round(hs["value"] / out[other]["value"], 3)
-    # launches per step: 2 pushes x (prep, push, post, bounds; FP32 mode's push
-    # is two launches, move and deposit) + 4 sub-steps x (sweep, exchange) + move
-    out["gpu_launches"] = args.steps * (2 * (5 if head == "fp32" else 4) + 4 * 2 + 1)
+    # launches per step: 2 pushes x (prep, push, post, bounds) + 4 sub-steps x
+    # (sweep, exchange) + move
+    out["gpu_launches"] = args.steps * (2 * 4 + 4 * 2 + 1)
     if rank == 0 and not args.no_compare:
         out["accuracy_fp32_vs_fp64"] = accuracy(cfg, spec, bunch)
     if not args.no_ensemble:

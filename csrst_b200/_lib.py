@@ -14,6 +14,8 @@ SO = HERE / "libcsrst_gpu.so"
 D = C.POINTER(C.c_double)
 I = C.POINTER(C.c_int)
 U8 = C.POINTER(C.c_uint8)
+F32 = C.POINTER(C.c_float)
+I64 = C.POINTER(C.c_longlong)
 
 
 class Config(C.Structure):
@@ -108,6 +110,9 @@ def lib():
                            C.c_int, C.c_int, C.c_int, C.c_double, D], C.c_int),
         "csrst_charge_diff": ([C.c_int, D, D, D, D, D, C.c_size_t, D, D, C.c_int, C.c_int, C.c_int,
                                C.c_int, C.c_double, D], C.c_int),
+        "csrst_flux32": ([C.c_int, C.c_int, I, F32, F32, I, F32, F32, F32, C.c_size_t, C.c_double, C.c_int,
+                          C.c_int, C.c_int, C.c_int, I64, I64], C.c_int),
+        "csrst_get_bunch32": ([P, C.c_int, I, F32, F32, F32, F32, F32], C.c_int),
         "csrst_deposit_noalloc": ([C.c_int, C.c_int, P, P, P, P, P, C.c_size_t, D, D, C.c_double,
                                    C.c_int, C.c_int, C.c_int, C.c_int, C.c_double, P, P], C.c_int),
     }

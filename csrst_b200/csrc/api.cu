@@ -64,6 +64,16 @@ __global__ void k_check_bunch(const double *x, const double *y, const double *px
   if (bad != ~0ull) atomicMin(&out[0], bad);
   if (qm) atomicMax(&out[1], qm);
 }
+// FP32-mode positions (cell + offset) as FP64 positions.
+__global__ void k_old32_to64(const int *cell, const float *o0, const float *o1, long long n, double org0, double org1,
+                             double h0, double h1, double *x, double *y) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int c = cell[i];
+  const int ci = c & 0xffff, cj = (int)((unsigned)c >> 16);
+  x[i] = __dadd_rn(org0, __dmul_rn(__dadd_rn((double)ci, (double)o0[i]), h0));
+  y[i] = __dadd_rn(org1, __dmul_rn(__dadd_rn((double)cj, (double)o1[i]), h1));
+}
 __global__ void k_acc_to_plane(const unsigned long long *acc, Plane p, int L0, int L1, double inv) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= L0 * L1) return;
@@ -129,6 +139,9 @@ struct csrst_handle {
   std::string err;
   // FP32 mode (CSRST_FLAG_FP32): FP32 static and window planes, FP32 bunch
   bool fp32 = false;
+  Ref32 R32{};                // reference momentum and drift constants in FP32
+  int *old_cell = nullptr;    // CSRST_FLAG_KEEP_OLD in FP32 mode: start of each particle's last move
+  float *old_o0 = nullptr, *old_o1 = nullptr;
   int pitch32 = 0;
   float *Exf = nullptr, *Eyf = nullptr, *Hxf = nullptr, *Hyf = nullptr;
   float *winf = nullptr, *scratchf = nullptr;
@@ -220,8 +233,11 @@ FieldArgs field_args(csrst_handle *h, int comp) {
   a.cells = h->cells; a.ncells = h->ncells;
   a.ws = h->ws;
   a.acc = h->acc ? h->acc + (size_t)(comp == 1 ? 1 : 0) * h->L0 * h->L1 : nullptr;
-  a.acc_inv = h->acc_scale > 0 ? 1.0 / h->acc_scale : 0.0;
   const double h0 = h->b.hr0, h1 = h->b.hr1, dt = h->dt;
+  // FP64 path: the accumulator holds J * scale; FP32 mode: the flux
+  // F = J dt h_other / q in units of 1 / scale per unit charge (flux32.cuh)
+  a.acc_inv = h->acc_scale > 0 ? (h->fp32 ? 1.0 / (h->acc_scale * dt * (comp == 1 ? h0 : h1)) : 1.0 / h->acc_scale)
+                               : 0.0;
   // TETMSolver.hh:121-125 and TETMSolver.cpp:87-127
   const double etax = kC * dt / h0, etay = kC * dt / h1;
   const double Z0 = std::sqrt(kMu0 / kEps0);
@@ -306,6 +322,8 @@ void free_particles(csrst_handle *h) {
   h->win = h->scratch = nullptr; h->acc = nullptr;
   cudaFree(h->b32.cell); cudaFree(h->b32.ox); cudaFree(h->b32.oy); cudaFree(h->b32.dpx); cudaFree(h->b32.dpy);
   cudaFree(h->b32.q); cudaFree(h->winf); cudaFree(h->scratchf); cudaFree(h->d64);
+  cudaFree(h->old_cell); cudaFree(h->old_o0); cudaFree(h->old_o1);
+  h->old_cell = nullptr; h->old_o0 = h->old_o1 = nullptr;
   h->b32 = Bunch32{};
   h->winf = h->scratchf = nullptr;
   h->d64 = nullptr;
@@ -357,18 +375,13 @@ Push32Args push_args32(csrst_handle *h, int jcomp) {
   a.acc_scale = h->acc_scale;
   a.jcomp = jcomp;
   a.pending = h->pending ? 1 : 0;
-  a.P0 = h->P0; a.P1 = h->P1;
-  a.kh0 = h->kh0; a.kh1 = h->kh1;
+  a.R = h->R32;
   const double fact1 = h->half * h->cfg.charge_mass;
   a.f1 = (float)fact1; a.f2 = (float)(fact1 * kC);
-  a.h0 = h->b.hr0; a.h1 = h->b.hr1; a.dt = h->dt;
-  a.org0 = h->b.org0; a.org1 = h->b.org1;
+  a.org0 = h->b.org0; a.org1 = h->b.org1; a.h0 = h->b.hr0; a.h1 = h->b.hr1;
   a.bz = h->cfg.bz; a.Lb = h->b.Lb; a.hw = 0.5 * h->b.w;
   a.chh = h->chh; a.shh = h->shh; a.bwidth = h->bwidth;
-  // the FP64 bunch copy (diagnostics scratch, 4 n doubles) carries the
-  // move -> deposit hand-over inside a push
-  a.dep_r0 = h->d64;
-  a.dep_cell = reinterpret_cast<int *>(h->d64 + 2 * (size_t)h->n);
+  a.old_cell = h->old_cell; a.old_o0 = h->old_o0; a.old_o1 = h->old_o1;
   return a;
 }
 
@@ -376,7 +389,7 @@ Push32Args push_args32(csrst_handle *h, int jcomp) {
 int push_async(csrst_handle *h, int jcomp) {
   const bool bb_ok = h->bb == kBBValid || (h->bb == kBBValidIfPending && h->pending);
   if (h->fp32) {
-    if (!bb_ok) launch_bbox32(h->b32, h->P0, h->P1, h->kh0, h->kh1, h->pending ? 1 : 0, h->ws, h->s);
+    if (!bb_ok) launch_bbox32(h->b32, h->R32, h->pending ? 1 : 0, h->ws, h->s);
     launch_prep32(h->ws, h->order, h->s);
     launch_push32(push_args32(h, jcomp), h->order, h->s);
     launch_bounds32(h->ws, h->s);
@@ -403,7 +416,7 @@ int push_async(csrst_handle *h, int jcomp) {
 
 void drift_now(csrst_handle *h, double dt) {
   if (h->fp32)
-    launch_drift32(h->b32, h->P0, h->P1, dt * kC / h->b.hr0, dt * kC / h->b.hr1, h->s);
+    launch_drift32(h->b32, h->R32, (float)(dt * kC / h->b.hr0), (float)(dt * kC / h->b.hr1), h->s);
   else
     launch_drift(h->x, h->y, h->px, h->py, h->n, dt * kC, h->s);
 }
@@ -486,7 +499,7 @@ void bunch64(csrst_handle *h, const double **x, const double **y, const double *
     return;
   }
   const size_t n = (size_t)h->n;
-  launch_to64(h->b32, h->P0, h->P1, h->kh0, h->kh1, h->pending ? 1 : 0, h->b.org0, h->b.org1, h->b.hr0,
+  launch_to64(h->b32, h->R32, h->P0, h->P1, h->pending ? 1 : 0, h->b.org0, h->b.org1, h->b.hr0,
               h->b.hr1, h->d64, h->d64 + n, h->d64 + 2 * n, h->d64 + 3 * n, h->s);
   *x = h->d64; *y = h->d64 + n; *px = h->d64 + 2 * n; *py = h->d64 + 3 * n; *pending = 0;
 }
@@ -495,7 +508,7 @@ void bunch64(csrst_handle *h, const double **x, const double **y, const double *
 // host synchronisation; FP32 mode reads its bunch in place.
 void moments_async(csrst_handle *h) {
   if (h->fp32) {
-    launch_moments32(Bunch32View{h->b32, h->P0, h->P1, h->kh0, h->kh1, h->pending ? 1 : 0, h->b.org0, h->b.org1,
+    launch_moments32(Bunch32View{h->b32, h->R32, h->P0, h->P1, h->pending ? 1 : 0, h->b.org0, h->b.org1,
                                  h->b.hr0, h->b.hr1},
                      h->dscratch, h->dmean, h->dout, h->s);
     return;
@@ -517,6 +530,26 @@ void step_async(csrst_handle *h) {
   move_async(h);
 }
 
+// FP32 mode's reference momentum and drift constants, rounded once.
+void set_ref32(csrst_handle *h) {
+  h->R32.P0 = (float)h->P0;
+  h->R32.P1 = (float)h->P1;
+  h->R32.G2 = (float)(1.0 + (h->P0 * h->P0 + h->P1 * h->P1));
+  h->R32.kh0 = (float)h->kh0;
+  h->R32.kh1 = (float)h->kh1;
+}
+
+// Start positions of the last move (CSRST_FLAG_KEEP_OLD in FP32 mode).
+cudaError_t alloc_old32(csrst_handle *h) {
+  if (!(h->cfg.flags & CSRST_FLAG_KEEP_OLD) || !h->fp32) return cudaSuccess;
+  const size_t n = (size_t)h->n;
+  cudaError_t e = cudaMalloc(&h->old_cell, n * sizeof(int));
+  if (e == cudaSuccess) e = cudaMalloc(&h->old_o0, n * sizeof(float));
+  if (e == cudaSuccess) e = cudaMalloc(&h->old_o1, n * sizeof(float));
+  if (e == cudaSuccess) e = cudaMemsetAsync(h->old_cell, 0, n * sizeof(int), h->s);
+  return e;
+}
+
 int need_bunch(csrst_handle *h) {
   if (!h) return CSRST_E_ARG;
   if (h->n <= 0 || !(h->win || h->winf)) return fail(h, CSRST_E_NO_PARTICLES, "no bunch loaded");
@@ -533,8 +566,6 @@ int csrst_create(const csrst_config *cfg, csrst_handle **out) {
   if (cfg->Nx < 8 || cfg->Ny < 8 || cfg->shape_order < 0 || cfg->shape_order > 2 || !(cfg->width > 0))
     return fail(nullptr, CSRST_E_ARG, "invalid configuration");
   if (cfg->flags & ~(CSRST_FLAG_KEEP_OLD | CSRST_FLAG_FP32)) return fail(nullptr, CSRST_E_ARG, "unknown flags");
-  if ((cfg->flags & CSRST_FLAG_FP32) && (cfg->flags & CSRST_FLAG_KEEP_OLD))
-    return fail(nullptr, CSRST_E_ARG, "CSRST_FLAG_KEEP_OLD is an FP64-path option");
   if ((cfg->flags & CSRST_FLAG_FP32) && (cfg->Nx > 32767 || cfg->Ny > 32767))
     return fail(nullptr, CSRST_E_ARG, "FP32 mode packs cell indices in 16 bits: Nx, Ny <= 32767");
   int ndev = 0;
@@ -840,6 +871,11 @@ int csrst_load_particles(csrst_handle *h, const double *x, const double *y, cons
     cudaFree(part);
     h->P0 = sums[0] / (double)N;
     h->P1 = sums[1] / (double)N;
+    set_ref32(h);
+    // FP32 mode accumulates the flux q-units of flux32.cuh: every particle
+    // carries K = q scale, and a cell's flux stays below 4 N max|q| scale
+    const double fbound = 4.0 * (double)n * (qmax > 0 ? qmax : 1e-30) * (1.0 + 1e-6);
+    h->acc_scale = std::ldexp(1.0, (int)std::floor(std::log2(std::ldexp(1.0, 62) / fbound)));
     Bunch32 &b = h->b32;
     b.n = N;
     CK(cudaMalloc(&b.cell, n * sizeof(int)));
@@ -849,7 +885,8 @@ int csrst_load_particles(csrst_handle *h, const double *x, const double *y, cons
                   h->s);
     CK(cudaStreamSynchronize(h->s));
     for (double **p : {&h->x, &h->y, &h->px, &h->py, &h->q, &h->ox, &h->oy}) { cudaFree(*p); *p = nullptr; }
-    launch_bbox32(b, h->P0, h->P1, h->kh0, h->kh1, 0, h->ws, h->s);
+    CK(alloc_old32(h));
+    launch_bbox32(b, h->R32, 0, h->ws, h->s);
   } else {
     launch_bbox_next(h->x, h->y, h->px, h->py, N, h->half, 0, h->ws, h->s);
   }
@@ -945,6 +982,15 @@ int csrst_get_old_positions(csrst_handle *h, double *ox, double *oy) {
   if (!(h->cfg.flags & CSRST_FLAG_KEEP_OLD))
     return fail(h, CSRST_E_ARG, "create the handle with CSRST_FLAG_KEEP_OLD to keep oldR");
   const size_t nb = (size_t)h->n * sizeof(double);
+  if (h->fp32) {  // the start of each particle's last move, as FP64 positions
+    k_old32_to64<<<(unsigned)((h->n + 255) / 256), 256, 0, h->s>>>(h->old_cell, h->old_o0, h->old_o1, h->n, h->b.org0,
+                                                                     h->b.org1, h->b.hr0, h->b.hr1, h->d64,
+                                                                     h->d64 + h->n);
+    if (ox) CK(cudaMemcpyAsync(ox, h->d64, nb, cudaMemcpyDeviceToHost, h->s));
+    if (oy) CK(cudaMemcpyAsync(oy, h->d64 + h->n, nb, cudaMemcpyDeviceToHost, h->s));
+    CK(cudaStreamSynchronize(h->s));
+    return CSRST_OK;
+  }
   if (ox) CK(cudaMemcpyAsync(ox, h->ox, nb, cudaMemcpyDeviceToHost, h->s));
   if (oy) CK(cudaMemcpyAsync(oy, h->oy, nb, cudaMemcpyDeviceToHost, h->s));
   CK(cudaStreamSynchronize(h->s));
@@ -976,7 +1022,7 @@ int csrst_get_window_field(csrst_handle *h, int which, double *out) {
       const int c = which - 4;
       k_acc_to_plane<<<(h->L0 * h->L1 + 255) / 256, 256, 0, h->s>>>(h->acc + (size_t)c * h->L0 * h->L1,
                                                                   Plane{tmp, h->wpitch}, h->L0, h->L1,
-                                                                  1.0 / h->acc_scale);
+                                                                  field_args(h, c).acc_inv);
     } else {
       launch_f2d(h->winf + (size_t)which * wp, (int)wp, tmp, (int)wp, 1, (int)wp, h->s);
     }
@@ -1294,7 +1340,7 @@ cudaError_t part_build(csrst_ensemble *e, EnsPart &P) {
     for (int c = 0; c < 2; ++c) {
       void *args = e->fp32 ? (void *)dev_copy(G.p32[c], err) : (void *)dev_copy(G.p64[c], err);
       P.blocks.push_back(args);
-      P.groups[c].push_back(PushGroup{o, gm, args, ok, pp, G.ppre.back(), 0, G.smem});
+      P.groups[c].push_back(PushGroup{o, gm, c, args, ok, pp, G.ppre.back(), 0, G.smem});
     }
   }
   for (int c = 0; c < 2; ++c) {
@@ -1684,6 +1730,62 @@ int csrst_charge_diff(int order, const double *ox, const double *oy, const doubl
   return run_fixed(1, order, 0, ox, oy, x, y, q, n, o2, hh2, 0.0, i0, j0, ni, nj, scale, rho);
 }
 
+int csrst_flux32(int order, int comp, const int *cell0, const float *a0, const float *a1, const int *cell1,
+                 const float *b0, const float *b1, const float *q, size_t n, double scale, int i0, int j0, int ni,
+                 int nj, long long *F, long long *drho) {
+  csrst_handle *h = nullptr;
+  if (order < 0 || order > 2 || (comp != 0 && comp != 1) || ni <= 0 || nj <= 0 || !F || !(scale > 0) ||
+      (n > 0 && (!cell0 || !a0 || !a1 || !cell1 || !b0 || !b1 || !q)))
+    return fail(h, CSRST_E_ARG, "invalid flux arguments");
+  const size_t m = (size_t)ni * nj;
+  unsigned long long *dF = nullptr, *dR = nullptr;
+  int *derr = nullptr;
+  CK(cudaMalloc(&dF, m * 8)); CK(cudaMemset(dF, 0, m * 8));
+  if (drho) { CK(cudaMalloc(&dR, m * 8)); CK(cudaMemset(dR, 0, m * 8)); }
+  CK(cudaMalloc(&derr, 8)); CK(cudaMemset(derr, 0, 8));
+  void *d[7] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+  const void *src[7] = {cell0, a0, a1, cell1, b0, b1, q};
+  if (n > 0)
+    for (int k = 0; k < 7; ++k) {
+      CK(cudaMalloc(&d[k], n * 4));
+      CK(cudaMemcpy(d[k], src[k], n * 4, cudaMemcpyHostToDevice));
+    }
+  launch_flux32(order, comp, (const int *)d[0], (const float *)d[1], (const float *)d[2], (const int *)d[3],
+                (const float *)d[4], (const float *)d[5], (const float *)d[6], (long long)n, scale, i0, j0, ni, nj, dF,
+                dR, derr, 0);
+  int e[2] = {0, 0};
+  CK(cudaMemcpy(F, dF, m * 8, cudaMemcpyDeviceToHost));
+  if (drho) CK(cudaMemcpy(drho, dR, m * 8, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(e, derr, 8, cudaMemcpyDeviceToHost));
+  cudaFree(dF); cudaFree(dR); cudaFree(derr);
+  for (void *p : d) cudaFree(p);
+  CK(cudaGetLastError());
+  if (e[0]) return fail(h, e[0], "a move spans more than one cell on an axis");
+  if (e[1]) {
+    fail(h, CSRST_W_OUTSIDE, "contributions outside the patch were dropped");
+    return CSRST_W_OUTSIDE;
+  }
+  return CSRST_OK;
+}
+
+int csrst_get_bunch32(csrst_handle *h, int which, int *cell, float *o0, float *o1, float *d0, float *d1, float *q) {
+  int rc = need_bunch(h);
+  if (rc) return rc;
+  if (!h->fp32) return fail(h, CSRST_E_ARG, "csrst_get_bunch32 reads an FP32-mode bunch");
+  if (which != 0 && which != 1) return fail(h, CSRST_E_ARG, "which must be 0 (bunch) or 1 (start of the last move)");
+  if (which == 1 && !h->old_cell)
+    return fail(h, CSRST_E_ARG, "create the handle with CSRST_FLAG_KEEP_OLD to keep the start of each move");
+  if (which == 1 && (d0 || d1 || q)) return fail(h, CSRST_E_ARG, "the start of a move has no momentum or charge");
+  const size_t n4 = (size_t)h->n * 4;
+  const void *src[6] = {which ? (const void *)h->old_cell : h->b32.cell, which ? (const void *)h->old_o0 : h->b32.ox,
+                        which ? (const void *)h->old_o1 : h->b32.oy, h->b32.dpx, h->b32.dpy, h->b32.q};
+  void *dst[6] = {cell, o0, o1, d0, d1, q};
+  for (int k = 0; k < 6; ++k)
+    if (dst[k]) CK(cudaMemcpyAsync(dst[k], src[k], n4, cudaMemcpyDeviceToHost, h->s));
+  CK(cudaStreamSynchronize(h->s));
+  return CSRST_OK;
+}
+
 }  // extern "C"
 
 // ---- checkpoint / restart ----
@@ -1692,7 +1794,7 @@ namespace {
 
 constexpr char kCkMagic[8] = {'C', 'S', 'R', 'S', 'T', 'C', 'K', '1'};
 constexpr char kCkEnd[8] = {'C', 'S', 'R', 'S', 'T', 'E', 'N', 'D'};
-constexpr uint32_t kCkVersion = 1;
+constexpr uint32_t kCkVersion = 2;  // 2: FP32 mode's current accumulator holds flux units
 
 bool ck_put(FILE *f, const void *p, size_t n) { return n == 0 || std::fwrite(p, 1, n, f) == n; }
 bool ck_get(FILE *f, void *p, size_t n) { return n == 0 || std::fread(p, 1, n, f) == n; }
@@ -1848,6 +1950,10 @@ int csrst_checkpoint_read(csrst_handle *h, const char *path, long long *step, do
   h->bb = (BBoxState)bb;
   h->P0 = mom[0];
   h->P1 = mom[1];
+  if (h->fp32) {
+    set_ref32(h);
+    CK(alloc_old32(h));
+  }
   if (step) *step = st;
   if (time) *time = tm;
   return CSRST_OK;

@@ -89,16 +89,17 @@ __host__ __device__ inline double ord_dbl(long long b) {
 }
 
 // The reference's float fast inverse square root used for 1/gamma
-// (src/utils.hh:491-504).  The kernels are built with --fmad=false so every
-// float multiply and subtract here rounds separately, as on the host.
+// (src/utils.hh:491-504).  Every float multiply and subtract rounds
+// separately (explicit round-to-nearest operations), as on the host, in
+// every translation unit whatever its contraction setting.
 __device__ __forceinline__ float q_rsqrt(float x) {
-  float xhalf = 0.5f * x;
-  float xqhalf = 0.5010936f * x;
+  const float xhalf = __fmul_rn(0.5f, x);
+  const float xqhalf = __fmul_rn(0.5010936f, x);
   unsigned int i = __float_as_uint(x);
   i = 0x5f3759dfu - (i >> 1);
   x = __uint_as_float(i);
-  x = x * (1.5f - xhalf * x * x);
-  x = x * (1.5010936f - xqhalf * x * x);
+  x = __fmul_rn(x, __fsub_rn(1.5f, __fmul_rn(__fmul_rn(xhalf, x), x)));
+  x = __fmul_rn(x, __fsub_rn(1.5010936f, __fmul_rn(__fmul_rn(xqhalf, x), x)));
   return x;
 }
 

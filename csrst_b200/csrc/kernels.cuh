@@ -78,7 +78,7 @@ struct PrepArgs {
 // The members of one shape order in a batched push (device arrays of m
 // entries; ppre: first particle of each member, m + 1 entries).
 struct PushGroup {
-  int order, m;
+  int order, m, jcomp;
   const void *args;                 // PushArgs or Push32Args
   const unsigned char *smem_ok;     // the member's window accumulator fits in shared memory
   const long long *ppre;
@@ -197,24 +197,28 @@ struct Bunch32 {
   long long n;
 };
 
+// FP32-mode reference momentum and drift constants, rounded once from FP64:
+// P, 1 + |P|^2 and 0.5 c dt / h (cells per half step per unit beta).
+struct Ref32 {
+  float P0, P1, G2, kh0, kh1;
+};
+
 struct Push32Args {
   Bunch32 b;
   WinState *ws;
   const float *mEx, *mEy, *mHx, *mHy;  // window planes, pitch wpitch
   int wpitch;
-  unsigned long long *acc;             // L0 * L1 fixed-point current for jcomp
-  double acc_scale;
+  unsigned long long *acc;             // L0 * L1 fixed-point flux (flux32.cuh) for jcomp
+  double acc_scale;                    // fixed-point units per unit of charge
   int jcomp, pending;
-  double P0, P1;                       // reference momentum
-  double kh0, kh1;                     // 0.5 c dt / h: cells per half step per unit beta
+  Ref32 R;
   float f1, f2;                        // 0.5 c dt q/m and f1 c
-  double h0, h1, dt;                   // spacing and time step (current scale)
-  double org0, org1;                   // static mesh origin (dipole position)
+  double org0, org1, h0, h1;           // static mesh origin and spacing (bend frame)
   double bz, Lb, hw, chh, shh, bwidth; // hard-edge dipole
-  // the move launch's hand-over to the deposit launch, n entries each
-  // (deposit start R0 in cells from the old cell, NaN if not moved; old cell)
-  double *dep_r0;                      // 2 n
-  int *dep_cell;                       // n
+  // start position of every particle's move (CSRST_FLAG_KEEP_OLD), or null:
+  // old cell, offsets from it
+  int *old_cell;
+  float *old_o0, *old_o1;
 };
 
 int launch_push32(const Push32Args &a, int order, cudaStream_t s);
@@ -223,16 +227,22 @@ void launch_push32_batch(const PushGroup *groups, int ngroups, int m, int grid, 
                          cudaStream_t s, int parts = 3);
 void launch_prep32(WinState *ws, int order, cudaStream_t s);
 void launch_bounds32(WinState *ws, cudaStream_t s);
-void launch_bbox32(const Bunch32 &b, double P0, double P1, double kh0, double kh1, int pending, WinState *ws,
-                   cudaStream_t s);
-void launch_drift32(const Bunch32 &b, double P0, double P1, double kd0, double kd1, cudaStream_t s);
+void launch_bbox32(const Bunch32 &b, const Ref32 &R, int pending, WinState *ws, cudaStream_t s);
+// R += dt c v / h: kd = the drift's dt c / h per axis (Ref32.kh replaced)
+void launch_drift32(const Bunch32 &b, const Ref32 &R, float kd0, float kd1, cudaStream_t s);
 void launch_from64(const double *x, const double *y, const double *px, const double *py, const double *q,
                    long long n, double org0, double org1, double h0, double h1, double P0, double P1,
                    const Bunch32 &b, cudaStream_t s);
 // pending > 0: the stored positions still owe the drift by -kh (cells)
-void launch_to64(const Bunch32 &b, double P0, double P1, double kh0, double kh1, int pending, double org0,
-                 double org1, double h0, double h1, double *x, double *y, double *px, double *py,
-                 cudaStream_t s);
+void launch_to64(const Bunch32 &b, const Ref32 &R, double P0, double P1, int pending, double org0, double org1,
+                 double h0, double h1, double *x, double *y, double *px, double *py, cudaStream_t s);
+// Stand-alone FP32-mode deposit (csrst_flux32): n moves from (cell0, a) to
+// (cell1, b), integer flux of component comp and (if drho) the integer charge
+// change into dense ni x nj patches at static-mesh index (i0, j0); err[0]:
+// crossing overflow, err[1]: a non-zero contribution fell outside the patch.
+void launch_flux32(int order, int comp, const int *cell0, const float *a0, const float *a1, const int *cell1,
+                   const float *b0, const float *b1, const float *q, long long n, double scale, int i0, int j0,
+                   int ni, int nj, unsigned long long *F, unsigned long long *drho, int *err, cudaStream_t s);
 void launch_psum(const double *px, const double *py, long long n, double *part, double *out2,
                  cudaStream_t s);
 // Plane copies between FP64 and FP32 (rows x cols elements, pitches in elements).

@@ -1,25 +1,29 @@
-// FP32 mode particle kernels: the same fused push as particles.cu
+// FP32 mode particle kernels: the fused push of particles.cu
 // (PartBunch::push_particles, PartBunch.cpp:215-519) on a bunch stored as
 // FP32 offsets from FP64 cell origins and FP32 momentum deviations from an
-// FP64 reference momentum.
+// FP64 reference momentum, in FP32 arithmetic.
 //
-// Precision split (what stays FP64 and why):
-//   - 1/gamma: the reference's float Q_rsqrt of 1 + |P|^2 formed in FP64, so
-//     velocities match the FP64 path's (utils.hh:491-504);
-//   - positions during the push: cell-relative doubles built exactly from
-//     the stored offsets, so no precision is lost to the distance from the
-//     mesh origin; the stored offset is rounded to FP32 once per push;
-//   - the current deposit: FP64 weights on those exact positions, so the
-//     discrete continuity equation holds to FP64 rounding;
-//   - the hard-edge dipole test: absolute position in FP64 (the bend frame).
-// The field gather (27 taps for TSC) and the kick/rotation run in FP32; the
-// gather is anchored at the particle's own window cell, so its coordinates
-// are offsets of magnitude < 2 and keep FP32's full resolution.
-// This file is built with FMA contraction on: FP32 mode is checked against
-// the FP64 path to a tolerance, not bit for bit.
+// Precision split:
+//   - FP32: 1/gamma (the reference's float Q_rsqrt of 1 + |P|^2 formed from
+//     the FP32 deviation, bunch32.cuh), the drifts, the positions during the
+//     push (offsets from the particle's old cell), the field gather (anchored
+//     at the particle's own window cell, so its coordinates keep FP32's full
+//     resolution), the kick and rotation, and the current's path integral
+//     (flux32.cuh);
+//   - FP64: the hard-edge dipole test on the absolute position (the bend
+//     frame), and the 1D charge weights of each move's end points from which
+//     the fixed-point charge and, by exact integer continuity, the x current
+//     are formed (flux32.cuh); the deposited current then satisfies the
+//     discrete continuity equation exactly for the charge each particle
+//     carries.
+// This file is built with FMA contraction on; the bunch arithmetic shared
+// with other kernels (bunch32.cuh) rounds every operation explicitly.
+#include <climits>
+
 #include "accum.cuh"
 #include "bbox.cuh"
 #include "bunch32.cuh"
+#include "flux32.cuh"
 #include "kernels.cuh"
 #include "shapes.cuh"
 
@@ -39,172 +43,111 @@ struct SumView32 {
 };
 
 // Cell of the cell-relative coordinate t of cell c, as c' + 0.5 (exact).
-__device__ __forceinline__ double cellc(int c, double t) { return (double)(c + (int)floor(t)) + 0.5; }
+__device__ __forceinline__ double cellc(int c, float t) { return (double)(c + (int)floorf(t)) + 0.5; }
 
-// Store a cell-relative position t (cells) of cell (ci, cj) as cell + offset.
-__device__ __forceinline__ void store_pos(double t0, double t1, int ci, int cj, int &cell, float &o0, float &o1) {
-  double f0 = floor(t0), f1 = floor(t1);
-  float a0 = (float)(t0 - f0), a1 = (float)(t1 - f1);
-  if (a0 >= 1.0f) { a0 = 0.0f; f0 += 1.0; }  // rounded up to the next cell
-  if (a1 >= 1.0f) { a1 = 0.0f; f1 += 1.0; }
+// Store a position t (cells from cell (ci, cj)) as cell + offset in [0, 1).
+__device__ __forceinline__ void store32(float t0, float t1, int ci, int cj, int &cell, float &o0, float &o1) {
+  float f0 = floorf(t0), f1 = floorf(t1);
+  float a0 = fsub(t0, f0), a1 = fsub(t1, f1);
+  if (a0 >= 1.0f) { a0 = 0.0f; f0 += 1.0f; }  // a negative t rounded up to the next cell
+  if (a1 >= 1.0f) { a1 = 0.0f; f1 += 1.0f; }
   cell = ((ci + (int)f0) & 0xffff) | ((cj + (int)f1) << 16);
   o0 = a0; o1 = a1;
 }
 
-// One particle's move: gather at R1, kick + rotation, drift to R2, R2 stored
-// (cell + FP32 offset) and the new momentum deviation stored.  On return,
-// when ok: r0 = R0 (deposit start) and e = R2 (end, as stored) in cells from
-// the old cell (ci, cj); (ni, nj) the new cell and w the half drift of the
-// new momentum.  Particles that fail the window-fit checks set the member's
-// error and come back with ok false, unchanged.
+// One particle's move: start A = stored position (minus the pending half
+// drift), gather at R1, kick + rotation, drift to R2, R2 and the new momentum
+// deviation stored.  On return, when ok: A in cells from the old cell
+// (ci, cj), the stored end point as new cell (ni, nj) + offset (o0, o1).
+// Particles that fail the window-fit checks set the member's error and come
+// back with ok false, unchanged.
 struct Move32 {
   bool ok;
   int ci, cj, ni, nj;
-  double r00, r01, e0, e1, w0, w1, q;
-  float o0, o1;
+  float a0, a1, o0, o1, q;
 };
 
 template <int ORDER_OF_PUSH>
-__device__ __forceinline__ void move32(const Push32Args &a, long long n, bool ok, int L0, int L1, int WP0, int WP1,
+__device__ __forceinline__ void move32(const Push32Args &a, long long n, int L0, int L1, int WP0, int WP1,
                                        Move32 &m) {
   WinState *ws = a.ws;
   const int wp = a.wpitch;
-  const double P0 = a.P0, P1 = a.P1;
-  const float Pf0 = (float)P0, Pf1 = (float)P1;
-  int ci = 0, cj = 0;
-  double s0 = 0.0, s1 = 0.0, q = 0.0;
-  float d0 = 0.0f, d1 = 0.0f;
-  if (ok) {
-    unpack(a.b.cell[n], ci, cj);
-    s0 = a.b.ox[n]; s1 = a.b.oy[n];
-    d0 = a.b.dpx[n]; d1 = a.b.dpy[n];
-    q = a.b.q[n];
-    if (!(isfinite(d0) && isfinite(d1) && s0 >= 0.0 && s0 < 1.0 && s1 >= 0.0 && s1 < 1.0)) {
-      set_err(ws, kErrWindowFit);
-      ok = false;
-    }
+  const Ref32 &R = a.R;
+  int ci, cj;
+  unpack(a.b.cell[n], ci, cj);
+  const float s0 = a.b.ox[n], s1 = a.b.oy[n];
+  float d0 = a.b.dpx[n], d1 = a.b.dpy[n];
+  m.q = a.b.q[n];
+  m.ci = ci; m.cj = cj; m.ni = ci; m.nj = cj;
+  m.a0 = s0; m.a1 = s1; m.o0 = s0; m.o1 = s1;
+  m.ok = isfinite(d0) && isfinite(d1) && s0 >= 0.0f && s0 < 1.0f && s1 >= 0.0f && s1 < 1.0f;
+  if (!m.ok) { set_err(ws, kErrWindowFit); return; }
+  // R0 and R1: with the trailing -dt/2 drift pending, the particle sits at
+  // s - w and the push's first half drift brings it back to s
+  float x0 = s0, x1 = s1;
+  {
+    const float r = rgam32(R, d0, d1);
+    const float w0 = drift32(R.kh0, R.P0, d0, r), w1 = drift32(R.kh1, R.P1, d1, r);
+    if (a.pending) { m.a0 = fsub(s0, w0); m.a1 = fsub(s1, w1); }
+    else { x0 = fadd(s0, w0); x1 = fadd(s1, w1); }
   }
-  double p0 = 0.0, p1 = 0.0, w0 = 0.0, w1 = 0.0, r00 = 0.0, r01 = 0.0, x0 = 0.0, x1 = 0.0;
-  if (ok) {
-    const float r = rgam(P0, P1, d0, d1, p0, p1);
-    w0 = half_drift(a.kh0, p0, r); w1 = half_drift(a.kh1, p1, r);
-    r00 = s0; r01 = s1;
-    if (a.pending) { r00 = dsub(s0, w0); r01 = dsub(s1, w1); }  // drift_particles(-dt/2)
-    x0 = dadd(r00, w0); x1 = dadd(r01, w1);                     // R1, cells from (ci, cj)
-    const int wi = ci - WP0, wj = cj - WP1;
-    // gather (FieldPatch::gather x3) anchored at the window cell of R1; the
-    // offset inside it is clamped below 1 so that FP32 rounding cannot move
-    // the stencil to the next cell (the window-fit check counts cells in FP64)
-    const double c0 = floor(x0), c1 = floor(x1);
-    const int ai = wi + (int)c0, aj = wj + (int)c1;
-    if (ai - 2 < -1 || ai + 2 > L0 || aj - 2 < -1 || aj + 2 > L1) {  // stencil outside the window planes
-      set_err(ws, kErrWindowFit);
-      ok = false;
-    } else {
-      const float g0 = fminf((float)(x0 - c0), 0x1.fffffep-1f), g1 = fminf((float)(x1 - c1), 0x1.fffffep-1f);
-      const size_t o = (size_t)(aj + 1) * wp + (ai + 1);
-      const View32 vex{a.mEx + o, wp}, vey{a.mEy + o, wp}, vhx{a.mHx + o, wp}, vhy{a.mHy + o, wp};
-      const float E0 = gather_edge<ORDER_OF_PUSH>(vex, g0, g1, 0);
-      const float E1 = gather_edge<ORDER_OF_PUSH>(vey, g0, g1, 1);
-      const float Hf = gather_cell<ORDER_OF_PUSH>(SumView32{vhx, vhy}, g0, g1);
-      // hard-edge dipole at the absolute position of R1
-      const double X = a.org0 + ((double)ci + x0) * a.h0, Y = a.org1 + ((double)cj + x1) * a.h1;
-      const double dist = a.chh * (X - a.Lb) - a.shh * (Y - a.hw);
-      const float bext = (dist > 0.0 && dist < a.bwidth) ? (float)a.bz : 0.0f;
-      const float B = (float)kMu0 * Hf + 0.5f * bext;
-      // kick + rotation (PartBunch.cpp:366-383) on u - P
-      const float k0 = a.f1 * E0, k1 = a.f1 * E1;
-      const float du0 = d0 + k0, du1 = d1 + k1;
-      double U0, U1;
-      const float ru = rgam(P0, P1, du0, du1, U0, U1);
-      const float aa = a.f2 * B * ru;
-      const float sv0 = du0 + aa * (Pf1 + du1), sv1 = du1 - aa * (Pf0 + du0);  // s - P
-      const float cf = aa / (1.0f + aa * aa);
-      d0 = (sv0 + cf * (Pf1 + sv1)) + k0;
-      d1 = (sv1 - cf * (Pf0 + sv0)) + k1;
-      a.b.dpx[n] = d0; a.b.dpy[n] = d1;
-    }
+  const int wi = ci - WP0, wj = cj - WP1;
+  // gather (FieldPatch::gather x3) anchored at the window cell of R1
+  const float c0 = floorf(x0), c1 = floorf(x1);
+  const int ai = wi + (int)c0, aj = wj + (int)c1;
+  if (ai - 2 < -1 || ai + 2 > L0 || aj - 2 < -1 || aj + 2 > L1) {  // stencil outside the window planes
+    set_err(ws, kErrWindowFit);
+    m.ok = false;
+    return;
   }
-  m.ok = ok;
-  m.ci = ci; m.cj = cj; m.r00 = r00; m.r01 = r01; m.q = q;
-  m.ni = 0; m.nj = 0; m.e0 = 0.0; m.e1 = 0.0; m.o0 = 0.0f; m.o1 = 0.0f; m.w0 = 0.0; m.w1 = 0.0;
-  if (ok) {
-    const float r = rgam(P0, P1, d0, d1, p0, p1);
-    w0 = half_drift(a.kh0, p0, r); w1 = half_drift(a.kh1, p1, r);
-    int nc;
-    float o0, o1;
-    store_pos(dadd(x0, w0), dadd(x1, w1), ci, cj, nc, o0, o1);  // R2
-    a.b.cell[n] = nc; a.b.ox[n] = o0; a.b.oy[n] = o1;
-    // the move ends at the stored (FP32-rounded) position, so that every
-    // move's current conserves charge for the positions the bunch holds
-    unpack(nc, m.ni, m.nj);
-    m.e0 = (double)(m.ni - ci) + (double)o0; m.e1 = (double)(m.nj - cj) + (double)o1;
-    m.o0 = o0; m.o1 = o1; m.w0 = w0; m.w1 = w1;
-  }
+  const float g0 = x0 - c0, g1 = x1 - c1;
+  const size_t o = (size_t)(aj + 1) * wp + (ai + 1);
+  const View32 vex{a.mEx + o, wp}, vey{a.mEy + o, wp}, vhx{a.mHx + o, wp}, vhy{a.mHy + o, wp};
+  const float E0 = gather_edge<ORDER_OF_PUSH>(vex, g0, g1, 0);
+  const float E1 = gather_edge<ORDER_OF_PUSH>(vey, g0, g1, 1);
+  const float Hf = gather_cell<ORDER_OF_PUSH>(SumView32{vhx, vhy}, g0, g1);
+  // hard-edge dipole at the absolute position of R1 (bend frame, FP64)
+  const double X = a.org0 + ((double)ci + (double)x0) * a.h0, Y = a.org1 + ((double)cj + (double)x1) * a.h1;
+  const double dist = a.chh * (X - a.Lb) - a.shh * (Y - a.hw);
+  const float bext = (dist > 0.0 && dist < a.bwidth) ? (float)a.bz : 0.0f;
+  const float B = (float)kMu0 * Hf + 0.5f * bext;
+  // kick + rotation (PartBunch.cpp:366-383) on u - P
+  const float k0 = a.f1 * E0, k1 = a.f1 * E1;
+  const float du0 = d0 + k0, du1 = d1 + k1;
+  const float ru = rgam32(R, du0, du1);
+  const float aa = a.f2 * B * ru;
+  const float sv0 = du0 + aa * (R.P1 + du1), sv1 = du1 - aa * (R.P0 + du0);  // s - P
+  const float cf = aa / (1.0f + aa * aa);
+  d0 = (sv0 + cf * (R.P1 + sv1)) + k0;
+  d1 = (sv1 - cf * (R.P0 + sv0)) + k1;
+  a.b.dpx[n] = d0; a.b.dpy[n] = d1;
+  // second half drift to R2, stored as cell + offset
+  const float r = rgam32(R, d0, d1);
+  int nc;
+  store32(fadd(x0, drift32(R.kh0, R.P0, d0, r)), fadd(x1, drift32(R.kh1, R.P1, d1, r)), ci, cj, nc, m.o0, m.o1);
+  a.b.cell[n] = nc; a.b.ox[n] = m.o0; a.b.oy[n] = m.o1;
+  unpack(nc, m.ni, m.nj);
+  if (a.old_cell) { a.old_cell[n] = (ci & 0xffff) | (cj << 16); a.old_o0[n] = m.a0; a.old_o1[n] = m.a1; }
 }
 
 // Boxes of one moved particle: R0 u R2 (the deposit bounds) and the next
-// push's gather position.  Boxes hold cell index + 0.5: only the cells are
-// used, and a cell-relative coordinate added to a large index could round
-// across a cell border.
+// push's gather position, the stored R2, as static-mesh cell indices; they
+// are merged as cell + 0.5 (only the cells are used).
 struct Boxes32 {
-  double amn0 = INFINITY, amn1 = INFINITY, amx0 = -INFINITY, amx1 = -INFINITY;  // R0 u R2 (cells)
-  double bmn0 = INFINITY, bmn1 = INFINITY, bmx0 = -INFINITY, bmx1 = -INFINITY;  // next R1 (cells)
+  int amn0 = INT_MAX, amn1 = INT_MAX, amx0 = INT_MIN, amx1 = INT_MIN;  // R0 u R2
+  int bmn0 = INT_MAX, bmn1 = INT_MAX, bmx0 = INT_MIN, bmx1 = INT_MIN;  // next R1
   __device__ __forceinline__ void add(const Move32 &m) {
-    amn0 = fmin(amn0, cellc(m.ci, fmin(m.r00, m.e0))); amn1 = fmin(amn1, cellc(m.cj, fmin(m.r01, m.e1)));
-    amx0 = fmax(amx0, cellc(m.ci, fmax(m.r00, m.e0))); amx1 = fmax(amx1, cellc(m.cj, fmax(m.r01, m.e1)));
-    // next push gathers at (stored R2 - w) + w
-    const double n0 = cellc(m.ni, dadd(dsub((double)m.o0, m.w0), m.w0));
-    const double n1 = cellc(m.nj, dadd(dsub((double)m.o1, m.w1), m.w1));
-    bmn0 = fmin(bmn0, n0); bmn1 = fmin(bmn1, n1); bmx0 = fmax(bmx0, n0); bmx1 = fmax(bmx1, n1);
+    const int r0 = m.ci + (int)floorf(m.a0), r1 = m.cj + (int)floorf(m.a1);
+    amn0 = min(amn0, min(r0, m.ni)); amn1 = min(amn1, min(r1, m.nj));
+    amx0 = max(amx0, max(r0, m.ni)); amx1 = max(amx1, max(r1, m.nj));
+    bmn0 = min(bmn0, m.ni); bmn1 = min(bmn1, m.nj); bmx0 = max(bmx0, m.ni); bmx1 = max(bmx1, m.nj);
+  }
+  __device__ __forceinline__ static double c(int v, bool lo) {
+    return lo ? (v == INT_MAX ? INFINITY : v + 0.5) : (v == INT_MIN ? -INFINITY : v + 0.5);
   }
   __device__ __forceinline__ void store(WinState *ws, PushShared &sh) {
-    block_bbox(amn0, amn1, amx0, amx1, ws->bball, sh.sb);
-    block_bbox(bmn0, bmn1, bmx0, bmx1, ws->bb[1 - ws->cur], sh.sb);
-  }
-};
-
-// Deposit state of one CTA: the warp tiles (dynamic shared memory) over the
-// member's window accumulator in global memory.
-template <int ORDER>
-struct Depositor32 {
-  using Tile = typename TileFor<ORDER>::T;
-  Tile tile;
-  unsigned long long *win;
-  int L0, L1;
-  double scale;
-  bool overflow = false;
-
-  // Called by all threads of the CTA; ends with a barrier.
-  __device__ __forceinline__ void begin(const Push32Args &a, unsigned long long *sm, int l0, int l1) {
-    L0 = l0; L1 = l1; scale = a.acc_scale;
-    win = a.acc;
-    for (int k = threadIdx.x; k < Tile::kSize * (int)blockDim.x; k += blockDim.x) sm[k] = 0ull;
-    __syncthreads();
-    tile.init(sm, L0, L1);
-  }
-
-  // Current of one move R0 -> R2 (cells from the old cell, whose window cell
-  // is (wi, wj)), FP64 weights summed in the warp's tile.  Called by all
-  // lanes of the warp together (has: this lane has a particle).
-  __device__ __forceinline__ void particle(const Push32Args &a, bool has, int wi, int wj, double q, double r00,
-                                           double r01, double e0, double e1) {
-    tile.template rebase<false>(has, has ? wi + (int)floor(r00) : 0, has ? wj + (int)floor(r01) : 0, win, L0, L1);
-    if (has) {
-      auto sink = [&](int i, int j, double v) {
-        tile.template add<false>(i + wi, j + wj, __double2ll_rn(v * scale), win, L0, L1);
-      };
-      if (!deposit_particle<ORDER>(a.jcomp, q, r00, r01, e0, e1, 0.0, 0.0, 1.0, 1.0, a.h0, a.h1, a.dt, sink))
-        overflow = true;
-    }
-  }
-
-  // Called by all threads of the CTA after their last particle(); ends with
-  // a barrier.
-  __device__ __forceinline__ void end(const Push32Args &a) {
-    tile.template flush<false>(win, L0, L1);
-    if (overflow) set_err(a.ws, kErrCrossings);
-    __syncthreads();
+    block_bbox(c(amn0, true), c(amn1, true), c(amx0, false), c(amx1, false), ws->bball, sh.sb);
+    block_bbox(c(bmn0, true), c(bmn1, true), c(bmx0, false), c(bmx1, false), ws->bb[1 - ws->cur], sh.sb);
   }
 };
 
@@ -216,127 +159,72 @@ __device__ __forceinline__ bool entry_error(WinState *ws, PushShared &sh) {
   return sh.err != 0;
 }
 
-// Move and deposit of one CTA's share [beg, end) of one member; called by
-// all threads of the CTA, each ends with a barrier, so that a CTA may run
-// them for several members in turn.
-template <int ORDER>
-__device__ __forceinline__ void move32_range(const Push32Args &a, long long beg, long long end, PushShared &sh) {
+// The fused push of one CTA's share [beg, end) of one member: every lane
+// moves its particle, then the warp deposits the moves' flux (flux32.cuh)
+// into per-lane shared-memory tiles around a base cell the warp shares,
+// which drain into the member's window accumulator in global memory.  Called
+// by all threads of the CTA; ends with a barrier, so a CTA may run it for
+// several members in turn.
+template <int ORDER, int COMP>
+__device__ __forceinline__ void push32_range(const Push32Args &a, long long beg, long long end, PushShared &sh,
+                                             unsigned long long *sm) {
   if (entry_error(a.ws, sh)) return;  // the whole CTA leaves together
   WinState *ws = a.ws;
   const int L0 = ws->L0, L1 = ws->L1, WP0 = ws->P0, WP1 = ws->P1;
+  using Tile = typename TileFor<ORDER>::T;
+  for (int k = threadIdx.x; k < Tile::kSize * (int)blockDim.x; k += blockDim.x) sm[k] = 0ull;
+  __syncthreads();
+  Tile tile;
+  tile.init(sm, L0, L1);
   Boxes32 box;
-  for (long long n = beg + threadIdx.x; n < end; n += blockDim.x) {
+  bool overflow = false;
+  const long long rounds = end > beg ? (end - beg + blockDim.x - 1) / blockDim.x : 0;
+  for (long long it = 0; it < rounds; ++it) {  // the same rounds for every lane of the warp
+    const long long n = beg + it * blockDim.x + threadIdx.x;
     Move32 m;
-    move32<ORDER>(a, n, true, L0, L1, WP0, WP1, m);
-    a.dep_r0[2 * n] = m.ok ? m.r00 : NAN;
-    a.dep_r0[2 * n + 1] = m.r01;
-    a.dep_cell[n] = (m.ci & 0xffff) | (m.cj << 16);
-    if (m.ok) box.add(m);
+    m.ok = false;
+    m.ci = WP0; m.cj = WP1;
+    if (n < end) {
+      move32<ORDER>(a, n, L0, L1, WP0, WP1, m);
+      if (m.ok) box.add(m);
+    }
+    const int wi = m.ci - WP0, wj = m.cj - WP1;
+    tile.template rebase<false>(m.ok, wi, wj, a.acc, L0, L1);
+    if (m.ok) {
+      const double K = (double)m.q * a.acc_scale;
+      auto sink = [&](int i, int j, long long v) { tile.template add<false>(wi + i, wj + j, v, a.acc, L0, L1); };
+      if (!flux_particle<ORDER, COMP>(m.a0, m.a1, m.ni - m.ci, m.nj - m.cj, m.o0, m.o1, K, __double2ll_rn(K),
+                                      sink))
+        overflow = true;
+    }
   }
+  tile.template flush<false>(a.acc, L0, L1);
+  if (overflow) set_err(ws, kErrCrossings);
   box.store(ws, sh);
   __syncthreads();
 }
 
+// CTAs per SM of the push launches: three for CIC and TSC, two for the
+// cubic shape, whose 5 x 5 stencil box needs more registers.
 template <int ORDER>
-__device__ __forceinline__ void dep32_range(const Push32Args &a, long long beg, long long end, PushShared &sh,
-                                            unsigned long long *sacc) {
-  if (entry_error(a.ws, sh)) return;
-  WinState *ws = a.ws;
-  const int L0 = ws->L0, L1 = ws->L1, WP0 = ws->P0, WP1 = ws->P1;
-  Depositor32<ORDER> dep;
-  dep.begin(a, sacc, L0, L1);
-  // a round's inputs are loaded together, one round ahead, so that their
-  // latency overlaps the deposit of the round before
-  struct In {
-    double2 r0;
-    int c0, c1;
-    float o0, o1, q;
-  };
-  auto load = [&](long long n, In &v) {
-    if (n < end) {
-      v.r0 = reinterpret_cast<const double2 *>(a.dep_r0)[n];
-      v.c0 = a.dep_cell[n]; v.c1 = a.b.cell[n];
-      v.o0 = a.b.ox[n]; v.o1 = a.b.oy[n]; v.q = a.b.q[n];
-    } else {
-      v.r0.x = NAN; v.r0.y = 0.0; v.c0 = v.c1 = 0; v.o0 = v.o1 = v.q = 0.0f;
-    }
-  };
-  const long long rounds = end > beg ? (end - beg + blockDim.x - 1) / blockDim.x : 0;
-  In cur, nxt;
-  load(beg + threadIdx.x, cur);
-  for (long long it = 0; it < rounds; ++it) {  // the same rounds for every lane
-    if (it + 1 < rounds) load(beg + (it + 1) * blockDim.x + threadIdx.x, nxt);
-    const bool has = !isnan(cur.r0.x);
-    double e0 = 0.0, e1 = 0.0;
-    int ci = 0, cj = 0;
-    if (has) {
-      unpack(cur.c0, ci, cj);
-      int ni, nj;
-      unpack(cur.c1, ni, nj);
-      e0 = (double)(ni - ci) + (double)cur.o0;
-      e1 = (double)(nj - cj) + (double)cur.o1;
-    }
-    dep.particle(a, has, ci - WP0, cj - WP1, (double)cur.q, cur.r0.x, cur.r0.y, e0, e1);
-    cur = nxt;
-  }
-  dep.end(a);
-}
+struct Push32Occ { static constexpr int kCtas = ORDER == 2 ? 2 : 3; };
 
-// The FP32 push in two launches.  The move launch moves every particle
-// (gather, kick, drift, stores, boxes) with no shared memory and leaves for
-// the deposit each particle's start R0 and old cell in a.dep_r0 / a.dep_cell
-// (NaN for a particle it did not move); the deposit launch then adds the
-// current of every move R0 -> R2, CTA by CTA over contiguous (cell-sorted)
-// ranges.  Both run at three CTAs per SM and are bound by the latency of
-// dependent FP64 chains, not by bytes: split, each runs at 24 warps per SM
-// where the fused push's 128 registers and 98 KB of shared memory (window
-// accumulator copy + tiles) allowed 16 (4e6-particle TSC bunch, 8192 x 1024
-// mesh: 0.50 -> 0.40 ms per push).  The extra traffic is 20 bytes written
-// and 36 read per particle.
-template <int ORDER>
-__global__ void __launch_bounds__(256, 3) k_push32_move(Push32Args a) {
-  __shared__ PushShared sh;
-  const long long per = (a.b.n + gridDim.x - 1) / gridDim.x;
-  const long long beg = (long long)blockIdx.x * per;
-  move32_range<ORDER>(a, beg, beg + per < a.b.n ? beg + per : a.b.n, sh);
-}
-
-template <int ORDER>
-__global__ void __launch_bounds__(256, 3) k_push32_dep(Push32Args a) {
+template <int ORDER, int COMP>
+__global__ void __launch_bounds__(256, Push32Occ<ORDER>::kCtas) k_push32(Push32Args a) {
   extern __shared__ unsigned long long sacc[];
   __shared__ PushShared sh;
   const long long per = (a.b.n + gridDim.x - 1) / gridDim.x;
   const long long beg = (long long)blockIdx.x * per;
-  dep32_range<ORDER>(a, beg, beg + per < a.b.n ? beg + per : a.b.n, sh, sacc);
+  push32_range<ORDER, COMP>(a, beg, beg + per < a.b.n ? beg + per : a.b.n, sh, sacc);
 }
 
-// One push over a batch of FP32-mode members in two launches, as for one
-// member: the members' particles form one index range (ppre: first particle
-// of each member, m + 1 entries) cut into equal contiguous shares, one per
-// CTA; a CTA runs the move (then, in the second launch, the deposit) of every
-// member its share overlaps.
-template <int ORDER>
-__global__ void __launch_bounds__(256, 3) k_push32_batch_move(const Push32Args *args, const long long *ppre, int m,
-                                                            long long per) {
-  __shared__ PushShared sh;
-  __shared__ Push32Args sa;
-  const long long total = ppre[m];
-  const long long g0 = (long long)blockIdx.x * per;
-  const long long g1 = g0 + per < total ? g0 + per : total;
-  for (int mm = 0; mm < m; ++mm) {
-    const long long b0 = ppre[mm], b1 = ppre[mm + 1];
-    if (b1 <= g0 || b0 >= g1) continue;
-    const long long lb = (g0 > b0 ? g0 : b0) - b0, le = (g1 < b1 ? g1 : b1) - b0;
-    __syncthreads();
-    if (threadIdx.x == 0) sa = args[mm];
-    __syncthreads();
-    move32_range<ORDER>(sa, lb, le, sh);
-  }
-}
-
-template <int ORDER>
-__global__ void __launch_bounds__(256, 3) k_push32_batch_dep(const Push32Args *args, const long long *ppre, int m,
-                                                           long long per) {
+// One push over a batch of FP32-mode members: the members' particles form one
+// index range (ppre: first particle of each member, m + 1 entries) cut into
+// equal contiguous shares, one per CTA; a CTA runs the push of every member
+// its share overlaps.
+template <int ORDER, int COMP>
+__global__ void __launch_bounds__(256, Push32Occ<ORDER>::kCtas) k_push32_batch(const Push32Args *args, const long long *ppre, int m,
+                                                       long long per) {
   extern __shared__ unsigned long long sacc[];
   __shared__ PushShared sh;
   __shared__ Push32Args sa;
@@ -350,7 +238,49 @@ __global__ void __launch_bounds__(256, 3) k_push32_batch_dep(const Push32Args *a
     __syncthreads();
     if (threadIdx.x == 0) sa = args[mm];
     __syncthreads();
-    dep32_range<ORDER>(sa, lb, le, sh, sacc);
+    push32_range<ORDER, COMP>(sa, lb, le, sh, sacc);
+  }
+}
+
+// Stand-alone flux of n moves (csrst_flux32) into dense patches, one thread
+// per move, with 64-bit atomics; err[0]: crossing overflow, err[1]: a
+// non-zero contribution fell outside the patch.
+template <int ORDER, int COMP>
+__global__ void k_flux32(const int *cell0, const float *a0, const float *a1, const int *cell1, const float *b0,
+                         const float *b1, const float *q, long long n, double scale, int i0, int j0, int ni, int nj,
+                         unsigned long long *F, unsigned long long *drho, int *err) {
+  using SH = Flux32Shape<ORDER>;
+  for (long long k = gtid(); k < n; k += (long long)gridDim.x * blockDim.x) {
+    int ci, cj, ni_, nj_;
+    unpack(cell0[k], ci, cj);
+    unpack(cell1[k], ni_, nj_);
+    const double K = (double)q[k] * scale;
+    const long long Ki = __double2ll_rn(K);
+    bool dropped = false;
+    auto put = [&](unsigned long long *dst, int i, int j, long long v) {
+      i += ci - i0; j += cj - j0;
+      if (i < 0 || j < 0 || i >= ni || j >= nj) { if (v) dropped = true; return; }
+      atomicAdd(&dst[(size_t)j * ni + i], (unsigned long long)v);
+    };
+    auto sink = [&](int i, int j, long long v) { put(F, i, j, v); };
+    if (!flux_particle<ORDER, COMP>(a0[k], a1[k], ni_ - ci, nj_ - cj, b0[k], b1[k], K, Ki, sink)) {
+      atomicExch(&err[0], kErrCrossings);
+      continue;
+    }
+    if (drho) {  // the charge the flux conserves: rho(end) - rho(start), rows first
+      for (int e = 0; e < 2; ++e) {
+        double wx[SH::S], wy[SH::S];
+        long long R[SH::S], Q[SH::S];
+        const int I = (e ? ni_ - ci : 0) + charge_weights<ORDER>(e ? b0[k] : a0[k], wx);
+        const int J = (e ? nj_ - cj : 0) + charge_weights<ORDER>(e ? b1[k] : a1[k], wy);
+        quantise<ORDER>(wy, K, Ki, R);
+        for (int r = 0; r < SH::S; ++r) {
+          quantise<ORDER>(wx, (double)R[r], R[r], Q);
+          for (int c = 0; c < SH::S; ++c) put(drho, I + SH::OFF + c, J + SH::OFF + r, e ? Q[c] : -Q[c]);
+        }
+      }
+    }
+    if (dropped) atomicExch(&err[1], 1);
   }
 }
 
@@ -410,47 +340,51 @@ __global__ void k_bbox32_clear(WinState *ws) {
   if (threadIdx.x == 0) bbox_reset(ws->bb[ws->cur]);
 }
 
-// Box of the next push's gather positions R1 = (R - w) + w or R + w.
-__global__ void k_bbox32(Bunch32 b, double P0, double P1, double kh0, double kh1, int pending, WinState *ws) {
+// Box of the next push's gather positions R1: the stored position when the
+// trailing -dt/2 drift is pending, else stored + w.
+__global__ void k_bbox32(Bunch32 b, Ref32 R, int pending, WinState *ws) {
   double mn0 = INFINITY, mn1 = INFINITY, mx0 = -INFINITY, mx1 = -INFINITY;
   for (long long n = gtid(); n < b.n; n += (long long)gridDim.x * blockDim.x) {
     int ci, cj;
     unpack(b.cell[n], ci, cj);
-    double p0, p1;
-    const float r = rgam(P0, P1, b.dpx[n], b.dpy[n], p0, p1);
-    const double w0 = half_drift(kh0, p0, r), w1 = half_drift(kh1, p1, r);
-    double s0 = b.ox[n], s1 = b.oy[n];
-    if (pending) { s0 = dsub(s0, w0); s1 = dsub(s1, w1); }
-    const double x0 = cellc(ci, dadd(s0, w0)), x1 = cellc(cj, dadd(s1, w1));
-    mn0 = fmin(mn0, x0); mn1 = fmin(mn1, x1); mx0 = fmax(mx0, x0); mx1 = fmax(mx1, x1);
+    float x0 = b.ox[n], x1 = b.oy[n];
+    if (!pending) {
+      const float d0 = b.dpx[n], d1 = b.dpy[n], r = rgam32(R, d0, d1);
+      x0 = fadd(x0, drift32(R.kh0, R.P0, d0, r));
+      x1 = fadd(x1, drift32(R.kh1, R.P1, d1, r));
+    }
+    const double c0 = cellc(ci, x0), c1 = cellc(cj, x1);
+    mn0 = fmin(mn0, c0); mn1 = fmin(mn1, c1); mx0 = fmax(mx0, c0); mx1 = fmax(mx1, c1);
   }
   __shared__ double sb[4][32];
   block_bbox(mn0, mn1, mx0, mx1, ws->bb[ws->cur], sb);
 }
 
 // R += kd * v (cells), kd = dt c / h (PartBunch::drift_particles).
-__global__ void k_drift32(Bunch32 b, double P0, double P1, double kd0, double kd1) {
+__global__ void k_drift32(Bunch32 b, Ref32 R, float kd0, float kd1) {
   for (long long n = gtid(); n < b.n; n += (long long)gridDim.x * blockDim.x) {
     int ci, cj;
     unpack(b.cell[n], ci, cj);
-    double p0, p1;
-    const float r = rgam(P0, P1, b.dpx[n], b.dpy[n], p0, p1);
+    const float d0 = b.dpx[n], d1 = b.dpy[n], r = rgam32(R, d0, d1);
     int nc;
     float o0, o1;
-    store_pos(dadd((double)b.ox[n], half_drift(kd0, p0, r)), dadd((double)b.oy[n], half_drift(kd1, p1, r)), ci, cj,
-              nc, o0, o1);
+    store32(fadd(b.ox[n], drift32(kd0, R.P0, d0, r)), fadd(b.oy[n], drift32(kd1, R.P1, d1, r)), ci, cj, nc, o0, o1);
     b.cell[n] = nc; b.ox[n] = o0; b.oy[n] = o1;
   }
 }
 
+// FP64 bunch -> FP32 form: cell of (x - origin) / h and the offset in it.
 __global__ void k_from64(const double *x, const double *y, const double *px, const double *py, const double *q,
                          long long nn, double org0, double org1, double h0, double h1, double P0, double P1,
                          Bunch32 b) {
   for (long long n = gtid(); n < nn; n += (long long)gridDim.x * blockDim.x) {
-    int c;
-    float o0, o1;
-    store_pos((x[n] - org0) / h0, (y[n] - org1) / h1, 0, 0, c, o0, o1);
-    b.cell[n] = c; b.ox[n] = o0; b.oy[n] = o1;
+    const double t0 = (x[n] - org0) / h0, t1 = (y[n] - org1) / h1;
+    double f0 = floor(t0), f1 = floor(t1);
+    float a0 = (float)(t0 - f0), a1 = (float)(t1 - f1);
+    if (a0 >= 1.0f) { a0 = 0.0f; f0 += 1.0; }  // rounded up to the next cell
+    if (a1 >= 1.0f) { a1 = 0.0f; f1 += 1.0; }
+    b.cell[n] = ((int)f0 & 0xffff) | ((int)f1 << 16);
+    b.ox[n] = a0; b.oy[n] = a1;
     b.dpx[n] = (float)(px[n] - P0);
     b.dpy[n] = (float)(py[n] - P1);
     b.q[n] = (float)q[n];
@@ -503,25 +437,23 @@ inline unsigned grid_for(long long n, unsigned cap = 4096) {
   return (unsigned)(g < 1 ? 1 : (g > cap ? cap : g));
 }
 
-// The deposit launch keeps only the warp tiles in dynamic shared memory
-// (48-56 KB, above the 48 KB a launch gets without opting in) and adds into
-// the window accumulator in global memory: measured on the 4e6-particle TSC
-// bunch, a CTA copy of the accumulator in shared memory cost more (zeroing,
-// flushing its touched box) than the global adds it saves, and its size kept
-// the SM to two CTAs.
-template <int ORDER>
-size_t dep_smem32() {
+// The push keeps only the warp tiles in dynamic shared memory (48-56 KB,
+// above the 48 KB a launch gets without opting in) and adds into the window
+// accumulator in global memory, so that three CTAs fit on an SM.
+template <int ORDER, int COMP>
+size_t push_smem32() {
   static int set = 0;
   const size_t tiles = (size_t)TileFor<ORDER>::T::kSize * 256 * sizeof(unsigned long long);
   if (!set) {
-    cudaFuncSetAttribute(k_push32_dep<ORDER>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tiles);
+    cudaFuncSetAttribute(k_push32<ORDER, COMP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tiles);
+    cudaFuncSetAttribute(k_push32_batch<ORDER, COMP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tiles);
     cudaGetLastError();
     set = 1;
   }
   return tiles;
 }
 
-// CTAs of the move and deposit launches: three per SM.
+// CTAs of a push launch: three per SM.
 int push_grid32() {
   static int g = 0;
   if (!g) {
@@ -535,8 +467,27 @@ int push_grid32() {
 
 template <int ORDER>
 void push32_order(const Push32Args &a, cudaStream_t s) {
-  k_push32_move<ORDER><<<push_grid32(), 256, 0, s>>>(a);
-  k_push32_dep<ORDER><<<push_grid32(), 256, dep_smem32<ORDER>(), s>>>(a);
+  const int g = push_grid32() / 3 * Push32Occ<ORDER>::kCtas;
+  if (a.jcomp == 0) k_push32<ORDER, 0><<<g, 256, push_smem32<ORDER, 0>(), s>>>(a);
+  else k_push32<ORDER, 1><<<g, 256, push_smem32<ORDER, 1>(), s>>>(a);
+}
+
+template <int ORDER>
+void push32_batch_order(const Push32Args *args, const long long *ppre, int m, int ctas, long long per, int jcomp,
+                        cudaStream_t s) {
+  if (jcomp == 0) k_push32_batch<ORDER, 0><<<ctas, 256, push_smem32<ORDER, 0>(), s>>>(args, ppre, m, per);
+  else k_push32_batch<ORDER, 1><<<ctas, 256, push_smem32<ORDER, 1>(), s>>>(args, ppre, m, per);
+}
+
+template <int ORDER>
+void flux32_order(int comp, const int *cell0, const float *a0, const float *a1, const int *cell1, const float *b0,
+                  const float *b1, const float *q, long long n, double scale, int i0, int j0, int ni, int nj,
+                  unsigned long long *F, unsigned long long *drho, int *err, cudaStream_t s) {
+  const unsigned g = grid_for(n);
+  if (comp == 0)
+    k_flux32<ORDER, 0><<<g, 256, 0, s>>>(cell0, a0, a1, cell1, b0, b1, q, n, scale, i0, j0, ni, nj, F, drho, err);
+  else
+    k_flux32<ORDER, 1><<<g, 256, 0, s>>>(cell0, a0, a1, cell1, b0, b1, q, n, scale, i0, j0, ni, nj, F, drho, err);
 }
 
 }  // namespace
@@ -550,24 +501,11 @@ int launch_push32(const Push32Args &a, int order, cudaStream_t s) {
 }
 
 // The batched FP32 push keeps no window copy in shared memory (0: no member
-// "fits"); its deposit launch takes the warp tiles of the largest shape order.
-long long push32_batch_smem_limit() {
-  static int set = 0;
-  if (!set) {
-    cudaFuncSetAttribute(k_push32_batch_dep<0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)(TileFor<0>::T::kSize * 256 * sizeof(unsigned long long)));
-    cudaFuncSetAttribute(k_push32_batch_dep<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)(TileFor<1>::T::kSize * 256 * sizeof(unsigned long long)));
-    cudaFuncSetAttribute(k_push32_batch_dep<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)(TileFor<2>::T::kSize * 256 * sizeof(unsigned long long)));
-    cudaGetLastError();
-    set = 1;
-  }
-  return 0;
-}
+// "fits"); its launches take the warp tiles of their shape order.
+long long push32_batch_smem_limit() { return 0; }
 
 void launch_push32_batch(const PushGroup *groups, int ngroups, int m, int grid, const PrepArgs *prep, cudaStream_t s,
-            int parts) {
+                         int parts) {
   const int tb = (m + 127) / 128;
   if (parts & 1) k_prep32_batch<<<tb, 128, 0, s>>>(prep, m);
   for (int g = 0; g < ngroups; ++g) {
@@ -576,23 +514,24 @@ void launch_push32_batch(const PushGroup *groups, int ngroups, int m, int grid, 
     const int ctas = (int)((long long)grid * G.total / (G.all > 0 ? G.all : G.total)) + 1;
     const long long per = (G.total + ctas - 1) / ctas;
     const Push32Args *args = static_cast<const Push32Args *>(G.args);
-    push32_batch_smem_limit();
-    const size_t tiles = push_tile_bytes(G.order);
-    if (G.order == 0) {
-      k_push32_batch_move<0><<<ctas, 256, 0, s>>>(args, G.ppre, G.m, per);
-      k_push32_batch_dep<0><<<ctas, 256, tiles, s>>>(args, G.ppre, G.m, per);
-    } else if (G.order == 1) {
-      k_push32_batch_move<1><<<ctas, 256, 0, s>>>(args, G.ppre, G.m, per);
-      k_push32_batch_dep<1><<<ctas, 256, tiles, s>>>(args, G.ppre, G.m, per);
-    } else {
-      k_push32_batch_move<2><<<ctas, 256, 0, s>>>(args, G.ppre, G.m, per);
-      k_push32_batch_dep<2><<<ctas, 256, tiles, s>>>(args, G.ppre, G.m, per);
-    }
+    const int jcomp = G.jcomp;
+    if (G.order == 0) push32_batch_order<0>(args, G.ppre, G.m, ctas, per, jcomp, s);
+    else if (G.order == 1) push32_batch_order<1>(args, G.ppre, G.m, ctas, per, jcomp, s);
+    else push32_batch_order<2>(args, G.ppre, G.m, ctas, per, jcomp, s);
   }
   if (parts & 2) {
     k_post32_batch<<<tb, 128, 0, s>>>(prep, m);
     k_bounds32_batch<<<tb, 128, 0, s>>>(prep, m);
   }
+}
+
+void launch_flux32(int order, int comp, const int *cell0, const float *a0, const float *a1, const int *cell1,
+                   const float *b0, const float *b1, const float *q, long long n, double scale, int i0, int j0,
+                   int ni, int nj, unsigned long long *F, unsigned long long *drho, int *err, cudaStream_t s) {
+  if (n <= 0) return;
+  if (order == 0) flux32_order<0>(comp, cell0, a0, a1, cell1, b0, b1, q, n, scale, i0, j0, ni, nj, F, drho, err, s);
+  else if (order == 1) flux32_order<1>(comp, cell0, a0, a1, cell1, b0, b1, q, n, scale, i0, j0, ni, nj, F, drho, err, s);
+  else flux32_order<2>(comp, cell0, a0, a1, cell1, b0, b1, q, n, scale, i0, j0, ni, nj, F, drho, err, s);
 }
 
 void launch_prep32(WinState *ws, int order, cudaStream_t s) {
@@ -602,14 +541,13 @@ void launch_prep32(WinState *ws, int order, cudaStream_t s) {
 
 void launch_bounds32(WinState *ws, cudaStream_t s) { k_bounds32<<<1, 32, 0, s>>>(ws); }
 
-void launch_bbox32(const Bunch32 &b, double P0, double P1, double kh0, double kh1, int pending, WinState *ws,
-                   cudaStream_t s) {
+void launch_bbox32(const Bunch32 &b, const Ref32 &R, int pending, WinState *ws, cudaStream_t s) {
   k_bbox32_clear<<<1, 32, 0, s>>>(ws);
-  k_bbox32<<<grid_for(b.n, 1184), 256, 0, s>>>(b, P0, P1, kh0, kh1, pending, ws);
+  k_bbox32<<<grid_for(b.n, 1184), 256, 0, s>>>(b, R, pending, ws);
 }
 
-void launch_drift32(const Bunch32 &b, double P0, double P1, double kd0, double kd1, cudaStream_t s) {
-  if (b.n > 0) k_drift32<<<grid_for(b.n), 256, 0, s>>>(b, P0, P1, kd0, kd1);
+void launch_drift32(const Bunch32 &b, const Ref32 &R, float kd0, float kd1, cudaStream_t s) {
+  if (b.n > 0) k_drift32<<<grid_for(b.n), 256, 0, s>>>(b, R, kd0, kd1);
 }
 
 void launch_from64(const double *x, const double *y, const double *px, const double *py, const double *q,
@@ -618,12 +556,10 @@ void launch_from64(const double *x, const double *y, const double *px, const dou
   if (n > 0) k_from64<<<grid_for(n), 256, 0, s>>>(x, y, px, py, q, n, org0, org1, h0, h1, P0, P1, b);
 }
 
-void launch_to64(const Bunch32 &b, double P0, double P1, double kh0, double kh1, int pending, double org0,
-                 double org1, double h0, double h1, double *x, double *y, double *px, double *py,
-                 cudaStream_t s) {
+void launch_to64(const Bunch32 &b, const Ref32 &R, double P0, double P1, int pending, double org0, double org1,
+                 double h0, double h1, double *x, double *y, double *px, double *py, cudaStream_t s) {
   if (b.n > 0)
-    k_to64<<<grid_for(b.n), 256, 0, s>>>(Bunch32View{b, P0, P1, kh0, kh1, pending, org0, org1, h0, h1}, x, y, px,
-                                         py);
+    k_to64<<<grid_for(b.n), 256, 0, s>>>(Bunch32View{b, R, P0, P1, pending, org0, org1, h0, h1}, x, y, px, py);
 }
 
 // Mean-momentum sums: part holds 2 x 296 doubles, out2 receives the two sums.

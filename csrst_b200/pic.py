@@ -29,8 +29,10 @@ class Simulation:
     FLAG_FP32 = 2
 
     def __init__(self, cfg, keep_old=False, fp32=False):
-        """fp32: FP32 mode (FP32 fields, gather and kick; positions as FP32
-        offsets from FP64 cell origins; FP64 current deposit)."""
+        """fp32: FP32 mode (FP32 fields, gather, kick and positions, the
+        positions as FP32 offsets from FP64 cell origins; FP32 current path
+        integral with exact integer charge conservation, csrst_flux32).
+        keep_old: keep the start of every particle's last move."""
         c = Config()
         for k, v in cfg.dict().items():
             setattr(c, k, v)
@@ -117,6 +119,18 @@ class Simulation:
         a = [np.zeros(self.n) for _ in range(2)]
         self._ck(lib().csrst_get_old_positions(self.h, *map(ptr, a)))
         return a
+
+    def bunch32(self, which=0):
+        """FP32 mode's bunch as stored: which=0 -> (cell, ox, oy, dpx, dpy, q),
+        cells packed as i | j << 16; which=1 -> (cell, o0, o1) of the start of
+        every particle's last move (keep_old)."""
+        F = C.POINTER(C.c_float)
+        cell = np.zeros(self.n, np.int32)
+        f = [np.zeros(self.n, np.float32) for _ in range(5 if which == 0 else 2)]
+        args = [cell.ctypes.data_as(C.POINTER(C.c_int))] + [v.ctypes.data_as(F) for v in f]
+        args += [None] * (6 - len(args))
+        self._ck(lib().csrst_get_bunch32(self.h, which, *args))
+        return [cell] + f
 
     def window(self):
         w = (C.c_int * 4)()
@@ -352,6 +366,23 @@ class ShapeFunction:
         check(lib().csrst_deposit(self.order, comp, *map(ptr, a), len(a[0]), ptr(o), ptr(hh), dt, i0,
                                   j0, ni, nj, scale, ptr(J)))
         return J
+
+    def flux32(self, comp, cell0, a0, a1, cell1, b0, b1, q, scale, i0, j0, ni, nj, with_charge=False):
+        """FP32 mode's deposit (csrst_flux32) of moves cell0 + a -> cell1 + b:
+        the integer flux of component comp on a dense (nj, ni) patch at mesh
+        index (i0, j0) and, with_charge, the integer charge change, for which
+        drho + div F = 0 holds exactly."""
+        I, F, Q = C.POINTER(C.c_int), C.POINTER(C.c_float), C.POINTER(C.c_longlong)
+        i32 = lambda v: np.ascontiguousarray(v, dtype=np.int32)
+        f32 = lambda v: np.ascontiguousarray(v, dtype=np.float32)
+        a = [i32(cell0), f32(a0), f32(a1), i32(cell1), f32(b0), f32(b1), f32(q)]
+        out = np.zeros((nj, ni), np.int64)
+        rho = np.zeros((nj, ni), np.int64) if with_charge else None
+        tp = [I, F, F, I, F, F, F]
+        check(lib().csrst_flux32(self.order, comp, *[v.ctypes.data_as(t) for v, t in zip(a, tp)], len(a[0]),
+                                 float(scale), int(i0), int(j0), int(ni), int(nj), out.ctypes.data_as(Q),
+                                 rho.ctypes.data_as(Q) if with_charge else None))
+        return (out, rho) if with_charge else out
 
     def getChargeDensityDiff(self, ox, oy, x, y, q, origin, spacing, i0, j0, ni, nj, scale):
         r = np.zeros((nj, ni))

@@ -42,10 +42,11 @@ extern "C" {
 typedef struct csrst_handle csrst_handle;
 
 /* csrst_config.flags */
-#define CSRST_FLAG_KEEP_OLD 1  /* keep oldR of every push for csrst_get_old_positions (FP64 only) */
-#define CSRST_FLAG_FP32 2      /* FP32 mode: FP32 fields, gather and kick; positions as FP32 offsets
-                                * from FP64 cell origins, momenta as FP32 deviations from an FP64
-                                * reference momentum; FP64 current deposit.  No reference
+#define CSRST_FLAG_KEEP_OLD 1  /* keep oldR of every push for csrst_get_old_positions */
+#define CSRST_FLAG_FP32 2      /* FP32 mode: FP32 fields, gather, kick, drifts and positions (FP32
+                                * offsets from FP64 cell origins; momenta as FP32 deviations from an
+                                * FP64 reference momentum) and FP32 current path integral with exact
+                                * integer charge conservation (csrst_flux32).  No reference
                                 * counterpart; checked against the FP64 path to a tolerance. */
 
 /* Run set-up.  Mirrors the command line of src/main.cpp:111-136 for the
@@ -77,7 +78,7 @@ void *csrst_stream(csrst_handle *h);
 int csrst_sync(csrst_handle *h);
 
 /* Geometry: info8 = hx, hy, origin x, origin y, dt, fixed-point scale of the
- * current deposit, number of cut cells, window pitch.  Replaces Bend::Init /
+ * current deposit (FP32 mode: of the flux, csrst_flux32), number of cut cells, window pitch.  Replaces Bend::Init /
  * getInsideMask / SCBoundaryCondition::getBoundaryCells (Bend.cpp:85-124,
  * SCBoundaryCondition.hh:433-441). */
 int csrst_get_info(csrst_handle *h, double *info8);
@@ -280,6 +281,30 @@ int csrst_deposit(int order, int comp, const double *ox, const double *oy, const
 int csrst_charge_diff(int order, const double *ox, const double *oy, const double *x,
                       const double *y, const double *q, size_t n, const double *o2,
                       const double *hh2, int i0, int j0, int ni, int nj, double scale, double *rho);
+
+/* FP32 mode's charge-conserving deposit (no reference counterpart; the
+ * push of a CSRST_FLAG_FP32 handle deposits with it).  n moves from start
+ * cell0 + offset (a0, a1) (cells, any value) to end cell1 + offset (b0, b1)
+ * (in [0, 1)), cells packed as i | j << 16 like the FP32 bunch, charge q.
+ * F receives the integer flux of component comp (Fx = Jx dt hy / q, Fy =
+ * Jy dt hx / q, times scale * q) in a dense (ni x nj) patch at mesh index
+ * (i0, j0), at the elements of Jx(i, j) / Jy(i, j); drho (may be NULL) the
+ * integer charge change rho(end) - rho(start) in the same units at the
+ * vertices.  drho + div F = 0 holds exactly in integers:
+ *   drho(i,j) + Fx(i,j) - Fx(i-1,j) + Fy(i,j) - Fy(i,j-1) = 0.
+ * The path integral of the reference's current (Zeroth/First/Second-
+ * OrderShapeFunction) runs in FP32, the end points' charge weights in FP64.
+ * Host arrays.  Returns CSRST_E_CROSSINGS for a move of more than one cell
+ * on an axis, CSRST_W_OUTSIDE when contributions fell outside the patch. */
+int csrst_flux32(int order, int comp, const int *cell0, const float *a0, const float *a1, const int *cell1,
+                 const float *b0, const float *b1, const float *q, size_t n, double scale, int i0, int j0, int ni,
+                 int nj, long long *F, long long *drho);
+/* Raw FP32-mode bunch of a CSRST_FLAG_FP32 handle (host arrays, NULL to skip):
+ * which = 0: packed cells, offsets, momentum deviations and charges of the
+ * bunch as stored; which = 1: the packed cell and offsets of the start of
+ * each particle's last move (CSRST_FLAG_KEEP_OLD; d0, d1, q must be NULL).
+ * The reference momentum is csrst_get_particles' momentum minus d. */
+int csrst_get_bunch32(csrst_handle *h, int which, int *cell, float *o0, float *o1, float *d0, float *d1, float *q);
 
 /* Allocation-free csrst_deposit, for callers that cannot let a library
  * allocate device memory: a host framework that owns all device memory
