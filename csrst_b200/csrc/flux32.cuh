@@ -110,7 +110,7 @@ __device__ __forceinline__ void fy_segment(float p0, float p1, float e0, float e
                                            float d1, float (&v)[Flux32Shape<ORDER>::S][Flux32Shape<ORDER>::S - 1]) {
   if (ORDER == 0) {
     const float c0 = 0.5f * (p0 + e0);
-    const float D = e1 - p1;
+    const float D = tau * d1;  // e1 - p1 without the cancellation of two O(1) coordinates
     v[0][0] = D * ((float)(I + 1) - c0);
     v[1][0] = D * (c0 - (float)I);
   } else if (ORDER == 1) {
@@ -184,53 +184,67 @@ __device__ __forceinline__ float cross_fraction(float X, float a, float d) {
   return fminf(fmaxf((X - a) / d, 0.0f), 1.0f);
 }
 
+// Base indices of a move's end points (old-cell relative), for choosing the
+// deposit's form before running it.
+template <int ORDER>
+__device__ __forceinline__ int base_index(float o) {
+  return (int)floorf(ORDER == 1 ? o + 0.5f : o);
+}
+
 // The charge-conserving deposit of one move (see the top of the file).
 // (a0, a1): start offset in cells from the old cell (ci, cj), any value;
 // (dc0, dc1) = new cell - old cell, (b0, b1): end offset in the new cell;
 // K = q * scale, Kint = its integer value.  COMP selects the emitted
 // component; sink(i, j, v) gets old-cell-relative Jx / Jy indices.
+// FAST: the move keeps its y base index and advances its x base index by 0
+// or 1 (a bunch moving along +x at CFL <= 1, nearly every particle); the
+// stencil box then has S + 1 columns and S rows at compile-time offsets.
+// The caller checks that before choosing FAST (base_index).
 // Returns false when the move spans more than one base index on an axis
 // (more than one cell for CFL <= 1); nothing is emitted then.
-template <int ORDER, int COMP, class Sink>
+template <int ORDER, int COMP, bool FAST, class Sink>
 __device__ __forceinline__ bool flux_particle(float a0, float a1, int dc0, int dc1, float b0, float b1, double K,
                                               long long Kint, Sink &&sink) {
   using SH = Flux32Shape<ORDER>;
-  constexpr int S = SH::S, OFF = SH::OFF, B = S + 1;
+  constexpr int S = SH::S, OFF = SH::OFF, BX = S + 1, BY = FAST ? S : S + 1, NSEG = FAST ? 2 : 3;
   // 1. charge weights of both end points and their base indices (old-cell
   //    relative); the box starts at the lower base index of each axis
   double wAy[S], wBy[S];
   const int JA = charge_weights<ORDER>(a1, wAy);
   const int JB = dc1 + charge_weights<ORDER>(b1, wBy);
-  if (abs(JB - JA) > 1) return false;
-  const int jmin = JA < JB ? JA : JB;
-  long long RA[B], RB[B];  // row totals in the box frame
+  if (!FAST && abs(JB - JA) > 1) return false;
+  const int jmin = FAST ? JA : (JA < JB ? JA : JB);
+  const bool syA = FAST ? false : JA != jmin, syB = FAST ? false : JB != jmin;
+  long long RA[BY], RB[BY];  // row totals in the box frame
   {
     long long r[S];
     quantise<ORDER>(wAy, K, Kint, r);
-    shift_into(r, JA != jmin, RA);
+    shift_into(r, syA, RA);
     quantise<ORDER>(wBy, K, Kint, r);
-    shift_into(r, JB != jmin, RB);
+    shift_into(r, syB, RB);
   }
   double wAx[S], wBx[S];
   const int IA = charge_weights<ORDER>(a0, wAx);
   const int IB = dc0 + charge_weights<ORDER>(b0, wBx);
-  if (abs(IB - IA) > 1) return false;
-  const int imin = IA < IB ? IA : IB;
-  const bool sxA = IA != imin, sxB = IB != imin;
+  if (!FAST && abs(IB - IA) > 1) return false;
+  const int imin = FAST ? IA : (IA < IB ? IA : IB);
+  const bool sxA = FAST ? false : IA != imin, sxB = IB != imin;
   const int ib = imin + OFF, jb = jmin + OFF;
 
   // 2. y-current path integral in FP32 over the segments between crossings,
   //    each segment's values moved into the box frame by its vertex's offset
-  //    from the lower base index
-  const float e0 = (float)dc0 + b0, e1 = (float)dc1 + b1;  // end point, old-cell relative
-  const float d0 = e0 - a0, d1 = e1 - a1;
-  float fy[B][B - 1];
+  //    from the lower base index.  The displacement comes from the exact end
+  //    points in FP64 (a difference of O(1) FP32 coordinates would carry an
+  //    absolute error of their ulp).
+  const float d0 = (float)((double)dc0 + ((double)b0 - (double)a0));
+  const float d1 = (float)((double)dc1 + ((double)b1 - (double)a1));
+  float fy[BX][BY - 1];
 #pragma unroll
-  for (int c = 0; c < B; ++c)
+  for (int c = 0; c < BX; ++c)
 #pragma unroll
-    for (int r = 0; r < B - 1; ++r) fy[c][r] = 0.0f;
+    for (int r = 0; r < BY - 1; ++r) fy[c][r] = 0.0f;
   {
-    const bool hx = IB != IA, hy = JB != JA;
+    const bool hx = IB != IA, hy = FAST ? false : JB != JA;
     const float fx = hx ? cross_fraction(split_border<SH::DUAL>(imin), a0, d0) : 2.0f;
     const float fyc = hy ? cross_fraction(split_border<SH::DUAL>(jmin), a1, d1) : 2.0f;
     // up to three segments in order of the crossing fractions; the vertex of
@@ -240,20 +254,20 @@ __device__ __forceinline__ bool flux_particle(float a0, float a1, int dc0, int d
     float ts = 0.0f;
     int I = IA, J = JA;
 #pragma unroll
-    for (int sg = 0; sg < 3; ++sg) {
-      const float te = sg == 0 ? fminf(f1, 1.0f) : sg == 1 ? fminf(f2, 1.0f) : 1.0f;
+    for (int sg = 0; sg < NSEG; ++sg) {
+      const float te = sg == NSEG - 1 ? 1.0f : sg == 0 ? fminf(f1, 1.0f) : fminf(f2, 1.0f);
       const float tau = te - ts;
       if (tau > 0.0f) {
         float v[S][S - 1];
         fy_segment<ORDER>(a0 + ts * d0, a1 + ts * d1, a0 + te * d0, a1 + te * d1, I, J, tau, d0, d1, v);
-        float w[S][S];  // moved along the face rows
+        float w[S][BY - 1];  // moved along the face rows
 #pragma unroll
-        for (int t = 0; t < S; ++t) shift_into(v[t], J != jmin, w[t]);
+        for (int t = 0; t < S; ++t) shift_into(v[t], FAST ? false : J != jmin, w[t]);
         const bool cx = I != imin;
 #pragma unroll
-        for (int c = 0; c < B; ++c)
+        for (int c = 0; c < BX; ++c)
 #pragma unroll
-          for (int r = 0; r < B - 1; ++r) {
+          for (int r = 0; r < BY - 1; ++r) {
             const float lo = c < S ? w[c][r] : 0.0f, hi = c >= 1 ? w[c - 1][r] : 0.0f;
             fy[c][r] += cx ? hi : lo;
           }
@@ -268,32 +282,32 @@ __device__ __forceinline__ bool flux_particle(float a0, float a1, int dc0, int d
   const float Kf = (float)K;
   const int cstar = IA - imin - OFF;  // the box column of A's base vertex
   long long Y = 0;                    // total y flux of the face row below
-  long long fyPrev[B];                // corrected Fy of the face row below
+  long long fyPrev[BX];               // corrected Fy of the face row below
 #pragma unroll
-  for (int c = 0; c < B; ++c) fyPrev[c] = 0;
+  for (int c = 0; c < BX; ++c) fyPrev[c] = 0;
 #pragma unroll
-  for (int r = 0; r < B; ++r) {
-    long long fyRow[B];
-    if (r < B - 1) {
+  for (int r = 0; r < BY; ++r) {
+    long long fyRow[BX];
+    if (r < BY - 1) {
       Y -= RB[r] - RA[r];
       long long sum = 0;
 #pragma unroll
-      for (int c = 0; c < B; ++c) { fyRow[c] = __float2ll_rn(Kf * fy[c][r]); sum += fyRow[c]; }
+      for (int c = 0; c < BX; ++c) { fyRow[c] = __float2ll_rn(Kf * fy[c][r]); sum += fyRow[c]; }
 #pragma unroll
-      for (int c = 0; c < B; ++c)
+      for (int c = 0; c < BX; ++c)
         if (c == cstar) fyRow[c] += Y - sum;
       if (COMP == 1) {
 #pragma unroll
-        for (int c = 0; c < B; ++c)
+        for (int c = 0; c < BX; ++c)
           if (fyRow[c] != 0) sink(ib + c, jb + r, fyRow[c]);
       }
     } else {
 #pragma unroll
-      for (int c = 0; c < B; ++c) fyRow[c] = 0;
+      for (int c = 0; c < BX; ++c) fyRow[c] = 0;
     }
     if (COMP == 0) {
       // this row's charges in the box frame, each row summing to its R exactly
-      long long qA[B], qB[B];
+      long long qA[BX], qB[BX];
       {
         long long t[S];
         quantise<ORDER>(wAx, (double)RA[r], RA[r], t);
@@ -303,13 +317,13 @@ __device__ __forceinline__ bool flux_particle(float a0, float a1, int dc0, int d
       }
       long long fx = 0;
 #pragma unroll
-      for (int c = 0; c < B - 1; ++c) {
+      for (int c = 0; c < BX - 1; ++c) {
         fx -= (qB[c] - qA[c]) + fyRow[c] - fyPrev[c];
         if (fx != 0) sink(ib + c, jb + r, fx);
       }
     }
 #pragma unroll
-    for (int c = 0; c < B; ++c) fyPrev[c] = fyRow[c];
+    for (int c = 0; c < BX; ++c) fyPrev[c] = fyRow[c];
   }
   return true;
 }

@@ -190,12 +190,18 @@ __device__ __forceinline__ void push32_range(const Push32Args &a, long long beg,
     }
     const int wi = m.ci - WP0, wj = m.cj - WP1;
     tile.template rebase<false>(m.ok, wi, wj, a.acc, L0, L1);
+    // the compact form when every particle of the warp keeps its y base index
+    // and advances by at most one x base index
+    const int dx = m.ni - m.ci + base_index<ORDER>(m.o0) - base_index<ORDER>(m.a0);
+    const bool fast = !m.ok || ((unsigned)dx <= 1u && m.nj - m.cj + base_index<ORDER>(m.o1) == base_index<ORDER>(m.a1));
+    const bool all_fast = __all_sync(0xffffffffu, fast);
     if (m.ok) {
       const double K = (double)m.q * a.acc_scale;
       auto sink = [&](int i, int j, long long v) { tile.template add<false>(wi + i, wj + j, v, a.acc, L0, L1); };
-      if (!flux_particle<ORDER, COMP>(m.a0, m.a1, m.ni - m.ci, m.nj - m.cj, m.o0, m.o1, K, __double2ll_rn(K),
-                                      sink))
-        overflow = true;
+      const bool ok = all_fast
+          ? flux_particle<ORDER, COMP, true>(m.a0, m.a1, m.ni - m.ci, m.nj - m.cj, m.o0, m.o1, K, __double2ll_rn(K), sink)
+          : flux_particle<ORDER, COMP, false>(m.a0, m.a1, m.ni - m.ci, m.nj - m.cj, m.o0, m.o1, K, __double2ll_rn(K), sink);
+      if (!ok) overflow = true;
     }
   }
   tile.template flush<false>(a.acc, L0, L1);
@@ -263,7 +269,7 @@ __global__ void k_flux32(const int *cell0, const float *a0, const float *a1, con
       atomicAdd(&dst[(size_t)j * ni + i], (unsigned long long)v);
     };
     auto sink = [&](int i, int j, long long v) { put(F, i, j, v); };
-    if (!flux_particle<ORDER, COMP>(a0[k], a1[k], ni_ - ci, nj_ - cj, b0[k], b1[k], K, Ki, sink)) {
+    if (!flux_particle<ORDER, COMP, false>(a0[k], a1[k], ni_ - ci, nj_ - cj, b0[k], b1[k], K, Ki, sink)) {
       atomicExch(&err[0], kErrCrossings);
       continue;
     }

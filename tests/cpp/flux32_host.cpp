@@ -16,7 +16,8 @@ namespace {
 
 template <int ORDER, int COMP>
 int run(const int *c0, const float *a0, const float *a1, const int *c1, const float *b0, const float *b1,
-        const float *q, long n, double scale, int i0, int j0, int ni, int nj, long long *F, long long *drho) {
+        const float *q, long n, double scale, int i0, int j0, int ni, int nj, long long *F, long long *drho,
+        bool fast_ok) {
   using SH = csrst::Flux32Shape<ORDER>;
   int bad = 0;
   for (long k = 0; k < n; ++k) {
@@ -30,7 +31,14 @@ int run(const int *c0, const float *a0, const float *a1, const int *c1, const fl
       else if (v) bad |= 2;
     };
     auto sink = [&](int i, int j, long long v) { put(F, i, j, v); };
-    if (!csrst::flux_particle<ORDER, COMP>(a0[k], a1[k], ni_ - ci, nj_ - cj, b0[k], b1[k], K, Ki, sink)) {
+    const int dx = ni_ - ci + csrst::base_index<ORDER>(b0[k]) - csrst::base_index<ORDER>(a0[k]);
+    const bool fast = fast_ok && (unsigned)dx <= 1u &&
+                      nj_ - cj + csrst::base_index<ORDER>(b1[k]) == csrst::base_index<ORDER>(a1[k]);
+    const bool ok = fast ? csrst::flux_particle<ORDER, COMP, true>(a0[k], a1[k], ni_ - ci, nj_ - cj, b0[k], b1[k], K,
+                                                                   Ki, sink)
+                         : csrst::flux_particle<ORDER, COMP, false>(a0[k], a1[k], ni_ - ci, nj_ - cj, b0[k], b1[k],
+                                                                    K, Ki, sink);
+    if (!ok) {
       bad |= 1;
       continue;
     }
@@ -52,13 +60,14 @@ int run(const int *c0, const float *a0, const float *a1, const int *c1, const fl
 
 }  // namespace
 
+// fast: take the compact form for the moves that allow it (as the push does)
 extern "C" int flux32_host(int order, int comp, const int *c0, const float *a0, const float *a1, const int *c1,
                            const float *b0, const float *b1, const float *q, long n, double scale, int i0, int j0,
-                           int ni, int nj, long long *F, long long *drho) {
-  if (order == 0) return comp ? run<0, 1>(c0, a0, a1, c1, b0, b1, q, n, scale, i0, j0, ni, nj, F, drho)
-                              : run<0, 0>(c0, a0, a1, c1, b0, b1, q, n, scale, i0, j0, ni, nj, F, drho);
-  if (order == 1) return comp ? run<1, 1>(c0, a0, a1, c1, b0, b1, q, n, scale, i0, j0, ni, nj, F, drho)
-                              : run<1, 0>(c0, a0, a1, c1, b0, b1, q, n, scale, i0, j0, ni, nj, F, drho);
-  return comp ? run<2, 1>(c0, a0, a1, c1, b0, b1, q, n, scale, i0, j0, ni, nj, F, drho)
-              : run<2, 0>(c0, a0, a1, c1, b0, b1, q, n, scale, i0, j0, ni, nj, F, drho);
+                           int ni, int nj, long long *F, long long *drho, int fast) {
+  if (order == 0) return comp ? run<0, 1>(c0, a0, a1, c1, b0, b1, q, n, scale, i0, j0, ni, nj, F, drho, fast != 0)
+                              : run<0, 0>(c0, a0, a1, c1, b0, b1, q, n, scale, i0, j0, ni, nj, F, drho, fast != 0);
+  if (order == 1) return comp ? run<1, 1>(c0, a0, a1, c1, b0, b1, q, n, scale, i0, j0, ni, nj, F, drho, fast != 0)
+                              : run<1, 0>(c0, a0, a1, c1, b0, b1, q, n, scale, i0, j0, ni, nj, F, drho, fast != 0);
+  return comp ? run<2, 1>(c0, a0, a1, c1, b0, b1, q, n, scale, i0, j0, ni, nj, F, drho, fast != 0)
+              : run<2, 0>(c0, a0, a1, c1, b0, b1, q, n, scale, i0, j0, ni, nj, F, drho, fast != 0);
 }

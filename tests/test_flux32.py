@@ -28,7 +28,7 @@ def host(tmp_path_factory):
     L = C.CDLL(str(so))
     I, F, Q = C.POINTER(C.c_int), C.POINTER(C.c_float), C.POINTER(C.c_longlong)
     L.flux32_host.argtypes = [C.c_int, C.c_int, I, F, F, I, F, F, F, C.c_long, C.c_double, C.c_int, C.c_int,
-                              C.c_int, C.c_int, Q, Q]
+                              C.c_int, C.c_int, Q, Q, C.c_int]
     L.flux32_host.restype = C.c_int
     return L
 
@@ -63,7 +63,7 @@ def random_moves(n, seed, cfl=0.9):
     return pack(ci, cj), a0, a1, pack(ni, nj), b0, b1, q, (ci, cj, ni, nj)
 
 
-def flux(host, order, comp, mv, scale, ni=48, nj=48, drho=False):
+def flux(host, order, comp, mv, scale, ni=48, nj=48, drho=False, fast=True):
     c0, a0, a1, c1, b0, b1, q, _ = mv
     F = np.zeros((nj, ni), dtype=np.int64)
     R = np.zeros((nj, ni), dtype=np.int64) if drho else None
@@ -71,7 +71,7 @@ def flux(host, order, comp, mv, scale, ni=48, nj=48, drho=False):
     rc = host.flux32_host(order, comp, P(c0, C.c_int), P(a0, C.c_float), P(a1, C.c_float), P(c1, C.c_int),
                           P(b0, C.c_float), P(b1, C.c_float), P(q, C.c_float), len(q), scale, 0, 0, ni, nj,
                           F.ctypes.data_as(C.POINTER(C.c_longlong)),
-                          R.ctypes.data_as(C.POINTER(C.c_longlong)) if drho else None)
+                          R.ctypes.data_as(C.POINTER(C.c_longlong)) if drho else None, 1 if fast else 0)
     assert rc == 0
     return F, R
 
@@ -119,6 +119,18 @@ def test_flux32_matches_fp64_reference_current(host, oracle, order):
     assert np.abs(rho32 - ref_rho).max() <= 1e-12 * np.abs(ref_rho).max()
 
 
+@pytest.mark.parametrize("order", [0, 1, 2])
+def test_flux32_compact_form_is_bit_identical(host, order):
+    """The compact form the push takes for moves that keep their y base index
+    and advance x by at most one gives the same integers as the general form."""
+    mv = random_moves(20000, 31 + order, cfl=0.6)
+    scale = flux_scale(mv[6])
+    for comp in (0, 1):
+        a, ra = flux(host, order, comp, mv, scale, drho=True, fast=True)
+        b, rb = flux(host, order, comp, mv, scale, drho=True, fast=False)
+        assert np.array_equal(a, b) and np.array_equal(ra, rb)
+
+
 def test_flux32_rejects_moves_of_more_than_one_cell(host):
     mv = list(random_moves(100, 3))
     c0, c1 = mv[0].copy(), mv[3].copy()
@@ -128,5 +140,5 @@ def test_flux32_rejects_moves_of_more_than_one_cell(host):
     P = lambda a, t: np.ascontiguousarray(a).ctypes.data_as(C.POINTER(t))
     rc = host.flux32_host(1, 0, P(mv[0], C.c_int), P(mv[1], C.c_float), P(mv[2], C.c_float), P(mv[3], C.c_int),
                           P(mv[4], C.c_float), P(mv[5], C.c_float), P(mv[6], C.c_float), 100, 2.0 ** 40, 0, 0, 48,
-                          48, F.ctypes.data_as(C.POINTER(C.c_longlong)), None)
+                          48, F.ctypes.data_as(C.POINTER(C.c_longlong)), None, 0)
     assert rc & 1

@@ -106,7 +106,9 @@ def test_fp32_push_current_conserves_charge_exactly(gpu_lib, order):
         oy = info["oy"] + (cj + a1.astype(np.float64)) * h[1]
         assert np.abs(ox - xo).max() < 1e-12 and np.abs(oy - yo).max() < 1e-12  # the start is the bunch as read
         q64 = q.astype(np.float64)
-        ref = sf.getCurrentDensityBase(comp, ox, oy, xn, yn, q64, org, h, dt, 0, 0, L0, L1, 2.0 ** 40)
+        jscale = 2.0 ** np.floor(np.log2(2.0 ** 62 / (4.0 * len(q64) * np.abs(q64).max() * 299792458.0
+                                                      / (h[0] * h[1]))))
+        ref = sf.getCurrentDensityBase(comp, ox, oy, xn, yn, q64, org, h, dt, 0, 0, L0, L1, jscale)
         assert np.abs(jwin - ref).max() <= 1e-6 * np.abs(ref).max()
         qs = 2.0 ** np.floor(np.log2(2.0 ** 62 / (4 * np.abs(q64).sum())))
         rho = sf.getChargeDensityDiff(ox, oy, xn, yn, q64, org, h, 0, 0, L0, L1, qs)
