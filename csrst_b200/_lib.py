@@ -89,6 +89,8 @@ def lib():
         "csrst_get_old_positions": ([P, D, D], C.c_int),
         "csrst_get_window": ([P, I, D, I], C.c_int),
         "csrst_get_window_field": ([P, C.c_int, D], C.c_int),
+        "csrst_set_pml": ([P, C.c_int, C.c_int, C.c_double], C.c_int),
+        "csrst_get_pml": ([P, I, I], C.c_int),
         "csrst_push": ([P, C.c_int], C.c_int),
         "csrst_drift": ([P, C.c_double], C.c_int),
         "csrst_half_h": ([P], C.c_int),

@@ -149,6 +149,12 @@ struct csrst_handle {
   double P0 = 0, P1 = 0;      // reference momentum
   double kh0 = 0, kh1 = 0;    // 0.5 c dt / h
   double *d64 = nullptr;      // 4 n doubles: the bunch in FP64 for diagnostics and reads
+  // absorbing layers at the open ends (csrst_set_pml), null when off
+  PmlCellT<double> *pml = nullptr;
+  PmlCellT<float> *pml32 = nullptr;
+  int npml = 0;
+  int2 *pml_rows = nullptr;
+  void *psi = nullptr;        // the layers' convolution state, 4 per cell, field type
 };
 
 // One part of a batch: its members' argument tables in device memory and the
@@ -247,6 +253,8 @@ FieldArgs field_args(csrst_handle *h, int comp) {
   a.mhx = -0.5 * (dt / (h0 * kMu0)); a.mhy = +0.5 * (dt / (h1 * kMu0));
   a.de = dt / kEps0;
   a.h0 = h0; a.h1 = h1;
+  a.pml = h->pml; a.npml = h->npml; a.pml_rows = h->pml_rows;
+  a.psi = static_cast<double *>(h->psi);
   return a;
 }
 
@@ -271,6 +279,8 @@ FieldArgsT<float> field_args32(csrst_handle *h, int comp) {
   a.chx = (float)d.chx; a.chy = (float)d.chy; a.kex = (float)d.kex; a.key = (float)d.key;
   a.dteps = (float)d.dteps; a.mhx = (float)d.mhx; a.mhy = (float)d.mhy; a.de = (float)d.de;
   a.h0 = (float)d.h0; a.h1 = (float)d.h1;
+  a.pml = h->pml32; a.npml = d.npml; a.pml_rows = d.pml_rows;
+  a.psi = static_cast<float *>(h->psi);
   return a;
 }
 
@@ -633,6 +643,7 @@ int csrst_destroy(csrst_handle *h) {
   cudaFree(h->Exf); cudaFree(h->Eyf); cudaFree(h->Hxf); cudaFree(h->Hyf);
   cudaFree(h->mask); cudaFree(h->cells); cudaFree(h->cutidx); cudaFree(h->ws);
   cudaFree(h->dscratch); cudaFree(h->dmean); cudaFree(h->dout);
+  cudaFree(h->pml); cudaFree(h->pml32); cudaFree(h->pml_rows); cudaFree(h->psi);
   if (h->s) cudaStreamDestroy(h->s);
   delete h;
   return CSRST_OK;
@@ -1652,6 +1663,142 @@ int csrst_ensemble_tune(csrst_ensemble *e, int steps, double *report, int max_ro
   if (nrows) *nrows = rows < max_rows ? rows : max_rows;
   if ((rc = ensemble_build(e))) return rc;
   return ensemble_release(e);
+}
+
+// ---- absorbing layers at the open ends ----
+
+}  // extern "C"
+
+namespace {
+
+// Conductivity of the absorbing layers of thickness W at the point (x, y),
+// split along the pipe axis into sx, sy: the layers at the entry plane x = 0
+// of the first straight section (axis +x) and at the end plane of the second
+// (the centreline's end: the arc of radius R and angle |phi| about the bend
+// centre of Bend::Init, then length_after along the outgoing axis).  Each
+// layer stops kPmlGap cells before its end plane: a slanted end wall is made
+// of conformal cut cells, and a strongly damped layer cell next to them made
+// the coupled update grow without bound, while a regular strip in between
+// keeps it stable.  sigma(depth) = smax (depth / W)^m.
+constexpr double kPmlGap = 2.0;
+void pml_sigma(const BendDev &b, double W, int m, double smax, double x, double y, double *sx, double *sy) {
+  *sx = 0.0; *sy = 0.0;
+  const double gap = kPmlGap * b.hr0;
+  const double din = x - gap;  // distance from the entry plane, past the gap
+  if (din >= 0.0 && din < W) *sx += smax * std::pow((W - din) / W, m);
+  const double ph = std::fabs(b.phi);
+  const double ry = 0.5 * b.w - b.cen1;  // bend entry relative to the centre: (0, ry), |ry| = R
+  const double sg = ry > 0.0 ? -1.0 : 1.0;
+  const double t0 = std::cos(ph), t1 = sg * std::sin(ph);
+  const double e0 = b.cen0 + b.R * std::sin(ph) + b.La * t0;
+  const double e1 = b.cen1 - sg * b.R * std::cos(ph) + b.La * t1;
+  const double dout = (e0 - x) * t0 + (e1 - y) * t1 - gap;  // from the end plane, past the gap
+  if (dout >= 0.0 && dout < W) {
+    const double v = smax * std::pow((W - dout) / W, m);
+    *sx += v * std::fabs(t0);
+    *sy += v * std::fabs(t1);
+  }
+}
+
+// The convolution's recursion over the update interval dt':
+// b = exp(-sigma dt'/eps0), a = b - 1.
+void pml_coef(double sigma, double dtp, double *b, double *a) {
+  if (!(sigma > 0.0)) { *b = 1.0; *a = 0.0; return; }
+  *b = std::exp(-sigma * dtp / kEps0);
+  *a = *b - 1.0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int csrst_set_pml(csrst_handle *h, int width, int order, double reflection) {
+  if (!h) return CSRST_E_ARG;
+  if (width < 0 || width > 1000 || order < 0 || order > 8 || (width > 0 && !(reflection > 0 && reflection < 1)))
+    return fail(h, CSRST_E_ARG, "absorbing layer: width 0..1000 cells, order 0..8, reflection in (0, 1)");
+  CK(cudaStreamSynchronize(h->s));
+  cudaFree(h->pml); cudaFree(h->pml32); cudaFree(h->pml_rows); cudaFree(h->psi);
+  h->pml = nullptr; h->pml32 = nullptr; h->pml_rows = nullptr; h->psi = nullptr; h->npml = 0;
+  if (h->graph) { cudaGraphExecDestroy(h->graph); h->graph = nullptr; }
+  if (width == 0) return CSRST_OK;
+  const int Nx = h->b.Nx, Ny = h->b.Ny;
+  std::vector<uint8_t> inside((size_t)Nx * Ny);
+  CK(cudaMemcpy(inside.data(), h->mask, inside.size(), cudaMemcpyDeviceToHost));
+  const FieldArgs f = field_args(h, 0);
+  const double h0 = h->b.hr0, h1 = h->b.hr1, o0 = h->b.org0, o1 = h->b.org1, dt = h->dt;
+  const double W = width * h0;
+  const double smax = -(order + 1) * kEps0 * kC * std::log(reflection) / (2.0 * W);
+  // per row: the regular sweep's columns [lo, hi); the cells outside them are the layer's
+  std::vector<int2> rows(Ny);
+  std::vector<PmlCellT<double>> cells;
+  for (int j = 0; j < Ny; ++j) {
+    int lo = 0, hi = Nx;
+    for (int i = 0; i < Nx; ++i) {
+      if (!inside[(size_t)j * Nx + i]) continue;
+      double sx, sy, tx, ty, ux, uy;
+      pml_sigma(h->b, W, order, smax, o0 + (i + 0.5) * h0, o1 + (j + 0.5) * h1, &sx, &sy);   // Hz
+      pml_sigma(h->b, W, order, smax, o0 + (i + 0.5) * h0, o1 + j * h1, &tx, &ty);           // Ex
+      pml_sigma(h->b, W, order, smax, o0 + i * h0, o1 + (j + 0.5) * h1, &ux, &uy);           // Ey
+      if (sx > 0 || sy > 0 || ty > 0 || ux > 0) {
+        if (i < Nx / 2) lo = std::max(lo, i + 1);
+        else hi = std::min(hi, i);
+      }
+    }
+    if (hi < lo) hi = lo;
+    rows[j] = make_int2(lo, hi);
+    for (int i = 0; i < Nx; ++i) {
+      if (!inside[(size_t)j * Nx + i] || (i >= lo && i < hi)) continue;
+      double sx, sy, tx, ty, ux, uy;
+      pml_sigma(h->b, W, order, smax, o0 + (i + 0.5) * h0, o1 + (j + 0.5) * h1, &sx, &sy);
+      pml_sigma(h->b, W, order, smax, o0 + (i + 0.5) * h0, o1 + j * h1, &tx, &ty);
+      pml_sigma(h->b, W, order, smax, o0 + i * h0, o1 + (j + 0.5) * h1, &ux, &uy);
+      PmlCellT<double> c{};
+      c.i = i; c.j = j;
+      pml_coef(sx, 0.5 * dt, &c.bhx, &c.ahx);
+      pml_coef(sy, 0.5 * dt, &c.bhy, &c.ahy);
+      pml_coef(ty, dt, &c.bex, &c.aex);
+      pml_coef(ux, dt, &c.bey, &c.aey);
+      cells.push_back(c);
+    }
+  }
+  std::vector<PmlCellT<float>> c32(cells.size());
+  for (size_t k = 0; k < cells.size(); ++k) {
+    const PmlCellT<double> &c = cells[k];
+    c32[k] = PmlCellT<float>{c.i, c.j, (float)c.bhx, (float)c.ahx, (float)c.bhy, (float)c.ahy,
+                             (float)c.bex, (float)c.aex, (float)c.bey, (float)c.aey};
+  }
+  h->npml = (int)cells.size();
+  CK(cudaMalloc(&h->pml_rows, rows.size() * sizeof(int2)));
+  CK(cudaMemcpy(h->pml_rows, rows.data(), rows.size() * sizeof(int2), cudaMemcpyHostToDevice));
+  if (h->npml > 0) {
+    CK(cudaMalloc(&h->pml, cells.size() * sizeof(PmlCellT<double>)));
+    CK(cudaMemcpy(h->pml, cells.data(), cells.size() * sizeof(PmlCellT<double>), cudaMemcpyHostToDevice));
+    CK(cudaMalloc(&h->pml32, c32.size() * sizeof(PmlCellT<float>)));
+    CK(cudaMemcpy(h->pml32, c32.data(), c32.size() * sizeof(PmlCellT<float>), cudaMemcpyHostToDevice));
+    const size_t pb = 4 * cells.size() * (h->fp32 ? sizeof(float) : sizeof(double));
+    CK(cudaMalloc(&h->psi, pb));
+    CK(cudaMemset(h->psi, 0, pb));
+  }
+  // a loaded window must not overlap a layer
+  if (h->win || h->winf) {
+    if (h->fp32) launch_check_window(field_args32(h, 0), h->s);
+    else launch_check_window(field_args(h, 0), h->s);
+    return check_err(h);
+  }
+  return CSRST_OK;
+}
+
+int csrst_get_pml(csrst_handle *h, int *ncells, int *rows2) {
+  if (!h || !ncells) return CSRST_E_ARG;
+  *ncells = h->npml;
+  if (rows2) {
+    if (h->pml_rows) {
+      CK(cudaMemcpy(rows2, h->pml_rows, (size_t)h->b.Ny * sizeof(int2), cudaMemcpyDeviceToHost));
+    } else {
+      for (int j = 0; j < h->b.Ny; ++j) { rows2[2 * j] = 0; rows2[2 * j + 1] = h->b.Nx; }
+    }
+  }
+  return CSRST_OK;
 }
 
 // ---- stand-alone ScatterGatherImpl / ShapeFunction entry points ----

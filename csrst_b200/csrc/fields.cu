@@ -48,16 +48,20 @@ __device__ __forceinline__ bool static_vec(const FieldArgsT<T> &a, int b, int &c
   return j < a.Ny;  // uniform over the warp
 }
 
-// Inside-mask bits of the cells i = c - 1 + e of row j that are on the mesh.
+// Inside-mask bits of the cells i = c - 1 + e of row j that are on the mesh
+// (and, with absorbing layers, outside them: those cells have their own
+// block range).
 template <class T>
 __device__ __forceinline__ unsigned static_mask(const FieldArgsT<T> &a, int c, int j) {
   constexpr int V = Vec16<T>::N;
   unsigned m = 0;
   const uint8_t *row = a.mask + (size_t)j * a.Nx;
+  int lo = 0, hi = a.Nx;
+  if (a.pml_rows) { const int2 r = a.pml_rows[j]; lo = r.x; hi = r.y; }
 #pragma unroll
   for (int e = 0; e < V; ++e) {
     const int i = c - 1 + e;
-    if (i >= 0 && i < a.Nx && row[i]) m |= 1u << e;
+    if (i >= lo && i < hi && row[i]) m |= 1u << e;
   }
   return m;
 }
@@ -119,8 +123,20 @@ __device__ __forceinline__ void half_h_body(const FieldArgsT<T> &a, int b) {
     const T u1 = a.mhy * (n0 * a.Ex.at(c.i, c.j + 1) - l0 * a.Ex.at(c.i, c.j)) / area;
     a.Hx.at(c.i, c.j) += u0;
     a.Hy.at(c.i, c.j) += u1;
-  } else {
+  } else if (b < a.nbS + a.nbC + a.nbP) {
     const int k = (b - a.nbS - a.nbC) * blockDim.x + threadIdx.x;
+    if (k >= a.npml) return;
+    const PmlCellT<T> c = a.pml[k];
+    T *ps = a.psi + 4 * (size_t)k;
+    const T dey = a.Ey.at(c.i + 1, c.j) - a.Ey.at(c.i, c.j);
+    const T dex = a.Ex.at(c.i, c.j + 1) - a.Ex.at(c.i, c.j);
+    const T p0 = c.bhx * ps[0] + c.ahx * dey, p1 = c.bhy * ps[1] + c.ahy * dex;
+    ps[0] = p0; ps[1] = p1;
+    T &hx = a.Hx.at(c.i, c.j), &hy = a.Hy.at(c.i, c.j);
+    hx = hx - a.chx * (dey + p0);
+    hy = hy + a.chy * (dex + p1);
+  } else {
+    const int k = (b - a.nbS - a.nbC - a.nbP) * blockDim.x + threadIdx.x;
     if (k >= a.L0 * a.L1) return;
     const int i = k % a.L0, j = k / a.L0;
     T &hx = a.mHx.at(i, j), &hy = a.mHy.at(i, j);
@@ -199,8 +215,26 @@ __device__ __forceinline__ void update_e_body(const FieldArgsT<T> &a, int b, T z
       const T u1 = -(a.Hy.at(c.i, c.j) - a.Hy.at(c.i - 1, c.j)) / a.h0;
       a.Ey.at(c.i, c.j) += a.de * (u0 + u1 - zeroJ);
     }
-  } else {
+  } else if (b < a.nbS + a.nbC + a.nbP) {
     const int k = (b - a.nbS - a.nbC) * blockDim.x + threadIdx.x;
+    if (k >= a.npml) return;
+    const PmlCellT<T> c = a.pml[k];
+    T &ps = a.psi[4 * (size_t)k + 2 + COMP];
+    if (COMP == 0) {
+      const T dh = a.Hx.at(c.i, c.j) - a.Hx.at(c.i, c.j - 1) + a.Hy.at(c.i, c.j) - a.Hy.at(c.i, c.j - 1);
+      const T p = c.bex * ps + c.aex * dh;
+      ps = p;
+      T &e = a.Ex.at(c.i, c.j);
+      e = e + (a.kex * (dh + p) - a.dteps * zeroJ);
+    } else {
+      const T dh = a.Hx.at(c.i, c.j) - a.Hx.at(c.i - 1, c.j) + a.Hy.at(c.i, c.j) - a.Hy.at(c.i - 1, c.j);
+      const T p = c.bey * ps + c.aey * dh;
+      ps = p;
+      T &e = a.Ey.at(c.i, c.j);
+      e = e - (a.key * (dh + p) + a.dteps * zeroJ);
+    }
+  } else {
+    const int k = (b - a.nbS - a.nbC - a.nbP) * blockDim.x + threadIdx.x;
     if (k >= a.L0 * a.L1) return;
     const int i = k % a.L0, j = k / a.L0;
     const T J = (T)((double)(long long)a.acc[k] * a.acc_inv);
@@ -286,7 +320,7 @@ __global__ void k_copy_to_window(FieldArgsT<T> a) {
 
 // Set err if the window or its one-cell ring touches a cell that is not a
 // regular inside cell: the fused sub-step launches assume the strip exchange
-// and the cut-cell corrections never meet.
+// and the cut-cell (or absorbing-layer) updates never meet.
 template <class T>
 __device__ void check_window_clear(const FieldArgsT<T> &a, WinState *ws) {
   const int P0 = ws->P0, P1 = ws->P1;
@@ -298,7 +332,8 @@ __device__ void check_window_clear(const FieldArgsT<T> &a, WinState *ws) {
     else if (k < 2 * (a.L0 + 2) + a.L1) { i = -1; j = k - 2 * (a.L0 + 2); }
     else { i = a.L0; j = k - 2 * (a.L0 + 2) - a.L1; }
     const int si = i + P0, sj = j + P1;
-    if (si < 0 || sj < 0 || si >= a.Nx || sj >= a.Ny || !a.mask[(size_t)sj * a.Nx + si])
+    if (si < 0 || sj < 0 || si >= a.Nx || sj >= a.Ny || !a.mask[(size_t)sj * a.Nx + si] ||
+        (a.pml_rows && (si < a.pml_rows[sj].x || si >= a.pml_rows[sj].y)))  // or an absorbing-layer cell
       set_err(ws, kErrWindowWall);
   }
 }
@@ -550,8 +585,9 @@ int sub_grid(FieldArgsT<T> &a) {
   a.tilesX = (a.Nx + 2 + a.tx * (16 / (int)sizeof(T)) - 1) / (a.tx * (16 / (int)sizeof(T)));
   a.nbS = a.tilesX * ((a.Ny + a.ty - 1) / a.ty);
   a.nbC = (a.ncells + 255) / 256;
+  a.nbP = a.pml ? (a.npml + 255) / 256 : 0;
   const int nbM = (a.L0 * a.L1 + 255) / 256;
-  return a.nbS + a.nbC + nbM;
+  return a.nbS + a.nbC + a.nbP + nbM;
 }
 
 template <class T>

@@ -26,6 +26,20 @@ struct PushArgs {
   double bz, Lb, hw, chh, shh, bwidth;
 };
 
+// One cell of the absorbing layer at an open end of the pipe (convolutional
+// PML with kappa = 1, csrst_set_pml): each component's curl difference d is
+// replaced by d + psi, with psi <- b psi + a d updated first, b = exp(-sigma
+// dt'/eps0), a = b - 1 over the component's update interval dt' (dt/2 for the
+// half H updates, dt for E).  sigma is the layer's conductivity split along
+// the pipe axis: sigma_x for Hzx and Ey, sigma_y for Hzy and Ex, each at its
+// component's position.  psi lives in its own array, 4 per cell.
+template <class T>
+struct PmlCellT {
+  int i, j;
+  T bhx, ahx, bhy, ahy;  // Hzx, Hzy (half step)
+  T bex, aex, bey, aey;  // Ex, Ey
+};
+
 // One field sub-step over the static mesh, the cut cells and the window.
 // T is the field type: double on the FP64 path, float in FP32 mode.
 template <class T>
@@ -50,6 +64,12 @@ struct FieldArgsT {
   T h0, h1;
   int nbS, nbC, tilesX;            // block ranges: static tiles, cut-cell blocks
   int tx, ty;                      // static-sweep tile (tx * ty = 256; 0 = 32 x 8)
+  // absorbing layers (csrst_set_pml; null when off): the cells, and per row
+  // the columns [lo, hi) left to the regular sweep
+  const PmlCellT<T> *pml;
+  T *psi;                          // 4 per layer cell: Hzx, Hzy, Ex, Ey
+  int npml, nbP;
+  const int2 *pml_rows;
 };
 using FieldArgs = FieldArgsT<double>;
 

@@ -95,6 +95,19 @@ class Simulation:
     def reset_outside(self):
         self._ck(lib().csrst_reset_outside(self.h))
 
+    def set_pml(self, width=10, order=4, reflection=float(np.exp(-16.0))):
+        """Absorbing layers at the pipe's open ends (csrst_set_pml; the
+        reference's PML_WIDTH, PML_ORD, PML_RED by default); width 0 = off,
+        the reference's PEC ends."""
+        self._ck(lib().csrst_set_pml(self.h, int(width), int(order), float(reflection)))
+
+    def pml(self):
+        """(number of layer cells, per row the regular sweep's columns [lo, hi))."""
+        n = C.c_int()
+        rows = np.zeros(2 * self.Ny, np.int32)
+        self._ck(lib().csrst_get_pml(self.h, C.byref(n), rows.ctypes.data_as(C.POINTER(C.c_int))))
+        return n.value, rows.reshape(self.Ny, 2)
+
     def load(self, x, y, px, py, q):
         a = list(map(f64, (x, y, px, py, q)))
         self.n = len(a[0])

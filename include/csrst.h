@@ -119,6 +119,30 @@ int csrst_get_window(csrst_handle *h, int *w4, double *origin2, int *gb4);
 /* which: 0 Ex, 1 Ey, 2 Hzx, 3 Hzy, 4 Jx, 5 Jy of the window, incl. guards. */
 int csrst_get_window_field(csrst_handle *h, int which, double *out);
 
+/* Absorbing layers at the two open ends of the pipe.  The reference computes
+ * PML conductivities in Bend::calculatePMLCoefficients (Bend.cpp:355-425)
+ * but zeroes them in TETMSolver::initMaps (TETMSolver.cpp:59-63) and never
+ * uses them: its domain ends are PEC walls.  Off by default here too, so
+ * that the loop matches the reference; csrst_set_pml turns on a
+ * convolutional PML (kappa = 1) over `width` cells before the entry plane of
+ * the first straight section and the end plane of the second, each layer
+ * ending 2 cells before its end wall (conformal cut cells of a slanted wall
+ * next to a strongly damped cell made the update unstable).  Graded
+ * sigma = smax (depth / width)^order along the pipe axis, split into its x
+ * and y parts, with smax = -(order + 1) eps0 c ln(reflection) / (2 width hx)
+ * (the reflection of a normally incident plane wave in the continuum).  The
+ * reference's defaults are width 10, order 4, reflection exp(-16)
+ * (Bend.cpp:28-32).  width 0 turns the layers off.  Inside cells only (the
+ * cut cells at the pipe walls keep their conformal update); a window that
+ * touches a layer is an error (CSRST_E_WINDOW_WALL).  Call it before
+ * stepping (it drops the captured step) and before creating an ensemble of
+ * the handle; the layers' convolution state starts at zero and is not part
+ * of a checkpoint (call it again after a restart). */
+int csrst_set_pml(csrst_handle *h, int width, int order, double reflection);
+/* Number of layer cells, and per static-mesh row the columns [lo, hi) that
+ * the regular update keeps (rows2: 2 * Ny ints, may be NULL). */
+int csrst_get_pml(csrst_handle *h, int *ncells, int *rows2);
+
 /* PartBunch::push_particles(mmE, mmH, mmJ, dt, Jcomp) (PartBunch.cpp:215-519). */
 int csrst_push(csrst_handle *h, int jcomp);
 /* PartBunch::drift_particles(dt) (PartBunch.cpp:179-187). */

@@ -753,6 +753,14 @@ struct Sim {
   bool fixed = false;                    // fixed-point deposit mode
   double fscale = 0;
   int err = 0;
+  // absorbing layers at the open ends (no reference counterpart in use:
+  // Bend::calculatePMLCoefficients is zeroed by TETMSolver::initMaps)
+  // convolutional PML (kappa = 1): psi <- b psi + a (curl difference), the
+  // difference used in the update is (curl difference + psi)
+  struct Pml { int i, j; double bhx, ahx, bhy, ahy, bex, aex, bey, aey; };
+  std::vector<Pml> pml;
+  std::vector<double> psi;  // 4 per layer cell: Hzx, Hzy, Ex, Ey
+  std::vector<int> plo, phi;  // per row: columns [lo, hi) of the regular update
 };
 
 // PartBunch::getLocalPDomain / getLocalPDomainInclOld relative to the window origin.
@@ -953,6 +961,41 @@ void exchange(Sim &s, int which) {
   }
 }
 
+// Convolutional PML (kappa = 1) of thickness W at the two open ends of the
+// pipe, restated independently of the GPU library: the entry plane x = 0
+// (axis +x) and the end plane of the second straight section (the
+// centreline's end after the arc of radius R and angle |phi| about the bend
+// centre and length_after along the outgoing axis).  Each layer stops kPmlGap
+// cells before its end plane, so that no layer cell neighbours the conformal
+// cut cells of a slanted end wall.  sigma(depth) = smax (depth / W)^m, split
+// along the axis into sx, sy.
+constexpr double kPmlGap = 2.0;
+void pml_sigma(const Bend &b, double W, int m, double smax, double x, double y, double &sx, double &sy) {
+  sx = 0.0; sy = 0.0;
+  const double gap = kPmlGap * b.hr0;
+  const double sin_ = x - gap;  // distance from the entry plane, past the gap
+  if (sin_ >= 0.0 && sin_ < W) sx += smax * std::pow((W - sin_) / W, m);
+  const double ph = std::fabs(b.phi);
+  const double ry = 0.5 * b.w - b.cen1;
+  const double sg = ry > 0.0 ? -1.0 : 1.0;
+  const double t0 = std::cos(ph), t1 = sg * std::sin(ph);
+  const double e0 = b.cen0 + b.R * std::sin(ph) + b.La * t0;
+  const double e1 = b.cen1 - sg * b.R * std::cos(ph) + b.La * t1;
+  const double sout = (e0 - x) * t0 + (e1 - y) * t1 - gap;
+  if (sout >= 0.0 && sout < W) {
+    const double v = smax * std::pow((W - sout) / W, m);
+    sx += v * std::fabs(t0);
+    sy += v * std::fabs(t1);
+  }
+}
+
+// CPML recursion over the update interval dt': b = exp(-sigma dt'/eps0), a = b - 1
+void pml_coef(double sigma, double dtp, double &b, double &a) {
+  if (!(sigma > 0.0)) { b = 1.0; a = 0.0; return; }
+  b = std::exp(-sigma * dtp / EPS0);
+  a = b - 1.0;
+}
+
 // Static + window H half update (TETMSolver.hh:142-149) followed by the
 // exchange and the cut-cell correction (:154-163).
 void half_h(Sim &s) {
@@ -961,12 +1004,24 @@ void half_h(Sim &s) {
   const double Z0 = std::sqrt(MU0 / EPS0);
   const double cx = 0.5 * etax / Z0, cy = 0.5 * etay / Z0;
   const int Nx = s.b.Nx, Ny = s.b.Ny;
+  const bool layers = !s.plo.empty();
   for (int j = 0; j < Ny; ++j)
     for (int i = 0; i < Nx; ++i) {
       if (!s.inside[(size_t)j * Nx + i]) continue;
+      if (layers && (i < s.plo[j] || i >= s.phi[j])) continue;
       s.Hx.at(i, j) = s.Hx.at(i, j) - cx * (s.Ey.at(i + 1, j) - s.Ey.at(i, j));
       s.Hy.at(i, j) = s.Hy.at(i, j) + cy * (s.Ex.at(i, j + 1) - s.Ex.at(i, j));
     }
+  for (size_t k = 0; k < s.pml.size(); ++k) {
+    const Sim::Pml &c = s.pml[k];
+    double *ps = &s.psi[4 * k];
+    const double dey = s.Ey.at(c.i + 1, c.j) - s.Ey.at(c.i, c.j);
+    const double dex = s.Ex.at(c.i, c.j + 1) - s.Ex.at(c.i, c.j);
+    ps[0] = c.bhx * ps[0] + c.ahx * dey;
+    ps[1] = c.bhy * ps[1] + c.ahy * dex;
+    s.Hx.at(c.i, c.j) = s.Hx.at(c.i, c.j) - cx * (dey + ps[0]);
+    s.Hy.at(c.i, c.j) = s.Hy.at(c.i, c.j) + cy * (dex + ps[1]);
+  }
   for (int j = 0; j < s.L1; ++j)
     for (int i = 0; i < s.L0; ++i) {
       s.mHx.at(i, j) = s.mHx.at(i, j) - cx * (s.mEy.at(i + 1, j) - s.mEy.at(i, j));
@@ -996,8 +1051,16 @@ void update_e(Sim &s, int comp) {
     for (int j = 0; j < Ny; ++j)
       for (int i = 0; i < Nx; ++i) {
         if (!s.inside[(size_t)j * Nx + i]) continue;
+        if (!s.plo.empty() && (i < s.plo[j] || i >= s.phi[j])) continue;
         s.Ex.at(i, j) = s.Ex.at(i, j) + (k * (s.Hx.at(i, j) - s.Hx.at(i, j - 1) + s.Hy.at(i, j) - s.Hy.at(i, j - 1)) - dteps * zeroJ);
       }
+    for (size_t q = 0; q < s.pml.size(); ++q) {
+      const Sim::Pml &c = s.pml[q];
+      double &ps = s.psi[4 * q + 2];
+      const double dh = s.Hx.at(c.i, c.j) - s.Hx.at(c.i, c.j - 1) + s.Hy.at(c.i, c.j) - s.Hy.at(c.i, c.j - 1);
+      ps = c.bex * ps + c.aex * dh;
+      s.Ex.at(c.i, c.j) = s.Ex.at(c.i, c.j) + (k * (dh + ps) - dteps * zeroJ);
+    }
     for (int j = 0; j < s.L1; ++j)
       for (int i = 0; i < s.L0; ++i)
         s.mEx.at(i, j) = s.mEx.at(i, j) + (k * (s.mHx.at(i, j) - s.mHx.at(i, j - 1) + s.mHy.at(i, j) - s.mHy.at(i, j - 1)) - dteps * s.mJx.at(i, j));
@@ -1016,8 +1079,16 @@ void update_e(Sim &s, int comp) {
     for (int j = 0; j < Ny; ++j)
       for (int i = 0; i < Nx; ++i) {
         if (!s.inside[(size_t)j * Nx + i]) continue;
+        if (!s.plo.empty() && (i < s.plo[j] || i >= s.phi[j])) continue;
         s.Ey.at(i, j) = s.Ey.at(i, j) - (k * (s.Hx.at(i, j) - s.Hx.at(i - 1, j) + s.Hy.at(i, j) - s.Hy.at(i - 1, j)) + dteps * zeroJ);
       }
+    for (size_t q = 0; q < s.pml.size(); ++q) {
+      const Sim::Pml &c = s.pml[q];
+      double &ps = s.psi[4 * q + 3];
+      const double dh = s.Hx.at(c.i, c.j) - s.Hx.at(c.i - 1, c.j) + s.Hy.at(c.i, c.j) - s.Hy.at(c.i - 1, c.j);
+      ps = c.bey * ps + c.aey * dh;
+      s.Ey.at(c.i, c.j) = s.Ey.at(c.i, c.j) - (k * (dh + ps) + dteps * zeroJ);
+    }
     for (int j = 0; j < s.L1; ++j)
       for (int i = 0; i < s.L0; ++i)
         s.mEy.at(i, j) = s.mEy.at(i, j) - (k * (s.mHx.at(i, j) - s.mHx.at(i - 1, j) + s.mHy.at(i, j) - s.mHy.at(i - 1, j)) + dteps * s.mJy.at(i, j));
@@ -1626,6 +1697,51 @@ void orc_get_window_field(void *h, int which, double *out) {
 void orc_push(void *h, int jcomp) { push(*(Sim *)h, jcomp); }
 void orc_drift(void *h, double dt) { drift(*(Sim *)h, dt); }
 void orc_half_h(void *h) { half_h(*(Sim *)h); }
+// Absorbing layers (width cells, grading order, normal-incidence reflection); width 0 = off.
+void orc_set_pml(void *h, int width, int order, double reflection) {
+  Sim &s = *(Sim *)h;
+  s.pml.clear(); s.plo.clear(); s.phi.clear(); s.psi.clear();
+  if (width <= 0) return;
+  const int Nx = s.b.Nx, Ny = s.b.Ny;
+  const double h0 = s.b.hr0, h1 = s.b.hr1, o0 = s.b.org0, o1 = s.b.org1, dt = s.dt;
+  const double W = width * h0;
+  const double smax = -(order + 1) * EPS0 * C * std::log(reflection) / (2.0 * W);
+  s.plo.assign(Ny, 0);
+  s.phi.assign(Ny, Nx);
+  for (int j = 0; j < Ny; ++j) {
+    auto sig = [&](int i, double &sx, double &sy, double &tx, double &ty, double &ux, double &uy) {
+      pml_sigma(s.b, W, order, smax, o0 + (i + 0.5) * h0, o1 + (j + 0.5) * h1, sx, sy);
+      pml_sigma(s.b, W, order, smax, o0 + (i + 0.5) * h0, o1 + j * h1, tx, ty);
+      pml_sigma(s.b, W, order, smax, o0 + i * h0, o1 + (j + 0.5) * h1, ux, uy);
+    };
+    int lo = 0, hi = Nx;
+    for (int i = 0; i < Nx; ++i) {
+      if (!s.inside[(size_t)j * Nx + i]) continue;
+      double sx, sy, tx, ty, ux, uy;
+      sig(i, sx, sy, tx, ty, ux, uy);
+      if (sx > 0 || sy > 0 || ty > 0 || ux > 0) {
+        if (i < Nx / 2) lo = std::max(lo, i + 1);
+        else hi = std::min(hi, i);
+      }
+    }
+    if (hi < lo) hi = lo;
+    s.plo[j] = lo; s.phi[j] = hi;
+    for (int i = 0; i < Nx; ++i) {
+      if (!s.inside[(size_t)j * Nx + i] || (i >= lo && i < hi)) continue;
+      double sx, sy, tx, ty, ux, uy;
+      sig(i, sx, sy, tx, ty, ux, uy);
+      Sim::Pml c{};
+      c.i = i; c.j = j;
+      pml_coef(sx, 0.5 * dt, c.bhx, c.ahx);
+      pml_coef(sy, 0.5 * dt, c.bhy, c.ahy);
+      pml_coef(ty, dt, c.bex, c.aex);
+      pml_coef(ux, dt, c.bey, c.aey);
+      s.pml.push_back(c);
+    }
+  }
+  s.psi.assign(4 * s.pml.size(), 0.0);
+}
+int orc_pml_cells(void *h) { return (int)((Sim *)h)->pml.size(); }
 void orc_update_e(void *h, int comp) { update_e(*(Sim *)h, comp); }
 int orc_move(void *h) { return move_window(*(Sim *)h); }
 

@@ -66,6 +66,8 @@ def lib():
         L.orc_push.argtypes = [C.c_void_p, C.c_int]
         L.orc_drift.argtypes = [C.c_void_p, C.c_double]
         L.orc_half_h.argtypes = [C.c_void_p]
+        L.orc_set_pml.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_double]
+        L.orc_pml_cells.argtypes = [C.c_void_p]
         L.orc_update_e.argtypes = [C.c_void_p, C.c_int]
         L.orc_move.argtypes = [C.c_void_p]
         L.orc_step.argtypes = [C.c_void_p, C.c_int]
@@ -217,6 +219,12 @@ class Sim:
 
     def drift(self, dt):
         lib().orc_drift(self.h, dt)
+
+    def set_pml(self, width=10, order=4, reflection=float(np.exp(-16.0))):
+        lib().orc_set_pml(self.h, int(width), int(order), float(reflection))
+
+    def pml_cells(self):
+        return int(lib().orc_pml_cells(self.h))
 
     def half_h(self):
         lib().orc_half_h(self.h)
