@@ -100,14 +100,39 @@ def peaks(bf16=False):
     return 6650.0, "fallback"
 
 
-def profile_traffic(key):
-    """Per-step DRAM bytes of a kernel group from the committed ncu summary
-    (profiles/*.md lines 'traffic[<key>] = <bytes>'), or None."""
-    for f in sorted((ROOT / "profiles").glob("*.md")):
-        m = re.search(r"traffic\[" + re.escape(key) + r"\]\s*=\s*([0-9.eE+]+)", f.read_text())
-        if m:
-            return float(m.group(1))
-    return None
+# The launches of one time step per kernel group (order 1 = TSC), as the
+# profile launch lists name them.
+STEP_LAUNCHES = {
+    ("push", "fp32", 1): {"k_push32<1, 0>": 1, "k_push32<1, 1>": 1, "k_prep32": 2, "k_post32": 2, "k_bounds32": 2},
+    ("yee", "fp32", 1): {"k_half_h<float>": 2, "k_update_e<float, 0>": 1, "k_update_e<float, 1>": 1,
+                         "k_exchange<float>": 4},
+    ("push", "fp64", 1): {"k_push<1>": 2, "k_push_prep": 2, "k_push_post": 2, "k_global_bounds": 2},
+    ("yee", "fp64", 1): {"k_half_h<double>": 2, "k_update_e<double, 0>": 1, "k_update_e<double, 1>": 1,
+                         "k_exchange<double>": 4},
+}
+LAUNCH_LISTS = {"fp32": "profiles/c2_tsc_fp32_step_launches.txt", "fp64": "profiles/c2_tsc_fp64_step_launches.txt"}
+
+
+def profile_traffic(group, prec, order):
+    """Per-step DRAM bytes (read + write) of a kernel group from the committed
+    ncu launch list of the c2 workload (LAUNCH_LISTS: one row per kernel with
+    its DRAM MB per launch), summed over the step's launches of that group.
+    None when the list is missing or does not name every kernel the step
+    launches (e.g. after a kernel was replaced), so the figure never outlives
+    the kernels it was measured on.  Returns (bytes, source file)."""
+    want = STEP_LAUNCHES.get((group, prec, order))
+    f = ROOT / LAUNCH_LISTS[prec]
+    if not want or not f.exists():
+        return None, None
+    rows = {}
+    for line in f.read_text().splitlines():
+        if line.startswith("#") or "|" not in line:
+            continue
+        c = [v.strip() for v in line.split("|")]
+        rows[c[0]] = (float(c[5]) + float(c[6])) * 1e6
+    if any(k not in rows for k in want):
+        return None, None
+    return sum(n * rows[k] for k, n in want.items()), LAUNCH_LISTS[prec]
 
 
 class Clocks:
@@ -288,6 +313,9 @@ def accuracy(cfg, spec, bunch, steps=50):
     de64, de32 = slice_energy_change(bcfg, bspec, make_bunch(bspec), 300)
     slice_err = float(np.abs(de32 - de64).max() / np.abs(de64).max())
     exact, cont = continuity32(sims[True], ShapeFunction(cfg.shape_order))
+    # through the dipole: the c1 geometry from the dipole entrance, 2000 steps
+    from csrst_b200.compare import fp32_vs_fp64
+    dip = fp32_vs_fp64("c1-bend", 2000, every=100)
     for v in sims.values():
         v.close()
     return {"steps": steps, "wake_rel_err": float("%.3g" % wake_err),
@@ -297,6 +325,12 @@ def accuracy(cfg, spec, bunch, steps=50):
                                         "fp64_mev": [float("%.4g" % v) for v in de64]},
             "continuity_residual_rel": float("%.3g" % cont),
             "continuity_integer_residual": exact,
+            "through_dipole": {"case": "c1 geometry (2048x512, 10 um, R = 1 m, 2e5 particles, CIC), bunch from the "
+                                       "dipole entrance, 2000 steps, wake sampled every 100 steps",
+                               "wake_rel_err": float("%.3g" % dip["wake_rel_err"]),
+                               "integrated_wake_rel_err": float("%.3g" % dip["integrated_rel_err"]),
+                               "energy_change_per_slice_rel_err": float("%.3g" % dip["slice_rel_err"]),
+                               "fp64_slice_mev": [float("%.4g" % v) for v in dip["slice_mev_fp64"]]},
             "bar": "wake <= 1e-3 of the FP64 path's maximum; continuity <= 1e-10 (FP64 check against the FP64 "
                    "charge shape); the integer residual against the charge the deposit assigns is exactly 0"}
 
@@ -574,9 +608,10 @@ def run_b200(args, world, rank, local):
 
     def roof(key, prec, bytes_step, ms_):
         ach = bytes_step / (ms_ * 1e-3) / 1e9
-        tr = profile_traffic(f"{key},{args.workload},{prec}")
+        tr, tsrc = profile_traffic(key, prec, cfg.shape_order) if args.workload == "c2" else (None, None)
         return {"kernel": key, "bound": "hbm", "achieved": round(ach, 1), "peak": hbm, "unit": "GB/s",
-                "frac": round(ach / hbm, 4), "traffic": tr, "peak_source": f"{src} hbm_gbs",
+                "frac": round(ach / hbm, 4), "traffic": tr, "traffic_source": tsrc,
+                "peak_source": f"{src} hbm_gbs",
                 "algorithmic_bytes_per_step": bytes_step, "ms_per_step": round(ms_, 4)}
 
     def summary(prec):

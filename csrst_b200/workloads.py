@@ -100,11 +100,14 @@ def make_bunch(spec: BunchSpec):
 # the "small" ones are the same physics on meshes the CPU oracle runs in
 # seconds.
 def workload(name):
-    if name == "c1":      # 2048 x 512, h = 10 um, R = 1 m, 5 mm pipe, CIC, CFL 0.5, 2e5 particles
+    if name in ("c1", "c1-bend"):  # 2048 x 512, h = 10 um, R = 1 m, 5 mm pipe, CIC, CFL 0.5, 2e5 particles
+        # "-bend": the bunch starts at the dipole entrance (6 sigma_s into the
+        # arc), so that its steps run through the dipole
         h = 10e-6
         cfg = bend_config(2048, 512, h, 1.0, 5e-3, 1000.0, shape_order=0, cfl=0.5)
+        x0 = cfg.length_before + 6 * 50e-6 if name == "c1-bend" else 50 * h + 6 * 50e-6
         spec = BunchSpec(n=200_000, gamma=1000.0, sigma_s=50e-6, sigma_x=20e-6,
-                         energy_spread=1e-4, charge=-1e-9, x0=50 * h + 6 * 50e-6,
+                         energy_spread=1e-4, charge=-1e-9, x0=x0,
                          y0=0.5 * 5e-3, seed=11)
     elif name == "c2":    # 8192 x 1024, h = 5 um, TSC, 4e6 particles
         h = 5e-6

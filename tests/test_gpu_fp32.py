@@ -182,3 +182,19 @@ def test_fp32_energy_change_per_slice_in_the_dipole(gpu_lib):
     e32 = np.bincount(idx, dg[True], minlength=16) / cnt
     assert np.abs(e64).max() > 0
     assert np.abs(e32 - e64).max() <= 1e-3 * np.abs(e64).max()
+
+
+def test_fp32_csr_wake_through_the_dipole_c1(gpu_lib):
+    """The c1 geometry (2048 x 512 at 10 um, R = 1 m, 5 mm pipe, 2e5
+    particles, CIC) with the bunch starting at the dipole entrance, 2000 steps
+    (1000 cells of the 1440-cell arc): FP32 mode's wake on the bunch axis, its
+    time integral (the reference's energy change, sampled every 100 steps)
+    and the energy change of 16 slices stay within 1e-3 of the FP64 path's
+    maxima."""
+    from csrst_b200.compare import fp32_vs_fp64
+    r = fp32_vs_fp64("c1-bend", 2000, every=100)
+    assert r["wake_samples"] > 50 and r["integrated_columns"] > 50
+    assert r["wake_rel_err"] <= WAKE_TOL, r
+    assert r["integrated_rel_err"] <= WAKE_TOL, r
+    assert r["slice_rel_err"] <= 1e-3, r
+    assert max(abs(v) for v in r["slice_mev_fp64"]) > 0
