@@ -1418,6 +1418,14 @@ struct orc_config {
 };
 
 float orc_q_rsqrt(float x) { return q_rsqrt(x); }
+// The crossing split of one move (cell borders, or dual-cell borders when dual != 0).
+long orc_crossings(int dual, double o0, double o1, double n0, double n1, double h0, double h1, double org0,
+                   double org1, double *frac, double *s0, double *s1) {
+  Xing xs[32];
+  const size_t n = border_crossings(xs, o0, o1, n0, n1, h0, h1, org0, org1, dual != 0);
+  for (size_t k = 0; k < n; ++k) { frac[k] = xs[k].fraction; s0[k] = xs[k].s0; s1[k] = xs[k].s1; }
+  return (long)n;
+}
 
 // Bend setup: writes hr0, hr1, origin0, origin1, center0, center1, R, phi.
 void orc_bend(int Nx, int Ny, double Lb, double La, double w, double phi_deg, double ekin,

@@ -40,6 +40,8 @@ def lib():
         L.orc_q_rsqrt.restype = C.c_float
         L.orc_q_rsqrt.argtypes = [C.c_float]
         L.orc_bend.argtypes = [C.c_int, C.c_int] + [C.c_double] * 6 + [D]
+        L.orc_crossings.restype = C.c_long
+        L.orc_crossings.argtypes = [C.c_int] + [C.c_double] * 8 + [D, D, D]
         L.orc_geometry.restype = C.c_long
         L.orc_geometry.argtypes = [C.c_int, C.c_int] + [C.c_double] * 6 + [U8, D, C.c_long]
         L.orc_gather.argtypes = [C.c_int, C.c_int, D, C.c_int, C.c_int] + [C.c_double] * 4 + [D, D, C.c_long, D]
@@ -90,6 +92,14 @@ def f64(a):
 
 def q_rsqrt(x):
     return lib().orc_q_rsqrt(float(x))
+
+
+def crossings(dual, old, new, spacing, origin):
+    """(fractions, points[n][2]) of the crossing split of one move."""
+    fr, s0, s1 = np.zeros(32), np.zeros(32), np.zeros(32)
+    n = lib().orc_crossings(1 if dual else 0, old[0], old[1], new[0], new[1], spacing[0], spacing[1], origin[0],
+                            origin[1], _p(fr), _p(s0), _p(s1))
+    return fr[:n], np.stack([s0[:n], s1[:n]], axis=1)
 
 
 def bend(Nx, Ny, Lb, La, w, phi_deg, ekin, bz):

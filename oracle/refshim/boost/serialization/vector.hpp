@@ -1,0 +1,3 @@
+// FieldPatch.hh's serialisation is not used in one process.
+#pragma once
+namespace boost { namespace serialization { class access; } }
