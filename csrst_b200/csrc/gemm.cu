@@ -16,8 +16,11 @@
 //     affine index maps (transposed and mode-major layouts come out
 //     directly), each swept in the order - along rows or along columns -
 //     that puts a warp's stores next to each other under its map.
-// Waits on mbarriers are bounded; a wait that gives up sets *err, skips the
-// epilogue and still frees the TMEM.
+// Waits on mbarriers are bounded (a launch parameter, csrst_gemm_set_wait_limit):
+// a wait that gives up sets *err and skips the epilogue; the kernel then waits,
+// with the default bound, for the tensor-core work it has issued and for its
+// copies in flight before it frees the TMEM and returns, so that nothing
+// still writes into TMEM or shared memory it no longer owns.
 #include <cuda_bf16.h>
 #include <stdint.h>
 
@@ -27,7 +30,7 @@ namespace csrst {
 namespace {
 
 constexpr int kBM = 128, kBK = 64, kThreads = 128;
-constexpr long long kSpin = 1ll << 24;  // mbarrier polls before a wait gives up
+constexpr long long kSpin = 1ll << 24;  // default mbarrier polls before a wait gives up
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
   return (uint32_t)__cvta_generic_to_shared(p);
@@ -50,8 +53,8 @@ __device__ __forceinline__ bool mbar_try(uint64_t *bar, uint32_t parity) {
 }
 
 // Bounded wait for completion `parity` of an mbarrier.
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
-  for (long long k = 0; k < kSpin; ++k)
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, long long spin) {
+  for (long long k = 0; k < spin; ++k)
     if (mbar_try(bar, parity)) return true;
   return false;
 }
@@ -163,11 +166,11 @@ struct Seg {
 
 template <int BN>
 __global__ void __launch_bounds__(kThreads) k_gemm(Seg g0, Seg g1, int M, int N, csrst_gemm_epilogue ep, int *err,
-                                                   int o_mfast, int t_mfast) {
+                                                   int o_mfast, int t_mfast, long long spin) {
   extern __shared__ __align__(1024) uint8_t smem[];
   __shared__ uint64_t bar[2];
   __shared__ uint32_t tmem_base;
-  __shared__ int s_fail;
+  __shared__ int s_fail, s_last;  // a wait gave up; the last MMA commit issued
   constexpr int kA = kBM * kBK * 2, kB = BN * kBK * 2, kStage = kA + kB;
   uint8_t *base = smem + ((1024 - (smem_u32(smem) & 1023)) & 1023);
   const int z = blockIdx.z, m0 = blockIdx.y * kBM, n0 = blockIdx.x * BN;
@@ -196,6 +199,7 @@ __global__ void __launch_bounds__(kThreads) k_gemm(Seg g0, Seg g1, int M, int N,
     mbar_init(&bar[1], 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     s_fail = 0;
+    s_last = -1;
   }
   asm volatile("tcgen05.fence::before_thread_sync;");
   __syncthreads();
@@ -210,7 +214,7 @@ __global__ void __launch_bounds__(kThreads) k_gemm(Seg g0, Seg g1, int M, int N,
     if (kt + 1 < nk) {
       const int s1 = (kt + 1) & 1;
       if (kt >= 1) {  // the MMAs of tile kt - 1 still read stage s1
-        if (threadIdx.x == 0 && !mbar_wait(&bar[s1], ((kt - 1) >> 1) & 1)) s_fail = 1;
+        if (threadIdx.x == 0 && !mbar_wait(&bar[s1], ((kt - 1) >> 1) & 1, spin)) { s_fail = 1; s_last = kt - 1; }
         __syncthreads();
         if (s_fail) break;
       }
@@ -236,11 +240,22 @@ __global__ void __launch_bounds__(kThreads) k_gemm(Seg g0, Seg g1, int M, int N,
     }
   }
   // the last commit covers every MMA issued before it
-  if (threadIdx.x == 0 && !s_fail && nk > 0 && !mbar_wait(&bar[(nk - 1) & 1], ((nk - 1) >> 1) & 1)) s_fail = 1;
+  if (threadIdx.x == 0 && !s_fail && nk > 0 && !mbar_wait(&bar[(nk - 1) & 1], ((nk - 1) >> 1) & 1, spin)) {
+    s_fail = 1;
+    s_last = nk - 1;
+  }
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;");
   if (s_fail) {
-    if (threadIdx.x == 0) atomicExch(err, 1);
+    // the MMAs issued so far complete in order: wait for the last commit with
+    // the default bound before the TMEM they write is freed
+    if (threadIdx.x == 0) {
+      atomicExch(err, 1);
+      if (s_last >= 0 && !mbar_wait(&bar[s_last & 1], (s_last >> 1) & 1, kSpin)) atomicExch(err, 2);
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;");
   } else {
     // The MMAs have completed and every copy has landed: the operand stages
     // become an FP32 staging tile [128][BN + 1] (the +1 keeps both row- and
@@ -348,6 +363,9 @@ int rows_fast(int md, int nd, long long sm0, long long sm1, long long sn0, long 
   return warp_sectors(md, nd, sm0, sm1, sn0, sn1, 1, bytes) < warp_sectors(md, nd, sm0, sm1, sn0, sn1, 0, bytes);
 }
 
+// Polls an mbarrier wait makes before it gives up (csrst_gemm_set_wait_limit).
+long long g_wait_polls = kSpin;
+
 template <int BN>
 int launch_gemm(const Seg &g0, const Seg &g1, int M, int N, int batch, const csrst_gemm_epilogue &ep, int *err,
                 cudaStream_t s) {
@@ -364,7 +382,7 @@ int launch_gemm(const Seg &g0, const Seg &g1, int M, int N, int batch, const csr
   const int o_bytes = (ep.out32 || ep.res || ep.pre) ? 4 : 2;
   const int o_mfast = rows_fast(ep.md, ep.nd, ep.sm0, ep.sm1, ep.sn0, ep.sn1, o_bytes);
   const int t_mfast = ep.out16t ? rows_fast(ep.tmd, ep.tnd, ep.tm0, ep.tm1, ep.tn0, ep.tn1, 2) : 0;
-  k_gemm<BN><<<grid, kThreads, smem, s>>>(g0, g1, M, N, ep, err, o_mfast, t_mfast);
+  k_gemm<BN><<<grid, kThreads, smem, s>>>(g0, g1, M, N, ep, err, o_mfast, t_mfast, g_wait_polls);
   return cudaGetLastError() == cudaSuccess ? CSRST_OK : CSRST_E_CUDA;
 }
 
@@ -386,6 +404,11 @@ int gemm_dispatch(const Seg &g0, const Seg &g1, int M, int N, int batch, const c
 
 }  // namespace
 }  // namespace csrst
+
+extern "C" int csrst_gemm_set_wait_limit(long long polls) {
+  csrst::g_wait_polls = polls > 0 ? polls : csrst::kSpin;
+  return CSRST_OK;
+}
 
 extern "C" int csrst_gemm_bf16(const void *A, long long lda, long long stride_a, const void *B, long long ldb,
                                long long stride_b, int M, int N, int K, int batch, const csrst_gemm_epilogue *ep,

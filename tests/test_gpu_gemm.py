@@ -74,3 +74,35 @@ def test_gemm_dual_segments_and_row_bias(gpu_lib):
     for z in range(Z):
         r = ref(a1[z], b1) + ref(a2, b2[z]) + bm.double().numpy()[:, None]
         assert np.abs(out[z].cpu().numpy() - r).max() <= 1e-4 * np.abs(r).max()
+
+
+def test_gemm_wait_that_gives_up_reports_and_recovers(gpu_lib):
+    """The tensor-core waits are bounded.  With a limit of one poll the first
+    wait for an MMA commit gives up: the GEMM reports it through its error
+    word (1: a wait gave up, and its clean-up wait for the issued MMAs
+    succeeded), writes nothing, and returns; with the default limit restored
+    the same GEMM is correct again, so the context and the TMEM allocator are
+    intact."""
+    import torch
+    from csrst_b200._lib import lib
+    from csrst_b200.tensor import _err, gemm
+    rng = np.random.default_rng(3)
+    M, N, K = 256, 128, 512            # 8 K tiles: waits inside the loop and after it
+    a, b = bf16(rng, (M, K)), bf16(rng, (N, K))
+    out = torch.full((M, N), 7.0, dtype=torch.float32, device="cuda")
+    err = _err(torch.device("cuda"))
+    err.zero_()
+    try:
+        lib().csrst_gemm_set_wait_limit(1)
+        gemm(a.cuda(), b.cuda(), M, N, K, out32=out)
+        torch.cuda.synchronize()
+    finally:
+        lib().csrst_gemm_set_wait_limit(0)
+    assert int(err.item()) == 1
+    assert bool((out == 7.0).all())    # the epilogue was skipped
+    err.zero_()
+    gemm(a.cuda(), b.cuda(), M, N, K, out32=out)
+    torch.cuda.synchronize()
+    assert int(err.item()) == 0
+    r = ref(a, b)
+    assert np.abs(out.cpu().numpy() - r).max() <= 1e-4 * np.abs(r).max()
