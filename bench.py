@@ -104,11 +104,9 @@ def peaks(bf16=False):
 # profile launch lists name them.
 STEP_LAUNCHES = {
     ("push", "fp32", 1): {"k_push32<1, 0>": 1, "k_push32<1, 1>": 1, "k_prep32": 2, "k_post32": 2, "k_bounds32": 2},
-    ("yee", "fp32", 1): {"k_half_h<float>": 2, "k_update_e<float, 0>": 1, "k_update_e<float, 1>": 1,
-                         "k_exchange<float>": 4},
+    ("yee", "fp32", 1): {"k_yee_tiles<float>": 1, "k_yee_fixup<float>": 1, "k_window_ey<float>": 1},
     ("push", "fp64", 1): {"k_push<1>": 2, "k_push_prep": 2, "k_push_post": 2, "k_global_bounds": 2},
-    ("yee", "fp64", 1): {"k_half_h<double>": 2, "k_update_e<double, 0>": 1, "k_update_e<double, 1>": 1,
-                         "k_exchange<double>": 4},
+    ("yee", "fp64", 1): {"k_yee_tiles<double>": 1, "k_yee_fixup<double>": 1, "k_window_ey<double>": 1},
 }
 LAUNCH_LISTS = {"fp32": "profiles/c2_tsc_fp32_step_launches.txt", "fp64": "profiles/c2_tsc_fp64_step_launches.txt"}
 
@@ -206,23 +204,15 @@ def time_mode(args, cfg, bunch, world, fp32, clocks):
     ms = max_over_ranks(t0.elapsed_time(t1), world)
     if world > 1:
         torch.distributed.barrier()
-    # ---- kernel attribution: the same steps launched group by group ----
+    # ---- kernel attribution: the same steps' kernels, eagerly, with CUDA
+    # events between the groups on the library's stream (csrst_step_timed) ----
     groups = {"push": 0.0, "yee": 0.0, "move": 0.0}
-    ev = [torch.cuda.Event(enable_timing=True) for _ in range(8)]
-    dt = sim.info()["dt"]
     ksteps = min(args.steps, 10)
     for _ in range(ksteps):
-        ev[0].record(stream); sim.push(0); ev[1].record(stream)
-        sim.half_h(); sim.update_e(0); sim.half_h(); ev[2].record(stream)
-        sim.drift(-0.5 * dt)
-        ev[3].record(stream); sim.push(1); ev[4].record(stream)
-        sim.update_e(1); ev[5].record(stream)
-        sim.drift(-0.5 * dt)
-        ev[6].record(stream); sim.move(); ev[7].record(stream)
-        sim.sync()
-        groups["push"] += ev[0].elapsed_time(ev[1]) + ev[3].elapsed_time(ev[4])
-        groups["yee"] += ev[1].elapsed_time(ev[2]) + ev[4].elapsed_time(ev[5])
-        groups["move"] += ev[6].elapsed_time(ev[7])
+        t = sim.step_timed()
+        groups["push"] += t["push"]
+        groups["yee"] += t["fields"]
+        groups["move"] += t["move"]
     for k in groups:
         groups[k] /= ksteps
     window = sim.window()[0][2:]
@@ -644,9 +634,9 @@ def run_b200(args, world, rank, local):
     if other in runs:
         out[other] = summary(other)
         out[f"{head}_over_{other}"] = round(hs["value"] / out[other]["value"], 3)
-    # launches per step: 2 pushes x (prep, push, post, bounds) + 4 sub-steps x
-    # (sweep, exchange) + move
-    out["gpu_launches"] = args.steps * (2 * 4 + 4 * 2 + 1)
+    # launches per step: 2 pushes x (prep, push, post, bounds) + the fused
+    # field sweep (tiles, window fix-up, window Ey) + move
+    out["gpu_launches"] = args.steps * (2 * 4 + 3 + 1)
     if rank == 0 and not args.no_compare:
         out["accuracy_fp32_vs_fp64"] = accuracy(cfg, spec, bunch)
     if not args.no_ensemble:

@@ -28,7 +28,7 @@ class Config(C.Structure):
 
 ERRORS = {0: "ok", -1: "invalid argument", -2: "CUDA error", -3: "geometry",
           -4: "no particles", -5: "window fit", -6: "window move", -7: "crossings",
-          -8: "window wall", -9: "i/o", 1: "outside the patch"}
+          -8: "window wall", -9: "i/o", -10: "field staging", 1: "outside the patch"}
 
 
 class CsrstError(RuntimeError):
@@ -100,6 +100,7 @@ def lib():
         "csrst_step_first": ([P], C.c_int),
         "csrst_step_second": ([P], C.c_int),
         "csrst_step": ([P, C.c_int], C.c_int),
+        "csrst_step_timed": ([P, D], C.c_int),
         "csrst_diag_moments": ([P, D], C.c_int),
         "csrst_diag_wake": ([P, D, C.c_int], C.c_int),
         "csrst_diag_wake_async": ([P, P, C.c_int, P], C.c_int),

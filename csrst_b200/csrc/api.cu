@@ -134,8 +134,10 @@ struct csrst_handle {
   int push_grid = 0;
   // diagnostics scratch
   double *dscratch = nullptr, *dmean = nullptr, *dout = nullptr;
-  // graph of one step
-  cudaGraphExec_t graph = nullptr;
+  // graphs of one step: the fused sweep swaps the static plane sets every
+  // step, so there is one graph per set that is current when it starts
+  cudaGraphExec_t graph[2] = {nullptr, nullptr};
+  bool graph_fused = false;   // the sweep the graphs were recorded with
   std::string err;
   // FP32 mode (CSRST_FLAG_FP32): FP32 static and window planes, FP32 bunch
   bool fp32 = false;
@@ -155,6 +157,18 @@ struct csrst_handle {
   int npml = 0;
   int2 *pml_rows = nullptr;
   void *psi = nullptr;        // the layers' convolution state, 4 per cell, field type
+  // the fused field sweep: the other static plane set (a fused step reads the
+  // current set and writes this one, then the two swap), the cell kinds in
+  // the static storage layout, and the scratch of the fix-up around the window
+  double *ExB = nullptr, *EyB = nullptr, *HxB = nullptr, *HyB = nullptr;
+  float *ExfB = nullptr, *EyfB = nullptr, *HxfB = nullptr, *HyfB = nullptr;
+  uint8_t *kind = nullptr;
+  int kpitch = 0;
+  void *zfix = nullptr;
+  int zpitch = 0, zrows = 0;
+  int par = 0;                // plane-set swaps so far, mod 2
+  int ens_refs = 0;           // ensembles whose argument tables hold this handle's planes
+  cudaEvent_t *tev = nullptr; // csrst_step_timed: 8 events around the step's kernel groups
 };
 
 // One part of a batch: its members' argument tables in device memory and the
@@ -192,6 +206,7 @@ struct csrst_ensemble {
   // launch shapes (set by csrst_ensemble_set_shape / csrst_ensemble_tune)
   int push_grid = 0, tx = 32, ty = 8, nparts = 1;
   cudaGraphExec_t graph = nullptr;
+  bool holds = false;        // the members' ens_refs count this ensemble
   std::string err;
 };
 
@@ -324,6 +339,11 @@ void bend_setup(csrst_handle *h) {
   h->bwidth = 2 * b.R * std::abs(h->shh);
 }
 
+void drop_graphs(csrst_handle *h) {
+  for (cudaGraphExec_t &g : h->graph)
+    if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+}
+
 void free_particles(csrst_handle *h) {
   cudaFree(h->x); cudaFree(h->y); cudaFree(h->px); cudaFree(h->py); cudaFree(h->q);
   cudaFree(h->ox); cudaFree(h->oy);
@@ -337,7 +357,9 @@ void free_particles(csrst_handle *h) {
   h->b32 = Bunch32{};
   h->winf = h->scratchf = nullptr;
   h->d64 = nullptr;
-  if (h->graph) { cudaGraphExecDestroy(h->graph); h->graph = nullptr; }
+  cudaFree(h->zfix);
+  h->zfix = nullptr;
+  drop_graphs(h);
   h->n = 0;
 }
 
@@ -527,17 +549,87 @@ void moments_async(csrst_handle *h) {
                  h->s);
 }
 
+// Polls of a fused-sweep tile's staging wait before it gives up.
+constexpr long long kStagingPolls = 1ll << 22;
+
+// The fused static sweep runs unless something needs the sub-step kernels:
+// absorbing layers, an ensemble whose tables hold this handle's planes, or
+// CSRST_FLAG_SUBSTEP_FIELDS.
+bool fused_ok(const csrst_handle *h) {
+  return h->zfix && h->kind && !h->pml && h->ens_refs == 0 && !(h->cfg.flags & CSRST_FLAG_SUBSTEP_FIELDS);
+}
+
+void swap_sets(csrst_handle *h) {
+  std::swap(h->Ex, h->ExB); std::swap(h->Ey, h->EyB); std::swap(h->Hx, h->HxB); std::swap(h->Hy, h->HyB);
+  std::swap(h->Exf, h->ExfB); std::swap(h->Eyf, h->EyfB); std::swap(h->Hxf, h->HxfB); std::swap(h->Hyf, h->HyfB);
+  h->par ^= 1;
+}
+
+// Half H, Ex and half H of the static mesh and the window with their strip
+// exchanges, and the static Ey, as one sweep into the other plane set
+// (fields.cu); the sets then swap.
+int fused_fields_async(csrst_handle *h) {
+  int rc;
+  if (h->fp32) {
+    const PlaneT<float> dst[4] = {{h->ExfB, h->pitch32}, {h->EyfB, h->pitch32}, {h->HxfB, h->pitch32},
+                                  {h->HyfB, h->pitch32}};
+    rc = launch_yee_fused(field_args32(h, 0), dst, h->kind, h->kpitch, h->cutidx, static_cast<float *>(h->zfix),
+                          h->zpitch, h->zrows, kStagingPolls, h->s);
+  } else {
+    const Plane dst[4] = {{h->ExB, h->pitch}, {h->EyB, h->pitch}, {h->HxB, h->pitch}, {h->HyB, h->pitch}};
+    rc = launch_yee_fused(field_args(h, 0), dst, h->kind, h->kpitch, h->cutidx, static_cast<double *>(h->zfix),
+                          h->zpitch, h->zrows, kStagingPolls, h->s);
+  }
+  if (rc != kOk) return fail(h, rc == kErrArg ? CSRST_E_ARG : CSRST_E_CUDA, "fused field sweep: tensor-map set-up");
+  h->acc_fresh[0] = false;
+  swap_sets(h);
+  return CSRST_OK;
+}
+
+// The window's Ey sub-step and Ey exchange after the second push.
+void window_ey_async(csrst_handle *h) {
+  if (h->fp32) launch_window_ey(field_args32(h, 1), h->s);
+  else launch_window_ey(field_args(h, 1), h->s);
+  h->acc_fresh[1] = false;
+}
+
+void mark(csrst_handle *h, int k) {
+  if (h->tev) cudaEventRecord(h->tev[k], h->s);
+}
+
 // TETMSolver::updateField_firstStep + updateField_secondStep + moveMesh.
-void step_async(csrst_handle *h) {
+// Events 0..7 (csrst_step_timed) bracket the pushes, the field work of each
+// half and the move.
+int step_async(csrst_handle *h) {
+  mark(h, 0);
   push_async(h, 0);
-  half_h_async(h);
-  update_e_async(h, 0);
-  half_h_async(h);
+  mark(h, 1);
+  if (fused_ok(h)) {
+    const int rc = fused_fields_async(h);
+    if (rc) return rc;
+    mark(h, 2);
+    drift_back(h);
+    mark(h, 3);
+    push_async(h, 1);
+    mark(h, 4);
+    window_ey_async(h);
+  } else {
+    half_h_async(h);
+    update_e_async(h, 0);
+    half_h_async(h);
+    mark(h, 2);
+    drift_back(h);
+    mark(h, 3);
+    push_async(h, 1);
+    mark(h, 4);
+    update_e_async(h, 1);
+  }
+  mark(h, 5);
   drift_back(h);
-  push_async(h, 1);
-  update_e_async(h, 1);
-  drift_back(h);
+  mark(h, 6);
   move_async(h);
+  mark(h, 7);
+  return CSRST_OK;
 }
 
 // FP32 mode's reference momentum and drift constants, rounded once.
@@ -575,7 +667,8 @@ int csrst_create(const csrst_config *cfg, csrst_handle **out) {
   *out = nullptr;
   if (cfg->Nx < 8 || cfg->Ny < 8 || cfg->shape_order < 0 || cfg->shape_order > 2 || !(cfg->width > 0))
     return fail(nullptr, CSRST_E_ARG, "invalid configuration");
-  if (cfg->flags & ~(CSRST_FLAG_KEEP_OLD | CSRST_FLAG_FP32)) return fail(nullptr, CSRST_E_ARG, "unknown flags");
+  if (cfg->flags & ~(CSRST_FLAG_KEEP_OLD | CSRST_FLAG_FP32 | CSRST_FLAG_SUBSTEP_FIELDS))
+    return fail(nullptr, CSRST_E_ARG, "unknown flags");
   if ((cfg->flags & CSRST_FLAG_FP32) && (cfg->Nx > 32767 || cfg->Ny > 32767))
     return fail(nullptr, CSRST_E_ARG, "FP32 mode packs cell indices in 16 bits: Nx, Ny <= 32767");
   int ndev = 0;
@@ -601,13 +694,13 @@ int csrst_create(const csrst_config *cfg, csrst_handle **out) {
   if (h->fp32) {  // FP32 static planes only; FP64 copies are made on demand
     h->pitch32 = ((Nx + 2 + 63) / 64) * 64;
     const size_t ps32 = (size_t)h->pitch32 * (Ny + 2);
-    float **planes[4] = {&h->Exf, &h->Eyf, &h->Hxf, &h->Hyf};
+    float **planes[8] = {&h->Exf, &h->Eyf, &h->Hxf, &h->Hyf, &h->ExfB, &h->EyfB, &h->HxfB, &h->HyfB};
     for (float **p : planes) {
       if ((e = cudaMalloc(p, ps32 * sizeof(float))) != cudaSuccess) return bad(e, "static fields");
       if ((e = cudaMemsetAsync(*p, 0, ps32 * sizeof(float), h->s)) != cudaSuccess) return bad(e, "memset");
     }
   } else {
-    double **planes[4] = {&h->Ex, &h->Ey, &h->Hx, &h->Hy};
+    double **planes[8] = {&h->Ex, &h->Ey, &h->Hx, &h->Hy, &h->ExB, &h->EyB, &h->HxB, &h->HyB};
     for (double **p : planes) {
       if ((e = cudaMalloc(p, ps * sizeof(double))) != cudaSuccess) return bad(e, "static fields");
       if ((e = cudaMemsetAsync(*p, 0, ps * sizeof(double), h->s)) != cudaSuccess) return bad(e, "memset");
@@ -627,6 +720,13 @@ int csrst_create(const csrst_config *cfg, csrst_handle **out) {
     csrst_destroy(h);
     return rc;
   }
+  // cell kinds of the fused sweep, in the static storage layout
+  h->kpitch = ((Nx + 2 + 15) / 16) * 16;
+  const size_t kb = (size_t)h->kpitch * (Ny + 2);
+  if ((e = cudaMalloc(&h->kind, kb)) != cudaSuccess) return bad(e, "cell kinds");
+  if ((e = cudaMemsetAsync(h->kind, 0, kb, h->s)) != cudaSuccess) return bad(e, "memset");
+  launch_build_kind(h->mask, h->cutidx, Nx, Ny, h->kind, h->kpitch, h->s);
+  if ((e = cudaGetLastError()) != cudaSuccess) return bad(e, "cell kinds");
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -639,8 +739,12 @@ int csrst_destroy(csrst_handle *h) {
   if (!h) return CSRST_OK;
   if (h->s) cudaStreamSynchronize(h->s);
   free_particles(h);
+  drop_graphs(h);
   cudaFree(h->Ex); cudaFree(h->Ey); cudaFree(h->Hx); cudaFree(h->Hy);
   cudaFree(h->Exf); cudaFree(h->Eyf); cudaFree(h->Hxf); cudaFree(h->Hyf);
+  cudaFree(h->ExB); cudaFree(h->EyB); cudaFree(h->HxB); cudaFree(h->HyB);
+  cudaFree(h->ExfB); cudaFree(h->EyfB); cudaFree(h->HxfB); cudaFree(h->HyfB);
+  cudaFree(h->kind);
   cudaFree(h->mask); cudaFree(h->cells); cudaFree(h->cutidx); cudaFree(h->ws);
   cudaFree(h->dscratch); cudaFree(h->dmean); cudaFree(h->dout);
   cudaFree(h->pml); cudaFree(h->pml32); cudaFree(h->pml_rows); cudaFree(h->psi);
@@ -837,6 +941,11 @@ int csrst_load_particles(csrst_handle *h, const double *x, const double *y, cons
   }
   CK(cudaMalloc(&h->acc, 2 * (size_t)h->L0 * h->L1 * sizeof(unsigned long long)));
   CK(cudaMemsetAsync(h->acc, 0, 2 * (size_t)h->L0 * h->L1 * sizeof(unsigned long long), h->s));
+  // scratch of the fused sweep's fix-up: the window's footprint widened by
+  // two cells and the cells its sub-steps read (launch_yee_fused)
+  h->zpitch = h->L0 + 6;
+  h->zrows = h->L1 + 7;
+  CK(cudaMalloc(&h->zfix, 4 * (size_t)h->zpitch * h->zrows * (h->fp32 ? sizeof(float) : sizeof(double))));
   // PartBunch::sortParticles: y slice of the window, then x (stable radix sorts)
   {
     unsigned long long *kx = nullptr, *kx2 = nullptr;
@@ -1125,23 +1234,65 @@ int csrst_step(csrst_handle *h, int nsteps) {
   // positions owe the trailing -dt/2 drift and the box of the next gather
   // positions is current.  Anything else runs one step eagerly first.
   while (nsteps > 0 && !(h->pending && h->bb == kBBValid)) {
-    step_async(h);
+    if ((rc = step_async(h))) return rc;
     --nsteps;
   }
   if (nsteps == 0) return CSRST_OK;
-  if (!h->graph) {
-    cudaGraph_t g;
-    CK(cudaStreamBeginCapture(h->s, cudaStreamCaptureModeThreadLocal));
-    step_async(h);
-    CK(cudaStreamEndCapture(h->s, &g));
-    cudaError_t e = cudaGraphInstantiate(&h->graph, g, 0);
-    cudaGraphDestroy(g);
-    if (e != cudaSuccess) return cuda_fail(h, e, "cudaGraphInstantiate");
-    --nsteps;
-    CK(cudaGraphLaunch(h->graph, h->s));
+  const bool fused = fused_ok(h);
+  if (fused != h->graph_fused) {
+    drop_graphs(h);
+    h->graph_fused = fused;
   }
-  for (int k = 0; k < nsteps; ++k) CK(cudaGraphLaunch(h->graph, h->s));
+  for (; nsteps > 0; --nsteps) {
+    const int p = h->par;
+    if (!h->graph[p]) {  // recorded on the first step that starts from this plane set
+      cudaGraph_t g;
+      CK(cudaStreamBeginCapture(h->s, cudaStreamCaptureModeThreadLocal));
+      rc = step_async(h);
+      const cudaError_t ce = cudaStreamEndCapture(h->s, &g);
+      if (rc) {
+        if (ce == cudaSuccess) cudaGraphDestroy(g);
+        return rc;
+      }
+      if (ce != cudaSuccess) return cuda_fail(h, ce, "cudaStreamEndCapture");
+      cudaError_t e = cudaGraphInstantiate(&h->graph[p], g, 0);
+      cudaGraphDestroy(g);
+      if (e != cudaSuccess) return cuda_fail(h, e, "cudaGraphInstantiate");
+    } else if (fused) {
+      swap_sets(h);  // what the recorded step does to the host's view of the planes
+    }
+    CK(cudaGraphLaunch(h->graph[p], h->s));
+  }
   return CSRST_OK;
+}
+
+int csrst_step_timed(csrst_handle *h, double *ms4) {
+  int rc = need_bunch(h);
+  if (rc) return rc;
+  if (!ms4) return fail(h, CSRST_E_ARG, "ms4 is NULL");
+  cudaEvent_t ev[8] = {};
+  for (cudaEvent_t &e : ev) CK(cudaEventCreate(&e));
+  h->tev = ev;
+  rc = step_async(h);
+  h->tev = nullptr;
+  cudaError_t e = cudaStreamSynchronize(h->s);
+  float t[4] = {0, 0, 0, 0};
+  if (!rc && e == cudaSuccess) {
+    float a = 0, b = 0;
+    cudaEventElapsedTime(&a, ev[0], ev[1]);
+    cudaEventElapsedTime(&b, ev[3], ev[4]);
+    t[0] = a + b;
+    cudaEventElapsedTime(&a, ev[1], ev[2]);
+    cudaEventElapsedTime(&b, ev[4], ev[5]);
+    t[1] = a + b;
+    cudaEventElapsedTime(&t[2], ev[6], ev[7]);
+    cudaEventElapsedTime(&t[3], ev[0], ev[7]);
+  }
+  for (cudaEvent_t &v : ev) cudaEventDestroy(v);
+  if (rc) return rc;
+  if (e != cudaSuccess) return cuda_fail(h, e, "csrst_step_timed");
+  for (int k = 0; k < 4; ++k) ms4[k] = t[k];
+  return check_err(h);
 }
 
 int csrst_diag_moments(csrst_handle *h, double *out18) {
@@ -1534,6 +1685,10 @@ int csrst_ensemble_create(csrst_handle *const *members, int m, csrst_ensemble **
     csrst_ensemble_destroy(e);
     return efail(nullptr, CSRST_E_CUDA, "ensemble: stream");
   }
+  // the argument tables hold the members' plane pointers: their single
+  // steps keep to the sub-step kernels (no plane-set swap) from here on
+  for (csrst_handle *h : e->mem) ++h->ens_refs;
+  e->holds = true;
   const int rc = ensemble_build(e);
   if (rc) {
     g_create_error = e->err;
@@ -1546,6 +1701,8 @@ int csrst_ensemble_create(csrst_handle *const *members, int m, csrst_ensemble **
 
 int csrst_ensemble_destroy(csrst_ensemble *e) {
   if (!e) return CSRST_OK;
+  if (e->holds)
+    for (csrst_handle *h : e->mem) --h->ens_refs;
   ensemble_free_tables(e);
   if (e->done) cudaEventDestroy(e->done);
   if (e->fork) cudaEventDestroy(e->fork);
@@ -1719,7 +1876,7 @@ int csrst_set_pml(csrst_handle *h, int width, int order, double reflection) {
   CK(cudaStreamSynchronize(h->s));
   cudaFree(h->pml); cudaFree(h->pml32); cudaFree(h->pml_rows); cudaFree(h->psi);
   h->pml = nullptr; h->pml32 = nullptr; h->pml_rows = nullptr; h->psi = nullptr; h->npml = 0;
-  if (h->graph) { cudaGraphExecDestroy(h->graph); h->graph = nullptr; }
+  drop_graphs(h);
   if (width == 0) return CSRST_OK;
   const int Nx = h->b.Nx, Ny = h->b.Ny;
   std::vector<uint8_t> inside((size_t)Nx * Ny);

@@ -31,6 +31,7 @@ enum : int {
   kErrWindowMove = -6,
   kErrCrossings = -7,
   kErrWindowWall = -8,
+  kErrStaging = -10,
 };
 
 template <class T>

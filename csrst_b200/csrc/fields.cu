@@ -13,7 +13,10 @@
 // disjoint element sets (Communicator::exchangeBoundaries,
 // Communicator.hh:575-876), launched separately because the next sub-step
 // reads what it writes.
+#include <cuda.h>
+
 #include "kernels.cuh"
+#include "tma.cuh"
 
 namespace csrst {
 
@@ -107,6 +110,34 @@ __device__ __forceinline__ void half_h_static(const FieldArgsT<T> &a, int b) {
   store_masked(hyp, hy, m);
 }
 
+// Window cell k (x fastest) of the half H sub-step.
+template <class T>
+__device__ __forceinline__ void window_h(const FieldArgsT<T> &a, int k) {
+  const int i = k % a.L0, j = k / a.L0;
+  T &hx = a.mHx.at(i, j), &hy = a.mHy.at(i, j);
+  hx = hx - a.chx * (a.mEy.at(i + 1, j) - a.mEy.at(i, j));
+  hy = hy + a.chy * (a.mEx.at(i, j + 1) - a.mEx.at(i, j));
+}
+
+// Window cell k of the E sub-step: the window current comes from the
+// fixed-point accumulator of the last push, which is converted, stored for
+// diagnostics and cleared for the next deposit.
+template <class T, int COMP>
+__device__ __forceinline__ void window_e(const FieldArgsT<T> &a, int k) {
+  const int i = k % a.L0, j = k / a.L0;
+  const T J = (T)((double)(long long)a.acc[k] * a.acc_inv);
+  a.acc[k] = 0ull;
+  if (COMP == 0) {
+    a.mJx.at(i, j) = J;
+    T &e = a.mEx.at(i, j);
+    e = e + (a.kex * (a.mHx.at(i, j) - a.mHx.at(i, j - 1) + a.mHy.at(i, j) - a.mHy.at(i, j - 1)) - a.dteps * J);
+  } else {
+    a.mJy.at(i, j) = J;
+    T &e = a.mEy.at(i, j);
+    e = e - (a.key * (a.mHx.at(i, j) - a.mHx.at(i - 1, j) + a.mHy.at(i, j) - a.mHy.at(i - 1, j)) + a.dteps * J);
+  }
+}
+
 // Half H update (first and third sub-step), block b of the sub-step grid.
 // Static blocks cover the mesh in tiles of tx x ty vectors (tx * ty = 256
 // threads, tx a multiple of 32; the shape is a tuning parameter).
@@ -138,10 +169,7 @@ __device__ __forceinline__ void half_h_body(const FieldArgsT<T> &a, int b) {
   } else {
     const int k = (b - a.nbS - a.nbC - a.nbP) * blockDim.x + threadIdx.x;
     if (k >= a.L0 * a.L1) return;
-    const int i = k % a.L0, j = k / a.L0;
-    T &hx = a.mHx.at(i, j), &hy = a.mHy.at(i, j);
-    hx = hx - a.chx * (a.mEy.at(i + 1, j) - a.mEy.at(i, j));
-    hy = hy + a.chy * (a.mEx.at(i, j + 1) - a.mEx.at(i, j));
+    window_h(a, k);
   }
 }
 
@@ -236,18 +264,7 @@ __device__ __forceinline__ void update_e_body(const FieldArgsT<T> &a, int b, T z
   } else {
     const int k = (b - a.nbS - a.nbC - a.nbP) * blockDim.x + threadIdx.x;
     if (k >= a.L0 * a.L1) return;
-    const int i = k % a.L0, j = k / a.L0;
-    const T J = (T)((double)(long long)a.acc[k] * a.acc_inv);
-    a.acc[k] = 0ull;
-    if (COMP == 0) {
-      a.mJx.at(i, j) = J;
-      T &e = a.mEx.at(i, j);
-      e = e + (a.kex * (a.mHx.at(i, j) - a.mHx.at(i, j - 1) + a.mHy.at(i, j) - a.mHy.at(i, j - 1)) - a.dteps * J);
-    } else {
-      a.mJy.at(i, j) = J;
-      T &e = a.mEy.at(i, j);
-      e = e - (a.key * (a.mHx.at(i, j) - a.mHx.at(i - 1, j) + a.mHy.at(i, j) - a.mHy.at(i - 1, j)) + a.dteps * J);
-    }
+    window_e<T, COMP>(a, k);
   }
 }
 
@@ -495,6 +512,374 @@ __device__ __forceinline__ void move_body(const MoveArgs<T> &m) {
   check_window_clear(a, ws);
 }
 
+// --- fused static sweep: the four sub-steps of one time step in one pass ----
+//
+// The static mesh carries no current, and between the first and the last of
+// its four sub-steps (half H, Ex, half H, Ey) it meets the rest of the step
+// only through the window's strips.  So one launch (k_yee_tiles) takes every
+// static cell through all four sub-steps: a CTA stages a tile of Ex, Ey, Hx,
+// Hy and the cell-kind map into shared memory with TMA (a one-cell halo on
+// each side and two rows above: the cells the later sub-steps of its own
+// cells read), runs the sub-steps there, regular and cut cells alike, with
+// the arithmetic of the sub-step kernels, and writes its cells into the
+// OTHER plane set.  Reading one set and writing the other is what lets
+// neighbouring tiles run in any order.  Cells within two of the window's
+// footprint are then redone by k_yee_fixup (one cluster) from the source set
+// with the window's own sub-steps and the strip exchanges in between, in the
+// reference's order; the window's Ey sub-step, which needs the second push's
+// current, follows that push (k_window_ey) with its Ey exchange.  The static
+// Ey the exchange overwrites (the window's first column) is the only static
+// value the push-dependent part changes.
+//
+// The absorbing layers are not part of this path (their cells keep the
+// sub-step kernels).
+
+// Cell kinds of the kind map (static storage layout with guards, one byte).
+enum : uint8_t { kKindNone = 0, kKindRegular = 1, kKindCut = 2 };
+
+// Updates of one static cell, shared by the tile and the fix-up kernels: the
+// same expressions as the sub-step kernels' regular-cell and cut-cell
+// branches (TETMSolver.hh:142-206, :241-261; SCBoundaryCondition.hh:391-431).
+template <class T>
+__device__ __forceinline__ void h_cell(const FieldArgsT<T> &a, uint8_t kind, const CutCellDev *cc, T &hx, T &hy,
+                                       T ey0, T ey1, T ex0, T ex1) {
+  if (kind == kKindRegular) {
+    hx = hx - a.chx * (ey1 - ey0);
+    hy = hy + a.chy * (ex1 - ex0);
+  } else {
+    const T n0 = (T)cc->n0, n1 = (T)cc->n1, l0 = (T)cc->l0, l1 = (T)cc->l1, area = (T)cc->area;
+    const T u0 = a.mhx * (n1 * ey1 - l1 * ey0) / area;
+    const T u1 = a.mhy * (n0 * ex1 - l0 * ex0) / area;
+    hx += u0;
+    hy += u1;
+  }
+}
+
+// Ex of one static cell; hxm, hym: H of the cell below.
+template <class T>
+__device__ __forceinline__ void ex_cell(const FieldArgsT<T> &a, uint8_t kind, const CutCellDev *cc, T &e, T hx, T hxm,
+                                        T hy, T hym, T zeroJ) {
+  if (kind == kKindRegular) {
+    e = e + (a.kex * (hx - hxm + hy - hym) - a.dteps * zeroJ);
+  } else {
+    if (cc->area < kMinArea || !(cc->l0 > kSpaceEps)) return;
+    const T u0 = (hx - hxm) / a.h1;
+    const T u1 = (hy - hym) / a.h1;
+    e += a.de * (u0 + u1 - zeroJ);
+  }
+}
+
+// Ey of one static cell; hxl, hyl: H of the cell to the left.
+template <class T>
+__device__ __forceinline__ void ey_cell(const FieldArgsT<T> &a, uint8_t kind, const CutCellDev *cc, T &e, T hx, T hxl,
+                                        T hy, T hyl, T zeroJ) {
+  if (kind == kKindRegular) {
+    e = e - (a.key * (hx - hxl + hy - hyl) + a.dteps * zeroJ);
+  } else {
+    if (cc->area < kMinArea || !(cc->l1 > kSpaceEps)) return;
+    const T u0 = -(hx - hxl) / a.h0;
+    const T u1 = -(hy - hyl) / a.h0;
+    e += a.de * (u0 + u1 - zeroJ);
+  }
+}
+
+// Tile geometry.  A tile is TX storage columns [s0, s0 + TX) (s0 a multiple
+// of TX; storage column s holds cell s - 1) by TY cell rows [y0, y0 + TY).
+// The plane boxes cover storage columns [s0 - V, s0 + TX + V) (V elements =
+// 16 bytes, so that the box starts on a 16-byte boundary and its rows are a
+// whole number of 16-byte pieces) and cell rows y0 - 1 .. y0 + TY + 1; the
+// kind box covers storage columns [s0 - 16, s0 + TX + 16) of the same rows.
+template <class T>
+struct YeeTile {
+  static constexpr int V = 16 / (int)sizeof(T);
+  static constexpr int TX = sizeof(T) == 4 ? 64 : 32;
+  static constexpr int TY = 32;
+  static constexpr int W = TX + 2 * V;
+  static constexpr int H = TY + 3;
+  static constexpr int KW = TX + 32;
+  static constexpr int KO = 16 - V;  // kind-box column of plane-box column c: c + KO
+  static constexpr int PLANE_BYTES = (W * H * (int)sizeof(T) + 127) / 128 * 128;
+  static constexpr int KIND_BYTES = (KW * H + 127) / 128 * 128;
+  static constexpr uint32_t TX_BYTES = 4u * W * H * sizeof(T) + (uint32_t)KW * H;
+  static constexpr int SMEM = 4 * PLANE_BYTES + KIND_BYTES + 16 + 128;  // + barrier, + base alignment
+  static constexpr int THREADS = 256;
+};
+
+template <class T>
+struct alignas(64) YeeTileArgs {
+  CUtensorMap map[5];   // Ex, Ey, Hx, Hy of the source set, then the kind map
+  FieldArgsT<T> f;      // coefficients, cut cells, mesh size (static planes: the source set)
+  PlaneT<T> out[4];     // Ex, Ey, Hx, Hy of the destination set
+  const int *cutidx;    // cell -> cut-cell entry
+  int tilesX;
+  T zeroJ;
+  long long spin;       // polls of the staging wait before it gives up (kErrStaging)
+};
+
+template <class T>
+__global__ void __launch_bounds__(256) k_yee_tiles(const __grid_constant__ YeeTileArgs<T> a) {
+  using G = YeeTile<T>;
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t *base = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~(uintptr_t)127);
+  T *sEx = reinterpret_cast<T *>(base);
+  T *sEy = reinterpret_cast<T *>(base + G::PLANE_BYTES);
+  T *sHx = reinterpret_cast<T *>(base + 2 * G::PLANE_BYTES);
+  T *sHy = reinterpret_cast<T *>(base + 3 * G::PLANE_BYTES);
+  uint8_t *sK = base + 4 * G::PLANE_BYTES;
+  uint64_t *bar = reinterpret_cast<uint64_t *>(sK + G::KIND_BYTES);
+  const FieldArgsT<T> &f = a.f;
+  const int s0 = (int)(blockIdx.x % (unsigned)a.tilesX) * G::TX;
+  const int y0 = (int)(blockIdx.x / (unsigned)a.tilesX) * G::TY;
+  if (threadIdx.x == 0) {
+    mbar_init(bar, 1);
+    mbar_init_fence();
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    mbar_expect_tx(bar, G::TX_BYTES);
+    // storage row of cell row y0 - 1 is y0
+    tma_load_2d(sEx, &a.map[0], s0 - G::V, y0, bar);
+    tma_load_2d(sEy, &a.map[1], s0 - G::V, y0, bar);
+    tma_load_2d(sHx, &a.map[2], s0 - G::V, y0, bar);
+    tma_load_2d(sHy, &a.map[3], s0 - G::V, y0, bar);
+    tma_load_2d(sK, &a.map[4], s0 - 16, y0, bar);
+  }
+  const bool ok = mbar_wait(bar, 0, a.spin);
+  if (__syncthreads_or(!ok)) {  // the copies did not arrive: report, wait once more for them, write nothing
+    if (threadIdx.x == 0) {
+      set_err(f.ws, kErrStaging);
+      mbar_wait(bar, 0, a.spin);
+    }
+    return;
+  }
+  // plane-box column c, row r is cell (s0 - V - 1 + c, y0 - 1 + r)
+  const int i0 = s0 - G::V - 1, j0 = y0 - 1;
+  constexpr int W = G::W;
+  // 1: half H on columns [V - 1, V + TX), rows [0, TY + 2)
+  {
+    constexpr int CW = G::TX + 1, C0 = G::V - 1;
+    for (int k = threadIdx.x; k < CW * (G::TY + 2); k += G::THREADS) {
+      const int c = C0 + k % CW, r = k / CW;
+      const uint8_t kd = sK[r * G::KW + c + G::KO];
+      if (kd == kKindNone) continue;
+      const int o = r * W + c;
+      const CutCellDev *cc = kd == kKindCut ? f.cells + a.cutidx[(size_t)(j0 + r) * f.Nx + (i0 + c)] : nullptr;
+      h_cell(f, kd, cc, sHx[o], sHy[o], sEy[o], sEy[o + 1], sEx[o], sEx[o + W]);
+    }
+  }
+  __syncthreads();
+  // 2: Ex on columns [V - 1, V + TX), rows [1, TY + 2)
+  {
+    constexpr int CW = G::TX + 1, C0 = G::V - 1;
+    for (int k = threadIdx.x; k < CW * (G::TY + 1); k += G::THREADS) {
+      const int c = C0 + k % CW, r = 1 + k / CW;
+      const uint8_t kd = sK[r * G::KW + c + G::KO];
+      if (kd == kKindNone) continue;
+      const int o = r * W + c;
+      const CutCellDev *cc = kd == kKindCut ? f.cells + a.cutidx[(size_t)(j0 + r) * f.Nx + (i0 + c)] : nullptr;
+      ex_cell(f, kd, cc, sEx[o], sHx[o], sHx[o - W], sHy[o], sHy[o - W], a.zeroJ);
+    }
+  }
+  __syncthreads();
+  // 3: half H on columns [V - 1, V + TX), rows [1, TY + 1)
+  {
+    constexpr int CW = G::TX + 1, C0 = G::V - 1;
+    for (int k = threadIdx.x; k < CW * G::TY; k += G::THREADS) {
+      const int c = C0 + k % CW, r = 1 + k / CW;
+      const uint8_t kd = sK[r * G::KW + c + G::KO];
+      if (kd == kKindNone) continue;
+      const int o = r * W + c;
+      const CutCellDev *cc = kd == kKindCut ? f.cells + a.cutidx[(size_t)(j0 + r) * f.Nx + (i0 + c)] : nullptr;
+      h_cell(f, kd, cc, sHx[o], sHy[o], sEy[o], sEy[o + 1], sEx[o], sEx[o + W]);
+    }
+  }
+  __syncthreads();
+  // 4: Ey on columns [V, V + TX), rows [1, TY + 1)
+  {
+    constexpr int CW = G::TX, C0 = G::V;
+    for (int k = threadIdx.x; k < CW * G::TY; k += G::THREADS) {
+      const int c = C0 + k % CW, r = 1 + k / CW;
+      const uint8_t kd = sK[r * G::KW + c + G::KO];
+      if (kd == kKindNone) continue;
+      const int o = r * W + c;
+      const CutCellDev *cc = kd == kKindCut ? f.cells + a.cutidx[(size_t)(j0 + r) * f.Nx + (i0 + c)] : nullptr;
+      ey_cell(f, kd, cc, sEy[o], sHx[o], sHx[o - 1], sHy[o], sHy[o - 1], a.zeroJ);
+    }
+  }
+  __syncthreads();
+  // the tile's cells, every one (unchanged ones too), into the destination set:
+  // 16-byte pieces of storage columns [s0, s0 + TX) (inside the padded row)
+  constexpr int NV = G::TX / G::V;
+#pragma unroll
+  for (int p = 0; p < 4; ++p) {
+    const T *sp = p == 0 ? sEx : p == 1 ? sEy : p == 2 ? sHx : sHy;
+    const PlaneT<T> &out = a.out[p];
+    for (int k = threadIdx.x; k < G::TY * NV; k += G::THREADS) {
+      const int r = 1 + k / NV, v = k % NV, j = j0 + r;
+      if (j >= f.Ny) break;  // rows grow with k
+      const Vec16<T> val = *reinterpret_cast<const Vec16<T> *>(sp + r * W + G::V + v * G::V);
+      st16(out.p + (size_t)(j + 1) * out.pitch + s0 + v * G::V, val);
+    }
+  }
+}
+
+// The fix-up of the cells around the window (one cluster of kFixCtas CTAs,
+// synchronised by cluster barriers between the phases).  Its region is the
+// window's footprint widened by two cells, clipped to the mesh: the strip
+// exchanges change static cells at most one cell outside the footprint over
+// the four sub-steps.  It copies the source set over the region and the
+// cells the later sub-steps of the region read into scratch planes, runs the
+// static and window sub-steps and exchanges there in the order of the
+// sub-step kernels, and writes the region into the destination set.
+constexpr int kFixCtas = 8, kFixThreads = 512;
+
+template <class T>
+struct YeeFixArgs {
+  PlaneT<T> out[4];   // Ex, Ey, Hx, Hy of the destination set
+  T *z;               // 4 scratch planes, zpitch x zrows each
+  int zpitch, zrows;
+  const uint8_t *kind;
+  int kpitch;
+  const int *cutidx;
+  T zeroJ;
+};
+
+// Orders every thread's earlier global and shared writes of the cluster
+// before its later reads (release / acquire at cluster scope).
+__device__ __forceinline__ void cluster_barrier() {
+  __threadfence();
+  asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+
+__device__ __forceinline__ int exchange_items(int L0, int L1, int which) {
+  return which == 0 ? 2 * (L0 + L1) + 4 : which == 1 ? 2 * L0 + 2 : 2 * L1 + 2;
+}
+
+template <class T>
+__global__ void __cluster_dims__(kFixCtas, 1, 1) __launch_bounds__(kFixThreads)
+    k_yee_fixup(FieldArgsT<T> a, YeeFixArgs<T> x) {
+  const int P0 = a.ws->P0, P1 = a.ws->P1, L0 = a.L0, L1 = a.L1;
+  // the window and its ring on the mesh (as the move and the initial
+  // placement check, kErrWindowWall), else the scratch box would not hold
+  // the strips: nothing is done, uniformly over the cluster
+  if (P0 < 1 || P1 < 1 || P0 + L0 >= a.Nx || P1 + L1 >= a.Ny) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) set_err(a.ws, kErrWindowWall);
+    return;
+  }
+  const int c0 = max(P0 - 2, 0), c1 = min(P0 + L0 + 2, a.Nx);
+  const int r0 = max(P1 - 2, 0), r1 = min(P1 + L1 + 2, a.Ny);
+  // scratch box: cells [c0 - 1, c1 + 1) x [r0 - 1, r1 + 2); PlaneT's guard
+  // offset puts cell (c0 - 1, r0 - 1) at the start of each scratch plane
+  const int zw = c1 - c0 + 2, zh = r1 - r0 + 3;
+  const ptrdiff_t zoff = (ptrdiff_t)r0 * x.zpitch + c0;
+  const size_t zs = (size_t)x.zpitch * x.zrows;
+  FieldArgsT<T> z = a;
+  z.Ex = PlaneT<T>{x.z - zoff, x.zpitch};
+  z.Ey = PlaneT<T>{x.z + zs - zoff, x.zpitch};
+  z.Hx = PlaneT<T>{x.z + 2 * zs - zoff, x.zpitch};
+  z.Hy = PlaneT<T>{x.z + 3 * zs - zoff, x.zpitch};
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
+  const int nw = L0 * L1;
+  auto kind_of = [&](int i, int j) { return x.kind[(size_t)(j + 1) * x.kpitch + (i + 1)]; };
+  auto cut_of = [&](uint8_t kd, int i, int j) -> const CutCellDev * {
+    return kd == kKindCut ? a.cells + x.cutidx[(size_t)j * a.Nx + i] : nullptr;
+  };
+  // the box from the source set (cells off the stored planes read zero, as
+  // the tile kernel's staging fills them)
+  {
+    const int nb = zw * zh;
+    for (int k = tid; k < 4 * nb; k += nth) {
+      const int p = k / nb, rem = k % nb, i = c0 - 1 + rem % zw, j = r0 - 1 + rem / zw;
+      const PlaneT<T> &src = p == 0 ? a.Ex : p == 1 ? a.Ey : p == 2 ? a.Hx : a.Hy;
+      const PlaneT<T> &dst = p == 0 ? z.Ex : p == 1 ? z.Ey : p == 2 ? z.Hx : z.Hy;
+      const bool stored = i >= -1 && i <= a.Nx && j >= -1 && j <= a.Ny;
+      dst.at(i, j) = stored ? src.at(i, j) : T(0);
+    }
+  }
+  cluster_barrier();
+  // 1: half H, static [c0 - 1, c1) x [r0 - 1, r1 + 1), and the window
+  {
+    const int w = c1 - c0 + 1, ns = w * (r1 - r0 + 2);
+    for (int k = tid; k < ns + nw; k += nth) {
+      if (k >= ns) { window_h(a, k - ns); continue; }
+      const int i = c0 - 1 + k % w, j = r0 - 1 + k / w;
+      const uint8_t kd = kind_of(i, j);
+      if (kd == kKindNone) continue;
+      h_cell(a, kd, cut_of(kd, i, j), z.Hx.at(i, j), z.Hy.at(i, j), z.Ey.at(i, j), z.Ey.at(i + 1, j), z.Ex.at(i, j),
+             z.Ex.at(i, j + 1));
+    }
+  }
+  cluster_barrier();
+  for (int k = tid; k < exchange_items(L0, L1, 0); k += nth) exchange_body(z, 0, k);
+  cluster_barrier();
+  // 2: Ex, static [c0 - 1, c1) x [r0, r1 + 1), and the window with the first push's current
+  {
+    const int w = c1 - c0 + 1, ns = w * (r1 - r0 + 1);
+    for (int k = tid; k < ns + nw; k += nth) {
+      if (k >= ns) { window_e<T, 0>(a, k - ns); continue; }
+      const int i = c0 - 1 + k % w, j = r0 + k / w;
+      const uint8_t kd = kind_of(i, j);
+      if (kd == kKindNone) continue;
+      ex_cell(a, kd, cut_of(kd, i, j), z.Ex.at(i, j), z.Hx.at(i, j), z.Hx.at(i, j - 1), z.Hy.at(i, j),
+              z.Hy.at(i, j - 1), x.zeroJ);
+    }
+  }
+  cluster_barrier();
+  for (int k = tid; k < exchange_items(L0, L1, 1); k += nth) exchange_body(z, 1, k);
+  cluster_barrier();
+  // 3: half H, static [c0 - 1, c1) x [r0, r1), and the window
+  {
+    const int w = c1 - c0 + 1, ns = w * (r1 - r0);
+    for (int k = tid; k < ns + nw; k += nth) {
+      if (k >= ns) { window_h(a, k - ns); continue; }
+      const int i = c0 - 1 + k % w, j = r0 + k / w;
+      const uint8_t kd = kind_of(i, j);
+      if (kd == kKindNone) continue;
+      h_cell(a, kd, cut_of(kd, i, j), z.Hx.at(i, j), z.Hy.at(i, j), z.Ey.at(i, j), z.Ey.at(i + 1, j), z.Ex.at(i, j),
+             z.Ex.at(i, j + 1));
+    }
+  }
+  cluster_barrier();
+  for (int k = tid; k < exchange_items(L0, L1, 0); k += nth) exchange_body(z, 0, k);
+  cluster_barrier();
+  // 4: static Ey on [c0, c1) x [r0, r1) (the window's Ey follows the second push)
+  {
+    const int w = c1 - c0, ns = w * (r1 - r0);
+    for (int k = tid; k < ns; k += nth) {
+      const int i = c0 + k % w, j = r0 + k / w;
+      const uint8_t kd = kind_of(i, j);
+      if (kd == kKindNone) continue;
+      ey_cell(a, kd, cut_of(kd, i, j), z.Ey.at(i, j), z.Hx.at(i, j), z.Hx.at(i - 1, j), z.Hy.at(i, j),
+              z.Hy.at(i - 1, j), x.zeroJ);
+    }
+  }
+  cluster_barrier();
+  {
+    const int w = c1 - c0, nr = w * (r1 - r0);
+    for (int k = tid; k < 4 * nr; k += nth) {
+      const int p = k / nr, rem = k % nr, i = c0 + rem % w, j = r0 + rem / w;
+      const PlaneT<T> &src = p == 0 ? z.Ex : p == 1 ? z.Ey : p == 2 ? z.Hx : z.Hy;
+      const PlaneT<T> &dst = p == 0 ? x.out[0] : p == 1 ? x.out[1] : p == 2 ? x.out[2] : x.out[3];
+      dst.at(i, j) = src.at(i, j);
+    }
+  }
+}
+
+// The window's Ey sub-step with the second push's current, and the Ey strip
+// exchange: the thread of window cell (0, j) also writes it to the static
+// mesh; the static column right of the window fills the window's guard
+// column (the static Ey there is final since the fused sweep).
+template <class T>
+__global__ void __launch_bounds__(256) k_window_ey(FieldArgsT<T> a) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x, nw = a.L0 * a.L1;
+  if (k < nw) {
+    window_e<T, 1>(a, k);
+    if (k % a.L0 == 0) exchange_body(a, 2, k / a.L0);
+  } else if (k - nw < a.L1 + 2) {
+    exchange_body(a, 2, a.L1 + (k - nw));
+  }
+}
+
 // --- kernels: one member, and a batch of members in one launch --------------
 
 template <class T>
@@ -654,6 +1039,96 @@ void launch_reset_outside(FieldArgsT<T> a, const int *cutidx, cudaStream_t s) {
   k_reset_outside<T><<<(unsigned)((n + 255) / 256), 256, 0, s>>>(a, cutidx);
 }
 
+// --- fused sweep: host side ---------------------------------------------------
+
+using EncodeTiled = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                 const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                 CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+// cuTensorMapEncodeTiled of the driver, found once through the runtime.
+static EncodeTiled tensor_map_encoder() {
+  static const EncodeTiled fn = [] {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      return (EncodeTiled) nullptr;
+    return reinterpret_cast<EncodeTiled>(p);
+  }();
+  return fn;
+}
+
+// Row-major 2-D map of w x h elements, rows pitch_bytes apart, box bw x bh;
+// reads outside the tensor return zero.
+static bool encode_2d(CUtensorMap *m, CUtensorMapDataType dt, const void *base, uint64_t w, uint64_t h,
+                      uint64_t pitch_bytes, uint32_t bw, uint32_t bh) {
+  const EncodeTiled enc = tensor_map_encoder();
+  if (!enc) return false;
+  const cuuint64_t dims[2] = {w, h};
+  const cuuint64_t strides[1] = {pitch_bytes};
+  const cuuint32_t box[2] = {bw, bh};
+  const cuuint32_t es[2] = {1, 1};
+  return enc(m, dt, 2, const_cast<void *>(base), dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+             CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+template <class T>
+int launch_yee_fused(const FieldArgsT<T> &a, const PlaneT<T> *dst, const uint8_t *kind, int kpitch,
+                     const int *cutidx, T *z, int zpitch, int zrows, long long spin, cudaStream_t s) {
+  using G = YeeTile<T>;
+  if (zpitch < a.L0 + 6 || zrows < a.L1 + 7 || kpitch < a.Nx + 2 || kpitch % 16) return kErrArg;
+  YeeTileArgs<T> t;
+  const CUtensorMapDataType dt = sizeof(T) == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
+  const PlaneT<T> *src[4] = {&a.Ex, &a.Ey, &a.Hx, &a.Hy};
+  for (int p = 0; p < 4; ++p) {
+    if ((src[p]->pitch * sizeof(T)) % 16 || (reinterpret_cast<uintptr_t>(src[p]->p) & 15)) return kErrArg;
+    if (!encode_2d(&t.map[p], dt, src[p]->p, (uint64_t)a.Nx + 2, (uint64_t)a.Ny + 2,
+                   (uint64_t)src[p]->pitch * sizeof(T), G::W, G::H))
+      return kErrCuda;
+  }
+  if (!encode_2d(&t.map[4], CU_TENSOR_MAP_DATA_TYPE_UINT8, kind, (uint64_t)a.Nx + 2, (uint64_t)a.Ny + 2,
+                 (uint64_t)kpitch, G::KW, G::H))
+    return kErrCuda;
+  t.f = a;
+  for (int p = 0; p < 4; ++p) t.out[p] = dst[p];
+  t.cutidx = cutidx;
+  t.tilesX = (a.Nx + 2 + G::TX - 1) / G::TX;
+  const int tilesY = (a.Ny + G::TY - 1) / G::TY;
+  t.zeroJ = T(0);
+  t.spin = spin;
+  if (cudaFuncSetAttribute(k_yee_tiles<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM) != cudaSuccess)
+    return kErrCuda;
+  k_yee_tiles<T><<<t.tilesX * tilesY, G::THREADS, G::SMEM, s>>>(t);
+  YeeFixArgs<T> x;
+  for (int p = 0; p < 4; ++p) x.out[p] = dst[p];
+  x.z = z; x.zpitch = zpitch; x.zrows = zrows;
+  x.kind = kind; x.kpitch = kpitch; x.cutidx = cutidx;
+  x.zeroJ = T(0);
+  k_yee_fixup<T><<<kFixCtas, kFixThreads, 0, s>>>(a, x);
+  return kOk;
+}
+
+template <class T>
+void launch_window_ey(const FieldArgsT<T> &a, cudaStream_t s) {
+  const int n = a.L0 * a.L1 + a.L1 + 2;
+  k_window_ey<T><<<(n + 255) / 256, 256, 0, s>>>(a);
+}
+
+// Cell kinds in the static storage layout (guards and padding stay none).
+__global__ void k_build_kind(const uint8_t *mask, const int *cutidx, int Nx, int Ny, uint8_t *kind, int kpitch) {
+  const long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (k >= (long long)Nx * Ny) return;
+  const int i = (int)(k % Nx), j = (int)(k / Nx);
+  kind[(size_t)(j + 1) * kpitch + (i + 1)] = mask[k] ? kKindRegular : cutidx[k] >= 0 ? kKindCut : kKindNone;
+}
+
+void launch_build_kind(const uint8_t *mask, const int *cutidx, int Nx, int Ny, uint8_t *kind, int kpitch,
+                       cudaStream_t s) {
+  const long long n = (long long)Nx * Ny;
+  k_build_kind<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(mask, cutidx, Nx, Ny, kind, kpitch);
+}
+
 #define CSRST_FIELDS_INSTANTIATE(T)                                                         \
   template void launch_half_h<T>(FieldArgsT<T>, cudaStream_t);                              \
   template void launch_update_e<T>(FieldArgsT<T>, int, cudaStream_t);                       \
@@ -666,7 +1141,10 @@ void launch_reset_outside(FieldArgsT<T> a, const int *cutidx, cudaStream_t s) {
   template void launch_half_h_batch<T>(const FieldArgsT<T> *, const int *, int, int, cudaStream_t); \
   template void launch_update_e_batch<T>(const FieldArgsT<T> *, const int *, int, int, int, cudaStream_t); \
   template void launch_exchange_batch<T>(const FieldArgsT<T> *, const int *, int, int, int, cudaStream_t); \
-  template void launch_move_batch<T>(const MoveArgs<T> *, int, cudaStream_t);
+  template void launch_move_batch<T>(const MoveArgs<T> *, int, cudaStream_t);                        \
+  template int launch_yee_fused<T>(const FieldArgsT<T> &, const PlaneT<T> *, const uint8_t *, int, const int *, T *, \
+                                   int, int, long long, cudaStream_t);                                \
+  template void launch_window_ey<T>(const FieldArgsT<T> &, cudaStream_t);
 CSRST_FIELDS_INSTANTIATE(double)
 CSRST_FIELDS_INSTANTIATE(float)
 

@@ -25,39 +25,13 @@
 #include <stdint.h>
 
 #include "../../include/csrst.h"
+#include "tma.cuh"
 
 namespace csrst {
 namespace {
 
 constexpr int kBM = 128, kBK = 64, kThreads = 128;
 constexpr long long kSpin = 1ll << 24;  // default mbarrier polls before a wait gives up
-
-__device__ __forceinline__ uint32_t smem_u32(const void *p) {
-  return (uint32_t)__cvta_generic_to_shared(p);
-}
-
-__device__ __forceinline__ void mbar_init(uint64_t *bar, int count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
-}
-
-__device__ __forceinline__ bool mbar_try(uint64_t *bar, uint32_t parity) {
-  uint32_t ok;
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-      "selp.u32 %0, 1, 0, p;\n\t}"
-      : "=r"(ok)
-      : "r"(smem_u32(bar)), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-
-// Bounded wait for completion `parity` of an mbarrier.
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, long long spin) {
-  for (long long k = 0; k < spin; ++k)
-    if (mbar_try(bar, parity)) return true;
-  return false;
-}
 
 __device__ __forceinline__ void cp_async16(void *dst, const void *src) {
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src) : "memory");

@@ -154,6 +154,20 @@ template <class T>
 void launch_exchange_batch(const FieldArgsT<T> *args, const int *bpre, int m, int nblocks, int which,
                            cudaStream_t s);
 template <class T> void launch_move_batch(const MoveArgs<T> *args, int m, cudaStream_t s);
+// The fused static sweep of one time step (fields.cu): a's static planes are
+// the source set, dst the destination set (Ex, Ey, Hx, Hy); a carries the
+// window, its first push's current and that component's acc_inv.  kind: the
+// cell-kind map (static storage layout, kpitch bytes per row, a multiple of
+// 16); z: 4 scratch planes of zpitch >= L0 + 6 by zrows >= L1 + 7 elements;
+// spin: polls of a tile's staging wait.  Returns kOk or kErrArg / kErrCuda
+// (tensor-map set-up) before anything is launched.
+template <class T>
+int launch_yee_fused(const FieldArgsT<T> &a, const PlaneT<T> *dst, const uint8_t *kind, int kpitch,
+                     const int *cutidx, T *z, int zpitch, int zrows, long long spin, cudaStream_t s);
+// The window's Ey sub-step after the second push, with its strip exchange.
+template <class T> void launch_window_ey(const FieldArgsT<T> &a, cudaStream_t s);
+void launch_build_kind(const uint8_t *mask, const int *cutidx, int Nx, int Ny, uint8_t *kind, int kpitch,
+                       cudaStream_t s);
 // geometry.cu
 int build_geometry(const BendDev &b, uint8_t *d_mask, CutCellDev **d_cells, int *ncells, int **d_cutidx,
                    cudaStream_t s);

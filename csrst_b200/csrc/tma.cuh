@@ -1,0 +1,72 @@
+// Shared-memory barriers and TMA copies (sm_100a), used by the GEMM and the
+// fused field sweep.  Every wait is bounded by a poll count: a wait that
+// gives up returns false and the caller reports it.
+#pragma once
+#include <stdint.h>
+
+namespace csrst {
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, int count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+
+// Makes the initialised barrier visible to the TMA unit.
+__device__ __forceinline__ void mbar_init_fence() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try(uint64_t *bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// Non-blocking check of completion `parity` of an mbarrier.
+__device__ __forceinline__ bool mbar_test(uint64_t *bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// Bounded wait for completion `parity` of an mbarrier: `spin` polls, the
+// first one non-blocking (so that a limit of one poll gives up at once on
+// work still in flight), the others try_wait, which may suspend the thread
+// for a short time of the hardware's choosing before it reports.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, long long spin) {
+  if (spin <= 0) return false;
+  if (mbar_test(bar, parity)) return true;
+  for (long long k = 1; k < spin; ++k)
+    if (mbar_try(bar, parity)) return true;
+  return false;
+}
+
+// 2-D tiled TMA load of the box at (x, y) of a tensor map (a kernel
+// parameter, so that its generic address is valid for the copy) into this
+// CTA's shared memory, completing on `bar`.  x * element size must be a
+// multiple of 16 bytes; x and y may lie outside the tensor (zero fill).
+__device__ __forceinline__ void tma_load_2d(void *dst, const void *map, int x, int y, uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
+      ::"r"(smem_u32(dst)), "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
+      : "memory");
+}
+
+}  // namespace csrst

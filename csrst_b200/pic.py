@@ -27,12 +27,15 @@ class Simulation:
 
     FLAG_KEEP_OLD = 1
     FLAG_FP32 = 2
+    FLAG_SUBSTEP_FIELDS = 4
 
-    def __init__(self, cfg, keep_old=False, fp32=False):
+    def __init__(self, cfg, keep_old=False, fp32=False, substep_fields=False):
         """fp32: FP32 mode (FP32 fields, gather, kick and positions, the
         positions as FP32 offsets from FP64 cell origins; FP32 current path
         integral with exact integer charge conservation, csrst_flux32).
-        keep_old: keep the start of every particle's last move."""
+        keep_old: keep the start of every particle's last move.
+        substep_fields: one launch per field sub-step instead of the fused
+        static sweep (the same results, bit for bit)."""
         c = Config()
         for k, v in cfg.dict().items():
             setattr(c, k, v)
@@ -40,6 +43,8 @@ class Simulation:
             c.flags |= self.FLAG_KEEP_OLD
         if fp32:
             c.flags |= self.FLAG_FP32
+        if substep_fields:
+            c.flags |= self.FLAG_SUBSTEP_FIELDS
         self.fp32 = bool(c.flags & self.FLAG_FP32)
         self.cfg = cfg
         h = C.c_void_p()
@@ -184,6 +189,13 @@ class Simulation:
 
     def step(self, n=1):
         self._ck(lib().csrst_step(self.h, n))
+
+    def step_timed(self):
+        """One step with device times of its kernel groups (ms): push,
+        fields, move, total."""
+        out = np.zeros(4)
+        self._ck(lib().csrst_step_timed(self.h, ptr(out)))
+        return dict(zip(("push", "fields", "move", "total"), out.tolist()))
 
     def sync(self):
         self._ck(lib().csrst_sync(self.h))

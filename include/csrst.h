@@ -37,6 +37,7 @@ extern "C" {
 #define CSRST_E_CROSSINGS (-7)     /* a particle crossed more cell borders than one push allows */
 #define CSRST_E_WINDOW_WALL (-8)   /* window or its ring touches a non-inside cell */
 #define CSRST_E_IO (-9)            /* checkpoint file could not be written or read */
+#define CSRST_E_STAGING (-10)      /* a field tile's staging copy did not arrive (bounded wait gave up) */
 #define CSRST_W_OUTSIDE 1          /* warning: contributions outside the caller's patch were dropped */
 
 typedef struct csrst_handle csrst_handle;
@@ -48,6 +49,9 @@ typedef struct csrst_handle csrst_handle;
                                 * FP64 reference momentum) and FP32 current path integral with exact
                                 * integer charge conservation (csrst_flux32).  No reference
                                 * counterpart; checked against the FP64 path to a tolerance. */
+#define CSRST_FLAG_SUBSTEP_FIELDS 4 /* one launch per field sub-step instead of the fused static
+                                * sweep (same results, bit for bit; the sweep is also off while
+                                * absorbing layers are set or the handle is in an ensemble) */
 
 /* Run set-up.  Mirrors the command line of src/main.cpp:111-136 for the
  * parts the time step uses.  shape_order: 0 = IntCIC (ZerothOrderShapeFunction),
@@ -157,8 +161,17 @@ int csrst_move_window(csrst_handle *h);
 int csrst_step_first(csrst_handle *h);
 int csrst_step_second(csrst_handle *h);
 /* nsteps iterations of the main loop body (main.cpp:390-506): first step,
- * second step, window move.  Captured once as a CUDA graph and replayed. */
+ * second step, window move.  Captured as a CUDA graph and replayed.  The
+ * static mesh's four sub-steps run as one fused sweep from one plane set into
+ * another (the sets swap every step; every read and write of the fields goes
+ * to the current set), bit for bit what the sub-step calls above give. */
 int csrst_step(csrst_handle *h, int nsteps);
+/* One step as csrst_step takes it (same kernels, launched eagerly) with CUDA
+ * events between its kernel groups; waits for it and returns the device
+ * times in ms4 [ms]: both pushes, the field work (the fused sweep, or the
+ * four sub-steps with their exchanges, and the window's Ey), the window move,
+ * and the whole step. */
+int csrst_step_timed(csrst_handle *h, double *ms4);
 
 /* Batched ensemble (no reference counterpart: the reference runs one bunch
  * per job).  Independent members, each a loaded handle with its own mesh,
@@ -167,7 +180,8 @@ int csrst_step(csrst_handle *h, int nsteps);
  * members and the whole step is one CUDA graph.  Each member's state after a
  * batched step is bitwise the state its own csrst_step would give.  The
  * member handles stay valid for reads between ensemble steps; reloading a
- * member invalidates the ensemble. */
+ * member invalidates the ensemble.  Destroy the ensemble before its members;
+ * while it exists their own steps use the sub-step kernels. */
 typedef struct csrst_ensemble csrst_ensemble;
 int csrst_ensemble_create(csrst_handle *const *members, int m, csrst_ensemble **out);
 int csrst_ensemble_destroy(csrst_ensemble *e);

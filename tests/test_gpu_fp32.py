@@ -195,7 +195,7 @@ def test_fp32_csr_wake_through_the_dipole_c1(gpu_lib):
     4000 rounded kicks)."""
     from csrst_b200.compare import fp32_vs_fp64
     r = fp32_vs_fp64("c1-bend", 2000, every=100)
-    assert r["wake_samples"] > 50 and r["integrated_columns"] > 50
+    assert r["wake_samples"] >= 50 and r["integrated_columns"] > 500
     assert r["wake_rel_err"] <= WAKE_TOL, r
     assert r["integrated_rel_err"] <= WAKE_TOL, r
     assert r["slice_rel_err"] <= 3e-3, r
