@@ -169,6 +169,8 @@ struct csrst_handle {
   int par = 0;                // plane-set swaps so far, mod 2
   int ens_refs = 0;           // ensembles whose argument tables hold this handle's planes
   cudaEvent_t *tev = nullptr; // csrst_step_timed: 8 events around the step's kernel groups
+  cudaStream_t s2 = nullptr;  // the fused sweep's window fix-up, beside its tiles
+  cudaEvent_t fork = nullptr, join = nullptr;
 };
 
 // One part of a batch: its members' argument tables in device memory and the
@@ -574,11 +576,11 @@ int fused_fields_async(csrst_handle *h) {
     const PlaneT<float> dst[4] = {{h->ExfB, h->pitch32}, {h->EyfB, h->pitch32}, {h->HxfB, h->pitch32},
                                   {h->HyfB, h->pitch32}};
     rc = launch_yee_fused(field_args32(h, 0), dst, h->kind, h->kpitch, h->cutidx, static_cast<float *>(h->zfix),
-                          h->zpitch, h->zrows, kStagingPolls, h->s);
+                          h->zpitch, h->zrows, kStagingPolls, h->s, h->s2, h->fork, h->join);
   } else {
     const Plane dst[4] = {{h->ExB, h->pitch}, {h->EyB, h->pitch}, {h->HxB, h->pitch}, {h->HyB, h->pitch}};
     rc = launch_yee_fused(field_args(h, 0), dst, h->kind, h->kpitch, h->cutidx, static_cast<double *>(h->zfix),
-                          h->zpitch, h->zrows, kStagingPolls, h->s);
+                          h->zpitch, h->zrows, kStagingPolls, h->s, h->s2, h->fork, h->join);
   }
   if (rc != kOk) return fail(h, rc == kErrArg ? CSRST_E_ARG : CSRST_E_CUDA, "fused field sweep: tensor-map set-up");
   h->acc_fresh[0] = false;
@@ -688,6 +690,9 @@ int csrst_create(const csrst_config *cfg, csrst_handle **out) {
   };
   cudaError_t e;
   if ((e = cudaStreamCreateWithFlags(&h->s, cudaStreamNonBlocking)) != cudaSuccess) return bad(e, "stream");
+  if ((e = cudaStreamCreateWithFlags(&h->s2, cudaStreamNonBlocking)) != cudaSuccess) return bad(e, "stream");
+  if ((e = cudaEventCreateWithFlags(&h->fork, cudaEventDisableTiming)) != cudaSuccess) return bad(e, "event");
+  if ((e = cudaEventCreateWithFlags(&h->join, cudaEventDisableTiming)) != cudaSuccess) return bad(e, "event");
   const int Nx = cfg->Nx, Ny = cfg->Ny;
   h->pitch = ((Nx + 2 + 31) / 32) * 32;
   const size_t ps = (size_t)h->pitch * (Ny + 2);
@@ -748,6 +753,10 @@ int csrst_destroy(csrst_handle *h) {
   cudaFree(h->mask); cudaFree(h->cells); cudaFree(h->cutidx); cudaFree(h->ws);
   cudaFree(h->dscratch); cudaFree(h->dmean); cudaFree(h->dout);
   cudaFree(h->pml); cudaFree(h->pml32); cudaFree(h->pml_rows); cudaFree(h->psi);
+  if (h->s2) cudaStreamSynchronize(h->s2);
+  if (h->fork) cudaEventDestroy(h->fork);
+  if (h->join) cudaEventDestroy(h->join);
+  if (h->s2) cudaStreamDestroy(h->s2);
   if (h->s) cudaStreamDestroy(h->s);
   delete h;
   return CSRST_OK;

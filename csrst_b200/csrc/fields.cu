@@ -524,9 +524,10 @@ __device__ __forceinline__ void move_body(const MoveArgs<T> &m) {
 // the arithmetic of the sub-step kernels, and writes its cells into the
 // OTHER plane set.  Reading one set and writing the other is what lets
 // neighbouring tiles run in any order.  Cells within two of the window's
-// footprint are then redone by k_yee_fixup (one cluster) from the source set
-// with the window's own sub-steps and the strip exchanges in between, in the
-// reference's order; the window's Ey sub-step, which needs the second push's
+// footprint are left to k_yee_fixup (one cluster, beside the tiles on a
+// second stream), which redoes them from the source set with the window's
+// own sub-steps and the strip exchanges in between, in the reference's
+// order; the window's Ey sub-step, which needs the second push's
 // current, follows that push (k_window_ey) with its Ey exchange.  The static
 // Ey the exchange overwrites (the window's first column) is the only static
 // value the push-dependent part changes.
@@ -603,6 +604,7 @@ struct YeeTile {
   static constexpr uint32_t TX_BYTES = 4u * W * H * sizeof(T) + (uint32_t)KW * H;
   static constexpr int SMEM = 4 * PLANE_BYTES + KIND_BYTES + 16 + 128;  // + barrier, + base alignment
   static constexpr int THREADS = 256;
+  static constexpr int E = TX / 32;  // cells per lane in a row
 };
 
 template <class T>
@@ -615,6 +617,136 @@ struct alignas(64) YeeTileArgs {
   T zeroJ;
   long long spin;       // polls of the staging wait before it gives up (kErrStaging)
 };
+
+// The region the fix-up rewrites: the window's footprint widened by two
+// cells, clipped to the mesh, cells [c0, c1) x [r0, r1).
+struct FixRegion {
+  int c0, c1, r0, r1;
+};
+__device__ __forceinline__ FixRegion fix_region(int P0, int P1, int L0, int L1, int Nx, int Ny) {
+  return FixRegion{max(P0 - 2, 0), min(P0 + L0 + 2, Nx), max(P1 - 2, 0), min(P1 + L1 + 2, Ny)};
+}
+
+// E consecutive elements of a shared-memory row (E = 2 floats or 1 double:
+// one 8-byte access per lane).
+template <class T, int E>
+struct alignas(E * sizeof(T)) Pack {
+  T v[E];
+};
+template <class T, int E>
+__device__ __forceinline__ Pack<T, E> ldp(const T *p) { return *reinterpret_cast<const Pack<T, E> *>(p); }
+template <class T, int E>
+__device__ __forceinline__ void stp(T *p, const Pack<T, E> &x) { *reinterpret_cast<Pack<T, E> *>(p) = x; }
+
+// The E kinds of the cells at kind-box offset q (q a multiple of E).
+template <int E>
+__device__ __forceinline__ void kinds(const uint8_t *sK, int q, uint8_t *kd) {
+  if (E == 2) {
+    const uint16_t w = *reinterpret_cast<const uint16_t *>(sK + q);
+    kd[0] = (uint8_t)(w & 0xff);
+    kd[E - 1] = (uint8_t)(w >> 8);
+  } else {
+    kd[0] = sK[q];
+  }
+}
+
+// Shared-memory tile of the sweep: the four planes and the kinds, box
+// column c / row r = cell (i0 + c, j0 + r).
+template <class T>
+struct TileSm {
+  T *ex, *ey, *hx, *hy;
+  const uint8_t *k;
+  int i0, j0;
+};
+
+template <class T, class G>
+__device__ __forceinline__ const CutCellDev *tile_cut(const YeeTileArgs<T> &a, const TileSm<T> &t, int c, int r) {
+  return a.f.cells + a.cutidx[(size_t)(t.j0 + r) * a.f.Nx + (t.i0 + c)];
+}
+
+// Half H on cells [c, c + E) of row r.
+template <class T, class G>
+__device__ __forceinline__ void tile_h(const YeeTileArgs<T> &a, const TileSm<T> &t, int c, int r) {
+  constexpr int E = G::E, W = G::W;
+  const int o = r * W + c;
+  uint8_t kd[E];
+  kinds<E>(t.k, r * G::KW + c + G::KO, kd);
+  bool any = false;
+#pragma unroll
+  for (int e = 0; e < E; ++e) any |= kd[e] != kKindNone;
+  if (!any) return;
+  Pack<T, E> hx = ldp<T, E>(t.hx + o), hy = ldp<T, E>(t.hy + o);
+  const Pack<T, E> ey = ldp<T, E>(t.ey + o), ex0 = ldp<T, E>(t.ex + o), ex1 = ldp<T, E>(t.ex + o + W);
+  const T eyn = t.ey[o + E];
+#pragma unroll
+  for (int e = 0; e < E; ++e) {
+    if (kd[e] == kKindNone) continue;
+    const T ey1 = e + 1 < E ? ey.v[e + 1 < E ? e + 1 : 0] : eyn;
+    h_cell(a.f, kd[e], kd[e] == kKindCut ? tile_cut<T, G>(a, t, c + e, r) : nullptr, hx.v[e], hy.v[e], ey.v[e], ey1,
+           ex0.v[e], ex1.v[e]);
+  }
+  stp<T, E>(t.hx + o, hx);
+  stp<T, E>(t.hy + o, hy);
+}
+
+// Ex on cells [c, c + E) of row r.
+template <class T, class G>
+__device__ __forceinline__ void tile_ex(const YeeTileArgs<T> &a, const TileSm<T> &t, int c, int r) {
+  constexpr int E = G::E, W = G::W;
+  const int o = r * W + c;
+  uint8_t kd[E];
+  kinds<E>(t.k, r * G::KW + c + G::KO, kd);
+  bool any = false;
+#pragma unroll
+  for (int e = 0; e < E; ++e) any |= kd[e] != kKindNone;
+  if (!any) return;
+  Pack<T, E> ex = ldp<T, E>(t.ex + o);
+  const Pack<T, E> hx = ldp<T, E>(t.hx + o), hxm = ldp<T, E>(t.hx + o - W);
+  const Pack<T, E> hy = ldp<T, E>(t.hy + o), hym = ldp<T, E>(t.hy + o - W);
+#pragma unroll
+  for (int e = 0; e < E; ++e) {
+    if (kd[e] == kKindNone) continue;
+    ex_cell(a.f, kd[e], kd[e] == kKindCut ? tile_cut<T, G>(a, t, c + e, r) : nullptr, ex.v[e], hx.v[e], hxm.v[e],
+            hy.v[e], hym.v[e], a.zeroJ);
+  }
+  stp<T, E>(t.ex + o, ex);
+}
+
+// Ey on cells [c, c + E) of row r.
+template <class T, class G>
+__device__ __forceinline__ void tile_ey(const YeeTileArgs<T> &a, const TileSm<T> &t, int c, int r) {
+  constexpr int E = G::E, W = G::W;
+  const int o = r * W + c;
+  uint8_t kd[E];
+  kinds<E>(t.k, r * G::KW + c + G::KO, kd);
+  bool any = false;
+#pragma unroll
+  for (int e = 0; e < E; ++e) any |= kd[e] != kKindNone;
+  if (!any) return;
+  Pack<T, E> ey = ldp<T, E>(t.ey + o);
+  const Pack<T, E> hx = ldp<T, E>(t.hx + o), hy = ldp<T, E>(t.hy + o);
+  const T hxl0 = t.hx[o - 1], hyl0 = t.hy[o - 1];
+#pragma unroll
+  for (int e = 0; e < E; ++e) {
+    if (kd[e] == kKindNone) continue;
+    const T hxl = e > 0 ? hx.v[e > 0 ? e - 1 : 0] : hxl0, hyl = e > 0 ? hy.v[e > 0 ? e - 1 : 0] : hyl0;
+    ey_cell(a.f, kd[e], kd[e] == kKindCut ? tile_cut<T, G>(a, t, c + e, r) : nullptr, ey.v[e], hx.v[e], hxl, hy.v[e],
+            hyl, a.zeroJ);
+  }
+  stp<T, E>(t.ey + o, ey);
+}
+
+// One cell of the halo column (box column V - 1) for the first three phases.
+template <class T, class G, int PHASE>
+__device__ __forceinline__ void tile_halo(const YeeTileArgs<T> &a, const TileSm<T> &t, int r) {
+  constexpr int W = G::W, c = G::V - 1;
+  const uint8_t kd = t.k[r * G::KW + c + G::KO];
+  if (kd == kKindNone) return;
+  const int o = r * W + c;
+  const CutCellDev *cc = kd == kKindCut ? tile_cut<T, G>(a, t, c, r) : nullptr;
+  if (PHASE == 2) ex_cell(a.f, kd, cc, t.ex[o], t.hx[o], t.hx[o - W], t.hy[o], t.hy[o - W], a.zeroJ);
+  else h_cell(a.f, kd, cc, t.hx[o], t.hy[o], t.ey[o], t.ey[o + 1], t.ex[o], t.ex[o + W]);
+}
 
 template <class T>
 __global__ void __launch_bounds__(256) k_yee_tiles(const __grid_constant__ YeeTileArgs<T> a) {
@@ -644,6 +776,8 @@ __global__ void __launch_bounds__(256) k_yee_tiles(const __grid_constant__ YeeTi
     tma_load_2d(sHy, &a.map[3], s0 - G::V, y0, bar);
     tma_load_2d(sK, &a.map[4], s0 - 16, y0, bar);
   }
+  // the fix-up's region, whose cells this sweep leaves to it (read while the copies fly)
+  const FixRegion R = fix_region(f.ws->P0, f.ws->P1, f.L0, f.L1, f.Nx, f.Ny);
   const bool ok = mbar_wait(bar, 0, a.spin);
   if (__syncthreads_or(!ok)) {  // the copies did not arrive: report, wait once more for them, write nothing
     if (threadIdx.x == 0) {
@@ -652,73 +786,42 @@ __global__ void __launch_bounds__(256) k_yee_tiles(const __grid_constant__ YeeTi
     }
     return;
   }
-  // plane-box column c, row r is cell (s0 - V - 1 + c, y0 - 1 + r)
-  const int i0 = s0 - G::V - 1, j0 = y0 - 1;
-  constexpr int W = G::W;
-  // 1: half H on columns [V - 1, V + TX), rows [0, TY + 2)
-  {
-    constexpr int CW = G::TX + 1, C0 = G::V - 1;
-    for (int k = threadIdx.x; k < CW * (G::TY + 2); k += G::THREADS) {
-      const int c = C0 + k % CW, r = k / CW;
-      const uint8_t kd = sK[r * G::KW + c + G::KO];
-      if (kd == kKindNone) continue;
-      const int o = r * W + c;
-      const CutCellDev *cc = kd == kKindCut ? f.cells + a.cutidx[(size_t)(j0 + r) * f.Nx + (i0 + c)] : nullptr;
-      h_cell(f, kd, cc, sHx[o], sHy[o], sEy[o], sEy[o + 1], sEx[o], sEx[o + W]);
-    }
-  }
+  // box column c, row r is cell (s0 - V - 1 + c, y0 - 1 + r); each lane takes
+  // E consecutive cells of a row of the tile's TX columns [V, V + TX), the
+  // halo column V - 1 (phases 1-3) goes to the last two warps
+  const TileSm<T> t{sEx, sEy, sHx, sHy, sK, s0 - G::V - 1, y0 - 1};
+  const int warp = threadIdx.x >> 5, c = G::V + (threadIdx.x & 31) * G::E, th = threadIdx.x - 192;
+  for (int r = warp; r < G::TY + 2; r += 8) tile_h<T, G>(a, t, c, r);
+  if (th >= 0 && th < G::TY + 2) tile_halo<T, G, 1>(a, t, th);
   __syncthreads();
-  // 2: Ex on columns [V - 1, V + TX), rows [1, TY + 2)
-  {
-    constexpr int CW = G::TX + 1, C0 = G::V - 1;
-    for (int k = threadIdx.x; k < CW * (G::TY + 1); k += G::THREADS) {
-      const int c = C0 + k % CW, r = 1 + k / CW;
-      const uint8_t kd = sK[r * G::KW + c + G::KO];
-      if (kd == kKindNone) continue;
-      const int o = r * W + c;
-      const CutCellDev *cc = kd == kKindCut ? f.cells + a.cutidx[(size_t)(j0 + r) * f.Nx + (i0 + c)] : nullptr;
-      ex_cell(f, kd, cc, sEx[o], sHx[o], sHx[o - W], sHy[o], sHy[o - W], a.zeroJ);
-    }
-  }
+  for (int r = 1 + warp; r < G::TY + 2; r += 8) tile_ex<T, G>(a, t, c, r);
+  if (th >= 0 && th < G::TY + 1) tile_halo<T, G, 2>(a, t, 1 + th);
   __syncthreads();
-  // 3: half H on columns [V - 1, V + TX), rows [1, TY + 1)
-  {
-    constexpr int CW = G::TX + 1, C0 = G::V - 1;
-    for (int k = threadIdx.x; k < CW * G::TY; k += G::THREADS) {
-      const int c = C0 + k % CW, r = 1 + k / CW;
-      const uint8_t kd = sK[r * G::KW + c + G::KO];
-      if (kd == kKindNone) continue;
-      const int o = r * W + c;
-      const CutCellDev *cc = kd == kKindCut ? f.cells + a.cutidx[(size_t)(j0 + r) * f.Nx + (i0 + c)] : nullptr;
-      h_cell(f, kd, cc, sHx[o], sHy[o], sEy[o], sEy[o + 1], sEx[o], sEx[o + W]);
-    }
-  }
+  for (int r = 1 + warp; r < G::TY + 1; r += 8) tile_h<T, G>(a, t, c, r);
+  if (th >= 0 && th < G::TY) tile_halo<T, G, 3>(a, t, 1 + th);
   __syncthreads();
-  // 4: Ey on columns [V, V + TX), rows [1, TY + 1)
-  {
-    constexpr int CW = G::TX, C0 = G::V;
-    for (int k = threadIdx.x; k < CW * G::TY; k += G::THREADS) {
-      const int c = C0 + k % CW, r = 1 + k / CW;
-      const uint8_t kd = sK[r * G::KW + c + G::KO];
-      if (kd == kKindNone) continue;
-      const int o = r * W + c;
-      const CutCellDev *cc = kd == kKindCut ? f.cells + a.cutidx[(size_t)(j0 + r) * f.Nx + (i0 + c)] : nullptr;
-      ey_cell(f, kd, cc, sEy[o], sHx[o], sHx[o - 1], sHy[o], sHy[o - 1], a.zeroJ);
-    }
-  }
+  for (int r = 1 + warp; r < G::TY + 1; r += 8) tile_ey<T, G>(a, t, c, r);
   __syncthreads();
-  // the tile's cells, every one (unchanged ones too), into the destination set:
-  // 16-byte pieces of storage columns [s0, s0 + TX) (inside the padded row)
+  // the tile's cells, every one (unchanged ones too) except the fix-up's,
+  // into the destination set: 16-byte pieces of storage columns [s0, s0 + TX)
   constexpr int NV = G::TX / G::V;
 #pragma unroll
   for (int p = 0; p < 4; ++p) {
     const T *sp = p == 0 ? sEx : p == 1 ? sEy : p == 2 ? sHx : sHy;
     const PlaneT<T> &out = a.out[p];
     for (int k = threadIdx.x; k < G::TY * NV; k += G::THREADS) {
-      const int r = 1 + k / NV, v = k % NV, j = j0 + r;
+      const int r = 1 + k / NV, v = k % NV, j = t.j0 + r;
       if (j >= f.Ny) break;  // rows grow with k
-      const Vec16<T> val = *reinterpret_cast<const Vec16<T> *>(sp + r * W + G::V + v * G::V);
-      st16(out.p + (size_t)(j + 1) * out.pitch + s0 + v * G::V, val);
+      const T *src = sp + r * G::W + G::V + v * G::V;
+      T *dst = out.p + (size_t)(j + 1) * out.pitch + s0 + v * G::V;
+      const int i = s0 + v * G::V - 1;  // cell of the piece's first element
+      if (j < R.r0 || j >= R.r1 || i + G::V <= R.c0 || i >= R.c1) {
+        st16(dst, *reinterpret_cast<const Vec16<T> *>(src));
+      } else {
+#pragma unroll
+        for (int e = 0; e < G::V; ++e)
+          if (i + e < R.c0 || i + e >= R.c1) dst[e] = src[e];
+      }
     }
   }
 }
@@ -766,8 +869,8 @@ __global__ void __cluster_dims__(kFixCtas, 1, 1) __launch_bounds__(kFixThreads)
     if (blockIdx.x == 0 && threadIdx.x == 0) set_err(a.ws, kErrWindowWall);
     return;
   }
-  const int c0 = max(P0 - 2, 0), c1 = min(P0 + L0 + 2, a.Nx);
-  const int r0 = max(P1 - 2, 0), r1 = min(P1 + L1 + 2, a.Ny);
+  const FixRegion R = fix_region(P0, P1, L0, L1, a.Nx, a.Ny);
+  const int c0 = R.c0, c1 = R.c1, r0 = R.r0, r1 = R.r1;
   // scratch box: cells [c0 - 1, c1 + 1) x [r0 - 1, r1 + 2); PlaneT's guard
   // offset puts cell (c0 - 1, r0 - 1) at the start of each scratch plane
   const int zw = c1 - c0 + 2, zh = r1 - r0 + 3;
@@ -1075,7 +1178,8 @@ static bool encode_2d(CUtensorMap *m, CUtensorMapDataType dt, const void *base, 
 
 template <class T>
 int launch_yee_fused(const FieldArgsT<T> &a, const PlaneT<T> *dst, const uint8_t *kind, int kpitch,
-                     const int *cutidx, T *z, int zpitch, int zrows, long long spin, cudaStream_t s) {
+                     const int *cutidx, T *z, int zpitch, int zrows, long long spin, cudaStream_t s, cudaStream_t s2,
+                     cudaEvent_t fork, cudaEvent_t join) {
   using G = YeeTile<T>;
   if (zpitch < a.L0 + 6 || zrows < a.L1 + 7 || kpitch < a.Nx + 2 || kpitch % 16) return kErrArg;
   YeeTileArgs<T> t;
@@ -1099,13 +1203,17 @@ int launch_yee_fused(const FieldArgsT<T> &a, const PlaneT<T> *dst, const uint8_t
   t.spin = spin;
   if (cudaFuncSetAttribute(k_yee_tiles<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM) != cudaSuccess)
     return kErrCuda;
-  k_yee_tiles<T><<<t.tilesX * tilesY, G::THREADS, G::SMEM, s>>>(t);
   YeeFixArgs<T> x;
   for (int p = 0; p < 4; ++p) x.out[p] = dst[p];
   x.z = z; x.zpitch = zpitch; x.zrows = zrows;
   x.kind = kind; x.kpitch = kpitch; x.cutidx = cutidx;
   x.zeroJ = T(0);
-  k_yee_fixup<T><<<kFixCtas, kFixThreads, 0, s>>>(a, x);
+  // the tiles and the fix-up write disjoint cells and read only the source
+  // set: the fix-up runs on s2 beside the tiles, s waits for both
+  if (cudaEventRecord(fork, s) != cudaSuccess || cudaStreamWaitEvent(s2, fork, 0) != cudaSuccess) return kErrCuda;
+  k_yee_fixup<T><<<kFixCtas, kFixThreads, 0, s2>>>(a, x);
+  k_yee_tiles<T><<<t.tilesX * tilesY, G::THREADS, G::SMEM, s>>>(t);
+  if (cudaEventRecord(join, s2) != cudaSuccess || cudaStreamWaitEvent(s, join, 0) != cudaSuccess) return kErrCuda;
   return kOk;
 }
 
@@ -1143,7 +1251,7 @@ void launch_build_kind(const uint8_t *mask, const int *cutidx, int Nx, int Ny, u
   template void launch_exchange_batch<T>(const FieldArgsT<T> *, const int *, int, int, int, cudaStream_t); \
   template void launch_move_batch<T>(const MoveArgs<T> *, int, cudaStream_t);                        \
   template int launch_yee_fused<T>(const FieldArgsT<T> &, const PlaneT<T> *, const uint8_t *, int, const int *, T *, \
-                                   int, int, long long, cudaStream_t);                                \
+                                   int, int, long long, cudaStream_t, cudaStream_t, cudaEvent_t, cudaEvent_t); \
   template void launch_window_ey<T>(const FieldArgsT<T> &, cudaStream_t);
 CSRST_FIELDS_INSTANTIATE(double)
 CSRST_FIELDS_INSTANTIATE(float)

@@ -159,11 +159,14 @@ template <class T> void launch_move_batch(const MoveArgs<T> *args, int m, cudaSt
 // window, its first push's current and that component's acc_inv.  kind: the
 // cell-kind map (static storage layout, kpitch bytes per row, a multiple of
 // 16); z: 4 scratch planes of zpitch >= L0 + 6 by zrows >= L1 + 7 elements;
-// spin: polls of a tile's staging wait.  Returns kOk or kErrArg / kErrCuda
-// (tensor-map set-up) before anything is launched.
+// spin: polls of a tile's staging wait.  The window fix-up runs on s2
+// between the events fork (recorded on s) and join (s waits for it).
+// Returns kOk, or kErrArg / kErrCuda (tensor-map set-up) before anything is
+// launched.
 template <class T>
 int launch_yee_fused(const FieldArgsT<T> &a, const PlaneT<T> *dst, const uint8_t *kind, int kpitch,
-                     const int *cutidx, T *z, int zpitch, int zrows, long long spin, cudaStream_t s);
+                     const int *cutidx, T *z, int zpitch, int zrows, long long spin, cudaStream_t s, cudaStream_t s2,
+                     cudaEvent_t fork, cudaEvent_t join);
 // The window's Ey sub-step after the second push, with its strip exchange.
 template <class T> void launch_window_ey(const FieldArgsT<T> &a, cudaStream_t s);
 void launch_build_kind(const uint8_t *mask, const int *cutidx, int Nx, int Ny, uint8_t *kind, int kpitch,

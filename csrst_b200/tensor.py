@@ -26,6 +26,11 @@ def _ptr(t):
 
 
 def _err(device):
+    """The device's error word of the tensor-core waits ("cuda" and "cuda:0"
+    name the same one)."""
+    device = torch.device(device)
+    if device.type == "cuda" and device.index is None:
+        device = torch.device("cuda", torch.cuda.current_device())
     if device not in _ERR:
         _ERR[device] = torch.zeros(1, dtype=torch.int32, device=device)
     return _ERR[device]
