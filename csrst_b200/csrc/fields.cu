@@ -602,7 +602,9 @@ struct YeeTile {
   static constexpr int PLANE_BYTES = (W * H * (int)sizeof(T) + 127) / 128 * 128;
   static constexpr int KIND_BYTES = (KW * H + 127) / 128 * 128;
   static constexpr uint32_t TX_BYTES = 4u * W * H * sizeof(T) + (uint32_t)KW * H;
-  static constexpr int SMEM = 4 * PLANE_BYTES + KIND_BYTES + 16 + 128;  // + barrier, + base alignment
+  static constexpr int CUTS = 256;  // cut cells the tile's list holds (more: the phases scan the kinds)
+  // planes, kinds, barrier (16 bytes), cut list, base alignment; 5 CTAs per SM
+  static constexpr int SMEM = 4 * PLANE_BYTES + KIND_BYTES + 16 + 2 * CUTS + 128;
   static constexpr int THREADS = 256;
   static constexpr int E = TX / 32;  // cells per lane in a row
 };
@@ -664,7 +666,13 @@ __device__ __forceinline__ const CutCellDev *tile_cut(const YeeTileArgs<T> &a, c
   return a.f.cells + a.cutidx[(size_t)(t.j0 + r) * a.f.Nx + (t.i0 + c)];
 }
 
-// Half H on cells [c, c + E) of row r.
+// Regular cells of a piece: the row passes handle only kind-regular cells
+// (with the regular branch of h_cell / ex_cell / ey_cell) and store only
+// those elements back; cut cells have their own pass over the tile's list,
+// halo-column cells their own pass, so that no store of one pass covers a
+// cell another pass of the same phase writes.
+
+// Half H, regular cells [c, c + E) of row r.
 template <class T, class G>
 __device__ __forceinline__ void tile_h(const YeeTileArgs<T> &a, const TileSm<T> &t, int c, int r) {
   constexpr int E = G::E, W = G::W;
@@ -673,23 +681,23 @@ __device__ __forceinline__ void tile_h(const YeeTileArgs<T> &a, const TileSm<T> 
   kinds<E>(t.k, r * G::KW + c + G::KO, kd);
   bool any = false;
 #pragma unroll
-  for (int e = 0; e < E; ++e) any |= kd[e] != kKindNone;
+  for (int e = 0; e < E; ++e) any |= kd[e] == kKindRegular;
   if (!any) return;
   Pack<T, E> hx = ldp<T, E>(t.hx + o), hy = ldp<T, E>(t.hy + o);
   const Pack<T, E> ey = ldp<T, E>(t.ey + o), ex0 = ldp<T, E>(t.ex + o), ex1 = ldp<T, E>(t.ex + o + W);
   const T eyn = t.ey[o + E];
 #pragma unroll
   for (int e = 0; e < E; ++e) {
-    if (kd[e] == kKindNone) continue;
     const T ey1 = e + 1 < E ? ey.v[e + 1 < E ? e + 1 : 0] : eyn;
-    h_cell(a.f, kd[e], kd[e] == kKindCut ? tile_cut<T, G>(a, t, c + e, r) : nullptr, hx.v[e], hy.v[e], ey.v[e], ey1,
-           ex0.v[e], ex1.v[e]);
+    h_cell(a.f, kKindRegular, nullptr, hx.v[e], hy.v[e], ey.v[e], ey1, ex0.v[e], ex1.v[e]);
+    if (kd[e] == kKindRegular) {
+      t.hx[o + e] = hx.v[e];
+      t.hy[o + e] = hy.v[e];
+    }
   }
-  stp<T, E>(t.hx + o, hx);
-  stp<T, E>(t.hy + o, hy);
 }
 
-// Ex on cells [c, c + E) of row r.
+// Ex, regular cells [c, c + E) of row r.
 template <class T, class G>
 __device__ __forceinline__ void tile_ex(const YeeTileArgs<T> &a, const TileSm<T> &t, int c, int r) {
   constexpr int E = G::E, W = G::W;
@@ -698,21 +706,19 @@ __device__ __forceinline__ void tile_ex(const YeeTileArgs<T> &a, const TileSm<T>
   kinds<E>(t.k, r * G::KW + c + G::KO, kd);
   bool any = false;
 #pragma unroll
-  for (int e = 0; e < E; ++e) any |= kd[e] != kKindNone;
+  for (int e = 0; e < E; ++e) any |= kd[e] == kKindRegular;
   if (!any) return;
   Pack<T, E> ex = ldp<T, E>(t.ex + o);
   const Pack<T, E> hx = ldp<T, E>(t.hx + o), hxm = ldp<T, E>(t.hx + o - W);
   const Pack<T, E> hy = ldp<T, E>(t.hy + o), hym = ldp<T, E>(t.hy + o - W);
 #pragma unroll
   for (int e = 0; e < E; ++e) {
-    if (kd[e] == kKindNone) continue;
-    ex_cell(a.f, kd[e], kd[e] == kKindCut ? tile_cut<T, G>(a, t, c + e, r) : nullptr, ex.v[e], hx.v[e], hxm.v[e],
-            hy.v[e], hym.v[e], a.zeroJ);
+    ex_cell(a.f, kKindRegular, nullptr, ex.v[e], hx.v[e], hxm.v[e], hy.v[e], hym.v[e], a.zeroJ);
+    if (kd[e] == kKindRegular) t.ex[o + e] = ex.v[e];
   }
-  stp<T, E>(t.ex + o, ex);
 }
 
-// Ey on cells [c, c + E) of row r.
+// Ey, regular cells [c, c + E) of row r.
 template <class T, class G>
 __device__ __forceinline__ void tile_ey(const YeeTileArgs<T> &a, const TileSm<T> &t, int c, int r) {
   constexpr int E = G::E, W = G::W;
@@ -721,37 +727,65 @@ __device__ __forceinline__ void tile_ey(const YeeTileArgs<T> &a, const TileSm<T>
   kinds<E>(t.k, r * G::KW + c + G::KO, kd);
   bool any = false;
 #pragma unroll
-  for (int e = 0; e < E; ++e) any |= kd[e] != kKindNone;
+  for (int e = 0; e < E; ++e) any |= kd[e] == kKindRegular;
   if (!any) return;
   Pack<T, E> ey = ldp<T, E>(t.ey + o);
   const Pack<T, E> hx = ldp<T, E>(t.hx + o), hy = ldp<T, E>(t.hy + o);
   const T hxl0 = t.hx[o - 1], hyl0 = t.hy[o - 1];
 #pragma unroll
   for (int e = 0; e < E; ++e) {
-    if (kd[e] == kKindNone) continue;
     const T hxl = e > 0 ? hx.v[e > 0 ? e - 1 : 0] : hxl0, hyl = e > 0 ? hy.v[e > 0 ? e - 1 : 0] : hyl0;
-    ey_cell(a.f, kd[e], kd[e] == kKindCut ? tile_cut<T, G>(a, t, c + e, r) : nullptr, ey.v[e], hx.v[e], hxl, hy.v[e],
-            hyl, a.zeroJ);
+    ey_cell(a.f, kKindRegular, nullptr, ey.v[e], hx.v[e], hxl, hy.v[e], hyl, a.zeroJ);
+    if (kd[e] == kKindRegular) t.ey[o + e] = ey.v[e];
   }
-  stp<T, E>(t.ey + o, ey);
 }
 
-// One cell of the halo column (box column V - 1) for the first three phases.
+// One cell (box column c, row r) of a phase, of either kind; none is left alone.
 template <class T, class G, int PHASE>
-__device__ __forceinline__ void tile_halo(const YeeTileArgs<T> &a, const TileSm<T> &t, int r) {
-  constexpr int W = G::W, c = G::V - 1;
-  const uint8_t kd = t.k[r * G::KW + c + G::KO];
+__device__ __forceinline__ void tile_cell(const YeeTileArgs<T> &a, const TileSm<T> &t, uint8_t kd, int c, int r) {
+  constexpr int W = G::W;
   if (kd == kKindNone) return;
   const int o = r * W + c;
   const CutCellDev *cc = kd == kKindCut ? tile_cut<T, G>(a, t, c, r) : nullptr;
   if (PHASE == 2) ex_cell(a.f, kd, cc, t.ex[o], t.hx[o], t.hx[o - W], t.hy[o], t.hy[o - W], a.zeroJ);
+  else if (PHASE == 4) ey_cell(a.f, kd, cc, t.ey[o], t.hx[o], t.hx[o - 1], t.hy[o], t.hy[o - 1], a.zeroJ);
   else h_cell(a.f, kd, cc, t.hx[o], t.hy[o], t.ey[o], t.ey[o + 1], t.ex[o], t.ex[o + W]);
 }
 
+// The cut cells and the halo column of a phase over rows [rlo, rhi): the
+// cut cells from the tile's list (or, when the list overflowed, by a scan of
+// the kinds), the halo column's regular cells; run by the threads from
+// `first` on, which have the fewest rows in the row pass.
+template <class T, class G, int PHASE>
+__device__ __forceinline__ void tile_rest(const YeeTileArgs<T> &a, const TileSm<T> &t, const uint16_t *cuts, int ncut,
+                                          int rlo, int rhi, int first) {
+  const int tid = (int)threadIdx.x - first, nt = G::THREADS - first;
+  if (tid < 0) return;
+  constexpr int clo = PHASE == 4 ? G::V : G::V - 1;
+  if (ncut <= G::CUTS) {
+    for (int n = tid; n < ncut; n += nt) {
+      const int c = cuts[n] & 0x7f, r = cuts[n] >> 7;
+      if (r >= rlo && r < rhi && c >= clo) tile_cell<T, G, PHASE>(a, t, kKindCut, c, r);
+    }
+  } else {  // more cut cells than the list holds: scan the phase's cells
+    constexpr int CW = G::V + G::TX - clo;
+    for (int k = tid; k < CW * (rhi - rlo); k += nt) {
+      const int c = clo + k % CW, r = rlo + k / CW;
+      if (t.k[r * G::KW + c + G::KO] == kKindCut) tile_cell<T, G, PHASE>(a, t, kKindCut, c, r);
+    }
+  }
+  if (PHASE != 4)
+    for (int r = rlo + tid; r < rhi; r += nt) {
+      constexpr int c = G::V - 1;
+      if (t.k[r * G::KW + c + G::KO] == kKindRegular) tile_cell<T, G, PHASE>(a, t, kKindRegular, c, r);
+    }
+}
+
 template <class T>
-__global__ void __launch_bounds__(256) k_yee_tiles(const __grid_constant__ YeeTileArgs<T> a) {
+__global__ void __launch_bounds__(256, 5) k_yee_tiles(const __grid_constant__ YeeTileArgs<T> a) {
   using G = YeeTile<T>;
   extern __shared__ uint8_t smem_raw[];
+  __shared__ int s_ncut;
   uint8_t *base = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~(uintptr_t)127);
   T *sEx = reinterpret_cast<T *>(base);
   T *sEy = reinterpret_cast<T *>(base + G::PLANE_BYTES);
@@ -759,12 +793,14 @@ __global__ void __launch_bounds__(256) k_yee_tiles(const __grid_constant__ YeeTi
   T *sHy = reinterpret_cast<T *>(base + 3 * G::PLANE_BYTES);
   uint8_t *sK = base + 4 * G::PLANE_BYTES;
   uint64_t *bar = reinterpret_cast<uint64_t *>(sK + G::KIND_BYTES);
+  uint16_t *cuts = reinterpret_cast<uint16_t *>(sK + G::KIND_BYTES + 16);
   const FieldArgsT<T> &f = a.f;
   const int s0 = (int)(blockIdx.x % (unsigned)a.tilesX) * G::TX;
   const int y0 = (int)(blockIdx.x / (unsigned)a.tilesX) * G::TY;
   if (threadIdx.x == 0) {
     mbar_init(bar, 1);
     mbar_init_fence();
+    s_ncut = 0;
   }
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -786,21 +822,36 @@ __global__ void __launch_bounds__(256) k_yee_tiles(const __grid_constant__ YeeTi
     }
     return;
   }
-  // box column c, row r is cell (s0 - V - 1 + c, y0 - 1 + r); each lane takes
-  // E consecutive cells of a row of the tile's TX columns [V, V + TX), the
-  // halo column V - 1 (phases 1-3) goes to the last two warps
+  // box column c, row r is cell (s0 - V - 1 + c, y0 - 1 + r)
   const TileSm<T> t{sEx, sEy, sHx, sHy, sK, s0 - G::V - 1, y0 - 1};
-  const int warp = threadIdx.x >> 5, c = G::V + (threadIdx.x & 31) * G::E, th = threadIdx.x - 192;
+  // the tile's cut cells (columns [V - 1, V + TX), rows [0, TY + 2)), as 7-bit column | row << 7
+  {
+    constexpr int CW = G::TX + 1;
+    for (int k = threadIdx.x; k < CW * (G::TY + 2); k += G::THREADS) {
+      const int c = G::V - 1 + k % CW, r = k / CW;
+      if (sK[r * G::KW + c + G::KO] == kKindCut) {
+        const int n = atomicAdd(&s_ncut, 1);
+        if (n < G::CUTS) cuts[n] = (uint16_t)(c | r << 7);
+      }
+    }
+  }
+  __syncthreads();
+  const int ncut = s_ncut;
+  // each lane takes E consecutive cells of a row of the tile's TX columns
+  // [V, V + TX); the halo column V - 1 and the cut cells go to the warps
+  // from 2 on (34 rows over 8 warps leave warps 0 and 1 with the extra row)
+  const int warp = threadIdx.x >> 5, c = G::V + (threadIdx.x & 31) * G::E;
   for (int r = warp; r < G::TY + 2; r += 8) tile_h<T, G>(a, t, c, r);
-  if (th >= 0 && th < G::TY + 2) tile_halo<T, G, 1>(a, t, th);
+  tile_rest<T, G, 1>(a, t, cuts, ncut, 0, G::TY + 2, 64);
   __syncthreads();
   for (int r = 1 + warp; r < G::TY + 2; r += 8) tile_ex<T, G>(a, t, c, r);
-  if (th >= 0 && th < G::TY + 1) tile_halo<T, G, 2>(a, t, 1 + th);
+  tile_rest<T, G, 2>(a, t, cuts, ncut, 1, G::TY + 2, 64);
   __syncthreads();
   for (int r = 1 + warp; r < G::TY + 1; r += 8) tile_h<T, G>(a, t, c, r);
-  if (th >= 0 && th < G::TY) tile_halo<T, G, 3>(a, t, 1 + th);
+  tile_rest<T, G, 3>(a, t, cuts, ncut, 1, G::TY + 1, 0);
   __syncthreads();
   for (int r = 1 + warp; r < G::TY + 1; r += 8) tile_ey<T, G>(a, t, c, r);
+  tile_rest<T, G, 4>(a, t, cuts, ncut, 1, G::TY + 1, 0);
   __syncthreads();
   // the tile's cells, every one (unchanged ones too) except the fix-up's,
   // into the destination set: 16-byte pieces of storage columns [s0, s0 + TX)
@@ -834,7 +885,7 @@ __global__ void __launch_bounds__(256) k_yee_tiles(const __grid_constant__ YeeTi
 // cells the later sub-steps of the region read into scratch planes, runs the
 // static and window sub-steps and exchanges there in the order of the
 // sub-step kernels, and writes the region into the destination set.
-constexpr int kFixCtas = 8, kFixThreads = 512;
+constexpr int kFixCtas = 8, kFixThreads = 1024;
 
 template <class T>
 struct YeeFixArgs {
@@ -856,6 +907,19 @@ __device__ __forceinline__ void cluster_barrier() {
 
 __device__ __forceinline__ int exchange_items(int L0, int L1, int which) {
   return which == 0 ? 2 * (L0 + L1) + 4 : which == 1 ? 2 * L0 + 2 : 2 * L1 + 2;
+}
+
+// Half H of static cell (i, j) of the fix-up's scratch planes: every operand
+// is loaded before the kind decides (the loads overlap the kind's).
+template <class T, class Cut>
+__device__ __forceinline__ void fix_h(const FieldArgsT<T> &a, const FieldArgsT<T> &z, uint8_t kd, int i, int j,
+                                      const Cut &cut_of) {
+  T hx = z.Hx.at(i, j), hy = z.Hy.at(i, j);
+  const T ey0 = z.Ey.at(i, j), ey1 = z.Ey.at(i + 1, j), ex0 = z.Ex.at(i, j), ex1 = z.Ex.at(i, j + 1);
+  if (kd == kKindNone) return;
+  h_cell(a, kd, cut_of(kd, i, j), hx, hy, ey0, ey1, ex0, ex1);
+  z.Hx.at(i, j) = hx;
+  z.Hy.at(i, j) = hy;
 }
 
 template <class T>
@@ -906,10 +970,7 @@ __global__ void __cluster_dims__(kFixCtas, 1, 1) __launch_bounds__(kFixThreads)
     for (int k = tid; k < ns + nw; k += nth) {
       if (k >= ns) { window_h(a, k - ns); continue; }
       const int i = c0 - 1 + k % w, j = r0 - 1 + k / w;
-      const uint8_t kd = kind_of(i, j);
-      if (kd == kKindNone) continue;
-      h_cell(a, kd, cut_of(kd, i, j), z.Hx.at(i, j), z.Hy.at(i, j), z.Ey.at(i, j), z.Ey.at(i + 1, j), z.Ex.at(i, j),
-             z.Ex.at(i, j + 1));
+      fix_h(a, z, kind_of(i, j), i, j, cut_of);
     }
   }
   cluster_barrier();
@@ -922,9 +983,11 @@ __global__ void __cluster_dims__(kFixCtas, 1, 1) __launch_bounds__(kFixThreads)
       if (k >= ns) { window_e<T, 0>(a, k - ns); continue; }
       const int i = c0 - 1 + k % w, j = r0 + k / w;
       const uint8_t kd = kind_of(i, j);
+      T e = z.Ex.at(i, j);
+      const T hx = z.Hx.at(i, j), hxm = z.Hx.at(i, j - 1), hy = z.Hy.at(i, j), hym = z.Hy.at(i, j - 1);
       if (kd == kKindNone) continue;
-      ex_cell(a, kd, cut_of(kd, i, j), z.Ex.at(i, j), z.Hx.at(i, j), z.Hx.at(i, j - 1), z.Hy.at(i, j),
-              z.Hy.at(i, j - 1), x.zeroJ);
+      ex_cell(a, kd, cut_of(kd, i, j), e, hx, hxm, hy, hym, x.zeroJ);
+      z.Ex.at(i, j) = e;
     }
   }
   cluster_barrier();
@@ -936,10 +999,7 @@ __global__ void __cluster_dims__(kFixCtas, 1, 1) __launch_bounds__(kFixThreads)
     for (int k = tid; k < ns + nw; k += nth) {
       if (k >= ns) { window_h(a, k - ns); continue; }
       const int i = c0 - 1 + k % w, j = r0 + k / w;
-      const uint8_t kd = kind_of(i, j);
-      if (kd == kKindNone) continue;
-      h_cell(a, kd, cut_of(kd, i, j), z.Hx.at(i, j), z.Hy.at(i, j), z.Ey.at(i, j), z.Ey.at(i + 1, j), z.Ex.at(i, j),
-             z.Ex.at(i, j + 1));
+      fix_h(a, z, kind_of(i, j), i, j, cut_of);
     }
   }
   cluster_barrier();
@@ -951,9 +1011,11 @@ __global__ void __cluster_dims__(kFixCtas, 1, 1) __launch_bounds__(kFixThreads)
     for (int k = tid; k < ns; k += nth) {
       const int i = c0 + k % w, j = r0 + k / w;
       const uint8_t kd = kind_of(i, j);
+      T e = z.Ey.at(i, j);
+      const T hx = z.Hx.at(i, j), hxl = z.Hx.at(i - 1, j), hy = z.Hy.at(i, j), hyl = z.Hy.at(i - 1, j);
       if (kd == kKindNone) continue;
-      ey_cell(a, kd, cut_of(kd, i, j), z.Ey.at(i, j), z.Hx.at(i, j), z.Hx.at(i - 1, j), z.Hy.at(i, j),
-              z.Hy.at(i - 1, j), x.zeroJ);
+      ey_cell(a, kd, cut_of(kd, i, j), e, hx, hxl, hy, hyl, x.zeroJ);
+      z.Ey.at(i, j) = e;
     }
   }
   cluster_barrier();

@@ -142,7 +142,7 @@ template <int BN>
 __global__ void __launch_bounds__(kThreads) k_gemm(Seg g0, Seg g1, int M, int N, csrst_gemm_epilogue ep, int *err,
                                                    int o_mfast, int t_mfast, long long spin) {
   extern __shared__ __align__(1024) uint8_t smem[];
-  __shared__ uint64_t bar[2];
+  __shared__ uint64_t bar[3];  // MMA commits of the two stages; bar[2]: nothing arrives on it
   __shared__ uint32_t tmem_base;
   __shared__ int s_fail, s_last;  // a wait gave up; the last MMA commit issued
   constexpr int kA = kBM * kBK * 2, kB = BN * kBK * 2, kStage = kA + kB;
@@ -171,6 +171,7 @@ __global__ void __launch_bounds__(kThreads) k_gemm(Seg g0, Seg g1, int M, int N,
   if (threadIdx.x == 0) {
     mbar_init(&bar[0], 1);
     mbar_init(&bar[1], 1);
+    mbar_init(&bar[2], 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     s_fail = 0;
     s_last = -1;
@@ -180,6 +181,10 @@ __global__ void __launch_bounds__(kThreads) k_gemm(Seg g0, Seg g1, int M, int N,
   asm volatile("tcgen05.fence::after_thread_sync;");
   const uint32_t tmem = tmem_base;
   const int nk = g0.nk + g1.nk;
+  // spin < 0: the first wait in the loop is on bar[2], which nothing
+  // completes, with -spin polls (the stuck wait the error path is tested with)
+  const bool stuck = spin < 0;
+  if (stuck) spin = -spin;
 
   load_k(base, 0);
   cp_async_commit();
@@ -188,7 +193,11 @@ __global__ void __launch_bounds__(kThreads) k_gemm(Seg g0, Seg g1, int M, int N,
     if (kt + 1 < nk) {
       const int s1 = (kt + 1) & 1;
       if (kt >= 1) {  // the MMAs of tile kt - 1 still read stage s1
-        if (threadIdx.x == 0 && !mbar_wait(&bar[s1], ((kt - 1) >> 1) & 1, spin)) { s_fail = 1; s_last = kt - 1; }
+        uint64_t *wb = stuck && kt == 1 ? &bar[2] : &bar[s1];
+        if (threadIdx.x == 0 && !mbar_wait(wb, stuck && kt == 1 ? 0u : ((kt - 1) >> 1) & 1, spin)) {
+          s_fail = 1;
+          s_last = kt - 1;
+        }
         __syncthreads();
         if (s_fail) break;
       }
@@ -380,7 +389,7 @@ int gemm_dispatch(const Seg &g0, const Seg &g1, int M, int N, int batch, const c
 }  // namespace csrst
 
 extern "C" int csrst_gemm_set_wait_limit(long long polls) {
-  csrst::g_wait_polls = polls > 0 ? polls : csrst::kSpin;
+  csrst::g_wait_polls = polls != 0 ? polls : csrst::kSpin;
   return CSRST_OK;
 }
 

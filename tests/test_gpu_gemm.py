@@ -77,12 +77,13 @@ def test_gemm_dual_segments_and_row_bias(gpu_lib):
 
 
 def test_gemm_wait_that_gives_up_reports_and_recovers(gpu_lib):
-    """The tensor-core waits are bounded.  With a limit of one poll the first
-    wait for an MMA commit gives up: the GEMM reports it through its error
-    word (1: a wait gave up, and its clean-up wait for the issued MMAs
-    succeeded), writes nothing, and returns; with the default limit restored
-    the same GEMM is correct again, so the context and the TMEM allocator are
-    intact."""
+    """The tensor-core waits are bounded.  With the stuck-wait hook (a
+    negative limit: the first wait in the K loop is on a barrier nothing
+    completes, 1000 polls) the wait gives up: the GEMM reports it through its
+    error word (1: a wait gave up, and its clean-up wait for the MMAs it had
+    issued succeeded), writes nothing, and returns; with the default limit
+    restored the same GEMM is correct again, so the context and the TMEM
+    allocator are intact."""
     import torch
     from csrst_b200._lib import lib
     from csrst_b200.tensor import _err, gemm
@@ -90,10 +91,10 @@ def test_gemm_wait_that_gives_up_reports_and_recovers(gpu_lib):
     M, N, K = 256, 128, 512            # 8 K tiles: waits inside the loop and after it
     a, b = bf16(rng, (M, K)), bf16(rng, (N, K))
     out = torch.full((M, N), 7.0, dtype=torch.float32, device="cuda")
-    err = _err(torch.device("cuda"))
+    err = _err(torch.device("cuda", torch.cuda.current_device()))
     err.zero_()
     try:
-        lib().csrst_gemm_set_wait_limit(1)
+        lib().csrst_gemm_set_wait_limit(-1000)
         gemm(a.cuda(), b.cuda(), M, N, K, out32=out)
         torch.cuda.synchronize()
     finally:
