@@ -15,6 +15,8 @@
 // reads what it writes.
 #include <cuda.h>
 
+#include <algorithm>
+
 #include "kernels.cuh"
 #include "tma.cuh"
 
@@ -359,59 +361,96 @@ template <class T>
 __global__ void k_check_window(FieldArgsT<T> a) { check_window_clear(a, a.ws); }
 
 // Window move (moveMesh, main.cpp:562-652, and exchangeBoundariesMovingMesh,
-// Communicator.cpp:123-642).  One CTA: reads the last deposit's particle
-// bounds, shifts the window by whole cells through a scratch copy, updates
-// the window position and origin, then refreshes the strips.
+// Communicator.cpp:123-642): from the last deposit's particle bounds the
+// window shifts by whole cells through a scratch copy, its position and
+// origin are updated and the strips refreshed.
 
+// The move of the window (main.cpp:567-600): ok, whole-cell shift (moveI in
+// x, dj in y) and the error code when the bunch no longer fits or would move
+// too far.  Reads only the bounds, so every CTA of a launch can take it.
+struct MoveDecision {
+  int ok, moveI, dj, err;
+};
+__device__ __forceinline__ MoveDecision move_decision(const WinState *ws, int L0, int L1) {
+  MoveDecision r{1, 0, 0, kOk};
+  const int L[2] = {L0, L1};
+  int ideal1[2] = {0, 0};
+  for (int d = 0; d < 2; ++d) {
+    const int len = ws->gb[2 * d + 1] - ws->gb[2 * d] + 1;
+    if (len >= L[d]) { r.ok = 0; r.err = kErrWindowFit; return r; }
+    const unsigned diff = (unsigned)(L[d] - len);
+    const unsigned up = (unsigned)floor(diff / 2.0);
+    ideal1[d] = L[d] - (int)up - 2;
+  }
+  r.moveI = ws->gb[1] - ideal1[0] - 1;
+  r.dj = ws->gb[3] - ideal1[1] - 1;
+  if (r.moveI < 0 || r.moveI > 1 || r.dj < -1 || r.dj > 1) { r.ok = 0; r.err = kErrWindowMove; }
+  return r;
+}
+
+// Window plane f (0 Ex, 1 Ey, 2 Hzx, 3 Hzy, 4 Jx, 5 Jy).
+template <class T>
+__device__ __forceinline__ const PlaneT<T> &wplane_of(const FieldArgsT<T> &a, int f) {
+  return f == 0 ? a.mEx : f == 1 ? a.mEy : f == 2 ? a.mHx : f == 3 ? a.mHy : f == 4 ? a.mJx : a.mJy;
+}
+
+// Phase A (stage 0: the window planes into scratch) or phase B (stage 1: the
+// shifted copy back, over the reference's loop ranges) of a move, items
+// [tid, ...) in steps of nth.
+template <class T>
+__device__ __forceinline__ void move_copy(const MoveArgs<T> &m, int moveI, int m1, int stage, int tid, int nth) {
+  const FieldArgsT<T> &a = m.f;
+  const int W0 = a.L0 + 2, W1 = a.L1 + 2, np = W0 * W1;
+  if (stage == 0) {
+    for (int k = tid; k < 6 * np; k += nth) {
+      const int f = k / np, r = k % np;
+      m.scratch[k] = wplane_of(a, f).p[r];
+    }
+    return;
+  }
+  const int i0 = -moveI, i1 = a.L0 - 1;
+  int j0 = -(m1 > 0 ? m1 : 0), j1 = a.L1 - 1 - (m1 < 0 ? m1 : 0);
+  if (m1 == 0) { j0 -= 1; j1 += 1; }
+  const int ni = i1 - i0 + 1, cnt = ni * (j1 - j0 + 1);
+  for (int k = tid; k < 6 * cnt; k += nth) {
+    const int f = k / cnt, r = k % cnt;
+    const int i = i0 + r % ni, j = j0 + r / ni;
+    wplane_of(a, f).at(i, j) = m.scratch[(size_t)f * np + (size_t)(j + m1 + 1) * W0 + (i + moveI + 1)];
+  }
+}
+
+template <class T>
+__device__ __forceinline__ void move_finish(const MoveArgs<T> &m, int moveI, int m1);
+
+// The whole move in one CTA (batched ensembles: one CTA per member).
 template <class T>
 __device__ __forceinline__ void move_body(const MoveArgs<T> &m) {
   const FieldArgsT<T> &a = m.f;
   WinState *ws = a.ws;
   if (ws->err) return;
-  const int L[2] = {a.L0, a.L1};
   __shared__ int s_move[3];
   if (threadIdx.x == 0) {
-    int ok = 1, ideal1[2];
-    for (int d = 0; d < 2; ++d) {
-      const int len = ws->gb[2 * d + 1] - ws->gb[2 * d] + 1;
-      if (len >= L[d]) { ok = 0; break; }
-      const unsigned diff = (unsigned)(L[d] - len);
-      const unsigned up = (unsigned)floor(diff / 2.0);
-      ideal1[d] = L[d] - (int)up - 2;
-    }
-    int moveI = 0, dj = 0;
-    if (!ok) set_err(ws, kErrWindowFit);
-    else {
-      moveI = ws->gb[1] - ideal1[0] - 1;
-      dj = ws->gb[3] - ideal1[1] - 1;
-      if (moveI < 0 || moveI > 1 || dj < -1 || dj > 1) { set_err(ws, kErrWindowMove); ok = 0; }
-    }
-    s_move[0] = ok; s_move[1] = moveI; s_move[2] = dj;
-    if (ok) { ws->moves[0] = moveI; ws->moves[1] = dj; }
+    const MoveDecision d = move_decision(ws, a.L0, a.L1);
+    if (!d.ok) set_err(ws, d.err);
+    s_move[0] = d.ok; s_move[1] = d.moveI; s_move[2] = d.dj;
+    if (d.ok) { ws->moves[0] = d.moveI; ws->moves[1] = d.dj; }
   }
   __syncthreads();
   if (!s_move[0]) return;
   const int moveI = s_move[1], m1 = s_move[2];
   if (moveI == 0 && m1 == 0) return;
-  const int W0 = a.L0 + 2, W1 = a.L1 + 2, np = W0 * W1;
-  const PlaneT<T> *pl[6] = {&a.mEx, &a.mEy, &a.mHx, &a.mHy, &a.mJx, &a.mJy};
-  // phase A: snapshot
-  for (int k = threadIdx.x; k < 6 * np; k += blockDim.x) {
-    const int f = k / np, r = k % np;
-    m.scratch[k] = pl[f]->p[r];
-  }
+  move_copy(m, moveI, m1, 0, threadIdx.x, blockDim.x);
   __syncthreads();
-  // phase B: shifted copy over the reference's loop ranges
-  const int i0 = -moveI, i1 = a.L0 - 1;
-  int j0 = -(m1 > 0 ? m1 : 0), j1 = a.L1 - 1 - (m1 < 0 ? m1 : 0);
-  if (m1 == 0) { j0 -= 1; j1 += 1; }
-  const int ni = i1 - i0 + 1, cnt = ni * (j1 - j0 + 1);
-  for (int k = threadIdx.x; k < 6 * cnt; k += blockDim.x) {
-    const int f = k / cnt, r = k % cnt;
-    const int i = i0 + r % ni, j = j0 + r / ni;
-    pl[f]->at(i, j) = m.scratch[(size_t)f * np + (size_t)(j + m1 + 1) * W0 + (i + moveI + 1)];
-  }
+  move_copy(m, moveI, m1, 1, threadIdx.x, blockDim.x);
   __syncthreads();
+  move_finish(m, moveI, m1);
+}
+
+// Position, origin and strips after the shifted copy (one CTA).
+template <class T>
+__device__ __forceinline__ void move_finish(const MoveArgs<T> &m, int moveI, int m1) {
+  const FieldArgsT<T> &a = m.f;
+  WinState *ws = a.ws;
   if (threadIdx.x == 0) {
     ws->P0 += moveI; ws->P1 += m1;
     ws->mo0 += moveI * m.h0;
@@ -541,8 +580,8 @@ enum : uint8_t { kKindNone = 0, kKindRegular = 1, kKindCut = 2 };
 // Updates of one static cell, shared by the tile and the fix-up kernels: the
 // same expressions as the sub-step kernels' regular-cell and cut-cell
 // branches (TETMSolver.hh:142-206, :241-261; SCBoundaryCondition.hh:391-431).
-template <class T>
-__device__ __forceinline__ void h_cell(const FieldArgsT<T> &a, uint8_t kind, const CutCellDev *cc, T &hx, T &hy,
+template <class T, class A>
+__device__ __forceinline__ void h_cell(const A &a, uint8_t kind, const CutCellDev *cc, T &hx, T &hy,
                                        T ey0, T ey1, T ex0, T ex1) {
   if (kind == kKindRegular) {
     hx = hx - a.chx * (ey1 - ey0);
@@ -557,8 +596,8 @@ __device__ __forceinline__ void h_cell(const FieldArgsT<T> &a, uint8_t kind, con
 }
 
 // Ex of one static cell; hxm, hym: H of the cell below.
-template <class T>
-__device__ __forceinline__ void ex_cell(const FieldArgsT<T> &a, uint8_t kind, const CutCellDev *cc, T &e, T hx, T hxm,
+template <class T, class A>
+__device__ __forceinline__ void ex_cell(const A &a, uint8_t kind, const CutCellDev *cc, T &e, T hx, T hxm,
                                         T hy, T hym, T zeroJ) {
   if (kind == kKindRegular) {
     e = e + (a.kex * (hx - hxm + hy - hym) - a.dteps * zeroJ);
@@ -571,8 +610,8 @@ __device__ __forceinline__ void ex_cell(const FieldArgsT<T> &a, uint8_t kind, co
 }
 
 // Ey of one static cell; hxl, hyl: H of the cell to the left.
-template <class T>
-__device__ __forceinline__ void ey_cell(const FieldArgsT<T> &a, uint8_t kind, const CutCellDev *cc, T &e, T hx, T hxl,
+template <class T, class A>
+__device__ __forceinline__ void ey_cell(const A &a, uint8_t kind, const CutCellDev *cc, T &e, T hx, T hxl,
                                         T hy, T hyl, T zeroJ) {
   if (kind == kKindRegular) {
     e = e - (a.key * (hx - hxl + hy - hyl) + a.dteps * zeroJ);
@@ -661,6 +700,13 @@ struct TileSm {
   int i0, j0;
 };
 
+// The coefficients in registers (h_cell / ex_cell / ey_cell read them by
+// name, as from FieldArgsT; the row passes use only the regular ones).
+template <class T>
+struct Coef {
+  T chx, chy, kex, key, dteps, mhx, mhy, de, h0, h1;
+};
+
 template <class T, class G>
 __device__ __forceinline__ const CutCellDev *tile_cut(const YeeTileArgs<T> &a, const TileSm<T> &t, int c, int r) {
   return a.f.cells + a.cutidx[(size_t)(t.j0 + r) * a.f.Nx + (t.i0 + c)];
@@ -672,34 +718,50 @@ __device__ __forceinline__ const CutCellDev *tile_cut(const YeeTileArgs<T> &a, c
 // halo-column cells their own pass, so that no store of one pass covers a
 // cell another pass of the same phase writes.
 
-// Half H, regular cells [c, c + E) of row r.
+// Stores a piece back: whole when every cell is regular, else the regular
+// cells one by one.
+template <class T, int E>
+__device__ __forceinline__ void store_regular(T *p, const Pack<T, E> &x, const uint8_t *kd) {
+  bool all = true;
+#pragma unroll
+  for (int e = 0; e < E; ++e) all &= kd[e] == kKindRegular;
+  if (all) {
+    stp<T, E>(p, x);
+    return;
+  }
+#pragma unroll
+  for (int e = 0; e < E; ++e)
+    if (kd[e] == kKindRegular) p[e] = x.v[e];
+}
+
+// Half H, regular cells [c, c + E) of row r (a warp takes a row: the cell
+// right of a lane's piece comes from the next lane).
 template <class T, class G>
-__device__ __forceinline__ void tile_h(const YeeTileArgs<T> &a, const TileSm<T> &t, int c, int r) {
+__device__ __forceinline__ void tile_h(const Coef<T> &k, const TileSm<T> &t, int c, int r) {
   constexpr int E = G::E, W = G::W;
-  const int o = r * W + c;
+  const int o = r * W + c, lane = threadIdx.x & 31;
   uint8_t kd[E];
   kinds<E>(t.k, r * G::KW + c + G::KO, kd);
   bool any = false;
 #pragma unroll
   for (int e = 0; e < E; ++e) any |= kd[e] == kKindRegular;
-  if (!any) return;
+  if (!__any_sync(0xffffffffu, any)) return;
   Pack<T, E> hx = ldp<T, E>(t.hx + o), hy = ldp<T, E>(t.hy + o);
   const Pack<T, E> ey = ldp<T, E>(t.ey + o), ex0 = ldp<T, E>(t.ex + o), ex1 = ldp<T, E>(t.ex + o + W);
-  const T eyn = t.ey[o + E];
+  T eyn = __shfl_down_sync(0xffffffffu, ey.v[0], 1);
+  if (lane == 31) eyn = t.ey[o + E];
 #pragma unroll
   for (int e = 0; e < E; ++e) {
     const T ey1 = e + 1 < E ? ey.v[e + 1 < E ? e + 1 : 0] : eyn;
-    h_cell(a.f, kKindRegular, nullptr, hx.v[e], hy.v[e], ey.v[e], ey1, ex0.v[e], ex1.v[e]);
-    if (kd[e] == kKindRegular) {
-      t.hx[o + e] = hx.v[e];
-      t.hy[o + e] = hy.v[e];
-    }
+    h_cell(k, kKindRegular, nullptr, hx.v[e], hy.v[e], ey.v[e], ey1, ex0.v[e], ex1.v[e]);
   }
+  store_regular<T, E>(t.hx + o, hx, kd);
+  store_regular<T, E>(t.hy + o, hy, kd);
 }
 
 // Ex, regular cells [c, c + E) of row r.
 template <class T, class G>
-__device__ __forceinline__ void tile_ex(const YeeTileArgs<T> &a, const TileSm<T> &t, int c, int r) {
+__device__ __forceinline__ void tile_ex(const Coef<T> &k, T zeroJ, const TileSm<T> &t, int c, int r) {
   constexpr int E = G::E, W = G::W;
   const int o = r * W + c;
   uint8_t kd[E];
@@ -712,32 +774,35 @@ __device__ __forceinline__ void tile_ex(const YeeTileArgs<T> &a, const TileSm<T>
   const Pack<T, E> hx = ldp<T, E>(t.hx + o), hxm = ldp<T, E>(t.hx + o - W);
   const Pack<T, E> hy = ldp<T, E>(t.hy + o), hym = ldp<T, E>(t.hy + o - W);
 #pragma unroll
-  for (int e = 0; e < E; ++e) {
-    ex_cell(a.f, kKindRegular, nullptr, ex.v[e], hx.v[e], hxm.v[e], hy.v[e], hym.v[e], a.zeroJ);
-    if (kd[e] == kKindRegular) t.ex[o + e] = ex.v[e];
-  }
+  for (int e = 0; e < E; ++e) ex_cell(k, kKindRegular, nullptr, ex.v[e], hx.v[e], hxm.v[e], hy.v[e], hym.v[e], zeroJ);
+  store_regular<T, E>(t.ex + o, ex, kd);
 }
 
-// Ey, regular cells [c, c + E) of row r.
+// Ey, regular cells [c, c + E) of row r (the cell left of a lane's piece
+// comes from the previous lane).
 template <class T, class G>
-__device__ __forceinline__ void tile_ey(const YeeTileArgs<T> &a, const TileSm<T> &t, int c, int r) {
+__device__ __forceinline__ void tile_ey(const Coef<T> &k, T zeroJ, const TileSm<T> &t, int c, int r) {
   constexpr int E = G::E, W = G::W;
-  const int o = r * W + c;
+  const int o = r * W + c, lane = threadIdx.x & 31;
   uint8_t kd[E];
   kinds<E>(t.k, r * G::KW + c + G::KO, kd);
   bool any = false;
 #pragma unroll
   for (int e = 0; e < E; ++e) any |= kd[e] == kKindRegular;
-  if (!any) return;
+  if (!__any_sync(0xffffffffu, any)) return;
   Pack<T, E> ey = ldp<T, E>(t.ey + o);
   const Pack<T, E> hx = ldp<T, E>(t.hx + o), hy = ldp<T, E>(t.hy + o);
-  const T hxl0 = t.hx[o - 1], hyl0 = t.hy[o - 1];
+  T hxl0 = __shfl_up_sync(0xffffffffu, hx.v[E - 1], 1), hyl0 = __shfl_up_sync(0xffffffffu, hy.v[E - 1], 1);
+  if (lane == 0) {
+    hxl0 = t.hx[o - 1];
+    hyl0 = t.hy[o - 1];
+  }
 #pragma unroll
   for (int e = 0; e < E; ++e) {
     const T hxl = e > 0 ? hx.v[e > 0 ? e - 1 : 0] : hxl0, hyl = e > 0 ? hy.v[e > 0 ? e - 1 : 0] : hyl0;
-    ey_cell(a.f, kKindRegular, nullptr, ey.v[e], hx.v[e], hxl, hy.v[e], hyl, a.zeroJ);
-    if (kd[e] == kKindRegular) t.ey[o + e] = ey.v[e];
+    ey_cell(k, kKindRegular, nullptr, ey.v[e], hx.v[e], hxl, hy.v[e], hyl, zeroJ);
   }
+  store_regular<T, E>(t.ey + o, ey, kd);
 }
 
 // One cell (box column c, row r) of a phase, of either kind; none is left alone.
@@ -841,16 +906,18 @@ __global__ void __launch_bounds__(256, 5) k_yee_tiles(const __grid_constant__ Ye
   // [V, V + TX); the halo column V - 1 and the cut cells go to the warps
   // from 2 on (34 rows over 8 warps leave warps 0 and 1 with the extra row)
   const int warp = threadIdx.x >> 5, c = G::V + (threadIdx.x & 31) * G::E;
-  for (int r = warp; r < G::TY + 2; r += 8) tile_h<T, G>(a, t, c, r);
+  const Coef<T> k{f.chx, f.chy, f.kex, f.key, f.dteps, f.mhx, f.mhy, f.de, f.h0, f.h1};
+  const T zeroJ = a.zeroJ;
+  for (int r = warp; r < G::TY + 2; r += 8) tile_h<T, G>(k, t, c, r);
   tile_rest<T, G, 1>(a, t, cuts, ncut, 0, G::TY + 2, 64);
   __syncthreads();
-  for (int r = 1 + warp; r < G::TY + 2; r += 8) tile_ex<T, G>(a, t, c, r);
+  for (int r = 1 + warp; r < G::TY + 2; r += 8) tile_ex<T, G>(k, zeroJ, t, c, r);
   tile_rest<T, G, 2>(a, t, cuts, ncut, 1, G::TY + 2, 64);
   __syncthreads();
-  for (int r = 1 + warp; r < G::TY + 1; r += 8) tile_h<T, G>(a, t, c, r);
+  for (int r = 1 + warp; r < G::TY + 1; r += 8) tile_h<T, G>(k, t, c, r);
   tile_rest<T, G, 3>(a, t, cuts, ncut, 1, G::TY + 1, 0);
   __syncthreads();
-  for (int r = 1 + warp; r < G::TY + 1; r += 8) tile_ey<T, G>(a, t, c, r);
+  for (int r = 1 + warp; r < G::TY + 1; r += 8) tile_ey<T, G>(k, zeroJ, t, c, r);
   tile_rest<T, G, 4>(a, t, cuts, ncut, 1, G::TY + 1, 0);
   __syncthreads();
   // the tile's cells, every one (unchanged ones too) except the fix-up's,
@@ -1059,6 +1126,34 @@ __global__ void k_exchange(FieldArgsT<T> a, int which) { exchange_body(a, which,
 template <class T>
 __global__ void __launch_bounds__(1024) k_move(MoveArgs<T> m) { move_body(m); }
 
+// The move of one member as three launches: the two copy phases over many
+// CTAs (each takes the decision itself; nothing it reads changes before the
+// last launch), then the decision's bookkeeping and the strips in one CTA.
+template <class T>
+__global__ void __launch_bounds__(256) k_move_copy(MoveArgs<T> m, int stage) {
+  const WinState *ws = m.f.ws;
+  if (ws->err) return;
+  const MoveDecision d = move_decision(ws, m.f.L0, m.f.L1);
+  if (!d.ok || (d.moveI == 0 && d.dj == 0)) return;
+  move_copy(m, d.moveI, d.dj, stage, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
+}
+
+template <class T>
+__global__ void __launch_bounds__(1024) k_move_finish(MoveArgs<T> m) {
+  WinState *ws = m.f.ws;
+  if (ws->err) return;
+  __shared__ int s_move[3];
+  if (threadIdx.x == 0) {
+    const MoveDecision d = move_decision(ws, m.f.L0, m.f.L1);
+    if (!d.ok) set_err(ws, d.err);
+    s_move[0] = d.ok; s_move[1] = d.moveI; s_move[2] = d.dj;
+    if (d.ok) { ws->moves[0] = d.moveI; ws->moves[1] = d.dj; }
+  }
+  __syncthreads();
+  if (!s_move[0] || (s_move[1] == 0 && s_move[2] == 0)) return;
+  move_finish(m, s_move[1], s_move[2]);
+}
+
 // Member of global block b: bpre holds the first block of every member (m + 1
 // entries).
 __device__ __forceinline__ int batch_member(const int *bpre, int m, int b) {
@@ -1170,7 +1265,10 @@ void launch_check_window(FieldArgsT<T> a, cudaStream_t s) { k_check_window<T><<<
 template <class T>
 void launch_move(FieldArgsT<T> a, T *scratch, double h0, double h1, cudaStream_t s) {
   MoveArgs<T> m{a, scratch, h0, h1};
-  k_move<T><<<1, 1024, 0, s>>>(m);
+  const int n = 6 * (a.L0 + 2) * (a.L1 + 2), g = std::min((n + 255) / 256, 592);
+  k_move_copy<T><<<g, 256, 0, s>>>(m, 0);
+  k_move_copy<T><<<g, 256, 0, s>>>(m, 1);
+  k_move_finish<T><<<1, 1024, 0, s>>>(m);
 }
 
 // Batched sub-steps over m members: args and bpre are device arrays (bpre:
