@@ -192,6 +192,16 @@ struct EnsPart {
   int *bpre_sub = nullptr, *bpre_ex[3] = {nullptr, nullptr, nullptr};
   int nsub = 0, nex[3] = {0, 0, 0};
   int push_grid = 0;
+  // the fused sweep (csrst_ensemble::fused): per plane-set parity p (p = 0:
+  // the members' sets as current at build time), the tile and fix-up tables
+  // reading the current set, the window-Ey (comp 1) and move arguments over
+  // the set current after the sweep; the members' first tiles; the blocks of
+  // the window-Ey launch; the work-queue counter
+  void *ytile[2] = {nullptr, nullptr}, *yfix[2] = {nullptr, nullptr};
+  void *fey[2] = {nullptr, nullptr}, *fmv[2] = {nullptr, nullptr};
+  int *tpre = nullptr, *bpre_ey = nullptr;
+  int ney = 0;
+  unsigned *queue = nullptr;
 };
 
 // A batch of members stepped together: every phase of the time step is one
@@ -205,9 +215,12 @@ struct csrst_ensemble {
   cudaStream_t s = nullptr;  // the ensemble's stream (graph launches, ordering with the members)
   cudaEvent_t done = nullptr, fork = nullptr;
   std::vector<EnsPart> parts;
-  // launch shapes (set by csrst_ensemble_set_shape / csrst_ensemble_tune)
-  int push_grid = 0, tx = 32, ty = 8, nparts = 1;
-  cudaGraphExec_t graph = nullptr;
+  // launch shapes (set by csrst_ensemble_set_shape / csrst_ensemble_tune);
+  // tx = ty = 0: the fused static sweep (one persistent launch per step)
+  int push_grid = 0, tx = 0, ty = 0, nparts = 1;
+  bool fused = false;        // the fused sweep is in use (shape and members allow it)
+  int epar = 0;              // plane-set swaps of the fused sweep since the tables were built, mod 2
+  cudaGraphExec_t graph[2] = {nullptr, nullptr};  // one step, per parity
   bool holds = false;        // the members' ens_refs count this ensemble
   std::string err;
 };
@@ -551,8 +564,10 @@ void moments_async(csrst_handle *h) {
                  h->s);
 }
 
-// Polls of a fused-sweep tile's staging wait before it gives up.
-constexpr long long kStagingPolls = 1ll << 22;
+// Polls of a fused-sweep tile's staging wait before it gives up
+// (csrst_set_staging_wait_limit; negative: the stuck-wait hook).
+constexpr long long kStagingDefault = 1ll << 22;
+long long g_staging_polls = kStagingDefault;
 
 // The fused static sweep runs unless something needs the sub-step kernels:
 // absorbing layers, an ensemble whose tables hold this handle's planes, or
@@ -576,11 +591,11 @@ int fused_fields_async(csrst_handle *h) {
     const PlaneT<float> dst[4] = {{h->ExfB, h->pitch32}, {h->EyfB, h->pitch32}, {h->HxfB, h->pitch32},
                                   {h->HyfB, h->pitch32}};
     rc = launch_yee_fused(field_args32(h, 0), dst, h->kind, h->kpitch, h->cutidx, static_cast<float *>(h->zfix),
-                          h->zpitch, h->zrows, kStagingPolls, h->s, h->s2, h->fork, h->join);
+                          h->zpitch, h->zrows, g_staging_polls, h->s, h->s2, h->fork, h->join);
   } else {
     const Plane dst[4] = {{h->ExB, h->pitch}, {h->EyB, h->pitch}, {h->HxB, h->pitch}, {h->HyB, h->pitch}};
     rc = launch_yee_fused(field_args(h, 0), dst, h->kind, h->kpitch, h->cutidx, static_cast<double *>(h->zfix),
-                          h->zpitch, h->zrows, kStagingPolls, h->s, h->s2, h->fork, h->join);
+                          h->zpitch, h->zrows, g_staging_polls, h->s, h->s2, h->fork, h->join);
   }
   if (rc != kOk) return fail(h, rc == kErrArg ? CSRST_E_ARG : CSRST_E_CUDA, "fused field sweep: tensor-map set-up");
   h->acc_fresh[0] = false;
@@ -690,7 +705,12 @@ int csrst_create(const csrst_config *cfg, csrst_handle **out) {
   };
   cudaError_t e;
   if ((e = cudaStreamCreateWithFlags(&h->s, cudaStreamNonBlocking)) != cudaSuccess) return bad(e, "stream");
-  if ((e = cudaStreamCreateWithFlags(&h->s2, cudaStreamNonBlocking)) != cudaSuccess) return bad(e, "stream");
+  {  // the window fix-up's stream at the highest priority: its cluster starts ahead of the sweep's tiles
+    int least = 0, greatest = 0;
+    if ((e = cudaDeviceGetStreamPriorityRange(&least, &greatest)) != cudaSuccess) return bad(e, "stream");
+    if ((e = cudaStreamCreateWithPriority(&h->s2, cudaStreamNonBlocking, greatest)) != cudaSuccess)
+      return bad(e, "stream");
+  }
   if ((e = cudaEventCreateWithFlags(&h->fork, cudaEventDisableTiming)) != cudaSuccess) return bad(e, "event");
   if ((e = cudaEventCreateWithFlags(&h->join, cudaEventDisableTiming)) != cudaSuccess) return bad(e, "event");
   const int Nx = cfg->Nx, Ny = cfg->Ny;
@@ -1275,6 +1295,11 @@ int csrst_step(csrst_handle *h, int nsteps) {
   return CSRST_OK;
 }
 
+int csrst_set_staging_wait_limit(long long polls) {
+  g_staging_polls = polls != 0 ? polls : kStagingDefault;
+  return CSRST_OK;
+}
+
 int csrst_step_timed(csrst_handle *h, double *ms4) {
   int rc = need_bunch(h);
   if (rc) return rc;
@@ -1420,6 +1445,13 @@ void part_free(EnsPart &P) {
   for (void *p : P.blocks) cudaFree(p);
   P.blocks.clear();
   cudaFree(P.mv64); cudaFree(P.mv32); cudaFree(P.prep); cudaFree(P.bpre_sub);
+  for (int k = 0; k < 2; ++k) {
+    cudaFree(P.ytile[k]); cudaFree(P.yfix[k]); cudaFree(P.fey[k]); cudaFree(P.fmv[k]);
+    P.ytile[k] = P.yfix[k] = P.fey[k] = P.fmv[k] = nullptr;
+  }
+  cudaFree(P.tpre); cudaFree(P.bpre_ey); cudaFree(P.queue);
+  P.tpre = P.bpre_ey = nullptr;
+  P.queue = nullptr;
   for (int k = 0; k < 3; ++k) { cudaFree(P.bpre_ex[k]); P.bpre_ex[k] = nullptr; }
   P.mv64 = nullptr; P.mv32 = nullptr; P.prep = nullptr; P.bpre_sub = nullptr;
   if (P.fork) cudaEventDestroy(P.fork);
@@ -1435,13 +1467,74 @@ void ensemble_free_tables(csrst_ensemble *e) {
   if (e->s) cudaStreamSynchronize(e->s);
   for (EnsPart &P : e->parts) part_free(P);
   e->parts.clear();
-  if (e->graph) { cudaGraphExecDestroy(e->graph); e->graph = nullptr; }
+  for (cudaGraphExec_t &g : e->graph)
+    if (g) { cudaGraphExecDestroy(g); g = nullptr; }
 }
 
 int efail(csrst_ensemble *e, int code, const std::string &msg) {
   if (e) e->err = msg;
   else g_create_error = msg;
   return code;
+}
+
+// The fused sweep's tables of one part, for both plane-set parities: parity
+// 0 reads the sets current now and writes the others, parity 1 the reverse;
+// the window-Ey and move arguments are those of the set written.
+template <class T>
+cudaError_t part_build_fused_t(csrst_ensemble *e, EnsPart &P) {
+  const int m = P.m;
+  const size_t tb = yee_batch_bytes<T>(0), fb = yee_batch_bytes<T>(1);
+  std::vector<uint8_t> tile[2], fix[2];
+  std::vector<FieldArgsT<T>> fey[2];
+  std::vector<MoveArgs<T>> fmv[2];
+  std::vector<int> tpre(1, 0), bey(1, 0);
+  for (int p = 0; p < 2; ++p) { tile[p].resize(tb * m); fix[p].resize(fb * m); }
+  cudaError_t err = cudaSuccess;
+  for (int k = 0; k < m && err == cudaSuccess; ++k) {
+    csrst_handle *h = P.mem[k];
+    for (int p = 0; p < 2; ++p) {  // each pass ends with the sets swapped: two passes restore them
+      FieldArgsT<T> a;
+      PlaneT<T> dst[4];
+      if constexpr (sizeof(T) == 4) {
+        a = field_args32(h, 0);
+        dst[0] = {h->ExfB, h->pitch32}; dst[1] = {h->EyfB, h->pitch32};
+        dst[2] = {h->HxfB, h->pitch32}; dst[3] = {h->HyfB, h->pitch32};
+      } else {
+        a = field_args(h, 0);
+        dst[0] = {h->ExB, h->pitch}; dst[1] = {h->EyB, h->pitch}; dst[2] = {h->HxB, h->pitch}; dst[3] = {h->HyB, h->pitch};
+      }
+      int nt = 0;
+      const int rc = yee_batch_entry<T>(a, dst, h->kind, h->kpitch, h->cutidx, static_cast<T *>(h->zfix), h->zpitch,
+                                        h->zrows, g_staging_polls, tile[p].data() + tb * k, fix[p].data() + fb * k,
+                                        &nt);
+      if (rc != kOk) err = cudaErrorInvalidValue;
+      if (p == 0) tpre.push_back(tpre.back() + nt);
+      swap_sets(h);
+      if constexpr (sizeof(T) == 4) {
+        fey[p].push_back(field_args32(h, 1));
+        fmv[p].push_back(MoveArgs<float>{field_args32(h, 0), h->scratchf, h->b.hr0, h->b.hr1});
+      } else {
+        fey[p].push_back(field_args(h, 1));
+        fmv[p].push_back(MoveArgs<double>{field_args(h, 0), h->scratch, h->b.hr0, h->b.hr1});
+      }
+    }
+    bey.push_back(bey.back() + (h->L0 * h->L1 + h->L1 + 2 + 255) / 256);
+  }
+  for (int p = 0; p < 2; ++p) {
+    P.ytile[p] = dev_copy(tile[p], err);
+    P.yfix[p] = dev_copy(fix[p], err);
+    P.fey[p] = dev_copy(fey[p], err);
+    P.fmv[p] = dev_copy(fmv[p], err);
+  }
+  P.tpre = dev_copy(tpre, err);
+  P.bpre_ey = dev_copy(bey, err);
+  P.ney = bey.back();
+  if (err == cudaSuccess) err = cudaMalloc(&P.queue, sizeof(unsigned));
+  return err;
+}
+
+cudaError_t part_build_fused(csrst_ensemble *e, EnsPart &P) {
+  return e->fp32 ? part_build_fused_t<float>(e, P) : part_build_fused_t<double>(e, P);
 }
 
 // Argument tables of the steady-state step (pending drift, current boxes) of
@@ -1524,6 +1617,7 @@ cudaError_t part_build(csrst_ensemble *e, EnsPart &P) {
   P.bpre_sub = dev_copy(bsub, err);
   for (int k = 0; k < 3; ++k) { P.bpre_ex[k] = dev_copy(bex[k], err); P.nex[k] = bex[k].back(); }
   P.nsub = bsub.back();
+  if (e->fused && err == cudaSuccess) err = part_build_fused(e, P);
   if (err == cudaSuccess) err = cudaStreamCreateWithFlags(&P.s, cudaStreamNonBlocking);
   if (err == cudaSuccess) err = cudaStreamCreateWithFlags(&P.s2, cudaStreamNonBlocking);
   if (err == cudaSuccess) err = cudaEventCreateWithFlags(&P.fork, cudaEventDisableTiming);
@@ -1536,6 +1630,11 @@ cudaError_t part_build(csrst_ensemble *e, EnsPart &P) {
 // first, each to the lightest part) and builds their tables.
 int ensemble_build(csrst_ensemble *e) {
   ensemble_free_tables(e);
+  // the fused sweep when the shape asks for it and every member allows it
+  e->fused = e->tx == 0 && e->ty == 0;
+  for (csrst_handle *h : e->mem)
+    e->fused = e->fused && h->zfix && h->kind && !h->pml && !(h->cfg.flags & CSRST_FLAG_SUBSTEP_FIELDS);
+  e->epar = 0;
   if (e->push_grid <= 0) {
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
@@ -1594,6 +1693,17 @@ void part_push(csrst_ensemble *e, EnsPart &P, int jcomp) {
 }
 
 template <class T>
+void part_fields_fused(const csrst_ensemble *e, EnsPart &P, int half) {
+  const int p = e->epar;
+  if (half == 0) {  // the static sweep of the whole step and the window's half H, Ex, half H
+    launch_yee_batch<T>(P.ytile[p], P.yfix[p], P.tpre, P.m, P.queue, P.s);
+  } else {          // the window's Ey (after the second push), then the window move
+    launch_window_ey_batch<T>(static_cast<const FieldArgsT<T> *>(P.fey[p]), P.bpre_ey, P.m, P.ney, P.s);
+    launch_move_batch<T>(static_cast<const MoveArgs<T> *>(P.fmv[p]), P.m, P.s);
+  }
+}
+
+template <class T>
 void part_fields(EnsPart &P, const FieldArgsT<T> *a0, const FieldArgsT<T> *a1, const MoveArgs<T> *mv, int half) {
   if (half == 0) {  // half H, Ex, half H (after the first push)
     launch_half_h_batch(a0, P.bpre_sub, P.m, P.nsub, P.s);
@@ -1609,21 +1719,33 @@ void part_fields(EnsPart &P, const FieldArgsT<T> *a0, const FieldArgsT<T> *a1, c
   }
 }
 
+// The host's view of a fused step: every member's plane sets swap.
+void ensemble_swap(csrst_ensemble *e) {
+  for (csrst_handle *h : e->mem) swap_sets(h);
+  e->epar ^= 1;
+}
+
 // One steady-state time step of every member (main.cpp:390-506), all parts
 // side by side, joined back on the ensemble stream.
 void ensemble_step_async(csrst_ensemble *e) {
   cudaEventRecord(e->fork, e->s);
   for (EnsPart &P : e->parts) {
     cudaStreamWaitEvent(P.s, e->fork, 0);
-    part_push(e, P, 0);
-    if (e->fp32) part_fields(P, P.f32[0], P.f32[1], P.mv32, 0);
-    else part_fields(P, P.f64[0], P.f64[1], P.mv64, 0);
-    part_push(e, P, 1);
-    if (e->fp32) part_fields(P, P.f32[0], P.f32[1], P.mv32, 1);
-    else part_fields(P, P.f64[0], P.f64[1], P.mv64, 1);
+    for (int half = 0; half < 2; ++half) {
+      part_push(e, P, half);
+      if (e->fused) {
+        if (e->fp32) part_fields_fused<float>(e, P, half);
+        else part_fields_fused<double>(e, P, half);
+      } else if (e->fp32) {
+        part_fields(P, P.f32[0], P.f32[1], P.mv32, half);
+      } else {
+        part_fields(P, P.f64[0], P.f64[1], P.mv64, half);
+      }
+    }
     cudaEventRecord(P.end, P.s);
     cudaStreamWaitEvent(e->s, P.end, 0);
   }
+  if (e->fused) ensemble_swap(e);
 }
 
 // Brings every member to the steady state of the loop (the stored positions
@@ -1733,18 +1855,22 @@ int csrst_ensemble_step(csrst_ensemble *e, int nsteps) {
   int rc = ensemble_steady(e, nsteps);
   if (rc) return rc;
   if (nsteps > 0) {
-    if (!e->graph) {
-      cudaGraph_t g;
-      if (cudaStreamBeginCapture(e->s, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
-        return efail(e, CSRST_E_CUDA, "ensemble graph capture");
-      ensemble_step_async(e);
-      if (cudaStreamEndCapture(e->s, &g) != cudaSuccess) return efail(e, CSRST_E_CUDA, "ensemble graph capture");
-      const cudaError_t c = cudaGraphInstantiate(&e->graph, g, 0);
-      cudaGraphDestroy(g);
-      if (c != cudaSuccess) return efail(e, CSRST_E_CUDA, std::string("ensemble graph: ") + cudaGetErrorString(c));
+    for (int k = 0; k < nsteps; ++k) {
+      const int p = e->epar;
+      if (!e->graph[p]) {  // recorded on the first step from this parity (the recording swaps the host's view)
+        cudaGraph_t g;
+        if (cudaStreamBeginCapture(e->s, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+          return efail(e, CSRST_E_CUDA, "ensemble graph capture");
+        ensemble_step_async(e);
+        if (cudaStreamEndCapture(e->s, &g) != cudaSuccess) return efail(e, CSRST_E_CUDA, "ensemble graph capture");
+        const cudaError_t c = cudaGraphInstantiate(&e->graph[p], g, 0);
+        cudaGraphDestroy(g);
+        if (c != cudaSuccess) return efail(e, CSRST_E_CUDA, std::string("ensemble graph: ") + cudaGetErrorString(c));
+      } else if (e->fused) {
+        ensemble_swap(e);
+      }
+      if (cudaGraphLaunch(e->graph[p], e->s) != cudaSuccess) return efail(e, CSRST_E_CUDA, "ensemble graph launch");
     }
-    for (int k = 0; k < nsteps; ++k)
-      if (cudaGraphLaunch(e->graph, e->s) != cudaSuccess) return efail(e, CSRST_E_CUDA, "ensemble graph launch");
     ensemble_mark(e);
   }
   return ensemble_release(e);
@@ -1769,7 +1895,7 @@ int csrst_ensemble_sync(csrst_ensemble *e, int *bad_member) {
 // the static-sweep tile (tx * ty = 256) and the number of parts that run side
 // by side.  Results do not depend on them.
 int csrst_ensemble_set_shape(csrst_ensemble *e, int push_ctas, int tx, int ty, int parts) {
-  if (!e || push_ctas < 0 || tx <= 0 || ty <= 0 || tx * ty != 256 || parts < 1)
+  if (!e || push_ctas < 0 || parts < 1 || !((tx == 0 && ty == 0) || (tx > 0 && ty > 0 && tx * ty == 256)))
     return efail(e, CSRST_E_ARG, "invalid shape");
   if (cudaStreamSynchronize(e->s) != cudaSuccess) return efail(e, CSRST_E_CUDA, "ensemble stream");
   e->push_grid = push_ctas;
@@ -1791,7 +1917,7 @@ int csrst_ensemble_tune(csrst_ensemble *e, int steps, double *report, int max_ro
   int rc = ensemble_steady(e, warm);
   if (rc) return rc;
   const int ctas[3] = {4 * sms, 16 * sms, 32 * sms};
-  const int tiles[2][2] = {{32, 8}, {128, 2}};
+  const int tiles[3][2] = {{0, 0}, {32, 8}, {128, 2}};  // the fused sweep, the sub-step tiles
   const int parts[3] = {1, 2, 4};
   cudaEvent_t t0, t1;
   cudaEventCreate(&t0);
@@ -1800,7 +1926,7 @@ int csrst_ensemble_tune(csrst_ensemble *e, int steps, double *report, int max_ro
   int bc = 2 * sms, bt = 0, bp = 1, rows = 0;
   for (int pa = 0; pa < 3; ++pa)
     for (int a = 0; a < 3; ++a)
-      for (int b = 0; b < 2; ++b) {
+      for (int b = 0; b < 3; ++b) {
         e->push_grid = ctas[a];
         e->tx = tiles[b][0]; e->ty = tiles[b][1];
         e->nparts = parts[pa];

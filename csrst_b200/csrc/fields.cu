@@ -551,6 +551,17 @@ __device__ __forceinline__ void move_finish(const MoveArgs<T> &m, int moveI, int
   check_window_clear(a, ws);
 }
 
+// Member of global block b: bpre holds the first block of every member (m + 1
+// entries).
+__device__ __forceinline__ int batch_member(const int *bpre, int m, int b) {
+  int lo = 0, hi = m - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (__ldg(bpre + mid) <= b) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
 // --- fused static sweep: the four sub-steps of one time step in one pass ----
 //
 // The static mesh carries no current, and between the first and the last of
@@ -645,7 +656,8 @@ struct YeeTile {
   // planes, kinds, barrier (16 bytes), cut list, base alignment; 5 CTAs per SM
   static constexpr int SMEM = 4 * PLANE_BYTES + KIND_BYTES + 16 + 2 * CUTS + 128;
   static constexpr int THREADS = 256;
-  static constexpr int E = TX / 32;  // cells per lane in a row
+  static constexpr int E = V;           // cells per lane in a row: 16 bytes
+  static constexpr int LPR = TX / E;    // lanes per row (16): a warp takes two rows at a time
 };
 
 template <class T>
@@ -682,7 +694,11 @@ __device__ __forceinline__ void stp(T *p, const Pack<T, E> &x) { *reinterpret_ca
 // The E kinds of the cells at kind-box offset q (q a multiple of E).
 template <int E>
 __device__ __forceinline__ void kinds(const uint8_t *sK, int q, uint8_t *kd) {
-  if (E == 2) {
+  if (E == 4) {
+    const uint32_t w = *reinterpret_cast<const uint32_t *>(sK + q);
+#pragma unroll
+    for (int e = 0; e < E; ++e) kd[e] = (uint8_t)(w >> (8 * e));
+  } else if (E == 2) {
     const uint16_t w = *reinterpret_cast<const uint16_t *>(sK + q);
     kd[0] = (uint8_t)(w & 0xff);
     kd[E - 1] = (uint8_t)(w >> 8);
@@ -734,22 +750,29 @@ __device__ __forceinline__ void store_regular(T *p, const Pack<T, E> &x, const u
     if (kd[e] == kKindRegular) p[e] = x.v[e];
 }
 
-// Half H, regular cells [c, c + E) of row r (a warp takes a row: the cell
-// right of a lane's piece comes from the next lane).
+// The row passes: half-warp h of a warp takes row r = rp + h, lane l of it
+// the cells [c, c + E) with c = V + l E; `valid` is false for the second
+// row past the phase's last, whose lanes only take part in the shuffles
+// (reading the last row).  A warp leaves a pass when none of its cells is
+// regular; the cell right (left) of a lane's piece comes from the next
+// (previous) lane of its half, the half's end lanes read it.
+
+// Half H, regular cells [c, c + E) of row r.
 template <class T, class G>
-__device__ __forceinline__ void tile_h(const Coef<T> &k, const TileSm<T> &t, int c, int r) {
+__device__ __forceinline__ void tile_h(const Coef<T> &k, const TileSm<T> &t, int c, int r, bool valid) {
   constexpr int E = G::E, W = G::W;
-  const int o = r * W + c, lane = threadIdx.x & 31;
+  const int o = r * W + c, l = threadIdx.x & (G::LPR - 1);
   uint8_t kd[E];
   kinds<E>(t.k, r * G::KW + c + G::KO, kd);
   bool any = false;
 #pragma unroll
   for (int e = 0; e < E; ++e) any |= kd[e] == kKindRegular;
-  if (!__any_sync(0xffffffffu, any)) return;
+  if (!__any_sync(0xffffffffu, any && valid)) return;
   Pack<T, E> hx = ldp<T, E>(t.hx + o), hy = ldp<T, E>(t.hy + o);
   const Pack<T, E> ey = ldp<T, E>(t.ey + o), ex0 = ldp<T, E>(t.ex + o), ex1 = ldp<T, E>(t.ex + o + W);
   T eyn = __shfl_down_sync(0xffffffffu, ey.v[0], 1);
-  if (lane == 31) eyn = t.ey[o + E];
+  if (l == G::LPR - 1) eyn = t.ey[o + E];
+  if (!valid) return;
 #pragma unroll
   for (int e = 0; e < E; ++e) {
     const T ey1 = e + 1 < E ? ey.v[e + 1 < E ? e + 1 : 0] : eyn;
@@ -761,8 +784,9 @@ __device__ __forceinline__ void tile_h(const Coef<T> &k, const TileSm<T> &t, int
 
 // Ex, regular cells [c, c + E) of row r.
 template <class T, class G>
-__device__ __forceinline__ void tile_ex(const Coef<T> &k, T zeroJ, const TileSm<T> &t, int c, int r) {
+__device__ __forceinline__ void tile_ex(const Coef<T> &k, T zeroJ, const TileSm<T> &t, int c, int r, bool valid) {
   constexpr int E = G::E, W = G::W;
+  if (!valid) return;
   const int o = r * W + c;
   uint8_t kd[E];
   kinds<E>(t.k, r * G::KW + c + G::KO, kd);
@@ -778,25 +802,25 @@ __device__ __forceinline__ void tile_ex(const Coef<T> &k, T zeroJ, const TileSm<
   store_regular<T, E>(t.ex + o, ex, kd);
 }
 
-// Ey, regular cells [c, c + E) of row r (the cell left of a lane's piece
-// comes from the previous lane).
+// Ey, regular cells [c, c + E) of row r.
 template <class T, class G>
-__device__ __forceinline__ void tile_ey(const Coef<T> &k, T zeroJ, const TileSm<T> &t, int c, int r) {
+__device__ __forceinline__ void tile_ey(const Coef<T> &k, T zeroJ, const TileSm<T> &t, int c, int r, bool valid) {
   constexpr int E = G::E, W = G::W;
-  const int o = r * W + c, lane = threadIdx.x & 31;
+  const int o = r * W + c, l = threadIdx.x & (G::LPR - 1);
   uint8_t kd[E];
   kinds<E>(t.k, r * G::KW + c + G::KO, kd);
   bool any = false;
 #pragma unroll
   for (int e = 0; e < E; ++e) any |= kd[e] == kKindRegular;
-  if (!__any_sync(0xffffffffu, any)) return;
+  if (!__any_sync(0xffffffffu, any && valid)) return;
   Pack<T, E> ey = ldp<T, E>(t.ey + o);
   const Pack<T, E> hx = ldp<T, E>(t.hx + o), hy = ldp<T, E>(t.hy + o);
   T hxl0 = __shfl_up_sync(0xffffffffu, hx.v[E - 1], 1), hyl0 = __shfl_up_sync(0xffffffffu, hy.v[E - 1], 1);
-  if (lane == 0) {
+  if (l == 0) {
     hxl0 = t.hx[o - 1];
     hyl0 = t.hy[o - 1];
   }
+  if (!valid) return;
 #pragma unroll
   for (int e = 0; e < E; ++e) {
     const T hxl = e > 0 ? hx.v[e > 0 ? e - 1 : 0] : hxl0, hyl = e > 0 ? hy.v[e > 0 ? e - 1 : 0] : hyl0;
@@ -846,12 +870,16 @@ __device__ __forceinline__ void tile_rest(const YeeTileArgs<T> &a, const TileSm<
     }
 }
 
+// One tile of the sweep (tile: its index in row-major tile order) in the
+// CTA's shared memory from base (128-byte aligned; planes, kinds, barrier,
+// cut list), the barrier initialised by the caller and at phase `parity`.
+// Returns 0; when the staging wait gives up, 1 if the copies arrived at the
+// second wait (the barrier's phase is used up as usual), 2 if they did not
+// (the barrier must not be used again).
 template <class T>
-__global__ void __launch_bounds__(256, 5) k_yee_tiles(const __grid_constant__ YeeTileArgs<T> a) {
+__device__ __forceinline__ int yee_tile(const YeeTileArgs<T> &a, int tile, uint32_t parity, uint8_t *base,
+                                        int *s_ncut) {
   using G = YeeTile<T>;
-  extern __shared__ uint8_t smem_raw[];
-  __shared__ int s_ncut;
-  uint8_t *base = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~(uintptr_t)127);
   T *sEx = reinterpret_cast<T *>(base);
   T *sEy = reinterpret_cast<T *>(base + G::PLANE_BYTES);
   T *sHx = reinterpret_cast<T *>(base + 2 * G::PLANE_BYTES);
@@ -860,15 +888,10 @@ __global__ void __launch_bounds__(256, 5) k_yee_tiles(const __grid_constant__ Ye
   uint64_t *bar = reinterpret_cast<uint64_t *>(sK + G::KIND_BYTES);
   uint16_t *cuts = reinterpret_cast<uint16_t *>(sK + G::KIND_BYTES + 16);
   const FieldArgsT<T> &f = a.f;
-  const int s0 = (int)(blockIdx.x % (unsigned)a.tilesX) * G::TX;
-  const int y0 = (int)(blockIdx.x / (unsigned)a.tilesX) * G::TY;
+  const int s0 = (tile % a.tilesX) * G::TX;
+  const int y0 = (tile / a.tilesX) * G::TY;
   if (threadIdx.x == 0) {
-    mbar_init(bar, 1);
-    mbar_init_fence();
-    s_ncut = 0;
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
+    *s_ncut = 0;
     mbar_expect_tx(bar, G::TX_BYTES);
     // storage row of cell row y0 - 1 is y0
     tma_load_2d(sEx, &a.map[0], s0 - G::V, y0, bar);
@@ -879,13 +902,18 @@ __global__ void __launch_bounds__(256, 5) k_yee_tiles(const __grid_constant__ Ye
   }
   // the fix-up's region, whose cells this sweep leaves to it (read while the copies fly)
   const FixRegion R = fix_region(f.ws->P0, f.ws->P1, f.L0, f.L1, f.Nx, f.Ny);
-  const bool ok = mbar_wait(bar, 0, a.spin);
-  if (__syncthreads_or(!ok)) {  // the copies did not arrive: report, wait once more for them, write nothing
+  // a.spin < 0: the staging wait is on a barrier nothing completes (the
+  // timeout test), with -a.spin polls
+  uint64_t *never = bar + 1;
+  const bool ok = a.spin < 0 ? mbar_wait(never, 0, -a.spin) : mbar_wait(bar, parity, a.spin);
+  if (__syncthreads_or(!ok)) {  // report, wait once more for the copies, write nothing
+    __shared__ int s_late;
     if (threadIdx.x == 0) {
       set_err(f.ws, kErrStaging);
-      mbar_wait(bar, 0, a.spin);
+      s_late = mbar_wait(bar, parity, a.spin < 0 ? -a.spin : a.spin) ? 1 : 2;
     }
-    return;
+    __syncthreads();
+    return s_late;
   }
   // box column c, row r is cell (s0 - V - 1 + c, y0 - 1 + r)
   const TileSm<T> t{sEx, sEy, sHx, sHy, sK, s0 - G::V - 1, y0 - 1};
@@ -895,29 +923,36 @@ __global__ void __launch_bounds__(256, 5) k_yee_tiles(const __grid_constant__ Ye
     for (int k = threadIdx.x; k < CW * (G::TY + 2); k += G::THREADS) {
       const int c = G::V - 1 + k % CW, r = k / CW;
       if (sK[r * G::KW + c + G::KO] == kKindCut) {
-        const int n = atomicAdd(&s_ncut, 1);
+        const int n = atomicAdd(s_ncut, 1);
         if (n < G::CUTS) cuts[n] = (uint16_t)(c | r << 7);
       }
     }
   }
   __syncthreads();
-  const int ncut = s_ncut;
-  // each lane takes E consecutive cells of a row of the tile's TX columns
-  // [V, V + TX); the halo column V - 1 and the cut cells go to the warps
-  // from 2 on (34 rows over 8 warps leave warps 0 and 1 with the extra row)
-  const int warp = threadIdx.x >> 5, c = G::V + (threadIdx.x & 31) * G::E;
+  const int ncut = *s_ncut;
+  // the row passes (tile_h, tile_ex, tile_ey); the halo column V - 1 and the
+  // cut cells go to the warps from 2 on in the first two phases (their row
+  // pairs leave warps 0 and 1 with one more)
+  const int warp = threadIdx.x >> 5, half = (threadIdx.x >> 4) & 1;
+  const int c = G::V + (threadIdx.x & (G::LPR - 1)) * G::E;
   const Coef<T> k{f.chx, f.chy, f.kex, f.key, f.dteps, f.mhx, f.mhy, f.de, f.h0, f.h1};
   const T zeroJ = a.zeroJ;
-  for (int r = warp; r < G::TY + 2; r += 8) tile_h<T, G>(k, t, c, r);
+  for (int rp = 2 * warp; rp < G::TY + 2; rp += 16) {
+    const int r = rp + half;
+    tile_h<T, G>(k, t, c, min(r, G::TY + 1), r < G::TY + 2);
+  }
   tile_rest<T, G, 1>(a, t, cuts, ncut, 0, G::TY + 2, 64);
   __syncthreads();
-  for (int r = 1 + warp; r < G::TY + 2; r += 8) tile_ex<T, G>(k, zeroJ, t, c, r);
+  for (int rp = 1 + 2 * warp; rp < G::TY + 2; rp += 16) {
+    const int r = rp + half;
+    tile_ex<T, G>(k, zeroJ, t, c, min(r, G::TY + 1), r < G::TY + 2);
+  }
   tile_rest<T, G, 2>(a, t, cuts, ncut, 1, G::TY + 2, 64);
   __syncthreads();
-  for (int r = 1 + warp; r < G::TY + 1; r += 8) tile_h<T, G>(k, t, c, r);
+  for (int rp = 1 + 2 * warp; rp < G::TY + 1; rp += 16) tile_h<T, G>(k, t, c, rp + half, true);
   tile_rest<T, G, 3>(a, t, cuts, ncut, 1, G::TY + 1, 0);
   __syncthreads();
-  for (int r = 1 + warp; r < G::TY + 1; r += 8) tile_ey<T, G>(k, zeroJ, t, c, r);
+  for (int rp = 1 + 2 * warp; rp < G::TY + 1; rp += 16) tile_ey<T, G>(k, zeroJ, t, c, rp + half, true);
   tile_rest<T, G, 4>(a, t, cuts, ncut, 1, G::TY + 1, 0);
   __syncthreads();
   // the tile's cells, every one (unchanged ones too) except the fix-up's,
@@ -942,6 +977,27 @@ __global__ void __launch_bounds__(256, 5) k_yee_tiles(const __grid_constant__ Ye
       }
     }
   }
+  return 0;
+}
+
+__device__ __forceinline__ uint8_t *align128(uint8_t *p) {
+  return reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(p) + 127) & ~(uintptr_t)127);
+}
+
+template <class T>
+__global__ void __launch_bounds__(256, 5) k_yee_tiles(const __grid_constant__ YeeTileArgs<T> a) {
+  using G = YeeTile<T>;
+  extern __shared__ uint8_t smem_raw[];
+  __shared__ int s_ncut;
+  uint8_t *base = align128(smem_raw);
+  uint64_t *bar = reinterpret_cast<uint64_t *>(base + 4 * G::PLANE_BYTES + G::KIND_BYTES);
+  if (threadIdx.x == 0) {
+    mbar_init(bar, 1);
+    mbar_init(bar + 1, 1);
+    mbar_init_fence();
+  }
+  __syncthreads();
+  yee_tile(a, (int)blockIdx.x, 0u, base, &s_ncut);
 }
 
 // The fix-up of the cells around the window (one cluster of kFixCtas CTAs,
@@ -989,15 +1045,17 @@ __device__ __forceinline__ void fix_h(const FieldArgsT<T> &a, const FieldArgsT<T
   z.Hy.at(i, j) = hy;
 }
 
-template <class T>
-__global__ void __cluster_dims__(kFixCtas, 1, 1) __launch_bounds__(kFixThreads)
-    k_yee_fixup(FieldArgsT<T> a, YeeFixArgs<T> x) {
+// The fix-up's body over threads tid of nth, sync() between its phases (a
+// cluster barrier over a cluster, __syncthreads in one CTA).
+template <class T, class Sync>
+__device__ __forceinline__ void yee_fixup(const FieldArgsT<T> &a, const YeeFixArgs<T> &x, int tid, int nth,
+                                          const Sync &sync) {
   const int P0 = a.ws->P0, P1 = a.ws->P1, L0 = a.L0, L1 = a.L1;
   // the window and its ring on the mesh (as the move and the initial
   // placement check, kErrWindowWall), else the scratch box would not hold
   // the strips: nothing is done, uniformly over the cluster
   if (P0 < 1 || P1 < 1 || P0 + L0 >= a.Nx || P1 + L1 >= a.Ny) {
-    if (blockIdx.x == 0 && threadIdx.x == 0) set_err(a.ws, kErrWindowWall);
+    if (tid == 0) set_err(a.ws, kErrWindowWall);
     return;
   }
   const FixRegion R = fix_region(P0, P1, L0, L1, a.Nx, a.Ny);
@@ -1012,7 +1070,6 @@ __global__ void __cluster_dims__(kFixCtas, 1, 1) __launch_bounds__(kFixThreads)
   z.Ey = PlaneT<T>{x.z + zs - zoff, x.zpitch};
   z.Hx = PlaneT<T>{x.z + 2 * zs - zoff, x.zpitch};
   z.Hy = PlaneT<T>{x.z + 3 * zs - zoff, x.zpitch};
-  const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
   const int nw = L0 * L1;
   auto kind_of = [&](int i, int j) { return x.kind[(size_t)(j + 1) * x.kpitch + (i + 1)]; };
   auto cut_of = [&](uint8_t kd, int i, int j) -> const CutCellDev * {
@@ -1030,7 +1087,7 @@ __global__ void __cluster_dims__(kFixCtas, 1, 1) __launch_bounds__(kFixThreads)
       dst.at(i, j) = stored ? src.at(i, j) : T(0);
     }
   }
-  cluster_barrier();
+  sync();
   // 1: half H, static [c0 - 1, c1) x [r0 - 1, r1 + 1), and the window
   {
     const int w = c1 - c0 + 1, ns = w * (r1 - r0 + 2);
@@ -1040,9 +1097,9 @@ __global__ void __cluster_dims__(kFixCtas, 1, 1) __launch_bounds__(kFixThreads)
       fix_h(a, z, kind_of(i, j), i, j, cut_of);
     }
   }
-  cluster_barrier();
+  sync();
   for (int k = tid; k < exchange_items(L0, L1, 0); k += nth) exchange_body(z, 0, k);
-  cluster_barrier();
+  sync();
   // 2: Ex, static [c0 - 1, c1) x [r0, r1 + 1), and the window with the first push's current
   {
     const int w = c1 - c0 + 1, ns = w * (r1 - r0 + 1);
@@ -1057,9 +1114,9 @@ __global__ void __cluster_dims__(kFixCtas, 1, 1) __launch_bounds__(kFixThreads)
       z.Ex.at(i, j) = e;
     }
   }
-  cluster_barrier();
+  sync();
   for (int k = tid; k < exchange_items(L0, L1, 1); k += nth) exchange_body(z, 1, k);
-  cluster_barrier();
+  sync();
   // 3: half H, static [c0 - 1, c1) x [r0, r1), and the window
   {
     const int w = c1 - c0 + 1, ns = w * (r1 - r0);
@@ -1069,9 +1126,9 @@ __global__ void __cluster_dims__(kFixCtas, 1, 1) __launch_bounds__(kFixThreads)
       fix_h(a, z, kind_of(i, j), i, j, cut_of);
     }
   }
-  cluster_barrier();
+  sync();
   for (int k = tid; k < exchange_items(L0, L1, 0); k += nth) exchange_body(z, 0, k);
-  cluster_barrier();
+  sync();
   // 4: static Ey on [c0, c1) x [r0, r1) (the window's Ey follows the second push)
   {
     const int w = c1 - c0, ns = w * (r1 - r0);
@@ -1085,7 +1142,7 @@ __global__ void __cluster_dims__(kFixCtas, 1, 1) __launch_bounds__(kFixThreads)
       z.Ey.at(i, j) = e;
     }
   }
-  cluster_barrier();
+  sync();
   {
     const int w = c1 - c0, nr = w * (r1 - r0);
     for (int k = tid; k < 4 * nr; k += nth) {
@@ -1097,19 +1154,96 @@ __global__ void __cluster_dims__(kFixCtas, 1, 1) __launch_bounds__(kFixThreads)
   }
 }
 
+struct ClusterSync {
+  __device__ __forceinline__ void operator()() const { cluster_barrier(); }
+};
+struct CtaSync {
+  __device__ __forceinline__ void operator()() const { __syncthreads(); }
+};
+
+template <class T>
+__global__ void __cluster_dims__(kFixCtas, 1, 1) __launch_bounds__(kFixThreads)
+    k_yee_fixup(FieldArgsT<T> a, YeeFixArgs<T> x) {
+  yee_fixup(a, x, (int)(blockIdx.x * blockDim.x + threadIdx.x), (int)(gridDim.x * blockDim.x), ClusterSync{});
+}
+
 // The window's Ey sub-step with the second push's current, and the Ey strip
 // exchange: the thread of window cell (0, j) also writes it to the static
 // mesh; the static column right of the window fills the window's guard
 // column (the static Ey there is final since the fused sweep).
 template <class T>
-__global__ void __launch_bounds__(256) k_window_ey(FieldArgsT<T> a) {
-  const int k = blockIdx.x * blockDim.x + threadIdx.x, nw = a.L0 * a.L1;
+__device__ __forceinline__ void window_ey_body(const FieldArgsT<T> &a, int k) {
+  const int nw = a.L0 * a.L1;
   if (k < nw) {
     window_e<T, 1>(a, k);
     if (k % a.L0 == 0) exchange_body(a, 2, k / a.L0);
   } else if (k - nw < a.L1 + 2) {
     exchange_body(a, 2, a.L1 + (k - nw));
   }
+}
+
+template <class T>
+__global__ void __launch_bounds__(256) k_window_ey(FieldArgsT<T> a) {
+  window_ey_body(a, (int)(blockIdx.x * blockDim.x + threadIdx.x));
+}
+
+// --- the fused sweep of a batch of members: one persistent launch ------------
+//
+// A work queue (one counter, reset before the launch) hands out the items in
+// order: first every member's window fix-up (one CTA each, the longest
+// items), then every member's tiles.  Items do not depend on one another (a
+// tile reads the source set only, the fix-up writes cells no tile writes), so
+// no CTA waits for another; each staging wait is bounded (kErrStaging).
+template <class T>
+struct YeeBatchFix {
+  FieldArgsT<T> a;   // static planes: the source set; the window; the first push's current
+  YeeFixArgs<T> x;
+};
+
+template <class T>
+__global__ void __launch_bounds__(256, 5) k_yee_batch(const YeeTileArgs<T> *targs, const YeeBatchFix<T> *fix,
+                                                      const int *tpre, int m, unsigned *queue) {
+  using G = YeeTile<T>;
+  extern __shared__ uint8_t smem_raw[];
+  __shared__ int s_ncut, s_item;
+  uint8_t *base = align128(smem_raw);
+  uint64_t *bar = reinterpret_cast<uint64_t *>(base + 4 * G::PLANE_BYTES + G::KIND_BYTES);
+  if (threadIdx.x == 0) {
+    mbar_init(bar, 1);
+    mbar_init(bar + 1, 1);
+    mbar_init_fence();
+  }
+  const int total = m + __ldg(tpre + m);
+  uint32_t parity = 0;
+  for (;;) {
+    // the previous item's shared-memory reads and writes come before the
+    // next staging copies overwrite it
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncthreads();
+    if (threadIdx.x == 0) s_item = (int)atomicAdd(queue, 1u);
+    __syncthreads();
+    const int item = s_item;
+    if (item >= total) break;
+    if (item < m) {
+      yee_fixup(fix[item].a, fix[item].x, (int)threadIdx.x, (int)blockDim.x, CtaSync{});
+      continue;
+    }
+    const int t = item - m;
+    int lo = 0, hi = m - 1;  // member of tile t
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (__ldg(tpre + mid) <= t) lo = mid; else hi = mid - 1;
+    }
+    const int rc = yee_tile(targs[lo], t - __ldg(tpre + lo), parity, base, &s_ncut);
+    if (rc == 2) break;  // the barrier may still receive copies: this CTA stops
+    parity ^= 1u;
+  }
+}
+
+template <class T>
+__global__ void __launch_bounds__(256) k_window_ey_batch(const FieldArgsT<T> *args, const int *bpre, int m) {
+  const int mm = batch_member(bpre, m, blockIdx.x);
+  window_ey_body(args[mm], (int)((blockIdx.x - bpre[mm]) * blockDim.x + threadIdx.x));
 }
 
 // --- kernels: one member, and a batch of members in one launch --------------
@@ -1154,16 +1288,6 @@ __global__ void __launch_bounds__(1024) k_move_finish(MoveArgs<T> m) {
   move_finish(m, s_move[1], s_move[2]);
 }
 
-// Member of global block b: bpre holds the first block of every member (m + 1
-// entries).
-__device__ __forceinline__ int batch_member(const int *bpre, int m, int b) {
-  int lo = 0, hi = m - 1;
-  while (lo < hi) {
-    const int mid = (lo + hi + 1) >> 1;
-    if (__ldg(bpre + mid) <= b) lo = mid; else hi = mid - 1;
-  }
-  return lo;
-}
 
 // The member's arguments are read in place: every thread of a block reads the
 // same words, which the L1 cache serves after the first.
@@ -1336,13 +1460,13 @@ static bool encode_2d(CUtensorMap *m, CUtensorMapDataType dt, const void *base, 
              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+// The tile arguments of one sweep (tensor maps over a's static planes, the
+// source set) and its tile-grid height.
 template <class T>
-int launch_yee_fused(const FieldArgsT<T> &a, const PlaneT<T> *dst, const uint8_t *kind, int kpitch,
-                     const int *cutidx, T *z, int zpitch, int zrows, long long spin, cudaStream_t s, cudaStream_t s2,
-                     cudaEvent_t fork, cudaEvent_t join) {
+static int fill_tile_args(YeeTileArgs<T> &t, const FieldArgsT<T> &a, const PlaneT<T> *dst, const uint8_t *kind,
+                          int kpitch, const int *cutidx, long long spin, int *tilesY) {
   using G = YeeTile<T>;
-  if (zpitch < a.L0 + 6 || zrows < a.L1 + 7 || kpitch < a.Nx + 2 || kpitch % 16) return kErrArg;
-  YeeTileArgs<T> t;
+  if (kpitch < a.Nx + 2 || kpitch % 16) return kErrArg;
   const CUtensorMapDataType dt = sizeof(T) == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
   const PlaneT<T> *src[4] = {&a.Ex, &a.Ey, &a.Hx, &a.Hy};
   for (int p = 0; p < 4; ++p) {
@@ -1358,16 +1482,35 @@ int launch_yee_fused(const FieldArgsT<T> &a, const PlaneT<T> *dst, const uint8_t
   for (int p = 0; p < 4; ++p) t.out[p] = dst[p];
   t.cutidx = cutidx;
   t.tilesX = (a.Nx + 2 + G::TX - 1) / G::TX;
-  const int tilesY = (a.Ny + G::TY - 1) / G::TY;
+  *tilesY = (a.Ny + G::TY - 1) / G::TY;
   t.zeroJ = T(0);
   t.spin = spin;
-  if (cudaFuncSetAttribute(k_yee_tiles<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM) != cudaSuccess)
-    return kErrCuda;
-  YeeFixArgs<T> x;
+  return kOk;
+}
+
+template <class T>
+static void fill_fix_args(YeeFixArgs<T> &x, const PlaneT<T> *dst, const uint8_t *kind, int kpitch,
+                          const int *cutidx, T *z, int zpitch, int zrows) {
   for (int p = 0; p < 4; ++p) x.out[p] = dst[p];
   x.z = z; x.zpitch = zpitch; x.zrows = zrows;
   x.kind = kind; x.kpitch = kpitch; x.cutidx = cutidx;
   x.zeroJ = T(0);
+}
+
+template <class T>
+int launch_yee_fused(const FieldArgsT<T> &a, const PlaneT<T> *dst, const uint8_t *kind, int kpitch,
+                     const int *cutidx, T *z, int zpitch, int zrows, long long spin, cudaStream_t s, cudaStream_t s2,
+                     cudaEvent_t fork, cudaEvent_t join) {
+  using G = YeeTile<T>;
+  if (zpitch < a.L0 + 6 || zrows < a.L1 + 7) return kErrArg;
+  YeeTileArgs<T> t;
+  int tilesY = 0;
+  const int rc = fill_tile_args(t, a, dst, kind, kpitch, cutidx, spin, &tilesY);
+  if (rc != kOk) return rc;
+  if (cudaFuncSetAttribute(k_yee_tiles<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM) != cudaSuccess)
+    return kErrCuda;
+  YeeFixArgs<T> x;
+  fill_fix_args(x, dst, kind, kpitch, cutidx, z, zpitch, zrows);
   // the tiles and the fix-up write disjoint cells and read only the source
   // set: the fix-up runs on s2 beside the tiles, s waits for both
   if (cudaEventRecord(fork, s) != cudaSuccess || cudaStreamWaitEvent(s2, fork, 0) != cudaSuccess) return kErrCuda;
@@ -1381,6 +1524,45 @@ template <class T>
 void launch_window_ey(const FieldArgsT<T> &a, cudaStream_t s) {
   const int n = a.L0 * a.L1 + a.L1 + 2;
   k_window_ey<T><<<(n + 255) / 256, 256, 0, s>>>(a);
+}
+
+template <class T>
+size_t yee_batch_bytes(int which) {
+  return which == 0 ? sizeof(YeeTileArgs<T>) : sizeof(YeeBatchFix<T>);
+}
+
+template <class T>
+int yee_batch_entry(const FieldArgsT<T> &a, const PlaneT<T> *dst, const uint8_t *kind, int kpitch, const int *cutidx,
+                    T *z, int zpitch, int zrows, long long spin, void *tile_out, void *fix_out, int *ntiles) {
+  if (zpitch < a.L0 + 6 || zrows < a.L1 + 7) return kErrArg;
+  YeeTileArgs<T> &t = *static_cast<YeeTileArgs<T> *>(tile_out);
+  int tilesY = 0;
+  const int rc = fill_tile_args(t, a, dst, kind, kpitch, cutidx, spin, &tilesY);
+  if (rc != kOk) return rc;
+  *ntiles = t.tilesX * tilesY;
+  YeeBatchFix<T> &f = *static_cast<YeeBatchFix<T> *>(fix_out);
+  f.a = a;
+  fill_fix_args(f.x, dst, kind, kpitch, cutidx, z, zpitch, zrows);
+  return kOk;
+}
+
+template <class T>
+int launch_yee_batch(const void *targs, const void *fix, const int *tpre, int m, unsigned *queue, cudaStream_t s) {
+  using G = YeeTile<T>;
+  int dev = 0, sms = 148;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+      cudaFuncSetAttribute(k_yee_batch<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM) != cudaSuccess ||
+      cudaMemsetAsync(queue, 0, sizeof(unsigned), s) != cudaSuccess)
+    return kErrCuda;
+  k_yee_batch<T><<<5 * sms, G::THREADS, G::SMEM, s>>>(static_cast<const YeeTileArgs<T> *>(targs),
+                                                        static_cast<const YeeBatchFix<T> *>(fix), tpre, m, queue);
+  return kOk;
+}
+
+template <class T>
+void launch_window_ey_batch(const FieldArgsT<T> *args, const int *bpre, int m, int nblocks, cudaStream_t s) {
+  if (nblocks > 0) k_window_ey_batch<T><<<nblocks, 256, 0, s>>>(args, bpre, m);
 }
 
 // Cell kinds in the static storage layout (guards and padding stay none).
@@ -1412,7 +1594,12 @@ void launch_build_kind(const uint8_t *mask, const int *cutidx, int Nx, int Ny, u
   template void launch_move_batch<T>(const MoveArgs<T> *, int, cudaStream_t);                        \
   template int launch_yee_fused<T>(const FieldArgsT<T> &, const PlaneT<T> *, const uint8_t *, int, const int *, T *, \
                                    int, int, long long, cudaStream_t, cudaStream_t, cudaEvent_t, cudaEvent_t); \
-  template void launch_window_ey<T>(const FieldArgsT<T> &, cudaStream_t);
+  template void launch_window_ey<T>(const FieldArgsT<T> &, cudaStream_t);                            \
+  template size_t yee_batch_bytes<T>(int);                                                          \
+  template int yee_batch_entry<T>(const FieldArgsT<T> &, const PlaneT<T> *, const uint8_t *, int, const int *, T *, \
+                                  int, int, long long, void *, void *, int *);                      \
+  template int launch_yee_batch<T>(const void *, const void *, const int *, int, unsigned *, cudaStream_t); \
+  template void launch_window_ey_batch<T>(const FieldArgsT<T> *, const int *, int, int, cudaStream_t);
 CSRST_FIELDS_INSTANTIATE(double)
 CSRST_FIELDS_INSTANTIATE(float)
 

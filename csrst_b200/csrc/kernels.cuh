@@ -169,6 +169,21 @@ int launch_yee_fused(const FieldArgsT<T> &a, const PlaneT<T> *dst, const uint8_t
                      cudaEvent_t fork, cudaEvent_t join);
 // The window's Ey sub-step after the second push, with its strip exchange.
 template <class T> void launch_window_ey(const FieldArgsT<T> &a, cudaStream_t s);
+// The fused sweep of a batch of members as one persistent launch over a work
+// queue: yee_batch_bytes(0 / 1) is the size of one member's entry in the tile
+// / fix-up table, yee_batch_entry fills a member's entries (host memory; the
+// arguments as for launch_yee_fused) and its tile count, launch_yee_batch
+// resets the queue counter and launches over the device tables (tpre: first
+// tile of every member, m + 1 entries).  Both return kOk, or kErrArg / kErrCuda
+// before anything is launched.
+template <class T> size_t yee_batch_bytes(int which);
+template <class T>
+int yee_batch_entry(const FieldArgsT<T> &a, const PlaneT<T> *dst, const uint8_t *kind, int kpitch, const int *cutidx,
+                    T *z, int zpitch, int zrows, long long spin, void *tile_out, void *fix_out, int *ntiles);
+template <class T>
+int launch_yee_batch(const void *targs, const void *fix, const int *tpre, int m, unsigned *queue, cudaStream_t s);
+template <class T>
+void launch_window_ey_batch(const FieldArgsT<T> *args, const int *bpre, int m, int nblocks, cudaStream_t s);
 void launch_build_kind(const uint8_t *mask, const int *cutidx, int Nx, int Ny, uint8_t *kind, int kpitch,
                        cudaStream_t s);
 // geometry.cu

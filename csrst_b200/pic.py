@@ -281,7 +281,9 @@ class Ensemble:
     def stream(self):
         return lib().csrst_ensemble_stream(self._e)
 
-    def set_shape(self, push_ctas, tx=32, ty=8, parts=1):
+    def set_shape(self, push_ctas, tx=0, ty=0, parts=1):
+        """Launch shapes: push CTAs, field path (tx = ty = 0: the fused
+        sweep; else sub-step tiles of tx x ty), parts."""
         self._ck(lib().csrst_ensemble_set_shape(self._e, int(push_ctas), int(tx), int(ty), int(parts)))
 
     def tune(self, steps=3):

@@ -172,6 +172,14 @@ int csrst_step(csrst_handle *h, int nsteps);
  * four sub-steps with their exchanges, and the window's Ey), the window move,
  * and the whole step. */
 int csrst_step_timed(csrst_handle *h, double *ms4);
+/* Polls a fused-sweep tile makes in its staging wait (the TMA copies of its
+ * fields) before it gives up, writes nothing and reports CSRST_E_STAGING at
+ * the next synchronising call; for sweeps recorded or tabled after this call
+ * (a new handle's first steps, an ensemble built after it).  polls == 0
+ * restores the default, 2^22.  polls < 0 exercises that path: every staging
+ * wait is then on a barrier that nothing completes, and gives up after
+ * -polls polls (the tile still waits for its real copies before it ends). */
+int csrst_set_staging_wait_limit(long long polls);
 
 /* Batched ensemble (no reference counterpart: the reference runs one bunch
  * per job).  Independent members, each a loaded handle with its own mesh,
@@ -191,14 +199,17 @@ void *csrst_ensemble_stream(csrst_ensemble *e);
 int csrst_ensemble_step(csrst_ensemble *e, int nsteps);
 /* Waits for the ensemble; returns the first member's sticky error (its index in *bad_member). */
 int csrst_ensemble_sync(csrst_ensemble *e, int *bad_member);
-/* Launch shapes: CTAs of the batched push (0 = two per SM), the static-sweep
- * tile tx x ty (tx * ty = 256) and the number of parts the members are split
- * into, which step side by side on their own streams.  Results do not depend
- * on them. */
+/* Launch shapes: CTAs of the batched push (0 = two per SM), the field path
+ * (tx = ty = 0: the fused static sweep, all members' tiles and window
+ * fix-ups from one work queue in one persistent launch per step, the
+ * default; else one launch per sub-step with static-sweep tiles of tx x ty,
+ * tx * ty = 256) and the number of parts the members are split into, which
+ * step side by side on their own streams.  Results do not depend on them. */
 int csrst_ensemble_set_shape(csrst_ensemble *e, int push_ctas, int tx, int ty, int parts);
 /* Autotuner: times `steps` steps for each candidate shape and keeps the
- * fastest; the timed steps are real steps of the members.  report: rows of
- * (push_ctas, tx, ty, parts, ms per step). */
+ * fastest; the timed steps are real steps of the members.  Candidates: push
+ * CTAs {4, 16, 32} per SM x field path {fused, 32 x 8, 128 x 2} x parts
+ * {1, 2, 4}.  report: rows of (push_ctas, tx, ty, parts, ms per step). */
 int csrst_ensemble_tune(csrst_ensemble *e, int steps, double *report, int max_rows, int *nrows);
 
 /* BF16 tensor-core GEMM of the wake surrogate (no reference counterpart):

@@ -53,8 +53,10 @@ def test_ensemble_matches_single_runs(gpu_lib, fp32):
 
 
 def test_launch_shapes_do_not_change_results(gpu_lib):
+    """Sub-step tiles of two shapes and the fused sweep (tx = ty = 0, one
+    persistent launch over a work queue) give the same states."""
     runs = []
-    for shape in ((148, 32, 8, 1), (1184, 128, 2, 3)):
+    for shape in ((148, 32, 8, 1), (1184, 128, 2, 3), (592, 0, 0, 2)):
         sims = members(True, NAMES[:4])
         ens = Ensemble(sims)
         ens.set_shape(*shape)
@@ -62,21 +64,23 @@ def test_launch_shapes_do_not_change_results(gpu_lib):
         ens.sync()
         runs.append([state(s) for s in sims])
         ens.close()
-    for ma, mb in zip(*runs):
-        for x, y in zip(ma, mb):
-            assert np.array_equal(x, y)
+    for other in runs[1:]:
+        for ma, mb in zip(runs[0], other):
+            for x, y in zip(ma, mb):
+                assert np.array_equal(x, y)
 
 
 def test_autotuner_steps_are_real_steps(gpu_lib):
     sims, ref = members(False, NAMES[:3]), members(False, NAMES[:3])
     ens = Ensemble(sims)
     rows = ens.tune(steps=1)
-    assert len(rows) == 18 and all(r[4] > 0 for r in rows)
+    assert len(rows) == 27 and all(r[4] > 0 for r in rows)
+    assert {(r[1], r[2]) for r in rows} == {(0, 0), (32, 8), (128, 2)}
     ens.step(2)
     ens.sync()
-    # one step to reach the steady state of the loop, then 18 shapes x (1 warm-up + 1 timed), then 2
+    # one step to reach the steady state of the loop, then 27 shapes x (1 warm-up + 1 timed), then 2
     for s in ref:
-        s.step(1 + 18 * 2 + 2)
+        s.step(1 + 27 * 2 + 2)
     for a, b in zip(sims, ref):
         assert_same(a, b)
     ens.close()
@@ -105,3 +109,38 @@ def test_mixed_precision_rejected(gpu_lib):
     a, b = members(False, ["small-0"]), members(True, ["small-1"])
     with pytest.raises(CsrstError):
         Ensemble(a + b)
+
+
+@pytest.mark.parametrize("fp32", [False, True])
+def test_staging_wait_that_gives_up(gpu_lib, fp32):
+    """The fused sweep's staging waits are bounded.  With the stuck-wait hook
+    (every staging wait on a barrier nothing completes, 200 polls) a batched
+    step and a single handle's step report CSRST_E_STAGING instead of
+    hanging; with the default limit restored, new members step correctly
+    (the context is intact)."""
+    from csrst_b200._lib import lib
+    try:
+        lib().csrst_set_staging_wait_limit(-200)
+        sims = members(fp32, NAMES[:2], fields=False)
+        ens = Ensemble(sims)
+        ens.step(3)
+        with pytest.raises(CsrstError) as ei:
+            ens.sync()
+        assert ei.value.code == -10
+        ens.close()
+        one = members(fp32, ["small-1"], fields=False)[0]
+        with pytest.raises(CsrstError) as ei:
+            one.step(3)
+            one.sync()
+        assert ei.value.code == -10
+    finally:
+        lib().csrst_set_staging_wait_limit(0)
+    batch, single = members(fp32, NAMES[:2], fields=False), members(fp32, NAMES[:2], fields=False)
+    ens = Ensemble(batch)
+    ens.step(4)
+    ens.sync()
+    for s in single:
+        s.step(4)
+    for a, b in zip(batch, single):
+        assert_same(a, b)
+    ens.close()
