@@ -102,6 +102,7 @@ def lib():
         "csrst_step": ([P, C.c_int], C.c_int),
         "csrst_step_timed": ([P, D], C.c_int),
         "csrst_set_staging_wait_limit": ([C.c_longlong], C.c_int),
+        "csrst_release_memory": ([], C.c_int),
         "csrst_diag_moments": ([P, D], C.c_int),
         "csrst_diag_wake": ([P, D, C.c_int], C.c_int),
         "csrst_diag_wake_async": ([P, P, C.c_int, P], C.c_int),

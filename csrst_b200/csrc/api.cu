@@ -6,6 +6,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -354,19 +355,56 @@ void bend_setup(csrst_handle *h) {
   h->bwidth = 2 * b.R * std::abs(h->shh);
 }
 
+// Stream-ordered allocations from the library's own memory pool (one per
+// device; memory freed into it stays there for the next allocation instead
+// of going back to the driver at every synchronisation): the bunch arrays of
+// a handle and the temporaries of a bunch upload, so that a reload, or a new
+// handle after an old one, allocates and frees without device-wide waits.
+cudaMemPool_t lib_pool() {
+  static std::mutex mu;
+  static cudaMemPool_t pools[64] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
+  std::lock_guard<std::mutex> lock(mu);
+  if (!pools[dev]) {
+    cudaMemPoolProps p{};
+    p.allocType = cudaMemAllocationTypePinned;
+    p.location.type = cudaMemLocationTypeDevice;
+    p.location.id = dev;
+    cudaMemPool_t m = nullptr;
+    if (cudaMemPoolCreate(&m, &p) != cudaSuccess) return nullptr;
+    uint64_t keep = UINT64_MAX;
+    cudaMemPoolSetAttribute(m, cudaMemPoolAttrReleaseThreshold, &keep);
+    pools[dev] = m;
+  }
+  return pools[dev];
+}
+
+template <class P>
+cudaError_t palloc(P **p, size_t bytes, cudaStream_t s) {
+  cudaMemPool_t m = lib_pool();
+  if (!m) return cudaErrorMemoryAllocation;
+  return cudaMallocFromPoolAsync(reinterpret_cast<void **>(p), bytes, m, s);
+}
+
+void pfree(void *p, cudaStream_t s) {
+  if (p) cudaFreeAsync(p, s);
+}
+
 void drop_graphs(csrst_handle *h) {
   for (cudaGraphExec_t &g : h->graph)
     if (g) { cudaGraphExecDestroy(g); g = nullptr; }
 }
 
 void free_particles(csrst_handle *h) {
-  cudaFree(h->x); cudaFree(h->y); cudaFree(h->px); cudaFree(h->py); cudaFree(h->q);
-  cudaFree(h->ox); cudaFree(h->oy);
+  // the bunch arrays come from the pool (palloc), freed in the handle's stream order
+  for (double *p : {h->x, h->y, h->px, h->py, h->q, h->ox, h->oy}) pfree(p, h->s);
   h->x = h->y = h->px = h->py = h->q = h->ox = h->oy = nullptr;
   cudaFree(h->win); cudaFree(h->scratch); cudaFree(h->acc);
   h->win = h->scratch = nullptr; h->acc = nullptr;
-  cudaFree(h->b32.cell); cudaFree(h->b32.ox); cudaFree(h->b32.oy); cudaFree(h->b32.dpx); cudaFree(h->b32.dpy);
-  cudaFree(h->b32.q); cudaFree(h->winf); cudaFree(h->scratchf); cudaFree(h->d64);
+  pfree(h->b32.cell, h->s); pfree(h->b32.ox, h->s); pfree(h->b32.oy, h->s); pfree(h->b32.dpx, h->s);
+  pfree(h->b32.dpy, h->s); pfree(h->b32.q, h->s); pfree(h->d64, h->s);
+  cudaFree(h->winf); cudaFree(h->scratchf);
   cudaFree(h->old_cell); cudaFree(h->old_o0); cudaFree(h->old_o1);
   h->old_cell = nullptr; h->old_o0 = h->old_o1 = nullptr;
   h->b32 = Bunch32{};
@@ -900,12 +938,12 @@ int csrst_load_particles(csrst_handle *h, const double *x, const double *y, cons
   double *tmp[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
   unsigned long long *chk = nullptr;
   auto drop = [&]() {
-    for (int k = 0; k < 5; ++k) cudaFree(tmp[k]);
-    cudaFree(chk);
+    for (int k = 0; k < 5; ++k) pfree(tmp[k], h->s);
+    pfree(chk, h->s);
   };
   for (int k = 0; k < 5; ++k)
-    if (cudaMalloc(&tmp[k], nb) != cudaSuccess) { drop(); return fail(h, CSRST_E_CUDA, "bunch upload: out of memory"); }
-  if (cudaMalloc(&chk, 2 * sizeof(unsigned long long)) != cudaSuccess) {
+    if (palloc(&tmp[k], nb, h->s) != cudaSuccess) { drop(); return fail(h, CSRST_E_CUDA, "bunch upload: out of memory"); }
+  if (palloc(&chk, 2 * sizeof(unsigned long long), h->s) != cudaSuccess) {
     drop();
     return fail(h, CSRST_E_CUDA, "bunch upload: out of memory");
   }
@@ -934,11 +972,11 @@ int csrst_load_particles(csrst_handle *h, const double *x, const double *y, cons
     return fail(h, CSRST_E_ARG, "particle outside the static mesh at index " + std::to_string(i));
   }
   const double qmax = bits_to_double(hchk[1]);
-  cudaFree(chk);
+  pfree(chk, h->s);
   chk = nullptr;
   free_particles(h);
   h->n = N;
-  for (double **p : {&h->x, &h->y, &h->px, &h->py, &h->q, &h->ox, &h->oy}) CK(cudaMalloc(p, nb));
+  for (double **p : {&h->x, &h->y, &h->px, &h->py, &h->q, &h->ox, &h->oy}) CK(palloc(p, nb, h->s));
   // particle box on the static mesh -> window +-5 cells (main.cpp:198-217)
   WinState w0{};
   w0.cur = 0;
@@ -982,23 +1020,22 @@ int csrst_load_particles(csrst_handle *h, const double *x, const double *y, cons
     long long *i1 = nullptr, *i2 = nullptr;
     void *ct = nullptr;
     size_t ctb = 0, ctb2 = 0;
-    CK(cudaMalloc(&kx, n * 8)); CK(cudaMalloc(&kx2, n * 8));
-    CK(cudaMalloc(&ks, n * 4)); CK(cudaMalloc(&ks2, n * 4));
-    CK(cudaMalloc(&i1, n * 8)); CK(cudaMalloc(&i2, n * 8));
+    CK(palloc(&kx, n * 8, h->s)); CK(palloc(&kx2, n * 8, h->s));
+    CK(palloc(&ks, n * 4, h->s)); CK(palloc(&ks2, n * 4, h->s));
+    CK(palloc(&i1, n * 8, h->s)); CK(palloc(&i2, n * 8, h->s));
     const unsigned g = (unsigned)((n + 255) / 256);
     k_sort_keys<<<g, 256, 0, h->s>>>(tmp[0], tmp[1], N, h->ws, h->b.hr1, kx, i1);
     CK(cub::DeviceRadixSort::SortPairs(nullptr, ctb, kx, kx2, i1, i2, (int)n, 0, 64, h->s));
     CK(cub::DeviceRadixSort::SortPairs(nullptr, ctb2, ks, ks2, i2, i1, (int)n, 0, 32, h->s));
-    CK(cudaMalloc(&ct, ctb > ctb2 ? ctb : ctb2));
+    CK(palloc(&ct, ctb > ctb2 ? ctb : ctb2, h->s));
     CK(cub::DeviceRadixSort::SortPairs(ct, ctb, kx, kx2, i1, i2, (int)n, 0, 64, h->s));
     k_slice_keys<<<g, 256, 0, h->s>>>(tmp[1], i2, N, h->ws, h->b.hr1, ks);
     CK(cub::DeviceRadixSort::SortPairs(ct, ctb2, ks, ks2, i2, i1, (int)n, 0, 32, h->s));
     double *dst[5] = {h->x, h->y, h->px, h->py, h->q};
     for (int k = 0; k < 5; ++k) k_gather_perm<<<g, 256, 0, h->s>>>(i1, N, tmp[k], dst[k]);
-    CK(cudaStreamSynchronize(h->s));
-    cudaFree(kx); cudaFree(kx2); cudaFree(ks); cudaFree(ks2); cudaFree(i1); cudaFree(i2); cudaFree(ct);
+    for (void *p : {(void *)kx, (void *)kx2, (void *)ks, (void *)ks2, (void *)i1, (void *)i2, ct}) pfree(p, h->s);
   }
-  for (int k = 0; k < 5; ++k) cudaFree(tmp[k]);
+  for (int k = 0; k < 5; ++k) pfree(tmp[k], h->s);
   CK(cudaMemcpyAsync(h->ox, h->x, nb, cudaMemcpyDeviceToDevice, h->s));
   CK(cudaMemcpyAsync(h->oy, h->y, nb, cudaMemcpyDeviceToDevice, h->s));
   // 64-bit fixed-point scale of the current: a power of two with the
@@ -1013,11 +1050,11 @@ int csrst_load_particles(csrst_handle *h, const double *x, const double *y, cons
   if (h->fp32) {
     // reference momentum = mean momentum; then the FP32 bunch replaces the FP64 arrays
     double *part = nullptr, sums[2];
-    CK(cudaMalloc(&part, (2 * 296 + 2) * sizeof(double)));
+    CK(palloc(&part, (2 * 296 + 2) * sizeof(double), h->s));
     launch_psum(h->px, h->py, N, part, part + 2 * 296, h->s);
     CK(cudaMemcpyAsync(sums, part + 2 * 296, sizeof(sums), cudaMemcpyDeviceToHost, h->s));
     CK(cudaStreamSynchronize(h->s));
-    cudaFree(part);
+    pfree(part, h->s);
     h->P0 = sums[0] / (double)N;
     h->P1 = sums[1] / (double)N;
     set_ref32(h);
@@ -1027,13 +1064,12 @@ int csrst_load_particles(csrst_handle *h, const double *x, const double *y, cons
     h->acc_scale = std::ldexp(1.0, (int)std::floor(std::log2(std::ldexp(1.0, 62) / fbound)));
     Bunch32 &b = h->b32;
     b.n = N;
-    CK(cudaMalloc(&b.cell, n * sizeof(int)));
-    for (float **p : {&b.ox, &b.oy, &b.dpx, &b.dpy, &b.q}) CK(cudaMalloc(p, n * sizeof(float)));
-    CK(cudaMalloc(&h->d64, 4 * nb));
+    CK(palloc(&b.cell, n * sizeof(int), h->s));
+    for (float **p : {&b.ox, &b.oy, &b.dpx, &b.dpy, &b.q}) CK(palloc(p, n * sizeof(float), h->s));
+    CK(palloc(&h->d64, 4 * nb, h->s));
     launch_from64(h->x, h->y, h->px, h->py, h->q, N, h->b.org0, h->b.org1, h->b.hr0, h->b.hr1, h->P0, h->P1, b,
                   h->s);
-    CK(cudaStreamSynchronize(h->s));
-    for (double **p : {&h->x, &h->y, &h->px, &h->py, &h->q, &h->ox, &h->oy}) { cudaFree(*p); *p = nullptr; }
+    for (double **p : {&h->x, &h->y, &h->px, &h->py, &h->q, &h->ox, &h->oy}) { pfree(*p, h->s); *p = nullptr; }
     CK(alloc_old32(h));
     launch_bbox32(b, h->R32, 0, h->ws, h->s);
   } else {
@@ -1293,6 +1329,12 @@ int csrst_step(csrst_handle *h, int nsteps) {
     CK(cudaGraphLaunch(h->graph[p], h->s));
   }
   return CSRST_OK;
+}
+
+int csrst_release_memory(void) {
+  cudaMemPool_t m = lib_pool();
+  if (!m) return CSRST_E_CUDA;
+  return cudaMemPoolTrimTo(m, 0) == cudaSuccess ? CSRST_OK : CSRST_E_CUDA;
 }
 
 int csrst_set_staging_wait_limit(long long polls) {
@@ -2371,11 +2413,11 @@ int csrst_checkpoint_read(csrst_handle *h, const char *path, long long *step, do
   if (h->fp32) {
     Bunch32 &b = h->b32;
     b.n = n;
-    CK(cudaMalloc(&b.cell, (size_t)n * sizeof(int)));
-    for (float **p : {&b.ox, &b.oy, &b.dpx, &b.dpy, &b.q}) CK(cudaMalloc(p, (size_t)n * sizeof(float)));
-    CK(cudaMalloc(&h->d64, 4 * nb));
+    CK(palloc(&b.cell, (size_t)n * sizeof(int), h->s));
+    for (float **p : {&b.ox, &b.oy, &b.dpx, &b.dpy, &b.q}) CK(palloc(p, (size_t)n * sizeof(float), h->s));
+    CK(palloc(&h->d64, 4 * nb, h->s));
   } else {
-    for (double **p : {&h->x, &h->y, &h->px, &h->py, &h->q, &h->ox, &h->oy}) CK(cudaMalloc(p, nb));
+    for (double **p : {&h->x, &h->y, &h->px, &h->py, &h->q, &h->ox, &h->oy}) CK(palloc(p, nb, h->s));
   }
   P = ck_plan(h);
   for (auto &pl : P.bunch)

@@ -180,6 +180,12 @@ int csrst_step_timed(csrst_handle *h, double *ms4);
  * wait is then on a barrier that nothing completes, and gives up after
  * -polls polls (the tile still waits for its real copies before it ends). */
 int csrst_set_staging_wait_limit(long long polls);
+/* A handle's bunch arrays and the temporaries of csrst_load_particles come
+ * from a stream-ordered memory pool the library keeps per device: memory a
+ * destroyed handle or a reload frees stays in the pool for the next load
+ * (no device-wide waits for cudaMalloc / cudaFree).  This returns the
+ * pool's unused memory of the current device to the driver. */
+int csrst_release_memory(void);
 
 /* Batched ensemble (no reference counterpart: the reference runs one bunch
  * per job).  Independent members, each a loaded handle with its own mesh,
