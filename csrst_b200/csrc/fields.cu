@@ -917,14 +917,24 @@ __device__ __forceinline__ int yee_tile(const YeeTileArgs<T> &a, int tile, uint3
   }
   // box column c, row r is cell (s0 - V - 1 + c, y0 - 1 + r)
   const TileSm<T> t{sEx, sEy, sHx, sHy, sK, s0 - G::V - 1, y0 - 1};
-  // the tile's cut cells (columns [V - 1, V + TX), rows [0, TY + 2)), as 7-bit column | row << 7
+  // the tile's cut cells (columns [V - 1, V + TX), rows [0, TY + 2)), as 7-bit
+  // column | row << 7: each thread tests 16 kinds at once (a cut kind is the
+  // only one with bit 1 set) and looks at single bytes only where one is
   {
-    constexpr int CW = G::TX + 1;
-    for (int k = threadIdx.x; k < CW * (G::TY + 2); k += G::THREADS) {
-      const int c = G::V - 1 + k % CW, r = k / CW;
-      if (sK[r * G::KW + c + G::KO] == kKindCut) {
-        const int n = atomicAdd(s_ncut, 1);
-        if (n < G::CUTS) cuts[n] = (uint16_t)(c | r << 7);
+    constexpr int CH = G::KW / 16;  // 16-byte pieces of a kind row
+    static_assert(CH * (G::TY + 2) <= G::THREADS, "one piece per thread");
+    const int k = threadIdx.x;
+    if (k < CH * (G::TY + 2)) {
+      const int r = k / CH, q0 = (k % CH) * 16;
+      const uint4 w = *reinterpret_cast<const uint4 *>(sK + r * G::KW + q0);
+      if ((w.x | w.y | w.z | w.w) & 0x02020202u) {
+        for (int b = 0; b < 16; ++b) {
+          const int c = q0 + b - G::KO;  // box column
+          if (c >= G::V - 1 && c < G::V + G::TX && sK[r * G::KW + q0 + b] == kKindCut) {
+            const int n = atomicAdd(s_ncut, 1);
+            if (n < G::CUTS) cuts[n] = (uint16_t)(c | r << 7);
+          }
+        }
       }
     }
   }
