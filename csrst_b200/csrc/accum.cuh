@@ -58,6 +58,7 @@ struct TileAcc {
 #pragma unroll 4
     for (int k = 0; k < kSize; ++k) {
       const unsigned long long v = tile[k * stride];
+      if (!__any_sync(0xffffffffu, v != 0ull)) continue;  // the warp never added to this entry
       tile[k * stride] = 0ull;
       const unsigned c0 = __reduce_add_sync(0xffffffffu, (unsigned)(v & 0x3FFFFFull));
       const unsigned c1 = __reduce_add_sync(0xffffffffu, (unsigned)((v >> 22) & 0x3FFFFFull));

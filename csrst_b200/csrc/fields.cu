@@ -870,15 +870,29 @@ __device__ __forceinline__ void tile_rest(const YeeTileArgs<T> &a, const TileSm<
     }
 }
 
+// Issues the staging copies of tile `tile` into the buffer at base (one thread).
+template <class T>
+__device__ __forceinline__ void yee_stage(const YeeTileArgs<T> &a, int tile, uint8_t *base) {
+  using G = YeeTile<T>;
+  uint8_t *sK = base + 4 * G::PLANE_BYTES;
+  uint64_t *bar = reinterpret_cast<uint64_t *>(sK + G::KIND_BYTES);
+  const int s0 = (tile % a.tilesX) * G::TX, y0 = (tile / a.tilesX) * G::TY;
+  mbar_expect_tx(bar, G::TX_BYTES);
+  // storage row of cell row y0 - 1 is y0
+  for (int p = 0; p < 4; ++p) tma_load_2d(base + p * G::PLANE_BYTES, &a.map[p], s0 - G::V, y0, bar);
+  tma_load_2d(sK, &a.map[4], s0 - 16, y0, bar);
+}
+
 // One tile of the sweep (tile: its index in row-major tile order) in the
 // CTA's shared memory from base (128-byte aligned; planes, kinds, barrier,
-// cut list), the barrier initialised by the caller and at phase `parity`.
+// cut list), the barrier initialised by the caller and at phase `parity`;
+// staged: its copies were issued already (yee_stage), else this issues them.
 // Returns 0; when the staging wait gives up, 1 if the copies arrived at the
 // second wait (the barrier's phase is used up as usual), 2 if they did not
 // (the barrier must not be used again).
 template <class T>
 __device__ __forceinline__ int yee_tile(const YeeTileArgs<T> &a, int tile, uint32_t parity, uint8_t *base,
-                                        int *s_ncut) {
+                                        int *s_ncut, bool staged = false) {
   using G = YeeTile<T>;
   T *sEx = reinterpret_cast<T *>(base);
   T *sEy = reinterpret_cast<T *>(base + G::PLANE_BYTES);
@@ -892,13 +906,7 @@ __device__ __forceinline__ int yee_tile(const YeeTileArgs<T> &a, int tile, uint3
   const int y0 = (tile / a.tilesX) * G::TY;
   if (threadIdx.x == 0) {
     *s_ncut = 0;
-    mbar_expect_tx(bar, G::TX_BYTES);
-    // storage row of cell row y0 - 1 is y0
-    tma_load_2d(sEx, &a.map[0], s0 - G::V, y0, bar);
-    tma_load_2d(sEy, &a.map[1], s0 - G::V, y0, bar);
-    tma_load_2d(sHx, &a.map[2], s0 - G::V, y0, bar);
-    tma_load_2d(sHy, &a.map[3], s0 - G::V, y0, bar);
-    tma_load_2d(sK, &a.map[4], s0 - 16, y0, bar);
+    if (!staged) yee_stage(a, tile, base);
   }
   // the fix-up's region, whose cells this sweep leaves to it (read while the copies fly)
   const FixRegion R = fix_region(f.ws->P0, f.ws->P1, f.L0, f.L1, f.Nx, f.Ny);

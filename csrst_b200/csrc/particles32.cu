@@ -67,17 +67,27 @@ struct Move32 {
   float a0, a1, o0, o1, q;
 };
 
+// The stored state of particle n, read one round ahead of its move.
+struct In32 {
+  int cell;
+  float s0, s1, d0, d1, q;
+};
+__device__ __forceinline__ In32 load32(const Bunch32 &b, long long n) {
+  return In32{__ldcs(b.cell + n), __ldcs(b.ox + n), __ldcs(b.oy + n), __ldcs(b.dpx + n), __ldcs(b.dpy + n),
+              __ldg(b.q + n)};
+}
+
 template <int ORDER_OF_PUSH>
-__device__ __forceinline__ void move32(const Push32Args &a, long long n, int L0, int L1, int WP0, int WP1,
-                                       Move32 &m) {
+__device__ __forceinline__ void move32(const Push32Args &a, long long n, const In32 &in, int L0, int L1, int WP0,
+                                       int WP1, Move32 &m) {
   WinState *ws = a.ws;
   const int wp = a.wpitch;
   const Ref32 &R = a.R;
   int ci, cj;
-  unpack(a.b.cell[n], ci, cj);
-  const float s0 = a.b.ox[n], s1 = a.b.oy[n];
-  float d0 = a.b.dpx[n], d1 = a.b.dpy[n];
-  m.q = a.b.q[n];
+  unpack(in.cell, ci, cj);
+  const float s0 = in.s0, s1 = in.s1;
+  float d0 = in.d0, d1 = in.d1;
+  m.q = in.q;
   m.ci = ci; m.cj = cj; m.ni = ci; m.nj = cj;
   m.a0 = s0; m.a1 = s1; m.o0 = s0; m.o1 = s1;
   m.ok = isfinite(d0) && isfinite(d1) && s0 >= 0.0f && s0 < 1.0f && s1 >= 0.0f && s1 < 1.0f;
@@ -179,13 +189,18 @@ __device__ __forceinline__ void push32_range(const Push32Args &a, long long beg,
   Boxes32 box;
   bool overflow = false;
   const long long rounds = end > beg ? (end - beg + blockDim.x - 1) / blockDim.x : 0;
+  // each lane's next particle is read while the current one moves
+  In32 next{};
+  if (beg + threadIdx.x < end) next = load32(a.b, beg + threadIdx.x);
   for (long long it = 0; it < rounds; ++it) {  // the same rounds for every lane of the warp
     const long long n = beg + it * blockDim.x + threadIdx.x;
+    const In32 cur = next;
+    if (n + blockDim.x < end) next = load32(a.b, n + blockDim.x);
     Move32 m;
     m.ok = false;
     m.ci = WP0; m.cj = WP1;
     if (n < end) {
-      move32<ORDER>(a, n, L0, L1, WP0, WP1, m);
+      move32<ORDER>(a, n, cur, L0, L1, WP0, WP1, m);
       if (m.ok) box.add(m);
     }
     const int wi = m.ci - WP0, wj = m.cj - WP1;
