@@ -306,11 +306,60 @@ def objective(X6, W):
     return np.sqrt((lam * (e - mean[:, None]) ** 2).sum(1) / wsum)
 
 
-def prescreen(models, cases, top=16, unc_limit=0.02, max_reruns=256, chunk=8192, log=print):
+def scalar_inputs(X6):
+    """A case's scalar inputs: the four log-scaled run parameters (gamma, R,
+    sigma_s, pipe width) and the log peak line density and log mean squared
+    slope of its profile (the amplitude law's features without the constant)."""
+    return amp_features(X6)[:, 1:]
+
+
+@dataclasses.dataclass
+class Calibration:
+    """The ensemble spread turned into an error estimate, from held-out cases.
+
+    spread  = ensemble standard deviation / |ensemble mean| of a prediction;
+    error   ~ k * spread, k the q-quantile over the held-out cases of
+              (relative wake error against PIC) / (relative wake spread);
+    edge    = a scalar input outside the [q_edge, 1 - q_edge] quantile range of
+              the training cases: an extrapolation, where the networks can share
+              a bias their spread does not show.
+    """
+    k: float
+    lo: np.ndarray
+    hi: np.ndarray
+    q: float
+    q_edge: float
+
+    def edge(self, X6):
+        z = scalar_inputs(X6)
+        return np.any((z < self.lo) | (z > self.hi), axis=1)
+
+
+def wake_spread(preds):
+    """Relative spread of an ensemble's wake predictions [models][N][bins][stations]."""
+    P = np.asarray(preds, dtype=np.float64)
+    sd = P.std(0).reshape(P.shape[1], -1)
+    mn = P.mean(0).reshape(P.shape[1], -1)
+    return np.linalg.norm(sd, axis=1) / np.maximum(np.linalg.norm(mn, axis=1), 1e-300)
+
+
+def calibrate(errors, spreads, X6_train, q=0.9, q_edge=0.01):
+    """Calibration from held-out relative errors and spreads and the training
+    cases' inputs (see Calibration)."""
+    ratio = np.asarray(errors) / np.maximum(np.asarray(spreads), 1e-12)
+    z = scalar_inputs(X6_train)
+    return Calibration(k=float(np.quantile(ratio, q)), lo=np.quantile(z, q_edge, axis=0),
+                       hi=np.quantile(z, 1 - q_edge, axis=0), q=q, q_edge=q_edge)
+
+
+def prescreen(models, cases, top=16, unc_limit=0.02, max_reruns=256, chunk=8192, log=print, calib=None):
     """Objective of every variant under each model of an ensemble; returns
     the variants to rerun in PIC (the `top` best by the ensemble mean, then
-    every variant whose ensemble spread exceeds unc_limit of its mean, most
-    uncertain first, up to max_reruns in all), with the screen's timing."""
+    every variant whose uncertainty exceeds unc_limit of its mean, most
+    uncertain first, up to max_reruns in all: PIC runs are the budget), with
+    the screen's timing.  The uncertainty is the ensemble spread, or with a
+    Calibration k times the spread, and every variant at the edge of the
+    training inputs counts as uncertain (ahead of the rest)."""
     from . import wakeset
     t = time.perf_counter()
     X6 = wakeset.features(cases)
@@ -327,12 +376,19 @@ def prescreen(models, cases, top=16, unc_limit=0.02, max_reruns=256, chunk=8192,
     t_net = time.perf_counter() - t
     J = np.array(J)
     mean, unc = J.mean(0), J.std(0) / J.mean(0)
+    edge = np.zeros(len(cases), dtype=bool)
+    if calib is not None:
+        unc = calib.k * unc
+        edge = calib.edge(X6)
     best = np.argsort(mean)[:top]
     bset = set(best.tolist())
-    risky = [k for k in np.argsort(-unc) if unc[k] > unc_limit and k not in bset]
+    order = np.lexsort((-unc, ~edge))          # edge cases first, then by uncertainty
+    risky = [k for k in order if (unc[k] > unc_limit or edge[k]) and k not in bset]
     rerun = list(best) + risky[:max(0, max_reruns - top)]
     rec = {"variants": len(cases), "models": len(models), "features_s": t_feat, "network_s": t_net,
-           "over_unc_limit": int(np.sum(unc > unc_limit)), "reruns": len(rerun),
+           "over_unc_limit": int(np.sum(unc > unc_limit)), "at_training_edge": int(edge.sum()),
+           "uncertain": int(np.sum((unc > unc_limit) | edge)), "reruns": len(rerun),
+           "rerun_budget": max_reruns, "calibrated": calib is not None,
            "unc_median": float(np.median(unc)), "unc_p99": float(np.quantile(unc, 0.99))}
     if log:
         log(json.dumps(rec))
@@ -451,16 +507,22 @@ def study(d, models=4, steps=40000, variants=100000, top=16, out=None, log=print
     mean, mask, runs = pic_reference(held, log=None)
     R["eval"] = [evaluate(m, d, ref=(mean, mask), log=None)[0] for m in nets]
     R["eval_against_single_pic"] = evaluate(nets[0], d, log=None)[0]
-    P = np.mean([m.predict(d["X"][te]) for m in nets], axis=0)
+    preds = [m.predict(d["X"][te]) for m in nets]
+    P = np.mean(preds, axis=0)
     err = rel_errors(P, mean, mask)
     kinds = np.array([c.kind for c in held])
     R["ensemble_mean_eval"] = {"all": _summary(err), **{n: _summary(err[kinds == i]) for i, n in
                                                         enumerate(("gaussian", "flat_top", "double_horn"))}}
+    # the spread calibrated on the held-out cases (the prescreen's uncertainty)
+    spread = wake_spread(preds)
+    calib = calibrate(err, spread, d["X"][tr])
+    R["calibration"] = {"k": calib.k, "quantile": calib.q, "edge_quantile": calib.q_edge,
+                        "spread": _summary(spread), "held_out_within_k_spread": float(np.mean(err <= calib.k * spread))}
     dump()
     t = time.perf_counter()
     var = c5_variants(variants)
     t_var = time.perf_counter() - t
-    rerun, best, J, unc, rec = prescreen(nets, var, top=top, log=None)
+    rerun, best, J, unc, rec = prescreen(nets, var, top=top, log=None, calib=calib)
     rec["variants_s"] = t_var
     R["prescreen"] = rec
     dump()
@@ -469,7 +531,8 @@ def study(d, models=4, steps=40000, variants=100000, top=16, out=None, log=print
     pm, pmask, _ = pic_reference(sel, log=None)
     t_pic = time.perf_counter() - t
     Xs = wakeset.features(sel)
-    Ps = np.mean([m.predict(Xs) for m in nets], axis=0)
+    preds_s = [m.predict(Xs) for m in nets]
+    Ps = np.mean(preds_s, axis=0)
     ran = np.all(np.isfinite(pm.reshape(len(sel), -1)), axis=1)     # the reference's geometry asserts for a few
     e_sel = np.full(len(sel), np.nan)
     e_sel[ran] = rel_errors(Ps[ran], pm[ran], pmask[ran])
@@ -478,6 +541,12 @@ def study(d, models=4, steps=40000, variants=100000, top=16, out=None, log=print
     rank = lambda a: np.argsort(np.argsort(a))
     istop = np.arange(len(sel)) < len(best)
     b = int(np.argmin(np.where(ran, Jp, np.inf)))
+    # how the calibrated wake uncertainty k * spread covers the reruns' actual errors
+    u_sel = calib.k * wake_spread(preds_s)
+    sel_edge = calib.edge(Xs)
+    R["calibration"]["reruns_within_k_spread"] = float(np.mean(e_sel[ran] <= u_sel[ran])) if ran.any() else None
+    R["calibration"]["reruns_calibrated_uncertainty"] = _summary(u_sel)
+    R["calibration"]["reruns_at_training_edge"] = int(sel_edge.sum())
     R["reruns"] = {"count": len(sel), "ran": int(ran.sum()), "pic_seconds_4_shifts": t_pic,
                    "wake_err": _summary(e_sel), "wake_err_top": _summary(e_sel[istop]),
                    "wake_err_uncertain": _summary(e_sel[~istop]),
