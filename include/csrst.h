@@ -380,13 +380,13 @@ int csrst_get_bunch32(csrst_handle *h, int which, int *cell, float *o0, float *o
  *    ni * nj above 2^20 is rejected with CSRST_E_ARG.  Nothing is allocated
  *    or freed (no cudaMalloc, cudaFree or allocating library call).
  *  - The first call on a device looks up the array's device address
- *    (cudaGetSymbolAddress) and keeps it for the life of the process; make
- *    that first call before any stream capture begins.  After
+ *    (cudaGetSymbolAddress) and keeps it for the life of the process.  After
  *    cudaDeviceReset the kept address is stale: calls after a reset are not
  *    supported.
  *  - Runs on `stream` (a cudaStream_t, NULL = default stream) and waits for
  *    that stream before it returns, because it reads the crossing and
- *    dropped-contribution flags back.  All calls share the one array per
+ *    dropped-contribution flags back; so it cannot be called while a stream
+ *    is being captured into a graph.  All calls share the one array per
  *    device, so calls that overlap on the GPU (other threads or streams) race.
  *  - Same return values as csrst_deposit (CSRST_E_CROSSINGS, CSRST_W_OUTSIDE);
  *    csrst_get_error(NULL) gives the message of a failure or warning. */
