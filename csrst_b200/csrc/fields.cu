@@ -974,19 +974,21 @@ __device__ __forceinline__ int yee_tile(const YeeTileArgs<T> &a, int tile, uint3
   tile_rest<T, G, 4>(a, t, cuts, ncut, 1, G::TY + 1, 0);
   __syncthreads();
   // the tile's cells, every one (unchanged ones too) except the fix-up's,
-  // into the destination set: 16-byte pieces of storage columns [s0, s0 + TX)
+  // into the destination set: 16-byte pieces of storage columns [s0, s0 + TX),
+  // the same piece of all four planes per step
   constexpr int NV = G::TX / G::V;
+  for (int k = threadIdx.x; k < G::TY * NV; k += G::THREADS) {
+    const int r = 1 + k / NV, v = k % NV, j = t.j0 + r;
+    if (j >= f.Ny) break;  // rows grow with k
+    const int so = r * G::W + G::V + v * G::V;        // shared-memory offset of the piece
+    const size_t go = (size_t)(j + 1) * a.out[0].pitch + s0 + v * G::V;  // the planes share one pitch
+    const int i = s0 + v * G::V - 1;  // cell of the piece's first element
+    const bool whole = j < R.r0 || j >= R.r1 || i + G::V <= R.c0 || i >= R.c1;
 #pragma unroll
-  for (int p = 0; p < 4; ++p) {
-    const T *sp = p == 0 ? sEx : p == 1 ? sEy : p == 2 ? sHx : sHy;
-    const PlaneT<T> &out = a.out[p];
-    for (int k = threadIdx.x; k < G::TY * NV; k += G::THREADS) {
-      const int r = 1 + k / NV, v = k % NV, j = t.j0 + r;
-      if (j >= f.Ny) break;  // rows grow with k
-      const T *src = sp + r * G::W + G::V + v * G::V;
-      T *dst = out.p + (size_t)(j + 1) * out.pitch + s0 + v * G::V;
-      const int i = s0 + v * G::V - 1;  // cell of the piece's first element
-      if (j < R.r0 || j >= R.r1 || i + G::V <= R.c0 || i >= R.c1) {
+    for (int p = 0; p < 4; ++p) {
+      const T *src = (p == 0 ? sEx : p == 1 ? sEy : p == 2 ? sHx : sHy) + so;
+      T *dst = a.out[p].p + go;
+      if (whole) {
         st16(dst, *reinterpret_cast<const Vec16<T> *>(src));
       } else {
 #pragma unroll
@@ -1485,6 +1487,8 @@ static int fill_tile_args(YeeTileArgs<T> &t, const FieldArgsT<T> &a, const Plane
                           int kpitch, const int *cutidx, long long spin, int *tilesY) {
   using G = YeeTile<T>;
   if (kpitch < a.Nx + 2 || kpitch % 16) return kErrArg;
+  for (int p = 1; p < 4; ++p)  // the tiles store the four planes with one row pitch
+    if (dst[p].pitch != dst[0].pitch) return kErrArg;
   const CUtensorMapDataType dt = sizeof(T) == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
   const PlaneT<T> *src[4] = {&a.Ex, &a.Ey, &a.Hx, &a.Hy};
   for (int p = 0; p < 4; ++p) {
