@@ -1448,12 +1448,7 @@ void launch_reset_outside(FieldArgsT<T> a, const int *cutidx, cudaStream_t s) {
 
 // --- fused sweep: host side ---------------------------------------------------
 
-using EncodeTiled = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
-                                 const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
-                                 CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
-
-// cuTensorMapEncodeTiled of the driver, found once through the runtime.
-static EncodeTiled tensor_map_encoder() {
+EncodeTiled tensor_map_encoder() {
   static const EncodeTiled fn = [] {
     void *p = nullptr;
     cudaDriverEntryPointQueryResult q{};

@@ -1,26 +1,43 @@
 // BF16 tensor-core GEMM on the 5th-generation tensor cores (tcgen05) for the
 // surrogate network: C[M, N] = A[M, K] . B[N, K]^T with FP32 accumulation, both
-// operands K-major (rows contiguous along K), batched over blockIdx.z.
+// operands K-major (rows contiguous along K), batched, over one or two K
+// segments into one accumulator.
 //
-// One CTA of 128 threads computes a 128 x BN tile:
-//   - the A and B tiles of 64 K-columns are copied to shared memory with
-//     cp.async in two stages, in the tensor core's canonical K-major layout
-//     without swizzle: 8-row x 16-byte core matrices, the 8-row groups 128 B
-//     apart (SBO) and the 8-element K chunks a whole tile column apart (LBO);
-//   - one thread issues four tcgen05.mma (M = 128, N = BN, K = 16 each) per
-//     stage into an FP32 accumulator in tensor memory (TMEM) and commits them
-//     to the stage's mbarrier, which frees the stage for the next copy;
-//   - the epilogue reads the accumulator with tcgen05.ld (warp w owns TMEM
-//     lanes 32w .. 32w + 31, i.e. rows) into an FP32 staging tile in the
-//     freed operand stages, then writes FP32 and/or BF16 outputs through
-//     affine index maps (transposed and mode-major layouts come out
-//     directly), each swept in the order - along rows or along columns -
-//     that puts a warp's stores next to each other under its map.
+// Persistent and warp-specialised: one CTA of 576 threads per SM walks the
+// 128 x BN output tiles (batch, row tile, column tile) in a fixed stride.
+//   - warp 0 (one lane) copies the A and B tiles of 64 K-columns with TMA
+//     (128-byte swizzle; 3-D tensor maps over (K, rows, batch) for batched
+//     operands, rows past the matrix read as zero) into a ring of stages, each
+//     stage completing on its `full` mbarrier;
+//   - warp 1 (one lane) issues four tcgen05.mma (M = 128, N = BN, K = 16) per
+//     stage into one of the FP32 accumulators in tensor memory (TMEM), commits
+//     them to the stage's `empty` mbarrier, which hands the stage back to the
+//     copies, and at the end of a tile to the accumulator's `acc_full`
+//     mbarrier;
+//   - warps 2..17 (the epilogue) read the accumulator with tcgen05.ld (warp w
+//     may read TMEM lanes 32 (w % 4) .. + 31, i.e. rows; the four warps of a
+//     row quarter take one 32-column chunk each, of the same tile when BN is
+//     128, else of 2 or 4 tiles in turn, with 4 or 8 accumulators of BN
+//     columns in the 256 TMEM columns), hand it back through
+//     `acc_empty` after their read, add the biases and write FP32 and/or BF16
+//     outputs through affine index maps: as 16-byte runs through a 32 x 33
+//     staging block in shared memory where the map allows (below), else
+//     element by element, a warp storing whole columns of its 32 rows (lanes
+//     on consecutive rows, straight from the registers) or, through the
+//     staging block, whole rows, whichever puts a warp's 32 stores next to
+//     each other under the map.  Sixteen epilogue warps, four per scheduler,
+//     hide the latency of each warp's dependent steps.
+// With two or more accumulators the epilogue of one tile overlaps the copies and
+// products of the next, and the copies run up to a ring ahead of the
+// products, so the kernel streams its operands and outputs at once.
+//
 // Waits on mbarriers are bounded (a launch parameter, csrst_gemm_set_wait_limit):
-// a wait that gives up sets *err and skips the epilogue; the kernel then waits,
-// with the default bound, for the tensor-core work it has issued and for its
-// copies in flight before it frees the TMEM and returns, so that nothing
-// still writes into TMEM or shared memory it no longer owns.
+// a wait that gives up sets *err = 1 and a shared flag that ends the other
+// roles' loops at their next wait.  Before the TMEM is freed, the copy warp
+// waits for every copy it issued and the MMA warp for every product it
+// issued (with the default bound; *err = 2 if even that gives up), so nothing
+// still writes into TMEM or shared memory the CTA no longer owns.
+#include <cuda.h>
 #include <cuda_bf16.h>
 #include <stdint.h>
 
@@ -30,24 +47,32 @@
 namespace csrst {
 namespace {
 
-constexpr int kBM = 128, kBK = 64, kThreads = 128;
+constexpr int kBM = 128, kBK = 64;
+constexpr int kEpiWarps = 16, kThreads = 64 + 32 * kEpiWarps;
 constexpr long long kSpin = 1ll << 24;  // default mbarrier polls before a wait gives up
 
-__device__ __forceinline__ void cp_async16(void *dst, const void *src) {
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+template <int BN>
+struct Cfg {
+  static constexpr int A_BYTES = kBM * kBK * 2;               // 16 KB, 128 rows of 128 B
+  static constexpr int B_BYTES = BN * kBK * 2;
+  static constexpr int STAGE = A_BYTES + B_BYTES;             // multiples of 1024 B: swizzle atoms stay aligned
+  static constexpr int STAGES = BN == 128 ? 4 : 6;
+  static constexpr int EPI = kEpiWarps * 32 * 33 * 4;         // per-warp 32 x 33 FP32 staging blocks
+  static constexpr int SMEM = STAGES * STAGE + EPI + 1024;    // + alignment slack
+  static constexpr int TMEM_COLS = 256;                       // NACC accumulators of BN columns
+  static constexpr int NACC = TMEM_COLS / BN;                 // 2, 4 or 8
+  static constexpr int CHUNKS = BN / 32;                      // 32-column pieces of a tile
+  static constexpr int TG = 4 / CHUNKS;                       // epilogue groups working on different tiles
+};
 
-// Shared-memory matrix descriptor, K-major, no swizzle (version 1 for sm_100).
-__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
-  uint64_t d = 0;
-  d |= (uint64_t)((addr >> 4) & 0x3FFF);
-  d |= (uint64_t)((lbo >> 4) & 0x3FFF) << 16;
-  d |= (uint64_t)((sbo >> 4) & 0x3FFF) << 32;
-  d |= (uint64_t)1 << 46;  // descriptor version
-  return d;                // base offset 0, legacy LBO mode, layout type 0 (no swizzle)
+// Shared-memory matrix descriptor of a K-major operand tile with 128-byte
+// swizzle (the layout a TMA copy with CU_TENSOR_MAP_SWIZZLE_128B writes):
+// rows 128 B apart, 8-row atoms 1024 B apart (SBO), LBO unused (1),
+// descriptor version 1, layout type 2.  Stepping K by 16 elements adds 32 B
+// to the start address inside the atom.
+__device__ __forceinline__ uint64_t sw128_desc(uint32_t addr) {
+  return (uint64_t)((addr >> 4) & 0x3FFF) | ((uint64_t)1 << 16) | ((uint64_t)(1024 >> 4) << 32) |
+         ((uint64_t)1 << 46) | ((uint64_t)2 << 61);
 }
 
 // Instruction descriptor of kind::f16: FP32 accumulator, BF16 A and B, both
@@ -66,64 +91,74 @@ __device__ __forceinline__ void mma_bf16(uint32_t tmem, uint64_t da, uint64_t db
       : "r"(tmem), "l"(da), "l"(db), "r"(idesc), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
 }
 
+// Arrives on `bar` once every tensor-core operation this thread issued before
+// it has completed.
 __device__ __forceinline__ void mma_commit(uint64_t *bar) {
   asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
                : "memory");
 }
 
-__device__ __forceinline__ float gelu(float x) { return 0.5f * x * (1.0f + erff(x * 0.70710678118654752f)); }
-
-// Copies rows [r0, r0 + R) x K-columns [k0, k0 + 64) of a K-major matrix into
-// the canonical layout: element (r, k) at ((k / 8) * (R / 8) + r / 8) * 128 +
-// (r % 8) * 16 + (k % 8) * 2 bytes.  Rows at or beyond `rows` are zero.
-template <int R>
-__device__ __forceinline__ void load_tile(uint8_t *dst, const __nv_bfloat16 *src, long long ld, int r0, int rows,
-                                          int k0) {
-  constexpr int chunks = R * (kBK / 8);  // 16-byte pieces
-#pragma unroll
-  for (int c = threadIdx.x; c < chunks; c += kThreads) {
-    const int r = c % 8 + 8 * ((c / 8) % (R / 8));  // row: 8 consecutive threads take one core matrix column
-    const int kc = c / R;                           // K chunk
-    uint8_t *d = dst + ((kc * (R / 8) + r / 8) * 128 + (r % 8) * 16);
-    if (r0 + r < rows) {
-      cp_async16(d, src + (long long)(r0 + r) * ld + k0 + kc * 8);
-    } else {
-      *reinterpret_cast<uint4 *>(d) = make_uint4(0, 0, 0, 0);
-    }
-  }
+// Starts the load of 32 accumulator columns (TMEM lanes of this warp, one row
+// per lane) into v; the registers hold the values only after tmem_wait(v).
+__device__ __forceinline__ void tmem_ld32(uint32_t ta, uint32_t *v) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+      "%15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]), "=r"(v[8]),
+        "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]), "=r"(v[16]),
+        "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]), "=r"(v[24]),
+        "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+      : "r"(ta));
 }
 
-// Affine output index of tile element (m, n) of batch z under a map.
-__device__ __forceinline__ long long map_index(long long zb, int m, int n, int md, int nd, long long s0, long long s1,
-                                               long long t0, long long t1) {
-  return zb + (long long)(m / md) * s0 + (long long)(m % md) * s1 + (long long)(n / nd) * t0 +
-         (long long)(n % nd) * t1;
+// Waits for this thread's TMEM loads; v is named so that no use of it moves
+// above the wait.
+__device__ __forceinline__ void tmem_wait(uint32_t *v) {
+  asm volatile("tcgen05.wait::ld.sync.aligned;"
+               : "+r"(v[0]), "+r"(v[1]), "+r"(v[2]), "+r"(v[3]), "+r"(v[4]), "+r"(v[5]), "+r"(v[6]), "+r"(v[7]),
+                 "+r"(v[8]), "+r"(v[9]), "+r"(v[10]), "+r"(v[11]), "+r"(v[12]), "+r"(v[13]), "+r"(v[14]),
+                 "+r"(v[15]), "+r"(v[16]), "+r"(v[17]), "+r"(v[18]), "+r"(v[19]), "+r"(v[20]), "+r"(v[21]),
+                 "+r"(v[22]), "+r"(v[23]), "+r"(v[24]), "+r"(v[25]), "+r"(v[26]), "+r"(v[27]), "+r"(v[28]),
+                 "+r"(v[29]), "+r"(v[30]), "+r"(v[31])
+               :
+               : "memory");
 }
 
-// Visits the tile's (row, column) pairs in groups of eight per thread, so
-// that the 32 lanes of a warp take consecutive columns (m_fast == 0) or
-// consecutive rows (m_fast == 1): the order in which the output map puts
-// neighbouring lanes next to each other.  A group's reads of global memory
-// (residual, accumulated output) are all issued before its first store.
-constexpr int kGroup = 8;
-template <int BN, class F>
-__device__ __forceinline__ void tile_order(int m_fast, F &&f) {
-  int rr[kGroup], cc[kGroup];
-  if (m_fast) {
-    for (int c = 0; c < BN; c += kGroup) {
-#pragma unroll
-      for (int j = 0; j < kGroup; ++j) rr[j] = threadIdx.x, cc[j] = c + j;
-      f(rr, cc);
-    }
-  } else {
-    constexpr int kRows = kThreads / BN;  // rows per sweep of the block
-    const int c = threadIdx.x % BN;
-    for (int r = threadIdx.x / BN; r < kBM; r += kGroup * kRows) {
-#pragma unroll
-      for (int j = 0; j < kGroup; ++j) rr[j] = r + j * kRows, cc[j] = c;
-      f(rr, cc);
-    }
+// GELU, erf form: 0.5 x (1 + erf(x / sqrt 2)), with erf from the rational
+// approximation of C. Hastings (Abramowitz & Stegun 7.1.28):
+//   1 - erf(u) = (1 + a1 u + a2 u^2 + ... + a6 u^6)^-16,  u >= 0,
+// absolute error at most 3e-7.  With r = that power, 1 + erf(x / sqrt 2) is
+// r for x < 0 and 2 - r for x >= 0, so GELU is 0.5 x r or x - 0.5 x r: one
+// reciprocal and no cancellation on the negative side.
+__device__ __forceinline__ float gelu(float x) {
+  const float u = fabsf(x) * 0.70710678118654752f;
+  float p = fmaf(u, 0.0000430638f, 0.0002765672f);
+  p = fmaf(u, p, 0.0001520143f);
+  p = fmaf(u, p, 0.0092705272f);
+  p = fmaf(u, p, 0.0422820123f);
+  p = fmaf(u, p, 0.0705230784f);
+  p = fmaf(u, p, 1.0f);
+  p *= p;
+  p *= p;
+  p *= p;
+  p *= p;
+  const float h = 0.5f * x * __fdividef(1.0f, p);
+  return x < 0.0f ? h : x - h;
+}
+
+// Bounded wait of one thread that also gives up when another role has
+// failed (the shared flag, read every 64 polls).  Returns false on either;
+// a wait that ran out of polls raises the flag and sets *err = 1.
+__device__ __forceinline__ bool wait_role(uint64_t *bar, uint32_t parity, long long spin, volatile int *fail,
+                                          int *err) {
+  if (spin > 0 && mbar_test(bar, parity)) return true;
+  for (long long k = 1; k < spin; ++k) {
+    if (mbar_try(bar, parity)) return true;
+    if ((k & 63) == 0 && *fail) return false;
   }
+  *fail = 1;
+  atomicExch(err, 1);
+  return false;
 }
 
 // One K segment of a product: A[M, Kseg] and B[N, Kseg], K-major, batch
@@ -138,187 +173,357 @@ struct Seg {
   int nk;
 };
 
-template <int BN>
-__global__ void __launch_bounds__(kThreads) k_gemm(Seg g0, Seg g1, int M, int N, csrst_gemm_epilogue ep, int *err,
-                                                   int o_mfast, int t_mfast, long long spin) {
-  extern __shared__ __align__(1024) uint8_t smem[];
-  __shared__ uint64_t bar[3];  // MMA commits of the two stages; bar[2]: nothing arrives on it
-  __shared__ uint32_t tmem_base;
-  __shared__ int s_fail, s_last;  // a wait gave up; the last MMA commit issued
-  constexpr int kA = kBM * kBK * 2, kB = BN * kBK * 2, kStage = kA + kB;
-  uint8_t *base = smem + ((1024 - (smem_u32(smem) & 1023)) & 1023);
-  const int z = blockIdx.z, m0 = blockIdx.y * kBM, n0 = blockIdx.x * BN;
-  g0.A += (long long)z * g0.sA;
-  g0.B += (long long)z * g0.sB;
-  if (g1.nk) {
-    g1.A += (long long)z * g1.sA;
-    g1.B += (long long)z * g1.sB;
-  }
-  // copies K tile kt (of either segment) into a stage
-  auto load_k = [&](uint8_t *stage, int kt) {
-    const Seg &g = kt < g0.nk ? g0 : g1;
-    const int k0 = (kt < g0.nk ? kt : kt - g0.nk) * kBK;
-    load_tile<kBM>(stage, g.A, g.lda, m0, M, k0);
-    load_tile<BN>(stage + kBM * kBK * 2, g.B, g.ldb, n0, N, k0);
-  };
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+// Vector stores.  Where an output map, restricted to a 32 x 32 piece of a
+// tile that starts on multiples of 32, is index = base + rdel[i] + cdel[j]
+// (row and column divisors that divide 32 or are multiples of it), the
+// piece is written as runs of 16 bytes (L = 8 BF16 or 4 FP32 elements at
+// consecutive indices), one per lane and store.  A run's elements lie, from
+// its origin (i0, j0), at
+//   shape 0: (i0, j0 + t)                      L columns of a row
+//   shape 1: (i0 + t, j0)                      L rows of a column
+//   shape 2: (i0 + t / 2, j0 + t % 2)          column pairs over L/2 rows
+//   shape 3: (i0 + t % 2, j0 + t / 2)          row pairs over L/2 columns
+// (the host finds the shape a map allows, checks every run of the piece and
+// the 16-byte alignment of every piece's base, and orders the lanes along
+// i or j, whichever keeps a warp's runs on fewer sectors).
+struct RunShape {
+  int shape;   // 0..3, or -1: the map has no vector form
+  int fast_j;  // lanes take consecutive run origins along j (else along i)
+};
 
-  if (warp == 0) {  // TMEM: BN FP32 columns x 128 lanes
+// Everything one launch reads: the operand tensor maps (A1, B1, A2, B2;
+// 3-D over (K, rows, batch) where the operand has a batch stride, else
+// 2-D), the epilogue, the tile grid, the sweep orders of the two maps and
+// their vector forms (vec: every output of the launch has one and there is
+// no residual or accumulation).
+struct alignas(64) GemmArgs {
+  CUtensorMap map[4];
+  csrst_gemm_epilogue ep;
+  int *err;
+  long long spin;
+  long long ntiles;
+  int nk1, nk2, M, N, tilesM, tilesN;
+  int rank3[4];
+  int o_mfast, t_mfast;
+  int vec;
+  RunShape rs[4];             // pre, out32, out16 (primary map), out16t (second map)
+  long long del[2][2][32];    // [map][rows, columns][i or j]
+};
+
+// Row and column parts of an output map's index: z*sb + (m/md)*s0 + (m%md)*s1
+// and (n/nd)*t0 + (n%nd)*t1.
+__device__ __forceinline__ long long row_part(long long zb, int m, int md, long long s0, long long s1) {
+  return zb + (long long)(m / md) * s0 + (long long)(m % md) * s1;
+}
+__device__ __forceinline__ long long col_part(int n, int nd, long long t0, long long t1) {
+  return (long long)(n / nd) * t0 + (long long)(n % nd) * t1;
+}
+
+// One element under the primary map: residual, pre-activation, activation,
+// FP32 and BF16 outputs; returns the value the second map copies.
+__device__ __forceinline__ float finish(const csrst_gemm_epilogue &ep, long long o, float x) {
+  if (ep.res) x += ep.res[o];
+  if (ep.pre) ep.pre[o] = x;
+  if (ep.act == 1) x = gelu(x);
+  if (ep.out32) ep.out32[o] = ep.accumulate ? ep.out32[o] + x : x;
+  if (ep.out16) reinterpret_cast<__nv_bfloat16 *>(ep.out16)[o] = __float2bfloat16(x);
+  return x;
+}
+
+// Writes one 32-row x 32-column piece of a tile held by a warp (lane = row
+// mrow + lane, x[j] = column ncol + j, biases added) through both output
+// maps.  Under a map whose consecutive rows are neighbours the warp stores a
+// column per instruction straight from the registers; otherwise the piece
+// goes through the warp's staging block st[32][33] (conflict-free both ways)
+// and the warp stores a row per instruction.
+__device__ __forceinline__ void store_piece(const GemmArgs &a, float (&x)[32], float *st, int lane, int mrow, int ncol,
+                                            long long orow, long long trow, long long ocol, long long tcol) {
+  const csrst_gemm_epilogue &ep = a.ep;
+  const bool mok = mrow + lane < a.M, nok = ncol + lane < a.N;
+  if (a.o_mfast) {
+#pragma unroll
+    for (int j = 0; j < 32; ++j) {
+      const long long oc = __shfl_sync(0xffffffffu, ocol, j);
+      if (mok && ncol + j < a.N) x[j] = finish(ep, orow + oc, x[j]);
+    }
+  } else {
+#pragma unroll
+    for (int j = 0; j < 32; ++j) st[lane * 33 + j] = x[j];
+    __syncwarp();
+#pragma unroll 4
+    for (int i = 0; i < 32; ++i) {
+      const long long ori = __shfl_sync(0xffffffffu, orow, i);
+      if (mrow + i < a.M && nok) st[i * 33 + lane] = finish(ep, ori + ocol, st[i * 33 + lane]);
+    }
+    __syncwarp();
+    if (ep.out16t && a.t_mfast) {
+#pragma unroll
+      for (int j = 0; j < 32; ++j) x[j] = st[lane * 33 + j];
+    }
+  }
+  if (ep.out16t) {
+    __nv_bfloat16 *t16 = reinterpret_cast<__nv_bfloat16 *>(ep.out16t);
+    if (a.t_mfast) {
+#pragma unroll
+      for (int j = 0; j < 32; ++j) {
+        const long long tc = __shfl_sync(0xffffffffu, tcol, j);
+        if (mok && ncol + j < a.N) t16[trow + tc] = __float2bfloat16(x[j]);
+      }
+    } else {
+      if (a.o_mfast) {
+#pragma unroll
+        for (int j = 0; j < 32; ++j) st[lane * 33 + j] = x[j];
+        __syncwarp();
+      }
+#pragma unroll 4
+      for (int i = 0; i < 32; ++i) {
+        const long long tri = __shfl_sync(0xffffffffu, trow, i);
+        if (mrow + i < a.M && nok) t16[tri + tcol] = __float2bfloat16(st[i * 33 + lane]);
+      }
+    }
+  }
+  __syncwarp();  // the staging block is free for the next piece
+}
+
+// Row and column offsets of element t of a run of shape S, and the run's
+// extent in rows (RI) and columns (RJ).
+template <int S, int L>
+struct Run {
+  static constexpr int RI = S == 0 ? 1 : S == 1 ? L : S == 2 ? L / 2 : 2;
+  static constexpr int RJ = S == 0 ? L : S == 1 ? 1 : S == 2 ? 2 : L / 2;
+  static __device__ __forceinline__ int di(int t) { return S == 0 ? 0 : S == 1 ? t : S == 2 ? t >> 1 : t & 1; }
+  static __device__ __forceinline__ int dj(int t) { return S == 0 ? t : S == 1 ? 0 : S == 2 ? t & 1 : t >> 1; }
+};
+
+__device__ __forceinline__ uint32_t bf16x2(float lo, float hi) {
+  const __nv_bfloat162 h = __floats2bfloat162_rn(lo, hi);
+  return *reinterpret_cast<const uint32_t *>(&h);
+}
+
+// Writes a staged piece st[32][33] (final values) as runs of shape S: the
+// warp's 32 lanes take 32 runs per store, 1024 / L runs in all.
+template <int S, int L>
+__device__ __forceinline__ void store_runs(const float *st, const long long *rdel, const long long *cdel, void *out,
+                                           long long base, int lane, int fast_j) {
+  using R = Run<S, L>;
+  constexpr int NI = 32 / R::RI, NJ = 32 / R::RJ;
+#pragma unroll
+  for (int k = 0; k < NI * NJ / 32; ++k) {
+    const int r = k * 32 + lane;
+    const int oi = (fast_j ? r / NJ : r % NI) * R::RI, oj = (fast_j ? r % NJ : r / NI) * R::RJ;
+    float v[L];
+#pragma unroll
+    for (int t = 0; t < L; ++t) v[t] = st[(oi + R::di(t)) * 33 + oj + R::dj(t)];
+    const long long o = base + rdel[oi] + cdel[oj];
+    if constexpr (L == 8) {
+      *reinterpret_cast<uint4 *>(reinterpret_cast<__nv_bfloat16 *>(out) + o) =
+          make_uint4(bf16x2(v[0], v[1]), bf16x2(v[2], v[3]), bf16x2(v[4], v[5]), bf16x2(v[6], v[7]));
+    } else {
+      *reinterpret_cast<float4 *>(reinterpret_cast<float *>(out) + o) = make_float4(v[0], v[1], v[2], v[3]);
+    }
+  }
+}
+
+template <int L>
+__device__ __forceinline__ void store_vec(const RunShape &rs, const float *st, const long long *rdel,
+                                          const long long *cdel, void *out, long long base, int lane) {
+  switch (rs.shape) {
+    case 0: store_runs<0, L>(st, rdel, cdel, out, base, lane, rs.fast_j); break;
+    case 1: store_runs<1, L>(st, rdel, cdel, out, base, lane, rs.fast_j); break;
+    case 2: store_runs<2, L>(st, rdel, cdel, out, base, lane, rs.fast_j); break;
+    default: store_runs<3, L>(st, rdel, cdel, out, base, lane, rs.fast_j); break;
+  }
+}
+
+// A whole 32 x 32 piece (lane = row, x[j] = column j, biases added) through
+// the vector forms: the pre-activation, then the activation, then the FP32
+// and BF16 copies, each from the warp's staging block.  obase / tbase: the
+// piece's base index under the primary and the second map.
+__device__ __forceinline__ void store_piece_vec(const GemmArgs &a, const long long (*del)[2][32], float (&x)[32],
+                                                float *st, int lane, long long obase, long long tbase) {
+  const csrst_gemm_epilogue &ep = a.ep;
+  if (ep.pre) {
+#pragma unroll
+    for (int j = 0; j < 32; ++j) st[lane * 33 + j] = x[j];
+    __syncwarp();
+    store_vec<4>(a.rs[0], st, del[0][0], del[0][1], ep.pre, obase, lane);
+    __syncwarp();
+  }
+  if (ep.act == 1) {
+#pragma unroll
+    for (int j = 0; j < 32; ++j) x[j] = gelu(x[j]);
+  }
+#pragma unroll
+  for (int j = 0; j < 32; ++j) st[lane * 33 + j] = x[j];
+  __syncwarp();
+  if (ep.out32) store_vec<4>(a.rs[1], st, del[0][0], del[0][1], ep.out32, obase, lane);
+  if (ep.out16) store_vec<8>(a.rs[2], st, del[0][0], del[0][1], ep.out16, obase, lane);
+  if (ep.out16t) store_vec<8>(a.rs[3], st, del[1][0], del[1][1], ep.out16t, tbase, lane);
+  __syncwarp();  // the staging block is free for the next piece
+}
+
+template <int BN>
+__global__ void __launch_bounds__(kThreads, 1) k_gemm(const __grid_constant__ GemmArgs a) {
+  using G = Cfg<BN>;
+  extern __shared__ __align__(1024) uint8_t smem[];
+  __shared__ uint64_t full[G::STAGES], empty[G::STAGES], acc_full[G::NACC], acc_empty[G::NACC], drain, never;
+  __shared__ uint32_t tmem_base;
+  __shared__ int s_fail;
+  __shared__ long long s_del[2][2][32];  // the maps' row and column offsets over a piece
+  uint8_t *base = smem + ((1024 - (smem_u32(smem) & 1023)) & 1023);
+  float *epi = reinterpret_cast<float *>(base + G::STAGES * G::STAGE);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  volatile int *fail = &s_fail;
+  // spin < 0: the epilogue's first wait is on `never`, which nothing
+  // completes, with -spin polls (the stuck wait the error path is tested with)
+  const bool stuck = a.spin < 0;
+  const long long spin = stuck ? -a.spin : a.spin;
+
+  if (warp == 1) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base)),
-                 "r"(BN));
+                 "r"(G::TMEM_COLS));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
   if (threadIdx.x == 0) {
-    mbar_init(&bar[0], 1);
-    mbar_init(&bar[1], 1);
-    mbar_init(&bar[2], 1);
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    for (int s = 0; s < G::STAGES; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    for (int b = 0; b < G::NACC; ++b) {
+      mbar_init(&acc_full[b], 1);
+      mbar_init(&acc_empty[b], 32 * 4 * G::CHUNKS);  // the warps that read one tile
+    }
+    mbar_init(&drain, 1);
+    mbar_init(&never, 1);
+    mbar_init_fence();
     s_fail = 0;
-    s_last = -1;
   }
+  for (int k = threadIdx.x; k < 128; k += kThreads) (&s_del[0][0][0])[k] = (&a.del[0][0][0])[k];
   asm volatile("tcgen05.fence::before_thread_sync;");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;");
   const uint32_t tmem = tmem_base;
-  const int nk = g0.nk + g1.nk;
-  // spin < 0: the first wait in the loop is on bar[2], which nothing
-  // completes, with -spin polls (the stuck wait the error path is tested with)
-  const bool stuck = spin < 0;
-  if (stuck) spin = -spin;
+  const int nk = a.nk1 + a.nk2;
 
-  load_k(base, 0);
-  cp_async_commit();
-  for (int kt = 0; kt < nk; ++kt) {
-    const int s = kt & 1;
-    if (kt + 1 < nk) {
-      const int s1 = (kt + 1) & 1;
-      if (kt >= 1) {  // the MMAs of tile kt - 1 still read stage s1
-        uint64_t *wb = stuck && kt == 1 ? &bar[2] : &bar[s1];
-        if (threadIdx.x == 0 && !mbar_wait(wb, stuck && kt == 1 ? 0u : ((kt - 1) >> 1) & 1, spin)) {
-          s_fail = 1;
-          s_last = kt - 1;
+  if (warp == 0) {
+    // ---- copies ----
+    if (lane == 0) {
+      long long it = 0;  // stage fills issued
+      bool ok = true;
+      for (long long t = blockIdx.x; t < a.ntiles && ok; t += gridDim.x) {
+        const long long r = t / a.tilesN;
+        const int n0 = (int)(t % a.tilesN) * BN, m0 = (int)(r % a.tilesM) * kBM, z = (int)(r / a.tilesM);
+        for (int kt = 0; kt < nk; ++kt) {
+          const int s = (int)(it % G::STAGES);
+          if (!wait_role(&empty[s], (uint32_t)((it / G::STAGES) & 1) ^ 1u, spin, fail, a.err)) {
+            ok = false;
+            break;
+          }
+          uint8_t *sa = base + s * G::STAGE, *sb = sa + G::A_BYTES;
+          mbar_expect_tx(&full[s], G::STAGE);
+          const int seg = kt < a.nk1 ? 0 : 1, k0 = (kt < a.nk1 ? kt : kt - a.nk1) * kBK;
+          const int ia = 2 * seg, ib = ia + 1;
+          if (a.rank3[ia]) tma_load_3d(sa, &a.map[ia], k0, m0, z, &full[s]);
+          else tma_load_2d(sa, &a.map[ia], k0, m0, &full[s]);
+          if (a.rank3[ib]) tma_load_3d(sb, &a.map[ib], k0, n0, z, &full[s]);
+          else tma_load_2d(sb, &a.map[ib], k0, n0, &full[s]);
+          ++it;
         }
-        __syncthreads();
-        if (s_fail) break;
       }
-      load_k(base + s1 * kStage, kt + 1);
-      cp_async_commit();
-      cp_async_wait<1>();
-    } else {
-      cp_async_wait<0>();
+      // every fill issued has landed before the CTA ends (fills older than
+      // the last STAGES were consumed by the products, so they had landed)
+      for (long long i = it > G::STAGES ? it - G::STAGES : 0; i < it; ++i)
+        if (!mbar_wait(&full[i % G::STAGES], (uint32_t)((i / G::STAGES) & 1), kSpin)) atomicExch(a.err, 2);
     }
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // copies visible to the tensor core
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      asm volatile("tcgen05.fence::after_thread_sync;");
-      const uint32_t a0 = smem_u32(base + s * kStage), b0 = a0 + kA;
+  } else if (warp == 1) {
+    // ---- products ----
+    if (lane == 0) {
+      long long it = 0;
+      int lt = 0;
+      bool ok = true, issued = false;
+      for (long long t = blockIdx.x; t < a.ntiles && ok; t += gridDim.x, ++lt) {
+        const int b = lt % G::NACC;
+        if (!wait_role(&acc_empty[b], (uint32_t)((lt / G::NACC) & 1) ^ 1u, spin, fail, a.err)) break;
+        asm volatile("tcgen05.fence::after_thread_sync;");
+        const uint32_t d = tmem + (uint32_t)(b * BN);
+        for (int kt = 0; kt < nk; ++kt) {
+          const int s = (int)(it % G::STAGES);
+          if (!wait_role(&full[s], (uint32_t)((it / G::STAGES) & 1), spin, fail, a.err)) {
+            ok = false;
+            break;
+          }
+          asm volatile("tcgen05.fence::after_thread_sync;");
+          const uint32_t a0 = smem_u32(base + s * G::STAGE), b0 = a0 + G::A_BYTES;
 #pragma unroll
-      for (int kk = 0; kk < kBK / 16; ++kk) {
-        // K = 16 is two 8-element chunks: advance by two chunk strides (LBO)
-        const uint64_t da = smem_desc(a0 + kk * 2 * (kBM / 8) * 128, (kBM / 8) * 128, 128);
-        const uint64_t db = smem_desc(b0 + kk * 2 * (BN / 8) * 128, (BN / 8) * 128, 128);
-        mma_bf16(tmem, da, db, instr_desc<BN>(), (kt > 0 || kk > 0) ? 1u : 0u);
+          for (int kk = 0; kk < kBK / 16; ++kk)
+            mma_bf16(d, sw128_desc(a0 + kk * 32), sw128_desc(b0 + kk * 32), instr_desc<BN>(),
+                     (kt > 0 || kk > 0) ? 1u : 0u);
+          mma_commit(&empty[s]);
+          issued = true;
+          ++it;
+        }
+        if (ok) mma_commit(&acc_full[b]);
       }
-      mma_commit(&bar[s]);
+      // every product issued has completed before the TMEM is freed
+      if (issued) {
+        mma_commit(&drain);
+        if (!mbar_wait(&drain, 0, kSpin)) atomicExch(a.err, 2);
+      }
     }
-  }
-  // the last commit covers every MMA issued before it
-  if (threadIdx.x == 0 && !s_fail && nk > 0 && !mbar_wait(&bar[(nk - 1) & 1], ((nk - 1) >> 1) & 1, spin)) {
-    s_fail = 1;
-    s_last = nk - 1;
-  }
-  __syncthreads();
-  asm volatile("tcgen05.fence::after_thread_sync;");
-  if (s_fail) {
-    // the MMAs issued so far complete in order: wait for the last commit with
-    // the default bound before the TMEM they write is freed
-    if (threadIdx.x == 0) {
-      atomicExch(err, 1);
-      if (s_last >= 0 && !mbar_wait(&bar[s_last & 1], (s_last >> 1) & 1, kSpin)) atomicExch(err, 2);
-    }
-    asm volatile("tcgen05.fence::before_thread_sync;");
-    __syncthreads();
-    asm volatile("tcgen05.fence::after_thread_sync;");
   } else {
-    // The MMAs have completed and every copy has landed: the operand stages
-    // become an FP32 staging tile [128][BN + 1] (the +1 keeps both row- and
-    // column-wise sweeps free of bank conflicts).
-    constexpr int LD = BN + 1;
-    float *tile = reinterpret_cast<float *>(base);
-    const int r = warp * 32 + lane;
-    for (int c0 = 0; c0 < BN; c0 += 16) {
-      uint32_t v[16];
-      const uint32_t ta = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0;
-      asm volatile(
-          "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
-          "%15}, [%16];"
-          : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
-            "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
-          : "r"(ta));
-      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+    // ---- epilogue: warp (q, h) owns rows 32q .. 32q + 31 and chunk h % CHUNKS (32 columns) of the
+    // tiles of group h / CHUNKS: with fewer than four chunks a tile, the groups take turns by tile ----
+    const int e = warp - 2, q = warp & 3, h = e >> 2, g = h / G::CHUNKS, c = h % G::CHUNKS;
+    float *st = epi + e * 32 * 33;
+    const csrst_gemm_epilogue &ep = a.ep;
+    int lt = 0;
+    bool first = true;
+    for (long long t = blockIdx.x; t < a.ntiles; t += gridDim.x, ++lt) {
+      if (lt % G::TG != g) continue;
+      const int b = lt % G::NACC;
+      int ok = 1;
+      if (lane == 0)
+        ok = stuck && first ? wait_role(&never, 0, spin, fail, a.err)
+                            : wait_role(&acc_full[b], (uint32_t)((lt / G::NACC) & 1), spin, fail, a.err);
+      first = false;
+      if (!__shfl_sync(0xffffffffu, ok, 0)) break;
+      asm volatile("tcgen05.fence::after_thread_sync;");
+      uint32_t v[32];
+      tmem_ld32(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(b * BN + c * 32), v);
+      tmem_wait(v);
+      asm volatile("tcgen05.fence::before_thread_sync;");
+      mbar_arrive(&acc_empty[b]);  // this warp's read of the accumulator is done: hand it back
+      const long long r = t / a.tilesN;
+      const int n0 = (int)(t % a.tilesN) * BN, m0 = (int)(r % a.tilesM) * kBM, z = (int)(r / a.tilesM);
+      const int mrow = m0 + 32 * q, m = mrow + lane;
+      const int ncol = n0 + c * 32, n = ncol + lane;
+      const long long orow = row_part((long long)z * ep.sb, m, ep.md, ep.sm0, ep.sm1);
+      const long long trow = ep.out16t ? row_part((long long)z * ep.tb, m, ep.tmd, ep.tm0, ep.tm1) : 0;
+      const long long ocol = col_part(n, ep.nd, ep.sn0, ep.sn1);
+      const long long tcol = ep.out16t ? col_part(n, ep.tnd, ep.tn0, ep.tn1) : 0;
+      const float bm = (ep.bias_m && m < a.M) ? ep.bias_m[m] : 0.0f;
+      float x[32];
+      if (ep.bias) {
+        const float bc = n < a.N ? ep.bias[n] : 0.0f;
 #pragma unroll
-      for (int j = 0; j < 16; ++j) tile[r * LD + c0 + j] = __uint_as_float(v[j]);
-    }
-    // Each map's address is a row part plus a column part: both computed once
-    // per tile (128 + BN divisions instead of two per element).
-    __shared__ long long s_row[2][kBM], s_col[2][BN];
-    {
-      const int m = m0 + threadIdx.x;
-      s_row[0][threadIdx.x] = (long long)z * ep.sb + map_index(0, m, 0, ep.md, ep.nd, ep.sm0, ep.sm1, 0, 0);
-      if (ep.out16t)
-        s_row[1][threadIdx.x] = (long long)z * ep.tb + map_index(0, m, 0, ep.tmd, ep.tnd, ep.tm0, ep.tm1, 0, 0);
-      if (threadIdx.x < BN) {
-        const int n = n0 + threadIdx.x;
-        s_col[0][threadIdx.x] = map_index(0, 0, n, 1, ep.nd, 0, 0, ep.sn0, ep.sn1);
-        if (ep.out16t) s_col[1][threadIdx.x] = map_index(0, 0, n, 1, ep.tnd, 0, 0, ep.tn0, ep.tn1);
+        for (int j = 0; j < 32; ++j) x[j] = ep.alpha * __uint_as_float(v[j]) + __shfl_sync(0xffffffffu, bc, j) + bm;
+      } else {
+#pragma unroll
+        for (int j = 0; j < 32; ++j) x[j] = ep.alpha * __uint_as_float(v[j]) + bm;
       }
-    }
-    __syncthreads();
-    // outputs through the primary map, in the order that map makes contiguous
-    tile_order<BN>(o_mfast, [&](const int *rr, const int *cc) {
-      long long o[kGroup];
-      bool ok[kGroup];
-      float rv[kGroup], ov[kGroup];
-#pragma unroll
-      for (int j = 0; j < kGroup; ++j) {
-        ok[j] = m0 + rr[j] < M && n0 + cc[j] < N;
-        o[j] = s_row[0][rr[j]] + s_col[0][cc[j]];
-      }
-#pragma unroll
-      for (int j = 0; j < kGroup; ++j) {
-        rv[j] = (ok[j] && ep.res) ? ep.res[o[j]] : 0.0f;
-        ov[j] = (ok[j] && ep.out32 && ep.accumulate) ? ep.out32[o[j]] : 0.0f;
-      }
-#pragma unroll
-      for (int j = 0; j < kGroup; ++j) {
-        if (!ok[j]) continue;
-        float x = ep.alpha * tile[rr[j] * LD + cc[j]];
-        if (ep.bias) x += ep.bias[n0 + cc[j]];
-        if (ep.bias_m) x += ep.bias_m[m0 + rr[j]];
-        if (ep.res) x += rv[j];
-        if (ep.pre) ep.pre[o[j]] = x;
-        if (ep.act == 1) x = gelu(x);
-        if (ep.out32) ep.out32[o[j]] = ep.accumulate ? ov[j] + x : x;
-        if (ep.out16) reinterpret_cast<__nv_bfloat16 *>(ep.out16)[o[j]] = __float2bfloat16(x);
-        tile[rr[j] * LD + cc[j]] = x;
-      }
-    });
-    if (ep.out16t) {  // the second BF16 copy through its own map and order
-      __syncthreads();
-      tile_order<BN>(t_mfast, [&](const int *rr, const int *cc) {
-#pragma unroll
-        for (int j = 0; j < kGroup; ++j) {
-          if (m0 + rr[j] >= M || n0 + cc[j] >= N) continue;
-          reinterpret_cast<__nv_bfloat16 *>(ep.out16t)[s_row[1][rr[j]] + s_col[1][cc[j]]] =
-              __float2bfloat16(tile[rr[j] * LD + cc[j]]);
-        }
-      });
+      if (a.vec && mrow + 32 <= a.M && ncol + 32 <= a.N)
+        store_piece_vec(a, s_del, x, st, lane, __shfl_sync(0xffffffffu, orow, 0) + __shfl_sync(0xffffffffu, ocol, 0),
+                        __shfl_sync(0xffffffffu, trow, 0) + __shfl_sync(0xffffffffu, tcol, 0));
+      else
+        store_piece(a, x, st, lane, mrow, ncol, orow, trow, ocol, tcol);
     }
   }
-  cp_async_wait<0>();  // nothing still landing in shared memory (an early exit leaves copies in flight)
   asm volatile("tcgen05.fence::before_thread_sync;");
   __syncthreads();
-  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(BN));
+  if (warp == 1) {
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(G::TMEM_COLS));
+  }
 }
 
 // 32-byte sectors one warp's 32 stores touch under a map when its lanes take
@@ -341,37 +546,173 @@ int warp_sectors(int md, int nd, long long sm0, long long sm1, long long sn0, lo
 }
 
 // 1 when a warp's stores touch fewer sectors with its lanes on consecutive
-// rows than on consecutive columns: the epilogue then sweeps the tile by rows.
+// rows than on consecutive columns: the epilogue then stores by columns.
 int rows_fast(int md, int nd, long long sm0, long long sm1, long long sn0, long long sn1, int bytes) {
   return warp_sectors(md, nd, sm0, sm1, sn0, sn1, 1, bytes) < warp_sectors(md, nd, sm0, sm1, sn0, sn1, 0, bytes);
+}
+
+// An output map as the host checks it.
+struct MapDesc {
+  int md, nd;
+  long long sb, s0, s1, t0, t1;  // batch; rows m/md, m%md; columns n/nd, n%nd
+};
+
+// Row and column offsets of a map over a 32 x 32 piece that starts on
+// multiples of 32: the same for every such piece when each divisor divides
+// 32 or is a multiple of it (false otherwise).
+bool piece_offsets(const MapDesc &d, long long *rdel, long long *cdel) {
+  if (!(32 % d.md == 0 || d.md % 32 == 0) || !(32 % d.nd == 0 || d.nd % 32 == 0)) return false;
+  for (int i = 0; i < 32; ++i) {
+    rdel[i] = (long long)(i / d.md) * d.s0 + (long long)(i % d.md) * d.s1;
+    cdel[i] = (long long)(i / d.nd) * d.t0 + (long long)(i % d.nd) * d.t1;
+  }
+  return true;
+}
+
+long long mod_pos(long long a, long long m) { return ((a % m) + m) % m; }
+
+// Every piece's base index a multiple of L (16 bytes) and the output 16-byte
+// aligned.  A piece starts at row 32p: its row part advances by (32 / md) s0
+// per piece when md divides 32, else by 32 s1 within a block of md rows and
+// by s0 between blocks; the same for columns.
+bool bases_aligned(const MapDesc &d, int M, int N, int batch, const void *p, int L) {
+  if ((uintptr_t)p % 16 || (batch > 1 && mod_pos(d.sb, L))) return false;
+  if (d.md <= 32 ? mod_pos((32 / d.md) * d.s0, L) : (mod_pos(32 * d.s1, L) || (M > d.md && mod_pos(d.s0, L))))
+    return false;
+  if (d.nd <= 32 ? mod_pos((32 / d.nd) * d.t0, L) : (mod_pos(32 * d.t1, L) || (N > d.nd && mod_pos(d.t0, L))))
+    return false;
+  return true;
+}
+
+// The first run shape (0..3) whose every run over the piece covers L
+// consecutive indices from a multiple of L, and the lane order that keeps a
+// warp's first 32 runs on fewer 32-byte sectors; shape -1 if none.
+RunShape run_shape(const long long *rdel, const long long *cdel, int L) {
+  for (int S = 0; S < 4; ++S) {
+    const int ri = S == 0 ? 1 : S == 1 ? L : S == 2 ? L / 2 : 2, rj = S == 0 ? L : S == 1 ? 1 : S == 2 ? 2 : L / 2;
+    bool ok = true;
+    for (int oi = 0; oi < 32 && ok; oi += ri)
+      for (int oj = 0; oj < 32 && ok; oj += rj) {
+        const long long o = rdel[oi] + cdel[oj];
+        ok = mod_pos(o, L) == 0;
+        for (int t = 0; t < L && ok; ++t) {
+          const int i = oi + (S == 0 ? 0 : S == 1 ? t : S == 2 ? t / 2 : t % 2);
+          const int j = oj + (S == 0 ? t : S == 1 ? 0 : S == 2 ? t % 2 : t / 2);
+          ok = rdel[i] + cdel[j] == o + t;
+        }
+      }
+    if (!ok) continue;
+    const int ni = 32 / ri, nj = 32 / rj;
+    int best = 1 << 30, fast = 1;
+    for (int f = 1; f >= 0; --f) {
+      int cost = 0;
+      for (const int unit : {32, 128}) {  // sectors, then 128-byte lines as the tie-break
+        long long seen_at[32];
+        int k = 0;
+        for (int r = 0; r < 32; ++r) {
+          const int oi = (f ? r / nj : r % ni) * ri, oj = (f ? r % nj : r / ni) * rj;
+          const long long b = (rdel[oi] + cdel[oj]) * (16 / L);
+          const long long s = (b - mod_pos(b, unit)) / unit;
+          bool seen = false;
+          for (int q = 0; q < k; ++q) seen |= seen_at[q] == s;
+          if (!seen) seen_at[k++] = s;
+        }
+        cost = cost * 64 + k;
+      }
+      if (cost < best) best = cost, fast = f;
+    }
+    return RunShape{S, fast};
+  }
+  return RunShape{-1, 0};
+}
+
+// Fills the launch's vector forms; a.vec = 1 when every output has one and
+// the epilogue has no residual or accumulation (read-modify-write outputs
+// keep the element-wise path).
+void vector_forms(GemmArgs &a, int M, int N, int batch) {
+  const csrst_gemm_epilogue &ep = a.ep;
+  a.vec = 0;
+  const MapDesc om{ep.md, ep.nd, ep.sb, ep.sm0, ep.sm1, ep.sn0, ep.sn1};
+  const MapDesc tm{ep.tmd, ep.tnd, ep.tb, ep.tm0, ep.tm1, ep.tn0, ep.tn1};
+  if (ep.res || ep.accumulate || !piece_offsets(om, a.del[0][0], a.del[0][1]) ||
+      (ep.out16t && !piece_offsets(tm, a.del[1][0], a.del[1][1])))
+    return;
+  bool ok = true;
+  const auto want = [&](int k, const void *p, int L, int mp) {
+    if (!p) return;
+    a.rs[k] = run_shape(a.del[mp][0], a.del[mp][1], L);
+    ok = ok && a.rs[k].shape >= 0 && bases_aligned(mp ? tm : om, M, N, batch, p, L);
+  };
+  want(0, ep.pre, 4, 0);
+  want(1, ep.out32, 4, 0);
+  want(2, ep.out16, 8, 0);
+  want(3, ep.out16t, 8, 1);
+  a.vec = ok;
 }
 
 // Polls an mbarrier wait makes before it gives up (csrst_gemm_set_wait_limit).
 long long g_wait_polls = kSpin;
 
+// Tensor map of a K-major BF16 operand: K x rows (x batch when it has a
+// batch stride), rows ld elements apart, box 64 x box_rows (x 1), 128-byte
+// swizzle; rows past `rows` read as zero.
+bool encode_operand(CUtensorMap *m, int *rank3, const __nv_bfloat16 *p, int K, long long rows, long long ld,
+                    long long stride, int batch, int box_rows) {
+  const EncodeTiled enc = tensor_map_encoder();
+  if (!enc) return false;
+  *rank3 = batch > 1 && stride != 0;
+  const cuuint64_t dims[3] = {(cuuint64_t)K, (cuuint64_t)rows, (cuuint64_t)batch};
+  const cuuint64_t strides[2] = {(cuuint64_t)ld * 2, (cuuint64_t)stride * 2};
+  const cuuint32_t box[3] = {(cuuint32_t)kBK, (cuuint32_t)box_rows, 1};
+  const cuuint32_t es[3] = {1, 1, 1};
+  return enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, *rank3 ? 3 : 2, const_cast<__nv_bfloat16 *>(p), dims, strides,
+             box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 template <int BN>
 int launch_gemm(const Seg &g0, const Seg &g1, int M, int N, int batch, const csrst_gemm_epilogue &ep, int *err,
                 cudaStream_t s) {
-  // operand stages, or the FP32 staging tile of the epilogue if larger, plus alignment slack
-  const int stages = 2 * (kBM * kBK * 2 + BN * kBK * 2), staging = kBM * (BN + 1) * 4;
-  const int smem = (stages > staging ? stages : staging) + 1024;
-  static bool attr = false;
-  if (!attr) {
-    if (cudaFuncSetAttribute(k_gemm<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess)
+  using G = Cfg<BN>;
+  int dev = 0, sms = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) !=
+                                                cudaSuccess)
+    return CSRST_E_CUDA;
+  static unsigned long long attr = 0;  // devices the shared-memory size was set on
+  if (dev < 64 && !(attr >> dev & 1ull)) {
+    if (cudaFuncSetAttribute(k_gemm<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM) != cudaSuccess)
       return CSRST_E_CUDA;
-    attr = true;
+    attr |= 1ull << dev;
   }
-  dim3 grid((N + BN - 1) / BN, (M + kBM - 1) / kBM, batch);
+  GemmArgs a{};
+  a.ep = ep;
+  a.err = err;
+  a.spin = g_wait_polls;
+  a.nk1 = g0.nk;
+  a.nk2 = g1.nk;
+  a.M = M;
+  a.N = N;
+  a.tilesM = (M + kBM - 1) / kBM;
+  a.tilesN = (N + BN - 1) / BN;
+  a.ntiles = (long long)batch * a.tilesM * a.tilesN;
+  if (!encode_operand(&a.map[0], &a.rank3[0], g0.A, g0.nk * kBK, M, g0.lda, g0.sA, batch, kBM) ||
+      !encode_operand(&a.map[1], &a.rank3[1], g0.B, g0.nk * kBK, N, g0.ldb, g0.sB, batch, BN))
+    return CSRST_E_ARG;
+  if (g1.nk && (!encode_operand(&a.map[2], &a.rank3[2], g1.A, g1.nk * kBK, M, g1.lda, g1.sA, batch, kBM) ||
+                !encode_operand(&a.map[3], &a.rank3[3], g1.B, g1.nk * kBK, N, g1.ldb, g1.sB, batch, BN)))
+    return CSRST_E_ARG;
   const int o_bytes = (ep.out32 || ep.res || ep.pre) ? 4 : 2;
-  const int o_mfast = rows_fast(ep.md, ep.nd, ep.sm0, ep.sm1, ep.sn0, ep.sn1, o_bytes);
-  const int t_mfast = ep.out16t ? rows_fast(ep.tmd, ep.tnd, ep.tm0, ep.tm1, ep.tn0, ep.tn1, 2) : 0;
-  k_gemm<BN><<<grid, kThreads, smem, s>>>(g0, g1, M, N, ep, err, o_mfast, t_mfast, g_wait_polls);
+  a.o_mfast = rows_fast(ep.md, ep.nd, ep.sm0, ep.sm1, ep.sn0, ep.sn1, o_bytes);
+  a.t_mfast = ep.out16t ? rows_fast(ep.tmd, ep.tnd, ep.tm0, ep.tm1, ep.tn0, ep.tn1, 2) : 0;
+  vector_forms(a, M, N, batch);
+  const long long grid = a.ntiles < sms ? a.ntiles : sms;
+  k_gemm<BN><<<(unsigned)grid, kThreads, G::SMEM, s>>>(a);
   return cudaGetLastError() == cudaSuccess ? CSRST_OK : CSRST_E_CUDA;
 }
 
 bool seg_ok(const void *A, long long lda, long long sa, const void *B, long long ldb, long long sb, int K) {
   return A && B && K > 0 && K % kBK == 0 && lda % 8 == 0 && ldb % 8 == 0 && lda >= K && ldb >= K &&
-         !((uintptr_t)A & 15) && !((uintptr_t)B & 15) && sa % 8 == 0 && sb % 8 == 0;
+         !((uintptr_t)A & 15) && !((uintptr_t)B & 15) && sa >= 0 && sb >= 0 && sa % 8 == 0 && sb % 8 == 0;
 }
 
 int gemm_dispatch(const Seg &g0, const Seg &g1, int M, int N, int batch, const csrst_gemm_epilogue *ep, int *err,

@@ -244,12 +244,13 @@ typedef struct {
 int csrst_gemm_bf16(const void *A, long long lda, long long stride_a, const void *B, long long ldb,
                     long long stride_b, int M, int N, int K, int batch, const csrst_gemm_epilogue *ep, int *err,
                     void *stream);
-/* Polls each tensor-core wait of the GEMM makes before it gives up and sets *err (for all later
+/* Polls each mbarrier wait of the GEMM makes before it gives up and sets *err = 1 (for all later
  * GEMM launches of the process; polls == 0 restores the default, 2^24).  A wait that gives up
- * skips the epilogue; the kernel still waits, with the default bound, for the tensor-core work
- * it issued and its copies in flight, frees its TMEM and returns (*err = 2 if even that wait
- * gave up).  polls < 0 exercises that path: the first wait of every GEMM with more than two
- * K tiles is then on a barrier that nothing completes, and gives up after -polls polls. */
+ * ends every role of its CTA at its next wait; the kernel still waits, with the default bound,
+ * for the copies and tensor-core work it issued, frees its TMEM and returns (*err = 2 if even
+ * that wait gave up).  polls < 0 exercises that path: the epilogue's first wait of every GEMM
+ * is then on a barrier that nothing completes, and gives up after -polls polls, before any
+ * output is written. */
 int csrst_gemm_set_wait_limit(long long polls);
 /* The same over two K segments into one accumulator: C = A1 B1^T + A2 B2^T (K1, K2 multiples of 64), each
  * segment with its own pointers, leading dimensions and batch strides (a stride may be 0: shared operand). */

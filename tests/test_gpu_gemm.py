@@ -77,18 +77,18 @@ def test_gemm_dual_segments_and_row_bias(gpu_lib):
 
 
 def test_gemm_wait_that_gives_up_reports_and_recovers(gpu_lib):
-    """The tensor-core waits are bounded.  With the stuck-wait hook (a
-    negative limit: the first wait in the K loop is on a barrier nothing
+    """The GEMM's mbarrier waits are bounded.  With the stuck-wait hook (a
+    negative limit: the epilogue's first wait is on a barrier nothing
     completes, 1000 polls) the wait gives up: the GEMM reports it through its
-    error word (1: a wait gave up, and its clean-up wait for the MMAs it had
-    issued succeeded), writes nothing, and returns; with the default limit
-    restored the same GEMM is correct again, so the context and the TMEM
-    allocator are intact."""
+    error word (1: a wait gave up, and the clean-up waits for the copies and
+    products already issued succeeded), writes nothing, and returns; with the
+    default limit restored the same GEMM is correct again, so the context and
+    the TMEM allocator are intact."""
     import torch
     from csrst_b200._lib import lib
     from csrst_b200.tensor import _err, gemm
     rng = np.random.default_rng(3)
-    M, N, K = 256, 128, 512            # 8 K tiles: waits inside the loop and after it
+    M, N, K = 256, 128, 512            # 8 K tiles per output tile, two output tiles
     a, b = bf16(rng, (M, K)), bf16(rng, (N, K))
     out = torch.full((M, N), 7.0, dtype=torch.float32, device="cuda")
     err = _err(torch.device("cuda", torch.cuda.current_device()))
@@ -107,3 +107,66 @@ def test_gemm_wait_that_gives_up_reports_and_recovers(gpu_lib):
     assert int(err.item()) == 0
     r = ref(a, b)
     assert np.abs(out.cpu().numpy() - r).max() <= 1e-4 * np.abs(r).max()
+
+
+def _gelu(h):
+    import math
+    return 0.5 * h * (1 + np.vectorize(math.erf)(h / np.sqrt(2)))
+
+
+def _scatter(h, M, N, Z, md, nd, sm0, sm1, sn0, sn1, sb):
+    """Element (z, m, n) of h at its index under an output map."""
+    m = np.arange(M)[:, None]
+    n = np.arange(N)[None, :]
+    idx = (m // md) * sm0 + (m % md) * sm1 + (n // nd) * sn0 + (n % nd) * sn1
+    return [(z * sb + idx, h[z]) for z in range(Z)]
+
+
+@pytest.mark.parametrize("case", ["rows_and_member_columns", "spectra_pairs", "dual_both_orders", "ragged"])
+def test_gemm_vector_epilogue_maps(gpu_lib, case):
+    """The epilogue's 16-byte runs (rows, columns, the spectra's interleaved
+    pairs) and the element-wise path of the pieces at ragged edges, against
+    an FP64 product of the same BF16 values: pre-activation (FP32), GELU,
+    FP32 and BF16 outputs under both maps."""
+    import torch
+    from csrst_b200.tensor import check_errors, gemm, gemm_dual
+    rng = np.random.default_rng(hash(case) % 1000)
+    dev = "cuda"
+    if case == "rows_and_member_columns":   # the lift's maps: rows, and per member (128 rows) columns
+        Z, M, N, K = 1, 384, 128, 64
+        om = dict(md=1, nd=1, sm0=N, sm1=0, sn0=1, sn1=0)
+        tm = dict(md=128, nd=1, sm0=N * 128, sm1=1, sn0=128, sn1=0)
+    elif case == "spectra_pairs":             # the forward DFT's map: U[k][b][2c + ri]
+        Z, M, N, K = 1, 256, 64, 256
+        om = dict(md=128, nd=2, sm0=256, sm1=2, sn0=512, sn1=1)
+        tm = None
+    elif case == "dual_both_orders":          # the inverse DFT's maps: V[b][n][o] and Tv[b][o][n]
+        Z, M, N, K = 3, 128, 256, 128
+        om = dict(md=1, nd=1, sm0=1, sm1=0, sn0=M, sn1=0)
+        tm = dict(md=1, nd=1, sm0=N, sm1=0, sn0=1, sn1=0)
+    else:                                     # edge pieces (rows past 200, columns past 80) element-wise
+        Z, M, N, K = 2, 200, 80, 128
+        om = dict(md=1, nd=1, sm0=N, sm1=0, sn0=1, sn1=0)
+        tm = dict(md=1, nd=1, sm0=1, sm1=0, sn0=M, sn1=0)
+    a, b = bf16(rng, (Z, M, K)), bf16(rng, (Z, N, K))
+    bias = torch.from_numpy(rng.standard_normal(N).astype(np.float32))
+    size = Z * M * N
+    pre = torch.zeros(size, device=dev)
+    o32 = torch.zeros(size, device=dev)
+    o16 = torch.zeros(size, dtype=torch.bfloat16, device=dev)
+    o16t = torch.zeros(size, dtype=torch.bfloat16, device=dev) if tm else None
+    gemm(a.cuda(), b.cuda(), M, N, K, batch=Z, stride_a=M * K, stride_b=N * K, alpha=0.75, bias=bias.cuda(),
+         pre=pre, out32=o32, out16=o16, act=1, omap=om, sb=M * N, out16t=o16t, tmap=tm, tb=M * N)
+    torch.cuda.synchronize()
+    check_errors()
+    h = np.stack([0.75 * ref(a[z], b[z]) + bias.double().numpy() for z in range(Z)])
+    g = _gelu(h)
+    P, O32, O16 = pre.cpu().numpy(), o32.cpu().numpy(), o16.float().cpu().numpy()
+    for (idx, hz), gz in zip(_scatter(h, M, N, Z, sb=M * N, **om), g):
+        assert np.abs(P[idx] - hz).max() <= 1e-4 * np.abs(h).max()
+        assert np.abs(O32[idx] - gz).max() <= 1e-4 * np.abs(g).max()
+        assert np.abs(O16[idx] - gz).max() <= 1e-2 * np.abs(g).max()
+    if tm:
+        T = o16t.float().cpu().numpy()
+        for idx, gz in _scatter(g, M, N, Z, sb=M * N, **tm):
+            assert np.abs(T[idx] - gz).max() <= 1e-2 * np.abs(g).max()
