@@ -20,6 +20,8 @@ diagnostic sampled on window columns, interpolated linearly onto the bins).
 """
 import json
 import math
+import os
+from concurrent.futures import ThreadPoolExecutor
 from dataclasses import dataclass, asdict
 
 import numpy as np
@@ -193,49 +195,77 @@ def shape_batch(P, z, kind):
     return ft + P["horn_a"] * np.exp(-(z + P["horn_pos"]) ** 2 / hw) + P["horn_b"] * np.exp(-(z - P["horn_pos"]) ** 2 / hw)
 
 
+_POOL = None
+
+
+def _pool():
+    """Host threads for the per-chunk feature work (numpy's and scipy's
+    element-wise kernels release the GIL); each chunk is computed exactly as
+    it would be alone, so the results do not depend on the thread count."""
+    global _POOL
+    if _POOL is None:
+        _POOL = ThreadPoolExecutor(max_workers=max(1, min(8, os.cpu_count() or 1)))
+    return _POOL
+
+
 def moments_batch(cases, fine=512):
     """(mass, centroid, rms) of the families' shapes, vectorised per family
     (a Gaussian analytically; the flat-top families, whose support lies
-    within +-3 of their scale, by the trapezoid rule on a fine grid)."""
+    within +-3 of their scale, by the trapezoid rule on a fine grid), chunks
+    of 4096 cases on the host threads."""
     z = np.linspace(-3.0, 3.0, fine)
     dz = z[1] - z[0]
     wq = np.full(fine, dz)
     wq[0] = wq[-1] = 0.5 * dz
     kinds = np.array([c.kind for c in cases])
     mass, mu, rms = np.full(len(cases), math.sqrt(2 * math.pi)), np.zeros(len(cases)), np.ones(len(cases))
+
+    def one(kind, sel, P):
+        d = shape_batch(P, z[None, :], kind)
+        mass[sel] = d @ wq
+        mu[sel] = (d * z) @ wq / mass[sel]
+        rms[sel] = np.sqrt((d * (z[None, :] - mu[sel, None]) ** 2) @ wq / mass[sel])
+
+    jobs = []
     for kind in (1, 2):
         idx = np.nonzero(kinds == kind)[0]
         for a in range(0, len(idx), 4096):
             sel = idx[a:a + 4096]
-            d = shape_batch(_params([cases[k] for k in sel]), z[None, :], kind)
-            mass[sel] = d @ wq
-            mu[sel] = (d * z) @ wq / mass[sel]
-            rms[sel] = np.sqrt((d * (z[None, :] - mu[sel, None]) ** 2) @ wq / mass[sel])
+            jobs.append(_pool().submit(one, kind, sel, _params([cases[k] for k in sel])))
+    for j in jobs:
+        j.result()
     return mass, mu, rms
 
 
-def features(cases, chunk=4096):
+def features(cases, chunk=1024):
     """[N][256][7] float32: line density per sigma_s, bin position / SPAN,
     log-scaled gamma, R, sigma_s, pipe width / sigma_s (each about [-1, 1]
     over the drawn ranges), and the slope of the line density (per sigma_s^2,
     / 4).  Vectorised per family over chunks of cases: a Gaussian is centred
     with unit rms; the flat-top families (support within +-3 of their scale)
     take centroid and rms from a fine grid; the density at the bins comes
-    from the shape itself."""
+    from the shape itself.  Chunks of cases run on the host threads (the
+    values do not depend on the chunking: every step is per case)."""
     N = len(cases)
     out = np.zeros((N, NBINS, NFEATURES), dtype=np.float32)
     sb = bin_centres()
     mass_all, mu_all, rms_all = moments_batch(cases)
     kinds = np.array([c.kind for c in cases])
+
+    def one(kind, sel, P):
+        mass, mu, rms = mass_all[sel], mu_all[sel], rms_all[sel]
+        lam = shape_batch(P, mu[:, None] + sb[None, :] * rms[:, None], kind) / mass[:, None] * rms[:, None]
+        out[sel, :, 0] = lam
+        out[sel, :, 6] = np.gradient(lam, 2 * SPAN / NBINS, axis=1) / 4.0
+
+    jobs = []
     for kind in (0, 1, 2):
         idx = np.nonzero(kinds == kind)[0]
         for a in range(0, len(idx), chunk):
             sel = idx[a:a + chunk]
-            P = _params([cases[k] for k in sel])
-            mass, mu, rms = mass_all[sel], mu_all[sel], rms_all[sel]
-            lam = shape_batch(P, mu[:, None] + sb[None, :] * rms[:, None], kind) / mass[:, None] * rms[:, None]
-            out[sel, :, 0] = lam
-            out[sel, :, 6] = np.gradient(lam, 2 * SPAN / NBINS, axis=1) / 4.0
+            jobs.append(_pool().submit(one, kind, sel, _params([cases[k] for k in sel])))
+    for j in jobs:
+        j.result()
     out[:, :, 1] = sb[None, :] / SPAN
     for j, (name, ref) in enumerate((("gamma", 632.5), ("R", 1.581), ("sigma_s", 63.25e-6))):
         out[:, :, 2 + j] = ((np.log([getattr(c, name) for c in cases]) - math.log(ref)) / 1.152)[:, None]
