@@ -103,7 +103,7 @@ def peaks(bf16=False):
 # The launches of one time step per kernel group (order 1 = TSC), as the
 # profile launch lists name them.
 STEP_LAUNCHES = {
-    ("push", "fp32", 1): {"k_push32<1, 0>": 1, "k_push32<1, 1>": 1, "k_prep32": 2, "k_post32": 2, "k_bounds32": 2},
+    ("push", "fp32", 1): {"k_push32<1, 0>": 1, "k_push32<1, 1>": 1, "k_prep32": 1, "k_after32": 2},
     ("yee", "fp32", 1): {"k_yee_tiles<float>": 1, "k_yee_fixup<float>": 1, "k_window_ey<float>": 1},
     ("push", "fp64", 1): {"k_push<1>": 2, "k_push_prep": 2, "k_push_post": 2, "k_global_bounds": 2},
     ("yee", "fp64", 1): {"k_yee_tiles<double>": 1, "k_yee_fixup<double>": 1, "k_window_ey<double>": 1},
@@ -634,9 +634,11 @@ def run_b200(args, world, rank, local):
     if other in runs:
         out[other] = summary(other)
         out[f"{head}_over_{other}"] = round(hs["value"] / out[other]["value"], 3)
-    # launches per step: 2 pushes x (prep, push, post, bounds) + the fused
-    # field sweep (tiles, window fix-up, window Ey) + move
-    out["gpu_launches"] = args.steps * (2 * 4 + 3 + 1)
+    # launches per FP32 step: the first push (prep, push, closing kernel that
+    # also sets up the second), the second push (push, closing kernel), the
+    # fused field sweep (tiles, window fix-up), the window's Ey, and the move
+    # (two copy stages, finish)
+    out["gpu_launches"] = args.steps * (3 + 2 + 2 + 1 + 3)
     if rank == 0 and not args.no_compare:
         out["accuracy_fp32_vs_fp64"] = accuracy(cfg, spec, bunch)
     if not args.no_ensemble:

@@ -131,6 +131,9 @@ struct csrst_handle {
   double *ox = nullptr, *oy = nullptr;
   bool pending = false;
   bool fresh = false;  // loaded, no push yet
+  // FP32 mode: the last push's closing kernel set up the next push's gather
+  // patch (prepped); the next push is to do so (prep_after)
+  bool prepped = false, prep_after = false;
   BBoxState bb = kBBInvalid;
   int push_grid = 0;
   // diagnostics scratch
@@ -474,10 +477,15 @@ Push32Args push_args32(csrst_handle *h, int jcomp) {
 int push_async(csrst_handle *h, int jcomp) {
   const bool bb_ok = h->bb == kBBValid || (h->bb == kBBValidIfPending && h->pending);
   if (h->fp32) {
-    if (!bb_ok) launch_bbox32(h->b32, h->R32, h->pending ? 1 : 0, h->ws, h->s);
-    launch_prep32(h->ws, h->order, h->s);
+    if (!bb_ok) {
+      launch_bbox32(h->b32, h->R32, h->pending ? 1 : 0, h->ws, h->s);
+      h->prepped = false;
+    }
+    if (!h->prepped) launch_prep32(h->ws, h->order, h->s);
     launch_push32(push_args32(h, jcomp), h->order, h->s);
-    launch_bounds32(h->ws, h->s);
+    launch_after32(h->ws, h->prep_after ? 1 : 0, h->s);
+    h->prepped = h->prep_after;
+    h->prep_after = false;
     h->pending = false;
     h->fresh = false;
     h->bb = kBBValidIfPending;
@@ -511,6 +519,7 @@ void drift_back(csrst_handle *h) {
   if (h->pending) {  // materialise the older one first
     drift_now(h, -0.5 * h->dt);
     h->bb = kBBInvalid;
+    h->prepped = false;
   }
   h->pending = true;
   if (h->bb == kBBValidIfPending) h->bb = kBBValid;
@@ -519,6 +528,7 @@ void drift_back(csrst_handle *h) {
 void materialise(csrst_handle *h) {
   if (!h->pending) return;
   drift_now(h, -0.5 * h->dt);
+  h->prepped = false;
   h->pending = false;
   if (h->fp32) h->bb = kBBInvalid;
   // the stored box of the next gather positions stays exact: R_true + h v(P)
@@ -657,11 +667,18 @@ void mark(csrst_handle *h, int k) {
 // half and the move.
 int step_async(csrst_handle *h) {
   mark(h, 0);
+  // in the fused step nothing moves the particles or the window between the
+  // two pushes: the first push's closing kernel also sets up the second
+  h->prepped = false;
+  h->prep_after = h->fp32 && fused_ok(h);
   push_async(h, 0);
   mark(h, 1);
   if (fused_ok(h)) {
     const int rc = fused_fields_async(h);
-    if (rc) return rc;
+    if (rc) {
+      h->prepped = false;
+      return rc;
+    }
     mark(h, 2);
     drift_back(h);
     mark(h, 3);

@@ -278,7 +278,10 @@ long long push32_batch_smem_limit();
 void launch_push32_batch(const PushGroup *groups, int ngroups, int m, int grid, const PrepArgs *prep,
                          cudaStream_t s, int parts = 3);
 void launch_prep32(WinState *ws, int order, cudaStream_t s);
-void launch_bounds32(WinState *ws, cudaStream_t s);
+// After a push: swap the box sets, the deposit bounds, and the next push's
+// gather-patch set-up when prep_next (nothing moves the particles or the
+// window before that push).
+void launch_after32(WinState *ws, int prep_next, cudaStream_t s);
 void launch_bbox32(const Bunch32 &b, const Ref32 &R, int pending, WinState *ws, cudaStream_t s);
 // R += dt c v / h: kd = the drift's dt c / h per axis (Ref32.kh replaced)
 void launch_drift32(const Bunch32 &b, const Ref32 &R, float kd0, float kd1, cudaStream_t s);

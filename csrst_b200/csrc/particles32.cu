@@ -336,25 +336,28 @@ __device__ __forceinline__ void bounds32_body(WinState *ws) {
   ws->gb[2] = (int)floor(mn1) - ws->P1; ws->gb[3] = (int)floor(mx1) - ws->P1;
 }
 
-__global__ void k_bounds32(WinState *ws) {
-  if (threadIdx.x == 0) bounds32_body(ws);
-}
 
 __global__ void k_prep32_batch(const PrepArgs *p, int m) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k < m) prep32_body(p[k].ws, 2);
 }
-__global__ void k_post32_batch(const PrepArgs *p, int m) {
+__global__ void k_after32_batch(const PrepArgs *p, int m) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k < m) p[k].ws->cur = 1 - p[k].ws->cur;
-}
-__global__ void k_bounds32_batch(const PrepArgs *p, int m) {
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k < m) bounds32_body(p[k].ws);
+  if (k < m) {
+    p[k].ws->cur = 1 - p[k].ws->cur;
+    bounds32_body(p[k].ws);
+  }
 }
 
-__global__ void k_post32(WinState *ws) {
-  if (threadIdx.x == 0) ws->cur = 1 - ws->cur;
+// After a push: the box sets swap (the push filled the other one), the
+// deposit bounds follow from the push's boxes, and, when the caller knows
+// the next push reads the same particles and window (prep_next), its gather
+// patch is set up here too, which saves that push its own set-up launch.
+__global__ void k_after32(WinState *ws, int prep_next) {
+  if (threadIdx.x != 0) return;
+  ws->cur = 1 - ws->cur;
+  bounds32_body(ws);
+  if (prep_next) prep32_body(ws, 2);
 }
 
 __global__ void k_bbox32_clear(WinState *ws) {
@@ -517,7 +520,6 @@ int launch_push32(const Push32Args &a, int order, cudaStream_t s) {
   if (order == 0) push32_order<0>(a, s);
   else if (order == 1) push32_order<1>(a, s);
   else push32_order<2>(a, s);
-  k_post32<<<1, 32, 0, s>>>(a.ws);
   return 0;
 }
 
@@ -540,10 +542,7 @@ void launch_push32_batch(const PushGroup *groups, int ngroups, int m, int grid, 
     else if (G.order == 1) push32_batch_order<1>(args, G.ppre, G.m, ctas, per, jcomp, s);
     else push32_batch_order<2>(args, G.ppre, G.m, ctas, per, jcomp, s);
   }
-  if (parts & 2) {
-    k_post32_batch<<<tb, 128, 0, s>>>(prep, m);
-    k_bounds32_batch<<<tb, 128, 0, s>>>(prep, m);
-  }
+  if (parts & 2) k_after32_batch<<<tb, 128, 0, s>>>(prep, m);
 }
 
 void launch_flux32(int order, int comp, const int *cell0, const float *a0, const float *a1, const int *cell1,
@@ -560,7 +559,7 @@ void launch_prep32(WinState *ws, int order, cudaStream_t s) {
   k_prep32<<<1, 32, 0, s>>>(ws, 2);
 }
 
-void launch_bounds32(WinState *ws, cudaStream_t s) { k_bounds32<<<1, 32, 0, s>>>(ws); }
+void launch_after32(WinState *ws, int prep_next, cudaStream_t s) { k_after32<<<1, 32, 0, s>>>(ws, prep_next); }
 
 void launch_bbox32(const Bunch32 &b, const Ref32 &R, int pending, WinState *ws, cudaStream_t s) {
   k_bbox32_clear<<<1, 32, 0, s>>>(ws);
