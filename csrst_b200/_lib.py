@@ -72,6 +72,8 @@ def lib():
         "csrst_ensemble_tune": ([P, C.c_int, D, C.c_int, I], C.c_int),
         "csrst_gemm_bf16": ([P, C.c_longlong, C.c_longlong, P, C.c_longlong, C.c_longlong, C.c_int, C.c_int,
                              C.c_int, C.c_int, P, P, P], C.c_int),
+        "csrst_gemm_bf16_ex": ([P, C.c_longlong, C.c_longlong, C.c_int, P, C.c_longlong, C.c_longlong, C.c_int,
+                                C.c_int, C.c_int, C.c_int, P, P, P], C.c_int),
         "csrst_gemm_set_wait_limit": ([C.c_longlong], C.c_int),
         "csrst_gemm_bf16_dual": ([P, C.c_longlong, C.c_longlong, P, C.c_longlong, C.c_longlong, C.c_int, P,
                                   C.c_longlong, C.c_longlong, P, C.c_longlong, C.c_longlong, C.c_int, C.c_int,

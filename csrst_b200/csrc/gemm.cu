@@ -75,11 +75,21 @@ __device__ __forceinline__ uint64_t sw128_desc(uint32_t addr) {
          ((uint64_t)1 << 46) | ((uint64_t)2 << 61);
 }
 
-// Instruction descriptor of kind::f16: FP32 accumulator, BF16 A and B, both
-// K-major, M = 128, N = BN.
+// The same for an MN-major A tile (rows contiguous along M) with 128-byte
+// swizzle, as two TMA boxes of 64 M x 64 K write it: each 64-row chunk holds
+// the tile's 64 K rows of 128 B (8-row atoms 1024 B apart: SBO), the second
+// chunk 8192 B after the first (LBO).  Stepping K by 16 rows adds 2048 B.
+__device__ __forceinline__ uint64_t sw128_mn_desc(uint32_t addr) {
+  return (uint64_t)((addr >> 4) & 0x3FFF) | ((uint64_t)(8192 >> 4) << 16) | ((uint64_t)(1024 >> 4) << 32) |
+         ((uint64_t)1 << 46) | ((uint64_t)2 << 61);
+}
+
+// Instruction descriptor of kind::f16: FP32 accumulator, BF16 A and B, B
+// K-major, A K-major or MN-major (bit 15), M = 128, N = BN.
 template <int BN>
-__device__ __forceinline__ uint32_t instr_desc() {
-  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(kBM >> 4) << 24);
+__device__ __forceinline__ uint32_t instr_desc(bool a_mn = false) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | (a_mn ? 1u << 15 : 0u) | ((uint32_t)(BN >> 3) << 17) |
+         ((uint32_t)(kBM >> 4) << 24);
 }
 
 __device__ __forceinline__ void mma_bf16(uint32_t tmem, uint64_t da, uint64_t db, uint32_t idesc, uint32_t acc) {
@@ -171,6 +181,7 @@ struct Seg {
   const __nv_bfloat16 *B;
   long long ldb, sB;
   int nk;
+  int amn;  // A is MN-major: element (m, k) of a batch at A[k * lda + m]
 };
 
 // Vector stores.  Where an output map, restricted to a 32 x 32 piece of a
@@ -204,6 +215,7 @@ struct alignas(64) GemmArgs {
   long long ntiles;
   int nk1, nk2, M, N, tilesM, tilesN;
   int rank3[4];
+  int amn[2];                 // per segment: A MN-major (two 64-row TMA boxes per stage)
   int o_mfast, t_mfast;
   int vec;
   RunShape rs[4];             // pre, out32, out16 (primary map), out16t (second map)
@@ -423,8 +435,16 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm(const __grid_constant__ Ge
           mbar_expect_tx(&full[s], G::STAGE);
           const int seg = kt < a.nk1 ? 0 : 1, k0 = (kt < a.nk1 ? kt : kt - a.nk1) * kBK;
           const int ia = 2 * seg, ib = ia + 1;
-          if (a.rank3[ia]) tma_load_3d(sa, &a.map[ia], k0, m0, z, &full[s]);
-          else tma_load_2d(sa, &a.map[ia], k0, m0, &full[s]);
+          if (a.amn[seg]) {  // (M, K) boxes of 64 x 64: the tile's two row chunks
+            for (int h = 0; h < 2; ++h) {
+              if (a.rank3[ia]) tma_load_3d(sa + h * 8192, &a.map[ia], m0 + 64 * h, k0, z, &full[s]);
+              else tma_load_2d(sa + h * 8192, &a.map[ia], m0 + 64 * h, k0, &full[s]);
+            }
+          } else if (a.rank3[ia]) {
+            tma_load_3d(sa, &a.map[ia], k0, m0, z, &full[s]);
+          } else {
+            tma_load_2d(sa, &a.map[ia], k0, m0, &full[s]);
+          }
           if (a.rank3[ib]) tma_load_3d(sb, &a.map[ib], k0, n0, z, &full[s]);
           else tma_load_2d(sb, &a.map[ib], k0, n0, &full[s]);
           ++it;
@@ -454,10 +474,12 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm(const __grid_constant__ Ge
           }
           asm volatile("tcgen05.fence::after_thread_sync;");
           const uint32_t a0 = smem_u32(base + s * G::STAGE), b0 = a0 + G::A_BYTES;
+          const bool amn = a.amn[kt < a.nk1 ? 0 : 1];
+          const uint32_t idesc = instr_desc<BN>(amn);
 #pragma unroll
           for (int kk = 0; kk < kBK / 16; ++kk)
-            mma_bf16(d, sw128_desc(a0 + kk * 32), sw128_desc(b0 + kk * 32), instr_desc<BN>(),
-                     (kt > 0 || kk > 0) ? 1u : 0u);
+            mma_bf16(d, amn ? sw128_mn_desc(a0 + kk * 2048) : sw128_desc(a0 + kk * 32), sw128_desc(b0 + kk * 32),
+                     idesc, (kt > 0 || kk > 0) ? 1u : 0u);
           mma_commit(&empty[s]);
           issued = true;
           ++it;
@@ -656,14 +678,16 @@ long long g_wait_polls = kSpin;
 // Tensor map of a K-major BF16 operand: K x rows (x batch when it has a
 // batch stride), rows ld elements apart, box 64 x box_rows (x 1), 128-byte
 // swizzle; rows past `rows` read as zero.
+// mn: the operand is MN-major (K rows of `rows` contiguous elements, ld
+// apart): rows x K (x batch), box 64 x 64.
 bool encode_operand(CUtensorMap *m, int *rank3, const __nv_bfloat16 *p, int K, long long rows, long long ld,
-                    long long stride, int batch, int box_rows) {
+                    long long stride, int batch, int box_rows, bool mn = false) {
   const EncodeTiled enc = tensor_map_encoder();
   if (!enc) return false;
   *rank3 = batch > 1 && stride != 0;
-  const cuuint64_t dims[3] = {(cuuint64_t)K, (cuuint64_t)rows, (cuuint64_t)batch};
+  const cuuint64_t dims[3] = {(cuuint64_t)(mn ? rows : K), (cuuint64_t)(mn ? K : rows), (cuuint64_t)batch};
   const cuuint64_t strides[2] = {(cuuint64_t)ld * 2, (cuuint64_t)stride * 2};
-  const cuuint32_t box[3] = {(cuuint32_t)kBK, (cuuint32_t)box_rows, 1};
+  const cuuint32_t box[3] = {(cuuint32_t)kBK, (cuuint32_t)(mn ? 64 : box_rows), 1};
   const cuuint32_t es[3] = {1, 1, 1};
   return enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, *rank3 ? 3 : 2, const_cast<__nv_bfloat16 *>(p), dims, strides,
              box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
@@ -695,10 +719,12 @@ int launch_gemm(const Seg &g0, const Seg &g1, int M, int N, int batch, const csr
   a.tilesM = (M + kBM - 1) / kBM;
   a.tilesN = (N + BN - 1) / BN;
   a.ntiles = (long long)batch * a.tilesM * a.tilesN;
-  if (!encode_operand(&a.map[0], &a.rank3[0], g0.A, g0.nk * kBK, M, g0.lda, g0.sA, batch, kBM) ||
+  a.amn[0] = g0.amn;
+  a.amn[1] = g1.amn;
+  if (!encode_operand(&a.map[0], &a.rank3[0], g0.A, g0.nk * kBK, M, g0.lda, g0.sA, batch, kBM, g0.amn) ||
       !encode_operand(&a.map[1], &a.rank3[1], g0.B, g0.nk * kBK, N, g0.ldb, g0.sB, batch, BN))
     return CSRST_E_ARG;
-  if (g1.nk && (!encode_operand(&a.map[2], &a.rank3[2], g1.A, g1.nk * kBK, M, g1.lda, g1.sA, batch, kBM) ||
+  if (g1.nk && (!encode_operand(&a.map[2], &a.rank3[2], g1.A, g1.nk * kBK, M, g1.lda, g1.sA, batch, kBM, g1.amn) ||
                 !encode_operand(&a.map[3], &a.rank3[3], g1.B, g1.nk * kBK, N, g1.ldb, g1.sB, batch, BN)))
     return CSRST_E_ARG;
   const int o_bytes = (ep.out32 || ep.res || ep.pre) ? 4 : 2;
@@ -740,8 +766,24 @@ extern "C" int csrst_gemm_bf16(const void *A, long long lda, long long stride_a,
   using namespace csrst;
   if (!seg_ok(A, lda, stride_a, B, ldb, stride_b, K)) return CSRST_E_ARG;
   const Seg g0{static_cast<const __nv_bfloat16 *>(A), lda, stride_a, static_cast<const __nv_bfloat16 *>(B), ldb,
-               stride_b, K / kBK};
-  const Seg g1{nullptr, 0, 0, nullptr, 0, 0, 0};
+               stride_b, K / kBK, 0};
+  const Seg g1{nullptr, 0, 0, nullptr, 0, 0, 0, 0};
+  return gemm_dispatch(g0, g1, M, N, batch, ep, err, stream);
+}
+
+extern "C" int csrst_gemm_bf16_ex(const void *A, long long lda, long long stride_a, int a_mn_major, const void *B,
+                                  long long ldb, long long stride_b, int M, int N, int K, int batch,
+                                  const csrst_gemm_epilogue *ep, int *err, void *stream) {
+  using namespace csrst;
+  if (!a_mn_major) return csrst_gemm_bf16(A, lda, stride_a, B, ldb, stride_b, M, N, K, batch, ep, err, stream);
+  // MN-major A: K rows of M elements, lda apart (the rules of seg_ok with M for K on A)
+  if (!(A && B && K > 0 && K % kBK == 0 && lda % 8 == 0 && ldb % 8 == 0 && lda >= M && ldb >= K &&
+        !((uintptr_t)A & 15) && !((uintptr_t)B & 15) && stride_a >= 0 && stride_b >= 0 && stride_a % 8 == 0 &&
+        stride_b % 8 == 0))
+    return CSRST_E_ARG;
+  const Seg g0{static_cast<const __nv_bfloat16 *>(A), lda, stride_a, static_cast<const __nv_bfloat16 *>(B), ldb,
+               stride_b, K / kBK, 1};
+  const Seg g1{nullptr, 0, 0, nullptr, 0, 0, 0, 0};
   return gemm_dispatch(g0, g1, M, N, batch, ep, err, stream);
 }
 
@@ -753,8 +795,8 @@ extern "C" int csrst_gemm_bf16_dual(const void *A1, long long lda1, long long st
   if (!seg_ok(A1, lda1, stride_a1, B1, ldb1, stride_b1, K1) || !seg_ok(A2, lda2, stride_a2, B2, ldb2, stride_b2, K2))
     return CSRST_E_ARG;
   const Seg g0{static_cast<const __nv_bfloat16 *>(A1), lda1, stride_a1, static_cast<const __nv_bfloat16 *>(B1), ldb1,
-               stride_b1, K1 / kBK};
+               stride_b1, K1 / kBK, 0};
   const Seg g1{static_cast<const __nv_bfloat16 *>(A2), lda2, stride_a2, static_cast<const __nv_bfloat16 *>(B2), ldb2,
-               stride_b2, K2 / kBK};
+               stride_b2, K2 / kBK, 0};
   return gemm_dispatch(g0, g1, M, N, batch, ep, err, stream);
 }

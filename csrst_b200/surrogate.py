@@ -14,12 +14,13 @@ Network (width w = 128, 32 Fourier modes, 4 layers, 32 outputs per bin):
   V_{l+1} = gelu(H_l) (l < 3), V_4 = H_3
   out     = gelu(V_4 Q1^T + q1) Q2^T + q2
 The spectral product is three GEMMs per layer: the forward DFT as a product
-with a [64 x 256] matrix of cosines and sines (rows in (member, channel)
-order, output written mode-major), the mode mixing as a batch of 32 real
-[2w x 2w] block matrices (one per mode: [[Wr, -Wi], [Wi, Wr]] interleaved),
-and, per member, the truncated inverse DFT with the layer's pointwise product
-as a second K segment of the same accumulator, and bias, activation, the
-BF16 copies and a transposed copy fused into its epilogue.
+with a [64 x 256] matrix of cosines and sines (per member, its channels as
+rows, reading V's rows of bins as an MN-major operand; output written
+mode-major), the mode mixing as a batch of 32 real [2w x 2w] block matrices
+(one per mode: [[Wr, -Wi], [Wi, Wr]] interleaved), and, per member, the
+truncated inverse DFT with the layer's pointwise product as a second K
+segment of the same accumulator, and bias, activation and the BF16 copy
+fused into its epilogue.
 
 Activations are BF16 between products (FP32 accumulation inside them); the
 loss, gradients of biases and the Adam state are FP32.  Reductions are in a
@@ -81,8 +82,8 @@ class _Buffers:
     layer's input for the backward pass; inference ping-pongs two).
 
     Layouts (b member, n bin, c channel, k mode, ri real/imaginary):
-      V16  [b][n][c]      rows of the pointwise products
-      Tv16 [b][c][n]      rows (b, c) of 256 bins: the forward DFT's operand
+      V16  [b][n][c]      rows of the pointwise products; per member, the forward
+                          DFT's operand read MN-major (its 256 bins are the K rows)
       Vg16 [c][b][n]      every bin of a channel in one row: weight gradients
       U16  [k][b][2c+ri]  spectra, the mode mixing's operand
       Z16  [k][b][2o+p]   mixed spectra; Zp16 [b][o][2k+p] the inverse DFT's operand
@@ -98,7 +99,6 @@ class _Buffers:
         bf, f32 = dict(dtype=torch.bfloat16, device=dev), dict(dtype=torch.float32, device=dev)
         nkeep = L + 1 if train else 2
         self.V16 = [torch.empty(R, w, **bf) for _ in range(nkeep)]
-        self.Tv16 = [torch.empty(B * w, NBINS, **bf) for _ in range(nkeep)]
         self.U16 = torch.empty(m, B, 2 * w, **bf)
         self.Z16 = torch.empty(m, B, 2 * w, **bf)
         self.Zp16 = torch.empty(B * w, 2 * m, **bf)
@@ -227,15 +227,15 @@ class FNO:
         tr = bf.train
         w16 = lambda n: self.view(n, self.w16)
         # lift: V0 in rows and in per-member channel rows
-        gemm(X16, w16("P"), R, w, NFEAT, bias=self.view("p"), out16=bf.V16[0], out16t=bf.Tv16[0],
-             tmap=dict(md=NBINS, nd=1, sm0=w * NBINS, sm1=1, sn0=NBINS, sn1=0))
+        gemm(X16, w16("P"), R, w, NFEAT, bias=self.view("p"), out16=bf.V16[0])
         for l in range(L):
             i, o = (l, l + 1) if tr else (l & 1, (l + 1) & 1)
             if tr:
                 self._tr16(bf.V16[i], bf.Vg16[i], 1, R, w)
-            # forward DFT over the bins: rows (member b, channel c) -> U[k][b][2c + ri]
-            gemm(bf.Tv16[i], self.F16, B * w, 2 * m, NBINS, out16=bf.U16,
-                 omap=dict(md=w, nd=2, sm0=2 * w, sm1=2, sn0=2 * w * B, sn1=1))
+            # forward DFT over the bins, per member b: rows c of V[b] read MN-major (the
+            # bins are V's rows) -> U[k][b][2c + ri]
+            gemm(bf.V16[i], self.F16, w, 2 * m, NBINS, a_mn=True, lda=w, batch=B, stride_a=NBINS * w,
+                 out16=bf.U16, omap=dict(md=1, nd=2, sm0=2, sm1=0, sn0=2 * w * B, sn1=1), sb=2 * w)
             if tr:
                 self._tr16(bf.U16, bf.Ut16[l], m, B, 2 * w)
             # mode mixing: per mode k, Z[b][2o + p] = sum U[b][2c + q] Mk[2o + p][2c + q]
@@ -247,13 +247,10 @@ class FNO:
             #                                          + sum_c W[o][c] V[b][n][c]    (pointwise product)
             # + bias[o]; pre-activation, activation, V in rows and in per-member channel rows
             act = l < L - 1
-            last = l == L - 1
             gemm_dual(bf.Zp16, self.G16, 2 * m, w16("W%d" % l), bf.V16[i], w, w, NBINS, stride_a1=2 * m * w,
                       stride_b2=NBINS * w, batch=B, bias_m=self.view("b%d" % l),
                       pre=bf.Hfull[l] if (tr and act) else None, act=1 if act else 0, out16=bf.V16[o],
-                      omap=dict(md=1, nd=1, sm0=1, sm1=0, sn0=w, sn1=0), sb=NBINS * w,
-                      out16t=None if last else bf.Tv16[o],
-                      tmap=dict(md=1, nd=1, sm0=NBINS, sm1=0, sn0=1, sn1=0), tb=w * NBINS)
+                      omap=dict(md=1, nd=1, sm0=1, sm1=0, sn0=w, sn1=0), sb=NBINS * w)
         Vl = bf.V16[L if tr else L & 1]
         if tr:
             self._tr16(Vl, bf.Vg16[L], 1, R, w)

@@ -58,15 +58,17 @@ def _epilogue(N, alpha, bias, bias_m, res, pre, out32, out16, out16t, act, accum
 
 def gemm(A, B, M, N, K, *, lda=None, ldb=None, batch=1, stride_a=0, stride_b=0, alpha=1.0, bias=None, bias_m=None,
          res=None, pre=None, out32=None, out16=None, out16t=None, act=0, accumulate=False, omap=None, tmap=None, sb=0,
-         tb=0):
+         tb=0, a_mn=False):
     """C[M, N] = alpha A[M, K] B[N, K]^T (+ bias[n] + bias_m[m] + res) on the
     tensor cores, batched over `batch`; outputs through the index maps omap /
-    tmap (dicts of md, nd, sm0, sm1, sn0, sn1, default row-major N)."""
+    tmap (dicts of md, nd, sm0, sm1, sn0, sn1, default row-major N).  a_mn:
+    A is MN-major (K rows of M elements, lda apart, default M)."""
     assert A.dtype == torch.bfloat16 and B.dtype == torch.bfloat16
     ep = _epilogue(N, alpha, bias, bias_m, res, pre, out32, out16, out16t, act, accumulate, omap, tmap, sb, tb)
     err = _err(A.device)
-    rc = lib().csrst_gemm_bf16(_ptr(A), lda or K, stride_a, _ptr(B), ldb or K, stride_b, M, N, K, batch,
-                               C.byref(ep), _ptr(err), C.c_void_p(torch.cuda.current_stream().cuda_stream))
+    rc = lib().csrst_gemm_bf16_ex(_ptr(A), lda or (M if a_mn else K), stride_a, 1 if a_mn else 0, _ptr(B),
+                                  ldb or K, stride_b, M, N, K, batch, C.byref(ep), _ptr(err),
+                                  C.c_void_p(torch.cuda.current_stream().cuda_stream))
     if rc:
         raise CsrstError(rc, "csrst_gemm_bf16: invalid arguments or launch failure")
 

@@ -245,20 +245,18 @@ def time_inference(model, X6, n=65536, chunk=8192, reps=3):
 def bytes_per_profile(net):
     """Bytes the forward pass must move per profile in this layer sequence
     (BF16 activations, each written once and read once per use): the lift
-    reads the 64 input features and writes V in rows and in channel rows; a
-    layer reads V's channel rows (forward DFT), writes and reads the spectra
-    (mode mixing), the mixed spectra (and their regrouping), reads them and
-    V's rows (inverse DFT + pointwise product) and writes V in both layouts
-    (rows only after the last layer); the projection reads V, writes and
-    reads its hidden layer and writes the FP32 output."""
+    reads the 64 input features and writes V; a layer reads V (forward DFT),
+    writes and reads the spectra (mode mixing), the mixed spectra (and their
+    regrouping), reads them and V again (inverse DFT + pointwise product) and
+    writes the next V; the projection reads V, writes and reads its hidden
+    layer and writes the FP32 output."""
     w, m, L, no = net.width, net.modes, net.layers, net.nout
-    act = NBINS * w * 2                       # one activation layout
+    act = NBINS * w * 2                       # one activation tensor
     spec = 2 * m * w * 2                      # spectra of one layer
-    lift = NBINS * NFEAT * 2 + 2 * act
-    layer = act + 2 * spec + 2 * spec + 2 * spec + act + 2 * act
-    last = layer - act
+    lift = NBINS * NFEAT * 2 + act
+    layer = act + 2 * spec + 2 * spec + 2 * spec + act + act
     proj = act + act + act + NBINS * no * 4
-    return lift + (L - 1) * layer + last + proj
+    return lift + L * layer + proj
 
 
 def _flops_per_profile(net):

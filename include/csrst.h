@@ -244,6 +244,12 @@ typedef struct {
 int csrst_gemm_bf16(const void *A, long long lda, long long stride_a, const void *B, long long ldb,
                     long long stride_b, int M, int N, int K, int batch, const csrst_gemm_epilogue *ep, int *err,
                     void *stream);
+/* The same with an MN-major A when a_mn_major: element (m, k) of batch z at
+ * A[z * stride_a + k * lda + m] (K rows of M contiguous elements; lda >= M, a
+ * multiple of 8); a_mn_major == 0 is csrst_gemm_bf16. */
+int csrst_gemm_bf16_ex(const void *A, long long lda, long long stride_a, int a_mn_major, const void *B,
+                       long long ldb, long long stride_b, int M, int N, int K, int batch,
+                       const csrst_gemm_epilogue *ep, int *err, void *stream);
 /* Polls each mbarrier wait of the GEMM makes before it gives up and sets *err = 1 (for all later
  * GEMM launches of the process; polls == 0 restores the default, 2^24).  A wait that gives up
  * ends every role of its CTA at its next wait; the kernel still waits, with the default bound,

@@ -170,3 +170,22 @@ def test_gemm_vector_epilogue_maps(gpu_lib, case):
         T = o16t.float().cpu().numpy()
         for idx, gz in _scatter(g, M, N, Z, sb=M * N, **tm):
             assert np.abs(T[idx] - gz).max() <= 1e-2 * np.abs(g).max()
+
+
+@pytest.mark.parametrize("M,N,K,Z", [(128, 64, 256, 3), (200, 48, 128, 2), (384, 128, 64, 1)])
+def test_gemm_mn_major_a(gpu_lib, M, N, K, Z):
+    """A read MN-major (K rows of M contiguous values, as the forward DFT reads
+    the activations V[b][n][c]): against the FP64 product of the same BF16
+    values, with ragged M (the second 64-row box of a tile past the matrix)."""
+    import torch
+    from csrst_b200.tensor import check_errors, gemm
+    rng = np.random.default_rng(M + N + K + Z)
+    at, b = bf16(rng, (Z, K, M)), bf16(rng, (Z, N, K))   # at[z][k][m] = A_z[m][k]
+    out = torch.zeros(Z, M, N, dtype=torch.float32, device="cuda")
+    gemm(at.cuda(), b.cuda(), M, N, K, a_mn=True, lda=M, batch=Z, stride_a=K * M, stride_b=N * K, out32=out,
+         sb=M * N)
+    torch.cuda.synchronize()
+    check_errors()
+    for z in range(Z):
+        r = ref(at[z].transpose(0, 1).contiguous(), b[z])
+        assert np.abs(out[z].cpu().numpy() - r).max() <= 1e-4 * np.abs(r).max()
