@@ -490,7 +490,7 @@ def run_surrogate(args):
     t0 = time.perf_counter()
     wakeset.features(variants)
     feat_s = (time.perf_counter() - t0) / len(variants)
-    # about 56 flop per byte: far below the B200's ridge point, so the bound is HBM
+    # about 65 flop per byte: far below the B200's ridge point, so the bound is HBM
     out["inference"] = dict(inf, roofline={"kernel": "the forward pass (tensor-core GEMMs + transposes)",
                                            "bound": "hbm", "achieved": round(inf["gbs"], 1), "peak": hbm,
                                            "unit": "GB/s", "frac": round(inf["gbs"] / hbm, 4),
