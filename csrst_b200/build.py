@@ -30,7 +30,8 @@ def nvcc():
 
 def build(force=False, verbose=False):
     srcs = [HERE / "csrc" / s for s in SRC]
-    deps = srcs + list((HERE / "csrc").glob("*.cuh")) + [HERE.parent / "include" / "csrst.h"]
+    deps = (srcs + list((HERE / "csrc").glob("*.cuh")) + list((HERE / "csrc").glob("*.h")) +
+            [HERE.parent / "include" / "csrst.h"])
     if not force and OUT.exists() and all(OUT.stat().st_mtime >= d.stat().st_mtime for d in deps):
         return OUT
     objdir = HERE / "_build"
