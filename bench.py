@@ -771,6 +771,13 @@ def run_reference(args, world, rank):
 def main():
     args = parse()
     world, rank, local = dist_setup()
+    if args.impl == "reference":
+        # CPU work of rank 0 alone: no process group and no GPU; the other
+        # ranks leave at once with status 0
+        out = run_reference(args, world, rank)
+        if out is not None:
+            print(json.dumps(out), flush=True)
+        return
     if world > 1:
         import torch
         import datetime
@@ -782,7 +789,7 @@ def main():
             torch.cuda.set_device(local)
             out = ensemble_only(args) if rank == 0 else None
         else:
-            out = run_reference(args, world, rank) if args.impl == "reference" else run_b200(args, world, rank, local)
+            out = run_b200(args, world, rank, local)
     finally:
         if world > 1:
             import torch
